@@ -1,0 +1,391 @@
+"""Benchmark of the fire-simulation step (one substep = Sim::step).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload pool_2cm|pool_small_8cm|pallets_5cm|bonfire_10cm]
+
+Workload (default): the 1 m n-heptane pool fire on a 2 cm grid at the named
+shape 150 x 365 x 150 = 8.21 M cells (x, y up, z), a synthetic scene of that
+shape (scene file pyro_b200/scenes/pool_2cm.toml with exact dims).  Before
+timing, the scene is simulated for --preroll-s seconds (default 1.0 s) so the
+flame and plume are developed; then W warm-up substeps; then exactly K timed
+substeps with dt from the CFL rule of the reference frame loop
+(src/main.rs:140-145, 30 frames/s) and statistics on the last substep of
+every frame.  The working set (~1.9 GB) is far larger than the 126 MB L2, so
+no flush is needed between steps.
+
+One JSON line on stdout (rank 0).  `value` is device time per substep (ms,
+lower is better) from CUDA events on the simulation's stream, max over
+ranks.  `e2e` is the same metric through the public Python API (Sim.step +
+Sim.read_stats every substep: the 576-byte parameter block goes host ->
+device and the 4160-byte statistics block device -> host each substep).
+`roofline` is the dominant single kernel's algorithmic bytes per launch over
+its CUDA-event duration, against the measured HBM copy bandwidth.
+`cpu_baseline` is the CPU oracle (a C++ restatement of the reference's
+kernels) on the host cores, timed on rank 0 over whole substeps of the same
+state.
+
+--impl reference times that CPU restatement alone (the reference itself is
+Rust + wgpu, with no Rust toolchain or graphics stack on the box): each step
+is one full substep of the same workload on all host cores.
+
+Multi-GPU (torchrun, one process per GPU): replicas only -- each rank steps
+its own copy of the scene; `value` is max over ranks and `throughput` sums
+cells*substeps/s over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "2cm pool-fire ms/step"
+UNIT = "ms/step"
+WORKLOADS = {
+    "pool_2cm": ("pool_2cm.toml", [150, 365, 150]),
+    "pool_small_8cm": ("pool_small_8cm.toml", [38, 75, 38]),
+    "pallets_5cm": ("pallets_5cm.toml", [120, 240, 120]),
+    "bonfire_10cm": ("bonfire_10cm.toml", [160, 240, 160]),
+}
+# Algorithmic bytes per cell per launch (each distinct array element read or
+# written once at the reference's width; read-modify-write twice).
+ALG_BYTES = {"solid": 68, "curl": 28, "adv_vel1": 24, "adv_vel2": 40, "adv_s1": 76,
+             "adv_s2": 108, "react": 116, "forces": 76, "divergence": 36, "project": 32}
+MG_LEVEL_BYTES = 122.5   # 4 sweeps (96) + restrict (13.5) + prolong (13) per level cell
+COARSE_SWEEP_BYTES = 24.0
+
+
+def mg_cycle_bytes(dims_list):
+    n0 = dims_list[0][0] * dims_list[0][1] * dims_list[0][2]
+    b = 0.0
+    for d in dims_list[:-1]:
+        b += MG_LEVEL_BYTES * d[0] * d[1] * d[2]
+    dc = dims_list[-1]
+    b += 80 * COARSE_SWEEP_BYTES * dc[0] * dc[1] * dc[2]
+    return b, n0
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed
+    region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                  "--format=csv,noheader,nounits", "-lms", "100"],
+                                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            return
+        try:
+            while not self._stop.is_set():
+                line = p.stdout.readline()
+                if not line:
+                    break
+                self.samples.append([x.strip() for x in line.split(",")])
+        finally:
+            p.terminate()
+            try:
+                p.wait(timeout=2)
+            except Exception:
+                p.kill()
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=3)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            try:
+                sm.append(float(s[0]))
+                mx = float(s[1])
+                for n, v in zip(names, s[3:7]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_workload(name):
+    from pyro_b200.scene import Scene
+    fname, dims = WORKLOADS[name]
+    sc = Scene.load(os.path.join(ROOT, "pyro_b200", "scenes", fname))
+    sc.dims_override = list(dims)
+    return sc
+
+
+def cfl_substeps(sc, max_u):
+    """src/main.rs:140-142."""
+    frame_dt = np.float32(1.0) / np.float32(sc.sim.fps)
+    dt_cfl = np.float32(sc.sim.cfl) * np.float32(sc.domain.cell) / np.float32(max(max_u, 1.0))
+    n = max(int(math.ceil(float(frame_dt / dt_cfl))), 1)
+    return n, np.float32(frame_dt / np.float32(n))
+
+
+def cpu_baseline_run(sc, P, sol, fields, n_steps, dt, t0, threads=None):
+    """Time whole oracle substeps of the given state; returns (ms/step, cores)."""
+    import oracle
+    if threads:
+        oracle.set_threads(threads)
+    cores = oracle.max_threads()
+    o = oracle.OracleSim(P, sol, sc.sim.pressure_cycles)
+    for f, a in fields.items():
+        o.write_field(f, a)
+    t = np.float32(t0)
+    times = []
+    for k in range(n_steps):
+        s = time.perf_counter()
+        o.step(float(dt), float(t), 1.0, k == n_steps - 1)
+        times.append(time.perf_counter() - s)
+        t = np.float32(t + dt)
+    o.close()
+    return 1e3 * float(np.mean(times)), cores
+
+
+def run_reference(args):
+    """CPU restatement of the reference step on all host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import oracle
+    from pyro_b200.scene import shapes_array
+    sc = build_workload(args.workload)
+    P = sc.params()
+    g = sc.grid()
+    sh = sc.shapes()
+    dens, kind = sc.slot_tables()
+    sol = oracle.voxelize(shapes_array(sh), len(sh), g.dims[0], g.dims[1], g.dims[2], g.dx,
+                          float(np.float32(sc.sim.ambient_temp)), sc.sim.seed, dens, kind)
+    n, dt = cfl_substeps(sc, 2.0)
+    cores = oracle.max_threads()
+    o = oracle.OracleSim(P, sol, sc.sim.pressure_cycles)
+    t = np.float32(0.0)
+    for k in range(args.warmup):
+        o.step(float(dt), float(t), 1.0, False)
+        t = np.float32(t + dt)
+    times = []
+    for k in range(args.steps):
+        s = time.perf_counter()
+        o.step(float(dt), float(t), 1.0, (k % n) == n - 1)
+        times.append(time.perf_counter() - s)
+        t = np.float32(t + dt)
+    ms = 1e3 * float(np.mean(times))
+    cells = g.dims[0] * g.dims[1] * g.dims[2]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": ms, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": {"workload": f"{args.workload} {g.dims[0]}x{g.dims[1]}x"
+                                        f"{g.dims[2]} (x,y-up,z)", "cells": cells,
+                                        "substeps_per_frame": n, "dt": float(dt)},
+        "cpu_baseline": {"value": ms, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} full substeps of the workload from ignition "
+                                   "(C++ oracle restating the reference's WGSL kernels, OpenMP)"},
+        "e2e": {"value": ms, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "throughput": {"value": cells / (ms * 1e-3), "unit": "cells*substeps/s"},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from pyro_b200 import _abi
+    from pyro_b200.sim import Sim
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+
+    sc = build_workload(args.workload)
+    sim = Sim(sc)
+    cells = sim.cells()
+    lib = _abi.load()
+    stream = torch.cuda.ExternalStream(sim.stream())
+
+    # preroll: develop the flame (frame loop of src/main.rs:139-147)
+    max_u = 2.0
+    t_pre = 0.0
+    while t_pre < args.preroll_s:
+        n, dt = cfl_substeps(sc, max_u)
+        for s in range(n):
+            sim.step(dt, s == n - 1)
+        st = sim.read_stats()
+        max_u = max(st.max_u, 1.0)
+        t_pre += float(n * dt)
+    n, dt = cfl_substeps(sc, max_u)
+    for k in range(args.warmup):
+        sim.step(dt, (k % n) == n - 1)
+    sim.sync()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- timed region: device-resident substeps
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    with ClockSampler(dev) as clocks:
+        e0.record(stream)
+        for k in range(args.steps):
+            sim.step(dt, (k % n) == n - 1)
+        e1.record(stream)
+        e1.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+
+    # ---- e2e through the public API with a host read every substep
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    e2.record(stream)
+    for k in range(args.steps):
+        sim.step(dt, True)
+        st = sim.read_stats()
+    e3.record(stream)
+    e3.synchronize()
+    barrier()
+    ms_e2e = e2.elapsed_time(e3) / args.steps
+
+    # ---- per-kernel device times (CUDA events around each launch)
+    phases = np.zeros(12)
+    nprof = max(3, min(args.steps, 10))
+    buf = (np.zeros(12, np.float32))
+    for k in range(nprof):
+        rc = lib.pyro_sim_profile_step(sim._h, float(dt), float(sim.time), 0.0, 1 if k == 0 else 0,
+                                       buf.ctypes.data_as(__import__("ctypes").c_void_p), 12)
+        _abi.check("pyro_sim_profile_step", rc)
+        sim.time = np.float32(sim.time + dt)
+        phases += buf
+    phases /= nprof
+    names = _abi.PROFILE_PHASES
+    kern = {names[i]: float(phases[i]) for i in range(12)}
+    single = {k: v for k, v in kern.items() if k in ALG_BYTES}
+    dom = max(single, key=single.get)
+    peak, peak_kind = load_peaks()
+    info = sim.info()
+    lvl = [tuple(info.level_dims[l]) for l in range(info.levels)]
+    cyc_bytes, _ = mg_cycle_bytes(lvl)
+    step_bytes = sum(ALG_BYTES.values()) * cells + sc.sim.pressure_cycles * cyc_bytes
+    dom_bytes = ALG_BYTES[dom] * cells
+    achieved = dom_bytes / (kern[dom] * 1e-3) / 1e9
+
+    # gather max over ranks
+    vals = torch.tensor([ms, ms_e2e], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(vals, op=dist.ReduceOp.MAX)
+    ms, ms_e2e = float(vals[0]), float(vals[1])
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        from pyro_b200 import _abi as A
+        fields = {A.F_S0: sim.read_field(A.F_S0), A.F_S1: sim.read_field(A.F_S1),
+                  A.F_SOL: sim.read_field(A.F_SOL), A.F_U: sim.read_field(A.F_U),
+                  A.F_V: sim.read_field(A.F_V), A.F_W: sim.read_field(A.F_W),
+                  A.F_PHI: sim.read_field(A.F_PHI)}
+        cms, cores = cpu_baseline_run(sc, sim.p, fields[A.F_SOL], fields, args.cpu_steps, dt,
+                                      float(sim.time))
+        cpu = {"value": cms, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"{args.cpu_steps} full substeps of the same developed state "
+                         "(C++ oracle restating the reference's WGSL kernels, OpenMP)"}
+
+    launches_per_step = 10 + sc.sim.pressure_cycles * (10 * (info.levels - 1) + 1)
+    line = {
+        "metric": METRIC, "value": ms, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{args.workload} {sim.dims[0]}x{sim.dims[1]}x{sim.dims[2]} "
+                               "(x,y-up,z), developed flame", "cells": cells,
+                   "preroll_s": args.preroll_s, "substeps_per_frame": n, "dt": float(dt),
+                   "ms_per_frame": ms * n, "pressure": f"{sc.sim.pressure_cycles} V-cycles, "
+                   f"{info.levels} levels", "l2": "working set 1.9 GB > L2, no flush",
+                   "parallelism": f"replicas x{world}"},
+        "e2e": {"value": ms_e2e, "unit": UNIT, "h2d_bytes_per_step": 576,
+                "d2h_bytes_per_step": 4 * _abi.STATS_N},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "alg_bytes_per_launch": dom_bytes,
+                     "launch_ms": kern[dom]},
+        "step_roofline": {"alg_bytes": step_bytes, "achieved_gbs": step_bytes / (ms * 1e-3) / 1e9,
+                          "frac": step_bytes / (ms * 1e-3) / 1e9 / peak},
+        "kernels_ms": kern,
+        "throughput": {"value": world * cells / (ms * 1e-3), "unit": "cells*substeps/s"},
+        "cpu_baseline": cpu,
+        "gpu_launches": launches_per_step * args.steps,
+        "clocks": clocks.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="pool_2cm", choices=sorted(WORKLOADS))
+    ap.add_argument("--preroll-s", type=float, default=1.0)
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,279 @@
+/*
+ * pyro_sim.h — C ABI of the B200 (sm_100a) fire-simulation step.
+ *
+ * This library replaces pyro's `Sim` (src/sim.rs:42-531) and the WGSL
+ * simulation kernels it dispatches (src/shaders/{advect,fluid,combust,mg}.wgsl)
+ * with hand-written CUDA kernels behind plain `extern "C"` entry points:
+ * no torch types, no C++ types, plain pointers and sizes.  Every entry point
+ * returns an int status (PYRO_OK == 0, negative on error) and never exits the
+ * process; pyro_last_error() gives a human-readable message for the calling
+ * thread's last failure.
+ *
+ * Layout (identical to the reference, src/shaders/common.wgsl:1-7):
+ *   grid nx*ny*nz cells, y up, cell index  x + nx*(y + ny*z)
+ *   face arrays u, v, w each padded to (nx+1)(ny+1)(nz+1), index
+ *       x + (nx+1)*(y + (ny+1)*z); u at (i, j+1/2, k+1/2) etc.
+ *   s0  = (T [K], Y_F, Y_O2, Y_soot)                 float4 per cell
+ *   s1  = (Y_smoke, q [W/m^3], S [1/s], 0)           float4 per cell
+ *   sol = (material slot, virgin fuel, char, Ts)     float4 per cell
+ *   pyr = (m'' volatiles, m'' char, exposed faces, 0) float4 per cell
+ *   curl= (wx, wy, wz, |w|)                          float4 per cell
+ *   flags uint32 per cell (1 = solid)
+ */
+#ifndef PYRO_SIM_H
+#define PYRO_SIM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define PYRO_OK 0
+#define PYRO_E_INVALID (-1)   /* bad argument (null pointer, size, dims)   */
+#define PYRO_E_CUDA (-2)      /* a CUDA runtime call failed                */
+#define PYRO_E_NOMEM (-3)     /* device or pinned allocation failed        */
+#define PYRO_E_STATE (-4)     /* call not valid in the object's state      */
+#define PYRO_E_NOCONV (-5)    /* iterative solve hit its iteration cap     */
+#define PYRO_E_TIMEOUT (-6)   /* a bounded device-side wait gave up        */
+
+/* Number of floats in the statistics block: 16 scalars + per-layer HRR
+ * (src/sim.rs:12 STATS_N).  Slot meaning (src/shaders/common.wgsl:90-92):
+ * 0 HRR W | 1 radiative loss W | 2 pyrolysis kg/s | 3 soot kg | 4 max T K |
+ * 5 max |u| m/s | 6 fuel gas kg | 7 solid mass kg | 8 smoke kg |
+ * 9 pyrolysing area m^2 | 10 sum r^2 | 11 sum b^2 | 16.. HRR per y layer W */
+#define PYRO_STATS_N 1040
+#define PYRO_MAX_LAYERS 1024
+
+/* ---- the uniform parameter block -------------------------------------- */
+/* Byte-for-byte the reference's `Params` (#[repr(C)], src/scene.rs:424-477,
+ * WGSL struct src/shaders/common.wgsl:14-28): 48 scalars + 8 materials of
+ * 12 floats = 576 bytes.  Material row: a = (density, L_g, T_p, kind),
+ * b = (char yield, emissivity, c_p, k), c = (smoke yield, burn-rate
+ * multiplier, 0, 0) (src/shaders/common.wgsl:9-12). */
+typedef struct PyroParams {
+  uint32_t nx, ny, nz, frame;
+  float dx, dt, time, t0;
+  float rho0, g, cp, yo2;
+  float vort, cs, buoy, smoke_w;
+  float wind_x, wind_z, wind_relax, sponge;
+  float t_ign, s_o2, dhc, tau_min;
+  float soot_form, soot_ox, soot_ox_t, smoke_conv;
+  float kap_gas, h_conv, ign_on, ign_temp;
+  float ign_x, ign_y, ign_z, ign_r;
+  float ign_flux, ign_fuel, char_a, char_e;
+  float dh_char, burnout, layer, rad_len;
+  float h_mass, vort_t, rad_frac, seed;
+  float mats[8][12];
+} PyroParams;
+
+/* ---- fields addressable through read/write/device_ptr ------------------- */
+enum PyroField {
+  PYRO_F_S0 = 0,    /* float4 * N                                         */
+  PYRO_F_S1 = 1,    /* float4 * N                                         */
+  PYRO_F_SOL = 2,   /* float4 * N, the current solid state (sol[sol_cur]) */
+  PYRO_F_PYR = 3,   /* float4 * N                                         */
+  PYRO_F_FLAGS = 4, /* uint32 * N                                         */
+  PYRO_F_CURL = 5,  /* float4 * N                                         */
+  PYRO_F_U = 6,     /* float * Nv, current velocity (vel[cur][0])          */
+  PYRO_F_V = 7,     /* float * Nv                                         */
+  PYRO_F_W = 8,     /* float * Nv                                         */
+  PYRO_F_PHI = 9,   /* float * N, level-0 pressure (warm start)           */
+  PYRO_F_B = 10     /* float * N, level-0 right-hand side                 */
+};
+
+/* Pressure solver modes for pyro_sim_set_solver / pyro_poisson_solve. */
+enum PyroSolver {
+  PYRO_SOLVER_VCYCLE = 0,     /* fixed count of V-cycles (the reference)  */
+  PYRO_SOLVER_VCYCLE_TOL = 1, /* V-cycles until relative residual <= tol  */
+  PYRO_SOLVER_MGPCG = 2,      /* flexible CG, FP32 V-cycle preconditioner */
+  PYRO_SOLVER_MGPCG_BF16 = 3  /* flexible CG, BF16-storage V-cycle        */
+};
+
+typedef struct PyroSolveInfo {
+  int32_t mode;        /* PyroSolver used                                 */
+  int32_t iterations;  /* V-cycles (modes 0,1) or CG iterations (2,3)     */
+  double rel_resid;    /* ||b - A phi|| / ||b|| over fluid cells, FP64     */
+  double b_norm;       /* ||b||                                           */
+  float ms;            /* device time of the solve, CUDA events            */
+  int32_t converged;   /* 1 when rel_resid <= tol                         */
+} PyroSolveInfo;
+
+typedef struct PyroSimInfo {
+  uint32_t nx, ny, nz, levels;
+  uint32_t level_dims[8][3];
+  uint64_t cells, faces;
+  uint64_t device_bytes; /* bytes of device memory the simulation holds  */
+} PyroSimInfo;
+
+/* Thread-local text of the last error (empty string when none). */
+const char* pyro_last_error(void);
+/* ABI version: bump on any signature or struct change. */
+int pyro_abi_version(void);
+
+/* ---- the simulation object (replaces `Sim`) ----------------------------- */
+typedef struct PyroSim PyroSim;
+
+/* Sim::new (src/sim.rs:108-232): allocate every field on the current CUDA
+ * device, set s0 to ambient (t0, 0, yo2, 0), upload the voxelized solid
+ * state `sol_init` (N float4, from Scene::voxelize) into both solid
+ * buffers, build the multigrid hierarchy (<= 4 levels, stop when the
+ * smallest dimension is < 16, halve with ceil, h doubles;
+ * src/sim.rs:142-168) and capture one substep as CUDA graphs.
+ * `pressure_cycles` is the V-cycle count per substep (scene default 4). */
+int pyro_sim_create(const PyroParams* params, const float* sol_init,
+                    uint32_t pressure_cycles, PyroSim** out);
+
+/* Sim::step (src/sim.rs:246-423): one substep.  The host patches dt, time
+ * and ign_on exactly as src/sim.rs:247-249 does; the 576-byte parameter
+ * block is uploaded on the simulation's stream.  Asynchronous: returns
+ * after enqueueing.  When want_stats != 0 the statistics block is cleared
+ * first, accumulated by this substep's kernels and copied to pinned host
+ * memory at the end (src/sim.rs:255-257,415-417). */
+int pyro_sim_step(PyroSim* sim, float dt, float time, float ign_on,
+                  int want_stats);
+
+/* Sim::read_stats raw block (src/sim.rs:510-530): waits for the last
+ * stats substep and copies min(n, PYRO_STATS_N) floats. */
+int pyro_sim_read_stats(PyroSim* sim, float* out, size_t n);
+
+/* Sim::read_scalars generalised (src/sim.rs:494-508): blocking copy of one
+ * field in the reference layout; `bytes` must equal the field's size. */
+int pyro_sim_read_field(PyroSim* sim, int field, void* host, size_t bytes);
+/* Upload a field (checkpoint resume, test set-up). Blocking. */
+int pyro_sim_write_field(PyroSim* sim, int field, const void* host,
+                         size_t bytes);
+/* Borrowed device pointer to a field, valid until the next step or
+ * destroy (zero-copy consumers such as a renderer, src/render.rs:255-270). */
+int pyro_sim_device_ptr(PyroSim* sim, int field, void** dptr, size_t* bytes);
+/* The simulation's CUDA stream (cudaStream_t as void*). */
+int pyro_sim_stream(PyroSim* sim, void** stream);
+/* One substep like pyro_sim_step, launched kernel by kernel (not as a
+ * graph) with CUDA events around each phase; blocks until done and writes
+ * the device time in ms of each phase to ms_out[0..min(n, 12)):
+ * 0 solid, 1 curl, 2 adv_vel1, 3 adv_vel2, 4 adv_s1, 5 adv_s2, 6 react,
+ * 7 forces, 8 divergence, 9 pressure solve, 10 resid+project, 11 total.
+ * The state advances exactly as a pyro_sim_step would. */
+#define PYRO_PROFILE_PHASES 12
+int pyro_sim_profile_step(PyroSim* sim, float dt, float time, float ign_on,
+                          int want_stats, float* ms_out, int n);
+/* Wait for all enqueued work. */
+int pyro_sim_sync(PyroSim* sim);
+int pyro_sim_info(PyroSim* sim, PyroSimInfo* info);
+/* Choose the pressure solver used by later steps.  Mode
+ * PYRO_SOLVER_VCYCLE with the create-time cycle count is the default and
+ * reproduces the reference; the tolerance modes stop at rel. residual
+ * `tol` or after `max_iters`. */
+int pyro_sim_set_solver(PyroSim* sim, int mode, float tol, int max_iters);
+/* Information on the last pressure solve of a tolerance-mode step. */
+int pyro_sim_last_solve(PyroSim* sim, PyroSolveInfo* info);
+int pyro_sim_destroy(PyroSim* sim);
+
+/* ---- scene voxelizer (Scene::voxelize, src/scene.rs:621-667) ---------- */
+enum PyroShapeKind {
+  PYRO_SHAPE_BOX = 0, PYRO_SHAPE_CYL = 1, PYRO_SHAPE_SPHERE = 2,
+  PYRO_SHAPE_POOL = 3
+};
+typedef struct PyroShape {
+  uint32_t kind;  /* PyroShapeKind                                       */
+  uint32_t slot;  /* material slot (index into PyroParams.mats)           */
+  float c[3];     /* box / sphere / pool centre; cylinder end a          */
+  float e[3];     /* box half sizes; cylinder end b                       */
+  float r;        /* cylinder / sphere / pool radius                      */
+  float depth;    /* pool depth                                           */
+  float sin_yaw, cos_yaw; /* box yaw about +y                            */
+} PyroShape;
+/* Fill `sol_out` (device pointer, N float4) with (slot, mass, 0, t0):
+ * shapes are tested in order and the last one containing the cell centre
+ * wins; mass = density * (0.85 + 0.3 * hash(idx ^ seed * 0x9e3779b9)) for
+ * combustible slots and 1 for inert ones.  slot_density/slot_kind are 8
+ * entries each (host pointers). */
+int pyro_voxelize(const PyroShape* shapes, uint32_t n_shapes, uint32_t nx,
+                  uint32_t ny, uint32_t nz, float dx, float t0, uint32_t seed,
+                  const float* slot_density, const uint32_t* slot_kind,
+                  float* sol_out, void* stream);
+
+/* ---- stand-alone pressure Poisson solver ------------------------------- */
+/* The multigrid hierarchy of Sim::new plus the solvers, on caller-owned
+ * level-0 arrays.  Operator (src/shaders/mg.wgsl:2,25-35):
+ * (sum over fluid neighbours phi_n - cnt*phi)/h^2 = b where
+ * out-of-domain neighbours count in cnt with phi = 0 (Dirichlet on the
+ * sides and the top), y < 0 is skipped (Neumann floor) and solid
+ * neighbours are skipped (Neumann at solids).  bc_mode 1 makes the sides
+ * Neumann too (Dirichlet on the top face only). */
+typedef struct PyroPoisson PyroPoisson;
+int pyro_poisson_create(uint32_t nx, uint32_t ny, uint32_t nz, float h,
+                        int bc_mode, PyroPoisson** out);
+/* Copy the level-0 solid flags (device uint32 * N) and rebuild the coarse
+ * flags. */
+int pyro_poisson_set_flags(PyroPoisson* ps, const uint32_t* flags);
+/* Solve in place: phi (device float * N) is the initial guess and the
+ * result; b (device float * N) the right-hand side. */
+int pyro_poisson_solve(PyroPoisson* ps, const float* b, float* phi, int mode,
+                       float tol, int max_iters, PyroSolveInfo* info);
+int pyro_poisson_stream(PyroPoisson* ps, void** stream);
+int pyro_poisson_destroy(PyroPoisson* ps);
+
+/* ---- individual kernels (parity hooks; device pointers) ----------------- */
+/* Each runs one reference kernel once on caller-owned device buffers with
+ * the parameter block `params_dev` (device copy of PyroParams).  `stats`
+ * (device float * PYRO_STATS_N) may be NULL to skip the statistics.
+ * `stream` is a cudaStream_t or NULL for the legacy stream. */
+int pyro_k_solid(const PyroParams* params_dev, uint32_t nx, uint32_t ny,
+                 uint32_t nz, const float* sol_in, float* sol_out, float* pyr,
+                 uint32_t* flags, const float* s0, float* stats, void* stream);
+int pyro_k_curl(const PyroParams* params_dev, uint32_t nx, uint32_t ny,
+                uint32_t nz, const float* u, const float* v, const float* w,
+                float* curl, float* stats, void* stream);
+int pyro_k_adv_vel(const PyroParams* params_dev, uint32_t nx, uint32_t ny,
+                   uint32_t nz, const float* u, const float* v, const float* w,
+                   float* hu, float* hv, float* hw, float* ou, float* ov,
+                   float* ow, const uint32_t* flags, void* stream);
+int pyro_k_adv_scalars(const PyroParams* params_dev, uint32_t nx, uint32_t ny,
+                       uint32_t nz, const float* u, const float* v,
+                       const float* w, const float* s0, const float* s1,
+                       float* h0, float* h1, float* o0, float* o1,
+                       void* stream);
+int pyro_k_react(const PyroParams* params_dev, uint32_t nx, uint32_t ny,
+                 uint32_t nz, const float* s0in, const float* s1in,
+                 float* s0out, float* s1out, const uint32_t* flags,
+                 const float* sol, const float* pyr, const float* curl,
+                 float* stats, void* stream);
+int pyro_k_forces(const PyroParams* params_dev, uint32_t nx, uint32_t ny,
+                  uint32_t nz, float* u, float* v, float* w, const float* s0,
+                  const float* s1, const float* curl, const uint32_t* flags,
+                  void* stream);
+int pyro_k_divergence(const PyroParams* params_dev, uint32_t nx, uint32_t ny,
+                      uint32_t nz, const float* u, const float* v,
+                      const float* w, const float* s1, const uint32_t* flags,
+                      float* b, void* stream);
+int pyro_k_project(const PyroParams* params_dev, uint32_t nx, uint32_t ny,
+                   uint32_t nz, float* u, float* v, float* w, const float* phi,
+                   const uint32_t* flags, void* stream);
+/* Multigrid kernels on one level (dims, spacing h). */
+int pyro_k_mg_smooth(uint32_t nx, uint32_t ny, uint32_t nz, float h,
+                     const float* b, const uint32_t* flags, float* phi,
+                     int color, float omega, void* stream);
+int pyro_k_mg_restrict(uint32_t fnx, uint32_t fny, uint32_t fnz, float fh,
+                       const float* pf, const float* bf, const uint32_t* ff,
+                       uint32_t cnx, uint32_t cny, uint32_t cnz, float* bc,
+                       float* pc, uint32_t* fc, void* stream);
+int pyro_k_mg_prolong(uint32_t fnx, uint32_t fny, uint32_t fnz,
+                      const float* pc, const uint32_t* ff, float* pf,
+                      uint32_t cnx, uint32_t cny, uint32_t cnz,
+                      const uint32_t* fc, void* stream);
+int pyro_k_mg_resid(uint32_t nx, uint32_t ny, uint32_t nz, float h,
+                    const float* phi, const float* b, const uint32_t* flags,
+                    float* stats, void* stream);
+/* Coarsest-level solve: `iters` red-black SOR sweeps (omega) in one
+ * launch (src/sim.rs:473 runs 80 sweeps at omega 1.6 as 160 dispatches). */
+int pyro_k_mg_coarse(uint32_t nx, uint32_t ny, uint32_t nz, float h,
+                     const float* b, const uint32_t* flags, float* phi,
+                     int iters, float omega, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PYRO_SIM_H */

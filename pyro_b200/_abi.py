@@ -1,0 +1,195 @@
+"""ctypes view of the C ABI declared in include/pyro_sim.h.
+
+The structures here are byte-for-byte the C structs; `PyroParams` is the
+reference's 576-byte uniform block (src/scene.rs:424-477,
+src/shaders/common.wgsl:14-28).  `load()` opens the in-tree CUDA library
+and raises when it is missing: there is no CPU fallback for the product path.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+PYRO_OK = 0
+PYRO_E_INVALID = -1
+PYRO_E_CUDA = -2
+PYRO_E_NOMEM = -3
+PYRO_E_STATE = -4
+PYRO_E_NOCONV = -5
+PYRO_E_TIMEOUT = -6
+
+STATS_N = 1040
+MAX_LAYERS = 1024
+ABI_VERSION = 1
+
+F_S0, F_S1, F_SOL, F_PYR, F_FLAGS, F_CURL, F_U, F_V, F_W, F_PHI, F_B = range(11)
+
+PROFILE_PHASES = ["solid", "curl", "adv_vel1", "adv_vel2", "adv_s1", "adv_s2", "react",
+                  "forces", "divergence", "pressure", "project", "total"]
+
+SOLVER_VCYCLE = 0
+SOLVER_VCYCLE_TOL = 1
+SOLVER_MGPCG = 2
+SOLVER_MGPCG_BF16 = 3
+
+SHAPE_BOX, SHAPE_CYL, SHAPE_SPHERE, SHAPE_POOL = range(4)
+
+PARAM_SCALARS = [
+    ("nx", ctypes.c_uint32), ("ny", ctypes.c_uint32), ("nz", ctypes.c_uint32),
+    ("frame", ctypes.c_uint32),
+    ("dx", ctypes.c_float), ("dt", ctypes.c_float), ("time", ctypes.c_float),
+    ("t0", ctypes.c_float),
+    ("rho0", ctypes.c_float), ("g", ctypes.c_float), ("cp", ctypes.c_float),
+    ("yo2", ctypes.c_float),
+    ("vort", ctypes.c_float), ("cs", ctypes.c_float), ("buoy", ctypes.c_float),
+    ("smoke_w", ctypes.c_float),
+    ("wind_x", ctypes.c_float), ("wind_z", ctypes.c_float),
+    ("wind_relax", ctypes.c_float), ("sponge", ctypes.c_float),
+    ("t_ign", ctypes.c_float), ("s_o2", ctypes.c_float), ("dhc", ctypes.c_float),
+    ("tau_min", ctypes.c_float),
+    ("soot_form", ctypes.c_float), ("soot_ox", ctypes.c_float),
+    ("soot_ox_t", ctypes.c_float), ("smoke_conv", ctypes.c_float),
+    ("kap_gas", ctypes.c_float), ("h_conv", ctypes.c_float),
+    ("ign_on", ctypes.c_float), ("ign_temp", ctypes.c_float),
+    ("ign_x", ctypes.c_float), ("ign_y", ctypes.c_float), ("ign_z", ctypes.c_float),
+    ("ign_r", ctypes.c_float),
+    ("ign_flux", ctypes.c_float), ("ign_fuel", ctypes.c_float),
+    ("char_a", ctypes.c_float), ("char_e", ctypes.c_float),
+    ("dh_char", ctypes.c_float), ("burnout", ctypes.c_float),
+    ("layer", ctypes.c_float), ("rad_len", ctypes.c_float),
+    ("h_mass", ctypes.c_float), ("vort_t", ctypes.c_float),
+    ("rad_frac", ctypes.c_float), ("seed", ctypes.c_float),
+]
+
+
+class PyroParams(ctypes.Structure):
+    _fields_ = PARAM_SCALARS + [("mats", (ctypes.c_float * 12) * 8)]
+
+    def to_bytes(self) -> bytes:
+        return bytes(memoryview(self).cast("B"))
+
+    def copy(self) -> "PyroParams":
+        c = PyroParams()
+        ctypes.memmove(ctypes.byref(c), ctypes.byref(self), ctypes.sizeof(self))
+        return c
+
+
+assert ctypes.sizeof(PyroParams) == 576
+
+
+class PyroShape(ctypes.Structure):
+    _fields_ = [
+        ("kind", ctypes.c_uint32), ("slot", ctypes.c_uint32),
+        ("c", ctypes.c_float * 3), ("e", ctypes.c_float * 3),
+        ("r", ctypes.c_float), ("depth", ctypes.c_float),
+        ("sin_yaw", ctypes.c_float), ("cos_yaw", ctypes.c_float),
+    ]
+
+
+class PyroSolveInfo(ctypes.Structure):
+    _fields_ = [
+        ("mode", ctypes.c_int32), ("iterations", ctypes.c_int32),
+        ("rel_resid", ctypes.c_double), ("b_norm", ctypes.c_double),
+        ("ms", ctypes.c_float), ("converged", ctypes.c_int32),
+    ]
+
+
+class PyroSimInfo(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_uint32), ("ny", ctypes.c_uint32), ("nz", ctypes.c_uint32),
+        ("levels", ctypes.c_uint32), ("level_dims", (ctypes.c_uint32 * 3) * 8),
+        ("cells", ctypes.c_uint64), ("faces", ctypes.c_uint64),
+        ("device_bytes", ctypes.c_uint64),
+    ]
+
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpyro_b200.so")
+
+_P = ctypes.c_void_p
+_U32 = ctypes.c_uint32
+_F = ctypes.c_float
+_I = ctypes.c_int
+
+# name -> argtypes; every entry point returns int.
+SIGNATURES = {
+    "pyro_abi_version": [],
+    "pyro_sim_create": [ctypes.POINTER(PyroParams), _P, _U32, ctypes.POINTER(_P)],
+    "pyro_sim_step": [_P, _F, _F, _F, _I],
+    "pyro_sim_read_stats": [_P, _P, ctypes.c_size_t],
+    "pyro_sim_read_field": [_P, _I, _P, ctypes.c_size_t],
+    "pyro_sim_write_field": [_P, _I, _P, ctypes.c_size_t],
+    "pyro_sim_device_ptr": [_P, _I, ctypes.POINTER(_P), ctypes.POINTER(ctypes.c_size_t)],
+    "pyro_sim_stream": [_P, ctypes.POINTER(_P)],
+    "pyro_sim_sync": [_P],
+    "pyro_sim_profile_step": [_P, _F, _F, _F, _I, _P, _I],
+    "pyro_sim_info": [_P, ctypes.POINTER(PyroSimInfo)],
+    "pyro_sim_set_solver": [_P, _I, _F, _I],
+    "pyro_sim_last_solve": [_P, ctypes.POINTER(PyroSolveInfo)],
+    "pyro_sim_destroy": [_P],
+    "pyro_voxelize": [ctypes.POINTER(PyroShape), _U32, _U32, _U32, _U32, _F, _F, _U32,
+                      _P, _P, _P, _P],
+    "pyro_poisson_create": [_U32, _U32, _U32, _F, _I, ctypes.POINTER(_P)],
+    "pyro_poisson_set_flags": [_P, _P],
+    "pyro_poisson_solve": [_P, _P, _P, _I, _F, _I, ctypes.POINTER(PyroSolveInfo)],
+    "pyro_poisson_stream": [_P, ctypes.POINTER(_P)],
+    "pyro_poisson_destroy": [_P],
+    "pyro_k_solid": [_P, _U32, _U32, _U32, _P, _P, _P, _P, _P, _P, _P],
+    "pyro_k_curl": [_P, _U32, _U32, _U32, _P, _P, _P, _P, _P, _P],
+    "pyro_k_adv_vel": [_P, _U32, _U32, _U32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
+    "pyro_k_adv_scalars": [_P, _U32, _U32, _U32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
+    "pyro_k_react": [_P, _U32, _U32, _U32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
+    "pyro_k_forces": [_P, _U32, _U32, _U32, _P, _P, _P, _P, _P, _P, _P, _P],
+    "pyro_k_divergence": [_P, _U32, _U32, _U32, _P, _P, _P, _P, _P, _P, _P],
+    "pyro_k_project": [_P, _U32, _U32, _U32, _P, _P, _P, _P, _P, _P],
+    "pyro_k_mg_smooth": [_U32, _U32, _U32, _F, _P, _P, _P, _I, _F, _P],
+    "pyro_k_mg_restrict": [_U32, _U32, _U32, _F, _P, _P, _P, _U32, _U32, _U32, _P, _P, _P, _P],
+    "pyro_k_mg_prolong": [_U32, _U32, _U32, _P, _P, _P, _U32, _U32, _U32, _P, _P],
+    "pyro_k_mg_resid": [_U32, _U32, _U32, _F, _P, _P, _P, _P, _P],
+    "pyro_k_mg_coarse": [_U32, _U32, _U32, _F, _P, _P, _P, _I, _F, _P],
+}
+
+_lib = None
+
+
+class PyroError(RuntimeError):
+    """A C-ABI call returned a negative status."""
+
+    def __init__(self, name: str, code: int, msg: str):
+        super().__init__(f"{name} failed with status {code}: {msg}")
+        self.code = code
+
+
+def load() -> ctypes.CDLL:
+    """Open libpyro_b200.so (built in-tree by pyro_b200.build).  Raises when
+    the library is absent: the simulation has no CPU path."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            f"pyro_b200 CUDA library not found at {LIB_PATH}; build it with "
+            "`python -m pyro_b200.build` (nvcc, sm_100a)")
+    lib = ctypes.CDLL(LIB_PATH)
+    lib.pyro_last_error.restype = ctypes.c_char_p
+    lib.pyro_last_error.argtypes = []
+    for name, args in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = ctypes.c_int
+        fn.argtypes = args
+    if lib.pyro_abi_version() != ABI_VERSION:
+        raise RuntimeError("libpyro_b200.so ABI version mismatch; rebuild it")
+    _lib = lib
+    return lib
+
+
+def check(name: str, code: int) -> int:
+    if code < 0:
+        msg = _lib.pyro_last_error().decode(errors="replace") if _lib else ""
+        raise PyroError(name, code, msg)
+    return code
+
+
+def call(name: str, *args) -> int:
+    lib = load()
+    return check(name, getattr(lib, name)(*args))

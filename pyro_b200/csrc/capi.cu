@@ -1,0 +1,229 @@
+// capi.cu — C entry points for single kernels, the voxelizer and the error
+// text (include/pyro_sim.h).  The simulation object lives in sim.cu, the
+// Poisson solver in solver.cu.
+#include <cstring>
+#include <string>
+
+#include "runtime.h"
+
+using namespace pyro;
+
+namespace {
+
+thread_local std::string g_err_copy;
+
+inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+int ret(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    set_error(std::string(what) + ": " + cudaGetErrorString(e));
+    return PYRO_E_CUDA;
+  }
+  return PYRO_OK;
+}
+
+bool dims_ok(uint32_t nx, uint32_t ny, uint32_t nz) {
+  return nx >= 2 && ny >= 2 && nz >= 2 &&
+         (uint64_t)(nx + 1) * (ny + 1) * (nz + 1) < (1ull << 31);
+}
+
+}  // namespace
+
+namespace pyro {
+// defined in runtime.cu
+const std::string& last_error_text();
+}
+
+extern "C" {
+
+const char* pyro_last_error(void) {
+  g_err_copy = pyro::last_error_text();
+  return g_err_copy.c_str();
+}
+
+#define KDIMS(name)                                                  \
+  clear_error();                                                     \
+  PYRO_REQUIRE(params_dev, #name ": null parameter block");          \
+  PYRO_REQUIRE(dims_ok(nx, ny, nz), #name ": invalid grid dimensions"); \
+  Dims3 d{(int)nx, (int)ny, (int)nz};
+
+int pyro_k_solid(const PyroParams* params_dev, uint32_t nx, uint32_t ny, uint32_t nz,
+                 const float* sol_in, float* sol_out, float* pyr, uint32_t* flags,
+                 const float* s0, float* stats, void* stream) {
+  KDIMS(pyro_k_solid)
+  PYRO_REQUIRE(sol_in && sol_out && pyr && flags && s0, "pyro_k_solid: null buffer");
+  return ret(launch_solid(params_dev, d, (const float4*)sol_in, (float4*)sol_out, (float4*)pyr,
+                          flags, (const float4*)s0, stats, S(stream)),
+             "pyro_k_solid");
+}
+
+int pyro_k_curl(const PyroParams* params_dev, uint32_t nx, uint32_t ny, uint32_t nz,
+                const float* u, const float* v, const float* w, float* curl, float* stats,
+                void* stream) {
+  KDIMS(pyro_k_curl)
+  PYRO_REQUIRE(u && v && w && curl, "pyro_k_curl: null buffer");
+  return ret(launch_curl(params_dev, d, u, v, w, (float4*)curl, stats, S(stream)), "pyro_k_curl");
+}
+
+int pyro_k_adv_vel(const PyroParams* params_dev, uint32_t nx, uint32_t ny, uint32_t nz,
+                   const float* u, const float* v, const float* w, float* hu, float* hv,
+                   float* hw, float* ou, float* ov, float* ow, const uint32_t* flags,
+                   void* stream) {
+  KDIMS(pyro_k_adv_vel)
+  PYRO_REQUIRE(u && v && w && hu && hv && hw && ou && ov && ow && flags,
+               "pyro_k_adv_vel: null buffer");
+  cudaError_t e = launch_adv_vel1(params_dev, d, u, v, w, hu, hv, hw, S(stream));
+  if (e == cudaSuccess)
+    e = launch_adv_vel2(params_dev, d, u, v, w, hu, hv, hw, ou, ov, ow, flags, S(stream));
+  return ret(e, "pyro_k_adv_vel");
+}
+
+int pyro_k_adv_scalars(const PyroParams* params_dev, uint32_t nx, uint32_t ny, uint32_t nz,
+                       const float* u, const float* v, const float* w, const float* s0,
+                       const float* s1, float* h0, float* h1, float* o0, float* o1,
+                       void* stream) {
+  KDIMS(pyro_k_adv_scalars)
+  PYRO_REQUIRE(u && v && w && s0 && s1 && h0 && h1 && o0 && o1,
+               "pyro_k_adv_scalars: null buffer");
+  cudaError_t e = launch_adv_s1(params_dev, d, u, v, w, (const float4*)s0, (const float4*)s1,
+                                (float4*)h0, (float4*)h1, S(stream));
+  if (e == cudaSuccess)
+    e = launch_adv_s2(params_dev, d, u, v, w, (const float4*)s0, (const float4*)s1,
+                      (const float4*)h0, (const float4*)h1, (float4*)o0, (float4*)o1, S(stream));
+  return ret(e, "pyro_k_adv_scalars");
+}
+
+int pyro_k_react(const PyroParams* params_dev, uint32_t nx, uint32_t ny, uint32_t nz,
+                 const float* s0in, const float* s1in, float* s0out, float* s1out,
+                 const uint32_t* flags, const float* sol, const float* pyr, const float* curl,
+                 float* stats, void* stream) {
+  KDIMS(pyro_k_react)
+  PYRO_REQUIRE(s0in && s1in && s0out && s1out && flags && sol && pyr && curl,
+               "pyro_k_react: null buffer");
+  return ret(launch_react(params_dev, d, (const float4*)s0in, (const float4*)s1in,
+                          (float4*)s0out, (float4*)s1out, flags, (const float4*)sol,
+                          (const float4*)pyr, (const float4*)curl, stats, S(stream)),
+             "pyro_k_react");
+}
+
+int pyro_k_forces(const PyroParams* params_dev, uint32_t nx, uint32_t ny, uint32_t nz, float* u,
+                  float* v, float* w, const float* s0, const float* s1, const float* curl,
+                  const uint32_t* flags, void* stream) {
+  KDIMS(pyro_k_forces)
+  PYRO_REQUIRE(u && v && w && s0 && s1 && curl && flags, "pyro_k_forces: null buffer");
+  return ret(launch_forces(params_dev, d, u, v, w, (const float4*)s0, (const float4*)s1,
+                           (const float4*)curl, flags, S(stream)),
+             "pyro_k_forces");
+}
+
+int pyro_k_divergence(const PyroParams* params_dev, uint32_t nx, uint32_t ny, uint32_t nz,
+                      const float* u, const float* v, const float* w, const float* s1,
+                      const uint32_t* flags, float* b, void* stream) {
+  KDIMS(pyro_k_divergence)
+  PYRO_REQUIRE(u && v && w && s1 && flags && b, "pyro_k_divergence: null buffer");
+  return ret(launch_divergence(params_dev, d, u, v, w, (const float4*)s1, flags, b, S(stream)),
+             "pyro_k_divergence");
+}
+
+int pyro_k_project(const PyroParams* params_dev, uint32_t nx, uint32_t ny, uint32_t nz,
+                   float* u, float* v, float* w, const float* phi, const uint32_t* flags,
+                   void* stream) {
+  KDIMS(pyro_k_project)
+  PYRO_REQUIRE(u && v && w && phi && flags, "pyro_k_project: null buffer");
+  return ret(launch_project(params_dev, d, u, v, w, phi, flags, S(stream)), "pyro_k_project");
+}
+
+int pyro_k_mg_smooth(uint32_t nx, uint32_t ny, uint32_t nz, float h, const float* b,
+                     const uint32_t* flags, float* phi, int color, float omega, void* stream) {
+  clear_error();
+  PYRO_REQUIRE(dims_ok(nx, ny, nz), "pyro_k_mg_smooth: invalid grid dimensions");
+  PYRO_REQUIRE(b && flags && phi, "pyro_k_mg_smooth: null buffer");
+  PYRO_REQUIRE(color == 0 || color == 1, "pyro_k_mg_smooth: color must be 0 or 1");
+  return ret(launch_mg_smooth(Dims3{(int)nx, (int)ny, (int)nz}, h, b, flags, phi, color, omega, 0,
+                              S(stream)),
+             "pyro_k_mg_smooth");
+}
+
+int pyro_k_mg_restrict(uint32_t fnx, uint32_t fny, uint32_t fnz, float fh, const float* pf,
+                       const float* bf, const uint32_t* ff, uint32_t cnx, uint32_t cny,
+                       uint32_t cnz, float* bc, float* pc, uint32_t* fc, void* stream) {
+  clear_error();
+  PYRO_REQUIRE(dims_ok(fnx, fny, fnz) && cnx >= 1 && cny >= 1 && cnz >= 1,
+               "pyro_k_mg_restrict: invalid grid dimensions");
+  PYRO_REQUIRE(cnx == (fnx + 1) / 2 && cny == (fny + 1) / 2 && cnz == (fnz + 1) / 2,
+               "pyro_k_mg_restrict: coarse dims must be ceil(fine / 2)");
+  PYRO_REQUIRE(pf && bf && ff && bc && pc && fc, "pyro_k_mg_restrict: null buffer");
+  return ret(launch_mg_restrict(Dims3{(int)fnx, (int)fny, (int)fnz}, fh, pf, bf, ff,
+                                Dims3{(int)cnx, (int)cny, (int)cnz}, bc, pc, fc, 0, S(stream)),
+             "pyro_k_mg_restrict");
+}
+
+int pyro_k_mg_prolong(uint32_t fnx, uint32_t fny, uint32_t fnz, const float* pc,
+                      const uint32_t* ff, float* pf, uint32_t cnx, uint32_t cny, uint32_t cnz,
+                      const uint32_t* fc, void* stream) {
+  clear_error();
+  PYRO_REQUIRE(dims_ok(fnx, fny, fnz), "pyro_k_mg_prolong: invalid grid dimensions");
+  PYRO_REQUIRE(cnx == (fnx + 1) / 2 && cny == (fny + 1) / 2 && cnz == (fnz + 1) / 2,
+               "pyro_k_mg_prolong: coarse dims must be ceil(fine / 2)");
+  PYRO_REQUIRE(pc && ff && pf && fc, "pyro_k_mg_prolong: null buffer");
+  return ret(launch_mg_prolong(Dims3{(int)fnx, (int)fny, (int)fnz}, pc, ff, pf,
+                               Dims3{(int)cnx, (int)cny, (int)cnz}, fc, S(stream)),
+             "pyro_k_mg_prolong");
+}
+
+int pyro_k_mg_resid(uint32_t nx, uint32_t ny, uint32_t nz, float h, const float* phi,
+                    const float* b, const uint32_t* flags, float* stats, void* stream) {
+  clear_error();
+  PYRO_REQUIRE(dims_ok(nx, ny, nz), "pyro_k_mg_resid: invalid grid dimensions");
+  PYRO_REQUIRE(phi && b && flags && stats, "pyro_k_mg_resid: null buffer");
+  return ret(launch_mg_resid(Dims3{(int)nx, (int)ny, (int)nz}, h, phi, b, flags, 0, stats,
+                             S(stream)),
+             "pyro_k_mg_resid");
+}
+
+int pyro_k_mg_coarse(uint32_t nx, uint32_t ny, uint32_t nz, float h, const float* b,
+                     const uint32_t* flags, float* phi, int iters, float omega, void* stream) {
+  clear_error();
+  PYRO_REQUIRE(dims_ok(nx, ny, nz), "pyro_k_mg_coarse: invalid grid dimensions");
+  PYRO_REQUIRE(b && flags && phi, "pyro_k_mg_coarse: null buffer");
+  PYRO_REQUIRE(iters >= 0, "pyro_k_mg_coarse: iters must be >= 0");
+  Dims3 d{(int)nx, (int)ny, (int)nz};
+  cudaError_t e = cudaSuccess;
+  if (mg_coarse_fits(d)) {
+    e = launch_mg_coarse(d, h, b, flags, phi, iters, omega, 0, S(stream));
+  } else {
+    for (int it = 0; it < iters && e == cudaSuccess; it++)
+      for (int c = 0; c < 2 && e == cudaSuccess; c++)
+        e = launch_mg_smooth(d, h, b, flags, phi, c, omega, 0, S(stream));
+  }
+  return ret(e, "pyro_k_mg_coarse");
+}
+
+int pyro_voxelize(const PyroShape* shapes, uint32_t n_shapes, uint32_t nx, uint32_t ny,
+                  uint32_t nz, float dx, float t0, uint32_t seed, const float* slot_density,
+                  const uint32_t* slot_kind, float* sol_out, void* stream) {
+  clear_error();
+  PYRO_REQUIRE(dims_ok(nx, ny, nz), "pyro_voxelize: invalid grid dimensions");
+  PYRO_REQUIRE(sol_out && slot_density && slot_kind && (shapes || n_shapes == 0),
+               "pyro_voxelize: null argument");
+  PYRO_REQUIRE(dx > 0.0f, "pyro_voxelize: dx must be positive");
+  // small set-up copy of the shape list and slot tables
+  size_t sb = sizeof(PyroShape) * (n_shapes ? n_shapes : 1);
+  DevBuf dshapes, dtab;
+  int rc;
+  if ((rc = dshapes.alloc(sb)) != PYRO_OK) return rc;
+  if ((rc = dtab.alloc(64)) != PYRO_OK) return rc;
+  cudaStream_t st = S(stream);
+  if (n_shapes) PYRO_CU(cudaMemcpyAsync(dshapes.p, shapes, sizeof(PyroShape) * n_shapes,
+                                        cudaMemcpyHostToDevice, st));
+  PYRO_CU(cudaMemcpyAsync(dtab.p, slot_density, 32, cudaMemcpyHostToDevice, st));
+  PYRO_CU(cudaMemcpyAsync((char*)dtab.p + 32, slot_kind, 32, cudaMemcpyHostToDevice, st));
+  PYRO_CU(launch_voxelize(dshapes.as<PyroShape>(), n_shapes, Dims3{(int)nx, (int)ny, (int)nz},
+                          dx, t0, seed, dtab.as<float>(),
+                          reinterpret_cast<const uint32_t*>((char*)dtab.p + 32),
+                          (float4*)sol_out, st));
+  PYRO_CU(cudaStreamSynchronize(st));
+  return PYRO_OK;
+}
+
+}  // extern "C"

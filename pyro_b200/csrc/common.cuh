@@ -1,0 +1,269 @@
+// common.cuh — device helpers shared by the simulation kernels.
+//
+// Field layout and physics helpers follow src/shaders/common.wgsl:1-89;
+// WGSL builtins are written with their specified formulas (mix = a*(1-t) +
+// b*t, smoothstep = t*t*(3-2t), clamp = min(max(x,lo),hi)).  The library is
+// compiled with --fmad=false so FP32 expressions keep the reference's
+// rounding (no contraction into fused multiply-adds).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/pyro_sim.h"
+
+namespace pyro {
+
+// ------------------------------------------------------------ small vectors
+struct F3 { float x, y, z; };
+struct I3 { int x, y, z; };
+
+__device__ __forceinline__ F3 mkf3(float x, float y, float z) { return F3{x, y, z}; }
+__device__ __forceinline__ F3 operator+(F3 a, F3 b) { return F3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ F3 operator-(F3 a, F3 b) { return F3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ F3 operator*(float s, F3 a) { return F3{s * a.x, s * a.y, s * a.z}; }
+__device__ __forceinline__ F3 operator*(F3 a, float s) { return F3{a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ F3 operator/(F3 a, float s) { return F3{a.x / s, a.y / s, a.z / s}; }
+__device__ __forceinline__ F3 tof3(I3 c) { return F3{(float)c.x, (float)c.y, (float)c.z}; }
+__device__ __forceinline__ I3 operator+(I3 a, I3 b) { return I3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ I3 operator-(I3 a, I3 b) { return I3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+
+__device__ __forceinline__ float4 operator+(float4 a, float4 b) {
+  return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
+}
+__device__ __forceinline__ float4 operator-(float4 a, float4 b) {
+  return make_float4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w);
+}
+__device__ __forceinline__ float4 operator*(float s, float4 a) {
+  return make_float4(s * a.x, s * a.y, s * a.z, s * a.w);
+}
+
+// ------------------------------------------------------------ WGSL builtins
+__device__ __forceinline__ float wclamp(float x, float lo, float hi) {
+  return fminf(fmaxf(x, lo), hi);
+}
+__device__ __forceinline__ float wmix(float a, float b, float t) { return a * (1.0f - t) + b * t; }
+__device__ __forceinline__ float4 wmix4(float4 a, float4 b, float t) {
+  return make_float4(wmix(a.x, b.x, t), wmix(a.y, b.y, t), wmix(a.z, b.z, t), wmix(a.w, b.w, t));
+}
+__device__ __forceinline__ float4 min4(float4 a, float4 b) {
+  return make_float4(fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z), fminf(a.w, b.w));
+}
+__device__ __forceinline__ float4 max4(float4 a, float4 b) {
+  return make_float4(fmaxf(a.x, b.x), fmaxf(a.y, b.y), fmaxf(a.z, b.z), fmaxf(a.w, b.w));
+}
+__device__ __forceinline__ float smoothstep(float e0, float e1, float x) {
+  float t = wclamp((x - e0) / (e1 - e0), 0.0f, 1.0f);
+  return t * t * (3.0f - 2.0f * t);
+}
+__device__ __forceinline__ float len3(F3 v) { return sqrtf(v.x * v.x + v.y * v.y + v.z * v.z); }
+__device__ __forceinline__ F3 cross3(F3 a, F3 b) {
+  return F3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ float pow4(float x) { float y = x * x; return y * y; }
+
+constexpr float SIGMA = 5.670374e-8f;
+constexpr float RGAS = 8.314f;
+constexpr float RHO_SOOT = 1800.0f;
+
+__device__ __forceinline__ I3 dir6(int k) {
+  // +x -x +y -y +z -z (common.wgsl:34)
+  return I3{k == 0 ? 1 : (k == 1 ? -1 : 0), k == 2 ? 1 : (k == 3 ? -1 : 0),
+            k == 4 ? 1 : (k == 5 ? -1 : 0)};
+}
+
+// ------------------------------------------------------------------- grid
+struct Grid {
+  int nx, ny, nz;
+  __device__ __forceinline__ bool inb(I3 c) const {
+    return (unsigned)c.x < (unsigned)nx && (unsigned)c.y < (unsigned)ny &&
+           (unsigned)c.z < (unsigned)nz;
+  }
+  __device__ __forceinline__ int sidx(I3 c) const { return c.x + nx * (c.y + ny * c.z); }
+  __device__ __forceinline__ int vidx(I3 c) const {
+    return c.x + (nx + 1) * (c.y + (ny + 1) * c.z);
+  }
+  __device__ __forceinline__ I3 clampC(I3 c) const {
+    return I3{min(max(c.x, 0), nx - 1), min(max(c.y, 0), ny - 1), min(max(c.z, 0), nz - 1)};
+  }
+  // staggered component k: offset and valid upper index (common.wgsl:61-72)
+  __device__ __forceinline__ I3 compHi(int k) const {
+    return I3{nx - 1 + (k == 0), ny - 1 + (k == 1), nz - 1 + (k == 2)};
+  }
+  __device__ __forceinline__ bool compValid(int k, I3 c) const {
+    I3 h = compHi(k);
+    return c.x >= 0 && c.y >= 0 && c.z >= 0 && c.x <= h.x && c.y <= h.y && c.z <= h.z;
+  }
+  // distance outside the open sides/top (common.wgsl:79-82)
+  __device__ __forceinline__ float outside(F3 gc) const {
+    float dx_ = (float)nx, dy_ = (float)ny, dz_ = (float)nz;
+    return fmaxf(fmaxf(-0.5f - gc.x, gc.x - (dx_ - 0.5f)),
+                 fmaxf(fmaxf(-0.5f - gc.z, gc.z - (dz_ - 0.5f)), gc.y - (dy_ - 0.5f)));
+  }
+};
+
+__device__ __forceinline__ F3 compOff(int k) {
+  return F3{k == 0 ? 0.0f : 0.5f, k == 1 ? 0.0f : 0.5f, k == 2 ? 0.0f : 0.5f};
+}
+__device__ __forceinline__ I3 unitI(int k) { return I3{k == 0, k == 1, k == 2}; }
+
+// Physics helpers (common.wgsl:44-58,84-89) on a parameter block.
+__device__ __forceinline__ float rhoOf(const PyroParams& P, float T) {
+  return P.rho0 * P.t0 / fmaxf(T, 200.0f);
+}
+__device__ __forceinline__ float kapP(const PyroParams& P, float T, float yo, float ys) {
+  float fv = rhoOf(P, T) * fmaxf(ys, 0.0f) / RHO_SOOT;
+  return 1862.0f * fv * T + P.kap_gas * wclamp(1.0f - yo / P.yo2, 0.0f, 1.0f);
+}
+__device__ __forceinline__ float cpOf(float T) {
+  return wclamp(1000.0f + 0.24f * (T - 300.0f), 1000.0f, 1450.0f);
+}
+__device__ __forceinline__ float spongeSide(const PyroParams& P, const Grid& g, I3 c) {
+  float e = (float)min(min(c.x, g.nx - 1 - c.x), min(c.z, g.nz - 1 - c.z));
+  return 1.0f - smoothstep(0.0f, P.sponge, e);
+}
+__device__ __forceinline__ float spongeTop(const PyroParams& P, const Grid& g, I3 c) {
+  float h = (float)g.ny;
+  return smoothstep(h - 1.5f * P.sponge, h - 1.0f, (float)c.y);
+}
+
+// --------------------------------------------------------------- samplers
+// Trilinear sample of staggered component X at grid point g0 (tmpl_comp.wgsl:2-15).
+__device__ __forceinline__ float triC(const float* __restrict__ X, const Grid& gr, F3 g0, I3 hi) {
+  float gx = wclamp(g0.x, 0.0f, (float)hi.x);
+  float gy = wclamp(g0.y, 0.0f, (float)hi.y);
+  float gz = wclamp(g0.z, 0.0f, (float)hi.z);
+  int bx = min((int)floorf(gx), hi.x - 1);
+  int by = min((int)floorf(gy), hi.y - 1);
+  int bz = min((int)floorf(gz), hi.z - 1);
+  float fx = gx - (float)bx, fy = gy - (float)by, fz = gz - (float)bz;
+  const int sy = gr.nx + 1, sz = (gr.nx + 1) * (gr.ny + 1);
+  int i = bx + sy * by + sz * bz;
+  float c00 = wmix(__ldg(X + i), __ldg(X + i + 1), fx);
+  float c10 = wmix(__ldg(X + i + sy), __ldg(X + i + sy + 1), fx);
+  float c01 = wmix(__ldg(X + i + sz), __ldg(X + i + sz + 1), fx);
+  float c11 = wmix(__ldg(X + i + sy + sz), __ldg(X + i + sy + sz + 1), fx);
+  return wmix(wmix(c00, c10, fy), wmix(c01, c11, fy), fz);
+}
+// 8-corner min/max (tmpl_comp.wgsl:16-25).
+__device__ __forceinline__ void mmC(const float* __restrict__ X, const Grid& gr, F3 g0, I3 hi,
+                                    float& lo, float& hv) {
+  float gx = wclamp(g0.x, 0.0f, (float)hi.x);
+  float gy = wclamp(g0.y, 0.0f, (float)hi.y);
+  float gz = wclamp(g0.z, 0.0f, (float)hi.z);
+  int bx = min((int)floorf(gx), hi.x - 1);
+  int by = min((int)floorf(gy), hi.y - 1);
+  int bz = min((int)floorf(gz), hi.z - 1);
+  const int sy = gr.nx + 1, sz = (gr.nx + 1) * (gr.ny + 1);
+  int i = bx + sy * by + sz * bz;
+  float v0 = __ldg(X + i), v1 = __ldg(X + i + 1), v2 = __ldg(X + i + sy),
+        v3 = __ldg(X + i + sy + 1), v4 = __ldg(X + i + sz), v5 = __ldg(X + i + sz + 1),
+        v6 = __ldg(X + i + sy + sz), v7 = __ldg(X + i + sy + sz + 1);
+  lo = fminf(fminf(fminf(fminf(fminf(fminf(fminf(1e30f, v0), v1), v2), v3), v4), v5), fminf(v6, v7));
+  hv = fmaxf(fmaxf(fmaxf(fmaxf(fmaxf(fmaxf(fmaxf(-1e30f, v0), v1), v2), v3), v4), v5), fmaxf(v6, v7));
+}
+// Cell-centred vec4 trilinear sample (tmpl_scalar.wgsl:2-15).
+__device__ __forceinline__ float4 triS(const float4* __restrict__ X, const Grid& gr, F3 gc0) {
+  float gx = wclamp(gc0.x, 0.0f, (float)(gr.nx - 1));
+  float gy = wclamp(gc0.y, 0.0f, (float)(gr.ny - 1));
+  float gz = wclamp(gc0.z, 0.0f, (float)(gr.nz - 1));
+  int bx = min((int)floorf(gx), gr.nx - 2);
+  int by = min((int)floorf(gy), gr.ny - 2);
+  int bz = min((int)floorf(gz), gr.nz - 2);
+  float fx = gx - (float)bx, fy = gy - (float)by, fz = gz - (float)bz;
+  const int sy = gr.nx, sz = gr.nx * gr.ny;
+  int i = bx + sy * by + sz * bz;
+  float4 c00 = wmix4(__ldg(X + i), __ldg(X + i + 1), fx);
+  float4 c10 = wmix4(__ldg(X + i + sy), __ldg(X + i + sy + 1), fx);
+  float4 c01 = wmix4(__ldg(X + i + sz), __ldg(X + i + sz + 1), fx);
+  float4 c11 = wmix4(__ldg(X + i + sy + sz), __ldg(X + i + sy + sz + 1), fx);
+  return wmix4(wmix4(c00, c10, fy), wmix4(c01, c11, fy), fz);
+}
+// 8-corner vec4 min/max (tmpl_scalar.wgsl:20-32).
+__device__ __forceinline__ void mmS(const float4* __restrict__ X, const Grid& gr, F3 gc0,
+                                    float4& lo, float4& hi) {
+  float gx = wclamp(gc0.x, 0.0f, (float)(gr.nx - 1));
+  float gy = wclamp(gc0.y, 0.0f, (float)(gr.ny - 1));
+  float gz = wclamp(gc0.z, 0.0f, (float)(gr.nz - 1));
+  int bx = min((int)floorf(gx), gr.nx - 2);
+  int by = min((int)floorf(gy), gr.ny - 2);
+  int bz = min((int)floorf(gz), gr.nz - 2);
+  const int sy = gr.nx, sz = gr.nx * gr.ny;
+  int i = bx + sy * by + sz * bz;
+  lo = make_float4(1e30f, 1e30f, 1e30f, 1e30f);
+  hi = make_float4(-1e30f, -1e30f, -1e30f, -1e30f);
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    float4 v = __ldg(X + i + (j & 1) + sy * ((j >> 1) & 1) + sz * ((j >> 2) & 1));
+    lo = min4(lo, v);
+    hi = max4(hi, v);
+  }
+}
+
+// Staggered velocity and RK2 traces in grid units (vel.wgsl:2-19).
+struct Vel {
+  const float* __restrict__ u;
+  const float* __restrict__ v;
+  const float* __restrict__ w;
+  __device__ __forceinline__ F3 at(const Grid& g, F3 p) const {
+    return F3{triC(u, g, p - compOff(0), g.compHi(0)), triC(v, g, p - compOff(1), g.compHi(1)),
+              triC(w, g, p - compOff(2), g.compHi(2))};
+  }
+  __device__ __forceinline__ F3 back(const Grid& g, float k, F3 x) const {
+    F3 u1 = at(g, x);
+    F3 u2 = at(g, x - (0.5f * k) * u1);
+    return x - k * u2;
+  }
+  __device__ __forceinline__ F3 fwd(const Grid& g, float k, F3 x) const {
+    F3 u1 = at(g, x);
+    F3 u2 = at(g, x + (0.5f * k) * u1);
+    return x + k * u2;
+  }
+};
+
+// -------------------------------------------------------------- statistics
+// Block-wide sum / max then one global atomic per block (replaces the
+// 64-lane tree + CAS add of stats.wgsl:1-36).  Every thread of the block must
+// call it.  `sh` needs 32 floats of shared memory.
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ int lin_tid() {
+  return threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+}
+__device__ __forceinline__ void block_add(float* sh, float v, float* dst) {
+  int t = lin_tid();
+  int nthreads = blockDim.x * blockDim.y * blockDim.z;
+  v = warp_sum(v);
+  __syncthreads();
+  if ((t & 31) == 0) sh[t >> 5] = v;
+  __syncthreads();
+  if (t < 32) {
+    float s = t < (nthreads >> 5) ? sh[t] : 0.0f;
+    s = warp_sum(s);
+    if (t == 0 && s != 0.0f) atomicAdd(dst, s);
+  }
+}
+// max of non-negative values via integer atomicMax on the bits (stats.wgsl:14)
+__device__ __forceinline__ void block_max(float* sh, float v, float* dst) {
+  int t = lin_tid();
+  int nthreads = blockDim.x * blockDim.y * blockDim.z;
+  v = warp_max(fmaxf(v, 0.0f));
+  __syncthreads();
+  if ((t & 31) == 0) sh[t >> 5] = v;
+  __syncthreads();
+  if (t < 32) {
+    float s = t < (nthreads >> 5) ? sh[t] : 0.0f;
+    s = warp_max(s);
+    if (t == 0) atomicMax(reinterpret_cast<unsigned int*>(dst), __float_as_uint(s));
+  }
+}
+
+}  // namespace pyro

@@ -1,0 +1,732 @@
+// k_sim.cu — the fire-simulation kernels of one substep.
+//
+// One thread per cell (or per face position of the padded (nx+1)(ny+1)(nz+1)
+// face grid), 32-wide in x so that every warp touches one contiguous row:
+// coalesced float4 loads of the cell fields and float loads of the faces.
+// Each kernel restates one reference WGSL entry point; the expression order
+// follows the WGSL source so FP32 results match the CPU oracle up to the
+// last-ulp differences of expf.
+//
+//   solid      src/shaders/combust.wgsl:3-137
+//   curl       src/shaders/fluid.wgsl:3-29
+//   adv_vel1   src/shaders/advect.wgsl:4-20
+//   adv_vel2   src/shaders/advect.wgsl:22-70
+//   adv_s1     src/shaders/advect.wgsl:72-91
+//   adv_s2     src/shaders/advect.wgsl:93-125
+//   react      src/shaders/combust.wgsl:139-273
+//   forces     src/shaders/fluid.wgsl:31-109
+//   divergence src/shaders/fluid.wgsl:111-128
+//   project    src/shaders/fluid.wgsl:130-152
+#include "common.cuh"
+#include "kernels.h"
+
+namespace pyro {
+
+namespace {
+
+constexpr int BX = 32, BY = 4, BZ = 2;
+
+inline dim3 grid_for(int x, int y, int z) {
+  return dim3((unsigned)((x + BX - 1) / BX), (unsigned)((y + BY - 1) / BY),
+              (unsigned)((z + BZ - 1) / BZ));
+}
+__device__ __forceinline__ I3 thread_cell() {
+  return I3{(int)(blockIdx.x * BX + threadIdx.x), (int)(blockIdx.y * BY + threadIdx.y),
+            (int)(blockIdx.z * BZ + threadIdx.z)};
+}
+
+// ------------------------------------------------------------------- solid
+struct SolidCtx {
+  const PyroParams& P;
+  Grid g;
+  const float4* __restrict__ solIn;
+  const float4* __restrict__ s0;
+
+  // material slot of a solid state; out-of-range slots clamp to the last
+  // row like the reference's restricted uniform-array indexing.
+  __device__ __forceinline__ static uint32_t slotOf(float4 s) {
+    return min(__float2uint_rz(s.x), 7u);
+  }
+  __device__ __forceinline__ uint32_t kindOf(float4 s) const {
+    return (uint32_t)(P.mats[slotOf(s)][3] + 0.5f);
+  }
+  __device__ __forceinline__ bool isSolidS(float4 s) const {
+    if (kindOf(s) == 2u) return s.y > 0.5f;
+    return s.y + s.z > P.burnout;
+  }
+  __device__ __forceinline__ bool solidN(I3 c) const {
+    if (!g.inb(c)) return false;
+    return isSolidS(__ldg(solIn + g.sidx(c)));
+  }
+  // combust.wgsl:18-39: emission-absorption march along one ray.
+  __device__ float rayIrr(I3 c0, I3 d) const {
+    I3 p = c0;
+    float tr = 1.0f, acc = 0.0f;
+    float dl = len3(tof3(d)) * P.dx;
+#pragma unroll 1
+    for (int s = 0; s < 10; s++) {
+      if (!g.inb(p)) break;
+      int j = g.sidx(p);
+      float4 so = __ldg(solIn + j);
+      if (isSolidS(so)) {
+        acc += tr * pow4(so.w);
+        tr = 0.0f;
+        break;
+      }
+      float4 gg = __ldg(s0 + j);
+      float T = gg.x;
+      // strides 1,1,1,2,2,3,4,5,7,9
+      int stv = s < 3 ? 1 : (s < 5 ? 2 : (s == 5 ? 3 : (s == 6 ? 4 : (s == 7 ? 5 : (s == 8 ? 7 : 9)))));
+      float len = (float)stv * dl;
+      float e = 1.0f - expf(-kapP(P, T, gg.z, gg.w) * len);
+      acc += tr * e * pow4(T);
+      tr *= 1.0f - e;
+      p = I3{p.x + d.x * stv, p.y + d.y * stv, p.z + d.z * stv};
+    }
+    acc += tr * pow4(P.t0);
+    return SIGMA * acc;
+  }
+  // combust.wgsl:41-48: normal + four 45-degree rays.
+  __device__ float faceIrr(I3 c0, int k) const {
+    I3 d = dir6(k);
+    I3 t1{0, 1, 0}, t2{0, 0, 1};
+    if (d.y != 0) t1 = I3{1, 0, 0};
+    if (d.z != 0) t2 = I3{1, 0, 0};
+    return 0.2f * (rayIrr(c0, d) + rayIrr(c0, d + t1) + rayIrr(c0, d - t1) + rayIrr(c0, d + t2) +
+                   rayIrr(c0, d - t2));
+  }
+};
+
+__global__ void __launch_bounds__(256) k_solid(const PyroParams* __restrict__ Pp, Grid g,
+                                               const float4* __restrict__ solIn,
+                                               float4* __restrict__ solOut,
+                                               float4* __restrict__ pyr,
+                                               uint32_t* __restrict__ flags,
+                                               const float4* __restrict__ s0,
+                                               float* __restrict__ stats) {
+  __shared__ float sh[32];
+  const PyroParams& P = *Pp;
+  SolidCtx C{P, g, solIn, s0};
+  I3 c = thread_cell();
+  float stPyro = 0.0f, stMass = 0.0f, stArea = 0.0f;
+  if (g.inb(c)) {
+    int i = g.sidx(c);
+    float4 s = __ldg(solIn + i);
+    float4 o = s;
+    float4 po = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    uint32_t fl = 0u;
+    if (C.isSolidS(s)) {
+      fl = 1u;
+      const float* m = P.mats[SolidCtx::slotOf(s)];
+      uint32_t kind = C.kindOf(s);
+      float fuel = s.y, chr = s.z, Ts = s.w;
+      if (kind != 2u) {
+        float nF = 0.0f, Tg = 0.0f, Yo = 0.0f, qin = 0.0f, qcond = 0.0f;
+        for (int k = 0; k < 6; k++) {
+          I3 n = c + dir6(k);
+          if (n.y < 0) continue;
+          if (C.solidN(n)) {
+            qcond += m[7] / P.dx * (__ldg(solIn + g.sidx(n)).w - Ts);
+            continue;
+          }
+          nF += 1.0f;
+          if (g.inb(n)) {
+            float4 gg = __ldg(s0 + g.sidx(n));
+            Tg += gg.x;
+            Yo += gg.z;
+            qin += C.faceIrr(n, k);
+          } else {
+            Tg += P.t0;
+            Yo += P.yo2;
+            qin += SIGMA * pow4(P.t0);
+          }
+        }
+        float layer = (kind == 1u) ? 0.001f : fminf(P.layer, P.dx);
+        float cap = m[0] * m[6] * layer;
+        if (nF > 0.0f) {
+          Tg /= nF;
+          Yo /= nF;
+          qin /= nF;
+          float qnet = m[5] * (qin - SIGMA * pow4(Ts)) + P.h_conv * (Tg - Ts) + qcond / nF;
+          if (P.ign_on > 0.5f) {
+            F3 pc = (tof3(c) + F3{0.5f, 0.5f, 0.5f}) * P.dx;
+            float dI = len3(pc - F3{P.ign_x, P.ign_y, P.ign_z});
+            qnet += P.ign_flux * wclamp(1.0f - dI / (1.5f * P.ign_r), 0.0f, 1.0f);
+          }
+          float mv = 0.0f, mc = 0.0f;
+          if (kind == 1u) {
+            float Tb = m[2];
+            mv = smoothstep(Tb - 60.0f, Tb, Ts) * fmaxf(qnet, 0.0f) / m[1] * m[9];
+            Ts = fminf(Ts + P.dt * fmaxf(qnet - mv * m[1], fminf(qnet, 0.0f)) / cap, Tb);
+            fuel -= mv * nF / P.dx * P.dt;
+          } else {
+            if (fuel > 0.0f)
+              mv = smoothstep(m[2] - 20.0f, m[2] + 30.0f, Ts) * fmaxf(qnet, 0.0f) / m[1] * m[9];
+            float chi = (kind == 0u) ? m[4] : 0.0f;
+            float kin = P.char_a * expf(-P.char_e / (RGAS * Ts)) * chr * layer;
+            float dif = P.h_mass * rhoOf(P, Tg) * Yo / 1.33f;
+            mc = fminf(kin, dif);
+            Ts += P.dt * (qnet - mv * m[1] + 0.5f * mc * P.dh_char) / cap;
+            float virgin = fminf(mv / (1.0f - chi) * nF / P.dx * P.dt, fuel);
+            fuel -= virgin;
+            chr += virgin * chi - mc * nF / P.dx * P.dt;
+          }
+          stPyro = mv * nF * P.dx * P.dx;
+          stArea = (mv > 1e-4f) ? nF * P.dx * P.dx : 0.0f;
+          po = make_float4(mv, mc, nF, 0.0f);
+        } else {
+          Ts += P.dt * qcond / (m[0] * m[6] * P.dx);
+        }
+        Ts = wclamp(Ts, 250.0f, 2000.0f);
+        fuel = fmaxf(fuel, 0.0f);
+        chr = fmaxf(chr, 0.0f);
+        o = make_float4(s.x, fuel, chr, Ts);
+        if (fuel + chr <= P.burnout) {
+          o = make_float4(0.0f, 0.0f, 0.0f, P.t0);
+          fl = 0u;
+          po = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+      }
+      stMass = (o.y + o.z) * P.dx * P.dx * P.dx * ((kind == 2u) ? 0.0f : 1.0f);
+    }
+    solOut[i] = o;
+    pyr[i] = po;
+    flags[i] = fl;
+  }
+  if (stats) {
+    block_add(sh, stPyro, stats + 2);
+    block_add(sh, stMass, stats + 7);
+    block_add(sh, stArea, stats + 9);
+  }
+}
+
+// -------------------------------------------------------------------- curl
+__device__ __forceinline__ F3 ucell(const Grid& g, const float* __restrict__ u,
+                                    const float* __restrict__ v, const float* __restrict__ w,
+                                    I3 c0) {
+  I3 c = g.clampC(c0);
+  int i = g.vidx(c);
+  const int sy = g.nx + 1, sz = (g.nx + 1) * (g.ny + 1);
+  return 0.5f * F3{__ldg(u + i) + __ldg(u + i + 1), __ldg(v + i) + __ldg(v + i + sy),
+                   __ldg(w + i) + __ldg(w + i + sz)};
+}
+
+__global__ void __launch_bounds__(256) k_curl(const PyroParams* __restrict__ Pp, Grid g,
+                                              const float* __restrict__ u,
+                                              const float* __restrict__ v,
+                                              const float* __restrict__ w,
+                                              float4* __restrict__ curl,
+                                              float* __restrict__ stats) {
+  __shared__ float sh[32];
+  I3 c = thread_cell();
+  float spd = 0.0f;
+  if (g.inb(c)) {
+    const I3 X{1, 0, 0}, Y{0, 1, 0}, Z{0, 0, 1};
+    F3 uxp = ucell(g, u, v, w, c + X), uxm = ucell(g, u, v, w, c - X);
+    F3 uyp = ucell(g, u, v, w, c + Y), uym = ucell(g, u, v, w, c - Y);
+    F3 uzp = ucell(g, u, v, w, c + Z), uzm = ucell(g, u, v, w, c - Z);
+    F3 om = F3{(uyp.z - uym.z) - (uzp.y - uzm.y), (uzp.x - uzm.x) - (uxp.z - uxm.z),
+               (uxp.y - uxm.y) - (uyp.x - uym.x)} /
+            (2.0f * Pp->dx);
+    curl[g.sidx(c)] = make_float4(om.x, om.y, om.z, len3(om));
+    if (stats) spd = len3(ucell(g, u, v, w, c));
+  }
+  if (stats) block_max(sh, spd, stats + 5);
+}
+
+// ---------------------------------------------------------------- advection
+__device__ __forceinline__ const float* pick3(int k, const float* a, const float* b,
+                                              const float* c) {
+  return k == 0 ? a : (k == 1 ? b : c);
+}
+
+__global__ void __launch_bounds__(256) k_adv_vel1(const PyroParams* __restrict__ Pp, Grid g,
+                                                  const float* __restrict__ u,
+                                                  const float* __restrict__ v,
+                                                  const float* __restrict__ w,
+                                                  float* __restrict__ hu,
+                                                  float* __restrict__ hv,
+                                                  float* __restrict__ hw) {
+  I3 c = thread_cell();
+  if (c.x > g.nx || c.y > g.ny || c.z > g.nz) return;
+  const float kk = Pp->dt / Pp->dx;
+  Vel V{u, v, w};
+  int i = g.vidx(c);
+#pragma unroll 1
+  for (int k = 0; k < 3; k++) {
+    if (!g.compValid(k, c)) continue;
+    F3 off = compOff(k);
+    float r = triC(pick3(k, u, v, w), g, V.back(g, kk, tof3(c) + off) - off, g.compHi(k));
+    if (k == 0) hu[i] = r; else if (k == 1) hv[i] = r; else hw[i] = r;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_adv_vel2(const PyroParams* __restrict__ Pp, Grid g,
+                                                  const float* __restrict__ u,
+                                                  const float* __restrict__ v,
+                                                  const float* __restrict__ w,
+                                                  const float* __restrict__ hu,
+                                                  const float* __restrict__ hv,
+                                                  const float* __restrict__ hw,
+                                                  float* __restrict__ ou,
+                                                  float* __restrict__ ov,
+                                                  float* __restrict__ ow,
+                                                  const uint32_t* __restrict__ flags) {
+  I3 c = thread_cell();
+  if (c.x > g.nx || c.y > g.ny || c.z > g.nz) return;
+  const float kk = Pp->dt / Pp->dx;
+  Vel V{u, v, w};
+  int i = g.vidx(c);
+  bool sc = g.inb(c) && __ldg(flags + g.sidx(c)) == 1u;
+#pragma unroll 1
+  for (int k = 0; k < 3; k++) {
+    if (!g.compValid(k, c)) continue;
+    I3 a = c - unitI(k);
+    bool sa = g.inb(a) && __ldg(flags + g.sidx(a)) == 1u;
+    float r;
+    if ((k == 1 && c.y == 0) || sc || sa) {
+      r = 0.0f;
+    } else {
+      F3 off = compOff(k);
+      I3 hi = g.compHi(k);
+      F3 x = tof3(c) + off;
+      F3 b = V.back(g, kk, x) - off;
+      F3 f = V.fwd(g, kk, x) - off;
+      const float* vk = pick3(k, u, v, w);
+      const float* hk = pick3(k, hu, hv, hw);
+      float lo, hv2;
+      mmC(vk, g, b, hi, lo, hv2);
+      r = wclamp(__ldg(hk + i) + 0.5f * (__ldg(vk + i) - triC(hk, g, f, hi)), lo, hv2);
+    }
+    if (k == 0) ou[i] = r; else if (k == 1) ov[i] = r; else ow[i] = r;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_adv_s1(const PyroParams* __restrict__ Pp, Grid g,
+                                                const float* __restrict__ u,
+                                                const float* __restrict__ v,
+                                                const float* __restrict__ w,
+                                                const float4* __restrict__ s0,
+                                                const float4* __restrict__ s1,
+                                                float4* __restrict__ h0,
+                                                float4* __restrict__ h1) {
+  I3 c = thread_cell();
+  if (!g.inb(c)) return;
+  const PyroParams& P = *Pp;
+  const float kk = P.dt / P.dx;
+  Vel V{u, v, w};
+  const F3 half{0.5f, 0.5f, 0.5f};
+  F3 b = V.back(g, kk, tof3(c) + half) - half;
+  float t = wclamp(g.outside(b), 0.0f, 1.0f);
+  int i = g.sidx(c);
+  h0[i] = wmix4(triS(s0, g, b), make_float4(P.t0, 0.0f, P.yo2, 0.0f), t);
+  h1[i] = wmix4(triS(s1, g, b), make_float4(0.0f, 0.0f, 0.0f, 0.0f), t);
+}
+
+__global__ void __launch_bounds__(256) k_adv_s2(const PyroParams* __restrict__ Pp, Grid g,
+                                                const float* __restrict__ u,
+                                                const float* __restrict__ v,
+                                                const float* __restrict__ w,
+                                                const float4* __restrict__ s0,
+                                                const float4* __restrict__ s1,
+                                                const float4* __restrict__ h0,
+                                                const float4* __restrict__ h1,
+                                                float4* __restrict__ o0,
+                                                float4* __restrict__ o1) {
+  I3 c = thread_cell();
+  if (!g.inb(c)) return;
+  const float kk = Pp->dt / Pp->dx;
+  Vel V{u, v, w};
+  const F3 half{0.5f, 0.5f, 0.5f};
+  F3 x = tof3(c) + half;
+  F3 b = V.back(g, kk, x) - half;
+  F3 f = V.fwd(g, kk, x) - half;
+  int i = g.sidx(c);
+  float4 r0 = __ldg(h0 + i), r1 = __ldg(h1 + i);
+  if (g.outside(b) <= 0.0f && g.outside(f) <= 0.0f) {
+    float4 l0, u0, l1, u1;
+    mmS(s0, g, b, l0, u0);
+    mmS(s1, g, b, l1, u1);
+    r0 = min4(max4(r0 + 0.5f * (__ldg(s0 + i) - triS(h0, g, f)), l0), u0);
+    r1 = min4(max4(r1 + 0.5f * (__ldg(s1 + i) - triS(h1, g, f)), l1), u1);
+  }
+  o0[i] = r0;
+  o1[i] = r1;
+}
+
+// ------------------------------------------------------------------- react
+__global__ void __launch_bounds__(256) k_react(const PyroParams* __restrict__ Pp, Grid g,
+                                               const float4* __restrict__ s0in,
+                                               const float4* __restrict__ s1in,
+                                               float4* __restrict__ s0out,
+                                               float4* __restrict__ s1out,
+                                               const uint32_t* __restrict__ flags,
+                                               const float4* __restrict__ sol,
+                                               const float4* __restrict__ pyr,
+                                               const float4* __restrict__ curl,
+                                               float* __restrict__ stats) {
+  __shared__ float sh[32];
+  const PyroParams& P = *Pp;
+  I3 c = thread_cell();
+  float stH = 0, stR = 0, stS = 0, stF = 0, stM = 0, stT = 0;
+  const float dV = P.dx * P.dx * P.dx;
+  bool active = g.inb(c);
+  if (active) {
+    int i = g.sidx(c);
+    if (__ldg(flags + i) == 1u) {
+      s0out[i] = make_float4(__ldg(sol + i).w, 0.0f, P.yo2, 0.0f);
+      s1out[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    } else {
+      float4 a = __ldg(s0in + i);
+      float4 b = __ldg(s1in + i);
+      float nut = (P.cs * P.dx) * (P.cs * P.dx) * __ldg(curl + i).w;
+      if (P.cs > 0.0f) {
+        float kd = fminf(nut / 0.5f * P.dt / (P.dx * P.dx), 0.15f);
+        float4 lapA = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        float lapB = 0.0f;
+        const float4 amb = make_float4(P.t0, 0.0f, P.yo2, 0.0f);
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+          I3 n = c + dir6(k);
+          if (g.inb(n)) {
+            int j = g.sidx(n);
+            if (__ldg(flags + j) != 1u) {
+              lapA = lapA + (__ldg(s0in + j) - a);
+              lapB += __ldg(s1in + j).x - b.x;
+            }
+          } else if (n.y >= 0) {
+            lapA = lapA + (amb - a);
+            lapB -= b.x;
+          }
+        }
+        a = a + kd * lapA;
+        b.x += kd * lapB;
+      }
+      float T = a.x;
+      float yf = fmaxf(a.y, 0.0f);
+      float yo = wclamp(a.z, 0.0f, P.yo2);
+      float ys = fmaxf(a.w, 0.0f);
+      float ym = fmaxf(b.x, 0.0f);
+      float S = 0.0f;
+#pragma unroll 1
+      for (int k = 0; k < 6; k++) {
+        I3 n = c + dir6(k);
+        if (!g.inb(n)) continue;
+        int j = g.sidx(n);
+        if (__ldg(flags + j) != 1u) continue;
+        float4 pr = __ldg(pyr + j);
+        float Ts = __ldg(sol + j).w;
+        float rho = rhoOf(P, T);
+        if (pr.x > 0.0f) {
+          float dm = pr.x * P.dt / (rho * P.dx);
+          float inv = 1.0f / (1.0f + dm);
+          yf = (yf + dm) * inv;
+          yo *= inv;
+          ys *= inv;
+          ym *= inv;
+          T = (T + dm * Ts) * inv;
+          S += pr.x / (rho * P.dx);
+        }
+        T += P.h_conv * (Ts - T) * P.dt / (rho * cpOf(T) * P.dx);
+        if (pr.y > 0.0f) {
+          yo = fmaxf(yo - 1.33f * pr.y * P.dt / (rho * P.dx), 0.0f);
+          T += 0.5f * P.dh_char * pr.y * P.dt / (rho * cpOf(T) * P.dx);
+        }
+      }
+      if (P.ign_on > 0.5f) {
+        F3 pc = (tof3(c) + F3{0.5f, 0.5f, 0.5f}) * P.dx;
+        float dI = len3(pc - F3{P.ign_x, P.ign_y, P.ign_z});
+        float wgt = wclamp(1.0f - dI / P.ign_r, 0.0f, 1.0f);
+        if (wgt > 0.0f) {
+          T = fmaxf(T, wmix(P.t0, P.ign_temp, smoothstep(0.0f, 0.5f, wgt)));
+          yf += P.ign_fuel * wgt * P.dt;
+        }
+      }
+      float rho = rhoOf(P, T);
+      float tauU = 0.049f * P.dx * P.dx / (nut + 1e-6f);
+      float tauG = sqrtf(2.0f * P.dx / P.g);
+      float tau = fmaxf(fminf(tauU, tauG), P.tau_min);
+      float gate = smoothstep(P.t_ign - 100.0f, P.t_ign + 100.0f, T);
+      float lim = fminf(yf, yo / P.s_o2);
+      float dY = lim * (1.0f - expf(-gate * P.dt / tau));
+      yf -= dY;
+      yo = fmaxf(yo - P.s_o2 * dY, 0.0f);
+      T += dY * P.dhc / cpOf(T + 0.5f * dY * P.dhc / cpOf(T));
+      float q = rho * dY * P.dhc / P.dt;
+      float rich = smoothstep(0.0f, 0.03f, yf);
+      ys += P.soot_form * dY * (0.25f + 0.75f * rich);
+      float oxg = smoothstep(P.soot_ox_t, P.soot_ox_t + 300.0f, T) * (yo / P.yo2);
+      ys *= expf(-P.soot_ox * oxg * P.dt);
+      float cold = 1.0f - smoothstep(450.0f, 650.0f, T);
+      float cv = yf * fminf(P.smoke_conv * cold * P.dt, 1.0f);
+      yf -= cv;
+      ym += cv;
+      rho = rhoOf(P, T);
+      float kap = kapP(P, T, yo, ys);
+      float tl = kap * P.rad_len;
+      float esc = (tl > 1e-3f) ? (1.0f - expf(-tl)) / tl : 1.0f;
+      float prad = 4.0f * kap * esc * SIGMA * (pow4(T) - pow4(P.t0));
+      float dTr = fminf(prad * P.dt / (rho * cpOf(T)), 0.5f * fmaxf(T - P.t0, 0.0f));
+      T -= dTr;
+      float prl = dTr * rho * cpOf(T) / P.dt;
+      S += (q - prl) / (rho * cpOf(T) * T);
+      float sp = fmaxf(spongeSide(P, g, c), spongeTop(P, g, c));
+      float dec = 1.0f - expf(-P.dt * 4.0f * sp);
+      T = wmix(T, P.t0, dec);
+      yf *= 1.0f - dec;
+      yo = wmix(yo, P.yo2, dec);
+      ys *= 1.0f - dec;
+      ym *= 1.0f - dec;
+      T = wclamp(T, 250.0f, 2600.0f);
+      s0out[i] = make_float4(T, yf, yo, ys);
+      s1out[i] = make_float4(ym, q, S, 0.0f);
+      if (stats) {
+        rho = rhoOf(P, T);
+        stH = q * dV;
+        stR = prl * dV;
+        stS = rho * ys * dV;
+        stF = rho * yf * dV;
+        stM = rho * ym * dV;
+        stT = T;
+      }
+    }
+  }
+  if (stats) {
+    // per-layer HRR (combust.wgsl:263): cells with q*dV > 1 W.  A warp is
+    // one x-row (blockDim.x == 32), so all its lanes share the layer.
+    float lay = (active && stH > 1.0f) ? stH : 0.0f;
+    lay = warp_sum(lay);
+    if (threadIdx.x == 0 && lay != 0.0f && c.y < PYRO_MAX_LAYERS) atomicAdd(stats + 16 + c.y, lay);
+    block_add(sh, stH, stats + 0);
+    block_add(sh, stR, stats + 1);
+    block_add(sh, stS, stats + 3);
+    block_add(sh, stF, stats + 6);
+    block_add(sh, stM, stats + 8);
+    block_max(sh, stT, stats + 4);
+  }
+}
+
+// ------------------------------------------------------------------ forces
+struct ForceCtx {
+  const PyroParams& P;
+  Grid g;
+  const float4* __restrict__ s0;
+  const float4* __restrict__ s1;
+  const float4* __restrict__ curl;
+  __device__ __forceinline__ float cm(I3 c) const { return __ldg(curl + g.sidx(g.clampC(c))).w; }
+  // fluid.wgsl:167-181: vorticity confinement body force at a cell centre.
+  __device__ F3 confine(I3 c) const {
+    int i = g.sidx(c);
+    float4 a = __ldg(s0 + i);
+    float T = a.x;
+    float smoke = a.w + __ldg(s1 + i).x;
+    float gate = fmaxf(smoothstep(P.vort_t, P.vort_t + 500.0f, T),
+                       0.35f * smoothstep(0.0f, 2e-4f, smoke));
+    if (gate <= 0.0f) return F3{0.0f, 0.0f, 0.0f};
+    const I3 X{1, 0, 0}, Y{0, 1, 0}, Z{0, 0, 1};
+    F3 gr{cm(c + X) - cm(c - X), cm(c + Y) - cm(c - Y), cm(c + Z) - cm(c - Z)};
+    float gl = len3(gr);
+    if (gl < 1e-6f) return F3{0.0f, 0.0f, 0.0f};
+    float4 cw = __ldg(curl + i);
+    F3 f = (P.vort * P.dx) * cross3(gr / gl, F3{cw.x, cw.y, cw.z}) * gate;
+    float fl = len3(f);
+    if (fl > 60.0f) f = f * (60.0f / fl);
+    return f;
+  }
+};
+
+__global__ void __launch_bounds__(256) k_forces(const PyroParams* __restrict__ Pp, Grid g,
+                                                float* __restrict__ u, float* __restrict__ v,
+                                                float* __restrict__ w,
+                                                const float4* __restrict__ s0,
+                                                const float4* __restrict__ s1,
+                                                const float4* __restrict__ curl,
+                                                const uint32_t* __restrict__ flags) {
+  I3 c = thread_cell();
+  if (c.x > g.nx || c.y > g.ny || c.z > g.nz) return;
+  const PyroParams& P = *Pp;
+  ForceCtx C{P, g, s0, s1, curl};
+  int i = g.vidx(c);
+  bool ib = g.inb(c);
+  bool sc = ib && __ldg(flags + g.sidx(c)) == 1u;
+  F3 fcc{0.0f, 0.0f, 0.0f};
+  bool have_cc = false;
+#pragma unroll 1
+  for (int k = 0; k < 3; k++) {
+    if (!g.compValid(k, c)) continue;
+    I3 a = c - unitI(k);
+    bool ia = g.inb(a);
+    bool sa = ia && __ldg(flags + g.sidx(a)) == 1u;
+    if ((k == 1 && c.y == 0) || sc || sa) continue;
+    float f = 0.0f;
+    if (k == 1) {
+      float Ta = P.t0, Tb = P.t0, ma = 0.0f, mb = 0.0f;
+      if (ia) { float4 s = __ldg(s0 + g.sidx(a)); Ta = s.x; ma = s.w + __ldg(s1 + g.sidx(a)).x; }
+      if (ib) { float4 s = __ldg(s0 + g.sidx(c)); Tb = s.x; mb = s.w + __ldg(s1 + g.sidx(c)).x; }
+      if (!ia) { Ta = Tb; ma = mb; }
+      if (!ib) { Tb = Ta; mb = ma; }
+      float Tf = 0.5f * (Ta + Tb);
+      f += P.g * P.buoy * (Tf - P.t0) / Tf - P.g * P.smoke_w * 0.5f * (ma + mb);
+    }
+    F3 fc{0.0f, 0.0f, 0.0f};
+    float n = 0.0f;
+    if (ia) { fc = fc + C.confine(a); n += 1.0f; }
+    if (ib) {
+      if (!have_cc) { fcc = C.confine(c); have_cc = true; }
+      fc = fc + fcc;
+      n += 1.0f;
+    }
+    if (n > 0.0f) f += (k == 0 ? fc.x : (k == 1 ? fc.y : fc.z)) / n;
+    float* vk = k == 0 ? u : (k == 1 ? v : w);
+    float uu = vk[i];
+    uu += f * P.dt;
+    I3 cc = g.clampC(c);
+    float ss = spongeSide(P, g, cc);
+    if (k != 1) {
+      float Tl = P.t0;
+      if (ib) Tl = __ldg(s0 + g.sidx(c)).x;
+      float hot = smoothstep(350.0f, 900.0f, Tl);
+      float kr = P.wind_relax * (1.0f - 0.85f * hot) + 8.0f * ss;
+      float wv = k == 0 ? P.wind_x : P.wind_z;
+      uu = wmix(uu, wv, 1.0f - expf(-kr * P.dt));
+    } else {
+      float st = spongeTop(P, g, cc);
+      if (st > 0.0f) uu = wmix(uu, fmaxf(uu, 0.0f), 1.0f - expf(-8.0f * st * P.dt));
+    }
+    uu = wclamp(uu, -40.0f, 40.0f);
+    vk[i] = uu;
+  }
+}
+
+// -------------------------------------------------------------- divergence
+__global__ void __launch_bounds__(256) k_divergence(const PyroParams* __restrict__ Pp, Grid g,
+                                                    const float* __restrict__ u,
+                                                    const float* __restrict__ v,
+                                                    const float* __restrict__ w,
+                                                    const float4* __restrict__ s1,
+                                                    const uint32_t* __restrict__ flags,
+                                                    float* __restrict__ b) {
+  I3 c = thread_cell();
+  if (!g.inb(c)) return;
+  int i = g.sidx(c);
+  if (__ldg(flags + i) == 1u) { b[i] = 0.0f; return; }
+  int j = g.vidx(c);
+  const int sy = g.nx + 1, sz = (g.nx + 1) * (g.ny + 1);
+  float d = (__ldg(u + j + 1) - __ldg(u + j) + __ldg(v + j + sy) - __ldg(v + j) +
+             __ldg(w + j + sz) - __ldg(w + j)) /
+            Pp->dx;
+  b[i] = d - __ldg(s1 + i).z;
+}
+
+// ----------------------------------------------------------------- project
+__global__ void __launch_bounds__(256) k_project(const PyroParams* __restrict__ Pp, Grid g,
+                                                 float* __restrict__ u, float* __restrict__ v,
+                                                 float* __restrict__ w,
+                                                 const float* __restrict__ phi,
+                                                 const uint32_t* __restrict__ flags) {
+  I3 c = thread_cell();
+  if (c.x > g.nx || c.y > g.ny || c.z > g.nz) return;
+  const float dx = Pp->dx;
+  int i = g.vidx(c);
+  bool ib = g.inb(c);
+  bool sc = ib && __ldg(flags + g.sidx(c)) == 1u;
+  float pc = ib ? __ldg(phi + g.sidx(c)) : 0.0f;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    if (!g.compValid(k, c)) continue;
+    I3 a = c - unitI(k);
+    bool ia = g.inb(a);
+    bool sa = ia && __ldg(flags + g.sidx(a)) == 1u;
+    float* vk = k == 0 ? u : (k == 1 ? v : w);
+    float uu = 0.0f;
+    if (!((k == 1 && c.y == 0) || sc || sa)) {
+      float pa = ia ? __ldg(phi + g.sidx(a)) : 0.0f;
+      uu = vk[i];
+      uu -= (pc - pa) / dx;
+    }
+    vk[i] = uu;
+  }
+}
+
+}  // namespace
+
+// ----------------------------------------------------------------- launchers
+#define PYRO_BLOCK dim3(BX, BY, BZ)
+
+cudaError_t launch_solid(const PyroParams* P, Dims3 d, const float4* solIn, float4* solOut,
+                         float4* pyr, uint32_t* flags, const float4* s0, float* stats,
+                         cudaStream_t st) {
+  Grid g{d.nx, d.ny, d.nz};
+  k_solid<<<grid_for(d.nx, d.ny, d.nz), PYRO_BLOCK, 0, st>>>(P, g, solIn, solOut, pyr, flags, s0,
+                                                           stats);
+  return cudaGetLastError();
+}
+cudaError_t launch_curl(const PyroParams* P, Dims3 d, const float* u, const float* v,
+                        const float* w, float4* curl, float* stats, cudaStream_t st) {
+  Grid g{d.nx, d.ny, d.nz};
+  k_curl<<<grid_for(d.nx, d.ny, d.nz), PYRO_BLOCK, 0, st>>>(P, g, u, v, w, curl, stats);
+  return cudaGetLastError();
+}
+cudaError_t launch_adv_vel1(const PyroParams* P, Dims3 d, const float* u, const float* v,
+                            const float* w, float* hu, float* hv, float* hw, cudaStream_t st) {
+  Grid g{d.nx, d.ny, d.nz};
+  k_adv_vel1<<<grid_for(d.nx + 1, d.ny + 1, d.nz + 1), PYRO_BLOCK, 0, st>>>(P, g, u, v, w, hu, hv,
+                                                                           hw);
+  return cudaGetLastError();
+}
+cudaError_t launch_adv_vel2(const PyroParams* P, Dims3 d, const float* u, const float* v,
+                            const float* w, const float* hu, const float* hv, const float* hw,
+                            float* ou, float* ov, float* ow, const uint32_t* flags,
+                            cudaStream_t st) {
+  Grid g{d.nx, d.ny, d.nz};
+  k_adv_vel2<<<grid_for(d.nx + 1, d.ny + 1, d.nz + 1), PYRO_BLOCK, 0, st>>>(
+      P, g, u, v, w, hu, hv, hw, ou, ov, ow, flags);
+  return cudaGetLastError();
+}
+cudaError_t launch_adv_s1(const PyroParams* P, Dims3 d, const float* u, const float* v,
+                          const float* w, const float4* s0, const float4* s1, float4* h0,
+                          float4* h1, cudaStream_t st) {
+  Grid g{d.nx, d.ny, d.nz};
+  k_adv_s1<<<grid_for(d.nx, d.ny, d.nz), PYRO_BLOCK, 0, st>>>(P, g, u, v, w, s0, s1, h0, h1);
+  return cudaGetLastError();
+}
+cudaError_t launch_adv_s2(const PyroParams* P, Dims3 d, const float* u, const float* v,
+                          const float* w, const float4* s0, const float4* s1, const float4* h0,
+                          const float4* h1, float4* o0, float4* o1, cudaStream_t st) {
+  Grid g{d.nx, d.ny, d.nz};
+  k_adv_s2<<<grid_for(d.nx, d.ny, d.nz), PYRO_BLOCK, 0, st>>>(P, g, u, v, w, s0, s1, h0, h1, o0,
+                                                            o1);
+  return cudaGetLastError();
+}
+cudaError_t launch_react(const PyroParams* P, Dims3 d, const float4* s0in, const float4* s1in,
+                         float4* s0out, float4* s1out, const uint32_t* flags, const float4* sol,
+                         const float4* pyr, const float4* curl, float* stats, cudaStream_t st) {
+  Grid g{d.nx, d.ny, d.nz};
+  k_react<<<grid_for(d.nx, d.ny, d.nz), PYRO_BLOCK, 0, st>>>(P, g, s0in, s1in, s0out, s1out, flags,
+                                                           sol, pyr, curl, stats);
+  return cudaGetLastError();
+}
+cudaError_t launch_forces(const PyroParams* P, Dims3 d, float* u, float* v, float* w,
+                          const float4* s0, const float4* s1, const float4* curl,
+                          const uint32_t* flags, cudaStream_t st) {
+  Grid g{d.nx, d.ny, d.nz};
+  k_forces<<<grid_for(d.nx + 1, d.ny + 1, d.nz + 1), PYRO_BLOCK, 0, st>>>(P, g, u, v, w, s0, s1,
+                                                                         curl, flags);
+  return cudaGetLastError();
+}
+cudaError_t launch_divergence(const PyroParams* P, Dims3 d, const float* u, const float* v,
+                              const float* w, const float4* s1, const uint32_t* flags, float* b,
+                              cudaStream_t st) {
+  Grid g{d.nx, d.ny, d.nz};
+  k_divergence<<<grid_for(d.nx, d.ny, d.nz), PYRO_BLOCK, 0, st>>>(P, g, u, v, w, s1, flags, b);
+  return cudaGetLastError();
+}
+cudaError_t launch_project(const PyroParams* P, Dims3 d, float* u, float* v, float* w,
+                           const float* phi, const uint32_t* flags, cudaStream_t st) {
+  Grid g{d.nx, d.ny, d.nz};
+  k_project<<<grid_for(d.nx + 1, d.ny + 1, d.nz + 1), PYRO_BLOCK, 0, st>>>(P, g, u, v, w, phi,
+                                                                          flags);
+  return cudaGetLastError();
+}
+
+}  // namespace pyro

@@ -1,0 +1,86 @@
+// kernels.h — host-side launchers of the simulation and multigrid kernels
+// (internal to libpyro_b200; the C ABI is include/pyro_sim.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/pyro_sim.h"
+
+namespace pyro {
+
+struct Dims3 {
+  int nx, ny, nz;
+  size_t cells() const { return (size_t)nx * ny * nz; }
+  size_t faces() const { return (size_t)(nx + 1) * (ny + 1) * (nz + 1); }
+};
+
+// Simulation kernels; P is a device pointer to the parameter block and
+// stats (device, PYRO_STATS_N floats) may be null.  All return the launch
+// status.
+cudaError_t launch_solid(const PyroParams* P, Dims3 d, const float4* solIn, float4* solOut,
+                         float4* pyr, uint32_t* flags, const float4* s0, float* stats,
+                         cudaStream_t st);
+cudaError_t launch_curl(const PyroParams* P, Dims3 d, const float* u, const float* v,
+                        const float* w, float4* curl, float* stats, cudaStream_t st);
+cudaError_t launch_adv_vel1(const PyroParams* P, Dims3 d, const float* u, const float* v,
+                            const float* w, float* hu, float* hv, float* hw, cudaStream_t st);
+cudaError_t launch_adv_vel2(const PyroParams* P, Dims3 d, const float* u, const float* v,
+                            const float* w, const float* hu, const float* hv, const float* hw,
+                            float* ou, float* ov, float* ow, const uint32_t* flags,
+                            cudaStream_t st);
+cudaError_t launch_adv_s1(const PyroParams* P, Dims3 d, const float* u, const float* v,
+                          const float* w, const float4* s0, const float4* s1, float4* h0,
+                          float4* h1, cudaStream_t st);
+cudaError_t launch_adv_s2(const PyroParams* P, Dims3 d, const float* u, const float* v,
+                          const float* w, const float4* s0, const float4* s1, const float4* h0,
+                          const float4* h1, float4* o0, float4* o1, cudaStream_t st);
+cudaError_t launch_react(const PyroParams* P, Dims3 d, const float4* s0in, const float4* s1in,
+                         float4* s0out, float4* s1out, const uint32_t* flags, const float4* sol,
+                         const float4* pyr, const float4* curl, float* stats, cudaStream_t st);
+cudaError_t launch_forces(const PyroParams* P, Dims3 d, float* u, float* v, float* w,
+                          const float4* s0, const float4* s1, const float4* curl,
+                          const uint32_t* flags, cudaStream_t st);
+cudaError_t launch_divergence(const PyroParams* P, Dims3 d, const float* u, const float* v,
+                              const float* w, const float4* s1, const uint32_t* flags, float* b,
+                              cudaStream_t st);
+cudaError_t launch_project(const PyroParams* P, Dims3 d, float* u, float* v, float* w,
+                           const float* phi, const uint32_t* flags, cudaStream_t st);
+
+// Multigrid level kernels (src/shaders/mg.wgsl).  bc_mode 0 = reference
+// boundaries, 1 = Dirichlet on the top face only.
+cudaError_t launch_mg_smooth(Dims3 d, float h, const float* b, const uint32_t* f, float* p,
+                             int color, float omega, int bc_mode, cudaStream_t st);
+cudaError_t launch_mg_restrict(Dims3 df, float hf, const float* pf, const float* bf,
+                               const uint32_t* ff, Dims3 dc, float* bc, float* pc, uint32_t* fc,
+                               int bc_mode, cudaStream_t st);
+cudaError_t launch_mg_prolong(Dims3 df, const float* pc, const uint32_t* ff, float* pf, Dims3 dc,
+                              const uint32_t* fc, cudaStream_t st);
+cudaError_t launch_mg_resid(Dims3 d, float h, const float* p, const float* b, const uint32_t* f,
+                            int bc_mode, float* stats, cudaStream_t st);
+// Whole coarsest-level solve in one CTA (shared memory); returns
+// cudaErrorInvalidValue when the level does not fit.
+bool mg_coarse_fits(Dims3 d);
+cudaError_t launch_mg_coarse(Dims3 d, float h, const float* b, const uint32_t* f, float* p,
+                             int iters, float omega, int bc_mode, cudaStream_t st);
+
+// BF16-storage variants (phi and b as __nv_bfloat16, FP32 arithmetic) for
+// the low-precision MGPCG preconditioner; pointers are bf16 arrays.
+cudaError_t launch_f32_to_bf16(const float* a, void* b, size_t n, cudaStream_t st);
+cudaError_t launch_bf16_to_f32(const void* a, float* b, size_t n, cudaStream_t st);
+cudaError_t launch_mg_smooth_bf16(Dims3 d, float h, const void* b, const uint32_t* f, void* p,
+                                  int color, float omega, int bc_mode, cudaStream_t st);
+cudaError_t launch_mg_restrict_bf16(Dims3 df, float hf, const void* pf, const void* bf,
+                                    const uint32_t* ff, Dims3 dc, void* bc, void* pc,
+                                    uint32_t* fc, int bc_mode, cudaStream_t st);
+cudaError_t launch_mg_prolong_bf16(Dims3 df, const void* pc, const uint32_t* ff, void* pf,
+                                   Dims3 dc, const uint32_t* fc, cudaStream_t st);
+cudaError_t launch_mg_coarse_bf16(Dims3 d, float h, const void* b, const uint32_t* f, void* p,
+                                  int iters, float omega, int bc_mode, cudaStream_t st);
+
+// Voxelizer.
+cudaError_t launch_voxelize(const PyroShape* shapes_dev, uint32_t n, Dims3 d, float dx, float t0,
+                            uint32_t seed, const float* dens_dev, const uint32_t* kind_dev,
+                            float4* sol, cudaStream_t st);
+
+}  // namespace pyro

@@ -1,0 +1,163 @@
+// runtime.cu — error state, device buffers, multigrid schedule.
+#include <cstring>
+
+#include "runtime.h"
+
+namespace pyro {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+void clear_error() { g_last_error.clear(); }
+const std::string& last_error_text() { return g_last_error; }
+
+int DevBuf::alloc(size_t n) {
+  release();
+  if (n == 0) return PYRO_OK;
+  cudaError_t e = cudaMalloc(&p, n);
+  if (e != cudaSuccess) {
+    p = nullptr;
+    set_error(std::string("cudaMalloc(") + std::to_string(n) + "): " + cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? PYRO_E_NOMEM : PYRO_E_CUDA;
+  }
+  bytes = n;
+  e = cudaMemset(p, 0, n);
+  if (e != cudaSuccess) {
+    set_error(std::string("cudaMemset: ") + cudaGetErrorString(e));
+    return PYRO_E_CUDA;
+  }
+  return PYRO_OK;
+}
+
+void DevBuf::release() {
+  if (p) cudaFree(p);
+  p = nullptr;
+  bytes = 0;
+}
+
+std::vector<Dims3> mg_level_dims(Dims3 d, int max_levels) {
+  std::vector<Dims3> v;
+  for (int l = 0; l < max_levels; l++) {
+    v.push_back(d);
+    if (std::min(std::min(d.nx, d.ny), d.nz) < 16) break;
+    d = Dims3{(d.nx + 1) / 2, (d.ny + 1) / 2, (d.nz + 1) / 2};
+  }
+  return v;
+}
+
+int Multigrid::init(Dims3 d0, float h0, int bc) {
+  bc_mode = bc;
+  dims = mg_level_dims(d0, 4);
+  size_t L = dims.size();
+  h.resize(L);
+  phi.assign(L, nullptr);
+  b.assign(L, nullptr);
+  f.assign(L, nullptr);
+  own_phi.resize(L);
+  own_b.resize(L);
+  own_f.resize(L);
+  float hh = h0;
+  for (size_t l = 0; l < L; l++) {
+    h[l] = hh;
+    hh *= 2.0f;
+    if (l == 0) continue;
+    size_t n = dims[l].cells();
+    int rc;
+    if ((rc = own_phi[l].alloc(n * 4)) != PYRO_OK) return rc;
+    if ((rc = own_b[l].alloc(n * 4)) != PYRO_OK) return rc;
+    if ((rc = own_f[l].alloc(n * 4)) != PYRO_OK) return rc;
+    phi[l] = own_phi[l].as<float>();
+    b[l] = own_b[l].as<float>();
+    f[l] = own_f[l].as<uint32_t>();
+  }
+  coarse_one_cta = mg_coarse_fits(dims.back());
+  return PYRO_OK;
+}
+
+size_t Multigrid::device_bytes() const {
+  size_t s = 0;
+  for (size_t l = 1; l < dims.size(); l++) s += own_phi[l].bytes + own_b[l].bytes + own_f[l].bytes;
+  return s;
+}
+
+cudaError_t Multigrid::smooth(int l, int iters, bool coarse, cudaStream_t st) {
+  float om = coarse ? 1.6f : 1.0f;
+  if (coarse && coarse_one_cta)
+    return launch_mg_coarse(dims[l], h[l], b[l], f[l], phi[l], iters, om, bc_mode, st);
+  for (int it = 0; it < iters; it++)
+    for (int c = 0; c < 2; c++) {
+      cudaError_t e = launch_mg_smooth(dims[l], h[l], b[l], f[l], phi[l], c, om, bc_mode, st);
+      if (e != cudaSuccess) return e;
+    }
+  return cudaSuccess;
+}
+
+cudaError_t Multigrid::vcycles(int cycles, cudaStream_t st) {
+  int nl = (int)dims.size();
+  cudaError_t e;
+  for (int cy = 0; cy < cycles; cy++) {
+    for (int l = 0; l < nl - 1; l++) {
+      if ((e = smooth(l, 2, false, st)) != cudaSuccess) return e;
+      e = launch_mg_restrict(dims[l], h[l], phi[l], b[l], f[l], dims[l + 1], b[l + 1],
+                             phi[l + 1], const_cast<uint32_t*>(f[l + 1]), bc_mode, st);
+      if (e != cudaSuccess) return e;
+    }
+    if ((e = smooth(nl - 1, 80, true, st)) != cudaSuccess) return e;
+    for (int l = nl - 2; l >= 0; l--) {
+      e = launch_mg_prolong(dims[l], phi[l + 1], f[l], phi[l], dims[l + 1], f[l + 1], st);
+      if (e != cudaSuccess) return e;
+      if ((e = smooth(l, 2, false, st)) != cudaSuccess) return e;
+    }
+  }
+  return cudaSuccess;
+}
+
+cudaError_t Multigrid::vcycles_bf16(int cycles, cudaStream_t st, DevBuf* bphi, DevBuf* bb) {
+  int nl = (int)dims.size();
+  for (int l = 0; l < nl; l++) {
+    size_t need = dims[l].cells() * 2;
+    if (bphi[l].bytes != need) {
+      if (bphi[l].alloc(need) != PYRO_OK || bb[l].alloc(need) != PYRO_OK)
+        return cudaErrorMemoryAllocation;
+    }
+  }
+  size_t n0 = dims[0].cells();
+  cudaError_t e;
+  // level 0: b <- r (BF16), phi <- current guess (BF16)
+  if ((e = launch_f32_to_bf16(b[0], bb[0].p, n0, st)) != cudaSuccess) return e;
+  if ((e = launch_f32_to_bf16(phi[0], bphi[0].p, n0, st)) != cudaSuccess) return e;
+  auto smooth16 = [&](int l, int iters, bool coarse) -> cudaError_t {
+    float om = coarse ? 1.6f : 1.0f;
+    if (coarse && coarse_one_cta)
+      return launch_mg_coarse_bf16(dims[l], h[l], bb[l].p, f[l], bphi[l].p, iters, om, bc_mode,
+                                   st);
+    for (int it = 0; it < iters; it++)
+      for (int c = 0; c < 2; c++) {
+        cudaError_t e2 =
+            launch_mg_smooth_bf16(dims[l], h[l], bb[l].p, f[l], bphi[l].p, c, om, bc_mode, st);
+        if (e2 != cudaSuccess) return e2;
+      }
+    return cudaSuccess;
+  };
+  for (int cy = 0; cy < cycles; cy++) {
+    for (int l = 0; l < nl - 1; l++) {
+      if ((e = smooth16(l, 2, false)) != cudaSuccess) return e;
+      e = launch_mg_restrict_bf16(dims[l], h[l], bphi[l].p, bb[l].p, f[l], dims[l + 1],
+                                  bb[l + 1].p, bphi[l + 1].p, const_cast<uint32_t*>(f[l + 1]),
+                                  bc_mode, st);
+      if (e != cudaSuccess) return e;
+    }
+    if ((e = smooth16(nl - 1, 80, true)) != cudaSuccess) return e;
+    for (int l = nl - 2; l >= 0; l--) {
+      e = launch_mg_prolong_bf16(dims[l], bphi[l + 1].p, f[l], bphi[l].p, dims[l + 1], f[l + 1],
+                                 st);
+      if (e != cudaSuccess) return e;
+      if ((e = smooth16(l, 2, false)) != cudaSuccess) return e;
+    }
+  }
+  return launch_bf16_to_f32(bphi[0].p, phi[0], n0, st);
+}
+
+}  // namespace pyro

@@ -1,0 +1,424 @@
+// solver.cu — pressure solvers (fixed V-cycles as in src/sim.rs:451-491,
+// V-cycles to a tolerance, and flexible MGPCG).
+//
+// MGPCG solves the reference system A phi = b (A negative semi-definite,
+// src/shaders/mg.wgsl:25-35) by CG on -A: with r = b - A phi, z = V(r) one
+// V-cycle from a zero guess, q = A p:
+//   alpha = <r,z> / <p,q>,  phi += alpha p,  r -= alpha q,
+//   beta  = <z_new, r_new - r_old> / <z_old, r_old> = -<z_new, q> / <p,q>
+// (Polak-Ribiere form, valid for the non-symmetric V-cycle), p = z + beta p.
+// Vectors are FP32; every dot product and norm is accumulated in FP64.
+#include <cmath>
+#include <cstring>
+
+#include "solver.h"
+
+namespace pyro {
+
+namespace {
+
+constexpr int BX = 32, BY = 4, BZ = 2;
+inline dim3 grid_for(Dims3 d) {
+  return dim3((unsigned)((d.nx + BX - 1) / BX), (unsigned)((d.ny + BY - 1) / BY),
+              (unsigned)((d.nz + BZ - 1) / BZ));
+}
+
+enum { SC_RZ = 0, SC_PQ, SC_RR, SC_BB, SC_ZQ, SC_RZN, SC_N = 8 };
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+// Block sum in FP64, one atomic per block.  Every thread must call.
+__device__ __forceinline__ void block_add_d(double* sh, double v, double* dst) {
+  int t = threadIdx.x + BX * (threadIdx.y + BY * threadIdx.z);
+  v = warp_sum_d(v);
+  __syncthreads();
+  if ((t & 31) == 0) sh[t >> 5] = v;
+  __syncthreads();
+  if (t < 32) {
+    double s = t < (BX * BY * BZ) / 32 ? sh[t] : 0.0;
+    s = warp_sum_d(s);
+    if (t == 0 && s != 0.0) atomicAdd(dst, s);
+  }
+}
+
+struct L3 {
+  int nx, ny, nz;
+  __device__ __forceinline__ bool inb(int x, int y, int z) const {
+    return (unsigned)x < (unsigned)nx && (unsigned)y < (unsigned)ny && (unsigned)z < (unsigned)nz;
+  }
+  __device__ __forceinline__ int idx(int x, int y, int z) const { return x + nx * (y + ny * z); }
+};
+
+// (A v)_i = (sum fluid nbrs v - cnt v_i) / h^2, 0 in solids.
+__device__ __forceinline__ float apply_A(const L3& d, float ih2, const float* __restrict__ v,
+                                         const uint32_t* __restrict__ f, int x, int y, int z,
+                                         int bc_mode, float vi) {
+  float sum = 0.0f, cnt = 0.0f;
+#pragma unroll
+  for (int k = 0; k < 6; k++) {
+    int a = x + (k == 0) - (k == 1), b = y + (k == 2) - (k == 3), c = z + (k == 4) - (k == 5);
+    if (b < 0) continue;
+    if (!d.inb(a, b, c)) {
+      if (bc_mode == 0 || b >= d.ny) cnt += 1.0f;
+      continue;
+    }
+    int j = d.idx(a, b, c);
+    if (__ldg(f + j) == 1u) continue;
+    sum += __ldg(v + j);
+    cnt += 1.0f;
+  }
+  return (sum - cnt * vi) * ih2;
+}
+
+#define CELL_PROLOGUE                          \
+  int x = blockIdx.x * BX + threadIdx.x;       \
+  int y = blockIdx.y * BY + threadIdx.y;       \
+  int z = blockIdx.z * BZ + threadIdx.z;       \
+  bool in = d.inb(x, y, z);                    \
+  int i = in ? d.idx(x, y, z) : 0;             \
+  bool fluid = in && __ldg(f + i) != 1u;
+
+__global__ void __launch_bounds__(256) k_resid(L3 d, float ih2, const float* __restrict__ phi,
+                                               const float* __restrict__ b,
+                                               const uint32_t* __restrict__ f, int bc_mode,
+                                               float* __restrict__ r, double* __restrict__ sc) {
+  __shared__ double sh[32];
+  CELL_PROLOGUE
+  double r2 = 0.0, b2 = 0.0;
+  if (in) {
+    float ri = 0.0f;
+    if (fluid) {
+      float bi = __ldg(b + i);
+      ri = bi - apply_A(d, ih2, phi, f, x, y, z, bc_mode, __ldg(phi + i));
+      r2 = (double)ri * (double)ri;
+      b2 = (double)bi * (double)bi;
+    }
+    if (r) r[i] = ri;
+  }
+  block_add_d(sh, r2, sc + SC_RR);
+  block_add_d(sh, b2, sc + SC_BB);
+}
+
+__global__ void __launch_bounds__(256) k_apply_dot(L3 d, float ih2, const float* __restrict__ p,
+                                                   const uint32_t* __restrict__ f, int bc_mode,
+                                                   float* __restrict__ q,
+                                                   double* __restrict__ sc) {
+  __shared__ double sh[32];
+  CELL_PROLOGUE
+  double pq = 0.0;
+  if (in) {
+    float qi = 0.0f;
+    if (fluid) {
+      float pi = __ldg(p + i);
+      qi = apply_A(d, ih2, p, f, x, y, z, bc_mode, pi);
+      pq = (double)pi * (double)qi;
+    }
+    q[i] = qi;
+  }
+  block_add_d(sh, pq, sc + SC_PQ);
+}
+
+// phi += alpha p; r -= alpha q; accumulate |r|^2
+__global__ void __launch_bounds__(256) k_update_xr(L3 d, const uint32_t* __restrict__ f,
+                                                   float* __restrict__ phi,
+                                                   float* __restrict__ r,
+                                                   const float* __restrict__ p,
+                                                   const float* __restrict__ q,
+                                                   double* __restrict__ sc) {
+  __shared__ double sh[32];
+  CELL_PROLOGUE
+  double rr = 0.0;
+  if (fluid) {
+    float alpha = (float)(sc[SC_RZ] / sc[SC_PQ]);
+    phi[i] += alpha * p[i];
+    float ri = r[i] - alpha * q[i];
+    r[i] = ri;
+    rr = (double)ri * (double)ri;
+  }
+  block_add_d(sh, rr, sc + SC_RR);
+}
+
+// <z,r> -> SC_RZN and, when q is given, <z,q> -> SC_ZQ
+__global__ void __launch_bounds__(256) k_dots(L3 d, const uint32_t* __restrict__ f,
+                                              const float* __restrict__ zv,
+                                              const float* __restrict__ r,
+                                              const float* __restrict__ q,
+                                              double* __restrict__ sc) {
+  __shared__ double sh[32];
+  CELL_PROLOGUE
+  double zr = 0.0, zq = 0.0;
+  if (fluid) {
+    float zi = zv[i];
+    zr = (double)zi * (double)r[i];
+    if (q) zq = (double)zi * (double)q[i];
+  }
+  block_add_d(sh, zr, sc + SC_RZN);
+  if (q) block_add_d(sh, zq, sc + SC_ZQ);
+}
+
+// p = z + beta p with beta = -<z,q>/<p,q> (first iteration: p = z)
+__global__ void __launch_bounds__(256) k_update_p(L3 d, const uint32_t* __restrict__ f,
+                                                  float* __restrict__ p,
+                                                  const float* __restrict__ zv,
+                                                  const double* __restrict__ sc, int first) {
+  CELL_PROLOGUE
+  if (!in) return;
+  if (!fluid) { p[i] = 0.0f; return; }
+  float beta = first ? 0.0f : (float)(-sc[SC_ZQ] / sc[SC_PQ]);
+  p[i] = first ? zv[i] : zv[i] + beta * p[i];
+}
+
+__global__ void k_roll(double* sc) {
+  // rz <- rz_new, clear the accumulators of the next iteration
+  sc[SC_RZ] = sc[SC_RZN];
+  sc[SC_RZN] = 0.0;
+  sc[SC_ZQ] = 0.0;
+  sc[SC_PQ] = 0.0;
+  sc[SC_RR] = 0.0;
+}
+
+}  // namespace
+
+int Solver::init(Multigrid* m) {
+  mg = m;
+  d = m->dims[0];
+  size_t n = d.cells();
+  int rc;
+  if ((rc = r.alloc(n * 4)) != PYRO_OK) return rc;
+  if ((rc = z.alloc(n * 4)) != PYRO_OK) return rc;
+  if ((rc = p.alloc(n * 4)) != PYRO_OK) return rc;
+  if ((rc = q.alloc(n * 4)) != PYRO_OK) return rc;
+  if ((rc = sc.alloc(SC_N * 8)) != PYRO_OK) return rc;
+  if (cudaMallocHost(&host_sc, SC_N * 8) != cudaSuccess) {
+    set_error("solver: pinned allocation failed");
+    return PYRO_E_NOMEM;
+  }
+  if (cudaEventCreate(&ev0) != cudaSuccess || cudaEventCreate(&ev1) != cudaSuccess) {
+    set_error("solver: cudaEventCreate failed");
+    return PYRO_E_CUDA;
+  }
+  return PYRO_OK;
+}
+
+Solver::~Solver() {
+  if (host_sc) cudaFreeHost(host_sc);
+  if (ev0) cudaEventDestroy(ev0);
+  if (ev1) cudaEventDestroy(ev1);
+}
+
+size_t Solver::device_bytes() const {
+  size_t s = r.bytes + z.bytes + p.bytes + q.bytes + sc.bytes;
+  for (int l = 0; l < 4; l++) s += bphi[l].bytes + bb[l].bytes;
+  return s;
+}
+
+int Solver::true_resid(cudaStream_t st, const float* phi, const float* b, double* rel,
+                       double* bn) {
+  L3 l{d.nx, d.ny, d.nz};
+  PYRO_CU(cudaMemsetAsync(sc.p, 0, SC_N * 8, st));
+  k_resid<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, 1.0f / (mg->h[0] * mg->h[0]), phi, b,
+                                                   mg->f[0], mg->bc_mode, nullptr,
+                                                   sc.as<double>());
+  PYRO_CU(cudaGetLastError());
+  PYRO_CU(cudaMemcpyAsync(host_sc, sc.p, SC_N * 8, cudaMemcpyDeviceToHost, st));
+  PYRO_CU(cudaStreamSynchronize(st));
+  double bb2 = host_sc[SC_BB];
+  *bn = std::sqrt(bb2);
+  *rel = bb2 > 0 ? std::sqrt(host_sc[SC_RR] / bb2) : 0.0;
+  return PYRO_OK;
+}
+
+cudaError_t Solver::precond(cudaStream_t st, bool bf16) {
+  // z = V(r): one V-cycle from a zero initial guess.
+  cudaError_t e = cudaMemsetAsync(z.p, 0, d.cells() * 4, st);
+  if (e != cudaSuccess) return e;
+  float* save_phi = mg->phi[0];
+  float* save_b = mg->b[0];
+  const uint32_t* save_f = mg->f[0];
+  mg->bind_level0(z.as<float>(), r.as<float>(), save_f);
+  e = bf16 ? mg->vcycles_bf16(1, st, bphi, bb) : mg->vcycles(1, st);
+  mg->bind_level0(save_phi, save_b, save_f);
+  return e;
+}
+
+int Solver::solve(cudaStream_t st, float* phi, const float* b, int mode, float tol,
+                  int max_iters, PyroSolveInfo* info) {
+  PYRO_REQUIRE(mode >= PYRO_SOLVER_VCYCLE && mode <= PYRO_SOLVER_MGPCG_BF16,
+               "solve: unknown mode");
+  PYRO_REQUIRE(max_iters > 0, "solve: max_iters must be positive");
+  std::memset(info, 0, sizeof(*info));
+  info->mode = mode;
+  float* save_phi = mg->phi[0];
+  float* save_b = mg->b[0];
+  const uint32_t* f0 = mg->f[0];
+  PYRO_CU(cudaEventRecord(ev0, st));
+  int iters = 0;
+  double rel = 0, bn = 0;
+  int rc = PYRO_OK;
+  L3 l{d.nx, d.ny, d.nz};
+  const float ih2 = 1.0f / (mg->h[0] * mg->h[0]);
+  if (mode == PYRO_SOLVER_VCYCLE || mode == PYRO_SOLVER_VCYCLE_TOL) {
+    mg->bind_level0(phi, b, f0);
+    if (mode == PYRO_SOLVER_VCYCLE) {
+      cudaError_t e = mg->vcycles(max_iters, st);
+      mg->bind_level0(save_phi, save_b, f0);
+      PYRO_CU(e);
+      iters = max_iters;
+      if ((rc = true_resid(st, phi, b, &rel, &bn)) != PYRO_OK) return rc;
+    } else {
+      if ((rc = true_resid(st, phi, b, &rel, &bn)) != PYRO_OK) return rc;
+      while (rel > tol && iters < max_iters) {
+        mg->bind_level0(phi, b, f0);
+        cudaError_t e = mg->vcycles(1, st);
+        mg->bind_level0(save_phi, save_b, f0);
+        PYRO_CU(e);
+        iters++;
+        if ((rc = true_resid(st, phi, b, &rel, &bn)) != PYRO_OK) return rc;
+      }
+    }
+  } else {
+    const bool bf16 = mode == PYRO_SOLVER_MGPCG_BF16;
+    double* S = sc.as<double>();
+    // r = b - A phi, |r|, |b|
+    PYRO_CU(cudaMemsetAsync(sc.p, 0, SC_N * 8, st));
+    k_resid<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, ih2, phi, b, f0, mg->bc_mode,
+                                                     r.as<float>(), S);
+    PYRO_CU(cudaGetLastError());
+    PYRO_CU(cudaMemcpyAsync(host_sc, sc.p, SC_N * 8, cudaMemcpyDeviceToHost, st));
+    PYRO_CU(cudaStreamSynchronize(st));
+    double bb2 = host_sc[SC_BB];
+    bn = std::sqrt(bb2);
+    rel = bb2 > 0 ? std::sqrt(host_sc[SC_RR] / bb2) : 0.0;
+    if (rel > tol) {
+      PYRO_CU(precond(st, bf16));
+      k_dots<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, f0, z.as<float>(), r.as<float>(),
+                                                      nullptr, S);
+      PYRO_CU(cudaGetLastError());
+      k_roll<<<1, 1, 0, st>>>(S);
+      k_update_p<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, f0, p.as<float>(), z.as<float>(),
+                                                          S, 1);
+      PYRO_CU(cudaGetLastError());
+      while (iters < max_iters) {
+        k_apply_dot<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, ih2, p.as<float>(), f0,
+                                                             mg->bc_mode, q.as<float>(), S);
+        k_update_xr<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, f0, phi, r.as<float>(),
+                                                             p.as<float>(), q.as<float>(), S);
+        PYRO_CU(cudaGetLastError());
+        PYRO_CU(cudaMemcpyAsync(host_sc, sc.p, SC_N * 8, cudaMemcpyDeviceToHost, st));
+        PYRO_CU(cudaStreamSynchronize(st));
+        iters++;
+        double rr = host_sc[SC_RR];
+        if (!(rr >= 0.0) || !(host_sc[SC_PQ] < 0.0 || host_sc[SC_PQ] > 0.0)) break;
+        if (bb2 > 0 && std::sqrt(rr / bb2) <= tol) break;
+        PYRO_CU(precond(st, bf16));
+        k_dots<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, f0, z.as<float>(), r.as<float>(),
+                                                        q.as<float>(), S);
+        k_update_p<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, f0, p.as<float>(),
+                                                            z.as<float>(), S, 0);
+        k_roll<<<1, 1, 0, st>>>(S);
+        PYRO_CU(cudaGetLastError());
+      }
+      if ((rc = true_resid(st, phi, b, &rel, &bn)) != PYRO_OK) return rc;
+    }
+  }
+  PYRO_CU(cudaEventRecord(ev1, st));
+  PYRO_CU(cudaEventSynchronize(ev1));
+  float ms = 0;
+  PYRO_CU(cudaEventElapsedTime(&ms, ev0, ev1));
+  info->iterations = iters;
+  info->rel_resid = rel;
+  info->b_norm = bn;
+  info->ms = ms;
+  info->converged = rel <= tol ? 1 : 0;
+  if (mode != PYRO_SOLVER_VCYCLE && !info->converged) {
+    set_error("solve: iteration cap reached before the tolerance");
+    return PYRO_E_NOCONV;
+  }
+  return PYRO_OK;
+}
+
+}  // namespace pyro
+
+// ------------------------------------------------------ stand-alone solver
+using namespace pyro;
+
+struct PyroPoisson {
+  Dims3 d{};
+  cudaStream_t stream = nullptr;
+  DevBuf flags;
+  Multigrid mg;
+  Solver solver;
+  ~PyroPoisson() {
+    if (stream) {
+      cudaStreamSynchronize(stream);
+      cudaStreamDestroy(stream);
+    }
+  }
+};
+
+extern "C" {
+
+int pyro_poisson_create(uint32_t nx, uint32_t ny, uint32_t nz, float h, int bc_mode,
+                        PyroPoisson** out) {
+  clear_error();
+  PYRO_REQUIRE(out, "pyro_poisson_create: null argument");
+  *out = nullptr;
+  PYRO_REQUIRE(nx >= 2 && ny >= 2 && nz >= 2, "pyro_poisson_create: dims must be >= 2");
+  PYRO_REQUIRE((uint64_t)nx * ny * nz < (1ull << 31), "pyro_poisson_create: grid too large");
+  PYRO_REQUIRE(h > 0.0f, "pyro_poisson_create: h must be positive");
+  PYRO_REQUIRE(bc_mode == 0 || bc_mode == 1, "pyro_poisson_create: bc_mode must be 0 or 1");
+  PyroPoisson* ps = new PyroPoisson();
+  ps->d = Dims3{(int)nx, (int)ny, (int)nz};
+  int rc;
+  if (cudaStreamCreateWithFlags(&ps->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete ps;
+    set_error("pyro_poisson_create: cudaStreamCreate failed");
+    return PYRO_E_CUDA;
+  }
+  if ((rc = ps->flags.alloc(ps->d.cells() * 4)) != PYRO_OK ||
+      (rc = ps->mg.init(ps->d, h, bc_mode)) != PYRO_OK) {
+    delete ps;
+    return rc;
+  }
+  ps->mg.bind_level0(nullptr, nullptr, ps->flags.as<uint32_t>());
+  if ((rc = ps->solver.init(&ps->mg)) != PYRO_OK) {
+    delete ps;
+    return rc;
+  }
+  *out = ps;
+  return PYRO_OK;
+}
+
+int pyro_poisson_set_flags(PyroPoisson* ps, const uint32_t* flags) {
+  clear_error();
+  PYRO_REQUIRE(ps && flags, "pyro_poisson_set_flags: null argument");
+  PYRO_CU(cudaMemcpyAsync(ps->flags.p, flags, ps->d.cells() * 4, cudaMemcpyDeviceToDevice,
+                          ps->stream));
+  PYRO_CU(cudaStreamSynchronize(ps->stream));
+  return PYRO_OK;
+}
+
+int pyro_poisson_solve(PyroPoisson* ps, const float* b, float* phi, int mode, float tol,
+                       int max_iters, PyroSolveInfo* info) {
+  clear_error();
+  PYRO_REQUIRE(ps && b && phi && info, "pyro_poisson_solve: null argument");
+  return ps->solver.solve(ps->stream, phi, b, mode, tol, max_iters, info);
+}
+
+int pyro_poisson_stream(PyroPoisson* ps, void** stream) {
+  clear_error();
+  PYRO_REQUIRE(ps && stream, "pyro_poisson_stream: null argument");
+  *stream = (void*)ps->stream;
+  return PYRO_OK;
+}
+
+int pyro_poisson_destroy(PyroPoisson* ps) {
+  clear_error();
+  delete ps;
+  return PYRO_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,34 @@
+// solver.h — pressure solvers on a multigrid hierarchy: fixed V-cycles,
+// V-cycles to a tolerance, and flexible preconditioned CG (MGPCG) with an
+// FP32 or BF16-storage V-cycle preconditioner.  Dot products and residual
+// norms are accumulated in FP64.
+#pragma once
+
+#include "runtime.h"
+
+namespace pyro {
+
+struct Solver {
+  Multigrid* mg = nullptr;
+  Dims3 d{};
+  DevBuf r, z, p, q;        // level-0 work vectors (FP32)
+  DevBuf sc;                // FP64 device scalars
+  double* host_sc = nullptr;  // pinned mirror
+  // BF16 hierarchy for the low-precision preconditioner
+  DevBuf bphi[4], bb[4];
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+  int init(Multigrid* m);
+  ~Solver();
+  size_t device_bytes() const;
+  // Solve A phi = b in place (phi = initial guess).  Returns PYRO_OK or
+  // PYRO_E_NOCONV (info filled either way) or an error.
+  int solve(cudaStream_t st, float* phi, const float* b, int mode, float tol, int max_iters,
+            PyroSolveInfo* info);
+
+ private:
+  cudaError_t precond(cudaStream_t st, bool bf16);
+  int true_resid(cudaStream_t st, const float* phi, const float* b, double* rel, double* bn);
+};
+
+}  // namespace pyro

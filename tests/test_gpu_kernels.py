@@ -1,0 +1,217 @@
+"""Per-kernel parity of the CUDA kernels against the CPU oracle on
+identical seeded inputs, through the C ABI.
+
+Kernels without transcendental functions keep the reference's FP32
+expression order on both sides (the library is built with --fmad=false, the
+oracle with -ffp-contract=off), so their outputs must agree bit for bit;
+kernels calling exp() (solid, react, forces) agree within 1e-5 relative with
+an absolute floor of 1e-6 of each channel's magnitude.  Masks (flags,
+coarse flags) are bit-exact.  Statistics are float atomics on the GPU and
+FP64 sums in the oracle: 1e-4 relative.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from fields import close, face_valid_mask, params_for, random_state
+from gpu_util import dev, host, params_dev, ptr, require_cuda, stats_dev
+
+pytestmark = pytest.mark.gpu
+
+CASES = [(24, 32, 20, 0), (19, 23, 17, 1), (40, 16, 33, 2)]
+
+
+@pytest.fixture(scope="module")
+def lib():
+    return require_cuda()
+
+
+def _setup(nx, ny, nz, seed, **kw):
+    P = params_for(nx, ny, nz, **kw)
+    return P, random_state(P, seed=seed)
+
+
+def _stats_close(gpu, ora, idx, rtol=1e-4):
+    for i in idx:
+        e = ora[i]
+        assert abs(gpu[i] - e) <= rtol * abs(e) + 1e-30 + 1e-6 * abs(e), (i, gpu[i], e)
+
+
+@pytest.mark.parametrize("nx,ny,nz,seed", CASES)
+def test_solid(lib, nx, ny, nz, seed):
+    P, S = _setup(nx, ny, nz, seed, dt=0.02)
+    st = np.zeros(1040)
+    sol_o, pyr_o, fl_o = oracle.solid(P, S["sol"], S["s0"], st)
+    Pd = params_dev(P)
+    sol_in, s0 = dev(S["sol"]), dev(S["s0"])
+    sol_out, pyr, flags = dev(np.zeros_like(S["sol"])), dev(np.zeros_like(S["sol"])), \
+        dev(np.zeros((nz, ny, nx), np.uint32))
+    sd = stats_dev()
+    assert lib.pyro_k_solid(ptr(Pd), nx, ny, nz, ptr(sol_in), ptr(sol_out), ptr(pyr), ptr(flags),
+                            ptr(s0), ptr(sd), None) == 0
+    assert np.array_equal(host(flags), fl_o)
+    close(host(sol_out), sol_o, name="sol")
+    close(host(pyr), pyr_o, name="pyr")
+    _stats_close(host(sd), st, [2, 7, 9])
+
+
+@pytest.mark.parametrize("nx,ny,nz,seed", CASES)
+def test_curl(lib, nx, ny, nz, seed):
+    P, S = _setup(nx, ny, nz, seed)
+    st = np.zeros(1040)
+    c_o = oracle.curl(P, S["u"], S["v"], S["w"], st)
+    Pd = params_dev(P)
+    u, v, w = dev(S["u"]), dev(S["v"]), dev(S["w"])
+    c = dev(np.zeros_like(c_o))
+    sd = stats_dev()
+    assert lib.pyro_k_curl(ptr(Pd), nx, ny, nz, ptr(u), ptr(v), ptr(w), ptr(c), ptr(sd), None) == 0
+    assert np.array_equal(host(c), c_o)
+    assert host(sd)[5] == np.float32(st[5])
+
+
+@pytest.mark.parametrize("nx,ny,nz,seed", CASES)
+def test_adv_vel(lib, nx, ny, nz, seed):
+    P, S = _setup(nx, ny, nz, seed, dt=0.02)
+    (hu_o, hv_o, hw_o), (ou_o, ov_o, ow_o) = oracle.adv_vel(P, S["u"], S["v"], S["w"],
+                                                            S["flags"])
+    Pd = params_dev(P)
+    u, v, w = dev(S["u"]), dev(S["v"]), dev(S["w"])
+    z = np.zeros_like(S["u"])
+    hu, hv, hw, ou, ov, ow = (dev(z) for _ in range(6))
+    fl = dev(S["flags"])
+    assert lib.pyro_k_adv_vel(ptr(Pd), nx, ny, nz, ptr(u), ptr(v), ptr(w), ptr(hu), ptr(hv),
+                              ptr(hw), ptr(ou), ptr(ov), ptr(ow), ptr(fl), None) == 0
+    for k, (g, e) in enumerate([(hu, hu_o), (hv, hv_o), (hw, hw_o)]):
+        m = face_valid_mask(P, k)
+        assert np.array_equal(host(g)[m], e[m]), f"hat {k}"
+    for k, (g, e) in enumerate([(ou, ou_o), (ov, ov_o), (ow, ow_o)]):
+        m = face_valid_mask(P, k)
+        assert np.array_equal(host(g)[m], e[m]), f"out {k}"
+
+
+@pytest.mark.parametrize("nx,ny,nz,seed", CASES)
+def test_adv_scalars(lib, nx, ny, nz, seed):
+    P, S = _setup(nx, ny, nz, seed, dt=0.02)
+    (h0_o, h1_o), (o0_o, o1_o) = oracle.adv_scalars(P, S["u"], S["v"], S["w"], S["s0"], S["s1"])
+    Pd = params_dev(P)
+    u, v, w = dev(S["u"]), dev(S["v"]), dev(S["w"])
+    s0, s1 = dev(S["s0"]), dev(S["s1"])
+    z = np.zeros_like(S["s0"])
+    h0, h1, o0, o1 = (dev(z) for _ in range(4))
+    assert lib.pyro_k_adv_scalars(ptr(Pd), nx, ny, nz, ptr(u), ptr(v), ptr(w), ptr(s0), ptr(s1),
+                                  ptr(h0), ptr(h1), ptr(o0), ptr(o1), None) == 0
+    assert np.array_equal(host(h0), h0_o)
+    assert np.array_equal(host(h1), h1_o)
+    assert np.array_equal(host(o0), o0_o)
+    assert np.array_equal(host(o1), o1_o)
+
+
+@pytest.mark.parametrize("nx,ny,nz,seed", CASES)
+@pytest.mark.parametrize("ign_on", [0.0, 1.0])
+def test_react(lib, nx, ny, nz, seed, ign_on):
+    P, S = _setup(nx, ny, nz, seed, dt=0.01, ign_on=ign_on)
+    st = np.zeros(1040)
+    o0_o, o1_o = oracle.react(P, S["s0"], S["s1"], S["flags"], S["sol"], S["pyr"], S["curl"], st)
+    Pd = params_dev(P)
+    args = [dev(S[k]) for k in ("s0", "s1")]
+    o0, o1 = dev(np.zeros_like(S["s0"])), dev(np.zeros_like(S["s1"]))
+    fl, sol, pyr, curl = dev(S["flags"]), dev(S["sol"]), dev(S["pyr"]), dev(S["curl"])
+    sd = stats_dev()
+    assert lib.pyro_k_react(ptr(Pd), nx, ny, nz, ptr(args[0]), ptr(args[1]), ptr(o0), ptr(o1),
+                            ptr(fl), ptr(sol), ptr(pyr), ptr(curl), ptr(sd), None) == 0
+    close(host(o0), o0_o, name="s0")
+    close(host(o1), o1_o, name="s1")
+    g = host(sd)
+    _stats_close(g, st, [0, 1, 3, 6, 8])
+    assert abs(g[4] - st[4]) <= 1e-5 * st[4]
+    lay = g[16:16 + ny]
+    close(lay, st[16:16 + ny].astype(np.float32), rtol=1e-4, floor=1e-6, name="layers")
+
+
+@pytest.mark.parametrize("nx,ny,nz,seed", CASES)
+def test_forces(lib, nx, ny, nz, seed):
+    P, S = _setup(nx, ny, nz, seed, dt=0.01, wind=2.0, sponge=3.0)
+    uo, vo, wo = oracle.forces(P, S["u"], S["v"], S["w"], S["s0"], S["s1"], S["curl"],
+                               S["flags"])
+    Pd = params_dev(P)
+    u, v, w = dev(S["u"]), dev(S["v"]), dev(S["w"])
+    s0, s1, curl, fl = dev(S["s0"]), dev(S["s1"]), dev(S["curl"]), dev(S["flags"])
+    assert lib.pyro_k_forces(ptr(Pd), nx, ny, nz, ptr(u), ptr(v), ptr(w), ptr(s0), ptr(s1),
+                             ptr(curl), ptr(fl), None) == 0
+    for k, (g, e) in enumerate([(u, uo), (v, vo), (w, wo)]):
+        m = face_valid_mask(P, k)
+        close(host(g)[m], e[m], name=f"vel{k}")
+
+
+@pytest.mark.parametrize("nx,ny,nz,seed", CASES)
+def test_divergence_and_project(lib, nx, ny, nz, seed):
+    P, S = _setup(nx, ny, nz, seed)
+    b_o = oracle.divergence(P, S["u"], S["v"], S["w"], S["s1"], S["flags"])
+    Pd = params_dev(P)
+    u, v, w = dev(S["u"]), dev(S["v"]), dev(S["w"])
+    s1, fl = dev(S["s1"]), dev(S["flags"])
+    b = dev(np.zeros((nz, ny, nx), np.float32))
+    assert lib.pyro_k_divergence(ptr(Pd), nx, ny, nz, ptr(u), ptr(v), ptr(w), ptr(s1), ptr(fl),
+                                 ptr(b), None) == 0
+    assert np.array_equal(host(b), b_o)
+    uo, vo, wo = oracle.project(P, S["u"], S["v"], S["w"], S["phi"], S["flags"])
+    phi = dev(S["phi"])
+    assert lib.pyro_k_project(ptr(Pd), nx, ny, nz, ptr(u), ptr(v), ptr(w), ptr(phi), ptr(fl),
+                              None) == 0
+    for k, (g, e) in enumerate([(u, uo), (v, vo), (w, wo)]):
+        m = face_valid_mask(P, k)
+        assert np.array_equal(host(g)[m], e[m]), f"project {k}"
+
+
+MG_CASES = [(32, 48, 32, 0, 0.05), (19, 46, 19, 1, 0.16), (17, 33, 9, 2, 0.1)]
+
+
+@pytest.mark.parametrize("nx,ny,nz,seed,h", MG_CASES)
+def test_mg_kernels(lib, nx, ny, nz, seed, h):
+    rng = np.random.default_rng(seed)
+    f = (rng.random((nz, ny, nx)) < 0.2).astype(np.uint32)
+    b = rng.normal(0, 1, (nz, ny, nx)).astype(np.float32)
+    p = rng.normal(0, 1, (nz, ny, nx)).astype(np.float32)
+    bd, fd = dev(b), dev(f)
+    for color, om in [(0, 1.0), (1, 1.0), (0, 1.6), (1, 1.6)]:
+        e = oracle.mg_smooth((nx, ny, nz), h, b, f, p, color, om)
+        pd = dev(p)
+        assert lib.pyro_k_mg_smooth(nx, ny, nz, h, ptr(bd), ptr(fd), ptr(pd), color, om,
+                                    None) == 0
+        assert np.array_equal(host(pd), e), (color, om)
+    cx, cy, cz = (nx + 1) // 2, (ny + 1) // 2, (nz + 1) // 2
+    bc_o, pc_o, fc_o = oracle.mg_restrict((nx, ny, nz), h, p, b, f)
+    bc, pc, fc = dev(np.ones_like(bc_o)), dev(np.ones_like(pc_o)), dev(np.ones_like(fc_o))
+    pd = dev(p)
+    assert lib.pyro_k_mg_restrict(nx, ny, nz, h, ptr(pd), ptr(bd), ptr(fd), cx, cy, cz, ptr(bc),
+                                  ptr(pc), ptr(fc), None) == 0
+    assert np.array_equal(host(fc), fc_o)
+    assert np.array_equal(host(bc), bc_o)
+    assert np.array_equal(host(pc), pc_o)
+    pcv = rng.normal(0, 1, bc_o.shape).astype(np.float32)
+    pf_o = oracle.mg_prolong((nx, ny, nz), pcv, f, p, fc_o)
+    pcd = dev(pcv)
+    assert lib.pyro_k_mg_prolong(nx, ny, nz, ptr(pcd), ptr(fd), ptr(pd), cx, cy, cz, ptr(fc),
+                                 None) == 0
+    assert np.array_equal(host(pd), pf_o)
+    r2, b2 = oracle.mg_resid((nx, ny, nz), h, p, b, f)
+    sd = stats_dev()
+    pd = dev(p)
+    assert lib.pyro_k_mg_resid(nx, ny, nz, h, ptr(pd), ptr(bd), ptr(fd), ptr(sd), None) == 0
+    g = host(sd)
+    assert abs(g[10] - r2) <= 1e-4 * r2 and abs(g[11] - b2) <= 1e-4 * b2
+
+
+@pytest.mark.parametrize("nx,ny,nz,seed,h", MG_CASES + [(8, 20, 8, 3, 0.32), (32, 32, 22, 4, 0.2)])
+def test_mg_coarse_solve_equals_80_sor_sweeps(lib, nx, ny, nz, seed, h):
+    rng = np.random.default_rng(seed)
+    f = (rng.random((nz, ny, nx)) < 0.1).astype(np.uint32)
+    b = rng.normal(0, 1, (nz, ny, nx)).astype(np.float32)
+    p = rng.normal(0, 0.1, (nz, ny, nx)).astype(np.float32)
+    e = p
+    for _ in range(80):
+        for c in (0, 1):
+            e = oracle.mg_smooth((nx, ny, nz), h, b, f, e, c, 1.6)
+    pd, bd, fd = dev(p), dev(b), dev(f)
+    assert lib.pyro_k_mg_coarse(nx, ny, nz, h, ptr(bd), ptr(fd), ptr(pd), 80, 1.6, None) == 0
+    assert np.array_equal(host(pd), e)

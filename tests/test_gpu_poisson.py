@@ -1,0 +1,85 @@
+"""Stand-alone pressure solver against the CPU oracle: the fixed V-cycle
+schedule is bit-exact with the oracle's restatement of src/sim.rs:451-491,
+and the tolerance solvers (V-cycles, FP32 MGPCG, BF16 MGPCG) reach their
+tolerance with the error against the FP64 solve stated."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import oracle
+from gpu_util import dev, host, ptr, require_cuda
+from pyro_b200 import _abi
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def lib():
+    return require_cuda()
+
+
+def _case(nx, ny, nz, seed, solid=0.05):
+    """Seeded axis-aligned solid boxes (2-20 cells per edge, up to the solid
+    fraction) and an N(0,1) right-hand side with zero fluid mean."""
+    rng = np.random.default_rng(seed)
+    f = np.zeros((nz, ny, nx), np.uint32)
+    while f.mean() < solid:
+        e = rng.integers(2, 21, size=3)
+        o = [rng.integers(0, max(1, d - e[i])) for i, d in enumerate((nx, ny, nz))]
+        f[o[2]:o[2] + e[2], o[1]:o[1] + e[1], o[0]:o[0] + e[0]] = 1
+    b = rng.normal(0, 1, (nz, ny, nx)).astype(np.float32)
+    b[f == 1] = 0
+    b[f == 0] -= b[f == 0].mean()
+    return f, b
+
+
+def _solver(lib, dims, h, f, bc_mode=0):
+    ps = ctypes.c_void_p()
+    assert lib.pyro_poisson_create(*dims, h, bc_mode, ctypes.byref(ps)) == 0
+    fd = dev(f)
+    assert lib.pyro_poisson_set_flags(ps, ptr(fd)) == 0
+    return ps
+
+
+@pytest.mark.parametrize("dims,cycles", [((64, 64, 64), 4), ((38, 75, 38), 2),
+                                         ((48, 96, 48), 1)])
+def test_fixed_vcycles_bit_exact(lib, dims, cycles):
+    nx, ny, nz = dims
+    f, b = _case(nx, ny, nz, 1)
+    h = 0.02
+    e = oracle.vcycles(dims, h, np.zeros_like(b), b, f, cycles)
+    ps = _solver(lib, dims, h, f)
+    bd, pd = dev(b), dev(np.zeros_like(b))
+    info = _abi.PyroSolveInfo()
+    assert lib.pyro_poisson_solve(ps, ptr(bd), ptr(pd), _abi.SOLVER_VCYCLE, 1e-3, cycles,
+                                  ctypes.byref(info)) == 0
+    assert np.array_equal(host(pd), e)
+    rel = oracle.poisson_relres(dims, h, e, b, f)
+    assert abs(info.rel_resid - rel) <= 1e-6 * rel
+    lib.pyro_poisson_destroy(ps)
+
+
+@pytest.mark.parametrize("mode,tol", [(_abi.SOLVER_VCYCLE_TOL, 1e-3), (_abi.SOLVER_VCYCLE_TOL, 1e-6),
+                                      (_abi.SOLVER_MGPCG, 1e-3), (_abi.SOLVER_MGPCG, 1e-6),
+                                      (_abi.SOLVER_MGPCG_BF16, 1e-3),
+                                      (_abi.SOLVER_MGPCG_BF16, 1e-6)])
+@pytest.mark.parametrize("bc_mode", [0, 1])
+def test_tolerance_solvers_vs_fp64(lib, mode, tol, bc_mode):
+    dims = (64, 64, 64)
+    f, b = _case(*dims, 2)
+    h = 0.02
+    x64, it, rel64 = oracle.poisson_f64(dims, h, b, f, tol=1e-12, bc_mode=bc_mode)
+    ps = _solver(lib, dims, h, f, bc_mode)
+    bd, pd = dev(b), dev(np.zeros_like(b))
+    info = _abi.PyroSolveInfo()
+    rc = lib.pyro_poisson_solve(ps, ptr(bd), ptr(pd), mode, tol, 200, ctypes.byref(info))
+    assert rc == 0, lib.pyro_last_error()
+    phi = host(pd)
+    rel = oracle.poisson_relres(dims, h, phi, b, f, bc_mode)
+    assert info.converged == 1 and rel <= tol * 1.05, (info.iterations, rel)
+    fl = f == 0
+    err = np.abs(phi[fl] - x64[fl]).max() / np.abs(x64[fl]).max()
+    # error against the FP64 solve scales with the residual tolerance
+    assert err <= 200 * tol, (mode, tol, err)
+    lib.pyro_poisson_destroy(ps)
