@@ -35,6 +35,7 @@ cells*substeps/s over ranks.
 from __future__ import annotations
 
 import argparse
+import faulthandler
 import json
 import math
 import os
@@ -48,6 +49,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+faulthandler.enable()
 METRIC = "2cm pool-fire ms/step"
 UNIT = "ms/step"
 WORKLOADS = {
@@ -225,6 +227,11 @@ def run_reference(args):
     return 0
 
 
+def log(msg):
+    sys.stderr.write(f"[bench {time.strftime('%H:%M:%S')}] {msg}\n")
+    sys.stderr.flush()
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -242,8 +249,10 @@ def run_ours(args):
     dev = torch.cuda.current_device()
 
     sc = build_workload(args.workload)
+    log(f"creating {args.workload} {sc.grid().dims}")
     sim = Sim(sc)
     cells = sim.cells()
+    log("created")
     lib = _abi.load()
     stream = torch.cuda.ExternalStream(sim.stream())
 
@@ -257,6 +266,7 @@ def run_ours(args):
         st = sim.read_stats()
         max_u = max(st.max_u, 1.0)
         t_pre += float(n * dt)
+    log(f"preroll done t={t_pre:.3f}s max_u={max_u:.2f}")
     n, dt = cfl_substeps(sc, max_u)
     for k in range(args.warmup):
         sim.step(dt, (k % n) == n - 1)
@@ -279,6 +289,7 @@ def run_ours(args):
         e1.synchronize()
     barrier()
     ms = e0.elapsed_time(e1) / args.steps
+    log(f"timed {ms:.3f} ms/step")
 
     # ---- e2e through the public API with a host read every substep
     e2 = torch.cuda.Event(enable_timing=True)
@@ -292,6 +303,7 @@ def run_ours(args):
     e3.synchronize()
     barrier()
     ms_e2e = e2.elapsed_time(e3) / args.steps
+    log(f"e2e {ms_e2e:.3f} ms/step")
 
     # ---- per-kernel device times (CUDA events around each launch)
     phases = np.zeros(12)
@@ -304,6 +316,7 @@ def run_ours(args):
         sim.time = np.float32(sim.time + dt)
         phases += buf
     phases /= nprof
+    log("profiled " + " ".join(f"{v:.3f}" for v in phases))
     names = _abi.PROFILE_PHASES
     kern = {names[i]: float(phases[i]) for i in range(12)}
     single = {k: v for k, v in kern.items() if k in ALG_BYTES}
@@ -329,6 +342,11 @@ def run_ours(args):
                   A.F_SOL: sim.read_field(A.F_SOL), A.F_U: sim.read_field(A.F_U),
                   A.F_V: sim.read_field(A.F_V), A.F_W: sim.read_field(A.F_W),
                   A.F_PHI: sim.read_field(A.F_PHI)}
+        log("cpu baseline")
+        for f, a in fields.items():
+            bad = int(np.size(a) - np.isfinite(a).sum())
+            if bad:
+                log(f"field {f}: {bad} non-finite values")
         cms, cores = cpu_baseline_run(sc, sim.p, fields[A.F_SOL], fields, args.cpu_steps, dt,
                                       float(sim.time))
         cpu = {"value": cms, "unit": UNIT, "cores": cores, "kind": "port",

@@ -57,9 +57,11 @@ inline I3 operator+(I3 a, I3 b) { return I3{a.x + b.x, a.y + b.y, a.z + b.z}; }
 inline I3 operator-(I3 a, I3 b) { return I3{a.x - b.x, a.y - b.y, a.z - b.z}; }
 inline I3 operator*(I3 a, int s) { return I3{a.x * s, a.y * s, a.z * s}; }
 
-// WGSL builtins (WGSL spec, section "Numeric built-in functions").
-inline float wmin(float a, float b) { return b < a ? b : a; }
-inline float wmax(float a, float b) { return a < b ? b : a; }
+// WGSL builtins (WGSL spec, section "Numeric built-in functions").  min/max
+// return the non-NaN operand when one is NaN (IEEE minNum/maxNum, what the
+// GPU's fminf/fmaxf do), so a NaN can never reach an index computation.
+inline float wmin(float a, float b) { return std::fmin(a, b); }
+inline float wmax(float a, float b) { return std::fmax(a, b); }
 inline float clampf(float x, float lo, float hi) { return wmin(wmax(x, lo), hi); }
 inline float mixf(float a, float b, float t) { return a * (1.0f - t) + b * t; }
 inline F4 mix4(F4 a, F4 b, float t) {

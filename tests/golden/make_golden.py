@@ -1,0 +1,320 @@
+"""Generate golden vectors by executing the reference's own WGSL kernels.
+
+    python tests/golden/make_golden.py [--ref /root/reference] [--only name,...]
+
+For each simulation kernel the script assembles the shader source exactly as
+the reference's host does (src/gpu.rs:190-237: common.wgsl first unless the
+kernel is a multigrid one, then the template / velocity / statistics blocks
+its //@ directives name, then the kernel body), interprets it with
+tests/golden/wgsl.py over the dispatch grid src/sim.rs uses (4x4x4
+workgroups, g3 over cells, gv over the padded face grid, the smoother over
+(ceil(nx/2), ny, nz)), and stores the seeded inputs and the outputs in
+tests/golden/<kernel>.npz.  The fixtures are committed; the tests only read
+them (the reference checkout is not needed to run the tests).
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import re
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+TESTS = os.path.dirname(HERE)
+ROOT = os.path.dirname(TESTS)
+sys.path.insert(0, ROOT)
+sys.path.insert(0, TESTS)
+sys.path.insert(0, HERE)
+
+import wgsl  # noqa: E402
+from fields import params_for, random_state  # noqa: E402
+
+GOLDEN_DIMS = (10, 12, 9)
+MG_DIMS = (11, 14, 9)
+
+
+def split_kernels(text: str):
+    """src/gpu.rs:190-209."""
+    out, name, body = {}, None, []
+    for line in text.splitlines():
+        if line.startswith("//#KERNEL "):
+            if name is not None:
+                out[name] = "\n".join(body) + "\n"
+            name, body = line[len("//#KERNEL "):].strip(), []
+        elif name is not None:
+            body.append(line)
+    if name is not None:
+        out[name] = "\n".join(body) + "\n"
+    return out
+
+
+class Ref:
+    def __init__(self, root):
+        sh = os.path.join(root, "src", "shaders")
+        rd = lambda n: open(os.path.join(sh, n), encoding="utf-8").read()  # noqa: E731
+        self.common = rd("common.wgsl")
+        self.t_scalar = rd("tmpl_scalar.wgsl")
+        self.t_comp = rd("tmpl_comp.wgsl")
+        self.vel = rd("vel.wgsl")
+        self.stats = rd("stats.wgsl")
+        self.kernels = {}
+        for f in ("advect.wgsl", "fluid.wgsl", "combust.wgsl", "mg.wgsl"):
+            self.kernels.update(split_kernels(rd(f)))
+
+    def assemble(self, name):
+        """src/gpu.rs:212-237."""
+        body = self.kernels[name]
+        s = self.common if not name.startswith("mg_") else ""
+        for line in body.splitlines():
+            t = line.strip()
+            if t.startswith("//@COMP "):
+                for n in t[len("//@COMP "):].split():
+                    s += self.t_comp.replace("XBUF", n)
+            elif t.startswith("//@SCAL "):
+                for n in t[len("//@SCAL "):].split():
+                    s += self.t_scalar.replace("XBUF", n)
+            elif t == "//@VEL":
+                s += self.vel
+            elif t.startswith("//@STATS "):
+                s += self.stats.replace("STATSB", t[len("//@STATS "):].strip())
+        return s + body
+
+
+# the 64-lane tree reductions become per-invocation values (see wgsl.py)
+IDENT = {"wsum": lambda li, v: v, "wmax": lambda li, v: v}
+
+
+def params_struct(P):
+    """The uniform block as the interpreter's struct value."""
+    from pyro_b200._abi import PARAM_SCALARS
+    d = {}
+    for name, ct in PARAM_SCALARS:
+        v = getattr(P, name)
+        d[name] = np.uint32(v) if ct.__name__ == "c_uint" else np.float32(v)
+    mats = []
+    for s in range(8):
+        row = np.array(list(P.mats[s]), dtype=np.float32)
+        mats.append({"a": row[0:4].copy(), "b": row[4:8].copy(), "c": row[8:12].copy()})
+    d["mats"] = mats
+    return d
+
+
+def groups3(d):
+    return tuple((v + 3) // 4 for v in d)
+
+
+def flat(a):
+    """(z,y,x[,4]) field -> the interpreter's flat buffer view."""
+    a = np.ascontiguousarray(a)
+    if a.ndim == 4:
+        return a.reshape(-1, 4).copy()
+    return a.reshape(-1).copy()
+
+
+def run_kernel(ref, name, P, binds, grid, overrides=None):
+    m = wgsl.Module(ref.assemble(name), overrides=overrides, replace=IDENT)
+    if 0 in m.bindings and P is not None:
+        m.bind(0, params_struct(P))
+    for b, arr in binds.items():
+        m.bind(b, arr)
+    t = time.time()
+    m.dispatch(grid)
+    return time.time() - t
+
+
+def stats_buf():
+    return np.zeros(1040, np.uint32)
+
+
+def gen_sim(ref, only):
+    nx, ny, nz = GOLDEN_DIMS
+    out = {}
+    n = (nz, ny, nx)
+    for case, (seed, dt, ign, wind) in enumerate([(11, 0.02, 1.0, 0.0), (12, 0.01, 0.0, 2.0)]):
+        P = params_for(nx, ny, nz, dx=0.05, dt=dt, ign_on=ign, wind=wind, sponge=2.0)
+        S = random_state(P, seed=seed)
+        pb = np.frombuffer(P.to_bytes(), np.uint8).copy()
+        g3 = groups3((nx, ny, nz))
+        gv = groups3((nx + 1, ny + 1, nz + 1))
+        tag = f"c{case}"
+
+        def want(k):
+            return only is None or k in only
+
+        if want("solid"):
+            solIn, s0 = flat(S["sol"]), flat(S["s0"])
+            solOut, pyr = np.zeros_like(solIn), np.zeros_like(solIn)
+            fl, st = np.zeros(nx * ny * nz, np.uint32), stats_buf()
+            t = run_kernel(ref, "solid", P, {1: solIn, 2: solOut, 3: pyr, 4: fl, 5: s0, 6: st}, g3)
+            out[f"solid_{tag}"] = dict(params=pb, sol=S["sol"], s0=S["s0"],
+                                       sol_out=solOut.reshape(n + (4,)), pyr=pyr.reshape(n + (4,)),
+                                       flags=fl.reshape(n), stats=st.view(np.float32))
+            print(f"solid {tag} {t:.1f}s", flush=True)
+        if want("curl"):
+            u, v, w = flat(S["u"]), flat(S["v"]), flat(S["w"])
+            c, st = np.zeros((nx * ny * nz, 4), np.float32), stats_buf()
+            t = run_kernel(ref, "curl", P, {1: u, 2: v, 3: w, 4: c, 5: st}, g3)
+            out[f"curl_{tag}"] = dict(params=pb, u=S["u"], v=S["v"], w=S["w"],
+                                      curl=c.reshape(n + (4,)), stats=st.view(np.float32))
+            print(f"curl {tag} {t:.1f}s", flush=True)
+        if want("adv_vel"):
+            u, v, w = flat(S["u"]), flat(S["v"]), flat(S["w"])
+            hu, hv, hw = np.zeros_like(u), np.zeros_like(v), np.zeros_like(w)
+            t1 = run_kernel(ref, "adv_vel1", P, {1: u, 2: v, 3: w, 4: hu, 5: hv, 6: hw}, gv)
+            ou, ov, ow = np.zeros_like(u), np.zeros_like(v), np.zeros_like(w)
+            fl = flat(S["flags"])
+            t2 = run_kernel(ref, "adv_vel2", P, {1: u, 2: v, 3: w, 4: hu, 5: hv, 6: hw, 7: ou,
+                                                 8: ov, 9: ow, 10: fl}, gv)
+            nv = (nz + 1, ny + 1, nx + 1)
+            out[f"adv_vel_{tag}"] = dict(params=pb, u=S["u"], v=S["v"], w=S["w"], flags=S["flags"],
+                                         hu=hu.reshape(nv), hv=hv.reshape(nv), hw=hw.reshape(nv),
+                                         ou=ou.reshape(nv), ov=ov.reshape(nv), ow=ow.reshape(nv))
+            print(f"adv_vel {tag} {t1:.1f}+{t2:.1f}s", flush=True)
+        if want("adv_scalars"):
+            u, v, w = flat(S["u"]), flat(S["v"]), flat(S["w"])
+            s0, s1 = flat(S["s0"]), flat(S["s1"])
+            h0, h1 = np.zeros_like(s0), np.zeros_like(s1)
+            t1 = run_kernel(ref, "adv_s1", P, {1: u, 2: v, 3: w, 4: s0, 5: s1, 6: h0, 7: h1}, g3)
+            o0, o1 = np.zeros_like(s0), np.zeros_like(s1)
+            t2 = run_kernel(ref, "adv_s2", P, {1: u, 2: v, 3: w, 4: s0, 5: s1, 6: h0, 7: h1,
+                                               8: o0, 9: o1}, g3)
+            out[f"adv_scalars_{tag}"] = dict(params=pb, u=S["u"], v=S["v"], w=S["w"], s0=S["s0"],
+                                             s1=S["s1"], h0=h0.reshape(n + (4,)),
+                                             h1=h1.reshape(n + (4,)), o0=o0.reshape(n + (4,)),
+                                             o1=o1.reshape(n + (4,)))
+            print(f"adv_scalars {tag} {t1:.1f}+{t2:.1f}s", flush=True)
+        if want("react"):
+            s0, s1 = flat(S["s0"]), flat(S["s1"])
+            o0, o1 = np.zeros_like(s0), np.zeros_like(s1)
+            st = stats_buf()
+            t = run_kernel(ref, "react", P, {1: s0, 2: s1, 3: o0, 4: o1, 5: flat(S["flags"]),
+                                             6: flat(S["sol"]), 7: flat(S["pyr"]),
+                                             8: flat(S["curl"]), 9: st}, g3)
+            out[f"react_{tag}"] = dict(params=pb, s0=S["s0"], s1=S["s1"], flags=S["flags"],
+                                       sol=S["sol"], pyr=S["pyr"], curl=S["curl"],
+                                       o0=o0.reshape(n + (4,)), o1=o1.reshape(n + (4,)),
+                                       stats=st.view(np.float32))
+            print(f"react {tag} {t:.1f}s", flush=True)
+        if want("forces"):
+            u, v, w = flat(S["u"]), flat(S["v"]), flat(S["w"])
+            t = run_kernel(ref, "forces", P, {1: u, 2: v, 3: w, 4: flat(S["s0"]),
+                                              5: flat(S["s1"]), 6: flat(S["curl"]),
+                                              7: flat(S["flags"])}, gv)
+            nv = (nz + 1, ny + 1, nx + 1)
+            out[f"forces_{tag}"] = dict(params=pb, u=S["u"], v=S["v"], w=S["w"], s0=S["s0"],
+                                        s1=S["s1"], curl=S["curl"], flags=S["flags"],
+                                        ou=u.reshape(nv), ov=v.reshape(nv), ow=w.reshape(nv))
+            print(f"forces {tag} {t:.1f}s", flush=True)
+        if want("divergence"):
+            b = np.zeros(nx * ny * nz, np.float32)
+            t = run_kernel(ref, "divergence", P, {1: flat(S["u"]), 2: flat(S["v"]),
+                                                  3: flat(S["w"]), 4: flat(S["s1"]),
+                                                  5: flat(S["flags"]), 6: b}, g3)
+            out[f"divergence_{tag}"] = dict(params=pb, u=S["u"], v=S["v"], w=S["w"], s1=S["s1"],
+                                            flags=S["flags"], b=b.reshape(n))
+            print(f"divergence {tag} {t:.1f}s", flush=True)
+        if want("project"):
+            u, v, w = flat(S["u"]), flat(S["v"]), flat(S["w"])
+            t = run_kernel(ref, "project", P, {1: u, 2: v, 3: w, 4: flat(S["phi"]),
+                                               5: flat(S["flags"])}, gv)
+            nv = (nz + 1, ny + 1, nx + 1)
+            out[f"project_{tag}"] = dict(params=pb, u=S["u"], v=S["v"], w=S["w"], phi=S["phi"],
+                                         flags=S["flags"], ou=u.reshape(nv), ov=v.reshape(nv),
+                                         ow=w.reshape(nv))
+            print(f"project {tag} {t:.1f}s", flush=True)
+    return out
+
+
+def lv(d, h):
+    return {"nx": np.uint32(d[0]), "ny": np.uint32(d[1]), "nz": np.uint32(d[2]), "h": np.float32(h)}
+
+
+def gen_mg(ref, only):
+    out = {}
+    if only is not None and not ({"mg"} & set(only)):
+        return out
+    rng = np.random.default_rng(21)
+    nx, ny, nz = MG_DIMS
+    n = (nz, ny, nx)
+    h = 0.1
+    f = (rng.random(n) < 0.2).astype(np.uint32)
+    b = rng.normal(0, 1, n).astype(np.float32)
+    p = rng.normal(0, 1, n).astype(np.float32)
+    # smoother: colour 0/1, omega 1 and 1.6
+    for color, om in [(0, 1.0), (1, 1.0), (0, 1.6), (1, 1.6)]:
+        pp = flat(p)
+        m = wgsl.Module(ref.assemble("mg_smooth"), overrides={"COLOR": color, "OMEGA": om},
+                        replace=IDENT)
+        m.bind(0, lv((nx, ny, nz), h))
+        m.bind(1, flat(b))
+        m.bind(2, flat(f))
+        m.bind(3, pp)
+        m.dispatch(groups3(((nx + 1) // 2, ny, nz)))
+        out[f"mg_smooth_c{color}_w{int(om * 10)}"] = dict(dims=np.array(MG_DIMS), h=np.float32(h),
+                                                         b=b, f=f, p=p, out=pp.reshape(n))
+    # restrict
+    cd = tuple((v + 1) // 2 for v in MG_DIMS)
+    cn = (cd[2], cd[1], cd[0])
+    bc = np.zeros(cd[0] * cd[1] * cd[2], np.float32)
+    pc = np.ones_like(bc)
+    fc = np.zeros(cd[0] * cd[1] * cd[2], np.uint32)
+    m = wgsl.Module(ref.assemble("mg_restrict"), replace=IDENT)
+    m.bind(0, lv(MG_DIMS, h))
+    m.bind(1, flat(p))
+    m.bind(2, flat(b))
+    m.bind(3, flat(f))
+    m.bind(4, bc)
+    m.bind(5, pc)
+    m.bind(6, fc)
+    m.bind(7, lv(cd, 2 * h))
+    m.dispatch(groups3(cd))
+    out["mg_restrict"] = dict(dims=np.array(MG_DIMS), h=np.float32(h), b=b, f=f, p=p,
+                              bc=bc.reshape(cn), pc=pc.reshape(cn), fc=fc.reshape(cn))
+    # prolong (coarse flags from the restriction above)
+    pcv = rng.normal(0, 1, cn).astype(np.float32)
+    pf = flat(p)
+    m = wgsl.Module(ref.assemble("mg_prolong"), replace=IDENT)
+    m.bind(0, lv(MG_DIMS, h))
+    m.bind(1, flat(pcv))
+    m.bind(2, flat(f))
+    m.bind(3, pf)
+    m.bind(4, lv(cd, 2 * h))
+    m.bind(5, fc.copy())
+    m.dispatch(groups3(MG_DIMS))
+    out["mg_prolong"] = dict(dims=np.array(MG_DIMS), pc=pcv, f=f, fc=fc.reshape(cn), p=p,
+                             out=pf.reshape(n))
+    # residual sums
+    st = stats_buf()
+    m = wgsl.Module(ref.assemble("mg_resid"), replace=IDENT)
+    m.bind(0, lv(MG_DIMS, h))
+    m.bind(1, flat(p))
+    m.bind(2, flat(b))
+    m.bind(3, flat(f))
+    m.bind(4, st)
+    m.dispatch(groups3(MG_DIMS))
+    out["mg_resid"] = dict(dims=np.array(MG_DIMS), h=np.float32(h), b=b, f=f, p=p,
+                           stats=st.view(np.float32))
+    print("mg done", flush=True)
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--only", default=None)
+    a = ap.parse_args()
+    only = set(a.only.split(",")) if a.only else None
+    ref = Ref(a.ref)
+    out = {}
+    out.update(gen_sim(ref, only))
+    out.update(gen_mg(ref, only))
+    for k, d in out.items():
+        np.savez_compressed(os.path.join(HERE, k + ".npz"), **d)
+    print(f"wrote {len(out)} fixtures to {HERE}")
+
+
+if __name__ == "__main__":
+    main()
