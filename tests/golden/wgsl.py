@@ -108,6 +108,12 @@ class Parser:
             out.append((name, args))
         return out
 
+    def _split_shift(self):
+        """Inside a template list '>>' closes two lists."""
+        if self.peek()[1] == ">>":
+            self.t[self.i] = ("op", ">")
+            self.t.insert(self.i + 1, ("op", ">"))
+
     def type_(self):
         name = self.ident()
         params = []
@@ -118,6 +124,7 @@ class Parser:
                     params.append(("num", self.next()[1]))
                 else:
                     params.append(self.type_())
+                self._split_shift()
                 if self.accept(">"):
                     break
                 self.expect(",")
