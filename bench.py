@@ -3,9 +3,10 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload pool_2cm|pool_small_8cm|pallets_5cm|bonfire_10cm]
 
-Workload (default): the 1 m n-heptane pool fire on a 2 cm grid at the named
-shape 150 x 365 x 150 = 8.21 M cells (x, y up, z), a synthetic scene of that
-shape (scene file pyro_b200/scenes/pool_2cm.toml with exact dims).  Before
+Workload (default): the 1 m n-heptane pool fire on a 2 cm grid,
+160 x 320 x 160 = 8.19 M cells (x, y up, z; scene file
+pyro_b200/scenes/pool_2cm.toml, synthetic: random-free scene geometry, no
+dataset).  Before
 timing, the scene is simulated for --preroll-s seconds (default 1.0 s) so the
 flame and plume are developed; then W warm-up substeps; then exactly K timed
 substeps with dt from the CFL rule of the reference frame loop
@@ -52,11 +53,14 @@ sys.path.insert(0, ROOT)
 faulthandler.enable()
 METRIC = "2cm pool-fire ms/step"
 UNIT = "ms/step"
+# Scene files with the reference's grid rule (every dimension a multiple of
+# 16): the reference V-cycle needs dimensions that halve evenly at every
+# level, and diverges on odd coarse dimensions (e.g. 150 x 365 x 150).
 WORKLOADS = {
-    "pool_2cm": ("pool_2cm.toml", [150, 365, 150]),
-    "pool_small_8cm": ("pool_small_8cm.toml", [38, 75, 38]),
-    "pallets_5cm": ("pallets_5cm.toml", [120, 240, 120]),
-    "bonfire_10cm": ("bonfire_10cm.toml", [160, 240, 160]),
+    "pool_2cm": "pool_2cm.toml",              # 160 x 320 x 160 = 8.19 M cells
+    "pool_small_8cm": "pool_small_8cm.toml",  # 32 x 80 x 32
+    "pallets_5cm": "pallets_5cm.toml",        # 128 x 240 x 128
+    "bonfire_10cm": "bonfire_10cm.toml",      # 160 x 240 x 160
 }
 # Algorithmic bytes per cell per launch (each distinct array element read or
 # written once at the reference's width; read-modify-write twice).
@@ -147,10 +151,7 @@ class ClockSampler:
 
 def build_workload(name):
     from pyro_b200.scene import Scene
-    fname, dims = WORKLOADS[name]
-    sc = Scene.load(os.path.join(ROOT, "pyro_b200", "scenes", fname))
-    sc.dims_override = list(dims)
-    return sc
+    return Scene.load(os.path.join(ROOT, "pyro_b200", "scenes", WORKLOADS[name]))
 
 
 def cfl_substeps(sc, max_u):

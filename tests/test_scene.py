@@ -109,7 +109,7 @@ def test_params_block_layout_and_constants():
 def test_scene_files_parse():
     files = sorted(glob.glob(os.path.join(SCENES, "*.toml")))
     assert len(files) >= 4
-    expect = {"pool_small_8cm": [32, 80, 32], "pool_2cm": [144, 368, 144],
+    expect = {"pool_small_8cm": [32, 80, 32], "pool_2cm": [160, 320, 160],
               "pallets_5cm": [128, 240, 128], "bonfire_10cm": [160, 240, 160]}
     for f in files:
         sc = Scene.load(f)
