@@ -219,6 +219,16 @@ struct Vel {
     F3 u2 = at(g, x + (0.5f * k) * u1);
     return x + k * u2;
   }
+  // Both traces from x; the velocity at x (identical in the two traces)
+  // is sampled once.
+  __device__ __forceinline__ void both(const Grid& g, float k, F3 x, F3& b, F3& f) const {
+    F3 u1 = at(g, x);
+    F3 h = (0.5f * k) * u1;
+    F3 ub = at(g, x - h);
+    F3 uf = at(g, x + h);
+    b = x - k * ub;
+    f = x + k * uf;
+  }
 };
 
 // -------------------------------------------------------------- statistics

@@ -13,8 +13,9 @@
 //   mg_prolong   mg.wgsl:85-120 fluid-weighted trilinear correction
 //   mg_resid     mg.wgsl:122-158 sums of r^2 and b^2
 //   mg_coarse    the whole coarsest-level solve (src/sim.rs:473: 80 SOR
-//                sweeps at omega 1.6) in one CTA with the level in shared
-//                memory, replacing 160 dispatches.
+//                sweeps at omega 1.6) in one thread-block cluster with the
+//                level in distributed shared memory, replacing 160 dispatches.
+#include <cooperative_groups.h>
 #include <cuda_bf16.h>
 
 #include "common.cuh"
@@ -192,53 +193,109 @@ __global__ void __launch_bounds__(256) k_mg_resid(Lvl d, float h2, const float* 
 }
 
 // ------------------------------------------------------------ coarse solve
-// One CTA of 1024 threads; thread t owns the (x, y) column t of the level
-// and walks z over the cells of the colour being swept.  phi, h^2 b and the
-// solid flags of the whole level live in shared memory (9 bytes per cell).
+// The coarsest level is swept 80 times per V-cycle (src/sim.rs:473), 160
+// dependent red-black passes over ~10-30 k cells.  One thread-block cluster
+// of up to 16 CTAs runs them all in a single launch: CTA r owns z-planes
+// [r*nz/C, (r+1)*nz/C) of phi in its shared memory, a thread owns up to
+// COARSE_K cells with their neighbour mask, count and h^2 b precomputed in
+// registers, neighbours across a slab boundary are read from the owning
+// CTA's shared memory (distributed shared memory), and the hardware cluster
+// barrier separates the colour passes.  The arithmetic per cell is the
+// reference's, in the same order, so the result equals 160 separate passes.
 constexpr int COARSE_THREADS = 1024;
-constexpr size_t COARSE_SMEM_CAP = 200 * 1024;
+constexpr int COARSE_K = 2;
+constexpr int COARSE_MAX_CLUSTER = 16;
+
+struct CoarseCell {
+  int j;             // index in the own slab (-1: none)
+  uint32_t meta;     // bits 0-5: fluid in-domain neighbour, bit 6: colour, bit 7: skip
+  float cnt;
+  float hb;
+  const float* zp;   // +z neighbour (local or remote), null when absent
+  const float* zm;   // -z neighbour
+};
 
 template <typename TS>
 __global__ void __launch_bounds__(COARSE_THREADS, 1)
-    k_mg_coarse(Lvl d, float h2, const TS* __restrict__ b, const uint32_t* __restrict__ f,
-                TS* __restrict__ p, int iters, float omega, int bc_mode) {
-  extern __shared__ float smem[];
-  const int n = d.nx * d.ny * d.nz;
-  float* sp = smem;
-  float* sb = smem + n;
-  uint8_t* sf = reinterpret_cast<uint8_t*>(smem + 2 * n);
-  for (int j = threadIdx.x; j < n; j += COARSE_THREADS) {
-    sp[j] = ldv(p + j);
-    sb[j] = h2 * ldv(b + j);
-    sf[j] = (uint8_t)(f[j] == 1u);
-  }
-  const int t = threadIdx.x;
-  const bool own = t < d.nx * d.ny;
-  const int x = own ? t % d.nx : 0;
-  const int y = own ? t / d.nx : 0;
+    k_mg_coarse_cluster(Lvl d, float h2, const TS* __restrict__ b,
+                        const uint32_t* __restrict__ f, TS* __restrict__ p, int iters,
+                        float omega, int bc_mode) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  extern __shared__ float sp[];
+  const int C = (int)cl.num_blocks();
+  const int rank = (int)cl.block_rank();
   const int plane = d.nx * d.ny;
-  __syncthreads();
+  const int z0 = rank * d.nz / C, z1 = (rank + 1) * d.nz / C;
+  const int own = (z1 - z0) * plane;
+  for (int j = threadIdx.x; j < own; j += COARSE_THREADS) sp[j] = ldv(p + z0 * plane + j);
+  cl.sync();  // every slab is loaded before any remote read
+  CoarseCell cell[COARSE_K];
+#pragma unroll
+  for (int r = 0; r < COARSE_K; r++) {
+    int j = threadIdx.x + r * COARSE_THREADS;
+    cell[r].j = -1;
+    cell[r].meta = 0x80u;
+    cell[r].cnt = 1.0f;
+    cell[r].hb = 0.0f;
+    cell[r].zp = nullptr;
+    cell[r].zm = nullptr;
+    if (j >= own) continue;
+    int zl = j / plane, rem = j - zl * plane;
+    int y = rem / d.nx, x = rem - y * d.nx, z = z0 + zl;
+    int gi = d.idx(x, y, z);
+    cell[r].j = j;
+    uint32_t meta = (uint32_t)((x + y + z) & 1) << 6;
+    float cnt = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+      int ax = x + (k == 0) - (k == 1), ay = y + (k == 2) - (k == 3), az = z + (k == 4) - (k == 5);
+      if (ay < 0) continue;
+      if (!d.inb(ax, ay, az)) {
+        if (bc_mode == 0 || ay >= d.ny) cnt += 1.0f;
+        continue;
+      }
+      if (f[d.idx(ax, ay, az)] == 1u) continue;
+      meta |= 1u << k;
+      cnt += 1.0f;
+      if (k >= 4) {
+        // owner of plane az and its slab-local index
+        int o = 0;
+        while (o + 1 < C && (o + 1) * d.nz / C <= az) o++;
+        const float* base = (az >= z0 && az < z1) ? sp : cl.map_shared_rank(sp, o);
+        int oz0 = o * d.nz / C;
+        const float* q = base + (az - oz0) * plane + rem;
+        if (k == 4) cell[r].zp = q; else cell[r].zm = q;
+      }
+    }
+    if (f[gi] == 1u || cnt < 0.5f) meta |= 0x80u;
+    cell[r].meta = meta;
+    cell[r].cnt = cnt;
+    cell[r].hb = h2 * ldv(b + gi);
+  }
+  const int nx = d.nx;
 #pragma unroll 1
   for (int it = 0; it < iters; it++) {
-#pragma unroll 1
+#pragma unroll
     for (int c = 0; c < 2; c++) {
-      if (own) {
-        // colour c of cell (x,y,z) is (x+y+z)&1
-#pragma unroll 1
-        for (int z = (c + x + y) & 1; z < d.nz; z += 2) {
-          int i = t + plane * z;
-          if (sf[i]) continue;
-          float sum, cnt;
-          neigh_sum(
-              d, x, y, z, bc_mode, [&](int j) { return sp[j]; },
-              [&](int j) { return sf[j] != 0; }, sum, cnt);
-          if (cnt >= 0.5f) sp[i] = wmix(sp[i], (sum - sb[i]) / cnt, omega);
-        }
+#pragma unroll
+      for (int r = 0; r < COARSE_K; r++) {
+        uint32_t m = cell[r].meta;
+        if ((m & 0x80u) || ((m >> 6) & 1u) != (uint32_t)c) continue;
+        int j = cell[r].j;
+        float sum = 0.0f;
+        if (m & 1u) sum += sp[j + 1];
+        if (m & 2u) sum += sp[j - 1];
+        if (m & 4u) sum += sp[j + nx];
+        if (m & 8u) sum += sp[j - nx];
+        if (m & 16u) sum += *cell[r].zp;
+        if (m & 32u) sum += *cell[r].zm;
+        sp[j] = wmix(sp[j], (sum - cell[r].hb) / cell[r].cnt, omega);
       }
-      __syncthreads();
+      cl.sync();
     }
   }
-  for (int j = threadIdx.x; j < n; j += COARSE_THREADS) stv(p + j, sp[j]);
+  for (int j = threadIdx.x; j < own; j += COARSE_THREADS) stv(p + z0 * plane + j, sp[j]);
 }
 
 __global__ void k_f32_to_bf16(const float* __restrict__ a, __nv_bfloat16* __restrict__ b,
@@ -278,25 +335,69 @@ cudaError_t mg_prolong_t(Dims3 df, const TS* pc, const uint32_t* ff, TS* pf, Dim
   return cudaGetLastError();
 }
 
+// Cluster size for a level: the largest of 16 / 8 whose slabs keep every
+// CTA within COARSE_K cells per thread and the level fits the cluster.
+int coarse_cluster_size(Dims3 d) {
+  for (int C : {COARSE_MAX_CLUSTER, 8}) {
+    if (d.nz < 1) return 0;
+    int max_planes = (d.nz + C - 1) / C;
+    size_t own = (size_t)max_planes * d.nx * d.ny;
+    if (own <= (size_t)COARSE_K * COARSE_THREADS && own * 4 <= 200 * 1024) return C;
+  }
+  return 0;
+}
+
 template <typename TS>
 cudaError_t mg_coarse_t(Dims3 d, float h, const TS* b, const uint32_t* f, TS* p, int iters,
                         float omega, int bc_mode, cudaStream_t st) {
-  if (!mg_coarse_fits(d)) return cudaErrorInvalidValue;
-  cudaError_t e = cudaFuncSetAttribute(k_mg_coarse<TS>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)COARSE_SMEM_CAP);
-  if (e != cudaSuccess) return e;
-  k_mg_coarse<TS><<<1, COARSE_THREADS, d.cells() * 9, st>>>(Lvl{d.nx, d.ny, d.nz}, h * h, b, f,
-                                                           p, iters, omega, bc_mode);
-  return cudaGetLastError();
+  static int attr_done = 0;  // attributes are per function, set once
+  static int max_cluster = 0;
+  cudaError_t e;
+  if (!(attr_done & (1 << sizeof(TS)))) {
+    e = cudaFuncSetAttribute(k_mg_coarse_cluster<TS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             200 * 1024);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_mg_coarse_cluster<TS>,
+                             cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e != cudaSuccess) return e;
+    attr_done |= 1 << sizeof(TS);
+    // the largest cluster this device co-schedules at this CTA shape
+    cudaLaunchConfig_t q = {};
+    q.gridDim = dim3(COARSE_MAX_CLUSTER, 1, 1);
+    q.blockDim = dim3(COARSE_THREADS, 1, 1);
+    q.dynamicSmemBytes = 64 * 1024;
+    int mc = 0;
+    if (cudaOccupancyMaxPotentialClusterSize(&mc, k_mg_coarse_cluster<TS>, &q) != cudaSuccess)
+      mc = 8;
+    max_cluster = mc >= COARSE_MAX_CLUSTER ? COARSE_MAX_CLUSTER : 8;
+  }
+  int C = coarse_cluster_size(d);
+  if (C > max_cluster) C = (max_cluster >= 8 && coarse_cluster_size(d) != 0) ? 8 : 0;
+  if (C == 0) return cudaErrorInvalidValue;
+  {
+    size_t own = (size_t)((d.nz + C - 1) / C) * d.nx * d.ny;
+    if (own > (size_t)COARSE_K * COARSE_THREADS) return cudaErrorInvalidValue;
+  }
+  size_t smem = (size_t)((d.nz + C - 1) / C) * d.nx * d.ny * 4;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)C, 1, 1);
+  cfg.blockDim = dim3(COARSE_THREADS, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = (unsigned)C;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_mg_coarse_cluster<TS>, Lvl{d.nx, d.ny, d.nz}, h * h, b, f, p,
+                            iters, omega, bc_mode);
 }
 
 }  // namespace
 
-bool mg_coarse_fits(Dims3 d) {
-  size_t n = d.cells();
-  return d.nx * d.ny <= COARSE_THREADS && n * 9 <= COARSE_SMEM_CAP;
-}
+bool mg_coarse_fits(Dims3 d) { return coarse_cluster_size(d) != 0; }
 
 cudaError_t launch_mg_smooth(Dims3 d, float h, const float* b, const uint32_t* f, float* p,
                              int color, float omega, int bc_mode, cudaStream_t st) {

@@ -252,7 +252,7 @@ __global__ void __launch_bounds__(256) k_adv_vel1(const PyroParams* __restrict__
   const float kk = Pp->dt / Pp->dx;
   Vel V{u, v, w};
   int i = g.vidx(c);
-#pragma unroll 1
+#pragma unroll
   for (int k = 0; k < 3; k++) {
     if (!g.compValid(k, c)) continue;
     F3 off = compOff(k);
@@ -278,7 +278,7 @@ __global__ void __launch_bounds__(256) k_adv_vel2(const PyroParams* __restrict__
   Vel V{u, v, w};
   int i = g.vidx(c);
   bool sc = g.inb(c) && __ldg(flags + g.sidx(c)) == 1u;
-#pragma unroll 1
+#pragma unroll
   for (int k = 0; k < 3; k++) {
     if (!g.compValid(k, c)) continue;
     I3 a = c - unitI(k);
@@ -290,8 +290,10 @@ __global__ void __launch_bounds__(256) k_adv_vel2(const PyroParams* __restrict__
       F3 off = compOff(k);
       I3 hi = g.compHi(k);
       F3 x = tof3(c) + off;
-      F3 b = V.back(g, kk, x) - off;
-      F3 f = V.fwd(g, kk, x) - off;
+      F3 b, f;
+      V.both(g, kk, x, b, f);
+      b = b - off;
+      f = f - off;
       const float* vk = pick3(k, u, v, w);
       const float* hk = pick3(k, hu, hv, hw);
       float lo, hv2;
@@ -339,8 +341,10 @@ __global__ void __launch_bounds__(256) k_adv_s2(const PyroParams* __restrict__ P
   Vel V{u, v, w};
   const F3 half{0.5f, 0.5f, 0.5f};
   F3 x = tof3(c) + half;
-  F3 b = V.back(g, kk, x) - half;
-  F3 f = V.fwd(g, kk, x) - half;
+  F3 b, f;
+  V.both(g, kk, x, b, f);
+  b = b - half;
+  f = f - half;
   int i = g.sidx(c);
   float4 r0 = __ldg(h0 + i), r1 = __ldg(h1 + i);
   if (g.outside(b) <= 0.0f && g.outside(f) <= 0.0f) {
