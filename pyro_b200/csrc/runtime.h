@@ -56,6 +56,8 @@ struct Multigrid {
   std::vector<float*> phi, b;
   std::vector<const uint32_t*> f;
   std::vector<DevBuf> own_phi, own_b, own_f;
+  std::vector<DevBuf> phi2;   // ping-pong partner of phi on every level
+  std::vector<DevBuf> meta;   // per-cell neighbour mask (k_mgf.cu)
   bool coarse_one_cta = false;
   float* stats = nullptr;  // device, for mg_resid
 
@@ -66,13 +68,20 @@ struct Multigrid {
     f[0] = f0;
   }
   size_t levels() const { return dims.size(); }
-  // One smoother pass schedule (src/sim.rs:425-449).
+  // One smoother pass schedule (src/sim.rs:425-449), one launch per colour.
   cudaError_t smooth(int l, int iters, bool coarse, cudaStream_t st);
-  // `cycles` V-cycles (src/sim.rs:451-491) on the bound level-0 arrays.
+  // Coarse solid flags and neighbour masks of every level from the bound
+  // level-0 flags; the V-cycles below need them (once per new flag field).
+  cudaError_t prepare(cudaStream_t st);
+  // `cycles` V-cycles (src/sim.rs:451-491) on the bound level-0 arrays with
+  // the fused kernels (k_mgf.cu); calls prepare() first.
   cudaError_t vcycles(int cycles, cudaStream_t st);
+  // The same schedule with one launch per colour pass (mg.wgsl as written).
+  cudaError_t vcycles_passes(int cycles, cudaStream_t st);
   // One BF16-storage V-cycle as a preconditioner: z = V(r) from a zero
   // guess, with bphi/bb the BF16 level arrays (allocated on first use).
-  cudaError_t vcycles_bf16(int cycles, cudaStream_t st, DevBuf* bphi, DevBuf* bb);
+  cudaError_t vcycles_bf16(int cycles, cudaStream_t st, DevBuf* bphi, DevBuf* bphi2,
+                           DevBuf* bb);
   size_t device_bytes() const;
 };
 

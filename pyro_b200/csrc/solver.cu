@@ -211,7 +211,7 @@ Solver::~Solver() {
 
 size_t Solver::device_bytes() const {
   size_t s = r.bytes + z.bytes + p.bytes + q.bytes + sc.bytes;
-  for (int l = 0; l < 4; l++) s += bphi[l].bytes + bb[l].bytes;
+  for (int l = 0; l < 4; l++) s += bphi[l].bytes + bphi2[l].bytes + bb[l].bytes;
   return s;
 }
 
@@ -239,7 +239,7 @@ cudaError_t Solver::precond(cudaStream_t st, bool bf16) {
   float* save_b = mg->b[0];
   const uint32_t* save_f = mg->f[0];
   mg->bind_level0(z.as<float>(), r.as<float>(), save_f);
-  e = bf16 ? mg->vcycles_bf16(1, st, bphi, bb) : mg->vcycles(1, st);
+  e = bf16 ? mg->vcycles_bf16(1, st, bphi, bphi2, bb) : mg->vcycles(1, st);
   mg->bind_level0(save_phi, save_b, save_f);
   return e;
 }

@@ -15,7 +15,7 @@ struct Solver {
   DevBuf sc;                // FP64 device scalars
   double* host_sc = nullptr;  // pinned mirror
   // BF16 hierarchy for the low-precision preconditioner
-  DevBuf bphi[4], bb[4];
+  DevBuf bphi[4], bphi2[4], bb[4];
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
   int init(Multigrid* m);
