@@ -111,9 +111,14 @@ int pyro_k_forces(const PyroParams* params_dev, uint32_t nx, uint32_t ny, uint32
                   const uint32_t* flags, void* stream) {
   KDIMS(pyro_k_forces)
   PYRO_REQUIRE(u && v && w && s0 && s1 && curl && flags, "pyro_k_forces: null buffer");
-  return ret(launch_forces(params_dev, d, u, v, w, (const float4*)s0, (const float4*)s1,
-                           (const float4*)curl, flags, S(stream)),
-             "pyro_k_forces");
+  DevBuf conf;
+  int rc = conf.alloc(d.cells() * 16);
+  if (rc != PYRO_OK) return rc;
+  rc = ret(launch_forces(params_dev, d, u, v, w, (const float4*)s0, (const float4*)s1,
+                         (const float4*)curl, conf.as<float4>(), flags, S(stream)),
+           "pyro_k_forces");
+  if (rc == PYRO_OK) PYRO_CU(cudaStreamSynchronize(S(stream)));
+  return rc;
 }
 
 int pyro_k_divergence(const PyroParams* params_dev, uint32_t nx, uint32_t ny, uint32_t nz,

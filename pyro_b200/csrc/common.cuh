@@ -200,14 +200,48 @@ __device__ __forceinline__ void mmS(const float4* __restrict__ X, const Grid& gr
   }
 }
 
+// One axis of a trilinear sample: clamp to [0, hi], base cell
+// min(floor, hi - 1), fraction and its complement (tmpl_comp.wgsl:3-5).
+struct Axis {
+  int b;
+  float f, omf;
+};
+__device__ __forceinline__ Axis axis(float g0, int hi) {
+  float g = wclamp(g0, 0.0f, (float)hi);
+  int b = min((int)floorf(g), hi - 1);
+  float f = g - (float)b;
+  return Axis{b, f, 1.0f - f};
+}
+// Trilinear sample of a staggered component from prepared axes
+// (tmpl_comp.wgsl:6-14; mix(a,b,t) = a*(1-t) + b*t).
+__device__ __forceinline__ float tri_axes(const float* __restrict__ X, const Grid& gr, Axis ax,
+                                          Axis ay, Axis az) {
+  const int sy = gr.nx + 1, sz = (gr.nx + 1) * (gr.ny + 1);
+  int i = ax.b + sy * ay.b + sz * az.b;
+  float c00 = __ldg(X + i) * ax.omf + __ldg(X + i + 1) * ax.f;
+  float c10 = __ldg(X + i + sy) * ax.omf + __ldg(X + i + sy + 1) * ax.f;
+  float c01 = __ldg(X + i + sz) * ax.omf + __ldg(X + i + sz + 1) * ax.f;
+  float c11 = __ldg(X + i + sy + sz) * ax.omf + __ldg(X + i + sy + sz + 1) * ax.f;
+  float c0 = c00 * ay.omf + c10 * ay.f;
+  float c1 = c01 * ay.omf + c11 * ay.f;
+  return c0 * az.omf + c1 * az.f;
+}
+
 // Staggered velocity and RK2 traces in grid units (vel.wgsl:2-19).
 struct Vel {
   const float* __restrict__ u;
   const float* __restrict__ v;
   const float* __restrict__ w;
+  // velAt(p): u at p - (0,.5,.5) clamped to (nx, ny-1, nz-1), v at
+  // p - (.5,0,.5) to (nx-1, ny, nz-1), w at p - (.5,.5,0) to
+  // (nx-1, ny-1, nz).  Per axis only two offset/bound pairs occur, so six
+  // axis set-ups serve the three samples.
   __device__ __forceinline__ F3 at(const Grid& g, F3 p) const {
-    return F3{triC(u, g, p - compOff(0), g.compHi(0)), triC(v, g, p - compOff(1), g.compHi(1)),
-              triC(w, g, p - compOff(2), g.compHi(2))};
+    Axis xu = axis(p.x - 0.0f, g.nx), xvw = axis(p.x - 0.5f, g.nx - 1);
+    Axis yv = axis(p.y - 0.0f, g.ny), yuw = axis(p.y - 0.5f, g.ny - 1);
+    Axis zw = axis(p.z - 0.0f, g.nz), zuv = axis(p.z - 0.5f, g.nz - 1);
+    return F3{tri_axes(u, g, xu, yuw, zuv), tri_axes(v, g, xvw, yv, zuv),
+              tri_axes(w, g, xvw, yuw, zw)};
   }
   __device__ __forceinline__ F3 back(const Grid& g, float k, F3 x) const {
     F3 u1 = at(g, x);

@@ -16,6 +16,7 @@
 //                sweeps at omega 1.6) in one thread-block cluster with the
 //                level in distributed shared memory, replacing 160 dispatches.
 #include <cooperative_groups.h>
+#include <cstdlib>
 #include <cuda_bf16.h>
 
 #include "common.cuh"
@@ -370,6 +371,9 @@ cudaError_t mg_coarse_t(Dims3 d, float h, const TS* b, const uint32_t* f, TS* p,
     if (cudaOccupancyMaxPotentialClusterSize(&mc, k_mg_coarse_cluster<TS>, &q) != cudaSuccess)
       mc = 8;
     max_cluster = mc >= COARSE_MAX_CLUSTER ? COARSE_MAX_CLUSTER : 8;
+    // tuning knob: PYRO_COARSE_CLUSTER=8 caps the cluster at 8 CTAs
+    const char* env = getenv("PYRO_COARSE_CLUSTER");
+    if (env && atoi(env) == 8) max_cluster = 8;
   }
   int C = coarse_cluster_size(d);
   if (C > max_cluster) C = (max_cluster >= 8 && coarse_cluster_size(d) != 0) ? 8 : 0;

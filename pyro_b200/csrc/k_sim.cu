@@ -511,90 +511,91 @@ __global__ void __launch_bounds__(256) k_react(const PyroParams* __restrict__ Pp
 }
 
 // ------------------------------------------------------------------ forces
-struct ForceCtx {
-  const PyroParams& P;
-  Grid g;
-  const float4* __restrict__ s0;
-  const float4* __restrict__ s1;
-  const float4* __restrict__ curl;
-  __device__ __forceinline__ float cm(I3 c) const { return __ldg(curl + g.sidx(g.clampC(c))).w; }
-  // fluid.wgsl:167-181: vorticity confinement body force at a cell centre.
-  __device__ F3 confine(I3 c) const {
-    int i = g.sidx(c);
-    float4 a = __ldg(s0 + i);
-    float T = a.x;
-    float smoke = a.w + __ldg(s1 + i).x;
-    float gate = fmaxf(smoothstep(P.vort_t, P.vort_t + 500.0f, T),
-                       0.35f * smoothstep(0.0f, 2e-4f, smoke));
-    if (gate <= 0.0f) return F3{0.0f, 0.0f, 0.0f};
+// Vorticity-confinement body force at each cell centre (fluid.wgsl:167-181),
+// computed once per cell; forces adds the two cells' vectors per face
+// exactly as the reference's fc += confine(a); fc += confine(c).
+__global__ void __launch_bounds__(256) k_confine(const PyroParams* __restrict__ Pp, Grid g,
+                                                 const float4* __restrict__ s0,
+                                                 const float4* __restrict__ s1,
+                                                 const float4* __restrict__ curl,
+                                                 float4* __restrict__ conf) {
+  I3 c = thread_cell();
+  if (!g.inb(c)) return;
+  const PyroParams& P = *Pp;
+  int i = g.sidx(c);
+  float4 a = __ldg(s0 + i);
+  float T = a.x;
+  float smoke = a.w + __ldg(s1 + i).x;
+  float gate = fmaxf(smoothstep(P.vort_t, P.vort_t + 500.0f, T),
+                     0.35f * smoothstep(0.0f, 2e-4f, smoke));
+  F3 f{0.0f, 0.0f, 0.0f};
+  if (gate > 0.0f) {
+    auto cm = [&](I3 q) { return __ldg(curl + g.sidx(g.clampC(q))).w; };
     const I3 X{1, 0, 0}, Y{0, 1, 0}, Z{0, 0, 1};
     F3 gr{cm(c + X) - cm(c - X), cm(c + Y) - cm(c - Y), cm(c + Z) - cm(c - Z)};
     float gl = len3(gr);
-    if (gl < 1e-6f) return F3{0.0f, 0.0f, 0.0f};
-    float4 cw = __ldg(curl + i);
-    F3 f = (P.vort * P.dx) * cross3(gr / gl, F3{cw.x, cw.y, cw.z}) * gate;
-    float fl = len3(f);
-    if (fl > 60.0f) f = f * (60.0f / fl);
-    return f;
+    if (!(gl < 1e-6f)) {
+      float4 cw = __ldg(curl + i);
+      f = (P.vort * P.dx) * cross3(gr / gl, F3{cw.x, cw.y, cw.z}) * gate;
+      float fl = len3(f);
+      if (fl > 60.0f) f = f * (60.0f / fl);
+    }
   }
-};
+  conf[i] = make_float4(f.x, f.y, f.z, 0.0f);
+}
+
+__device__ __forceinline__ float comp4(float4 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
 
 __global__ void __launch_bounds__(256) k_forces(const PyroParams* __restrict__ Pp, Grid g,
                                                 float* __restrict__ u, float* __restrict__ v,
                                                 float* __restrict__ w,
                                                 const float4* __restrict__ s0,
                                                 const float4* __restrict__ s1,
-                                                const float4* __restrict__ curl,
+                                                const float4* __restrict__ conf,
                                                 const uint32_t* __restrict__ flags) {
   I3 c = thread_cell();
   if (c.x > g.nx || c.y > g.ny || c.z > g.nz) return;
   const PyroParams& P = *Pp;
-  ForceCtx C{P, g, s0, s1, curl};
   int i = g.vidx(c);
   bool ib = g.inb(c);
-  bool sc = ib && __ldg(flags + g.sidx(c)) == 1u;
-  F3 fcc{0.0f, 0.0f, 0.0f};
-  bool have_cc = false;
-#pragma unroll 1
+  int ic = ib ? g.sidx(c) : 0;
+  bool sc = ib && __ldg(flags + ic) == 1u;
+  float4 cc = ib ? __ldg(conf + ic) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  float Tc = ib ? __ldg(s0 + ic).x : P.t0;
+  I3 cl = g.clampC(c);
+  float ss = spongeSide(P, g, cl);
+#pragma unroll
   for (int k = 0; k < 3; k++) {
     if (!g.compValid(k, c)) continue;
     I3 a = c - unitI(k);
     bool ia = g.inb(a);
-    bool sa = ia && __ldg(flags + g.sidx(a)) == 1u;
+    int iaa = ia ? g.sidx(a) : 0;
+    bool sa = ia && __ldg(flags + iaa) == 1u;
     if ((k == 1 && c.y == 0) || sc || sa) continue;
     float f = 0.0f;
     if (k == 1) {
       float Ta = P.t0, Tb = P.t0, ma = 0.0f, mb = 0.0f;
-      if (ia) { float4 s = __ldg(s0 + g.sidx(a)); Ta = s.x; ma = s.w + __ldg(s1 + g.sidx(a)).x; }
-      if (ib) { float4 s = __ldg(s0 + g.sidx(c)); Tb = s.x; mb = s.w + __ldg(s1 + g.sidx(c)).x; }
+      if (ia) { float4 s = __ldg(s0 + iaa); Ta = s.x; ma = s.w + __ldg(s1 + iaa).x; }
+      if (ib) { float4 s = __ldg(s0 + ic); Tb = s.x; mb = s.w + __ldg(s1 + ic).x; }
       if (!ia) { Ta = Tb; ma = mb; }
       if (!ib) { Tb = Ta; mb = ma; }
       float Tf = 0.5f * (Ta + Tb);
       f += P.g * P.buoy * (Tf - P.t0) / Tf - P.g * P.smoke_w * 0.5f * (ma + mb);
     }
-    F3 fc{0.0f, 0.0f, 0.0f};
-    float n = 0.0f;
-    if (ia) { fc = fc + C.confine(a); n += 1.0f; }
-    if (ib) {
-      if (!have_cc) { fcc = C.confine(c); have_cc = true; }
-      fc = fc + fcc;
-      n += 1.0f;
-    }
-    if (n > 0.0f) f += (k == 0 ? fc.x : (k == 1 ? fc.y : fc.z)) / n;
+    float fc = 0.0f, n = 0.0f;
+    if (ia) { fc = fc + comp4(__ldg(conf + iaa), k); n += 1.0f; }
+    if (ib) { fc = fc + comp4(cc, k); n += 1.0f; }
+    if (n > 0.0f) f += fc / n;
     float* vk = k == 0 ? u : (k == 1 ? v : w);
     float uu = vk[i];
     uu += f * P.dt;
-    I3 cc = g.clampC(c);
-    float ss = spongeSide(P, g, cc);
     if (k != 1) {
-      float Tl = P.t0;
-      if (ib) Tl = __ldg(s0 + g.sidx(c)).x;
-      float hot = smoothstep(350.0f, 900.0f, Tl);
+      float hot = smoothstep(350.0f, 900.0f, Tc);
       float kr = P.wind_relax * (1.0f - 0.85f * hot) + 8.0f * ss;
       float wv = k == 0 ? P.wind_x : P.wind_z;
       uu = wmix(uu, wv, 1.0f - expf(-kr * P.dt));
     } else {
-      float st = spongeTop(P, g, cc);
+      float st = spongeTop(P, g, cl);
       if (st > 0.0f) uu = wmix(uu, fmaxf(uu, 0.0f), 1.0f - expf(-8.0f * st * P.dt));
     }
     uu = wclamp(uu, -40.0f, 40.0f);
@@ -712,10 +713,11 @@ cudaError_t launch_react(const PyroParams* P, Dims3 d, const float4* s0in, const
 }
 cudaError_t launch_forces(const PyroParams* P, Dims3 d, float* u, float* v, float* w,
                           const float4* s0, const float4* s1, const float4* curl,
-                          const uint32_t* flags, cudaStream_t st) {
+                          float4* conf, const uint32_t* flags, cudaStream_t st) {
   Grid g{d.nx, d.ny, d.nz};
+  k_confine<<<grid_for(d.nx, d.ny, d.nz), PYRO_BLOCK, 0, st>>>(P, g, s0, s1, curl, conf);
   k_forces<<<grid_for(d.nx + 1, d.ny + 1, d.nz + 1), PYRO_BLOCK, 0, st>>>(P, g, u, v, w, s0, s1,
-                                                                         curl, flags);
+                                                                         conf, flags);
   return cudaGetLastError();
 }
 cudaError_t launch_divergence(const PyroParams* P, Dims3 d, const float* u, const float* v,

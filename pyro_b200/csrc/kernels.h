@@ -38,9 +38,11 @@ cudaError_t launch_adv_s2(const PyroParams* P, Dims3 d, const float* u, const fl
 cudaError_t launch_react(const PyroParams* P, Dims3 d, const float4* s0in, const float4* s1in,
                          float4* s0out, float4* s1out, const uint32_t* flags, const float4* sol,
                          const float4* pyr, const float4* curl, float* stats, cudaStream_t st);
+// forces runs a per-cell confinement kernel into `conf` (N float4 scratch)
+// and then the face kernel.
 cudaError_t launch_forces(const PyroParams* P, Dims3 d, float* u, float* v, float* w,
                           const float4* s0, const float4* s1, const float4* curl,
-                          const uint32_t* flags, cudaStream_t st);
+                          float4* conf, const uint32_t* flags, cudaStream_t st);
 cudaError_t launch_divergence(const PyroParams* P, Dims3 d, const float* u, const float* v,
                               const float* w, const float4* s1, const uint32_t* flags, float* b,
                               cudaStream_t st);

@@ -104,7 +104,7 @@ struct PyroSim {
                           curl.as<float4>(), S, st)) != cudaSuccess)
       return e;
     if ((e = launch_forces(P, d, ub, vb, wb, s0.as<float4>(), s1.as<float4>(), curl.as<float4>(),
-                           flags.as<uint32_t>(), st)) != cudaSuccess)
+                           h0.as<float4>(), flags.as<uint32_t>(), st)) != cudaSuccess)
       return e;
     return launch_divergence(P, d, ub, vb, wb, s1.as<float4>(), flags.as<uint32_t>(),
                              b0.as<float>(), st);
@@ -368,7 +368,7 @@ int pyro_sim_profile_step(PyroSim* S, float dt, float time, float ign_on, int wa
   mark();
   if (e == cudaSuccess)
     e = launch_forces(P, S->d, ub, vb, wb, S->s0.as<float4>(), S->s1.as<float4>(),
-                      S->curl.as<float4>(), S->flags.as<uint32_t>(), st);
+                      S->curl.as<float4>(), S->h0.as<float4>(), S->flags.as<uint32_t>(), st);
   mark();
   if (e == cudaSuccess)
     e = launch_divergence(P, S->d, ub, vb, wb, S->s1.as<float4>(), S->flags.as<uint32_t>(),
