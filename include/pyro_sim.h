@@ -245,6 +245,24 @@ int pyro_k_forces(const PyroParams* params_dev, uint32_t nx, uint32_t ny,
                   uint32_t nz, float* u, float* v, float* w, const float* s0,
                   const float* s1, const float* curl, const uint32_t* flags,
                   void* stream);
+/* pyro_k_forces without any device allocation (no counterpart in the
+ * reference).  For callers that cannot allocate device memory -- code running
+ * while another thread captures a CUDA graph, hosts whose pool allocator owns
+ * all device memory, loops that cannot afford cudaMalloc's implicit
+ * synchronisation -- the per-cell confinement scratch lives in a fixed
+ * device array of PYRO_NOALLOC_MAX_CELLS float4 (8 MiB) that the library
+ * holds on every GPU that loads it until the process exits.  Grids with more
+ * cells are rejected with PYRO_E_INVALID.  The first call on a device, with
+ * that device current, looks up the array's device address; make that first
+ * call before any stream capture.  All calls share the one array: calls that
+ * overlap on the GPU (different streams, other threads) race on it and must
+ * be serialised by the caller.  Results equal pyro_k_forces. */
+#define PYRO_NOALLOC_MAX_CELLS (1u << 19)
+int pyro_k_forces_noalloc(const PyroParams* params_dev, uint32_t nx,
+                          uint32_t ny, uint32_t nz, float* u, float* v,
+                          float* w, const float* s0, const float* s1,
+                          const float* curl, const uint32_t* flags,
+                          void* stream);
 int pyro_k_divergence(const PyroParams* params_dev, uint32_t nx, uint32_t ny,
                       uint32_t nz, const float* u, const float* v,
                       const float* w, const float* s1, const uint32_t* flags,

@@ -19,6 +19,7 @@ PYRO_E_NOCONV = -5
 PYRO_E_TIMEOUT = -6
 
 STATS_N = 1040
+NOALLOC_MAX_CELLS = 1 << 19
 MAX_LAYERS = 1024
 ABI_VERSION = 1
 
@@ -140,6 +141,7 @@ SIGNATURES = {
     "pyro_k_adv_scalars": [_P, _U32, _U32, _U32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
     "pyro_k_react": [_P, _U32, _U32, _U32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
     "pyro_k_forces": [_P, _U32, _U32, _U32, _P, _P, _P, _P, _P, _P, _P, _P],
+    "pyro_k_forces_noalloc": [_P, _U32, _U32, _U32, _P, _P, _P, _P, _P, _P, _P, _P],
     "pyro_k_divergence": [_P, _U32, _U32, _U32, _P, _P, _P, _P, _P, _P, _P],
     "pyro_k_project": [_P, _U32, _U32, _U32, _P, _P, _P, _P, _P, _P],
     "pyro_k_mg_smooth": [_U32, _U32, _U32, _F, _P, _P, _P, _I, _F, _P],
