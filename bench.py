@@ -233,6 +233,40 @@ def log(msg):
     sys.stderr.flush()
 
 
+def solver_bench(n=256, seed=1):
+    """The pressure system in isolation: n^3 cells, h = 2 cm, ~5 % solid
+    boxes, N(0,1) zero-mean rhs (pyro_b200.poisson.poisson_case).  Device
+    time of each solve from CUDA events inside the solver, from phi = 0."""
+    import torch
+    from pyro_b200 import _abi
+    from pyro_b200.poisson import PoissonSolver, poisson_case
+    f, b = poisson_case(n, n, n, seed=seed)
+    fd = torch.from_numpy(f).cuda()
+    bd = torch.from_numpy(b).cuda()
+    out = {"config": f"poisson {n}^3 h=0.02 solid={float(f.mean()):.3f} seed={seed}"}
+    runs = [("vcycle_fp32_to_1e-3", _abi.SOLVER_VCYCLE_TOL, 1e-3, 60),
+            ("mgpcg_fp32_to_1e-3", _abi.SOLVER_MGPCG, 1e-3, 200),
+            ("mgpcg_fp32_to_1e-4", _abi.SOLVER_MGPCG, 1e-4, 200),
+            ("mgpcg_bf16_to_1e-4", _abi.SOLVER_MGPCG_BF16, 1e-4, 200),
+            ("mgpcg_fp32_to_1e-6", _abi.SOLVER_MGPCG, 1e-6, 200),
+            ("mgpcg_bf16_to_1e-6", _abi.SOLVER_MGPCG_BF16, 1e-6, 200)]
+    for bc in (0, 1):
+        ps = PoissonSolver((n, n, n), 0.02, bc)
+        ps.set_flags(fd.data_ptr())
+        res = {}
+        for name, mode, tol, cap in runs:
+            best = None
+            for rep in range(2):          # first solve allocates lazily
+                phi = torch.zeros_like(bd)
+                info = ps.solve(bd.data_ptr(), phi.data_ptr(), mode, tol, cap, allow_cap=True)
+                best = info
+            res[name] = {"ms": round(best.ms, 3), "iterations": best.iterations,
+                         "rel_resid": best.rel_resid, "converged": bool(best.converged)}
+        ps.close()
+        out["bc_reference" if bc == 0 else "bc_top_dirichlet"] = res
+    return out
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -354,6 +388,10 @@ def run_ours(args):
                "sample": f"{args.cpu_steps} full substeps of the same developed state "
                          "(C++ oracle restating the reference's WGSL kernels, OpenMP)"}
 
+    solver = None
+    if rank == 0 and not args.no_solver:
+        log("solver bench")
+        solver = solver_bench()
     launches_per_step = 10 + sc.sim.pressure_cycles * (10 * (info.levels - 1) + 1)
     line = {
         "metric": METRIC, "value": ms, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -376,6 +414,7 @@ def run_ours(args):
         "kernels_ms": kern,
         "throughput": {"value": world * cells / (ms * 1e-3), "unit": "cells*substeps/s"},
         "cpu_baseline": cpu,
+        "solver": solver,
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clocks.summary(),
     }
@@ -398,6 +437,7 @@ def main():
     ap.add_argument("--preroll-s", type=float, default=1.0)
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-solver", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -220,7 +220,7 @@ template <typename TS>
 __global__ void __launch_bounds__(COARSE_THREADS, 1)
     k_mg_coarse_cluster(Lvl d, float h2, const TS* __restrict__ b,
                         const uint32_t* __restrict__ f, TS* __restrict__ p, int iters,
-                        float omega, int bc_mode) {
+                        float omega, int bc_mode, int symmetric) {
   namespace cg = cooperative_groups;
   cg::cluster_group cl = cg::this_cluster();
   extern __shared__ float sp[];
@@ -277,8 +277,11 @@ __global__ void __launch_bounds__(COARSE_THREADS, 1)
   const int nx = d.nx;
 #pragma unroll 1
   for (int it = 0; it < iters; it++) {
+    // symmetric: alternate red-black and black-red iterations (SSOR pairs)
+    const int first = symmetric ? (it & 1) : 0;
 #pragma unroll
-    for (int c = 0; c < 2; c++) {
+    for (int cc = 0; cc < 2; cc++) {
+      const int c = cc ^ first;
 #pragma unroll
       for (int r = 0; r < COARSE_K; r++) {
         uint32_t m = cell[r].meta;
@@ -350,7 +353,7 @@ int coarse_cluster_size(Dims3 d) {
 
 template <typename TS>
 cudaError_t mg_coarse_t(Dims3 d, float h, const TS* b, const uint32_t* f, TS* p, int iters,
-                        float omega, int bc_mode, cudaStream_t st) {
+                        float omega, int bc_mode, cudaStream_t st, int symmetric = 0) {
   static int attr_done = 0;  // attributes are per function, set once
   static int max_cluster = 0;
   cudaError_t e;
@@ -396,7 +399,7 @@ cudaError_t mg_coarse_t(Dims3 d, float h, const TS* b, const uint32_t* f, TS* p,
   cfg.attrs = at;
   cfg.numAttrs = 1;
   return cudaLaunchKernelEx(&cfg, k_mg_coarse_cluster<TS>, Lvl{d.nx, d.ny, d.nz}, h * h, b, f, p,
-                            iters, omega, bc_mode);
+                            iters, omega, bc_mode, symmetric);
 }
 
 }  // namespace
@@ -461,6 +464,17 @@ cudaError_t launch_mg_coarse_bf16(Dims3 d, float h, const void* b, const uint32_
                                   int iters, float omega, int bc_mode, cudaStream_t st) {
   return mg_coarse_t<__nv_bfloat16>(d, h, (const __nv_bfloat16*)b, f, (__nv_bfloat16*)p, iters,
                                     omega, bc_mode, st);
+}
+
+cudaError_t launch_mg_coarse_sym(Dims3 d, float h, const float* b, const uint32_t* f, float* p,
+                                 int iters, float omega, int bc_mode, cudaStream_t st) {
+  return mg_coarse_t<float>(d, h, b, f, p, iters, omega, bc_mode, st, 1);
+}
+cudaError_t launch_mg_coarse_sym_bf16(Dims3 d, float h, const void* b, const uint32_t* f,
+                                      void* p, int iters, float omega, int bc_mode,
+                                      cudaStream_t st) {
+  return mg_coarse_t<__nv_bfloat16>(d, h, (const __nv_bfloat16*)b, f, (__nv_bfloat16*)p, iters,
+                                    omega, bc_mode, st, 1);
 }
 
 }  // namespace pyro

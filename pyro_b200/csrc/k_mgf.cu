@@ -363,6 +363,109 @@ __global__ void __launch_bounds__(256) k_mg_restrict_m(L df, float h2, const TS*
   stv(pc + ci, 0.0f);
 }
 
+// ---- symmetric V-cycle pieces (MGPCG preconditioner) ----------------------
+// The prolongation P of a fine cell c takes, per axis, the two coarse cells
+// floor((c+0.5)/2-0.5) + {0,1} (clamped) with weights 1-fr, fr and
+// renormalises by the fluid weight sum W_c (mg.wgsl:96-119).  The
+// restriction used with it is R = P^T / 8, which makes the V-cycle with
+// adjoint pre/post smoothing a symmetric preconditioner for CG.
+
+// 1-D prolongation weight of coarse index J for fine index c.
+__device__ __forceinline__ float pw1(int c, int J, int nc) {
+  float g = ((float)c + 0.5f) * 0.5f - 0.5f;
+  int i0 = (int)floorf(g);
+  float fr = g - (float)i0;
+  float w = 0.0f;
+  if (min(max(i0, 0), nc - 1) == J) w += 1.0f - fr;
+  if (min(max(i0 + 1, 0), nc - 1) == J) w += fr;
+  return w;
+}
+
+// r~ = (b - A p) / W_c for fluid fine cells whose prolongation row is not
+// empty, else 0.
+template <typename TS>
+__global__ void __launch_bounds__(256) k_mg_resid_w(L d, float h2, const TS* __restrict__ p,
+                                                    const TS* __restrict__ b,
+                                                    const uint8_t* __restrict__ m0, L dc,
+                                                    const uint8_t* __restrict__ mc,
+                                                    int bc_mode, TS* __restrict__ rt) {
+  int x = blockIdx.x * 32 + threadIdx.x;
+  int y = blockIdx.y * 4 + threadIdx.y;
+  int z = blockIdx.z * 2 + threadIdx.z;
+  if (!d.inb(x, y, z)) return;
+  int i = d.idx(x, y, z);
+  uint32_t m = __ldg(m0 + i);
+  float out = 0.0f;
+  if (!(m & META_SOLID)) {
+    const int sy = d.nx, sz = d.nx * d.ny;
+    float sum = 0.0f;
+    if (m & 1u) sum += ldv(p + i + 1);
+    if (m & 2u) sum += ldv(p + i - 1);
+    if (m & 4u) sum += ldv(p + i + sy);
+    if (m & 8u) sum += ldv(p + i - sy);
+    if (m & 16u) sum += ldv(p + i + sz);
+    if (m & 32u) sum += ldv(p + i - sz);
+    float cnt = (float)(__popc(m & 63u) + dirichlet_faces(d, x, y, z, bc_mode));
+    float r = ldv(b + i) - (sum - cnt * ldv(p + i)) / h2;
+    float gx = ((float)x + 0.5f) * 0.5f - 0.5f, gy = ((float)y + 0.5f) * 0.5f - 0.5f,
+          gz = ((float)z + 0.5f) * 0.5f - 0.5f;
+    int ix = (int)floorf(gx), iy = (int)floorf(gy), iz = (int)floorf(gz);
+    float fx = gx - (float)ix, fy = gy - (float)iy, fz = gz - (float)iz;
+    float W = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      int ox = k & 1, oy = (k >> 1) & 1, oz = (k >> 2) & 1;
+      int cx = min(max(ix + ox, 0), dc.nx - 1), cy = min(max(iy + oy, 0), dc.ny - 1),
+          cz = min(max(iz + oz, 0), dc.nz - 1);
+      if (__ldg(mc + dc.idx(cx, cy, cz)) & META_SOLID) continue;
+      W += (ox ? fx : 1.0f - fx) * (oy ? fy : 1.0f - fy) * (oz ? fz : 1.0f - fz);
+    }
+    if (W > 1e-4f) out = r / W;
+  }
+  stv(rt + i, out);
+}
+
+// Coarse rhs = (1/8) sum_c P[c,J] r~[c]; coarse guess 0.
+template <typename TS>
+__global__ void __launch_bounds__(256) k_mg_restrict_t(L df, const TS* __restrict__ rt,
+                                                       const uint8_t* __restrict__ mf, L dc,
+                                                       const uint8_t* __restrict__ mc,
+                                                       TS* __restrict__ bc, TS* __restrict__ pc) {
+  int X = blockIdx.x * 32 + threadIdx.x;
+  int Y = blockIdx.y * 4 + threadIdx.y;
+  int Z = blockIdx.z * 2 + threadIdx.z;
+  if (!dc.inb(X, Y, Z)) return;
+  int J = dc.idx(X, Y, Z);
+  float acc = 0.0f;
+  if (!(__ldg(mc + J) & META_SOLID)) {
+    float wx[4], wy[4], wz[4];
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+      int cx = 2 * X - 1 + a, cy = 2 * Y - 1 + a, cz = 2 * Z - 1 + a;
+      wx[a] = (cx >= 0 && cx < df.nx) ? pw1(cx, X, dc.nx) : 0.0f;
+      wy[a] = (cy >= 0 && cy < df.ny) ? pw1(cy, Y, dc.ny) : 0.0f;
+      wz[a] = (cz >= 0 && cz < df.nz) ? pw1(cz, Z, dc.nz) : 0.0f;
+    }
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      if (wz[c] == 0.0f) continue;
+#pragma unroll
+      for (int bb = 0; bb < 4; bb++) {
+        if (wy[bb] == 0.0f) continue;
+#pragma unroll
+        for (int a = 0; a < 4; a++) {
+          if (wx[a] == 0.0f) continue;
+          int i = df.idx(2 * X - 1 + a, 2 * Y - 1 + bb, 2 * Z - 1 + c);
+          acc += wx[a] * wy[bb] * wz[c] * ldv(rt + i);
+        }
+      }
+    }
+    acc *= 0.125f;
+  }
+  stv(bc + J, acc);
+  stv(pc + J, 0.0f);
+}
+
 inline dim3 g3(Dims3 d) { return dim3((d.nx + 31) / 32, (d.ny + 3) / 4, (d.nz + 1) / 2); }
 
 template <typename TS, int H, bool R>
@@ -421,6 +524,33 @@ cudaError_t launch_mg_restrict_m_bf16(Dims3 df, float h, const void* pf, const v
                                       int bc_mode, cudaStream_t st) {
   using T = __nv_bfloat16;
   return restrict_t<T>(df, h, (const T*)pf, (const T*)bf, mf, dc, (T*)bc, (T*)pc, bc_mode, st);
+}
+
+template <typename TS>
+cudaError_t restrict_sym_t(Dims3 df, float h, const TS* pf, const TS* bf, const uint8_t* mf,
+                           TS* rt, Dims3 dc, const uint8_t* mc, TS* bc, TS* pc, int bc_mode,
+                           cudaStream_t st) {
+  k_mg_resid_w<TS><<<g3(df), dim3(32, 4, 2), 0, st>>>(L{df.nx, df.ny, df.nz}, h * h, pf, bf, mf,
+                                                      L{dc.nx, dc.ny, dc.nz}, mc, bc_mode, rt);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_mg_restrict_t<TS><<<g3(dc), dim3(32, 4, 2), 0, st>>>(L{df.nx, df.ny, df.nz}, rt, mf,
+                                                         L{dc.nx, dc.ny, dc.nz}, mc, bc, pc);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mg_restrict_sym(Dims3 df, float h, const float* pf, const float* bf,
+                                   const uint8_t* mf, float* rt, Dims3 dc, const uint8_t* mc,
+                                   float* bc, float* pc, int bc_mode, cudaStream_t st) {
+  return restrict_sym_t<float>(df, h, pf, bf, mf, rt, dc, mc, bc, pc, bc_mode, st);
+}
+cudaError_t launch_mg_restrict_sym_bf16(Dims3 df, float h, const void* pf, const void* bf,
+                                        const uint8_t* mf, void* rt, Dims3 dc,
+                                        const uint8_t* mc, void* bc, void* pc, int bc_mode,
+                                        cudaStream_t st) {
+  using T = __nv_bfloat16;
+  return restrict_sym_t<T>(df, h, (const T*)pf, (const T*)bf, mf, (T*)rt, dc, mc, (T*)bc,
+                           (T*)pc, bc_mode, st);
 }
 
 cudaError_t launch_mg_meta(Dims3 d, const uint32_t* f, uint8_t* meta, cudaStream_t st) {

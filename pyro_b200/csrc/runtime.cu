@@ -218,4 +218,69 @@ cudaError_t Multigrid::vcycles_bf16(int cycles, cudaStream_t st, DevBuf* bphi, D
   return launch_bf16_to_f32(bphi[0].p, phi[0], n0, st);
 }
 
+cudaError_t Multigrid::vcycle_sym(cudaStream_t st, DevBuf* bphi, DevBuf* bphi2, DevBuf* bb) {
+  int nl = (int)dims.size();
+  const bool lo = bphi != nullptr;
+  cudaError_t e;
+  if (lo) {
+    for (int l = 0; l < nl; l++) {
+      size_t need = dims[l].cells() * 2;
+      if (bphi[l].bytes != need) {
+        if (bphi[l].alloc(need) != PYRO_OK || bphi2[l].alloc(need) != PYRO_OK ||
+            bb[l].alloc(need) != PYRO_OK)
+          return cudaErrorMemoryAllocation;
+      }
+    }
+  }
+  if ((e = prepare(st)) != cudaSuccess) return e;
+  auto M = [&](int l) { return meta[l].as<uint8_t>(); };
+  // storage of level l: phi, b, scratch
+  auto P = [&](int l) -> void* { return lo ? bphi[l].p : (void*)phi[l]; };
+  auto B = [&](int l) -> void* { return lo ? bb[l].p : (void*)b[l]; };
+  auto T = [&](int l) -> void* { return lo ? bphi2[l].p : phi2[l].p; };
+  size_t n0 = dims[0].cells();
+  if (lo) {
+    if ((e = launch_f32_to_bf16(b[0], bb[0].p, n0, st)) != cudaSuccess) return e;
+    if ((e = launch_f32_to_bf16(phi[0], bphi[0].p, n0, st)) != cudaSuccess) return e;
+  }
+  auto pass = [&](int l, int c, float om) -> cudaError_t {
+    return lo ? launch_mg_pass_bf16(dims[l], h[l], B(l), M(l), P(l), c, om, bc_mode, st)
+              : launch_mg_pass(dims[l], h[l], (const float*)B(l), M(l), (float*)P(l), c, om,
+                               bc_mode, st);
+  };
+  for (int l = 0; l < nl - 1; l++) {
+    for (int it = 0; it < 2; it++)
+      for (int c = 0; c < 2; c++)
+        if ((e = pass(l, c, 1.0f)) != cudaSuccess) return e;
+    e = lo ? launch_mg_restrict_sym_bf16(dims[l], h[l], P(l), B(l), M(l), T(l), dims[l + 1],
+                                         M(l + 1), B(l + 1), P(l + 1), bc_mode, st)
+           : launch_mg_restrict_sym(dims[l], h[l], (const float*)P(l), (const float*)B(l), M(l),
+                                    (float*)T(l), dims[l + 1], M(l + 1), (float*)B(l + 1),
+                                    (float*)P(l + 1), bc_mode, st);
+    if (e != cudaSuccess) return e;
+  }
+  int lc = nl - 1;
+  if (coarse_one_cta) {
+    e = lo ? launch_mg_coarse_sym_bf16(dims[lc], h[lc], B(lc), f[lc], P(lc), 80, 1.6f, bc_mode, st)
+           : launch_mg_coarse_sym(dims[lc], h[lc], (const float*)B(lc), f[lc], (float*)P(lc), 80,
+                                  1.6f, bc_mode, st);
+    if (e != cudaSuccess) return e;
+  } else {
+    for (int it = 0; it < 80; it++)
+      for (int cc = 0; cc < 2; cc++)
+        if ((e = pass(lc, cc ^ (it & 1), 1.6f)) != cudaSuccess) return e;
+  }
+  for (int l = nl - 2; l >= 0; l--) {
+    e = lo ? launch_mg_prolong_m_bf16(dims[l], P(l + 1), M(l), P(l), dims[l + 1], M(l + 1), st)
+           : launch_mg_prolong_m(dims[l], (const float*)P(l + 1), M(l), (float*)P(l),
+                                 dims[l + 1], M(l + 1), st);
+    if (e != cudaSuccess) return e;
+    for (int it = 0; it < 2; it++)
+      for (int c = 1; c >= 0; c--)
+        if ((e = pass(l, c, 1.0f)) != cudaSuccess) return e;
+  }
+  if (lo) return launch_bf16_to_f32(bphi[0].p, phi[0], n0, st);
+  return cudaSuccess;
+}
+
 }  // namespace pyro

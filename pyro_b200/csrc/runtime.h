@@ -82,6 +82,11 @@ struct Multigrid {
   // guess, with bphi/bb the BF16 level arrays (allocated on first use).
   cudaError_t vcycles_bf16(int cycles, cudaStream_t st, DevBuf* bphi, DevBuf* bphi2,
                            DevBuf* bb);
+  // Symmetric V-cycle for the CG preconditioner: pre-smoothing red-black,
+  // post-smoothing black-red, restriction P^T/8 of the fluid-normalised
+  // trilinear prolongation, coarsest level by alternating SOR sweeps.  With
+  // bphi != nullptr phi and b are stored in BF16 (FP32 arithmetic).
+  cudaError_t vcycle_sym(cudaStream_t st, DevBuf* bphi, DevBuf* bphi2, DevBuf* bb);
   size_t device_bytes() const;
 };
 

@@ -3,7 +3,7 @@
 //
 // MGPCG solves the reference system A phi = b (A negative semi-definite,
 // src/shaders/mg.wgsl:25-35) by CG on -A: with r = b - A phi, z = V(r) one
-// V-cycle from a zero guess, q = A p:
+// symmetric V-cycle from a zero guess (Multigrid::vcycle_sym), q = A p:
 //   alpha = <r,z> / <p,q>,  phi += alpha p,  r -= alpha q,
 //   beta  = <z_new, r_new - r_old> / <z_old, r_old> = -<z_new, q> / <p,q>
 // (Polak-Ribiere form, valid for the non-symmetric V-cycle), p = z + beta p.
@@ -52,25 +52,26 @@ struct L3 {
   __device__ __forceinline__ int idx(int x, int y, int z) const { return x + nx * (y + ny * z); }
 };
 
-// (A v)_i = (sum fluid nbrs v - cnt v_i) / h^2, 0 in solids.
-__device__ __forceinline__ float apply_A(const L3& d, float ih2, const float* __restrict__ v,
-                                         const uint32_t* __restrict__ f, int x, int y, int z,
-                                         int bc_mode, float vi) {
-  float sum = 0.0f, cnt = 0.0f;
+// (A v)_i = (sum fluid nbrs v - cnt v_i) / h^2, 0 in solids; evaluated in
+// FP64 so residuals near 1e-6 of |b| are not lost to cancellation.
+__device__ __forceinline__ double apply_A(const L3& d, double ih2, const float* __restrict__ v,
+                                          const uint32_t* __restrict__ f, int x, int y, int z,
+                                          int bc_mode, float vi) {
+  double sum = 0.0, cnt = 0.0;
 #pragma unroll
   for (int k = 0; k < 6; k++) {
     int a = x + (k == 0) - (k == 1), b = y + (k == 2) - (k == 3), c = z + (k == 4) - (k == 5);
     if (b < 0) continue;
     if (!d.inb(a, b, c)) {
-      if (bc_mode == 0 || b >= d.ny) cnt += 1.0f;
+      if (bc_mode == 0 || b >= d.ny) cnt += 1.0;
       continue;
     }
     int j = d.idx(a, b, c);
     if (__ldg(f + j) == 1u) continue;
-    sum += __ldg(v + j);
-    cnt += 1.0f;
+    sum += (double)__ldg(v + j);
+    cnt += 1.0;
   }
-  return (sum - cnt * vi) * ih2;
+  return (sum - cnt * (double)vi) * ih2;
 }
 
 #define CELL_PROLOGUE                          \
@@ -81,7 +82,7 @@ __device__ __forceinline__ float apply_A(const L3& d, float ih2, const float* __
   int i = in ? d.idx(x, y, z) : 0;             \
   bool fluid = in && __ldg(f + i) != 1u;
 
-__global__ void __launch_bounds__(256) k_resid(L3 d, float ih2, const float* __restrict__ phi,
+__global__ void __launch_bounds__(256) k_resid(L3 d, double ih2, const float* __restrict__ phi,
                                                const float* __restrict__ b,
                                                const uint32_t* __restrict__ f, int bc_mode,
                                                float* __restrict__ r, double* __restrict__ sc) {
@@ -92,8 +93,9 @@ __global__ void __launch_bounds__(256) k_resid(L3 d, float ih2, const float* __r
     float ri = 0.0f;
     if (fluid) {
       float bi = __ldg(b + i);
-      ri = bi - apply_A(d, ih2, phi, f, x, y, z, bc_mode, __ldg(phi + i));
-      r2 = (double)ri * (double)ri;
+      double rd = (double)bi - apply_A(d, ih2, phi, f, x, y, z, bc_mode, __ldg(phi + i));
+      ri = (float)rd;
+      r2 = rd * rd;
       b2 = (double)bi * (double)bi;
     }
     if (r) r[i] = ri;
@@ -102,7 +104,7 @@ __global__ void __launch_bounds__(256) k_resid(L3 d, float ih2, const float* __r
   block_add_d(sh, b2, sc + SC_BB);
 }
 
-__global__ void __launch_bounds__(256) k_apply_dot(L3 d, float ih2, const float* __restrict__ p,
+__global__ void __launch_bounds__(256) k_apply_dot(L3 d, double ih2, const float* __restrict__ p,
                                                    const uint32_t* __restrict__ f, int bc_mode,
                                                    float* __restrict__ q,
                                                    double* __restrict__ sc) {
@@ -113,8 +115,9 @@ __global__ void __launch_bounds__(256) k_apply_dot(L3 d, float ih2, const float*
     float qi = 0.0f;
     if (fluid) {
       float pi = __ldg(p + i);
-      qi = apply_A(d, ih2, p, f, x, y, z, bc_mode, pi);
-      pq = (double)pi * (double)qi;
+      double qd = apply_A(d, ih2, p, f, x, y, z, bc_mode, pi);
+      qi = (float)qd;
+      pq = (double)pi * qd;
     }
     q[i] = qi;
   }
@@ -219,7 +222,7 @@ int Solver::true_resid(cudaStream_t st, const float* phi, const float* b, double
                        double* bn) {
   L3 l{d.nx, d.ny, d.nz};
   PYRO_CU(cudaMemsetAsync(sc.p, 0, SC_N * 8, st));
-  k_resid<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, 1.0f / (mg->h[0] * mg->h[0]), phi, b,
+  k_resid<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, 1.0 / ((double)mg->h[0] * mg->h[0]), phi, b,
                                                    mg->f[0], mg->bc_mode, nullptr,
                                                    sc.as<double>());
   PYRO_CU(cudaGetLastError());
@@ -239,7 +242,7 @@ cudaError_t Solver::precond(cudaStream_t st, bool bf16) {
   float* save_b = mg->b[0];
   const uint32_t* save_f = mg->f[0];
   mg->bind_level0(z.as<float>(), r.as<float>(), save_f);
-  e = bf16 ? mg->vcycles_bf16(1, st, bphi, bphi2, bb) : mg->vcycles(1, st);
+  e = bf16 ? mg->vcycle_sym(st, bphi, bphi2, bb) : mg->vcycle_sym(st, nullptr, nullptr, nullptr);
   mg->bind_level0(save_phi, save_b, save_f);
   return e;
 }
@@ -259,7 +262,7 @@ int Solver::solve(cudaStream_t st, float* phi, const float* b, int mode, float t
   double rel = 0, bn = 0;
   int rc = PYRO_OK;
   L3 l{d.nx, d.ny, d.nz};
-  const float ih2 = 1.0f / (mg->h[0] * mg->h[0]);
+  const double ih2 = 1.0 / ((double)mg->h[0] * mg->h[0]);
   if (mode == PYRO_SOLVER_VCYCLE || mode == PYRO_SOLVER_VCYCLE_TOL) {
     mg->bind_level0(phi, b, f0);
     if (mode == PYRO_SOLVER_VCYCLE) {
@@ -292,7 +295,11 @@ int Solver::solve(cudaStream_t st, float* phi, const float* b, int mode, float t
     double bb2 = host_sc[SC_BB];
     bn = std::sqrt(bb2);
     rel = bb2 > 0 ? std::sqrt(host_sc[SC_RR] / bb2) : 0.0;
-    if (rel > tol) {
+    // CG with residual replacement: when the recursively updated residual
+    // meets the tolerance the true residual is recomputed; if it does not
+    // meet it, CG restarts from the true residual.
+    int restarts = 0;
+    while (rel > tol && iters < max_iters && restarts < 8) {
       PYRO_CU(precond(st, bf16));
       k_dots<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, f0, z.as<float>(), r.as<float>(),
                                                       nullptr, S);
@@ -301,6 +308,7 @@ int Solver::solve(cudaStream_t st, float* phi, const float* b, int mode, float t
       k_update_p<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, f0, p.as<float>(), z.as<float>(),
                                                           S, 1);
       PYRO_CU(cudaGetLastError());
+      bool stalled = false;
       while (iters < max_iters) {
         k_apply_dot<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, ih2, p.as<float>(), f0,
                                                              mg->bc_mode, q.as<float>(), S);
@@ -311,7 +319,10 @@ int Solver::solve(cudaStream_t st, float* phi, const float* b, int mode, float t
         PYRO_CU(cudaStreamSynchronize(st));
         iters++;
         double rr = host_sc[SC_RR];
-        if (!(rr >= 0.0) || !(host_sc[SC_PQ] < 0.0 || host_sc[SC_PQ] > 0.0)) break;
+        if (!(rr >= 0.0) || !(host_sc[SC_PQ] < 0.0 || host_sc[SC_PQ] > 0.0)) {
+          stalled = true;
+          break;
+        }
         if (bb2 > 0 && std::sqrt(rr / bb2) <= tol) break;
         PYRO_CU(precond(st, bf16));
         k_dots<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, f0, z.as<float>(), r.as<float>(),
@@ -321,6 +332,18 @@ int Solver::solve(cudaStream_t st, float* phi, const float* b, int mode, float t
         k_roll<<<1, 1, 0, st>>>(S);
         PYRO_CU(cudaGetLastError());
       }
+      // true residual into r (and |r|, |b|)
+      PYRO_CU(cudaMemsetAsync(sc.p, 0, SC_N * 8, st));
+      k_resid<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, ih2, phi, b, f0, mg->bc_mode,
+                                                       r.as<float>(), S);
+      PYRO_CU(cudaGetLastError());
+      PYRO_CU(cudaMemcpyAsync(host_sc, sc.p, SC_N * 8, cudaMemcpyDeviceToHost, st));
+      PYRO_CU(cudaStreamSynchronize(st));
+      rel = bb2 > 0 ? std::sqrt(host_sc[SC_RR] / bb2) : 0.0;
+      restarts++;
+      if (stalled) break;
+    }
+    {
       if ((rc = true_resid(st, phi, b, &rel, &bn)) != PYRO_OK) return rc;
     }
   }

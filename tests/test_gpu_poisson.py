@@ -86,7 +86,7 @@ def test_vcycle_to_tolerance_follows_the_reference_cycle(lib):
 @pytest.mark.parametrize("mode,tol", [(_abi.SOLVER_MGPCG, 1e-3), (_abi.SOLVER_MGPCG, 1e-6),
                                       (_abi.SOLVER_MGPCG_BF16, 1e-3),
                                       (_abi.SOLVER_MGPCG_BF16, 1e-6)])
-@pytest.mark.parametrize("bc_mode", [0])
+@pytest.mark.parametrize("bc_mode", [0, 1])
 def test_tolerance_solvers_vs_fp64(lib, mode, tol, bc_mode):
     dims = (64, 64, 64)
     f, b = _case(*dims, 2)
@@ -102,6 +102,7 @@ def test_tolerance_solvers_vs_fp64(lib, mode, tol, bc_mode):
     assert info.converged == 1 and rel <= tol * 1.05, (info.iterations, rel)
     fl = f == 0
     err = np.abs(phi[fl] - x64[fl]).max() / np.abs(x64[fl]).max()
-    # error against the FP64 solve scales with the residual tolerance
-    assert err <= 200 * tol, (mode, tol, err)
+    # error against the FP64 solve scales with the residual tolerance (the
+    # Neumann-sided case is worse conditioned)
+    assert err <= (200 if bc_mode == 0 else 2000) * tol, (mode, tol, err)
     lib.pyro_poisson_destroy(ps)
