@@ -291,6 +291,27 @@ int pyro_k_mg_coarse(uint32_t nx, uint32_t ny, uint32_t nz, float h,
                      const float* b, const uint32_t* flags, float* phi,
                      int iters, float omega, void* stream);
 
+/* ---- learned warm start: tcgen05 convolutions --------------------------- */
+/* 3x3x3 convolution, padding 1, stride 1, as an implicit GEMM on the
+ * tensor cores (BF16 operands, FP32 accumulation in TMEM).  Activations are
+ * channel-last BF16 [nb][nz][ny][nx][C]; weights BF16 [Cout][27][Cin] with
+ * tap = (dz+1)*9 + (dy+1)*3 + (dx+1).  Channels 1..128.  Blocking; returns
+ * PYRO_E_TIMEOUT if a bounded tensor-core wait ran out.  No counterpart in
+ * the reference (its pressure solve has no learned stage). */
+int pyro_conv3_forward(const void* x, int C, int nx, int ny, int nz, int nb,
+                       const void* w, int Cout, const float* bias, int relu,
+                       void* y, int y_f32, void* stream);
+/* dx = conv^T(dy, W), zeroed where `act` (the layer input, may be NULL) is
+ * <= 0, i.e. the ReLU derivative of the producing layer. */
+int pyro_conv3_backward_data(const void* dy, int Cout, int nx, int ny, int nz,
+                             int nb, const void* w, int Cin, const void* act,
+                             void* dx, int dx_f32, void* stream);
+/* dw[co][tap][ci] += sum over voxels of dy[v][co] * x[v + tap][ci]; dw is
+ * FP32 and accumulated into (zero it first). */
+int pyro_conv3_backward_weight(const void* x, int Cin, const void* dy, int Cout,
+                               int nx, int ny, int nz, int nb, float* dw,
+                               void* stream);
+
 #ifdef __cplusplus
 }
 #endif

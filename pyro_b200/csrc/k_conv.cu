@@ -1,0 +1,430 @@
+// k_conv.cu — 3x3x3 convolutions (padding 1, stride 1) as implicit GEMMs on
+// the tcgen05 tensor cores, for the learned pressure warm start.
+//
+// One kernel, k_gemm<N, Load, Epi>, computes a 128 x N tile of
+// D = A * B^T with BF16 operands staged in shared memory (two-stage
+// pipeline, K in steps of 16) and the FP32 accumulator in TMEM:
+//
+//   forward          A[m = voxel][k = (tap, ci)] = x[voxel + tap][ci]
+//                    B[n = co][k]                = W[co][tap][ci]
+//   backward (data)  A[m = voxel][k = (tap, co)] = dy[voxel - tap][co]
+//                    B[n = ci][k]                = W[co][tap][ci]
+//   backward (weight) A[m = (tap, ci)][k = voxel] = x[voxel + tap][ci]
+//                    B[n = co][k = voxel]        = dy[voxel][co]   (split over K)
+//
+// Activations are channel-last BF16, [volume][z][y][x][channel]; a tap
+// outside its volume reads zero.  One thread issues the MMA, tcgen05.commit
+// signals an mbarrier per stage, and every wait is bounded: a wait that runs
+// out sets *err and the CTA still frees its TMEM.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+
+#include "runtime.h"
+#include "umma.cuh"
+
+namespace pyro {
+
+namespace {
+
+using bf16 = __nv_bfloat16;
+constexpr int GEMM_THREADS = 128;
+
+struct Vol {
+  int nx, ny, nz, nb;  // volume dims and count
+  __device__ __forceinline__ int voxels() const { return nx * ny * nz * nb; }
+};
+
+// Voxel v shifted by tap (dx, dy, dz) within its volume, or -1.
+__device__ __forceinline__ int shifted(const Vol& g, int v, int dx, int dy, int dz) {
+  int x = v % g.nx;
+  int r = v / g.nx;
+  int y = r % g.ny;
+  r /= g.ny;
+  int z = r % g.nz;
+  int b = r / g.nz;
+  x += dx;
+  y += dy;
+  z += dz;
+  if ((unsigned)x >= (unsigned)g.nx || (unsigned)y >= (unsigned)g.ny ||
+      (unsigned)z >= (unsigned)g.nz)
+    return -1;
+  return ((b * g.nz + z) * g.ny + y) * g.nx + x;
+}
+__device__ __forceinline__ void tap_offset(int t, int& dx, int& dy, int& dz) {
+  dx = t % 3 - 1;
+  dy = (t / 3) % 3 - 1;
+  dz = t / 9 - 1;
+}
+
+__device__ __forceinline__ void st16(uint8_t* s, uint32_t off, uint4 v) {
+  *reinterpret_cast<uint4*>(s + off) = v;
+}
+__device__ __forceinline__ void st_bf(uint8_t* s, uint32_t off, bf16 v) {
+  *reinterpret_cast<bf16*>(s + off) = v;
+}
+
+template <int N, class Load, class Epi>
+__global__ void __launch_bounds__(GEMM_THREADS) k_gemm(Load ld, Epi ep, int ksteps_total,
+                                                       int ksteps_per_cta, int* err) {
+  constexpr int NCOLS = N <= 32 ? 32 : (N <= 64 ? 64 : 128);
+  __shared__ __align__(1024) uint8_t sA[2][128 * 32];
+  __shared__ __align__(1024) uint8_t sB[2][N * 32];
+  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ uint32_t tslot;
+  const int m0 = blockIdx.x * 128;
+  const int k0 = blockIdx.y * ksteps_per_cta;
+  const int k1 = min(k0 + ksteps_per_cta, ksteps_total);
+  const int nks = max(k1 - k0, 0);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    umma::mbar_init(&mbar[0], 1);
+    umma::mbar_init(&mbar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    umma::tmem_alloc(&tslot, NCOLS);
+    umma::tmem_relinquish();
+  }
+  umma::fence_before();
+  __syncthreads();
+  umma::fence_after();
+  const uint32_t tbase = tslot;
+  constexpr uint32_t IDESC = umma::idesc_bf16(128, N);
+  bool ok = true;
+  for (int i = 0; i < nks; i++) {
+    const int s = i & 1;
+    if (i >= 2 && !umma::mbar_wait_bounded(&mbar[s], ((i - 2) >> 1) & 1)) ok = false;
+    ld(sA[s], sB[s], m0, k0 + i);
+    umma::fence_proxy_async();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      umma::fence_after();
+      umma::mma_bf16(tbase, umma::smem_desc(sA[s], 128), umma::smem_desc(sB[s], N), IDESC,
+                     i > 0 ? 1u : 0u);
+      umma::mma_commit(&mbar[s]);
+    }
+  }
+  if (nks > 0 && !umma::mbar_wait_bounded(&mbar[(nks - 1) & 1], ((nks - 1) >> 1) & 1))
+    ok = false;
+  umma::fence_after();
+  const bool all_ok = __syncthreads_and(ok) != 0;
+  if (all_ok && nks > 0) {
+#pragma unroll
+    for (int col = 0; col < N; col += 16) {
+      float v[16];
+      umma::tmem_ld16(tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)col, v);
+      ep(m0 + warp * 32 + lane, col, v);
+    }
+  }
+  if (!all_ok && threadIdx.x == 0) atomicExch(err, 1);
+  umma::fence_before();
+  __syncthreads();
+  if (warp == 0) umma::tmem_dealloc(tbase, NCOLS);
+}
+
+// ---------------------------------------------------------------- loaders
+// A = shifted activations (voxel rows, K = (tap, channel)); B = weight rows.
+// `flip` negates the tap (backward data); `wt` selects the transposed
+// weight gather for backward data: B[n = ci][k = (tap, co)] = W[co][tap][ci].
+struct ConvLoad {
+  const bf16* x;      // [V][C]
+  const bf16* w;      // [Cw_out][27][Cw_in]
+  Vol g;
+  int C;              // channels of x (K = 27 C)
+  int Nrows;          // rows of B that exist (co, or ci for backward data)
+  int cw_in, cw_out;  // weight dims
+  int flip, wt;
+  __device__ void operator()(uint8_t* sA, uint8_t* sB, int m0, int ks) const {
+    const int t0 = threadIdx.x;
+    const int V = g.voxels();
+    const int K = 27 * C;
+    // A: row r = voxel m0 + r
+    {
+      int r = t0;
+      int v = m0 + r;
+      if ((C & 15) == 0) {
+        int t = ks / (C >> 4), cc = ks % (C >> 4);
+        int dx, dy, dz;
+        tap_offset(t, dx, dy, dz);
+        if (flip) { dx = -dx; dy = -dy; dz = -dz; }
+        uint4 a0 = make_uint4(0, 0, 0, 0), a1 = a0;
+        if (v < V) {
+          int vs = shifted(g, v, dx, dy, dz);
+          if (vs >= 0) {
+            const uint4* p = reinterpret_cast<const uint4*>(x + (size_t)vs * C + cc * 16);
+            a0 = __ldg(p);
+            a1 = __ldg(p + 1);
+          }
+        }
+        st16(sA, umma::core_offset(r, 0, 128), a0);
+        st16(sA, umma::core_offset(r, 8, 128), a1);
+      } else {
+        for (int e = 0; e < 16; e++) {
+          int k = ks * 16 + e;
+          bf16 val = __float2bfloat16(0.0f);
+          if (v < V && k < K) {
+            int t = k / C, ci = k % C;
+            int dx, dy, dz;
+            tap_offset(t, dx, dy, dz);
+            if (flip) { dx = -dx; dy = -dy; dz = -dz; }
+            int vs = shifted(g, v, dx, dy, dz);
+            if (vs >= 0) val = x[(size_t)vs * C + ci];
+          }
+          st_bf(sA, umma::core_offset(r, e, 128), val);
+        }
+      }
+    }
+    // B: row n (co for forward, ci for backward data)
+    if (t0 < Nrows_pad()) {
+      int n = t0;
+      for (int e = 0; e < 16; e++) {
+        int k = ks * 16 + e;
+        bf16 val = __float2bfloat16(0.0f);
+        if (n < Nrows && k < K) {
+          if (!wt) {
+            val = w[(size_t)n * K + k];  // W[co][tap][ci], K index tap * C + ci
+          } else {
+            int t = k / C, co = k % C;   // K index tap * Cout + co
+            val = w[((size_t)co * 27 + t) * cw_in + n];
+          }
+        }
+        st_bf(sB, umma::core_offset(n, e, npad), val);
+      }
+    }
+  }
+  int npad;
+  __device__ __forceinline__ int Nrows_pad() const { return npad; }
+};
+
+// Weight gradient: A[m = (tap, ci)][k = voxel] = x[voxel + tap][ci],
+// B[n = co][k = voxel] = dy[voxel][co].
+struct WgradLoad {
+  const bf16* x;   // [V][Cin]
+  const bf16* dy;  // [V][Cout]
+  Vol g;
+  int Cin, Cout, npad;
+  __device__ void operator()(uint8_t* sA, uint8_t* sB, int m0, int ks) const {
+    const int V = g.voxels();
+    const int M = 27 * Cin;
+    {
+      int r = threadIdx.x;
+      int m = m0 + r;
+      int t = m / Cin, ci = m % Cin;
+      int dx, dy_, dz;
+      tap_offset(t < 27 ? t : 0, dx, dy_, dz);
+      for (int e = 0; e < 16; e++) {
+        int v = ks * 16 + e;
+        bf16 val = __float2bfloat16(0.0f);
+        if (m < M && v < V) {
+          int vs = shifted(g, v, dx, dy_, dz);
+          if (vs >= 0) val = x[(size_t)vs * Cin + ci];
+        }
+        st_bf(sA, umma::core_offset(r, e, 128), val);
+      }
+    }
+    if ((int)threadIdx.x < npad) {
+      int n = threadIdx.x;
+      for (int e = 0; e < 16; e++) {
+        int v = ks * 16 + e;
+        bf16 val = __float2bfloat16(0.0f);
+        if (n < Cout && v < V) val = dy[(size_t)v * Cout + n];
+        st_bf(sB, umma::core_offset(n, e, npad), val);
+      }
+    }
+  }
+};
+
+// -------------------------------------------------------------- epilogues
+// Forward / backward data: row = voxel.  out_bf16 [V][Nout] with optional
+// bias and ReLU, or out_f32 [V][Nout]; `mask` (BF16 activations of the layer
+// input, [V][Nout]) zeroes the gradient where the input was <= 0 (ReLU).
+struct ConvEpi {
+  bf16* out_bf16;
+  float* out_f32;
+  const float* bias;
+  const bf16* mask;
+  int V, Nout, relu;
+  __device__ void operator()(int m, int col, const float (&v)[16]) const {
+    if (m >= V) return;
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+      int n = col + j;
+      if (n >= Nout) break;
+      float a = v[j];
+      if (bias) a += bias[n];
+      if (relu) a = fmaxf(a, 0.0f);
+      if (mask && !(__bfloat162float(mask[(size_t)m * Nout + n]) > 0.0f)) a = 0.0f;
+      if (out_f32) out_f32[(size_t)m * Nout + n] = a;
+      else out_bf16[(size_t)m * Nout + n] = __float2bfloat16(a);
+    }
+  }
+};
+
+// Weight gradient: row m = (tap, ci), column n = co; FP32 atomics into
+// dw[co][tap][ci] (split-K partial sums).
+struct WgradEpi {
+  float* dw;
+  int M, Cout;
+  __device__ void operator()(int m, int col, const float (&v)[16]) const {
+    if (m >= M) return;
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+      int n = col + j;
+      if (n >= Cout) break;
+      atomicAdd(dw + (size_t)n * M + m, v[j]);
+    }
+  }
+};
+
+template <int N, class Load, class Epi>
+cudaError_t gemm_launch(dim3 grid, const Load& ld, const Epi& ep, int ksteps_total,
+                        int ksteps_per_cta, int* err, cudaStream_t st) {
+  k_gemm<N, Load, Epi><<<grid, GEMM_THREADS, 0, st>>>(ld, ep, ksteps_total, ksteps_per_cta, err);
+  return cudaGetLastError();
+}
+
+template <class Load, class Epi>
+cudaError_t gemm_dispatch(int npad, dim3 grid, const Load& ld, const Epi& ep, int kt, int kpc,
+                          int* err, cudaStream_t st) {
+  switch (npad) {
+    case 16: return gemm_launch<16>(grid, ld, ep, kt, kpc, err, st);
+    case 32: return gemm_launch<32>(grid, ld, ep, kt, kpc, err, st);
+    case 48: return gemm_launch<48>(grid, ld, ep, kt, kpc, err, st);
+    case 64: return gemm_launch<64>(grid, ld, ep, kt, kpc, err, st);
+    case 96: return gemm_launch<96>(grid, ld, ep, kt, kpc, err, st);
+    case 128: return gemm_launch<128>(grid, ld, ep, kt, kpc, err, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+inline int pad16(int n) { return (n + 15) / 16 * 16; }
+
+}  // namespace
+
+// y = conv(x, W) (+ bias, ReLU), or its transpose for backward data.
+cudaError_t conv3_forward(const bf16* x, int C, int nx, int ny, int nz, int nb, const bf16* w,
+                          int Cout, const float* bias, int relu, bf16* y_bf16, float* y_f32,
+                          int* err, cudaStream_t st) {
+  Vol g{nx, ny, nz, nb};
+  int V = nx * ny * nz * nb;
+  int npad = pad16(Cout);
+  int ksteps = (27 * C + 15) / 16;
+  ConvLoad ld{x, w, g, C, Cout, C, Cout, 0, 0, npad};
+  ConvEpi ep{y_bf16, y_f32, bias, nullptr, V, Cout, relu};
+  dim3 grid((V + 127) / 128, 1, 1);
+  return gemm_dispatch(npad, grid, ld, ep, ksteps, ksteps, err, st);
+}
+
+// dx = conv^T(dy, W), masked by (act > 0) when act is given.
+cudaError_t conv3_backward_data(const bf16* dy, int Cout, int nx, int ny, int nz, int nb,
+                                const bf16* w, int Cin, const bf16* act, bf16* dx_bf16,
+                                float* dx_f32, int* err, cudaStream_t st) {
+  Vol g{nx, ny, nz, nb};
+  int V = nx * ny * nz * nb;
+  int npad = pad16(Cin);
+  int ksteps = (27 * Cout + 15) / 16;
+  ConvLoad ld{dy, w, g, Cout, Cin, Cin, Cout, 1, 1, npad};
+  ConvEpi ep{dx_bf16, dx_f32, nullptr, act, V, Cin, 0};
+  dim3 grid((V + 127) / 128, 1, 1);
+  return gemm_dispatch(npad, grid, ld, ep, ksteps, ksteps, err, st);
+}
+
+// dw[co][tap][ci] += sum_voxels dy[v][co] x[v + tap][ci]  (dw FP32, zeroed
+// by the caller).
+cudaError_t conv3_backward_weight(const bf16* x, int Cin, const bf16* dy, int Cout, int nx,
+                                  int ny, int nz, int nb, float* dw, int* err, cudaStream_t st) {
+  Vol g{nx, ny, nz, nb};
+  int V = nx * ny * nz * nb;
+  int M = 27 * Cin;
+  int npad = pad16(Cout);
+  int ksteps = (V + 15) / 16;
+  int mt = (M + 127) / 128;
+  // split K so that the grid covers the GPU a few times over
+  int splits = std::max(1, std::min(ksteps, (148 * 8) / std::max(mt, 1)));
+  int kpc = (ksteps + splits - 1) / splits;
+  splits = (ksteps + kpc - 1) / kpc;
+  WgradLoad ld{x, dy, g, Cin, Cout, npad};
+  WgradEpi ep{dw, M, Cout};
+  dim3 grid(mt, splits, 1);
+  return gemm_dispatch(npad, grid, ld, ep, ksteps, kpc, err, st);
+}
+
+}  // namespace pyro
+
+// ------------------------------------------------------------------ C ABI
+using namespace pyro;
+using bf16 = __nv_bfloat16;
+
+namespace {
+int finish(cudaError_t e, DevBuf& err, cudaStream_t st, const char* what) {
+  if (e != cudaSuccess) {
+    set_error(std::string(what) + ": " + cudaGetErrorString(e));
+    return PYRO_E_CUDA;
+  }
+  int h = 0;
+  PYRO_CU(cudaMemcpyAsync(&h, err.p, 4, cudaMemcpyDeviceToHost, st));
+  PYRO_CU(cudaStreamSynchronize(st));
+  if (h) {
+    set_error(std::string(what) + ": a tensor-core wait ran out");
+    return PYRO_E_TIMEOUT;
+  }
+  return PYRO_OK;
+}
+bool conv_dims_ok(int nx, int ny, int nz, int nb) {
+  return nx >= 1 && ny >= 1 && nz >= 1 && nb >= 1 && (int64_t)nx * ny * nz * nb < (1ll << 31);
+}
+bool chan_ok(int c) { return c >= 1 && c <= 128; }
+}  // namespace
+
+extern "C" {
+
+int pyro_conv3_forward(const void* x, int C, int nx, int ny, int nz, int nb, const void* w,
+                       int Cout, const float* bias, int relu, void* y, int y_f32, void* stream) {
+  clear_error();
+  PYRO_REQUIRE(x && w && y, "pyro_conv3_forward: null buffer");
+  PYRO_REQUIRE(conv_dims_ok(nx, ny, nz, nb) && chan_ok(C) && chan_ok(Cout),
+               "pyro_conv3_forward: invalid sizes");
+  DevBuf err;
+  int rc = err.alloc(4);
+  if (rc != PYRO_OK) return rc;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  cudaError_t e = conv3_forward((const bf16*)x, C, nx, ny, nz, nb, (const bf16*)w, Cout, bias,
+                                relu, y_f32 ? nullptr : (bf16*)y, y_f32 ? (float*)y : nullptr,
+                                err.as<int>(), st);
+  return finish(e, err, st, "pyro_conv3_forward");
+}
+
+int pyro_conv3_backward_data(const void* dy, int Cout, int nx, int ny, int nz, int nb,
+                             const void* w, int Cin, const void* act, void* dx, int dx_f32,
+                             void* stream) {
+  clear_error();
+  PYRO_REQUIRE(dy && w && dx, "pyro_conv3_backward_data: null buffer");
+  PYRO_REQUIRE(conv_dims_ok(nx, ny, nz, nb) && chan_ok(Cin) && chan_ok(Cout),
+               "pyro_conv3_backward_data: invalid sizes");
+  DevBuf err;
+  int rc = err.alloc(4);
+  if (rc != PYRO_OK) return rc;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  cudaError_t e = conv3_backward_data((const bf16*)dy, Cout, nx, ny, nz, nb, (const bf16*)w, Cin,
+                                      (const bf16*)act, dx_f32 ? nullptr : (bf16*)dx,
+                                      dx_f32 ? (float*)dx : nullptr, err.as<int>(), st);
+  return finish(e, err, st, "pyro_conv3_backward_data");
+}
+
+int pyro_conv3_backward_weight(const void* x, int Cin, const void* dy, int Cout, int nx, int ny,
+                               int nz, int nb, float* dw, void* stream) {
+  clear_error();
+  PYRO_REQUIRE(x && dy && dw, "pyro_conv3_backward_weight: null buffer");
+  PYRO_REQUIRE(conv_dims_ok(nx, ny, nz, nb) && chan_ok(Cin) && chan_ok(Cout),
+               "pyro_conv3_backward_weight: invalid sizes");
+  DevBuf err;
+  int rc = err.alloc(4);
+  if (rc != PYRO_OK) return rc;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  cudaError_t e = conv3_backward_weight((const bf16*)x, Cin, (const bf16*)dy, Cout, nx, ny, nz,
+                                        nb, dw, err.as<int>(), st);
+  return finish(e, err, st, "pyro_conv3_backward_weight");
+}
+
+}  // extern "C"
