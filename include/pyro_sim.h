@@ -89,7 +89,12 @@ enum PyroSolver {
   PYRO_SOLVER_VCYCLE = 0,     /* fixed count of V-cycles (the reference)  */
   PYRO_SOLVER_VCYCLE_TOL = 1, /* V-cycles until relative residual <= tol  */
   PYRO_SOLVER_MGPCG = 2,      /* flexible CG, FP32 V-cycle preconditioner */
-  PYRO_SOLVER_MGPCG_BF16 = 3  /* flexible CG, BF16-storage V-cycle        */
+  PYRO_SOLVER_MGPCG_BF16 = 3, /* flexible CG, BF16-storage V-cycle        */
+  PYRO_SOLVER_MGPCG_LEARNED = 4 /* mode 3 after the learned warm start:
+                                   phi += alpha net(b - A phi) with alpha
+                                   minimising the A-norm error, kept only
+                                   when it lowers ||b - A phi|| (needs a
+                                   network: pyro_*_set_net)              */
 };
 
 typedef struct PyroSolveInfo {
@@ -99,7 +104,14 @@ typedef struct PyroSolveInfo {
   double b_norm;       /* ||b||                                           */
   float ms;            /* device time of the solve, CUDA events            */
   int32_t converged;   /* 1 when rel_resid <= tol                         */
+  int32_t learned;     /* learned stage: -1 not run, 0 discarded, 1 kept   */
+  float learned_ms;    /* device time of the learned stage                 */
+  double rel_resid_start;   /* relative residual of the initial guess      */
+  double rel_resid_learned; /* after the learned stage (start if discarded) */
 } PyroSolveInfo;
+
+/* The learned pressure stage (pyro_net_* below). */
+typedef struct PyroNet PyroNet;
 
 typedef struct PyroSimInfo {
   uint32_t nx, ny, nz, levels;
@@ -169,6 +181,9 @@ int pyro_sim_info(PyroSim* sim, PyroSimInfo* info);
 int pyro_sim_set_solver(PyroSim* sim, int mode, float tol, int max_iters);
 /* Information on the last pressure solve of a tolerance-mode step. */
 int pyro_sim_last_solve(PyroSim* sim, PyroSolveInfo* info);
+/* Network used by PYRO_SOLVER_MGPCG_LEARNED (NULL detaches; the caller
+ * keeps ownership and keeps it alive while attached). */
+int pyro_sim_set_net(PyroSim* sim, PyroNet* net);
 int pyro_sim_destroy(PyroSim* sim);
 
 /* ---- scene voxelizer (Scene::voxelize, src/scene.rs:621-667) ---------- */
@@ -214,6 +229,16 @@ int pyro_poisson_set_flags(PyroPoisson* ps, const uint32_t* flags);
 int pyro_poisson_solve(PyroPoisson* ps, const float* b, float* phi, int mode,
                        float tol, int max_iters, PyroSolveInfo* info);
 int pyro_poisson_stream(PyroPoisson* ps, void** stream);
+/* Network used by PYRO_SOLVER_MGPCG_LEARNED (NULL detaches). */
+int pyro_poisson_set_net(PyroPoisson* ps, PyroNet* net);
+/* The learned stage's keep-or-discard rule, on host scalars: given
+ * <r,e>, <e,Ae>, <r,Ae>, <Ae,Ae> and <r,r> for the residual r = b - A phi
+ * and the network's correction e, alpha = <r,e>/<e,Ae> and the new squared
+ * residual <r,r> - 2 alpha <r,Ae> + alpha^2 <Ae,Ae>.  Returns 1 (keep) when
+ * alpha is finite and the new residual is finite and below <r,r>, else 0;
+ * alpha and rr_new may be NULL. */
+int pyro_learned_accept(double re, double eae, double rae, double aeae, double rr,
+                        double* alpha, double* rr_new);
 int pyro_poisson_destroy(PyroPoisson* ps);
 
 /* ---- individual kernels (parity hooks; device pointers) ----------------- */
@@ -311,6 +336,47 @@ int pyro_conv3_backward_data(const void* dy, int Cout, int nx, int ny, int nz,
 int pyro_conv3_backward_weight(const void* x, int Cin, const void* dy, int Cout,
                                int nx, int ny, int nz, int nb, float* dw,
                                void* stream);
+
+/* ---- learned pressure stage (no counterpart in the reference) ----------
+ * A 3-level 3D convolutional encoder-decoder (16/32/64 channels, 3x3x3
+ * convolutions on the tcgen05 kernels above, BF16 weights and activations,
+ * FP32 accumulation) from (b, solid mask) to a pressure estimate
+ * phi = net(b / rms(b)) * out_scale * rms(b) * h^2 on fluid cells.  Inputs
+ * are nb volumes of nx*ny*nz cells stacked (x fastest), flags as the
+ * simulation's (1 = solid); all pointers are device memory.  Parameters are
+ * FP32: every layer's weights [Cout][27][Cin] in order, then every layer's
+ * biases.  `stream` may be NULL (the network's own stream).  The multigrid
+ * solve of src/sim.rs:451-491 remains the fallback (PYRO_SOLVER_MGPCG_LEARNED
+ * below). */
+int pyro_net_create(uint64_t seed, PyroNet** out);
+int pyro_net_destroy(PyroNet* net);
+int pyro_net_param_count(const PyroNet* net, uint64_t* count);
+int pyro_net_get_params(PyroNet* net, float* host, uint64_t count, float* out_scale);
+/* also resets the Adam state */
+int pyro_net_set_params(PyroNet* net, const float* host, uint64_t count, float out_scale);
+/* phi (device, nb*nx*ny*nz FP32) = the network's estimate; synchronous */
+int pyro_net_forward(PyroNet* net, const float* b, const uint32_t* flags, uint32_t nx,
+                     uint32_t ny, uint32_t nz, uint32_t nb, float h, float* phi,
+                     void* stream);
+/* Training loss = w_phi * mean over fluid cells of
+ *   (out - phi_t / (out_scale rms(b) h^2))^2
+ * + w_res * mean over the fluid cells with all six neighbours inside the
+ *   volume of res^2, res = b / rms(b) - out_scale (sum of the fluid
+ *   neighbours' out - their count * out), the normalised residual of the
+ *   prediction under the solver's operator (solid neighbours excluded).
+ * Defaults w_phi = 1, w_res = 0; both >= 0, not both 0. */
+int pyro_net_set_loss(PyroNet* net, float w_phi, float w_res);
+/* loss and, in grad_host (may be NULL), d loss / d params; synchronous */
+int pyro_net_loss_grad(PyroNet* net, const float* b, const uint32_t* flags,
+                       const float* phi_t, uint32_t nx, uint32_t ny, uint32_t nz,
+                       uint32_t nb, float h, double* loss, float* grad_host, void* stream);
+/* loss, gradients and one Adam step (gradient global norm clipped to
+ * `clip` when clip > 0); asynchronous on the stream */
+int pyro_net_train_step(PyroNet* net, const float* b, const uint32_t* flags,
+                        const float* phi_t, uint32_t nx, uint32_t ny, uint32_t nz,
+                        uint32_t nb, float h, float lr, float clip, void* stream);
+/* waits for the stream and reads the loss of the last step */
+int pyro_net_last_loss(PyroNet* net, double* loss, void* stream);
 
 #ifdef __cplusplus
 }

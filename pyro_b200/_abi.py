@@ -21,7 +21,7 @@ PYRO_E_TIMEOUT = -6
 STATS_N = 1040
 NOALLOC_MAX_CELLS = 1 << 19
 MAX_LAYERS = 1024
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 F_S0, F_S1, F_SOL, F_PYR, F_FLAGS, F_CURL, F_U, F_V, F_W, F_PHI, F_B = range(11)
 
@@ -32,6 +32,7 @@ SOLVER_VCYCLE = 0
 SOLVER_VCYCLE_TOL = 1
 SOLVER_MGPCG = 2
 SOLVER_MGPCG_BF16 = 3
+SOLVER_MGPCG_LEARNED = 4
 
 SHAPE_BOX, SHAPE_CYL, SHAPE_SPHERE, SHAPE_POOL = range(4)
 
@@ -92,6 +93,8 @@ class PyroSolveInfo(ctypes.Structure):
         ("mode", ctypes.c_int32), ("iterations", ctypes.c_int32),
         ("rel_resid", ctypes.c_double), ("b_norm", ctypes.c_double),
         ("ms", ctypes.c_float), ("converged", ctypes.c_int32),
+        ("learned", ctypes.c_int32), ("learned_ms", ctypes.c_float),
+        ("rel_resid_start", ctypes.c_double), ("rel_resid_learned", ctypes.c_double),
     ]
 
 
@@ -111,6 +114,8 @@ _P = ctypes.c_void_p
 _U32 = ctypes.c_uint32
 _F = ctypes.c_float
 _I = ctypes.c_int
+_U64 = ctypes.c_uint64
+_D = ctypes.c_double
 
 # name -> argtypes; every entry point returns int.
 SIGNATURES = {
@@ -152,6 +157,20 @@ SIGNATURES = {
     "pyro_conv3_forward": [_P, _I, _I, _I, _I, _I, _P, _I, _P, _I, _P, _I, _P],
     "pyro_conv3_backward_data": [_P, _I, _I, _I, _I, _I, _P, _I, _P, _P, _I, _P],
     "pyro_conv3_backward_weight": [_P, _I, _P, _I, _I, _I, _I, _I, _P, _P],
+    "pyro_sim_set_net": [_P, _P],
+    "pyro_poisson_set_net": [_P, _P],
+    "pyro_learned_accept": [_D, _D, _D, _D, _D, ctypes.POINTER(_D), ctypes.POINTER(_D)],
+    "pyro_net_create": [_U64, ctypes.POINTER(_P)],
+    "pyro_net_destroy": [_P],
+    "pyro_net_param_count": [_P, ctypes.POINTER(_U64)],
+    "pyro_net_get_params": [_P, _P, _U64, ctypes.POINTER(_F)],
+    "pyro_net_set_params": [_P, _P, _U64, _F],
+    "pyro_net_forward": [_P, _P, _P, _U32, _U32, _U32, _U32, _F, _P, _P],
+    "pyro_net_loss_grad": [_P, _P, _P, _P, _U32, _U32, _U32, _U32, _F, ctypes.POINTER(_D), _P,
+                           _P],
+    "pyro_net_train_step": [_P, _P, _P, _P, _U32, _U32, _U32, _U32, _F, _F, _F, _P],
+    "pyro_net_last_loss": [_P, ctypes.POINTER(_D), _P],
+    "pyro_net_set_loss": [_P, _F, _F],
 }
 
 _lib = None

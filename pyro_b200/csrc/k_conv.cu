@@ -16,9 +16,12 @@
 // outside its volume reads zero.  One thread issues the MMA, tcgen05.commit
 // signals an mbarrier per stage, and every wait is bounded: a wait that runs
 // out sets *err and the CTA still frees its TMEM.
+#include <cuda.h>
 #include <cuda_bf16.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include "runtime.h"
 #include "umma.cuh"
@@ -246,7 +249,7 @@ struct ConvEpi {
   const bf16* mask;
   int V, Nout, relu;
   __device__ void operator()(int m, int col, const float (&v)[16]) const {
-    if (m >= V) return;
+    if (m < 0 || m >= V) return;
 #pragma unroll
     for (int j = 0; j < 16; j++) {
       int n = col + j;
@@ -296,6 +299,177 @@ cudaError_t gemm_dispatch(int npad, dim3 grid, const Load& ld, const Epi& ep, in
     case 128: return gemm_launch<128>(grid, ld, ep, kt, kpc, err, st);
     default: return cudaErrorInvalidValue;
   }
+}
+
+
+// ------------------------------------------------------------ TMA path
+// Convolution with TMA-staged operands, for input channel counts that are
+// multiples of 16.  A CTA computes a tile of BX x BY output voxels of one
+// z-plane (BX * BY = 128 rows of the MMA).  For every group of 16 input
+// channels it loads, by 5-D TMA boxes with zero fill outside the volume,
+// three copies of the input patch shifted by dx = -1, 0, +1, each
+// BX x (BY + 2) x 3 voxels (y and z with their halo) as two 8-channel
+// chunks, plus the weight slice w_tap[27][N][16 channels].  Output row
+// r = x + BX y of tap (dx, dy, dz) then reads patch row
+// r + BX (dy + 1) + BX (BY + 2) (dz + 1) of copy dx, so each of the 27 taps
+// is one MMA whose A descriptor starts at that row: no gather, and every
+// input element is fetched three times per tile instead of 27.
+struct TmaGeom {
+  int nx, ny, nz, nb;
+  int BX, BY, tiles_x, tiles_y;
+  int groups, stages;
+  uint32_t box_a, box_b, stage_a, stage_bytes;
+};
+
+template <int N, class Epi>
+__global__ void __launch_bounds__(GEMM_THREADS) k_conv_tma(const __grid_constant__ CUtensorMap ta,
+                                                           const __grid_constant__ CUtensorMap tb,
+                                                           TmaGeom g, Epi ep, int* err) {
+  constexpr int NCOLS = N <= 32 ? 32 : (N <= 64 ? 64 : 128);
+  constexpr uint32_t IDESC = umma::idesc_bf16(128, N);
+  extern __shared__ uint8_t dsm[];
+  __shared__ __align__(8) uint64_t full[2], empty[2], done;
+  __shared__ uint32_t tslot;
+  uint8_t* base = dsm + ((1024u - (umma::smem_u32(dsm) & 1023u)) & 1023u);
+  int t = blockIdx.x;
+  const int tx = t % g.tiles_x;
+  t /= g.tiles_x;
+  const int ty = t % g.tiles_y;
+  t /= g.tiles_y;
+  const int z = t % g.nz, b = t / g.nz;
+  const int x0 = tx * g.BX, y0 = ty * g.BY;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < 2; s++) {
+      umma::mbar_init(&full[s], 1);
+      umma::mbar_init(&empty[s], 1);
+    }
+    umma::mbar_init(&done, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    umma::tmem_alloc(&tslot, NCOLS);
+    umma::tmem_relinquish();
+  }
+  umma::fence_before();
+  __syncthreads();
+  umma::fence_after();
+  const uint32_t tbase = tslot;
+  bool ok = true;
+  if (threadIdx.x == 0) {
+    auto issue = [&](int grp, int s) {
+      uint8_t* sa = base + (size_t)s * g.stage_bytes;
+      uint8_t* sb = sa + g.stage_a;
+      umma::mbar_expect_tx(&full[s], g.stage_a + 2 * g.box_b);
+      for (int d = 0; d < 3; d++)
+        for (int j = 0; j < 2; j++)
+          umma::tma_load_5d(sa + (d * 2 + j) * g.box_a, &ta, grp * 16 + j * 8, x0 + d - 1, y0 - 1,
+                            z - 1, b, &full[s]);
+      for (int j = 0; j < 2; j++)
+        umma::tma_load_3d(sb + j * g.box_b, &tb, grp * 16 + j * 8, 0, 0, &full[s]);
+    };
+    const int S = g.stages, G = g.groups;
+    int issued = 0, consumed = 0;
+    for (; issued < S && issued < G; issued++) issue(issued, issued);
+    for (int grp = 0; grp < G && ok; grp++) {
+      const int s = grp % S;
+      if (!umma::mbar_wait_bounded(&full[s], (grp / S) & 1)) {
+        ok = false;
+        break;
+      }
+      consumed++;
+      umma::fence_after();
+      uint8_t* sa = base + (size_t)s * g.stage_bytes;
+      uint8_t* sb = sa + g.stage_a;
+#pragma unroll 1
+      for (int tap = 0; tap < 27; tap++) {
+        const int dx = tap % 3, dy = (tap / 3) % 3, dz = tap / 9;
+        const uint32_t row = (uint32_t)(dy * g.BX + dz * g.BX * (g.BY + 2));
+        const uint64_t da = umma::smem_desc_lbo(sa + dx * 2 * g.box_a + row * 16, g.box_a);
+        const uint64_t db = umma::smem_desc_lbo(sb + tap * N * 16, g.box_b);
+        umma::mma_bf16(tbase, da, db, IDESC, (grp > 0 || tap > 0) ? 1u : 0u);
+      }
+      umma::mma_commit(&empty[s]);
+      if (issued < G) {
+        // the stage is refilled once the MMAs reading it are done
+        if (!umma::mbar_wait_bounded(&empty[s], (grp / S) & 1)) {
+          ok = false;
+          break;
+        }
+        issue(issued, s);
+        issued++;
+      }
+    }
+    umma::mma_commit(&done);
+    if (!ok) {
+      // let the copies still in flight land before the CTA exits
+      for (int q = consumed; q < issued; q++)
+        umma::mbar_wait_bounded(&full[q % S], (q / S) & 1);
+    }
+  }
+  __syncwarp();
+  if (!umma::mbar_wait_bounded(&done, 0)) ok = false;
+  umma::fence_after();
+  const bool all_ok = __syncthreads_and(ok) != 0;
+  if (all_ok) {
+    const int r = warp * 32 + lane;
+    const int x = x0 + r % g.BX, y = y0 + r / g.BX;
+    const int v = (x < g.nx && y < g.ny) ? ((b * g.nz + z) * g.ny + y) * g.nx + x : -1;
+#pragma unroll
+    for (int col = 0; col < N; col += 16) {
+      float vals[16];
+      umma::tmem_ld16(tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)col, vals);
+      ep(v, col, vals);
+    }
+  }
+  if (!all_ok && threadIdx.x == 0) atomicExch(err, 1);
+  umma::fence_before();
+  __syncthreads();
+  if (warp == 0) umma::tmem_dealloc(tbase, NCOLS);
+}
+
+__global__ void k_wprep(const bf16* __restrict__ w, int Cout, int Cin, int backward,
+                        bf16* __restrict__ out) {
+  const int n = Cout * 27 * Cin;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int co = i / (27 * Cin), t = (i / Cin) % 27, ci = i % Cin;
+    if (!backward)
+      out[((size_t)t * Cout + co) * Cin + ci] = w[i];
+    else
+      out[((size_t)(26 - t) * Cin + ci) * Cout + co] = w[i];
+  }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+int pick_bx(int nx) {
+  for (int c : {16, 8, 32, 64, 128})
+    if (nx % c == 0) return c;
+  return nx < 16 ? 8 : 16;
+}
+
+template <int N, class Epi>
+cudaError_t tma_launch(const CUtensorMap& ta, const CUtensorMap& tb, const TmaGeom& g,
+                       const Epi& ep, int* err, cudaStream_t st) {
+  const size_t smem = (size_t)g.stages * g.stage_bytes + 1024;
+  cudaError_t e = cudaFuncSetAttribute(k_conv_tma<N, Epi>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const unsigned grid = (unsigned)((size_t)g.tiles_x * g.tiles_y * g.nz * g.nb);
+  k_conv_tma<N, Epi><<<grid, GEMM_THREADS, smem, st>>>(ta, tb, g, ep, err);
+  return cudaGetLastError();
 }
 
 inline int pad16(int n) { return (n + 15) / 16 * 16; }
@@ -350,6 +524,73 @@ cudaError_t conv3_backward_weight(const bf16* x, int Cin, const bf16* dy, int Co
   return gemm_dispatch(npad, grid, ld, ep, ksteps, kpc, err, st);
 }
 
+
+// Weight layouts for conv3_tma: forward w_tap[t][co][ci] = w[co][t][ci];
+// backward (data) w_tap[t][ci][co] = w[co][26 - t][ci] (flipped taps,
+// transposed channels).
+cudaError_t conv3_prep_weights(const bf16* w, int Cout, int Cin, int backward, bf16* w_tap,
+                               cudaStream_t st) {
+  const int n = Cout * 27 * Cin;
+  k_wprep<<<std::min((n + 255) / 256, 1024), 256, 0, st>>>(w, Cout, Cin, backward, w_tap);
+  return cudaGetLastError();
+}
+
+// y[v][n] = sum_{t, k} w_tap[t][n][k] x[v + tap(t)][k] (+ bias, ReLU, or
+// zeroed where mask[v][n] <= 0); K (channels of x) a multiple of 16,
+// N <= 128 output channels.  The input tensor must be 16-byte aligned.
+cudaError_t conv3_tma(const bf16* x, int K, int nx, int ny, int nz, int nb, const bf16* w_tap,
+                      int N, const float* bias, int relu, const bf16* mask, bf16* y_bf16,
+                      float* y_f32, int* err, cudaStream_t st) {
+  if (K % 16 != 0 || N < 1 || N > 128) return cudaErrorInvalidValue;
+  PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
+  if (!enc) return cudaErrorNotSupported;
+  TmaGeom g{};
+  g.nx = nx;
+  g.ny = ny;
+  g.nz = nz;
+  g.nb = nb;
+  g.BX = pick_bx(nx);
+  g.BY = 128 / g.BX;
+  g.tiles_x = (nx + g.BX - 1) / g.BX;
+  g.tiles_y = (ny + g.BY - 1) / g.BY;
+  g.groups = K / 16;
+  const int npad = pad16(N);
+  g.box_a = (uint32_t)(g.BX * (g.BY + 2) * 3 * 16);
+  g.box_b = (uint32_t)(27 * npad * 16);
+  g.stage_a = 6 * g.box_a;
+  g.stage_bytes = (g.stage_a + 2 * g.box_b + 1023u) & ~1023u;
+  g.stages = (g.groups >= 2 && 2 * g.stage_bytes + 1024 <= 220 * 1024) ? 2 : 1;
+  if (g.stage_bytes + 1024 > 220 * 1024) return cudaErrorInvalidValue;
+  CUtensorMap ta, tb;
+  const cuuint64_t adim[5] = {(cuuint64_t)K, (cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz,
+                              (cuuint64_t)nb};
+  const cuuint64_t astr[4] = {(cuuint64_t)K * 2, (cuuint64_t)K * 2 * nx,
+                              (cuuint64_t)K * 2 * nx * ny, (cuuint64_t)K * 2 * nx * ny * nz};
+  const cuuint32_t abox[5] = {8, (cuuint32_t)g.BX, (cuuint32_t)(g.BY + 2), 3, 1};
+  const cuuint32_t es[5] = {1, 1, 1, 1, 1};
+  if (enc(&ta, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<bf16*>(x), adim, astr, abox, es,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+          CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return cudaErrorInvalidValue;
+  const cuuint64_t bdim[3] = {(cuuint64_t)K, (cuuint64_t)N, 27};
+  const cuuint64_t bstr[2] = {(cuuint64_t)K * 2, (cuuint64_t)K * 2 * N};
+  const cuuint32_t bbox[3] = {8, (cuuint32_t)npad, 27};
+  if (enc(&tb, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<bf16*>(w_tap), bdim, bstr, bbox,
+          es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+          CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return cudaErrorInvalidValue;
+  const int V = nx * ny * nz * nb;
+  ConvEpi ep{y_bf16, y_f32, bias, mask, V, N, relu};
+  switch (npad) {
+    case 16: return tma_launch<16>(ta, tb, g, ep, err, st);
+    case 32: return tma_launch<32>(ta, tb, g, ep, err, st);
+    case 48: return tma_launch<48>(ta, tb, g, ep, err, st);
+    case 64: return tma_launch<64>(ta, tb, g, ep, err, st);
+    case 96: return tma_launch<96>(ta, tb, g, ep, err, st);
+    case 128: return tma_launch<128>(ta, tb, g, ep, err, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
 }  // namespace pyro
 
 // ------------------------------------------------------------------ C ABI
@@ -389,9 +630,18 @@ int pyro_conv3_forward(const void* x, int C, int nx, int ny, int nz, int nb, con
   int rc = err.alloc(4);
   if (rc != PYRO_OK) return rc;
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-  cudaError_t e = conv3_forward((const bf16*)x, C, nx, ny, nz, nb, (const bf16*)w, Cout, bias,
-                                relu, y_f32 ? nullptr : (bf16*)y, y_f32 ? (float*)y : nullptr,
-                                err.as<int>(), st);
+  cudaError_t e;
+  if (C % 16 == 0) {  // TMA-staged kernel on tap-major weights
+    DevBuf wt;
+    if ((rc = wt.alloc((size_t)Cout * 27 * C * 2)) != PYRO_OK) return rc;
+    e = conv3_prep_weights((const bf16*)w, Cout, C, 0, wt.as<bf16>(), st);
+    if (e == cudaSuccess)
+      e = conv3_tma((const bf16*)x, C, nx, ny, nz, nb, wt.as<bf16>(), Cout, bias, relu, nullptr,
+                    y_f32 ? nullptr : (bf16*)y, y_f32 ? (float*)y : nullptr, err.as<int>(), st);
+    return finish(e, err, st, "pyro_conv3_forward");
+  }
+  e = conv3_forward((const bf16*)x, C, nx, ny, nz, nb, (const bf16*)w, Cout, bias, relu,
+                    y_f32 ? nullptr : (bf16*)y, y_f32 ? (float*)y : nullptr, err.as<int>(), st);
   return finish(e, err, st, "pyro_conv3_forward");
 }
 
@@ -406,9 +656,20 @@ int pyro_conv3_backward_data(const void* dy, int Cout, int nx, int ny, int nz, i
   int rc = err.alloc(4);
   if (rc != PYRO_OK) return rc;
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-  cudaError_t e = conv3_backward_data((const bf16*)dy, Cout, nx, ny, nz, nb, (const bf16*)w, Cin,
-                                      (const bf16*)act, dx_f32 ? nullptr : (bf16*)dx,
-                                      dx_f32 ? (float*)dx : nullptr, err.as<int>(), st);
+  cudaError_t e;
+  if (Cout % 16 == 0) {  // TMA-staged kernel on flipped, transposed weights
+    DevBuf wt;
+    if ((rc = wt.alloc((size_t)Cout * 27 * Cin * 2)) != PYRO_OK) return rc;
+    e = conv3_prep_weights((const bf16*)w, Cout, Cin, 1, wt.as<bf16>(), st);
+    if (e == cudaSuccess)
+      e = conv3_tma((const bf16*)dy, Cout, nx, ny, nz, nb, wt.as<bf16>(), Cin, nullptr, 0,
+                    (const bf16*)act, dx_f32 ? nullptr : (bf16*)dx, dx_f32 ? (float*)dx : nullptr,
+                    err.as<int>(), st);
+    return finish(e, err, st, "pyro_conv3_backward_data");
+  }
+  e = conv3_backward_data((const bf16*)dy, Cout, nx, ny, nz, nb, (const bf16*)w, Cin,
+                          (const bf16*)act, dx_f32 ? nullptr : (bf16*)dx,
+                          dx_f32 ? (float*)dx : nullptr, err.as<int>(), st);
   return finish(e, err, st, "pyro_conv3_backward_data");
 }
 

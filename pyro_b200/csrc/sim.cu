@@ -189,7 +189,7 @@ struct PyroSim {
 
 extern "C" {
 
-int pyro_abi_version(void) { return 1; }
+int pyro_abi_version(void) { return 2; }
 
 int pyro_sim_create(const PyroParams* params, const float* sol_init, uint32_t pressure_cycles,
                     PyroSim** out) {
@@ -483,13 +483,24 @@ int pyro_sim_info(PyroSim* S, PyroSimInfo* info) {
 int pyro_sim_set_solver(PyroSim* S, int mode, float tol, int max_iters) {
   clear_error();
   PYRO_REQUIRE(S, "pyro_sim_set_solver: null simulation");
-  PYRO_REQUIRE(mode >= PYRO_SOLVER_VCYCLE && mode <= PYRO_SOLVER_MGPCG_BF16,
+  PYRO_REQUIRE(mode >= PYRO_SOLVER_VCYCLE && mode <= PYRO_SOLVER_MGPCG_LEARNED,
                "pyro_sim_set_solver: unknown mode");
+  PYRO_REQUIRE(mode != PYRO_SOLVER_MGPCG_LEARNED || S->solver.net,
+               "pyro_sim_set_solver: the learned mode needs a network (pyro_sim_set_net)");
   PYRO_REQUIRE(mode == PYRO_SOLVER_VCYCLE || (tol > 0.0f && max_iters > 0),
                "pyro_sim_set_solver: tolerance modes need tol > 0 and max_iters > 0");
   S->mode = mode;
   S->tol = tol;
   S->max_iters = max_iters;
+  return PYRO_OK;
+}
+
+int pyro_sim_set_net(PyroSim* S, PyroNet* net) {
+  clear_error();
+  PYRO_REQUIRE(S, "pyro_sim_set_net: null simulation");
+  PYRO_REQUIRE(net || S->mode != PYRO_SOLVER_MGPCG_LEARNED,
+               "pyro_sim_set_net: the learned mode is selected; choose another mode first");
+  S->solver.net = net;
   return PYRO_OK;
 }
 

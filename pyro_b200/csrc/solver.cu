@@ -8,9 +8,11 @@
 //   beta  = <z_new, r_new - r_old> / <z_old, r_old> = -<z_new, q> / <p,q>
 // (Polak-Ribiere form, valid for the non-symmetric V-cycle), p = z + beta p.
 // Vectors are FP32; every dot product and norm is accumulated in FP64.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
+#include "net.h"
 #include "solver.h"
 
 namespace pyro {
@@ -199,7 +201,8 @@ int Solver::init(Multigrid* m) {
     set_error("solver: pinned allocation failed");
     return PYRO_E_NOMEM;
   }
-  if (cudaEventCreate(&ev0) != cudaSuccess || cudaEventCreate(&ev1) != cudaSuccess) {
+  if (cudaEventCreate(&ev0) != cudaSuccess || cudaEventCreate(&ev1) != cudaSuccess ||
+      cudaEventCreate(&evl0) != cudaSuccess || cudaEventCreate(&evl1) != cudaSuccess) {
     set_error("solver: cudaEventCreate failed");
     return PYRO_E_CUDA;
   }
@@ -210,6 +213,8 @@ Solver::~Solver() {
   if (host_sc) cudaFreeHost(host_sc);
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
+  if (evl0) cudaEventDestroy(evl0);
+  if (evl1) cudaEventDestroy(evl1);
 }
 
 size_t Solver::device_bytes() const {
@@ -247,13 +252,71 @@ cudaError_t Solver::precond(cudaStream_t st, bool bf16) {
   return e;
 }
 
+int Solver::learned_stage(cudaStream_t st, float* phi, double* rr, PyroSolveInfo* info) {
+  const uint32_t* f0 = mg->f[0];
+  L3 l{d.nx, d.ny, d.nz};
+  const double ih2 = 1.0 / ((double)mg->h[0] * mg->h[0]);
+  double* S = sc.as<double>();
+  PYRO_CU(cudaEventRecord(evl0, st));
+  // e = net(r) into z, q = A e
+  NetVol v{d.nx, d.ny, d.nz, 1};
+  int rc;
+  if ((rc = net->ensure(v, false)) || (rc = net->forward(r.as<float>(), f0, v, st)) ||
+      (rc = net->output(f0, mg->h[0], z.as<float>(), v, st)) || (rc = net->check_err(st)))
+    return rc;
+  PYRO_CU(cudaMemsetAsync(sc.p, 0, SC_N * 8, st));
+  k_apply_dot<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, ih2, z.as<float>(), f0, mg->bc_mode,
+                                                       q.as<float>(), S);
+  k_dots<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, f0, z.as<float>(), r.as<float>(), nullptr,
+                                                  S);
+  PYRO_CU(cudaGetLastError());
+  PYRO_CU(cudaMemcpyAsync(host_sc, sc.p, SC_N * 8, cudaMemcpyDeviceToHost, st));
+  PYRO_CU(cudaStreamSynchronize(st));
+  const double re = host_sc[SC_RZN], eae = host_sc[SC_PQ];
+  // <Ae, r>, <Ae, Ae>
+  PYRO_CU(cudaMemsetAsync(sc.p, 0, SC_N * 8, st));
+  k_dots<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, f0, q.as<float>(), r.as<float>(),
+                                                  q.as<float>(), S);
+  PYRO_CU(cudaGetLastError());
+  PYRO_CU(cudaMemcpyAsync(host_sc, sc.p, SC_N * 8, cudaMemcpyDeviceToHost, st));
+  PYRO_CU(cudaStreamSynchronize(st));
+  const double rae = host_sc[SC_RZN], aeae = host_sc[SC_ZQ];
+  double alpha = 0.0, rr_new = *rr;
+  const int keep = pyro_learned_accept(re, eae, rae, aeae, *rr, &alpha, &rr_new);
+  if (keep) {
+    // phi += alpha e, r -= alpha A e with alpha = S[RZ] / S[PQ]
+    std::memset(host_sc, 0, SC_N * 8);
+    host_sc[SC_RZ] = re;
+    host_sc[SC_PQ] = eae;
+    PYRO_CU(cudaMemcpyAsync(sc.p, host_sc, SC_N * 8, cudaMemcpyHostToDevice, st));
+    k_update_xr<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, f0, phi, r.as<float>(),
+                                                         z.as<float>(), q.as<float>(), S);
+    PYRO_CU(cudaGetLastError());
+    PYRO_CU(cudaMemcpyAsync(host_sc, sc.p, SC_N * 8, cudaMemcpyDeviceToHost, st));
+  }
+  PYRO_CU(cudaEventRecord(evl1, st));
+  PYRO_CU(cudaEventSynchronize(evl1));
+  if (keep) *rr = host_sc[SC_RR];
+  // the CG accumulators start from zero (a discarded correction may have
+  // left NaN in them)
+  PYRO_CU(cudaMemsetAsync(sc.p, 0, SC_N * 8, st));
+  float ms = 0.0f;
+  PYRO_CU(cudaEventElapsedTime(&ms, evl0, evl1));
+  info->learned = keep;
+  info->learned_ms = ms;
+  return PYRO_OK;
+}
+
 int Solver::solve(cudaStream_t st, float* phi, const float* b, int mode, float tol,
                   int max_iters, PyroSolveInfo* info) {
-  PYRO_REQUIRE(mode >= PYRO_SOLVER_VCYCLE && mode <= PYRO_SOLVER_MGPCG_BF16,
+  PYRO_REQUIRE(mode >= PYRO_SOLVER_VCYCLE && mode <= PYRO_SOLVER_MGPCG_LEARNED,
                "solve: unknown mode");
   PYRO_REQUIRE(max_iters > 0, "solve: max_iters must be positive");
+  PYRO_REQUIRE(mode != PYRO_SOLVER_MGPCG_LEARNED || net,
+               "solve: the learned mode needs a network (set_net)");
   std::memset(info, 0, sizeof(*info));
   info->mode = mode;
+  info->learned = -1;
   float* save_phi = mg->phi[0];
   float* save_b = mg->b[0];
   const uint32_t* f0 = mg->f[0];
@@ -283,7 +346,7 @@ int Solver::solve(cudaStream_t st, float* phi, const float* b, int mode, float t
       }
     }
   } else {
-    const bool bf16 = mode == PYRO_SOLVER_MGPCG_BF16;
+    const bool bf16 = mode == PYRO_SOLVER_MGPCG_BF16 || mode == PYRO_SOLVER_MGPCG_LEARNED;
     double* S = sc.as<double>();
     // r = b - A phi, |r|, |b|
     PYRO_CU(cudaMemsetAsync(sc.p, 0, SC_N * 8, st));
@@ -295,6 +358,14 @@ int Solver::solve(cudaStream_t st, float* phi, const float* b, int mode, float t
     double bb2 = host_sc[SC_BB];
     bn = std::sqrt(bb2);
     rel = bb2 > 0 ? std::sqrt(host_sc[SC_RR] / bb2) : 0.0;
+    info->rel_resid_start = rel;
+    info->rel_resid_learned = rel;
+    if (mode == PYRO_SOLVER_MGPCG_LEARNED && bb2 > 0 && rel > tol) {
+      double rr = host_sc[SC_RR];
+      if ((rc = learned_stage(st, phi, &rr, info)) != PYRO_OK) return rc;
+      rel = std::sqrt(rr / bb2);
+      info->rel_resid_learned = rel;
+    }
     // CG with residual replacement: when the recursively updated residual
     // meets the tolerance the true residual is recomputed; if it does not
     // meet it, CG restarts from the true residual.
@@ -429,6 +500,23 @@ int pyro_poisson_solve(PyroPoisson* ps, const float* b, float* phi, int mode, fl
   clear_error();
   PYRO_REQUIRE(ps && b && phi && info, "pyro_poisson_solve: null argument");
   return ps->solver.solve(ps->stream, phi, b, mode, tol, max_iters, info);
+}
+
+int pyro_poisson_set_net(PyroPoisson* ps, PyroNet* net) {
+  clear_error();
+  PYRO_REQUIRE(ps, "pyro_poisson_set_net: null solver");
+  ps->solver.net = net;
+  return PYRO_OK;
+}
+
+int pyro_learned_accept(double re, double eae, double rae, double aeae, double rr,
+                        double* alpha, double* rr_new) {
+  double a = re / eae;
+  double n = rr - 2.0 * a * rae + a * a * aeae;
+  bool keep = std::isfinite(a) && std::isfinite(n) && std::isfinite(rr) && n < rr;
+  if (alpha) *alpha = keep ? a : 0.0;
+  if (rr_new) *rr_new = keep ? std::max(n, 0.0) : rr;
+  return keep ? 1 : 0;
 }
 
 int pyro_poisson_stream(PyroPoisson* ps, void** stream) {

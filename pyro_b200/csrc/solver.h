@@ -16,7 +16,8 @@ struct Solver {
   double* host_sc = nullptr;  // pinned mirror
   // BF16 hierarchy for the low-precision preconditioner
   DevBuf bphi[4], bphi2[4], bb[4];
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, evl0 = nullptr, evl1 = nullptr;
+  PyroNet* net = nullptr;   // learned stage of PYRO_SOLVER_MGPCG_LEARNED (not owned)
 
   int init(Multigrid* m);
   ~Solver();
@@ -29,6 +30,9 @@ struct Solver {
  private:
   cudaError_t precond(cudaStream_t st, bool bf16);
   int true_resid(cudaStream_t st, const float* phi, const float* b, double* rel, double* bn);
+  // phi += alpha net(r) when that lowers |r| (r = b - A phi on entry, kept
+  // consistent); *rr is |r|^2 in and out.
+  int learned_stage(cudaStream_t st, float* phi, double* rr, PyroSolveInfo* info);
 };
 
 }  // namespace pyro

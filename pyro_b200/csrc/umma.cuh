@@ -32,6 +32,16 @@ __device__ __forceinline__ uint64_t smem_desc(const void* base, int rows) {
   return start | (lbo << 16) | (sbo << 32) | (1ull << 46);  // version 1, no swizzle
 }
 
+// Descriptor with an explicit leading-byte offset (distance between the two
+// 8-element K halves of a 16-wide K step); core matrices along M/N 128 B
+// apart.
+__device__ __forceinline__ uint64_t smem_desc_lbo(const void* base, uint32_t lbo_bytes) {
+  uint64_t start = (smem_u32(base) >> 4) & 0x3FFFull;
+  uint64_t lbo = ((uint64_t)lbo_bytes >> 4) & 0x3FFFull;
+  uint64_t sbo = (128ull >> 4) & 0x3FFFull;
+  return start | (lbo << 16) | (sbo << 32) | (1ull << 46);
+}
+
 // Instruction descriptor, kind::f16: D f32, A and B bf16, both K-major.
 __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
@@ -104,6 +114,36 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* mbar, uint32_t parit
   for (uint32_t i = 0; i < limit; i++)
     if (mbar_try_wait(mbar, parity)) return true;
   return false;
+}
+
+// Arm the barrier's phase with `bytes` of expected transactions (one
+// arrival).
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mbar)),
+               "r"(bytes)
+               : "memory");
+}
+
+// TMA tiled loads global -> shared (no multicast), completing on `mbar`.
+// Coordinates are element indices, innermost first; out-of-range boxes are
+// zero-filled.  The innermost coordinate times the element size must be a
+// multiple of 16 bytes.
+__device__ __forceinline__ void tma_load_5d(void* dst, const void* tmap, int c0, int c1, int c2,
+                                            int c3, int c4, uint64_t* mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+      "[%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(tmap)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4),
+      "r"(smem_u32(mbar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const void* tmap, int c0, int c1, int c2,
+                                            uint64_t* mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+      "[%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(tmap)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(mbar))
+      : "memory");
 }
 
 // 32 lanes x 16 columns of 32-bit TMEM into 16 registers per thread.

@@ -1,0 +1,148 @@
+"""The learned pressure stage over the C ABI (pyro_net_*).
+
+    net = Net(seed=0)                     # or Net.load("warmstart.pnet")
+    net.forward(b_ptr, flags_ptr, (nx, ny, nz), nb, h, phi_ptr)
+    loss, grad = net.loss_grad(...)       # gradient check
+    net.train_step(..., lr=1e-3)          # asynchronous; net.last_loss()
+    ps.set_net(net); ps.solve(..., mode=SOLVER_MGPCG_LEARNED, ...)
+
+Device pointers are plain ints (e.g. torch.Tensor.data_ptr()).  The
+network has no counterpart in the reference; it stands beside the
+multigrid solve of src/sim.rs:451-491, which remains the fallback.
+
+Weights file (little endian): b"PYRONET1", u32 version (1), u32 count,
+f32 out_scale, u32 reserved, then `count` f32 parameters (every layer's
+weights [Cout][27][Cin], then every layer's biases).
+"""
+from __future__ import annotations
+
+import ctypes
+import struct
+from typing import Optional, Tuple
+
+import numpy as np
+
+from . import _abi
+
+MAGIC = b"PYRONET1"
+# (cin, cout, level, relu) of conv1 .. conv9, as in csrc/net.h
+SPEC = [(2, 16, 0, 1), (16, 16, 0, 1), (16, 32, 1, 1), (32, 32, 1, 1), (32, 64, 2, 1),
+        (64, 64, 2, 1), (96, 32, 1, 1), (48, 16, 0, 1), (16, 1, 0, 0)]
+
+
+def _vp(p):
+    return ctypes.c_void_p(int(p)) if p else None
+
+
+class Net:
+    def __init__(self, seed: int = 0):
+        self._lib = _abi.load()
+        h = ctypes.c_void_p()
+        _abi.check("pyro_net_create", self._lib.pyro_net_create(seed, ctypes.byref(h)))
+        self._h = h
+        n = ctypes.c_uint64()
+        _abi.check("pyro_net_param_count", self._lib.pyro_net_param_count(h, ctypes.byref(n)))
+        self.n_params = int(n.value)
+
+    @property
+    def handle(self):
+        return self._h
+
+    # ---------------------------------------------------------- parameters
+    def get_params(self) -> Tuple[np.ndarray, float]:
+        p = np.empty(self.n_params, np.float32)
+        s = ctypes.c_float()
+        _abi.check("pyro_net_get_params", self._lib.pyro_net_get_params(
+            self._h, p.ctypes.data_as(ctypes.c_void_p), self.n_params, ctypes.byref(s)))
+        return p, float(s.value)
+
+    def set_params(self, p: np.ndarray, out_scale: float = 1.0) -> None:
+        p = np.ascontiguousarray(p, np.float32)
+        if p.size != self.n_params:
+            raise ValueError(f"expected {self.n_params} parameters, got {p.size}")
+        _abi.check("pyro_net_set_params", self._lib.pyro_net_set_params(
+            self._h, p.ctypes.data_as(ctypes.c_void_p), self.n_params, float(out_scale)))
+
+    def save(self, path: str) -> None:
+        p, s = self.get_params()
+        with open(path, "wb") as fh:
+            fh.write(MAGIC + struct.pack("<IIfI", 1, p.size, s, 0) + p.astype("<f4").tobytes())
+
+    @staticmethod
+    def read_file(path: str) -> Tuple[np.ndarray, float]:
+        with open(path, "rb") as fh:
+            data = fh.read()
+        if data[:8] != MAGIC:
+            raise ValueError(f"{path}: not a pyro network file")
+        ver, count, scale, _ = struct.unpack("<IIfI", data[8:24])
+        if ver != 1:
+            raise ValueError(f"{path}: unsupported version {ver}")
+        p = np.frombuffer(data[24:24 + 4 * count], "<f4").astype(np.float32)
+        if p.size != count:
+            raise ValueError(f"{path}: truncated")
+        return p, float(scale)
+
+    @classmethod
+    def load(cls, path: str) -> "Net":
+        p, s = cls.read_file(path)
+        net = cls()
+        net.set_params(p, s)
+        return net
+
+    def set_loss(self, w_phi: float = 1.0, w_res: float = 0.0) -> None:
+        """Training loss weights: pressure MSE and normalised residual
+        (pyro_net_set_loss)."""
+        _abi.check("pyro_net_set_loss", self._lib.pyro_net_set_loss(self._h, w_phi, w_res))
+        self.loss_weights = (float(w_phi), float(w_res))
+
+    # ------------------------------------------------------------- compute
+    def forward(self, b_ptr: int, flags_ptr: int, dims, nb: int, h: float, phi_ptr: int,
+                stream: Optional[int] = None) -> None:
+        nx, ny, nz = dims
+        _abi.check("pyro_net_forward", self._lib.pyro_net_forward(
+            self._h, _vp(b_ptr), _vp(flags_ptr), nx, ny, nz, nb, h, _vp(phi_ptr), _vp(stream)))
+
+    def loss_grad(self, b_ptr: int, flags_ptr: int, phi_ptr: int, dims, nb: int, h: float,
+                  want_grad: bool = True, stream: Optional[int] = None):
+        nx, ny, nz = dims
+        loss = ctypes.c_double()
+        g = np.empty(self.n_params, np.float32) if want_grad else None
+        _abi.check("pyro_net_loss_grad", self._lib.pyro_net_loss_grad(
+            self._h, _vp(b_ptr), _vp(flags_ptr), _vp(phi_ptr), nx, ny, nz, nb, h,
+            ctypes.byref(loss), g.ctypes.data_as(ctypes.c_void_p) if g is not None else None,
+            _vp(stream)))
+        return float(loss.value), g
+
+    def train_step(self, b_ptr: int, flags_ptr: int, phi_ptr: int, dims, nb: int, h: float,
+                   lr: float, clip: float = 1.0, stream: Optional[int] = None) -> None:
+        nx, ny, nz = dims
+        _abi.check("pyro_net_train_step", self._lib.pyro_net_train_step(
+            self._h, _vp(b_ptr), _vp(flags_ptr), _vp(phi_ptr), nx, ny, nz, nb, h, lr, clip,
+            _vp(stream)))
+
+    def last_loss(self, stream: Optional[int] = None) -> float:
+        loss = ctypes.c_double()
+        _abi.check("pyro_net_last_loss",
+                   self._lib.pyro_net_last_loss(self._h, ctypes.byref(loss), _vp(stream)))
+        return float(loss.value)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.pyro_net_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def learned_accept(re: float, eae: float, rae: float, aeae: float, rr: float):
+    """The keep-or-discard rule of the learned stage (pyro_learned_accept):
+    (keep, alpha, rr_new)."""
+    lib = _abi.load()
+    a = ctypes.c_double()
+    n = ctypes.c_double()
+    keep = lib.pyro_learned_accept(re, eae, rae, aeae, rr, ctypes.byref(a), ctypes.byref(n))
+    return bool(keep), float(a.value), float(n.value)

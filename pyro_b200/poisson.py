@@ -64,6 +64,13 @@ class PoissonSolver:
             _abi.check("pyro_poisson_solve", rc)
         return info
 
+    def set_net(self, net) -> None:
+        """Network for mode SOLVER_MGPCG_LEARNED (None detaches); the
+        caller keeps `net` alive while it is attached."""
+        self._net = net
+        _abi.check("pyro_poisson_set_net",
+                   self._lib.pyro_poisson_set_net(self._h, net.handle if net else None))
+
     def stream(self) -> int:
         s = ctypes.c_void_p()
         _abi.check("pyro_poisson_stream", self._lib.pyro_poisson_stream(self._h, ctypes.byref(s)))

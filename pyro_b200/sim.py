@@ -172,6 +172,13 @@ class Sim:
         _abi.check("pyro_sim_set_solver",
                    self._lib.pyro_sim_set_solver(self._h, mode, tol, max_iters))
 
+    def set_net(self, net) -> None:
+        """Network for mode SOLVER_MGPCG_LEARNED (None detaches); the
+        caller keeps `net` alive while it is attached."""
+        self._net = net
+        _abi.check("pyro_sim_set_net",
+                   self._lib.pyro_sim_set_net(self._h, net.handle if net else None))
+
     def last_solve(self) -> _abi.PyroSolveInfo:
         info = _abi.PyroSolveInfo()
         _abi.check("pyro_sim_last_solve",

@@ -1,5 +1,7 @@
 """tcgen05 implicit-GEMM convolutions against a plain PyTorch FP32 reference
-(torch.nn.functional.conv3d on the same BF16-rounded inputs).  Products of
+(torch.nn.functional.conv3d on the same BF16-rounded inputs).  Input
+channel counts that are multiples of 16 take the TMA-staged kernel, the
+others the gathering one; both are covered.  Products of
 BF16 values are exact in FP32, so the only differences are FP32 summation
 order: 1e-3 relative of each output's magnitude."""
 import numpy as np
@@ -43,7 +45,9 @@ def _wk(w):   # (Cout, C, 3, 3, 3) -> [Cout][27][C] bf16
 
 @pytest.mark.parametrize("C,Cout,dims,nb", [(16, 32, (8, 10, 12), 2), (2, 16, (9, 7, 11), 1),
                                             (96, 32, (6, 8, 8), 1), (16, 1, (8, 8, 8), 2),
-                                            (32, 64, (8, 16, 8), 1), (48, 16, (4, 8, 8), 1)])
+                                            (32, 64, (8, 16, 8), 1), (48, 16, (4, 8, 8), 1),
+                                            (32, 16, (5, 9, 13), 2), (16, 96, (6, 6, 40), 1),
+                                            (64, 128, (4, 8, 8), 1)])
 def test_forward(lib, C, Cout, dims, nb):
     nz, ny, nx = dims
     x, w, b = _tensors(nb, C, nz, ny, nx, Cout, 1)
@@ -57,7 +61,8 @@ def test_forward(lib, C, Cout, dims, nb):
 
 
 @pytest.mark.parametrize("Cin,Cout,dims", [(16, 32, (8, 10, 12)), (48, 16, (6, 8, 8)),
-                                           (96, 32, (4, 8, 8)), (32, 64, (8, 8, 8))])
+                                           (96, 32, (4, 8, 8)), (32, 64, (8, 8, 8)),
+                                           (16, 8, (5, 7, 9)), (64, 16, (3, 17, 20))])
 def test_backward_data_and_weight(lib, Cin, Cout, dims):
     nz, ny, nx = dims
     nb = 1
