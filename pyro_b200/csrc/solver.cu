@@ -185,7 +185,133 @@ __global__ void k_roll(double* sc) {
   sc[SC_RR] = 0.0;
 }
 
+// ---- cells the CG modes solve for ----------------------------------------
+// A fluid region sealed by solids with no Dirichlet face makes A singular
+// (its b need not sum to zero).  The CG modes solve only for fluid cells
+// connected through fluid faces to a Dirichlet face; the others keep their
+// initial phi and are treated as solid.  fa = 0 reached fluid, 1 solid or
+// unreached fluid; 2 marks fluid not reached yet while propagating.
+
+// order-independent 64-bit hash of the flag field
+__global__ void __launch_bounds__(256) k_flag_hash(L3 d, const uint32_t* __restrict__ f,
+                                                   unsigned long long* out) {
+  CELL_PROLOGUE
+  (void)fluid;
+  unsigned long long h = 0;
+  if (in && __ldg(f + i) == 1u) {
+    unsigned long long k = (unsigned long long)i * 0x9E3779B97F4A7C15ull + 0x632BE59BD9B4E019ull;
+    k ^= k >> 29;
+    k *= 0xBF58476D1CE4E5B9ull;
+    h = k ^ (k >> 32);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
+  if ((threadIdx.x & 31) == 0 && h) atomicAdd(out, h);
+}
+
+__global__ void __launch_bounds__(256) k_reach_init(L3 d, const uint32_t* __restrict__ f,
+                                                    int bc_mode, uint32_t* __restrict__ fa) {
+  CELL_PROLOGUE
+  if (!in) return;
+  if (!fluid) {
+    fa[i] = 1u;
+    return;
+  }
+  bool seed = y == d.ny - 1 ||
+              (bc_mode == 0 && (x == 0 || x == d.nx - 1 || z == 0 || z == d.nz - 1));
+  fa[i] = seed ? 0u : 2u;
+}
+
+// One 8x8x8 tile per block: propagate "reached" (0) into fluid (2) cells
+// through fluid faces until the tile stops changing (halo values read from
+// global memory), then write back; *changed is set when a cell was reached.
+constexpr int RT = 8;
+__global__ void __launch_bounds__(RT * RT * RT) k_reach_tile(L3 d, uint32_t* __restrict__ fa,
+                                                             int* __restrict__ changed) {
+  __shared__ uint8_t t[RT + 2][RT + 2][RT + 2];
+  const int lx = threadIdx.x % RT, ly = (threadIdx.x / RT) % RT, lz = threadIdx.x / (RT * RT);
+  const int bx = blockIdx.x * RT, by = blockIdx.y * RT, bz = blockIdx.z * RT;
+  for (int k = threadIdx.x; k < (RT + 2) * (RT + 2) * (RT + 2); k += RT * RT * RT) {
+    int hx = k % (RT + 2), hy = (k / (RT + 2)) % (RT + 2), hz = k / ((RT + 2) * (RT + 2));
+    int gx = bx + hx - 1, gy = by + hy - 1, gz = bz + hz - 1;
+    t[hz][hy][hx] = d.inb(gx, gy, gz) ? (uint8_t)fa[d.idx(gx, gy, gz)] : (uint8_t)1;
+  }
+  __syncthreads();
+  const int x = bx + lx, y = by + ly, z = bz + lz;
+  const bool mine = d.inb(x, y, z) && t[lz + 1][ly + 1][lx + 1] == 2;
+  bool got = false;
+  for (int it = 0; it < RT * RT * RT; it++) {
+    bool ch = false;
+    if (mine && !got) {
+      const int cx = lx + 1, cy = ly + 1, cz = lz + 1;
+      if (t[cz][cy][cx - 1] == 0 || t[cz][cy][cx + 1] == 0 || t[cz][cy - 1][cx] == 0 ||
+          t[cz][cy + 1][cx] == 0 || t[cz - 1][cy][cx] == 0 || t[cz + 1][cy][cx] == 0) {
+        t[cz][cy][cx] = 0;
+        got = true;
+        ch = true;
+      }
+    }
+    if (!__syncthreads_or(ch)) break;
+  }
+  if (got) {
+    fa[d.idx(x, y, z)] = 0u;
+    *changed = 1;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_reach_final(L3 d, uint32_t* __restrict__ fa) {
+  int x = blockIdx.x * BX + threadIdx.x, y = blockIdx.y * BY + threadIdx.y,
+      z = blockIdx.z * BZ + threadIdx.z;
+  if (!d.inb(x, y, z)) return;
+  int i = d.idx(x, y, z);
+  if (fa[i] == 2u) fa[i] = 1u;
+}
+
 }  // namespace
+
+int Solver::update_reach(cudaStream_t st) {
+  const uint32_t* f0 = mg->f[0];
+  L3 l{d.nx, d.ny, d.nz};
+  if (!fa.p) {
+    int rc;
+    if ((rc = fa.alloc(d.cells() * 4)) != PYRO_OK || (rc = reach_dev.alloc(16)) != PYRO_OK)
+      return rc;
+  }
+  unsigned long long* H = reach_dev.as<unsigned long long>();
+  PYRO_CU(cudaMemsetAsync(H, 0, 16, st));
+  k_flag_hash<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, f0, H);
+  PYRO_CU(cudaGetLastError());
+  PYRO_CU(cudaMemcpyAsync(host_sc, H, 8, cudaMemcpyDeviceToHost, st));
+  PYRO_CU(cudaStreamSynchronize(st));
+  unsigned long long h;
+  std::memcpy(&h, host_sc, 8);
+  if (reach_valid && h == reach_hash && reach_flags == f0) return PYRO_OK;
+  k_reach_init<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, f0, mg->bc_mode, fa.as<uint32_t>());
+  PYRO_CU(cudaGetLastError());
+  dim3 tg((unsigned)((d.nx + RT - 1) / RT), (unsigned)((d.ny + RT - 1) / RT),
+          (unsigned)((d.nz + RT - 1) / RT));
+  int* C = reinterpret_cast<int*>(H + 1);
+  // every launch reaches at least one more tile along each front; the
+  // number of launches is bounded by the tile count
+  const long max_rounds = (long)tg.x * tg.y * tg.z + 8;
+  bool done = false;
+  for (long r = 0; r < max_rounds && !done; r += 4) {
+    PYRO_CU(cudaMemsetAsync(C, 0, 4, st));
+    for (int k = 0; k < 4; k++) k_reach_tile<<<tg, RT * RT * RT, 0, st>>>(l, fa.as<uint32_t>(), C);
+    PYRO_CU(cudaGetLastError());
+    int c = 0;
+    PYRO_CU(cudaMemcpyAsync(host_sc, C, 4, cudaMemcpyDeviceToHost, st));
+    PYRO_CU(cudaStreamSynchronize(st));
+    std::memcpy(&c, host_sc, 4);
+    done = c == 0;
+  }
+  k_reach_final<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, fa.as<uint32_t>());
+  PYRO_CU(cudaGetLastError());
+  reach_hash = h;
+  reach_flags = f0;
+  reach_valid = true;
+  return PYRO_OK;
+}
 
 int Solver::init(Multigrid* m) {
   mg = m;
@@ -218,7 +344,7 @@ Solver::~Solver() {
 }
 
 size_t Solver::device_bytes() const {
-  size_t s = r.bytes + z.bytes + p.bytes + q.bytes + sc.bytes;
+  size_t s = r.bytes + z.bytes + p.bytes + q.bytes + sc.bytes + fa.bytes + reach_dev.bytes;
   for (int l = 0; l < 4; l++) s += bphi[l].bytes + bphi2[l].bytes + bb[l].bytes;
   return s;
 }
@@ -319,7 +445,8 @@ int Solver::solve(cudaStream_t st, float* phi, const float* b, int mode, float t
   info->learned = -1;
   float* save_phi = mg->phi[0];
   float* save_b = mg->b[0];
-  const uint32_t* f0 = mg->f[0];
+  const uint32_t* save_f0 = mg->f[0];
+  const uint32_t* f0 = save_f0;
   PYRO_CU(cudaEventRecord(ev0, st));
   int iters = 0;
   double rel = 0, bn = 0;
@@ -348,6 +475,17 @@ int Solver::solve(cudaStream_t st, float* phi, const float* b, int mode, float t
   } else {
     const bool bf16 = mode == PYRO_SOLVER_MGPCG_BF16 || mode == PYRO_SOLVER_MGPCG_LEARNED;
     double* S = sc.as<double>();
+    // CG and its V-cycle run on the reachable fluid cells only
+    if ((rc = update_reach(st)) != PYRO_OK) return rc;
+    f0 = fa.as<uint32_t>();
+    mg->bind_level0(save_phi, save_b, f0);
+    struct Rebind {
+      Multigrid* m;
+      float* p;
+      float* b;
+      const uint32_t* f;
+      ~Rebind() { m->bind_level0(p, b, f); }
+    } rebind{mg, save_phi, save_b, save_f0};
     // r = b - A phi, |r|, |b|
     PYRO_CU(cudaMemsetAsync(sc.p, 0, SC_N * 8, st));
     k_resid<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, ih2, phi, b, f0, mg->bc_mode,

@@ -18,6 +18,12 @@ struct Solver {
   DevBuf bphi[4], bphi2[4], bb[4];
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evl0 = nullptr, evl1 = nullptr;
   PyroNet* net = nullptr;   // learned stage of PYRO_SOLVER_MGPCG_LEARNED (not owned)
+  // flags of the CG modes: fluid cells without a fluid path to a Dirichlet
+  // face are marked solid (recomputed when the flag field changes)
+  DevBuf fa, reach_dev;
+  unsigned long long reach_hash = 0;
+  const uint32_t* reach_flags = nullptr;
+  bool reach_valid = false;
 
   int init(Multigrid* m);
   ~Solver();
@@ -33,6 +39,7 @@ struct Solver {
   // phi += alpha net(r) when that lowers |r| (r = b - A phi on entry, kept
   // consistent); *rr is |r|^2 in and out.
   int learned_stage(cudaStream_t st, float* phi, double* rr, PyroSolveInfo* info);
+  int update_reach(cudaStream_t st);
 };
 
 }  // namespace pyro

@@ -106,3 +106,43 @@ def test_tolerance_solvers_vs_fp64(lib, mode, tol, bc_mode):
     # Neumann-sided case is worse conditioned)
     assert err <= (200 if bc_mode == 0 else 2000) * tol, (mode, tol, err)
     lib.pyro_poisson_destroy(ps)
+
+
+@pytest.mark.parametrize("mode", [_abi.SOLVER_MGPCG, _abi.SOLVER_MGPCG_BF16])
+def test_mgpcg_sealed_pockets(lib, mode):
+    """Fluid sealed by solids (no path to a Dirichlet face) makes the system
+    singular; the CG modes leave such cells at their initial phi and solve
+    the rest (the bonfire's log pile seals a few cells like this)."""
+    from pyro_b200.poisson import PoissonSolver, poisson_case
+    n = 48
+    f, b = poisson_case(n, n, n, seed=11)
+    # a hollow solid box (walls 1 cell) enclosing a 4^3 fluid pocket, and a
+    # single sealed cell
+    f[10:16, 10:16, 10:16] = 1
+    f[11:15, 11:15, 11:15] = 0
+    f[30:33, 30:33, 30:33] = 1
+    f[31, 31, 31] = 0
+    b[11:15, 11:15, 11:15] = 3.0          # inconsistent source inside the pocket
+    b[31, 31, 31] = -2.0
+    ps = PoissonSolver((n, n, n), 0.05, bc_mode=0)
+    fd = dev(f.astype(np.int32))
+    ps.set_flags(fd.data_ptr())
+    bd = dev(b)
+    phi0 = np.zeros_like(b)
+    phi0[11:15, 11:15, 11:15] = 0.25
+    pd = dev(phi0)
+    info = ps.solve(bd.data_ptr(), pd.data_ptr(), mode, 1e-6, 100)
+    phi = host(pd)
+    assert info.converged and np.isfinite(info.rel_resid)
+    assert np.all(np.isfinite(phi))
+    assert np.all(phi[11:15, 11:15, 11:15] == 0.25) and phi[31, 31, 31] == 0.0
+    # the residual over the reachable cells agrees with the float64 oracle
+    reach = f == 0
+    reach[11:15, 11:15, 11:15] = False
+    reach[31, 31, 31] = False
+    flags_r = np.where(reach, 0, 1).astype(np.uint32)
+    b_r = np.where(reach, b, 0.0).astype(np.float32)
+    rel = oracle.poisson_relres((n, n, n), 0.05, phi, b_r, flags_r, bc_mode=0)
+    assert rel <= 1.5e-6, rel
+    assert abs(rel - info.rel_resid) <= 1e-7
+    ps.close()
