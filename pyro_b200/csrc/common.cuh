@@ -263,6 +263,78 @@ struct Vel {
     b = x - k * ub;
     f = x + k * uf;
   }
+
+  // velAt at a face or cell centre, where every trilinear fraction is 0,
+  // 1/2 or (clamped) 1: the same value as at() bit for bit (mix(a, b, 0) =
+  // a, mix(a, b, 1/2) = a * 0.5 + b * 0.5, mix(a, b, 1) = b), with only
+  // the loads and additions that remain, in at()'s x, y, z order.
+  __device__ __forceinline__ F3 at_face(const Grid& g, int k, I3 c) const {
+    return F3{face_comp(g, 0, k, c), face_comp(g, 1, k, c), face_comp(g, 2, k, c)};
+  }
+  __device__ __forceinline__ F3 at_center(const Grid& g, I3 c) const {
+    const int sy = g.nx + 1, sz = (g.nx + 1) * (g.ny + 1);
+    const int i = c.x + sy * c.y + sz * c.z;
+    return F3{__ldg(u + i) * 0.5f + __ldg(u + i + 1) * 0.5f,
+              __ldg(v + i) * 0.5f + __ldg(v + i + sy) * 0.5f,
+              __ldg(w + i) * 0.5f + __ldg(w + i + sz) * 0.5f};
+  }
+  // back / both with the first sample at the k-face of cell c (k = 3: the
+  // cell centre); x is that position.
+  __device__ __forceinline__ F3 first(const Grid& g, int k, I3 c) const {
+    return k == 3 ? at_center(g, c) : at_face(g, k, c);
+  }
+  __device__ __forceinline__ F3 back_at(const Grid& g, float kk, int k, I3 c, F3 x) const {
+    F3 u1 = first(g, k, c);
+    F3 u2 = at(g, x - (0.5f * kk) * u1);
+    return x - kk * u2;
+  }
+  __device__ __forceinline__ void both_at(const Grid& g, float kk, int k, I3 c, F3 x, F3& b,
+                                          F3& f) const {
+    F3 u1 = first(g, k, c);
+    F3 h = (0.5f * kk) * u1;
+    F3 ub = at(g, x - h);
+    F3 uf = at(g, x + h);
+    b = x - kk * ub;
+    f = x + kk * uf;
+  }
+
+ private:
+  // Component j sampled at the k-face position of cell c.  Along axis k the
+  // coordinate is c - 1/2 (clamped to [0, n - 1]: the lower value alone at
+  // c = 0, the upper alone past the top), along axis j it is c + 1/2, along
+  // the third axis c itself; for j == k the face value itself.
+  __device__ __forceinline__ float face_comp(const Grid& g, int j, int k, I3 c) const {
+    const float* X = j == 0 ? u : (j == 1 ? v : w);
+    const int sy = g.nx + 1, sz = (g.nx + 1) * (g.ny + 1);
+    const int cc[3] = {c.x, c.y, c.z}, n[3] = {g.nx, g.ny, g.nz}, st[3] = {1, sy, sz};
+    if (j == k) return __ldg(X + c.x + sy * c.y + sz * c.z);
+    // base index and the two averaged axes (ordered x < y < z)
+    int two[3];
+    int base = 0;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      int b = cc[a];
+      int t = 0;
+      if (a == k) {
+        if (b <= 0) b = 0;
+        else if (b > n[a] - 1) b = n[a] - 1;
+        else { b -= 1; t = 1; }
+      } else if (a == j) {
+        t = 1;
+      }
+      two[a] = t;
+      base += st[a] * b;
+    }
+    const int a1 = j < k ? j : k, a2 = j < k ? k : j;
+    const int s1 = st[a1], s2 = st[a2];
+    auto avg1 = [&](int i) {
+      return two[a1] ? __ldg(X + i) * 0.5f + __ldg(X + i + s1) * 0.5f : __ldg(X + i);
+    };
+    float r0 = avg1(base);
+    if (!two[a2]) return r0;
+    float r1 = avg1(base + s2);
+    return r0 * 0.5f + r1 * 0.5f;
+  }
 };
 
 // -------------------------------------------------------------- statistics

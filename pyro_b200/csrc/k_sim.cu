@@ -256,7 +256,8 @@ __global__ void __launch_bounds__(256) k_adv_vel1(const PyroParams* __restrict__
   for (int k = 0; k < 3; k++) {
     if (!g.compValid(k, c)) continue;
     F3 off = compOff(k);
-    float r = triC(pick3(k, u, v, w), g, V.back(g, kk, tof3(c) + off) - off, g.compHi(k));
+    float r = triC(pick3(k, u, v, w), g, V.back_at(g, kk, k, c, tof3(c) + off) - off,
+                   g.compHi(k));
     if (k == 0) hu[i] = r; else if (k == 1) hv[i] = r; else hw[i] = r;
   }
 }
@@ -291,7 +292,7 @@ __global__ void __launch_bounds__(256) k_adv_vel2(const PyroParams* __restrict__
       I3 hi = g.compHi(k);
       F3 x = tof3(c) + off;
       F3 b, f;
-      V.both(g, kk, x, b, f);
+      V.both_at(g, kk, k, c, x, b, f);
       b = b - off;
       f = f - off;
       const float* vk = pick3(k, u, v, w);
@@ -318,14 +319,14 @@ __global__ void __launch_bounds__(256) k_adv_s1(const PyroParams* __restrict__ P
   const float kk = P.dt / P.dx;
   Vel V{u, v, w};
   const F3 half{0.5f, 0.5f, 0.5f};
-  F3 b = V.back(g, kk, tof3(c) + half) - half;
+  F3 b = V.back_at(g, kk, 3, c, tof3(c) + half) - half;
   float t = wclamp(g.outside(b), 0.0f, 1.0f);
   int i = g.sidx(c);
   h0[i] = wmix4(triS(s0, g, b), make_float4(P.t0, 0.0f, P.yo2, 0.0f), t);
   h1[i] = wmix4(triS(s1, g, b), make_float4(0.0f, 0.0f, 0.0f, 0.0f), t);
 }
 
-__global__ void __launch_bounds__(256) k_adv_s2(const PyroParams* __restrict__ Pp, Grid g,
+__global__ void __launch_bounds__(256, 4) k_adv_s2(const PyroParams* __restrict__ Pp, Grid g,
                                                 const float* __restrict__ u,
                                                 const float* __restrict__ v,
                                                 const float* __restrict__ w,
@@ -342,7 +343,7 @@ __global__ void __launch_bounds__(256) k_adv_s2(const PyroParams* __restrict__ P
   const F3 half{0.5f, 0.5f, 0.5f};
   F3 x = tof3(c) + half;
   F3 b, f;
-  V.both(g, kk, x, b, f);
+  V.both_at(g, kk, 3, c, x, b, f);
   b = b - half;
   f = f - half;
   int i = g.sidx(c);

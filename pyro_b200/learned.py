@@ -146,3 +146,58 @@ def learned_accept(re: float, eae: float, rae: float, aeae: float, rr: float):
     n = ctypes.c_double()
     keep = lib.pyro_learned_accept(re, eae, rae, aeae, rr, ctypes.byref(a), ctypes.byref(n))
     return bool(keep), float(a.value), float(n.value)
+
+
+# Per-voxel multiply-adds of the network, x2 for FLOPs: level 0 convs 1, 2,
+# 8, 9 (K = 27 Cin, N = Cout), level 1 convs 3, 4, 7 (1/8 of the voxels),
+# level 2 convs 5, 6 (1/64).
+def flops_per_voxel() -> float:
+    f = 0.0
+    for ci, co, lvl, _ in SPEC:
+        f += 2.0 * 27 * ci * co / (8 ** lvl)
+    return f
+
+
+def main(argv=None) -> int:
+    """python -m pyro_b200.learned bench [--dims NX,NY,NZ] [--reps N]
+    [--weights FILE]: device time of the network's forward pass on a seeded
+    Poisson right-hand side."""
+    import argparse
+    import json
+
+    import torch
+
+    from .poisson import poisson_case
+    ap = argparse.ArgumentParser(prog="pyro_b200.learned")
+    ap.add_argument("cmd", choices=["bench"])
+    ap.add_argument("--dims", default="160,320,160")
+    ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--weights")
+    a = ap.parse_args(argv)
+    nx, ny, nz = (int(v) for v in a.dims.split(","))
+    f, b = poisson_case(nx, ny, nz, seed=1)
+    net = Net.load(a.weights) if a.weights else Net(seed=0)
+    bd = torch.from_numpy(b).cuda()
+    fd = torch.from_numpy(f.astype(np.int32)).cuda()
+    phi = torch.empty_like(bd)
+    s = torch.cuda.current_stream().cuda_stream
+    for _ in range(2):
+        net.forward(bd.data_ptr(), fd.data_ptr(), (nx, ny, nz), 1, 0.02, phi.data_ptr(), stream=s)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.reps):
+        net.forward(bd.data_ptr(), fd.data_ptr(), (nx, ny, nz), 1, 0.02, phi.data_ptr(), stream=s)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / a.reps
+    vox = nx * ny * nz
+    print(json.dumps(dict(dims=[nx, ny, nz], ms=ms, voxels=vox,
+                          tflops=flops_per_voxel() * vox / ms * 1e-9,
+                          flops_per_voxel=flops_per_voxel())))
+    return 0
+
+
+if __name__ == "__main__":
+    import sys
+    sys.exit(main())
