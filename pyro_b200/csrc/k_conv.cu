@@ -250,6 +250,43 @@ struct ConvEpi {
   int V, Nout, relu;
   __device__ void operator()(int m, int col, const float (&v)[16]) const {
     if (m < 0 || m >= V) return;
+    if (out_bf16 && (Nout & 15) == 0) {
+      // 16 channels of one row: 32 contiguous bytes, two 16-byte stores
+      float a[16];
+#pragma unroll
+      for (int j = 0; j < 16; j += 4) {
+        float4 bb = bias ? __ldg(reinterpret_cast<const float4*>(bias + col + j))
+                         : make_float4(0.f, 0.f, 0.f, 0.f);
+        a[j] = v[j] + bb.x;
+        a[j + 1] = v[j + 1] + bb.y;
+        a[j + 2] = v[j + 2] + bb.z;
+        a[j + 3] = v[j + 3] + bb.w;
+      }
+      if (!bias) {
+#pragma unroll
+        for (int j = 0; j < 16; j++) a[j] = v[j];
+      }
+      if (relu) {
+#pragma unroll
+        for (int j = 0; j < 16; j++) a[j] = fmaxf(a[j], 0.0f);
+      }
+      if (mask) {
+        const uint4* mp = reinterpret_cast<const uint4*>(mask + (size_t)m * Nout + col);
+        uint4 mk[2] = {__ldg(mp), __ldg(mp + 1)};
+        const bf16* mb = reinterpret_cast<const bf16*>(mk);
+#pragma unroll
+        for (int j = 0; j < 16; j++)
+          if (!(__bfloat162float(mb[j]) > 0.0f)) a[j] = 0.0f;
+      }
+      uint4 o[2];
+      __nv_bfloat162* ob = reinterpret_cast<__nv_bfloat162*>(o);
+#pragma unroll
+      for (int j = 0; j < 8; j++) ob[j] = __floats2bfloat162_rn(a[2 * j], a[2 * j + 1]);
+      uint4* op = reinterpret_cast<uint4*>(out_bf16 + (size_t)m * Nout + col);
+      op[0] = o[0];
+      op[1] = o[1];
+      return;
+    }
 #pragma unroll
     for (int j = 0; j < 16; j++) {
       int n = col + j;
