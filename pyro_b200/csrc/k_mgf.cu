@@ -298,32 +298,46 @@ __global__ void __launch_bounds__(256) k_mg_prolong_m(L df, const TS* __restrict
   if (ws > 1e-4f) stv(pf + i, ldv(pf + i) + acc / ws);
 }
 
-// One colour pass with the neighbour mask: thread (hx, y, z) updates the
-// cell x = 2 hx + ((y + z + colour) & 1) (mg.wgsl:17-36) reading its own
-// mask and b and the neighbours the mask marks.
+// One colour pass with the neighbour mask (mg.wgsl:17-36).  A cell's colour
+// is (x + y + z) & 1, so the cells of one colour in a column (x, y) sit at
+// every other z.  Thread (hx, y, zq) updates the four cells
+// z = z0, z0 + 2, z0 + 4, z0 + 6 (z0 = 8 (zq >> 1) + (zq & 1)) at
+// x = 2 hx + ((y + z0 + colour) & 1), carrying the phi above one cell as the
+// phi below the next.  Cells of one colour only read the other colour, so
+// the update is independent of this mapping.
 template <typename TS>
 __global__ void __launch_bounds__(256) k_mg_pass(L d, float h2, const TS* __restrict__ b,
                                                  const uint8_t* __restrict__ meta,
                                                  TS* __restrict__ p, int color, float omega,
                                                  int bc_mode) {
-  int y = blockIdx.y * 4 + threadIdx.y;
-  int z = blockIdx.z * 2 + threadIdx.z;
-  int x = (int)(blockIdx.x * 32 + threadIdx.x) * 2 + ((y + z + color) & 1);
-  if (x >= d.nx || y >= d.ny || z >= d.nz) return;
-  int i = d.idx(x, y, z);
-  uint32_t m = __ldg(meta + i);
-  if (m & META_SOLID) return;
+  const int y = blockIdx.y * 4 + threadIdx.y;
+  const int zq = blockIdx.z * 2 + threadIdx.z;
+  const int z0 = (zq >> 1) * 8 + (zq & 1);
+  const int x = (int)(blockIdx.x * 32 + threadIdx.x) * 2 + ((y + z0 + color) & 1);
+  if (x >= d.nx || y >= d.ny || z0 >= d.nz) return;
   const int sy = d.nx, sz = d.nx * d.ny;
-  float sum = 0.0f;
-  if (m & 1u) sum += ldv(p + i + 1);
-  if (m & 2u) sum += ldv(p + i - 1);
-  if (m & 4u) sum += ldv(p + i + sy);
-  if (m & 8u) sum += ldv(p + i - sy);
-  if (m & 16u) sum += ldv(p + i + sz);
-  if (m & 32u) sum += ldv(p + i - sz);
-  float cnt = (float)(__popc(m & 63u) + dirichlet_faces(d, x, y, z, bc_mode));
-  if (cnt < 0.5f) return;
-  stv(p + i, wmix(ldv(p + i), (sum - h2 * ldv(b + i)) / cnt, omega));
+  const int i0 = d.idx(x, y, z0);
+  float below = z0 > 0 ? ldv(p + i0 - sz) : 0.0f;
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const int z = z0 + 2 * j;
+    if (z >= d.nz) break;
+    const int i = i0 + 2 * j * sz;
+    const float above = z + 1 < d.nz ? ldv(p + i + sz) : 0.0f;
+    const uint32_t m = __ldg(meta + i);
+    if (!(m & META_SOLID)) {
+      float sum = 0.0f;
+      if (m & 1u) sum += ldv(p + i + 1);
+      if (m & 2u) sum += ldv(p + i - 1);
+      if (m & 4u) sum += ldv(p + i + sy);
+      if (m & 8u) sum += ldv(p + i - sy);
+      if (m & 16u) sum += above;
+      if (m & 32u) sum += below;
+      const float cnt = (float)(__popc(m & 63u) + dirichlet_faces(d, x, y, z, bc_mode));
+      if (cnt >= 0.5f) stv(p + i, wmix(ldv(p + i), (sum - h2 * ldv(b + i)) / cnt, omega));
+    }
+    below = above;
+  }
 }
 
 // Restriction with the neighbour mask (mg.wgsl:38-83): coarse rhs = mean of
@@ -491,7 +505,8 @@ cudaError_t rb_launch(Dims3 d, float h, const TS* b, const uint8_t* meta, const 
 template <typename TS>
 cudaError_t pass_t(Dims3 d, float h, const TS* b, const uint8_t* meta, TS* p, int color,
                    float omega, int bc_mode, cudaStream_t st) {
-  dim3 grid(((d.nx + 1) / 2 + 31) / 32, (d.ny + 3) / 4, (d.nz + 1) / 2);
+  // z: one block per 8 planes (two threads, one per z parity)
+  dim3 grid(((d.nx + 1) / 2 + 31) / 32, (d.ny + 3) / 4, (d.nz + 7) / 8);
   k_mg_pass<TS><<<grid, dim3(32, 4, 2), 0, st>>>(L{d.nx, d.ny, d.nz}, h * h, b, meta, p, color,
                                                 omega, bc_mode);
   return cudaGetLastError();
