@@ -315,6 +315,13 @@ int pyro_k_mg_resid(uint32_t nx, uint32_t ny, uint32_t nz, float h,
 int pyro_k_mg_coarse(uint32_t nx, uint32_t ny, uint32_t nz, float h,
                      const float* b, const uint32_t* flags, float* phi,
                      int iters, float omega, void* stream);
+/* Coarsest-level solve of the symmetric V-cycle (MGPCG preconditioner):
+ * `iters` SOR iterations alternating red-black and black-red (iteration
+ * it starts with colour it & 1); bc_mode as pyro_poisson_create.  No
+ * counterpart in the reference. */
+int pyro_k_mg_coarse_sym(uint32_t nx, uint32_t ny, uint32_t nz, float h,
+                         const float* b, const uint32_t* flags, float* phi,
+                         int iters, float omega, int bc_mode, void* stream);
 
 /* ---- learned warm start: tcgen05 convolutions --------------------------- */
 /* 3x3x3 convolution, padding 1, stride 1, as an implicit GEMM on the

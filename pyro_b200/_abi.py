@@ -154,6 +154,7 @@ SIGNATURES = {
     "pyro_k_mg_prolong": [_U32, _U32, _U32, _P, _P, _P, _U32, _U32, _U32, _P, _P],
     "pyro_k_mg_resid": [_U32, _U32, _U32, _F, _P, _P, _P, _P, _P],
     "pyro_k_mg_coarse": [_U32, _U32, _U32, _F, _P, _P, _P, _I, _F, _P],
+    "pyro_k_mg_coarse_sym": [_U32, _U32, _U32, _F, _P, _P, _P, _I, _F, _I, _P],
     "pyro_conv3_forward": [_P, _I, _I, _I, _I, _I, _P, _I, _P, _I, _P, _I, _P],
     "pyro_conv3_backward_data": [_P, _I, _I, _I, _I, _I, _P, _I, _P, _P, _I, _P],
     "pyro_conv3_backward_weight": [_P, _I, _P, _I, _I, _I, _I, _I, _P, _P],

@@ -204,6 +204,20 @@ int pyro_k_mg_coarse(uint32_t nx, uint32_t ny, uint32_t nz, float h, const float
   return ret(e, "pyro_k_mg_coarse");
 }
 
+int pyro_k_mg_coarse_sym(uint32_t nx, uint32_t ny, uint32_t nz, float h, const float* b,
+                         const uint32_t* flags, float* phi, int iters, float omega, int bc_mode,
+                         void* stream) {
+  clear_error();
+  PYRO_REQUIRE(dims_ok(nx, ny, nz), "pyro_k_mg_coarse_sym: invalid grid dimensions");
+  PYRO_REQUIRE(b && flags && phi, "pyro_k_mg_coarse_sym: null buffer");
+  PYRO_REQUIRE(iters >= 0, "pyro_k_mg_coarse_sym: iters must be >= 0");
+  PYRO_REQUIRE(bc_mode == 0 || bc_mode == 1, "pyro_k_mg_coarse_sym: bc_mode must be 0 or 1");
+  Dims3 d{(int)nx, (int)ny, (int)nz};
+  PYRO_REQUIRE(mg_coarse_fits(d), "pyro_k_mg_coarse_sym: level too large for one cluster");
+  return ret(launch_mg_coarse_sym(d, h, b, flags, phi, iters, omega, bc_mode, S(stream)),
+             "pyro_k_mg_coarse_sym");
+}
+
 int pyro_voxelize(const PyroShape* shapes, uint32_t n_shapes, uint32_t nx, uint32_t ny,
                   uint32_t nz, float dx, float t0, uint32_t seed, const float* slot_density,
                   const uint32_t* slot_kind, float* sol_out, void* stream) {

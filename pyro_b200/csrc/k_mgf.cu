@@ -298,46 +298,120 @@ __global__ void __launch_bounds__(256) k_mg_prolong_m(L df, const TS* __restrict
   if (ws > 1e-4f) stv(pf + i, ldv(pf + i) + acc / ws);
 }
 
-// One colour pass with the neighbour mask (mg.wgsl:17-36).  A cell's colour
-// is (x + y + z) & 1, so the cells of one colour in a column (x, y) sit at
-// every other z.  Thread (hx, y, zq) updates the four cells
-// z = z0, z0 + 2, z0 + 4, z0 + 6 (z0 = 8 (zq >> 1) + (zq & 1)) at
-// x = 2 hx + ((y + z0 + colour) & 1), carrying the phi above one cell as the
-// phi below the next.  Cells of one colour only read the other colour, so
-// the update is independent of this mapping.
+// One colour pass with the neighbour mask: thread (hx, y, z) updates the
+// cell x = 2 hx + ((y + z + colour) & 1) (mg.wgsl:17-36) reading its own
+// mask and b and the neighbours the mask marks.
 template <typename TS>
 __global__ void __launch_bounds__(256) k_mg_pass(L d, float h2, const TS* __restrict__ b,
                                                  const uint8_t* __restrict__ meta,
                                                  TS* __restrict__ p, int color, float omega,
                                                  int bc_mode) {
-  const int y = blockIdx.y * 4 + threadIdx.y;
-  const int zq = blockIdx.z * 2 + threadIdx.z;
-  const int z0 = (zq >> 1) * 8 + (zq & 1);
-  const int x = (int)(blockIdx.x * 32 + threadIdx.x) * 2 + ((y + z0 + color) & 1);
-  if (x >= d.nx || y >= d.ny || z0 >= d.nz) return;
+  int y = blockIdx.y * 4 + threadIdx.y;
+  int z = blockIdx.z * 2 + threadIdx.z;
+  int x = (int)(blockIdx.x * 32 + threadIdx.x) * 2 + ((y + z + color) & 1);
+  if (x >= d.nx || y >= d.ny || z >= d.nz) return;
+  int i = d.idx(x, y, z);
+  uint32_t m = __ldg(meta + i);
+  if (m & META_SOLID) return;
   const int sy = d.nx, sz = d.nx * d.ny;
-  const int i0 = d.idx(x, y, z0);
-  float below = z0 > 0 ? ldv(p + i0 - sz) : 0.0f;
+  float sum = 0.0f;
+  if (m & 1u) sum += ldv(p + i + 1);
+  if (m & 2u) sum += ldv(p + i - 1);
+  if (m & 4u) sum += ldv(p + i + sy);
+  if (m & 8u) sum += ldv(p + i - sy);
+  if (m & 16u) sum += ldv(p + i + sz);
+  if (m & 32u) sum += ldv(p + i - sz);
+  float cnt = (float)(__popc(m & 63u) + dirichlet_faces(d, x, y, z, bc_mode));
+  if (cnt < 0.5f) return;
+  stv(p + i, wmix(ldv(p + i), (sum - h2 * ldv(b + i)) / cnt, omega));
+}
+
+// The same pass four cells at a time, for rows of a multiple of 4 cells:
+// thread (tx, y, z) loads cells x0..x0+3 (x0 = 4 tx) of phi, b, the masks
+// and the four neighbour rows as vectors, takes phi at x0 - 1 and x0 + 4
+// from the neighbouring lanes, updates the two cells of the pass's colour
+// with the per-cell arithmetic above and stores the four values back (the
+// other colour's two unchanged; nothing else writes them in this pass).
+__device__ __forceinline__ float4 ld4(const float* p) {
+  return *reinterpret_cast<const float4*>(p);
+}
+__device__ __forceinline__ float4 ld4(const __nv_bfloat16* p) {
+  uint2 u = *reinterpret_cast<const uint2*>(p);
+  float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.x));
+  float2 c = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.y));
+  return make_float4(a.x, a.y, c.x, c.y);
+}
+__device__ __forceinline__ void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
+__device__ __forceinline__ void st4(__nv_bfloat16* p, float4 v) {
+  uint2 u;
+  *reinterpret_cast<__nv_bfloat162*>(&u.x) = __floats2bfloat162_rn(v.x, v.y);
+  *reinterpret_cast<__nv_bfloat162*>(&u.y) = __floats2bfloat162_rn(v.z, v.w);
+  *reinterpret_cast<uint2*>(p) = u;
+}
+__device__ __forceinline__ float el(const float4& v, int k) {
+  return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w));
+}
+__device__ __forceinline__ void set_el(float4& v, int k, float a) {
+  if (k == 0) v.x = a;
+  else if (k == 1) v.y = a;
+  else if (k == 2) v.z = a;
+  else v.w = a;
+}
+
+template <typename TS>
+__global__ void __launch_bounds__(256) k_mg_pass4(L d, float h2, const TS* __restrict__ b,
+                                                  const uint8_t* __restrict__ meta,
+                                                  TS* __restrict__ p, int color, float omega,
+                                                  int bc_mode) {
+  // chunk c of 4 cells, x fastest; rows of nx / 4 chunks
+  const int cpr = d.nx >> 2;
+  const int nchunks = cpr * d.ny * d.nz;
+  const int c = blockIdx.x * 256 + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const bool act = c < nchunks;
+  const int cc = act ? c : 0;
+  const int row = cc / cpr;
+  const int x0 = (cc - row * cpr) * 4;
+  const int y = row % d.ny, z = row / d.ny;
+  const int sy = d.nx, sz = d.nx * d.ny;
+  const int i0 = row * d.nx + x0;
+  // every load first
+  const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+  const float4 P0 = act ? ld4(p + i0) : zero;
+  const uint32_t m4 = act ? *reinterpret_cast<const uint32_t*>(meta + i0) : 0x40404040u;
+  const float4 B = act ? ld4(b + i0) : zero;
+  const float4 Yp = (act && y + 1 < d.ny) ? ld4(p + i0 + sy) : zero;
+  const float4 Ym = (act && y > 0) ? ld4(p + i0 - sy) : zero;
+  const float4 Zp = (act && z + 1 < d.nz) ? ld4(p + i0 + sz) : zero;
+  const float4 Zm = (act && z > 0) ? ld4(p + i0 - sz) : zero;
+  // phi at x0 - 1 and x0 + 4: the neighbouring lanes' chunks when they are
+  // in the same row, else a load
+  float left = __shfl_up_sync(0xffffffffu, P0.w, 1);
+  float right = __shfl_down_sync(0xffffffffu, P0.x, 1);
+  if (!act) return;
+  if (x0 > 0 && lane == 0) left = ldv(p + i0 - 1);
+  if (x0 + 4 < d.nx && lane == 31) right = ldv(p + i0 + 4);
+  const int par = (y + z + color) & 1;  // x0 is even: cells x0 + par, x0 + par + 2
+  float4 P = P0;
+  bool any = false;
 #pragma unroll
-  for (int j = 0; j < 4; j++) {
-    const int z = z0 + 2 * j;
-    if (z >= d.nz) break;
-    const int i = i0 + 2 * j * sz;
-    const float above = z + 1 < d.nz ? ldv(p + i + sz) : 0.0f;
-    const uint32_t m = __ldg(meta + i);
-    if (!(m & META_SOLID)) {
-      float sum = 0.0f;
-      if (m & 1u) sum += ldv(p + i + 1);
-      if (m & 2u) sum += ldv(p + i - 1);
-      if (m & 4u) sum += ldv(p + i + sy);
-      if (m & 8u) sum += ldv(p + i - sy);
-      if (m & 16u) sum += above;
-      if (m & 32u) sum += below;
-      const float cnt = (float)(__popc(m & 63u) + dirichlet_faces(d, x, y, z, bc_mode));
-      if (cnt >= 0.5f) stv(p + i, wmix(ldv(p + i), (sum - h2 * ldv(b + i)) / cnt, omega));
-    }
-    below = above;
+  for (int q = 0; q < 2; q++) {
+    const int k = par + 2 * q;
+    const uint32_t m = (m4 >> (8 * k)) & 0xFFu;
+    if (m & META_SOLID) continue;
+    float sum = 0.0f;
+    if (m & 1u) sum += k < 3 ? el(P0, k + 1) : right;
+    if (m & 2u) sum += k > 0 ? el(P0, k - 1) : left;
+    if (m & 4u) sum += el(Yp, k);
+    if (m & 8u) sum += el(Ym, k);
+    if (m & 16u) sum += el(Zp, k);
+    if (m & 32u) sum += el(Zm, k);
+    const float cnt = (float)(__popc(m & 63u) + dirichlet_faces(d, x0 + k, y, z, bc_mode));
+    if (cnt < 0.5f) continue;
+    set_el(P, k, wmix(el(P0, k), (sum - h2 * el(B, k)) / cnt, omega));
+    any = true;
   }
+  if (any) st4(p + i0, P);
 }
 
 // Restriction with the neighbour mask (mg.wgsl:38-83): coarse rhs = mean of
@@ -505,8 +579,14 @@ cudaError_t rb_launch(Dims3 d, float h, const TS* b, const uint8_t* meta, const 
 template <typename TS>
 cudaError_t pass_t(Dims3 d, float h, const TS* b, const uint8_t* meta, TS* p, int color,
                    float omega, int bc_mode, cudaStream_t st) {
-  // z: one block per 8 planes (two threads, one per z parity)
-  dim3 grid(((d.nx + 1) / 2 + 31) / 32, (d.ny + 3) / 4, (d.nz + 7) / 8);
+  if (d.nx % 4 == 0) {
+    const long chunks = (long)(d.nx / 4) * d.ny * d.nz;
+    k_mg_pass4<TS><<<(unsigned)((chunks + 255) / 256), 256, 0, st>>>(L{d.nx, d.ny, d.nz}, h * h, b,
+                                                                      meta, p, color, omega,
+                                                                      bc_mode);
+    return cudaGetLastError();
+  }
+  dim3 grid(((d.nx + 1) / 2 + 31) / 32, (d.ny + 3) / 4, (d.nz + 1) / 2);
   k_mg_pass<TS><<<grid, dim3(32, 4, 2), 0, st>>>(L{d.nx, d.ny, d.nz}, h * h, b, meta, p, color,
                                                 omega, bc_mode);
   return cudaGetLastError();

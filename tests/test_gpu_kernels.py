@@ -202,7 +202,11 @@ def test_mg_kernels(lib, nx, ny, nz, seed, h):
     assert abs(g[10] - r2) <= 1e-4 * r2 and abs(g[11] - b2) <= 1e-4 * b2
 
 
-@pytest.mark.parametrize("nx,ny,nz,seed,h", MG_CASES + [(8, 20, 8, 3, 0.32), (32, 32, 22, 4, 0.2)])
+COARSE_CASES = MG_CASES + [(8, 20, 8, 3, 0.32), (32, 32, 22, 4, 0.2), (20, 40, 20, 5, 0.16),
+                           (16, 30, 16, 6, 0.16), (20, 40, 17, 7, 0.16)]
+
+
+@pytest.mark.parametrize("nx,ny,nz,seed,h", COARSE_CASES)
 def test_mg_coarse_solve_equals_80_sor_sweeps(lib, nx, ny, nz, seed, h):
     rng = np.random.default_rng(seed)
     f = (rng.random((nz, ny, nx)) < 0.1).astype(np.uint32)
@@ -214,4 +218,22 @@ def test_mg_coarse_solve_equals_80_sor_sweeps(lib, nx, ny, nz, seed, h):
             e = oracle.mg_smooth((nx, ny, nz), h, b, f, e, c, 1.6)
     pd, bd, fd = dev(p), dev(b), dev(f)
     assert lib.pyro_k_mg_coarse(nx, ny, nz, h, ptr(bd), ptr(fd), ptr(pd), 80, 1.6, None) == 0
+    assert np.array_equal(host(pd), e)
+
+
+@pytest.mark.parametrize("nx,ny,nz,seed,h", [(20, 40, 20, 8, 0.16), (32, 32, 22, 9, 0.2),
+                                             (8, 20, 8, 10, 0.32)])
+@pytest.mark.parametrize("bc_mode", [0, 1])
+def test_mg_coarse_symmetric_equals_alternating_sweeps(lib, nx, ny, nz, seed, h, bc_mode):
+    rng = np.random.default_rng(seed)
+    f = (rng.random((nz, ny, nx)) < 0.1).astype(np.uint32)
+    b = rng.normal(0, 1, (nz, ny, nx)).astype(np.float32)
+    p = rng.normal(0, 0.1, (nz, ny, nx)).astype(np.float32)
+    e = p
+    for it in range(40):
+        for c in ((0, 1) if it % 2 == 0 else (1, 0)):
+            e = oracle.mg_smooth((nx, ny, nz), h, b, f, e, c, 1.6, bc_mode=bc_mode)
+    pd, bd, fd = dev(p), dev(b), dev(f)
+    assert lib.pyro_k_mg_coarse_sym(nx, ny, nz, h, ptr(bd), ptr(fd), ptr(pd), 40, 1.6, bc_mode,
+                                    None) == 0
     assert np.array_equal(host(pd), e)
