@@ -348,15 +348,6 @@ __device__ __forceinline__ void st4(__nv_bfloat16* p, float4 v) {
   *reinterpret_cast<__nv_bfloat162*>(&u.y) = __floats2bfloat162_rn(v.z, v.w);
   *reinterpret_cast<uint2*>(p) = u;
 }
-__device__ __forceinline__ float el(const float4& v, int k) {
-  return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w));
-}
-__device__ __forceinline__ void set_el(float4& v, int k, float a) {
-  if (k == 0) v.x = a;
-  else if (k == 1) v.y = a;
-  else if (k == 2) v.z = a;
-  else v.w = a;
-}
 
 template <typename TS>
 __global__ void __launch_bounds__(256) k_mg_pass4(L d, float h2, const TS* __restrict__ b,
@@ -391,25 +382,46 @@ __global__ void __launch_bounds__(256) k_mg_pass4(L d, float h2, const TS* __res
   if (!act) return;
   if (x0 > 0 && lane == 0) left = ldv(p + i0 - 1);
   if (x0 + 4 < d.nx && lane == 31) right = ldv(p + i0 + 4);
-  const int par = (y + z + color) & 1;  // x0 is even: cells x0 + par, x0 + par + 2
+  // the two cells of the pass's colour: x0 + par (a) and x0 + par + 2 (b)
+  const bool odd = ((y + z + color) & 1) != 0;
+  const uint32_t ma = (m4 >> (odd ? 8 : 0)) & 0xFFu, mb = (m4 >> (odd ? 24 : 16)) & 0xFFu;
+  if ((ma & META_SOLID) && (mb & META_SOLID)) return;
+  // Dirichlet faces: y and z terms shared, x terms only at the row ends
+  const int dyz = (y == d.ny - 1) + (bc_mode == 0 ? (z == 0) + (z == d.nz - 1) : 0);
+  const int da = dyz + (bc_mode == 0 && !odd && x0 == 0);
+  const int db = dyz + (bc_mode == 0 && odd && x0 + 4 == d.nx);
+  const float own_a = odd ? P0.y : P0.x, own_b = odd ? P0.w : P0.z;
   float4 P = P0;
   bool any = false;
-#pragma unroll
-  for (int q = 0; q < 2; q++) {
-    const int k = par + 2 * q;
-    const uint32_t m = (m4 >> (8 * k)) & 0xFFu;
-    if (m & META_SOLID) continue;
+  if (!(ma & META_SOLID)) {
     float sum = 0.0f;
-    if (m & 1u) sum += k < 3 ? el(P0, k + 1) : right;
-    if (m & 2u) sum += k > 0 ? el(P0, k - 1) : left;
-    if (m & 4u) sum += el(Yp, k);
-    if (m & 8u) sum += el(Ym, k);
-    if (m & 16u) sum += el(Zp, k);
-    if (m & 32u) sum += el(Zm, k);
-    const float cnt = (float)(__popc(m & 63u) + dirichlet_faces(d, x0 + k, y, z, bc_mode));
-    if (cnt < 0.5f) continue;
-    set_el(P, k, wmix(el(P0, k), (sum - h2 * el(B, k)) / cnt, omega));
-    any = true;
+    if (ma & 1u) sum += odd ? P0.z : P0.y;
+    if (ma & 2u) sum += odd ? P0.x : left;
+    if (ma & 4u) sum += odd ? Yp.y : Yp.x;
+    if (ma & 8u) sum += odd ? Ym.y : Ym.x;
+    if (ma & 16u) sum += odd ? Zp.y : Zp.x;
+    if (ma & 32u) sum += odd ? Zm.y : Zm.x;
+    const float cnt = (float)(__popc(ma & 63u) + da);
+    if (cnt >= 0.5f) {
+      const float v = wmix(own_a, (sum - h2 * (odd ? B.y : B.x)) / cnt, omega);
+      if (odd) P.y = v; else P.x = v;
+      any = true;
+    }
+  }
+  if (!(mb & META_SOLID)) {
+    float sum = 0.0f;
+    if (mb & 1u) sum += odd ? right : P0.w;
+    if (mb & 2u) sum += odd ? P0.z : P0.y;
+    if (mb & 4u) sum += odd ? Yp.w : Yp.z;
+    if (mb & 8u) sum += odd ? Ym.w : Ym.z;
+    if (mb & 16u) sum += odd ? Zp.w : Zp.z;
+    if (mb & 32u) sum += odd ? Zm.w : Zm.z;
+    const float cnt = (float)(__popc(mb & 63u) + db);
+    if (cnt >= 0.5f) {
+      const float v = wmix(own_b, (sum - h2 * (odd ? B.w : B.z)) / cnt, omega);
+      if (odd) P.w = v; else P.z = v;
+      any = true;
+    }
   }
   if (any) st4(p + i0, P);
 }
