@@ -233,6 +233,86 @@ def log(msg):
     sys.stderr.flush()
 
 
+def load_traffic():
+    """Per-launch DRAM bytes (read + write) of kernels captured with ncu,
+    from the committed summary profiles/ncu_traffic.json ({} if absent)."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles",
+                        "ncu_traffic.json")
+    try:
+        with open(path) as fh:
+            return json.load(fh)
+    except (OSError, ValueError):
+        return {}
+
+
+def _learned_net():
+    from pyro_b200.learned import Net
+    w = os.path.join(os.path.dirname(os.path.abspath(__file__)), "pyro_b200", "weights",
+                     "warmstart.pnet")
+    return Net.load(w) if os.path.exists(w) else None
+
+
+def solve_runs(ps, bd, runs, net=None):
+    """Each (name, mode, tol, cap) solved twice from phi = 0; the second
+    solve's device time (CUDA events inside the solver) is reported."""
+    import torch
+    from pyro_b200 import _abi
+    res = {}
+    for name, mode, tol, cap in runs:
+        if mode == _abi.SOLVER_MGPCG_LEARNED and net is None:
+            continue
+        best = None
+        for rep in range(2):          # first solve allocates lazily
+            phi = torch.zeros_like(bd)
+            torch.cuda.synchronize()
+            best = ps.solve(bd.data_ptr(), phi.data_ptr(), mode, tol, cap, allow_cap=True)
+        r = {"ms": round(best.ms, 3), "iterations": best.iterations,
+             "rel_resid": best.rel_resid, "converged": bool(best.converged)}
+        if mode == _abi.SOLVER_MGPCG_LEARNED:
+            r.update(learned=best.learned, learned_ms=round(best.learned_ms, 3),
+                     rel_resid_after_learned=best.rel_resid_learned)
+        res[name] = r
+    return res
+
+
+def metric_runs():
+    from pyro_b200 import _abi
+    return [("vcycle_fp32_to_1e-3", _abi.SOLVER_VCYCLE_TOL, 1e-3, 60),
+            ("mgpcg_fp32_to_1e-3", _abi.SOLVER_MGPCG, 1e-3, 200),
+            ("mgpcg_fp32_to_1e-4", _abi.SOLVER_MGPCG, 1e-4, 200),
+            ("mgpcg_bf16_to_1e-4", _abi.SOLVER_MGPCG_BF16, 1e-4, 200),
+            ("mgpcg_bf16_learned_to_1e-4", _abi.SOLVER_MGPCG_LEARNED, 1e-4, 200)]
+
+
+def sim_solver_bench(sim):
+    """The pressure system of the simulation's last substep (its b and
+    flags; reference boundaries), solved from phi = 0 by each solver."""
+    import torch
+    from pyro_b200 import _abi
+    from pyro_b200.poisson import PoissonSolver
+    b = sim.read_field(_abi.F_B)
+    f = sim.read_field(_abi.F_FLAGS)
+    bd = torch.from_numpy(b).cuda()
+    fd = torch.from_numpy(f.astype(np.int32)).cuda()
+    ps = PoissonSolver(tuple(sim.dims), sim.dx, 0)
+    ps.set_flags(fd.data_ptr())
+    net = _learned_net()
+    if net is not None:
+        ps.set_net(net)
+    res = solve_runs(ps, bd, metric_runs(), net)
+    ps.set_net(None)
+    ps.close()
+    v, l = res.get("vcycle_fp32_to_1e-3"), res.get("mgpcg_bf16_learned_to_1e-4")
+    out = {"config": f"the bench's last substep, {sim.dims[0]}x{sim.dims[1]}x{sim.dims[2]}, "
+                     "phi0 = 0", "runs": res}
+    if v and l:
+        out["speedup_learned_1e-4_vs_vcycle_1e-3"] = v["ms"] / l["ms"]
+    b16 = res.get("mgpcg_bf16_to_1e-4")
+    if v and b16:
+        out["speedup_bf16_1e-4_vs_vcycle_1e-3"] = v["ms"] / b16["ms"]
+    return out
+
+
 def solver_bench(n=256, seed=1):
     """The pressure system in isolation: n^3 cells, h = 2 cm, ~5 % solid
     boxes, N(0,1) zero-mean rhs (pyro_b200.poisson.poisson_case).  Device
@@ -244,24 +324,16 @@ def solver_bench(n=256, seed=1):
     fd = torch.from_numpy(f).cuda()
     bd = torch.from_numpy(b).cuda()
     out = {"config": f"poisson {n}^3 h=0.02 solid={float(f.mean()):.3f} seed={seed}"}
-    runs = [("vcycle_fp32_to_1e-3", _abi.SOLVER_VCYCLE_TOL, 1e-3, 60),
-            ("mgpcg_fp32_to_1e-3", _abi.SOLVER_MGPCG, 1e-3, 200),
-            ("mgpcg_fp32_to_1e-4", _abi.SOLVER_MGPCG, 1e-4, 200),
-            ("mgpcg_bf16_to_1e-4", _abi.SOLVER_MGPCG_BF16, 1e-4, 200),
-            ("mgpcg_fp32_to_1e-6", _abi.SOLVER_MGPCG, 1e-6, 200),
-            ("mgpcg_bf16_to_1e-6", _abi.SOLVER_MGPCG_BF16, 1e-6, 200)]
+    runs = metric_runs() + [("mgpcg_fp32_to_1e-6", _abi.SOLVER_MGPCG, 1e-6, 200),
+                            ("mgpcg_bf16_to_1e-6", _abi.SOLVER_MGPCG_BF16, 1e-6, 200)]
+    net = _learned_net()
     for bc in (0, 1):
         ps = PoissonSolver((n, n, n), 0.02, bc)
         ps.set_flags(fd.data_ptr())
-        res = {}
-        for name, mode, tol, cap in runs:
-            best = None
-            for rep in range(2):          # first solve allocates lazily
-                phi = torch.zeros_like(bd)
-                info = ps.solve(bd.data_ptr(), phi.data_ptr(), mode, tol, cap, allow_cap=True)
-                best = info
-            res[name] = {"ms": round(best.ms, 3), "iterations": best.iterations,
-                         "rel_resid": best.rel_resid, "converged": bool(best.converged)}
+        if net is not None:
+            ps.set_net(net)
+        res = solve_runs(ps, bd, runs, net)
+        ps.set_net(None)
         ps.close()
         out["bc_reference" if bc == 0 else "bc_top_dirichlet"] = res
     return out
@@ -363,6 +435,7 @@ def run_ours(args):
     step_bytes = sum(ALG_BYTES.values()) * cells + sc.sim.pressure_cycles * cyc_bytes
     dom_bytes = ALG_BYTES[dom] * cells
     achieved = dom_bytes / (kern[dom] * 1e-3) / 1e9
+    traffic = load_traffic().get(dom, {}).get("dram_bytes_per_launch")
 
     # gather max over ranks
     vals = torch.tensor([ms, ms_e2e], dtype=torch.float64, device="cuda")
@@ -391,7 +464,7 @@ def run_ours(args):
     solver = None
     if rank == 0 and not args.no_solver:
         log("solver bench")
-        solver = solver_bench()
+        solver = {"sim_pressure": sim_solver_bench(sim), "poisson_256": solver_bench()}
     launches_per_step = 10 + sc.sim.pressure_cycles * (10 * (info.levels - 1) + 1)
     line = {
         "metric": METRIC, "value": ms, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -407,7 +480,7 @@ def run_ours(args):
                 "d2h_bytes_per_step": 4 * _abi.STATS_N},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "alg_bytes_per_launch": dom_bytes,
+                     "traffic": traffic, "alg_bytes_per_launch": dom_bytes,
                      "launch_ms": kern[dom]},
         "step_roofline": {"alg_bytes": step_bytes, "achieved_gbs": step_bytes / (ms * 1e-3) / 1e9,
                           "frac": step_bytes / (ms * 1e-3) / 1e9 / peak},
