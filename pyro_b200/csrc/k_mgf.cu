@@ -261,41 +261,104 @@ __global__ void __launch_bounds__(RB_THREADS) k_mg_rb(L d, float h2, const TS* _
   }
 }
 
+// Two cells x0, x0 + 1 of a row (x0 even).  V2: the row length is even, so
+// both exist and the pair is aligned for one vector access; otherwise two
+// scalar accesses, the second only when `two`.
+__device__ __forceinline__ float2 ld2(const float* p) {
+  return *reinterpret_cast<const float2*>(p);
+}
+__device__ __forceinline__ float2 ld2(const __nv_bfloat16* p) {
+  return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(p));
+}
+__device__ __forceinline__ void st2(float* p, float2 v) { *reinterpret_cast<float2*>(p) = v; }
+__device__ __forceinline__ void st2(__nv_bfloat16* p, float2 v) {
+  *reinterpret_cast<__nv_bfloat162*>(p) = __floats2bfloat162_rn(v.x, v.y);
+}
+template <bool V2, typename TS>
+__device__ __forceinline__ float2 ldp(const TS* p, bool two) {
+  if constexpr (V2) return ld2(p);
+  return make_float2(ldv(p), two ? ldv(p + 1) : 0.0f);
+}
+template <bool V2, typename TS>
+__device__ __forceinline__ void stp(TS* p, float2 v, bool two) {
+  if constexpr (V2) {
+    st2(p, v);
+  } else {
+    stv(p, v.x);
+    if (two) stv(p + 1, v.y);
+  }
+}
+
 // Fluid-weighted trilinear prolongation with the coarse solid bit from the
-// coarse meta (mg.wgsl:85-120), in place on the fine level.
-template <typename TS>
+// coarse meta (mg.wgsl:85-120), in place on the fine level.  One thread per
+// coarse cell (X, Y, Z) updates its 2x2x2 fine children.  Per axis, a fine
+// cell 2X + s samples the coarse cells floor((2X + s + 0.5) / 2 - 0.5) + o,
+// o = 0, 1, which is X - 1 + s + o (clamped to the level), with weight
+// 1 - fr = 0.25, fr = 0.75 for s = 0 and 0.75, 0.25 for s = 1: every weight
+// and weight product is exact, so with the corners visited in the
+// reference's order (x fastest) the sums equal the per-fine-cell form bit
+// for bit.  The 27 clamped coarse cells are loaded once.
+template <typename TS, bool V2>
 __global__ void __launch_bounds__(256) k_mg_prolong_m(L df, const TS* __restrict__ pc,
                                                       const uint8_t* __restrict__ mf,
                                                       TS* __restrict__ pf, L dc,
                                                       const uint8_t* __restrict__ mc) {
-  int x = blockIdx.x * 32 + threadIdx.x;
-  int y = blockIdx.y * 4 + threadIdx.y;
-  int z = blockIdx.z * 2 + threadIdx.z;
-  if (!df.inb(x, y, z)) return;
-  int i = df.idx(x, y, z);
-  if (__ldg(mf + i) & META_SOLID) return;
-  float gx = ((float)x + 0.5f) * 0.5f - 0.5f;
-  float gy = ((float)y + 0.5f) * 0.5f - 0.5f;
-  float gz = ((float)z + 0.5f) * 0.5f - 0.5f;
-  int i0x = (int)floorf(gx), i0y = (int)floorf(gy), i0z = (int)floorf(gz);
-  float frx = gx - (float)i0x, fry = gy - (float)i0y, frz = gz - (float)i0z;
-  float acc = 0.0f, ws = 0.0f;
+  const int X = blockIdx.x * 32 + threadIdx.x;
+  const int Y = blockIdx.y * 4 + threadIdx.y;
+  const int Z = blockIdx.z * 2 + threadIdx.z;
+  if (!dc.inb(X, Y, Z)) return;
+  int cx[3], cy[3], cz[3];
 #pragma unroll
-  for (int k = 0; k < 8; k++) {
-    int ox = k & 1, oy = (k >> 1) & 1, oz = (k >> 2) & 1;
-    int cx = min(max(i0x + ox, 0), dc.nx - 1);
-    int cy = min(max(i0y + oy, 0), dc.ny - 1);
-    int cz = min(max(i0z + oz, 0), dc.nz - 1);
-    int j = dc.idx(cx, cy, cz);
-    if (__ldg(mc + j) & META_SOLID) continue;
-    float wx = ox ? frx : 1.0f - frx;
-    float wy = oy ? fry : 1.0f - fry;
-    float wz = oz ? frz : 1.0f - frz;
-    float w = wx * wy * wz;
-    acc += w * ldv(pc + j);
-    ws += w;
+  for (int q = 0; q < 3; q++) {
+    cx[q] = min(max(X - 1 + q, 0), dc.nx - 1);
+    cy[q] = min(max(Y - 1 + q, 0), dc.ny - 1) * dc.nx;
+    cz[q] = min(max(Z - 1 + q, 0), dc.nz - 1) * (dc.nx * dc.ny);
   }
-  if (ws > 1e-4f) stv(pf + i, ldv(pf + i) + acc / ws);
+  float cv[27];
+  uint32_t solid = 0;
+#pragma unroll
+  for (int q = 0; q < 27; q++) {
+    const int j = cx[q % 3] + cy[(q / 3) % 3] + cz[q / 9];
+    const bool s = (__ldg(mc + j) & META_SOLID) != 0;
+    solid |= (uint32_t)s << q;
+    cv[q] = s ? 0.0f : ldv(pc + j);
+  }
+  const int fx = 2 * X;
+  const bool two = fx + 1 < df.nx;
+#pragma unroll
+  for (int sz = 0; sz < 2; sz++) {
+    const int fz = 2 * Z + sz;
+    if (fz >= df.nz) break;
+#pragma unroll
+    for (int sy = 0; sy < 2; sy++) {
+      const int fy = 2 * Y + sy;
+      if (fy >= df.ny) break;
+      const int i = df.idx(fx, fy, fz);
+      const uint32_t m0 = __ldg(mf + i), m1 = two ? __ldg(mf + i + 1) : META_SOLID;
+      if (m0 & m1 & META_SOLID) continue;
+      float2 P = ldp<V2>(pf + i, two);
+#pragma unroll
+      for (int sx = 0; sx < 2; sx++) {
+        if ((sx ? m1 : m0) & META_SOLID) continue;
+        float acc = 0.0f, ws = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          const int ox = k & 1, oy = (k >> 1) & 1, oz = (k >> 2) & 1;
+          const int q = (sx + ox) + 3 * (sy + oy) + 9 * (sz + oz);
+          if ((solid >> q) & 1u) continue;
+          const float w = (sx != ox ? 0.75f : 0.25f) * (sy != oy ? 0.75f : 0.25f) *
+                          (sz != oz ? 0.75f : 0.25f);
+          acc += w * cv[q];
+          ws += w;
+        }
+        if (ws > 1e-4f) {
+          if (sx) P.y = P.y + acc / ws;
+          else P.x = P.x + acc / ws;
+        }
+      }
+      stp<V2>(pf + i, P, two);
+    }
+  }
 }
 
 // One colour pass with the neighbour mask: thread (hx, y, z) updates the
@@ -428,37 +491,72 @@ __global__ void __launch_bounds__(256) k_mg_pass4(L d, float h2, const TS* __res
 
 // Restriction with the neighbour mask (mg.wgsl:38-83): coarse rhs = mean of
 // the fine residuals of the fluid children, coarse guess 0.
-template <typename TS>
+// One thread per coarse cell; the children are visited in the reference's
+// order (x fastest) as two x-pairs per (y, z) row, whose own, b and +-y,
+// +-z neighbour values are loaded as pairs and whose outer x neighbours as
+// scalars.
+template <typename TS, bool V2>
 __global__ void __launch_bounds__(256) k_mg_restrict_m(L df, float h2, const TS* __restrict__ pf,
                                                        const TS* __restrict__ bf,
                                                        const uint8_t* __restrict__ mf, L dc,
                                                        TS* __restrict__ bc, TS* __restrict__ pc,
                                                        int bc_mode) {
-  int x = blockIdx.x * 32 + threadIdx.x;
-  int y = blockIdx.y * 4 + threadIdx.y;
-  int z = blockIdx.z * 2 + threadIdx.z;
-  if (!dc.inb(x, y, z)) return;
+  const int X = blockIdx.x * 32 + threadIdx.x;
+  const int Y = blockIdx.y * 4 + threadIdx.y;
+  const int Z = blockIdx.z * 2 + threadIdx.z;
+  if (!dc.inb(X, Y, Z)) return;
   const int sy = df.nx, sz = df.nx * df.ny;
+  const int fx = 2 * X;
+  const bool two = fx + 1 < df.nx;
+  const bool open = bc_mode == 0;
   float r = 0.0f, nfl = 0.0f;
 #pragma unroll
-  for (int k = 0; k < 8; k++) {
-    int cx = 2 * x + (k & 1), cy = 2 * y + ((k >> 1) & 1), cz = 2 * z + ((k >> 2) & 1);
-    if (!df.inb(cx, cy, cz)) continue;
-    int i = df.idx(cx, cy, cz);
-    uint32_t m = __ldg(mf + i);
-    if (m & META_SOLID) continue;
-    nfl += 1.0f;
-    float sum = 0.0f;
-    if (m & 1u) sum += ldv(pf + i + 1);
-    if (m & 2u) sum += ldv(pf + i - 1);
-    if (m & 4u) sum += ldv(pf + i + sy);
-    if (m & 8u) sum += ldv(pf + i - sy);
-    if (m & 16u) sum += ldv(pf + i + sz);
-    if (m & 32u) sum += ldv(pf + i - sz);
-    float cnt = (float)(__popc(m & 63u) + dirichlet_faces(df, cx, cy, cz, bc_mode));
-    r += ldv(bf + i) - (sum - cnt * ldv(pf + i)) / h2;
+  for (int s_z = 0; s_z < 2; s_z++) {
+    const int fz = 2 * Z + s_z;
+    if (fz >= df.nz) break;
+#pragma unroll
+    for (int s_y = 0; s_y < 2; s_y++) {
+      const int fy = 2 * Y + s_y;
+      if (fy >= df.ny) break;
+      const int i = df.idx(fx, fy, fz);
+      const uint32_t m0 = __ldg(mf + i), m1 = two ? __ldg(mf + i + 1) : META_SOLID;
+      if (m0 & m1 & META_SOLID) continue;
+      const float2 zero = make_float2(0.0f, 0.0f);
+      const float2 P = ldp<V2>(pf + i, two), B = ldp<V2>(bf + i, two);
+      const float2 Yp = fy + 1 < df.ny ? ldp<V2>(pf + i + sy, two) : zero;
+      const float2 Ym = fy > 0 ? ldp<V2>(pf + i - sy, two) : zero;
+      const float2 Zp = fz + 1 < df.nz ? ldp<V2>(pf + i + sz, two) : zero;
+      const float2 Zm = fz > 0 ? ldp<V2>(pf + i - sz, two) : zero;
+      const int dyz = (fy == df.ny - 1) + (open ? (fz == 0) + (fz == df.nz - 1) : 0);
+      if (!(m0 & META_SOLID)) {
+        nfl += 1.0f;
+        float sum = 0.0f;
+        if (m0 & 1u) sum += P.y;
+        if (m0 & 2u) sum += ldv(pf + i - 1);
+        if (m0 & 4u) sum += Yp.x;
+        if (m0 & 8u) sum += Ym.x;
+        if (m0 & 16u) sum += Zp.x;
+        if (m0 & 32u) sum += Zm.x;
+        const int dx = open ? (fx == 0) + (fx == df.nx - 1) : 0;
+        const float cnt = (float)(__popc(m0 & 63u) + dyz + dx);
+        r += B.x - (sum - cnt * P.x) / h2;
+      }
+      if (!(m1 & META_SOLID)) {
+        nfl += 1.0f;
+        float sum = 0.0f;
+        if (m1 & 1u) sum += ldv(pf + i + 2);
+        if (m1 & 2u) sum += P.x;
+        if (m1 & 4u) sum += Yp.y;
+        if (m1 & 8u) sum += Ym.y;
+        if (m1 & 16u) sum += Zp.y;
+        if (m1 & 32u) sum += Zm.y;
+        const int dx = open ? (fx + 1 == df.nx - 1) : 0;
+        const float cnt = (float)(__popc(m1 & 63u) + dyz + dx);
+        r += B.y - (sum - cnt * P.y) / h2;
+      }
+    }
   }
-  int ci = dc.idx(x, y, z);
+  const int ci = dc.idx(X, Y, Z);
   stv(bc + ci, (nfl > 0.0f) ? r / fmaxf(nfl, 1.0f) : 0.0f);
   stv(pc + ci, 0.0f);
 }
@@ -606,9 +704,12 @@ cudaError_t pass_t(Dims3 d, float h, const TS* b, const uint8_t* meta, TS* p, in
 template <typename TS>
 cudaError_t restrict_t(Dims3 df, float h, const TS* pf, const TS* bf, const uint8_t* mf,
                        Dims3 dc, TS* bc, TS* pc, int bc_mode, cudaStream_t st) {
-  k_mg_restrict_m<TS><<<g3(dc), dim3(32, 4, 2), 0, st>>>(L{df.nx, df.ny, df.nz}, h * h, pf, bf,
-                                                        mf, L{dc.nx, dc.ny, dc.nz}, bc, pc,
-                                                        bc_mode);
+  if (df.nx % 2 == 0)
+    k_mg_restrict_m<TS, true><<<g3(dc), dim3(32, 4, 2), 0, st>>>(
+        L{df.nx, df.ny, df.nz}, h * h, pf, bf, mf, L{dc.nx, dc.ny, dc.nz}, bc, pc, bc_mode);
+  else
+    k_mg_restrict_m<TS, false><<<g3(dc), dim3(32, 4, 2), 0, st>>>(
+        L{df.nx, df.ny, df.nz}, h * h, pf, bf, mf, L{dc.nx, dc.ny, dc.nz}, bc, pc, bc_mode);
   return cudaGetLastError();
 }
 
@@ -684,11 +785,21 @@ cudaError_t launch_mg_rb_restrict(Dims3 d, float h, const float* b, const uint8_
   return rb_launch<float, 3, true>(d, h, b, meta, pin, pout, omega, bc_mode, dc, bc, pc, st);
 }
 
+template <typename TS>
+cudaError_t prolong_t(Dims3 df, const TS* pc, const uint8_t* mf, TS* pf, Dims3 dc,
+                      const uint8_t* mc, cudaStream_t st) {
+  if (df.nx % 2 == 0)
+    k_mg_prolong_m<TS, true><<<g3(dc), dim3(32, 4, 2), 0, st>>>(L{df.nx, df.ny, df.nz}, pc, mf,
+                                                                pf, L{dc.nx, dc.ny, dc.nz}, mc);
+  else
+    k_mg_prolong_m<TS, false><<<g3(dc), dim3(32, 4, 2), 0, st>>>(L{df.nx, df.ny, df.nz}, pc, mf,
+                                                                 pf, L{dc.nx, dc.ny, dc.nz}, mc);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_mg_prolong_m(Dims3 df, const float* pc, const uint8_t* mf, float* pf,
                                 Dims3 dc, const uint8_t* mc, cudaStream_t st) {
-  k_mg_prolong_m<float><<<g3(df), dim3(32, 4, 2), 0, st>>>(L{df.nx, df.ny, df.nz}, pc, mf, pf,
-                                                          L{dc.nx, dc.ny, dc.nz}, mc);
-  return cudaGetLastError();
+  return prolong_t<float>(df, pc, mf, pf, dc, mc, st);
 }
 
 cudaError_t launch_mg_rb_bf16(Dims3 d, float h, const void* b, const uint8_t* meta,
@@ -710,9 +821,7 @@ cudaError_t launch_mg_rb_restrict_bf16(Dims3 d, float h, const void* b, const ui
 cudaError_t launch_mg_prolong_m_bf16(Dims3 df, const void* pc, const uint8_t* mf, void* pf,
                                      Dims3 dc, const uint8_t* mc, cudaStream_t st) {
   using T = __nv_bfloat16;
-  k_mg_prolong_m<T><<<g3(df), dim3(32, 4, 2), 0, st>>>(L{df.nx, df.ny, df.nz}, (const T*)pc, mf,
-                                                      (T*)pf, L{dc.nx, dc.ny, dc.nz}, mc);
-  return cudaGetLastError();
+  return prolong_t<T>(df, (const T*)pc, mf, (T*)pf, dc, mc, st);
 }
 
 }  // namespace pyro
