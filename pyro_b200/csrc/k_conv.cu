@@ -341,128 +341,306 @@ cudaError_t gemm_dispatch(int npad, dim3 grid, const Load& ld, const Epi& ep, in
 
 // ------------------------------------------------------------ TMA path
 // Convolution with TMA-staged operands, for input channel counts that are
-// multiples of 16.  A CTA computes a tile of BX x BY output voxels of one
-// z-plane (BX * BY = 128 rows of the MMA).  For every group of 16 input
-// channels it loads, by 5-D TMA boxes with zero fill outside the volume,
+// multiples of 16.  An output tile is BX x BY voxels of one z-plane
+// (BX * BY = 128 rows of the MMA).  For every group of 16 input channels a
+// tile needs, loaded by 5-D TMA boxes with zero fill outside the volume,
 // three copies of the input patch shifted by dx = -1, 0, +1, each
 // BX x (BY + 2) x 3 voxels (y and z with their halo) as two 8-channel
-// chunks, plus the weight slice w_tap[27][N][16 channels].  Output row
+// chunks, and the weight slice w_tap[27][N][16 channels].  Output row
 // r = x + BX y of tap (dx, dy, dz) then reads patch row
 // r + BX (dy + 1) + BX (BY + 2) (dz + 1) of copy dx, so each of the 27 taps
 // is one MMA whose A descriptor starts at that row: no gather, and every
 // input element is fetched three times per tile instead of 27.
+//
+// The kernel is persistent and warp-specialised.  CTA c takes tiles c,
+// c + grid, c + 2 grid, ...; warp 0 streams the (tile, channel group)
+// operand stages through a ring of S shared-memory stages, warp 1 issues
+// the MMAs into one of two TMEM accumulators, and warps 2-5 drain the other
+// accumulator (the epilogue) while the next tile accumulates.  When the
+// whole weight tensor fits beside two stages it is loaded once and stays
+// resident.  Every wait is bounded; a wait that runs out stops the CTA's
+// roles (shared abort flag), sets *err, lets the copies in flight land and
+// frees the TMEM.
 struct TmaGeom {
   int nx, ny, nz, nb;
-  int BX, BY, tiles_x, tiles_y;
-  int groups, stages;
-  uint32_t box_a, box_b, stage_a, stage_bytes;
+  int BX, BY, tiles_x, tiles_y, ntiles;
+  int groups, stages, resident_b;
+  uint32_t box_a, box_b, stage_a, stage_bytes, b_bytes;
 };
 
+constexpr int CONV_THREADS = 192;
+constexpr int CONV_MAX_STAGES = 8;
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(umma::smem_u32(mbar))
+               : "memory");
+}
+
 template <int N, class Epi>
-__global__ void __launch_bounds__(GEMM_THREADS) k_conv_tma(const __grid_constant__ CUtensorMap ta,
-                                                           const __grid_constant__ CUtensorMap tb,
-                                                           TmaGeom g, Epi ep, int* err) {
+__global__ void __launch_bounds__(CONV_THREADS, 1)
+    k_conv_tma(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb,
+               TmaGeom g, Epi ep, int* err) {
   constexpr int NCOLS = N <= 32 ? 32 : (N <= 64 ? 64 : 128);
   constexpr uint32_t IDESC = umma::idesc_bf16(128, N);
   extern __shared__ uint8_t dsm[];
-  __shared__ __align__(8) uint64_t full[2], empty[2], done;
+  __shared__ __align__(8) uint64_t full[CONV_MAX_STAGES], empty[CONV_MAX_STAGES], accf[2],
+      acce[2], bfull, done;
   __shared__ uint32_t tslot;
+  __shared__ volatile int abort_flag;
   uint8_t* base = dsm + ((1024u - (umma::smem_u32(dsm) & 1023u)) & 1023u);
-  int t = blockIdx.x;
-  const int tx = t % g.tiles_x;
-  t /= g.tiles_x;
-  const int ty = t % g.tiles_y;
-  t /= g.tiles_y;
-  const int z = t % g.nz, b = t / g.nz;
-  const int x0 = tx * g.BX, y0 = ty * g.BY;
+  uint8_t* sb_res = base + (size_t)g.stages * g.stage_bytes;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int S = g.stages, G = g.groups;
   if (threadIdx.x == 0) {
-    for (int s = 0; s < 2; s++) {
+    for (int s = 0; s < S; s++) {
       umma::mbar_init(&full[s], 1);
       umma::mbar_init(&empty[s], 1);
     }
+    for (int a = 0; a < 2; a++) {
+      umma::mbar_init(&accf[a], 1);
+      umma::mbar_init(&acce[a], 4);
+    }
+    umma::mbar_init(&bfull, 1);
     umma::mbar_init(&done, 1);
+    abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 0) {
-    umma::tmem_alloc(&tslot, NCOLS);
+  if (warp == 1) {
+    umma::tmem_alloc(&tslot, 2 * NCOLS);
     umma::tmem_relinquish();
   }
   umma::fence_before();
   __syncthreads();
   umma::fence_after();
   const uint32_t tbase = tslot;
-  bool ok = true;
-  if (threadIdx.x == 0) {
-    auto issue = [&](int grp, int s) {
-      uint8_t* sa = base + (size_t)s * g.stage_bytes;
-      uint8_t* sb = sa + g.stage_a;
-      umma::mbar_expect_tx(&full[s], g.stage_a + 2 * g.box_b);
-      for (int d = 0; d < 3; d++)
-        for (int j = 0; j < 2; j++)
-          umma::tma_load_5d(sa + (d * 2 + j) * g.box_a, &ta, grp * 16 + j * 8, x0 + d - 1, y0 - 1,
-                            z - 1, b, &full[s]);
-      for (int j = 0; j < 2; j++)
-        umma::tma_load_3d(sb + j * g.box_b, &tb, grp * 16 + j * 8, 0, 0, &full[s]);
-    };
-    const int S = g.stages, G = g.groups;
-    int issued = 0, consumed = 0;
-    for (; issued < S && issued < G; issued++) issue(issued, issued);
-    for (int grp = 0; grp < G && ok; grp++) {
-      const int s = grp % S;
-      if (!umma::mbar_wait_bounded(&full[s], (grp / S) & 1)) {
-        ok = false;
-        break;
+  const int my_tiles =
+      (int)blockIdx.x < g.ntiles ? (g.ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  bool timed_out = false;
+  if (warp == 0) {
+    if (lane == 0) {
+      // ---- producer
+      if (g.resident_b && my_tiles > 0) {
+        umma::mbar_expect_tx(&bfull, g.b_bytes);
+        for (int grp = 0; grp < G; grp++)
+          for (int j = 0; j < 2; j++)
+            umma::tma_load_3d(sb_res + (size_t)(grp * 2 + j) * g.box_b, &tb, grp * 16 + j * 8, 0,
+                              0, &bfull);
       }
-      consumed++;
-      umma::fence_after();
-      uint8_t* sa = base + (size_t)s * g.stage_bytes;
-      uint8_t* sb = sa + g.stage_a;
-#pragma unroll 1
-      for (int tap = 0; tap < 27; tap++) {
-        const int dx = tap % 3, dy = (tap / 3) % 3, dz = tap / 9;
-        const uint32_t row = (uint32_t)(dy * g.BX + dz * g.BX * (g.BY + 2));
-        const uint64_t da = umma::smem_desc_lbo(sa + dx * 2 * g.box_a + row * 16, g.box_a);
-        const uint64_t db = umma::smem_desc_lbo(sb + tap * N * 16, g.box_b);
-        umma::mma_bf16(tbase, da, db, IDESC, (grp > 0 || tap > 0) ? 1u : 0u);
+      const int items = my_tiles * G;
+      int issued = 0;
+      for (int i = 0; i < items; i++) {
+        if (abort_flag) break;
+        const int s = i % S;
+        if (i >= S && !umma::mbar_wait_bounded(&empty[s], ((i / S) - 1) & 1)) {
+          timed_out = true;
+          break;
+        }
+        const int jt = i / G, grp = i - jt * G;
+        int t = (int)blockIdx.x + jt * (int)gridDim.x;
+        const int tx = t % g.tiles_x;
+        t /= g.tiles_x;
+        const int ty = t % g.tiles_y;
+        t /= g.tiles_y;
+        const int z = t % g.nz, b = t / g.nz;
+        uint8_t* sa = base + (size_t)s * g.stage_bytes;
+        umma::mbar_expect_tx(&full[s], g.stage_a + (g.resident_b ? 0u : 2u * g.box_b));
+        for (int d = 0; d < 3; d++)
+          for (int j = 0; j < 2; j++)
+            umma::tma_load_5d(sa + (d * 2 + j) * g.box_a, &ta, grp * 16 + j * 8,
+                              tx * g.BX + d - 1, ty * g.BY - 1, z - 1, b, &full[s]);
+        if (!g.resident_b)
+          for (int j = 0; j < 2; j++)
+            umma::tma_load_3d(sa + g.stage_a + j * g.box_b, &tb, grp * 16 + j * 8, 0, 0,
+                              &full[s]);
+        issued = i + 1;
       }
-      umma::mma_commit(&empty[s]);
-      if (issued < G) {
-        // the stage is refilled once the MMAs reading it are done
-        if (!umma::mbar_wait_bounded(&empty[s], (grp / S) & 1)) {
+      if (timed_out) abort_flag = 1;
+      // every issued copy lands before the CTA may exit
+      for (int q = issued > S ? issued - S : 0; q < issued; q++)
+        if (!umma::mbar_wait_bounded(&full[q % S], (q / S) & 1)) timed_out = true;
+      if (g.resident_b && my_tiles > 0 && !umma::mbar_wait_bounded(&bfull, 0)) timed_out = true;
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // ---- MMA issuer
+      bool ok = true;
+      if (g.resident_b && my_tiles > 0 && !umma::mbar_wait_bounded(&bfull, 0)) ok = false;
+      const int items = my_tiles * G;
+      for (int i = 0; i < items && ok; i++) {
+        if (abort_flag) break;
+        const int s = i % S;
+        const int jt = i / G, grp = i - jt * G;
+        const int a = jt & 1;
+        if (grp == 0 && jt >= 2 && !umma::mbar_wait_bounded(&acce[a], ((jt >> 1) - 1) & 1)) {
           ok = false;
           break;
         }
-        issue(issued, s);
-        issued++;
+        if (!umma::mbar_wait_bounded(&full[s], (i / S) & 1)) {
+          ok = false;
+          break;
+        }
+        umma::fence_after();
+        uint8_t* sa = base + (size_t)s * g.stage_bytes;
+        const uint8_t* sb = g.resident_b ? sb_res + (size_t)grp * 2 * g.box_b : sa + g.stage_a;
+        const uint32_t dt = tbase + (uint32_t)(a * NCOLS);
+#pragma unroll 1
+        for (int tap = 0; tap < 27; tap++) {
+          const int dx = tap % 3, dy = (tap / 3) % 3, dz = tap / 9;
+          const uint32_t row = (uint32_t)(dy * g.BX + dz * g.BX * (g.BY + 2));
+          const uint64_t da = umma::smem_desc_lbo(sa + dx * 2 * g.box_a + row * 16, g.box_a);
+          const uint64_t db = umma::smem_desc_lbo(sb + tap * N * 16, g.box_b);
+          umma::mma_bf16(dt, da, db, IDESC, (grp > 0 || tap > 0) ? 1u : 0u);
+        }
+        umma::mma_commit(&empty[s]);
+        if (grp == G - 1) umma::mma_commit(&accf[a]);
+      }
+      if (!ok) {
+        timed_out = true;
+        abort_flag = 1;
+      }
+      // every MMA issued has finished before the TMEM is freed
+      umma::mma_commit(&done);
+      if (!umma::mbar_wait_bounded(&done, 0)) timed_out = true;
+    }
+    __syncwarp();
+  } else {
+    // ---- epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31
+    const int lb = (warp & 3) * 32;
+    const int r = lb + lane;
+    for (int jt = 0; jt < my_tiles; jt++) {
+      const int a = jt & 1;
+      const bool okw = umma::mbar_wait_bounded(&accf[a], (jt >> 1) & 1);
+      if (!__all_sync(0xffffffffu, okw)) {
+        timed_out = true;
+        abort_flag = 1;
+        break;
+      }
+      if (__any_sync(0xffffffffu, abort_flag != 0)) break;
+      umma::fence_after();
+      float v[N];
+#pragma unroll
+      for (int col = 0; col < N; col += 16) {
+        float c[16];
+        umma::tmem_ld16(tbase + (uint32_t)(a * NCOLS) + ((uint32_t)lb << 16) + (uint32_t)col, c);
+#pragma unroll
+        for (int j = 0; j < 16; j++) v[col + j] = c[j];
+      }
+      umma::fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acce[a]);
+      int t = (int)blockIdx.x + jt * (int)gridDim.x;
+      const int tx = t % g.tiles_x;
+      t /= g.tiles_x;
+      const int ty = t % g.tiles_y;
+      t /= g.tiles_y;
+      const int z = t % g.nz, b = t / g.nz;
+      const int x = tx * g.BX + r % g.BX, y = ty * g.BY + r / g.BX;
+      const int vox = (x < g.nx && y < g.ny) ? ((b * g.nz + z) * g.ny + y) * g.nx + x : -1;
+#pragma unroll
+      for (int col = 0; col < N; col += 16) {
+        float c[16];
+#pragma unroll
+        for (int j = 0; j < 16; j++) c[j] = v[col + j];
+        ep(vox, col, c);
       }
     }
-    umma::mma_commit(&done);
-    if (!ok) {
-      // let the copies still in flight land before the CTA exits
-      for (int q = consumed; q < issued; q++)
-        umma::mbar_wait_bounded(&full[q % S], (q / S) & 1);
-    }
   }
-  __syncwarp();
-  if (!umma::mbar_wait_bounded(&done, 0)) ok = false;
-  umma::fence_after();
-  const bool all_ok = __syncthreads_and(ok) != 0;
-  if (all_ok) {
-    const int r = warp * 32 + lane;
-    const int x = x0 + r % g.BX, y = y0 + r / g.BX;
-    const int v = (x < g.nx && y < g.ny) ? ((b * g.nz + z) * g.ny + y) * g.nx + x : -1;
-#pragma unroll
-    for (int col = 0; col < N; col += 16) {
-      float vals[16];
-      umma::tmem_ld16(tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)col, vals);
-      ep(v, col, vals);
-    }
-  }
-  if (!all_ok && threadIdx.x == 0) atomicExch(err, 1);
+  if (timed_out) atomicExch(err, 1);
   umma::fence_before();
   __syncthreads();
-  if (warp == 0) umma::tmem_dealloc(tbase, NCOLS);
+  if (warp == 1) umma::tmem_dealloc(tbase, 2 * NCOLS);
+}
+
+// --------------------------------------------------------- direct (CUDA cores)
+// Layers too narrow for the tensor cores to pay: 2 -> 16 channels (the
+// network's input layer, K = 54) and 16 -> 1 (its output layer, N = 1).
+// One thread per output voxel, the weights in shared memory as FP32
+// [tap][ci][co], FP32 accumulation with fused multiply-adds over the taps in
+// order (dz, dy, dx), taps outside the volume skipped (zero padding).
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(256) k_conv_direct(const bf16* __restrict__ x, Vol g,
+                                                     const bf16* __restrict__ w,
+                                                     const float* __restrict__ bias, int relu,
+                                                     bf16* __restrict__ y_bf16,
+                                                     float* __restrict__ y_f32) {
+  static_assert(CIN == 2 || CIN % 8 == 0, "input rows are loaded as 4- or 16-byte chunks");
+  __shared__ float ws[27 * CIN * COUT];
+  for (int i = threadIdx.x; i < 27 * CIN * COUT; i += blockDim.x) {
+    const int co = i / (27 * CIN), t = (i / CIN) % 27, ci = i % CIN;  // w[co][t][ci]
+    ws[(t * CIN + ci) * COUT + co] = __bfloat162float(w[i]);
+  }
+  __syncthreads();
+  const long V = (long)g.nx * g.ny * g.nz * g.nb;
+  const long v = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= V) return;
+  const int xx = (int)(v % g.nx);
+  long q = v / g.nx;
+  const int yy = (int)(q % g.ny);
+  q /= g.ny;
+  const int zz = (int)(q % g.nz);
+  float acc[COUT];
+#pragma unroll
+  for (int co = 0; co < COUT; co++) acc[co] = bias ? bias[co] : 0.0f;
+  const long sy = g.nx, sz = (long)g.nx * g.ny;
+#pragma unroll
+  for (int dz = -1; dz <= 1; dz++) {
+    if ((unsigned)(zz + dz) >= (unsigned)g.nz) continue;
+#pragma unroll
+    for (int dy = -1; dy <= 1; dy++) {
+      if ((unsigned)(yy + dy) >= (unsigned)g.ny) continue;
+#pragma unroll
+      for (int dx = -1; dx <= 1; dx++) {
+        if ((unsigned)(xx + dx) >= (unsigned)g.nx) continue;
+        const int t = (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
+        const long vs = v + dx + sy * dy + sz * dz;
+        float xin[CIN];
+        if constexpr (CIN == 2) {
+          const float2 f = __bfloat1622float2(
+              *reinterpret_cast<const __nv_bfloat162*>(x + vs * 2));
+          xin[0] = f.x;
+          xin[1] = f.y;
+        } else {
+#pragma unroll
+          for (int c8 = 0; c8 < CIN; c8 += 8) {
+            const uint4 u = __ldg(reinterpret_cast<const uint4*>(x + vs * CIN + c8));
+            const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+              const float2 f = __bfloat1622float2(h[j]);
+              xin[c8 + 2 * j] = f.x;
+              xin[c8 + 2 * j + 1] = f.y;
+            }
+          }
+        }
+        const float* wt = ws + t * CIN * COUT;
+#pragma unroll
+        for (int ci = 0; ci < CIN; ci++)
+#pragma unroll
+          for (int co = 0; co < COUT; co++)
+            acc[co] = __fmaf_rn(xin[ci], wt[ci * COUT + co], acc[co]);
+      }
+    }
+  }
+  if (relu) {
+#pragma unroll
+    for (int co = 0; co < COUT; co++) acc[co] = fmaxf(acc[co], 0.0f);
+  }
+  if (y_f32) {
+#pragma unroll
+    for (int co = 0; co < COUT; co++) y_f32[v * COUT + co] = acc[co];
+  } else if constexpr (COUT % 8 == 0) {
+#pragma unroll
+    for (int c8 = 0; c8 < COUT; c8 += 8) {
+      uint4 o;
+      __nv_bfloat162* ob = reinterpret_cast<__nv_bfloat162*>(&o);
+#pragma unroll
+      for (int j = 0; j < 4; j++) ob[j] = __floats2bfloat162_rn(acc[c8 + 2 * j], acc[c8 + 2 * j + 1]);
+      *reinterpret_cast<uint4*>(y_bf16 + v * COUT + c8) = o;
+    }
+  } else {
+#pragma unroll
+    for (int co = 0; co < COUT; co++) y_bf16[v * COUT + co] = __float2bfloat16_rn(acc[co]);
+  }
 }
 
 __global__ void k_wprep(const bf16* __restrict__ w, int Cout, int Cin, int backward,
@@ -500,12 +678,19 @@ int pick_bx(int nx) {
 template <int N, class Epi>
 cudaError_t tma_launch(const CUtensorMap& ta, const CUtensorMap& tb, const TmaGeom& g,
                        const Epi& ep, int* err, cudaStream_t st) {
-  const size_t smem = (size_t)g.stages * g.stage_bytes + 1024;
+  const size_t smem = (size_t)g.stages * g.stage_bytes + (g.resident_b ? g.b_bytes : 0) + 1024;
   cudaError_t e = cudaFuncSetAttribute(k_conv_tma<N, Epi>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  const unsigned grid = (unsigned)((size_t)g.tiles_x * g.tiles_y * g.nz * g.nb);
-  k_conv_tma<N, Epi><<<grid, GEMM_THREADS, smem, st>>>(ta, tb, g, ep, err);
+  int dev = 0, nsm = 148, occ = 1;
+  if (cudaGetDevice(&dev) == cudaSuccess)
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_conv_tma<N, Epi>, CONV_THREADS,
+                                                    smem) != cudaSuccess ||
+      occ < 1)
+    occ = 1;
+  const unsigned grid = (unsigned)std::min<long>((long)g.ntiles, (long)nsm * occ);
+  k_conv_tma<N, Epi><<<grid, CONV_THREADS, smem, st>>>(ta, tb, g, ep, err);
   return cudaGetLastError();
 }
 
@@ -562,6 +747,25 @@ cudaError_t conv3_backward_weight(const bf16* x, int Cin, const bf16* dy, int Co
 }
 
 
+// Direct convolution for the shapes k_conv_direct covers (2 -> 16 and
+// 16 -> 1 channels); cudaErrorInvalidValue for others.
+bool conv3_direct_fits(int C, int Cout) { return (C == 2 && Cout == 16) || (C == 16 && Cout == 1); }
+
+cudaError_t conv3_direct(const bf16* x, int C, int nx, int ny, int nz, int nb, const bf16* w,
+                         int Cout, const float* bias, int relu, bf16* y_bf16, float* y_f32,
+                         cudaStream_t st) {
+  Vol g{nx, ny, nz, nb};
+  const long V = (long)nx * ny * nz * nb;
+  const unsigned blocks = (unsigned)((V + 255) / 256);
+  if (C == 2 && Cout == 16)
+    k_conv_direct<2, 16><<<blocks, 256, 0, st>>>(x, g, w, bias, relu, y_bf16, y_f32);
+  else if (C == 16 && Cout == 1)
+    k_conv_direct<16, 1><<<blocks, 256, 0, st>>>(x, g, w, bias, relu, y_bf16, y_f32);
+  else
+    return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
 // Weight layouts for conv3_tma: forward w_tap[t][co][ci] = w[co][t][ci];
 // backward (data) w_tap[t][ci][co] = w[co][26 - t][ci] (flipped taps,
 // transposed channels).
@@ -592,12 +796,19 @@ cudaError_t conv3_tma(const bf16* x, int K, int nx, int ny, int nz, int nb, cons
   g.tiles_y = (ny + g.BY - 1) / g.BY;
   g.groups = K / 16;
   const int npad = pad16(N);
+  g.ntiles = g.tiles_x * g.tiles_y * nz * nb;
   g.box_a = (uint32_t)(g.BX * (g.BY + 2) * 3 * 16);
   g.box_b = (uint32_t)(27 * npad * 16);
   g.stage_a = 6 * g.box_a;
-  g.stage_bytes = (g.stage_a + 2 * g.box_b + 1023u) & ~1023u;
-  g.stages = (g.groups >= 2 && 2 * g.stage_bytes + 1024 <= 220 * 1024) ? 2 : 1;
-  if (g.stage_bytes + 1024 > 220 * 1024) return cudaErrorInvalidValue;
+  g.b_bytes = (uint32_t)g.groups * 2u * g.box_b;
+  // shared-memory budget for the stages (+ resident weights) and alignment
+  const uint32_t budget = 220u * 1024u - 1024u;
+  const uint32_t sa_al = (g.stage_a + 1023u) & ~1023u;
+  g.resident_b = (g.b_bytes + 2 * sa_al <= budget) ? 1 : 0;
+  g.stage_bytes = g.resident_b ? sa_al : ((g.stage_a + 2 * g.box_b + 1023u) & ~1023u);
+  const uint32_t room = budget - (g.resident_b ? g.b_bytes : 0u);
+  g.stages = (int)std::min<uint32_t>(CONV_MAX_STAGES, room / g.stage_bytes);
+  if (g.stages < 1) return cudaErrorInvalidValue;
   CUtensorMap ta, tb;
   const cuuint64_t adim[5] = {(cuuint64_t)K, (cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz,
                               (cuuint64_t)nb};
@@ -668,6 +879,11 @@ int pyro_conv3_forward(const void* x, int C, int nx, int ny, int nz, int nb, con
   if (rc != PYRO_OK) return rc;
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   cudaError_t e;
+  if (conv3_direct_fits(C, Cout)) {  // narrow layers on the CUDA cores
+    e = conv3_direct((const bf16*)x, C, nx, ny, nz, nb, (const bf16*)w, Cout, bias, relu,
+                     y_f32 ? nullptr : (bf16*)y, y_f32 ? (float*)y : nullptr, st);
+    return finish(e, err, st, "pyro_conv3_forward");
+  }
   if (C % 16 == 0) {  // TMA-staged kernel on tap-major weights
     DevBuf wt;
     if ((rc = wt.alloc((size_t)Cout * 27 * C * 2)) != PYRO_OK) return rc;

@@ -495,6 +495,9 @@ int PyroNet::forward(const float* b, const uint32_t* flags, NetVol v, cudaStream
   NET_CU(cudaGetLastError());
   auto conv = [&](const DevBuf& x, int l, NetVol g, DevBuf* y, float* yf) -> cudaError_t {
     const NetLayer& L = NET_SPEC[l];
+    if (conv3_direct_fits(L.cin, L.cout))
+      return conv3_direct(x.as<bf16>(), L.cin, g.nx, g.ny, g.nz, g.nb, w(l), L.cout, bias(l),
+                          L.relu, y ? y->as<bf16>() : nullptr, yf, st);
     if (L.cin % 16 == 0)
       return conv3_tma(x.as<bf16>(), L.cin, g.nx, g.ny, g.nz, g.nb, wf(l), L.cout, bias(l),
                        L.relu, nullptr, y ? y->as<bf16>() : nullptr, yf, E, st);

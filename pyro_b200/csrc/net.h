@@ -37,6 +37,12 @@ cudaError_t conv3_backward_weight(const __nv_bfloat16* x, int Cin, const __nv_bf
                                   int Cout, int nx, int ny, int nz, int nb, float* dw, int* err,
                                   cudaStream_t st);
 
+// Direct convolution on the CUDA cores for 2 -> 16 and 16 -> 1 channels.
+bool conv3_direct_fits(int C, int Cout);
+cudaError_t conv3_direct(const __nv_bfloat16* x, int C, int nx, int ny, int nz, int nb,
+                         const __nv_bfloat16* w, int Cout, const float* bias, int relu,
+                         __nv_bfloat16* y_bf16, float* y_f32, cudaStream_t st);
+
 // TMA-staged convolution (input channels K a multiple of 16) on tap-major
 // weights prepared by conv3_prep_weights.
 cudaError_t conv3_prep_weights(const __nv_bfloat16* w, int Cout, int Cin, int backward,

@@ -47,7 +47,12 @@ def _wk(w):   # (Cout, C, 3, 3, 3) -> [Cout][27][C] bf16
                                             (96, 32, (6, 8, 8), 1), (16, 1, (8, 8, 8), 2),
                                             (32, 64, (8, 16, 8), 1), (48, 16, (4, 8, 8), 1),
                                             (32, 16, (5, 9, 13), 2), (16, 96, (6, 6, 40), 1),
-                                            (64, 128, (4, 8, 8), 1)])
+                                            (64, 128, (4, 8, 8), 1),
+                                            # many tiles per CTA: every stage and both
+                                            # accumulators of the persistent kernel cycle
+                                            (48, 16, (40, 64, 64), 1), (16, 16, (24, 40, 48), 2),
+                                            (32, 64, (16, 32, 32), 1), (2, 16, (33, 35, 37), 1),
+                                            (16, 1, (33, 35, 37), 1)])
 def test_forward(lib, C, Cout, dims, nb):
     nz, ny, nx = dims
     x, w, b = _tensors(nb, C, nz, ny, nx, Cout, 1)
@@ -62,7 +67,8 @@ def test_forward(lib, C, Cout, dims, nb):
 
 @pytest.mark.parametrize("Cin,Cout,dims", [(16, 32, (8, 10, 12)), (48, 16, (6, 8, 8)),
                                            (96, 32, (4, 8, 8)), (32, 64, (8, 8, 8)),
-                                           (16, 8, (5, 7, 9)), (64, 16, (3, 17, 20))])
+                                           (16, 8, (5, 7, 9)), (64, 16, (3, 17, 20)),
+                                           (48, 16, (20, 32, 32))])
 def test_backward_data_and_weight(lib, Cin, Cout, dims):
     nz, ny, nx = dims
     nb = 1
