@@ -325,8 +325,10 @@ int pyro_k_mg_coarse_sym(uint32_t nx, uint32_t ny, uint32_t nz, float h,
 
 /* ---- learned warm start: tcgen05 convolutions --------------------------- */
 /* 3x3x3 convolution, padding 1, stride 1, as an implicit GEMM on the
- * tensor cores (BF16 operands, FP32 accumulation in TMEM).  Activations are
- * channel-last BF16 [nb][nz][ny][nx][C]; weights BF16 [Cout][27][Cin] with
+ * tensor cores (BF16 operands, FP32 accumulation in TMEM).  BF16 activations
+ * of C channels over V = nb*nz*ny*nx voxels (x fastest) are stored as C/8
+ * planes of [V][8 channels] when C is a multiple of 8, else as [V][C]; FP32
+ * outputs (y_f32, dx_f32) as [V][C].  Weights BF16 [Cout][27][Cin] with
  * tap = (dz+1)*9 + (dy+1)*3 + (dx+1).  Channels 1..128.  Blocking; returns
  * PYRO_E_TIMEOUT if a bounded tensor-core wait ran out.  No counterpart in
  * the reference (its pressure solve has no learned stage). */

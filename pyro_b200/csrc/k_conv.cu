@@ -12,7 +12,8 @@
 //   backward (weight) A[m = (tap, ci)][k = voxel] = x[voxel + tap][ci]
 //                    B[n = co][k = voxel]        = dy[voxel][co]   (split over K)
 //
-// Activations are channel-last BF16, [volume][z][y][x][channel]; a tap
+// Activations are BF16 in planes of 8 channels, [C / 8][volume][z][y][x][8]
+// (C a multiple of 8; [volume][z][y][x][C] otherwise); a tap
 // outside its volume reads zero.  One thread issues the MMA, tcgen05.commit
 // signals an mbarrier per stage, and every wait is bounded: a wait that runs
 // out sets *err and the CTA still frees its TMEM.
@@ -54,6 +55,12 @@ __device__ __forceinline__ int shifted(const Vol& g, int v, int dx, int dy, int 
     return -1;
   return ((b * g.nz + z) * g.ny + y) * g.nx + x;
 }
+// Activation layout: C a multiple of 8 -> C / 8 planes of [V][8 channels];
+// otherwise [V][C].  Element offset of channel c of voxel v:
+__device__ __forceinline__ size_t act_off(size_t v, int c, int C, size_t V) {
+  return (C & 7) ? v * C + c : ((size_t)(c >> 3) * V + v) * 8 + (c & 7);
+}
+
 __device__ __forceinline__ void tap_offset(int t, int& dx, int& dy, int& dz) {
   dx = t % 3 - 1;
   dy = (t / 3) % 3 - 1;
@@ -155,9 +162,9 @@ struct ConvLoad {
         if (v < V) {
           int vs = shifted(g, v, dx, dy, dz);
           if (vs >= 0) {
-            const uint4* p = reinterpret_cast<const uint4*>(x + (size_t)vs * C + cc * 16);
+            const uint4* p = reinterpret_cast<const uint4*>(x + act_off(vs, cc * 16, C, V));
             a0 = __ldg(p);
-            a1 = __ldg(p + 1);
+            a1 = __ldg(p + V);  // the next 8-channel plane
           }
         }
         st16(sA, umma::core_offset(r, 0, 128), a0);
@@ -172,7 +179,7 @@ struct ConvLoad {
             tap_offset(t, dx, dy, dz);
             if (flip) { dx = -dx; dy = -dy; dz = -dz; }
             int vs = shifted(g, v, dx, dy, dz);
-            if (vs >= 0) val = x[(size_t)vs * C + ci];
+            if (vs >= 0) val = x[act_off(vs, ci, C, V)];
           }
           st_bf(sA, umma::core_offset(r, e, 128), val);
         }
@@ -221,7 +228,7 @@ struct WgradLoad {
         bf16 val = __float2bfloat16(0.0f);
         if (m < M && v < V) {
           int vs = shifted(g, v, dx, dy_, dz);
-          if (vs >= 0) val = x[(size_t)vs * Cin + ci];
+          if (vs >= 0) val = x[act_off(vs, ci, Cin, V)];
         }
         st_bf(sA, umma::core_offset(r, e, 128), val);
       }
@@ -231,7 +238,7 @@ struct WgradLoad {
       for (int e = 0; e < 16; e++) {
         int v = ks * 16 + e;
         bf16 val = __float2bfloat16(0.0f);
-        if (n < Cout && v < V) val = dy[(size_t)v * Cout + n];
+        if (n < Cout && v < V) val = dy[act_off(v, n, Cout, V)];
         st_bf(sB, umma::core_offset(n, e, npad), val);
       }
     }
@@ -271,8 +278,8 @@ struct ConvEpi {
         for (int j = 0; j < 16; j++) a[j] = fmaxf(a[j], 0.0f);
       }
       if (mask) {
-        const uint4* mp = reinterpret_cast<const uint4*>(mask + (size_t)m * Nout + col);
-        uint4 mk[2] = {__ldg(mp), __ldg(mp + 1)};
+        const uint4* mp = reinterpret_cast<const uint4*>(mask + act_off(m, col, Nout, V));
+        uint4 mk[2] = {__ldg(mp), __ldg(mp + V)};
         const bf16* mb = reinterpret_cast<const bf16*>(mk);
 #pragma unroll
         for (int j = 0; j < 16; j++)
@@ -282,9 +289,9 @@ struct ConvEpi {
       __nv_bfloat162* ob = reinterpret_cast<__nv_bfloat162*>(o);
 #pragma unroll
       for (int j = 0; j < 8; j++) ob[j] = __floats2bfloat162_rn(a[2 * j], a[2 * j + 1]);
-      uint4* op = reinterpret_cast<uint4*>(out_bf16 + (size_t)m * Nout + col);
+      uint4* op = reinterpret_cast<uint4*>(out_bf16 + act_off(m, col, Nout, V));
       op[0] = o[0];
-      op[1] = o[1];
+      op[V] = o[1];  // the next 8-channel plane
       return;
     }
 #pragma unroll
@@ -294,9 +301,9 @@ struct ConvEpi {
       float a = v[j];
       if (bias) a += bias[n];
       if (relu) a = fmaxf(a, 0.0f);
-      if (mask && !(__bfloat162float(mask[(size_t)m * Nout + n]) > 0.0f)) a = 0.0f;
+      if (mask && !(__bfloat162float(mask[act_off(m, n, Nout, V)]) > 0.0f)) a = 0.0f;
       if (out_f32) out_f32[(size_t)m * Nout + n] = a;
-      else out_bf16[(size_t)m * Nout + n] = __float2bfloat16(a);
+      else out_bf16[act_off(m, n, Nout, V)] = __float2bfloat16(a);
     }
   }
 };
@@ -446,8 +453,8 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
         umma::mbar_expect_tx(&full[s], g.stage_a + (g.resident_b ? 0u : 2u * g.box_b));
         for (int d = 0; d < 3; d++)
           for (int j = 0; j < 2; j++)
-            umma::tma_load_5d(sa + (d * 2 + j) * g.box_a, &ta, grp * 16 + j * 8,
-                              tx * g.BX + d - 1, ty * g.BY - 1, z - 1, b, &full[s]);
+            umma::tma_load_4d(sa + (d * 2 + j) * g.box_a, &ta, (tx * g.BX + d - 1) * 8,
+                              ty * g.BY - 1, z - 1, (grp * 2 + j) * g.nb + b, &full[s]);
         if (!g.resident_b)
           for (int j = 0; j < 2; j++)
             umma::tma_load_3d(sa + g.stage_a + j * g.box_b, &tb, grp * 16 + j * 8, 0, 0,
@@ -602,7 +609,7 @@ __global__ void __launch_bounds__(256) k_conv_direct(const bf16* __restrict__ x,
         } else {
 #pragma unroll
           for (int c8 = 0; c8 < CIN; c8 += 8) {
-            const uint4 u = __ldg(reinterpret_cast<const uint4*>(x + vs * CIN + c8));
+            const uint4 u = __ldg(reinterpret_cast<const uint4*>(x + act_off(vs, c8, CIN, V)));
             const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
 #pragma unroll
             for (int j = 0; j < 4; j++) {
@@ -635,11 +642,11 @@ __global__ void __launch_bounds__(256) k_conv_direct(const bf16* __restrict__ x,
       __nv_bfloat162* ob = reinterpret_cast<__nv_bfloat162*>(&o);
 #pragma unroll
       for (int j = 0; j < 4; j++) ob[j] = __floats2bfloat162_rn(acc[c8 + 2 * j], acc[c8 + 2 * j + 1]);
-      *reinterpret_cast<uint4*>(y_bf16 + v * COUT + c8) = o;
+      *reinterpret_cast<uint4*>(y_bf16 + act_off(v, c8, COUT, V)) = o;
     }
   } else {
 #pragma unroll
-    for (int co = 0; co < COUT; co++) y_bf16[v * COUT + co] = __float2bfloat16_rn(acc[co]);
+    for (int co = 0; co < COUT; co++) y_bf16[act_off(v, co, COUT, V)] = __float2bfloat16_rn(acc[co]);
   }
 }
 
@@ -669,8 +676,9 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
+// Tile width in x: a TMA box row is 8 BX channels-elements, at most 256.
 int pick_bx(int nx) {
-  for (int c : {16, 8, 32, 64, 128})
+  for (int c : {16, 8, 32})
     if (nx % c == 0) return c;
   return nx < 16 ? 8 : 16;
 }
@@ -810,13 +818,15 @@ cudaError_t conv3_tma(const bf16* x, int K, int nx, int ny, int nz, int nb, cons
   g.stages = (int)std::min<uint32_t>(CONV_MAX_STAGES, room / g.stage_bytes);
   if (g.stages < 1) return cudaErrorInvalidValue;
   CUtensorMap ta, tb;
-  const cuuint64_t adim[5] = {(cuuint64_t)K, (cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz,
-                              (cuuint64_t)nb};
-  const cuuint64_t astr[4] = {(cuuint64_t)K * 2, (cuuint64_t)K * 2 * nx,
-                              (cuuint64_t)K * 2 * nx * ny, (cuuint64_t)K * 2 * nx * ny * nz};
-  const cuuint32_t abox[5] = {8, (cuuint32_t)g.BX, (cuuint32_t)(g.BY + 2), 3, 1};
+  // input planes of 8 channels: dims (8 nx, ny, nz, nb K / 8), x and the
+  // channel chunk innermost, so a box row is BX voxels x 16 bytes
+  const cuuint64_t adim[4] = {(cuuint64_t)nx * 8, (cuuint64_t)ny, (cuuint64_t)nz,
+                              (cuuint64_t)nb * (K / 8)};
+  const cuuint64_t astr[3] = {(cuuint64_t)nx * 16, (cuuint64_t)nx * 16 * ny,
+                              (cuuint64_t)nx * 16 * ny * nz};
+  const cuuint32_t abox[4] = {(cuuint32_t)(8 * g.BX), (cuuint32_t)(g.BY + 2), 3, 1};
   const cuuint32_t es[5] = {1, 1, 1, 1, 1};
-  if (enc(&ta, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<bf16*>(x), adim, astr, abox, es,
+  if (enc(&ta, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16*>(x), adim, astr, abox, es,
           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return cudaErrorInvalidValue;

@@ -69,6 +69,15 @@ struct Dv {  // volume dims on the device
 };
 inline Dv dv(NetVol v) { return Dv{v.nx, v.ny, v.nz, v.nb}; }
 
+// Activation layout: a tensor of C channels over V voxels with C a multiple
+// of 8 is stored as C / 8 planes of [V][8 channels] (a plane is one 16-byte
+// chunk per voxel, so a TMA box along x reads long contiguous rows); other
+// channel counts (the 2-channel input, 1-channel gradients) as [V][C].
+// Element offset of channel c of voxel v:
+__device__ __forceinline__ size_t act_off(size_t v, int c, int C, size_t V) {
+  return (C & 7) ? v * C + c : ((size_t)(c >> 3) * V + v) * 8 + (c & 7);
+}
+
 inline unsigned blocks_for(size_t n) {
   size_t b = (n + NT - 1) / NT;
   return (unsigned)std::min<size_t>(std::max<size_t>(b, 1), 148 * 32);
@@ -132,8 +141,8 @@ __global__ void __launch_bounds__(NT) k_pool(const bf16* __restrict__ in, int C,
   Dv cd{(fd.nx + 1) / 2, (fd.ny + 1) / 2, (fd.nz + 1) / 2, fd.nb};
   const int ch = C / 8;
   GRID_LOOP(i, cd.voxels() * ch) {
-    size_t cv = i / ch;
-    int c8 = (int)(i % ch);
+    const size_t cv = i % cd.voxels();
+    const int c8 = (int)(i / cd.voxels());
     int x, y, z, b;
     cd.coords(cv, x, y, z, b);
     float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -144,7 +153,9 @@ __global__ void __launch_bounds__(NT) k_pool(const bf16* __restrict__ in, int C,
           int fx = 2 * x + dx, fy = 2 * y + dy, fz = 2 * z + dz;
           if (fx >= fd.nx || fy >= fd.ny || fz >= fd.nz) continue;
           float t[8];
-          unpack8(*reinterpret_cast<const uint4*>(in + fd.idx(fx, fy, fz, b) * C + c8 * 8), t);
+          unpack8(*reinterpret_cast<const uint4*>(in + act_off(fd.idx(fx, fy, fz, b), c8 * 8, C,
+                                                               fd.voxels())),
+                  t);
 #pragma unroll
           for (int j = 0; j < 8; j++) acc[j] += t[j];
           cnt++;
@@ -152,7 +163,7 @@ __global__ void __launch_bounds__(NT) k_pool(const bf16* __restrict__ in, int C,
     float inv = 1.0f / (float)cnt;
 #pragma unroll
     for (int j = 0; j < 8; j++) acc[j] *= inv;
-    *reinterpret_cast<uint4*>(out + cv * C + c8 * 8) = pack8(acc);
+    *reinterpret_cast<uint4*>(out + act_off(cv, c8 * 8, C, cd.voxels())) = pack8(acc);
   }
 }
 
@@ -163,17 +174,18 @@ __global__ void __launch_bounds__(NT) k_upcat(const bf16* __restrict__ a, int Ca
   Dv cd{(fd.nx + 1) / 2, (fd.ny + 1) / 2, (fd.nz + 1) / 2, fd.nb};
   const int Ct = Ca + Cb, ch = Ct / 8;
   GRID_LOOP(i, fd.voxels() * ch) {
-    size_t fv = i / ch;
-    int c = (int)(i % ch) * 8;
+    const size_t fv = i % fd.voxels();
+    const int c = (int)(i / fd.voxels()) * 8;
     uint4 u;
     if (c < Ca) {
       int x, y, z, b;
       fd.coords(fv, x, y, z, b);
-      u = *reinterpret_cast<const uint4*>(a + cd.idx(x >> 1, y >> 1, z >> 1, b) * Ca + c);
+      u = *reinterpret_cast<const uint4*>(
+          a + act_off(cd.idx(x >> 1, y >> 1, z >> 1, b), c, Ca, cd.voxels()));
     } else {
-      u = *reinterpret_cast<const uint4*>(skip + fv * Cb + (c - Ca));
+      u = *reinterpret_cast<const uint4*>(skip + act_off(fv, c - Ca, Cb, fd.voxels()));
     }
-    *reinterpret_cast<uint4*>(out + fv * Ct + c) = u;
+    *reinterpret_cast<uint4*>(out + act_off(fv, c, Ct, fd.voxels())) = u;
   }
 }
 
@@ -183,8 +195,8 @@ __global__ void __launch_bounds__(NT) k_upback(const bf16* __restrict__ dc, int 
   Dv cd{(fd.nx + 1) / 2, (fd.ny + 1) / 2, (fd.nz + 1) / 2, fd.nb};
   const int ch = Ca / 8;
   GRID_LOOP(i, cd.voxels() * ch) {
-    size_t cv = i / ch;
-    int c = (int)(i % ch) * 8;
+    const size_t cv = i % cd.voxels();
+    const int c = (int)(i / cd.voxels()) * 8;
     int x, y, z, b;
     cd.coords(cv, x, y, z, b);
     float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -194,11 +206,13 @@ __global__ void __launch_bounds__(NT) k_upback(const bf16* __restrict__ dc, int 
           int fx = 2 * x + dx, fy = 2 * y + dy, fz = 2 * z + dz;
           if (fx >= fd.nx || fy >= fd.ny || fz >= fd.nz) continue;
           float t[8];
-          unpack8(*reinterpret_cast<const uint4*>(dc + fd.idx(fx, fy, fz, b) * Ct + c), t);
+          unpack8(*reinterpret_cast<const uint4*>(
+                      dc + act_off(fd.idx(fx, fy, fz, b), c, Ct, fd.voxels())),
+                  t);
 #pragma unroll
           for (int j = 0; j < 8; j++) acc[j] += t[j];
         }
-    *reinterpret_cast<uint4*>(out + cv * Ca + c) = pack8(acc);
+    *reinterpret_cast<uint4*>(out + act_off(cv, c, Ca, cd.voxels())) = pack8(acc);
   }
 }
 
@@ -212,24 +226,28 @@ __global__ void __launch_bounds__(NT) k_poolback(const bf16* __restrict__ dp, in
   Dv cd{(fd.nx + 1) / 2, (fd.ny + 1) / 2, (fd.nz + 1) / 2, fd.nb};
   const int ch = C / 8;
   GRID_LOOP(i, fd.voxels() * ch) {
-    size_t fv = i / ch;
-    int c = (int)(i % ch) * 8;
+    const size_t fv = i % fd.voxels();
+    const int c = (int)(i / fd.voxels()) * 8;
     int x, y, z, b;
     fd.coords(fv, x, y, z, b);
     int px = x >> 1, py = y >> 1, pz = z >> 1;
     int cnt = (2 * px + 1 < fd.nx ? 2 : 1) * (2 * py + 1 < fd.ny ? 2 : 1) *
               (2 * pz + 1 < fd.nz ? 2 : 1);
     float g[8], s[8], a[8];
-    unpack8(*reinterpret_cast<const uint4*>(dp + cd.idx(px, py, pz, b) * C + c), g);
-    unpack8(*reinterpret_cast<const uint4*>(act + fv * C + c), a);
-    if (skip) unpack8(*reinterpret_cast<const uint4*>(skip + fv * sstride + soff + c), s);
+    const size_t Vf = fd.voxels();
+    unpack8(*reinterpret_cast<const uint4*>(dp + act_off(cd.idx(px, py, pz, b), c, C,
+                                                         cd.voxels())),
+            g);
+    unpack8(*reinterpret_cast<const uint4*>(act + act_off(fv, c, C, Vf)), a);
+    if (skip)
+      unpack8(*reinterpret_cast<const uint4*>(skip + act_off(fv, soff + c, sstride, Vf)), s);
     float inv = 1.0f / (float)cnt;
 #pragma unroll
     for (int j = 0; j < 8; j++) {
       float v = g[j] * inv + (skip ? s[j] : 0.0f);
       g[j] = a[j] > 0.0f ? v : 0.0f;
     }
-    *reinterpret_cast<uint4*>(dz + fv * C + c) = pack8(g);
+    *reinterpret_cast<uint4*>(dz + act_off(fv, c, C, Vf)) = pack8(g);
   }
 }
 
@@ -240,7 +258,7 @@ __global__ void __launch_bounds__(NT) k_bias_grad(const bf16* __restrict__ dz, s
   const int c = threadIdx.x % C, lane = threadIdx.x / C, lanes = NT / C;
   float acc = 0.0f;
   for (size_t v = (size_t)blockIdx.x * lanes + lane; v < V; v += (size_t)gridDim.x * lanes)
-    acc += __bfloat162float(dz[v * C + c]);
+    acc += __bfloat162float(dz[act_off(v, c, C, V)]);
   sh[threadIdx.x] = acc;
   __syncthreads();
   if ((int)threadIdx.x < C) {

@@ -16,8 +16,9 @@
 // s is the root mean square of b over the fluid cells of each volume, so
 // the map is linear in the scale of b, as the Poisson solution is.  Pooling
 // halves with ceil (a coarse cell averages its children inside the volume);
-// up2 copies a coarse cell to its children.  Activations are channel-last,
-// [volume][z][y][x][channel].
+// up2 copies a coarse cell to its children.  Activations of C channels are
+// stored as C / 8 planes of [volume][z][y][x][8 channels] (C a multiple of
+// 8), the 2-channel input as [volume][z][y][x][2].
 #pragma once
 
 #include <cuda_bf16.h>

@@ -1,7 +1,8 @@
 """tcgen05 implicit-GEMM convolutions against a plain PyTorch FP32 reference
 (torch.nn.functional.conv3d on the same BF16-rounded inputs).  Input
-channel counts that are multiples of 16 take the TMA-staged kernel, the
-others the gathering one; both are covered.  Products of
+channel counts that are multiples of 16 take the TMA-staged kernel, 2 -> 16
+and 16 -> 1 the direct CUDA-core kernel, the others the gathering one; all
+are covered.  Products of
 BF16 values are exact in FP32, so the only differences are FP32 summation
 order: 1e-3 relative of each output's magnitude."""
 import numpy as np
@@ -35,8 +36,13 @@ def _tensors(nb, C, nz, ny, nx, Cout, seed):
     return x.cuda(), w.cuda(), b.cuda()
 
 
-def _cl(x):   # (nb, C, z, y, x) -> channel-last bf16 contiguous
-    return x.permute(0, 2, 3, 4, 1).contiguous().bfloat16()
+def _cl(x):
+    """(nb, C, z, y, x) -> the library's BF16 activation layout: C / 8 planes
+    of [voxel][8 channels] when C is a multiple of 8, else [voxel][C]."""
+    nb, C = x.shape[:2]
+    if C % 8:
+        return x.permute(0, 2, 3, 4, 1).contiguous().bfloat16()
+    return x.reshape(nb, C // 8, 8, *x.shape[2:]).permute(1, 0, 3, 4, 5, 2).contiguous().bfloat16()
 
 
 def _wk(w):   # (Cout, C, 3, 3, 3) -> [Cout][27][C] bf16
