@@ -561,9 +561,12 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
 // --------------------------------------------------------- direct (CUDA cores)
 // Layers too narrow for the tensor cores to pay: 2 -> 16 channels (the
 // network's input layer, K = 54) and 16 -> 1 (its output layer, N = 1).
-// One thread per output voxel, the weights in shared memory as FP32
-// [tap][ci][co], FP32 accumulation with fused multiply-adds over the taps in
-// order (dz, dy, dx), taps outside the volume skipped (zero padding).
+// A thread computes DV consecutive voxels of an x-row, so every weight read
+// from shared memory (FP32, [tap][ci][co]) feeds DV fused multiply-adds.
+// FP32 accumulation over the taps in order (dz, dy, dx); a tap outside the
+// volume reads zero (zero padding).
+constexpr int DIRECT_DV = 4;
+
 template <int CIN, int COUT>
 __global__ void __launch_bounds__(256) k_conv_direct(const bf16* __restrict__ x, Vol g,
                                                      const bf16* __restrict__ w,
@@ -571,51 +574,61 @@ __global__ void __launch_bounds__(256) k_conv_direct(const bf16* __restrict__ x,
                                                      bf16* __restrict__ y_bf16,
                                                      float* __restrict__ y_f32) {
   static_assert(CIN == 2 || CIN % 8 == 0, "input rows are loaded as 4- or 16-byte chunks");
-  __shared__ float ws[27 * CIN * COUT];
+  constexpr int DV = DIRECT_DV;
+  __shared__ __align__(16) float ws[27 * CIN * COUT];
   for (int i = threadIdx.x; i < 27 * CIN * COUT; i += blockDim.x) {
     const int co = i / (27 * CIN), t = (i / CIN) % 27, ci = i % CIN;  // w[co][t][ci]
     ws[(t * CIN + ci) * COUT + co] = __bfloat162float(w[i]);
   }
   __syncthreads();
   const long V = (long)g.nx * g.ny * g.nz * g.nb;
-  const long v = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= V) return;
-  const int xx = (int)(v % g.nx);
-  long q = v / g.nx;
-  const int yy = (int)(q % g.ny);
-  q /= g.ny;
-  const int zz = (int)(q % g.nz);
-  float acc[COUT];
+  const int cpr = (g.nx + DV - 1) / DV;  // chunks per x-row
+  const long nchunks = (long)cpr * g.ny * g.nz * g.nb;
+  const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nchunks) return;
+  const long row = c / cpr;  // (b, z, y) row index
+  const int x0 = (int)(c - row * cpr) * DV;
+  const int yy = (int)(row % g.ny);
+  const int zz = (int)((row / g.ny) % g.nz);
+  const long v0 = row * g.nx + x0;
+  float acc[DV][COUT];
 #pragma unroll
-  for (int co = 0; co < COUT; co++) acc[co] = bias ? bias[co] : 0.0f;
+  for (int i = 0; i < DV; i++)
+#pragma unroll
+    for (int co = 0; co < COUT; co++) acc[i][co] = bias ? bias[co] : 0.0f;
   const long sy = g.nx, sz = (long)g.nx * g.ny;
-#pragma unroll
+#pragma unroll 1
   for (int dz = -1; dz <= 1; dz++) {
     if ((unsigned)(zz + dz) >= (unsigned)g.nz) continue;
-#pragma unroll
+#pragma unroll 1
     for (int dy = -1; dy <= 1; dy++) {
       if ((unsigned)(yy + dy) >= (unsigned)g.ny) continue;
 #pragma unroll
       for (int dx = -1; dx <= 1; dx++) {
-        if ((unsigned)(xx + dx) >= (unsigned)g.nx) continue;
         const int t = (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
-        const long vs = v + dx + sy * dy + sz * dz;
-        float xin[CIN];
-        if constexpr (CIN == 2) {
-          const float2 f = __bfloat1622float2(
-              *reinterpret_cast<const __nv_bfloat162*>(x + vs * 2));
-          xin[0] = f.x;
-          xin[1] = f.y;
-        } else {
+        float xin[DV][CIN];
 #pragma unroll
-          for (int c8 = 0; c8 < CIN; c8 += 8) {
-            const uint4 u = __ldg(reinterpret_cast<const uint4*>(x + act_off(vs, c8, CIN, V)));
-            const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
+        for (int i = 0; i < DV; i++) {
+          const int xs = x0 + i + dx;
+          const bool in = (unsigned)xs < (unsigned)g.nx;
+          const long vs = v0 + i + dx + sy * dy + sz * dz;
+          if constexpr (CIN == 2) {
+            float2 f = make_float2(0.0f, 0.0f);
+            if (in) f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(x + vs * 2));
+            xin[i][0] = f.x;
+            xin[i][1] = f.y;
+          } else {
 #pragma unroll
-            for (int j = 0; j < 4; j++) {
-              const float2 f = __bfloat1622float2(h[j]);
-              xin[c8 + 2 * j] = f.x;
-              xin[c8 + 2 * j + 1] = f.y;
+            for (int c8 = 0; c8 < CIN; c8 += 8) {
+              uint4 u = make_uint4(0, 0, 0, 0);
+              if (in) u = __ldg(reinterpret_cast<const uint4*>(x + act_off(vs, c8, CIN, V)));
+              const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+              for (int j = 0; j < 4; j++) {
+                const float2 f = __bfloat1622float2(h[j]);
+                xin[i][c8 + 2 * j] = f.x;
+                xin[i][c8 + 2 * j + 1] = f.y;
+              }
             }
           }
         }
@@ -623,30 +636,40 @@ __global__ void __launch_bounds__(256) k_conv_direct(const bf16* __restrict__ x,
 #pragma unroll
         for (int ci = 0; ci < CIN; ci++)
 #pragma unroll
-          for (int co = 0; co < COUT; co++)
-            acc[co] = __fmaf_rn(xin[ci], wt[ci * COUT + co], acc[co]);
+          for (int co = 0; co < COUT; co++) {
+            const float wv = wt[ci * COUT + co];
+#pragma unroll
+            for (int i = 0; i < DV; i++) acc[i][co] = __fmaf_rn(xin[i][ci], wv, acc[i][co]);
+          }
       }
     }
   }
-  if (relu) {
 #pragma unroll
-    for (int co = 0; co < COUT; co++) acc[co] = fmaxf(acc[co], 0.0f);
-  }
-  if (y_f32) {
+  for (int i = 0; i < DV; i++) {
+    if (x0 + i >= g.nx) break;
+    const long v = v0 + i;
+    if (relu) {
 #pragma unroll
-    for (int co = 0; co < COUT; co++) y_f32[v * COUT + co] = acc[co];
-  } else if constexpr (COUT % 8 == 0) {
-#pragma unroll
-    for (int c8 = 0; c8 < COUT; c8 += 8) {
-      uint4 o;
-      __nv_bfloat162* ob = reinterpret_cast<__nv_bfloat162*>(&o);
-#pragma unroll
-      for (int j = 0; j < 4; j++) ob[j] = __floats2bfloat162_rn(acc[c8 + 2 * j], acc[c8 + 2 * j + 1]);
-      *reinterpret_cast<uint4*>(y_bf16 + act_off(v, c8, COUT, V)) = o;
+      for (int co = 0; co < COUT; co++) acc[i][co] = fmaxf(acc[i][co], 0.0f);
     }
-  } else {
+    if (y_f32) {
 #pragma unroll
-    for (int co = 0; co < COUT; co++) y_bf16[act_off(v, co, COUT, V)] = __float2bfloat16_rn(acc[co]);
+      for (int co = 0; co < COUT; co++) y_f32[v * COUT + co] = acc[i][co];
+    } else if constexpr (COUT % 8 == 0) {
+#pragma unroll
+      for (int c8 = 0; c8 < COUT; c8 += 8) {
+        uint4 o;
+        __nv_bfloat162* ob = reinterpret_cast<__nv_bfloat162*>(&o);
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+          ob[j] = __floats2bfloat162_rn(acc[i][c8 + 2 * j], acc[i][c8 + 2 * j + 1]);
+        *reinterpret_cast<uint4*>(y_bf16 + act_off(v, c8, COUT, V)) = o;
+      }
+    } else {
+#pragma unroll
+      for (int co = 0; co < COUT; co++)
+        y_bf16[act_off(v, co, COUT, V)] = __float2bfloat16_rn(acc[i][co]);
+    }
   }
 }
 
@@ -763,8 +786,8 @@ cudaError_t conv3_direct(const bf16* x, int C, int nx, int ny, int nz, int nb, c
                          int Cout, const float* bias, int relu, bf16* y_bf16, float* y_f32,
                          cudaStream_t st) {
   Vol g{nx, ny, nz, nb};
-  const long V = (long)nx * ny * nz * nb;
-  const unsigned blocks = (unsigned)((V + 255) / 256);
+  const long chunks = (long)((nx + DIRECT_DV - 1) / DIRECT_DV) * ny * nz * nb;
+  const unsigned blocks = (unsigned)((chunks + 255) / 256);
   if (C == 2 && Cout == 16)
     k_conv_direct<2, 16><<<blocks, 256, 0, st>>>(x, g, w, bias, relu, y_bf16, y_f32);
   else if (C == 16 && Cout == 1)
