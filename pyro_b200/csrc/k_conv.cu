@@ -348,54 +348,84 @@ cudaError_t gemm_dispatch(int npad, dim3 grid, const Load& ld, const Epi& ep, in
 
 // ------------------------------------------------------------ TMA path
 // Convolution with TMA-staged operands, for input channel counts that are
-// multiples of 16.  An output tile is BX x BY voxels of one z-plane
-// (BX * BY = 128 rows of the MMA).  For every group of 16 input channels a
-// tile needs, loaded by 5-D TMA boxes with zero fill outside the volume,
-// three copies of the input patch shifted by dx = -1, 0, +1, each
-// BX x (BY + 2) x 3 voxels (y and z with their halo) as two 8-channel
-// chunks, and the weight slice w_tap[27][N][16 channels].  Output row
-// r = x + BX y of tap (dx, dy, dz) then reads patch row
+// multiples of 16, computed transposed: D[co][voxel] = W[co][k] X[voxel][k]^T
+// with the output channels as the MMA's M (128 rows; rows past the channel
+// count are computed and never stored) and NT = 256 (or 128) voxels of a
+// tile as its N.  A tcgen05.mma of K = 16 costs the same issue time for any
+// N up to 256, so a wide voxel tile does the work of several narrow ones.
+//
+// A tile is BX x BY voxels of one z-plane (BX * BY = NT).  For every group
+// of 16 input channels a tile needs, loaded by 4-D TMA boxes with zero fill
+// outside the volume, three copies of the input patch shifted by
+// dx = -1, 0, +1, each BX x (BY + 2) x 3 voxels (y and z with their halo) as
+// two 8-channel chunks, and the weight slice w_tap[27][npad][16 channels].
+// Voxel row r = x + BX y of tap (dx, dy, dz) then reads patch row
 // r + BX (dy + 1) + BX (BY + 2) (dz + 1) of copy dx, so each of the 27 taps
-// is one MMA whose A descriptor starts at that row: no gather, and every
-// input element is fetched three times per tile instead of 27.
+// is one MMA whose B descriptor starts at that row: no gather, and every
+// input element is fetched three times per tile instead of 27.  The A
+// descriptor of tap t starts at weight row t * npad and reads 128 rows; the
+// rows past npad belong to the next taps (or to a slack area) and only feed
+// the D rows that are never stored.
 //
 // The kernel is persistent and warp-specialised.  CTA c takes tiles c,
 // c + grid, c + 2 grid, ...; warp 0 streams the (tile, channel group)
 // operand stages through a ring of S shared-memory stages, warp 1 issues
 // the MMAs into one of two TMEM accumulators, and warps 2-5 drain the other
-// accumulator (the epilogue) while the next tile accumulates.  When the
-// whole weight tensor fits beside two stages it is loaded once and stays
-// resident.  Every wait is bounded; a wait that runs out stops the CTA's
-// roles (shared abort flag), sets *err, lets the copies in flight land and
-// frees the TMEM.
+// accumulator (the epilogue; warp w reads TMEM lanes 32 (w % 4) ..,
+// i.e. output channels 32 (w % 4) ..) while the next tile accumulates.  When
+// the whole weight tensor fits beside two stages it is loaded once and
+// stays resident.  Every wait is bounded; a wait that runs out stops the
+// CTA's roles (shared abort flag), sets *err, lets the copies in flight land
+// and frees the TMEM.
 struct TmaGeom {
   int nx, ny, nz, nb;
   int BX, BY, tiles_x, tiles_y, ntiles;
-  int groups, stages, resident_b;
-  uint32_t box_a, box_b, stage_a, stage_bytes, b_bytes;
+  int groups, stages, resident_b, npad;
+  uint32_t box_a, box_b, stage_a, stage_bytes, b_bytes, stage_off;
 };
 
 constexpr int CONV_THREADS = 192;
 constexpr int CONV_MAX_STAGES = 8;
+// bytes the 128-row weight operand of the last tap reads past its rows
+constexpr uint32_t CONV_SLACK = 2048;
+// epilogue transpose buffer: 32 voxels x (128 + 8) BF16 channels
+constexpr uint32_t CONV_EPI_BYTES = 32u * 136u * 2u;
+
+// Named barrier 1 over the 128 epilogue threads; the _or form also returns
+// whether any of them passed true.
+__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+__device__ __forceinline__ bool epi_bar_or(bool p) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred pi, po;\n\t"
+      "setp.ne.u32 pi, %1, 0;\n\t"
+      "barrier.red.or.pred po, 1, 128, pi;\n\t"
+      "selp.u32 %0, 1, 0, po;\n\t}"
+      : "=r"(r)
+      : "r"((uint32_t)p)
+      : "memory");
+  return r != 0;
+}
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* mbar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(umma::smem_u32(mbar))
                : "memory");
 }
 
-template <int N, class Epi>
+template <int NT, int LOG2BX>
 __global__ void __launch_bounds__(CONV_THREADS, 1)
     k_conv_tma(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb,
-               TmaGeom g, Epi ep, int* err) {
-  constexpr int NCOLS = N <= 32 ? 32 : (N <= 64 ? 64 : 128);
-  constexpr uint32_t IDESC = umma::idesc_bf16(128, N);
+               TmaGeom g, ConvEpi ep, int* err) {
+  constexpr uint32_t IDESC = umma::idesc_bf16(128, NT);
+  constexpr int BX = 1 << LOG2BX;
   extern __shared__ uint8_t dsm[];
   __shared__ __align__(8) uint64_t full[CONV_MAX_STAGES], empty[CONV_MAX_STAGES], accf[2],
       acce[2], bfull, done;
   __shared__ uint32_t tslot;
   __shared__ volatile int abort_flag;
   uint8_t* base = dsm + ((1024u - (umma::smem_u32(dsm) & 1023u)) & 1023u);
-  uint8_t* sb_res = base + (size_t)g.stages * g.stage_bytes;
+  uint8_t* sb_res = base;
+  uint8_t* stages = base + g.stage_off;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int S = g.stages, G = g.groups;
   if (threadIdx.x == 0) {
@@ -413,7 +443,7 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) {
-    umma::tmem_alloc(&tslot, 2 * NCOLS);
+    umma::tmem_alloc(&tslot, 2 * NT);
     umma::tmem_relinquish();
   }
   umma::fence_before();
@@ -449,7 +479,7 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
         const int ty = t % g.tiles_y;
         t /= g.tiles_y;
         const int z = t % g.nz, b = t / g.nz;
-        uint8_t* sa = base + (size_t)s * g.stage_bytes;
+        uint8_t* sa = stages + (size_t)s * g.stage_bytes;
         umma::mbar_expect_tx(&full[s], g.stage_a + (g.resident_b ? 0u : 2u * g.box_b));
         for (int d = 0; d < 3; d++)
           for (int j = 0; j < 2; j++)
@@ -473,6 +503,7 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
       bool ok = true;
       if (g.resident_b && my_tiles > 0 && !umma::mbar_wait_bounded(&bfull, 0)) ok = false;
       const int items = my_tiles * G;
+      const uint32_t wrow = (uint32_t)g.npad * 16u;  // bytes per tap of a weight half
       for (int i = 0; i < items && ok; i++) {
         if (abort_flag) break;
         const int s = i % S;
@@ -487,16 +518,16 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
           break;
         }
         umma::fence_after();
-        uint8_t* sa = base + (size_t)s * g.stage_bytes;
-        const uint8_t* sb = g.resident_b ? sb_res + (size_t)grp * 2 * g.box_b : sa + g.stage_a;
-        const uint32_t dt = tbase + (uint32_t)(a * NCOLS);
+        uint8_t* sa = stages + (size_t)s * g.stage_bytes;
+        const uint8_t* sw = g.resident_b ? sb_res + (size_t)grp * 2 * g.box_b : sa + g.stage_a;
+        const uint32_t dt = tbase + (uint32_t)(a * NT);
 #pragma unroll 1
         for (int tap = 0; tap < 27; tap++) {
           const int dx = tap % 3, dy = (tap / 3) % 3, dz = tap / 9;
           const uint32_t row = (uint32_t)(dy * g.BX + dz * g.BX * (g.BY + 2));
-          const uint64_t da = umma::smem_desc_lbo(sa + dx * 2 * g.box_a + row * 16, g.box_a);
-          const uint64_t db = umma::smem_desc_lbo(sb + tap * N * 16, g.box_b);
-          umma::mma_bf16(dt, da, db, IDESC, (grp > 0 || tap > 0) ? 1u : 0u);
+          const uint64_t dw = umma::smem_desc_lbo(sw + tap * wrow, g.box_b);
+          const uint64_t dv = umma::smem_desc_lbo(sa + dx * 2 * g.box_a + row * 16, g.box_a);
+          umma::mma_bf16(dt, dw, dv, IDESC, (grp > 0 || tap > 0) ? 1u : 0u);
         }
         umma::mma_commit(&empty[s]);
         if (grp == G - 1) umma::mma_commit(&accf[a]);
@@ -511,51 +542,102 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
     }
     __syncwarp();
   } else {
-    // ---- epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31
-    const int lb = (warp & 3) * 32;
-    const int r = lb + lane;
+    // ---- epilogue (warps 2-5, 128 threads).  Warp w reads TMEM lanes
+    // 32 (w % 4) .. + 31, i.e. output channels co = 32 (w % 4) + lane, 32
+    // voxel columns at a time.  BF16 outputs in 8-channel planes go through
+    // a shared-memory transpose [voxel][channel] so that the global stores
+    // are 16-byte rows of one plane; other outputs are stored per lane.
+    const int q = warp & 3;
+    const int et = threadIdx.x - 64;  // 0..127
+    const int co = q * 32 + lane;
+    const bool active = q * 32 < ep.Nout;
+    const bool own = co < ep.Nout;
+    const float bias = (ep.bias && own) ? ep.bias[co] : 0.0f;
+    const bool planes = !ep.out_f32 && !(ep.Nout & 7);
+    const int cs = g.npad + 8;  // channel stride of a transpose row (bf16)
+    bf16* tr = reinterpret_cast<bf16*>(stages + (size_t)S * g.stage_bytes + CONV_SLACK);
+    const int nch8 = ep.Nout >> 3;
     for (int jt = 0; jt < my_tiles; jt++) {
       const int a = jt & 1;
-      const bool okw = umma::mbar_wait_bounded(&accf[a], (jt >> 1) & 1);
-      if (!__all_sync(0xffffffffu, okw)) {
-        timed_out = true;
+      const bool okw = __all_sync(0xffffffffu, umma::mbar_wait_bounded(&accf[a], (jt >> 1) & 1));
+      if (!okw) timed_out = true;
+      // the four epilogue warps leave the loop together
+      if (epi_bar_or(!okw || abort_flag != 0)) {
         abort_flag = 1;
         break;
       }
-      if (__any_sync(0xffffffffu, abort_flag != 0)) break;
       umma::fence_after();
-      float v[N];
-#pragma unroll
-      for (int col = 0; col < N; col += 16) {
-        float c[16];
-        umma::tmem_ld16(tbase + (uint32_t)(a * NCOLS) + ((uint32_t)lb << 16) + (uint32_t)col, c);
-#pragma unroll
-        for (int j = 0; j < 16; j++) v[col + j] = c[j];
-      }
-      umma::fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&acce[a]);
       int t = (int)blockIdx.x + jt * (int)gridDim.x;
       const int tx = t % g.tiles_x;
       t /= g.tiles_x;
       const int ty = t % g.tiles_y;
       t /= g.tiles_y;
       const int z = t % g.nz, b = t / g.nz;
-      const int x = tx * g.BX + r % g.BX, y = ty * g.BY + r / g.BX;
-      const int vox = (x < g.nx && y < g.ny) ? ((b * g.nz + z) * g.ny + y) * g.nx + x : -1;
+      const int x0 = tx * BX, y0 = ty * g.BY;
+      const size_t row0 = (((size_t)b * g.nz + z) * g.ny + y0) * g.nx + x0;
+#pragma unroll 1
+      for (int c0 = 0; c0 < NT; c0 += 32) {
+        float v[32];
+        if (active)
+          umma::tmem_ld32(tbase + (uint32_t)(a * NT + c0) + ((uint32_t)(q * 32) << 16), v);
+        if (planes) {
+          if (active && own) {
 #pragma unroll
-      for (int col = 0; col < N; col += 16) {
-        float c[16];
+            for (int j = 0; j < 32; j++) {
+              float val = v[j] + bias;
+              if (ep.relu) val = fmaxf(val, 0.0f);
+              tr[j * cs + co] = __float2bfloat16_rn(val);
+            }
+          }
+          epi_bar();
+          for (int it = et; it < 32 * nch8; it += 128) {
+            const int p = it >> 5, j = it & 31;
+            const int r = c0 + j;
+            const int lx = r & (BX - 1), ly = r >> LOG2BX;
+            if (x0 + lx < g.nx && y0 + ly < g.ny) {
+              const size_t vox = row0 + (size_t)ly * g.nx + lx;
+              uint4 u = *reinterpret_cast<const uint4*>(tr + j * cs + p * 8);
+              if (ep.mask) {
+                const uint4 m = __ldg(reinterpret_cast<const uint4*>(
+                    ep.mask + ((size_t)p * ep.V + vox) * 8));
+                const uint32_t* mw = reinterpret_cast<const uint32_t*>(&m);
+                uint32_t* uw = reinterpret_cast<uint32_t*>(&u);
 #pragma unroll
-        for (int j = 0; j < 16; j++) c[j] = v[col + j];
-        ep(vox, col, c);
+                for (int k = 0; k < 4; k++) {
+                  // keep a BF16 half only where the mask half is > 0
+                  const float lo = __uint_as_float(mw[k] << 16), hi = __uint_as_float(mw[k] & 0xFFFF0000u);
+                  uw[k] &= (lo > 0.0f ? 0x0000FFFFu : 0u) | (hi > 0.0f ? 0xFFFF0000u : 0u);
+                }
+              }
+              *reinterpret_cast<uint4*>(ep.out_bf16 + ((size_t)p * ep.V + vox) * 8) = u;
+            }
+          }
+          epi_bar();
+        } else if (active) {
+#pragma unroll
+          for (int j = 0; j < 32; j++) {
+            const int r = c0 + j;
+            const int lx = r & (BX - 1), ly = r >> LOG2BX;
+            if (!own || x0 + lx >= g.nx || y0 + ly >= g.ny) continue;
+            const size_t vox = row0 + (size_t)ly * g.nx + lx;
+            float val = v[j] + bias;
+            if (ep.relu) val = fmaxf(val, 0.0f);
+            if (ep.mask && !(__bfloat162float(ep.mask[act_off(vox, co, ep.Nout, ep.V)]) > 0.0f))
+              val = 0.0f;
+            if (ep.out_f32) ep.out_f32[vox * ep.Nout + co] = val;
+            else ep.out_bf16[act_off(vox, co, ep.Nout, ep.V)] = __float2bfloat16_rn(val);
+          }
+        }
       }
+      umma::fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acce[a]);
     }
   }
   if (timed_out) atomicExch(err, 1);
   umma::fence_before();
   __syncthreads();
-  if (warp == 1) umma::tmem_dealloc(tbase, 2 * NCOLS);
+  if (warp == 1) umma::tmem_dealloc(tbase, 2 * NT);
 }
 
 // --------------------------------------------------------- direct (CUDA cores)
@@ -699,30 +781,48 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-// Tile width in x: a TMA box row is 8 BX channels-elements, at most 256.
-int pick_bx(int nx) {
-  for (int c : {16, 8, 32})
-    if (nx % c == 0) return c;
+// Tile width in x for a tile of nt voxels: a TMA box row is 8 BX elements,
+// at most 256, so BX <= 32.
+int pick_bx(int nx, int nt) {
+  const int order256[3] = {16, 32, 8}, order128[3] = {16, 8, 32};
+  const int* o = nt == 256 ? order256 : order128;
+  for (int i = 0; i < 3; i++)
+    if (nx % o[i] == 0) return o[i];
   return nx < 16 ? 8 : 16;
 }
 
-template <int N, class Epi>
+template <int NT, int LOG2BX>
 cudaError_t tma_launch(const CUtensorMap& ta, const CUtensorMap& tb, const TmaGeom& g,
-                       const Epi& ep, int* err, cudaStream_t st) {
-  const size_t smem = (size_t)g.stages * g.stage_bytes + (g.resident_b ? g.b_bytes : 0) + 1024;
-  cudaError_t e = cudaFuncSetAttribute(k_conv_tma<N, Epi>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                       const ConvEpi& ep, int* err, cudaStream_t st) {
+  const size_t smem = (size_t)g.stage_off + (size_t)g.stages * g.stage_bytes + CONV_SLACK +
+                      CONV_EPI_BYTES + 1024;
+  auto kern = k_conv_tma<NT, LOG2BX>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
   if (e != cudaSuccess) return e;
   int dev = 0, nsm = 148, occ = 1;
   if (cudaGetDevice(&dev) == cudaSuccess)
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_conv_tma<N, Epi>, CONV_THREADS,
-                                                    smem) != cudaSuccess ||
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, CONV_THREADS, smem) !=
+          cudaSuccess ||
       occ < 1)
     occ = 1;
+  // the TMEM of 2 NT columns per CTA bounds the CTAs per SM as well
+  occ = std::min(occ, 512 / (2 * NT));
   const unsigned grid = (unsigned)std::min<long>((long)g.ntiles, (long)nsm * occ);
-  k_conv_tma<N, Epi><<<grid, CONV_THREADS, smem, st>>>(ta, tb, g, ep, err);
+  kern<<<grid, CONV_THREADS, smem, st>>>(ta, tb, g, ep, err);
   return cudaGetLastError();
+}
+
+template <int NT>
+cudaError_t tma_launch_bx(const CUtensorMap& ta, const CUtensorMap& tb, const TmaGeom& g,
+                          const ConvEpi& ep, int* err, cudaStream_t st) {
+  switch (g.BX) {
+    case 8: return tma_launch<NT, 3>(ta, tb, g, ep, err, st);
+    case 16: return tma_launch<NT, 4>(ta, tb, g, ep, err, st);
+    case 32: return tma_launch<NT, 5>(ta, tb, g, ep, err, st);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 inline int pad16(int n) { return (n + 15) / 16 * 16; }
@@ -821,25 +921,40 @@ cudaError_t conv3_tma(const bf16* x, int K, int nx, int ny, int nz, int nb, cons
   g.ny = ny;
   g.nz = nz;
   g.nb = nb;
-  g.BX = pick_bx(nx);
-  g.BY = 128 / g.BX;
+  g.groups = K / 16;
+  g.npad = pad16(N);
+  g.box_b = (uint32_t)(27 * g.npad * 16);
+  g.b_bytes = (uint32_t)g.groups * 2u * g.box_b;
+  // shared-memory plan: [resident weights][S stages][slack]; a voxel tile of
+  // 256 when two stages fit, else 128
+  const uint32_t budget = 226u * 1024u - 1024u - CONV_SLACK - CONV_EPI_BYTES;
+  int nt = 0;
+  for (int cand : {256, 128}) {
+    const int bx = pick_bx(nx, cand), by = cand / bx;
+    const uint32_t box_a = (uint32_t)(bx * (by + 2) * 3 * 16);
+    const uint32_t sa_al = (6 * box_a + 1023u) & ~1023u;
+    const uint32_t b_al = (g.b_bytes + 1023u) & ~1023u;
+    const bool res = b_al + 2 * sa_al <= budget;
+    const uint32_t stage = res ? sa_al : ((6 * box_a + 2 * g.box_b + 1023u) & ~1023u);
+    const uint32_t room = budget - (res ? b_al : 0u);
+    const int stg = (int)std::min<uint32_t>(CONV_MAX_STAGES, room / stage);
+    if (stg >= 2 || (cand == 128 && stg >= 1)) {
+      nt = cand;
+      g.BX = bx;
+      g.BY = by;
+      g.box_a = box_a;
+      g.stage_a = 6 * box_a;
+      g.resident_b = res ? 1 : 0;
+      g.stage_off = res ? b_al : 0u;
+      g.stage_bytes = stage;
+      g.stages = stg;
+      break;
+    }
+  }
+  if (nt == 0) return cudaErrorInvalidValue;
   g.tiles_x = (nx + g.BX - 1) / g.BX;
   g.tiles_y = (ny + g.BY - 1) / g.BY;
-  g.groups = K / 16;
-  const int npad = pad16(N);
   g.ntiles = g.tiles_x * g.tiles_y * nz * nb;
-  g.box_a = (uint32_t)(g.BX * (g.BY + 2) * 3 * 16);
-  g.box_b = (uint32_t)(27 * npad * 16);
-  g.stage_a = 6 * g.box_a;
-  g.b_bytes = (uint32_t)g.groups * 2u * g.box_b;
-  // shared-memory budget for the stages (+ resident weights) and alignment
-  const uint32_t budget = 220u * 1024u - 1024u;
-  const uint32_t sa_al = (g.stage_a + 1023u) & ~1023u;
-  g.resident_b = (g.b_bytes + 2 * sa_al <= budget) ? 1 : 0;
-  g.stage_bytes = g.resident_b ? sa_al : ((g.stage_a + 2 * g.box_b + 1023u) & ~1023u);
-  const uint32_t room = budget - (g.resident_b ? g.b_bytes : 0u);
-  g.stages = (int)std::min<uint32_t>(CONV_MAX_STAGES, room / g.stage_bytes);
-  if (g.stages < 1) return cudaErrorInvalidValue;
   CUtensorMap ta, tb;
   // input planes of 8 channels: dims (8 nx, ny, nz, nb K / 8), x and the
   // channel chunk innermost, so a box row is BX voxels x 16 bytes
@@ -855,22 +970,15 @@ cudaError_t conv3_tma(const bf16* x, int K, int nx, int ny, int nz, int nb, cons
     return cudaErrorInvalidValue;
   const cuuint64_t bdim[3] = {(cuuint64_t)K, (cuuint64_t)N, 27};
   const cuuint64_t bstr[2] = {(cuuint64_t)K * 2, (cuuint64_t)K * 2 * N};
-  const cuuint32_t bbox[3] = {8, (cuuint32_t)npad, 27};
+  const cuuint32_t bbox[3] = {8, (cuuint32_t)g.npad, 27};
   if (enc(&tb, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<bf16*>(w_tap), bdim, bstr, bbox,
           es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return cudaErrorInvalidValue;
   const int V = nx * ny * nz * nb;
   ConvEpi ep{y_bf16, y_f32, bias, mask, V, N, relu};
-  switch (npad) {
-    case 16: return tma_launch<16>(ta, tb, g, ep, err, st);
-    case 32: return tma_launch<32>(ta, tb, g, ep, err, st);
-    case 48: return tma_launch<48>(ta, tb, g, ep, err, st);
-    case 64: return tma_launch<64>(ta, tb, g, ep, err, st);
-    case 96: return tma_launch<96>(ta, tb, g, ep, err, st);
-    case 128: return tma_launch<128>(ta, tb, g, ep, err, st);
-    default: return cudaErrorInvalidValue;
-  }
+  return nt == 256 ? tma_launch_bx<256>(ta, tb, g, ep, err, st)
+                   : tma_launch_bx<128>(ta, tb, g, ep, err, st);
 }
 }  // namespace pyro
 
