@@ -386,10 +386,15 @@ struct TmaGeom {
 
 constexpr int CONV_THREADS = 192;
 constexpr int CONV_MAX_STAGES = 8;
-// bytes the 128-row weight operand of the last tap reads past its rows
-constexpr uint32_t CONV_SLACK = 2048;
-// epilogue transpose buffer: 32 voxels x (128 + 8) BF16 channels
-constexpr uint32_t CONV_EPI_BYTES = 32u * 136u * 2u;
+// Bytes the 128-row weight operand of the last tap reads past its rows:
+// (128 - npad) rows of 16 bytes, rounded up to 1 KB.
+__host__ __device__ __forceinline__ uint32_t conv_slack(int npad) {
+  return ((uint32_t)(128 - npad) * 16u + 1023u) & ~1023u;
+}
+// epilogue transpose buffer: 32 voxels x (npad + 8) BF16 channels
+__host__ __device__ __forceinline__ uint32_t conv_epi_bytes(int npad) {
+  return 32u * (uint32_t)(npad + 8) * 2u;
+}
 
 // Named barrier 1 over the 128 epilogue threads; the _or form also returns
 // whether any of them passed true.
@@ -555,7 +560,7 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
     const float bias = (ep.bias && own) ? ep.bias[co] : 0.0f;
     const bool planes = !ep.out_f32 && !(ep.Nout & 7);
     const int cs = g.npad + 8;  // channel stride of a transpose row (bf16)
-    bf16* tr = reinterpret_cast<bf16*>(stages + (size_t)S * g.stage_bytes + CONV_SLACK);
+    bf16* tr = reinterpret_cast<bf16*>(stages + (size_t)S * g.stage_bytes + conv_slack(g.npad));
     const int nch8 = ep.Nout >> 3;
     for (int jt = 0; jt < my_tiles; jt++) {
       const int a = jt & 1;
@@ -647,7 +652,9 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
 // from shared memory (FP32, [tap][ci][co]) feeds DV fused multiply-adds.
 // FP32 accumulation over the taps in order (dz, dy, dx); a tap outside the
 // volume reads zero (zero padding).
-constexpr int DIRECT_DV = 4;
+// voxels per thread: 4 for 2 -> 16 (weight reuse), 1 for 16 -> 1
+template <int CIN, int COUT>
+constexpr int direct_dv() { return CIN == 2 ? 4 : 1; }
 
 template <int CIN, int COUT>
 __global__ void __launch_bounds__(256) k_conv_direct(const bf16* __restrict__ x, Vol g,
@@ -656,7 +663,7 @@ __global__ void __launch_bounds__(256) k_conv_direct(const bf16* __restrict__ x,
                                                      bf16* __restrict__ y_bf16,
                                                      float* __restrict__ y_f32) {
   static_assert(CIN == 2 || CIN % 8 == 0, "input rows are loaded as 4- or 16-byte chunks");
-  constexpr int DV = DIRECT_DV;
+  constexpr int DV = direct_dv<CIN, COUT>();
   __shared__ __align__(16) float ws[27 * CIN * COUT];
   for (int i = threadIdx.x; i < 27 * CIN * COUT; i += blockDim.x) {
     const int co = i / (27 * CIN), t = (i / CIN) % 27, ci = i % CIN;  // w[co][t][ci]
@@ -794,8 +801,8 @@ int pick_bx(int nx, int nt) {
 template <int NT, int LOG2BX>
 cudaError_t tma_launch(const CUtensorMap& ta, const CUtensorMap& tb, const TmaGeom& g,
                        const ConvEpi& ep, int* err, cudaStream_t st) {
-  const size_t smem = (size_t)g.stage_off + (size_t)g.stages * g.stage_bytes + CONV_SLACK +
-                      CONV_EPI_BYTES + 1024;
+  const size_t smem = (size_t)g.stage_off + (size_t)g.stages * g.stage_bytes +
+                      conv_slack(g.npad) + conv_epi_bytes(g.npad) + 1024;
   auto kern = k_conv_tma<NT, LOG2BX>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
@@ -886,12 +893,15 @@ cudaError_t conv3_direct(const bf16* x, int C, int nx, int ny, int nz, int nb, c
                          int Cout, const float* bias, int relu, bf16* y_bf16, float* y_f32,
                          cudaStream_t st) {
   Vol g{nx, ny, nz, nb};
-  const long chunks = (long)((nx + DIRECT_DV - 1) / DIRECT_DV) * ny * nz * nb;
-  const unsigned blocks = (unsigned)((chunks + 255) / 256);
+  auto blocks = [&](int dv) {
+    return (unsigned)(((long)((nx + dv - 1) / dv) * ny * nz * nb + 255) / 256);
+  };
   if (C == 2 && Cout == 16)
-    k_conv_direct<2, 16><<<blocks, 256, 0, st>>>(x, g, w, bias, relu, y_bf16, y_f32);
+    k_conv_direct<2, 16><<<blocks(direct_dv<2, 16>()), 256, 0, st>>>(x, g, w, bias, relu, y_bf16,
+                                                                     y_f32);
   else if (C == 16 && Cout == 1)
-    k_conv_direct<16, 1><<<blocks, 256, 0, st>>>(x, g, w, bias, relu, y_bf16, y_f32);
+    k_conv_direct<16, 1><<<blocks(direct_dv<16, 1>()), 256, 0, st>>>(x, g, w, bias, relu, y_bf16,
+                                                                     y_f32);
   else
     return cudaErrorInvalidValue;
   return cudaGetLastError();
@@ -927,7 +937,8 @@ cudaError_t conv3_tma(const bf16* x, int K, int nx, int ny, int nz, int nb, cons
   g.b_bytes = (uint32_t)g.groups * 2u * g.box_b;
   // shared-memory plan: [resident weights][S stages][slack]; a voxel tile of
   // 256 when two stages fit, else 128
-  const uint32_t budget = 226u * 1024u - 1024u - CONV_SLACK - CONV_EPI_BYTES;
+  const uint32_t budget =
+      226u * 1024u - 1024u - conv_slack(g.npad) - ((conv_epi_bytes(g.npad) + 15u) & ~15u);
   int nt = 0;
   for (int cand : {256, 128}) {
     const int bx = pick_bx(nx, cand), by = cand / bx;
