@@ -72,6 +72,28 @@ __device__ __forceinline__ I3 dir6(int k) {
             k == 4 ? 1 : (k == 5 ? -1 : 0)};
 }
 
+// --------------------------------------------------------- integer division
+// Division of unsigned 32-bit values by a divisor fixed at launch, by a
+// multiply-high and shifts (Granlund and Montgomery, "Division by invariant
+// integers using multiplication", PLDI 1994, fig. 4.1): with
+// l = ceil(log2 d) and m = floor(2^32 (2^l - d) / d) + 1,
+// n / d = (t + ((n - t) >> 1)) >> (l - 1), t = umulhi(m, n), for every n.
+struct FastDiv {
+  uint32_t d, m, s1, s2;
+  FastDiv() = default;
+  __host__ explicit FastDiv(uint32_t dv) : d(dv) {
+    uint32_t l = 0;
+    while ((1ull << l) < dv) l++;
+    m = (uint32_t)(((1ull << 32) * ((1ull << l) - dv)) / dv + 1);
+    s1 = l > 0 ? 1u : 0u;
+    s2 = l > 0 ? l - 1u : 0u;
+  }
+  __device__ __forceinline__ uint32_t div(uint32_t n) const {
+    const uint32_t t = __umulhi(m, n);
+    return (t + ((n - t) >> s1)) >> s2;
+  }
+};
+
 // ------------------------------------------------------------------- grid
 struct Grid {
   int nx, ny, nz;

@@ -416,17 +416,18 @@ template <typename TS>
 __global__ void __launch_bounds__(256) k_mg_pass4(L d, float h2, const TS* __restrict__ b,
                                                   const uint8_t* __restrict__ meta,
                                                   TS* __restrict__ p, int color, float omega,
-                                                  int bc_mode) {
-  // chunk c of 4 cells, x fastest; rows of nx / 4 chunks
+                                                  int bc_mode, FastDiv by_cpr, FastDiv by_ny) {
+  // chunk c of 4 cells, x fastest; rows of nx / 4 chunks (divisions by the
+  // row length and ny by multiply-high)
   const int cpr = d.nx >> 2;
   const int nchunks = cpr * d.ny * d.nz;
   const int c = blockIdx.x * 256 + threadIdx.x;
   const int lane = threadIdx.x & 31;
   const bool act = c < nchunks;
   const int cc = act ? c : 0;
-  const int row = cc / cpr;
+  const int row = (int)by_cpr.div((uint32_t)cc);
   const int x0 = (cc - row * cpr) * 4;
-  const int y = row % d.ny, z = row / d.ny;
+  const int z = (int)by_ny.div((uint32_t)row), y = row - z * d.ny;
   const int sy = d.nx, sz = d.nx * d.ny;
   const int i0 = row * d.nx + x0;
   // every load first
@@ -691,9 +692,9 @@ cudaError_t pass_t(Dims3 d, float h, const TS* b, const uint8_t* meta, TS* p, in
                    float omega, int bc_mode, cudaStream_t st) {
   if (d.nx % 4 == 0) {
     const long chunks = (long)(d.nx / 4) * d.ny * d.nz;
-    k_mg_pass4<TS><<<(unsigned)((chunks + 255) / 256), 256, 0, st>>>(L{d.nx, d.ny, d.nz}, h * h, b,
-                                                                      meta, p, color, omega,
-                                                                      bc_mode);
+    k_mg_pass4<TS><<<(unsigned)((chunks + 255) / 256), 256, 0, st>>>(
+        L{d.nx, d.ny, d.nz}, h * h, b, meta, p, color, omega, bc_mode,
+        FastDiv((uint32_t)(d.nx / 4)), FastDiv((uint32_t)d.ny));
     return cudaGetLastError();
   }
   dim3 grid(((d.nx + 1) / 2 + 31) / 32, (d.ny + 3) / 4, (d.nz + 1) / 2);
