@@ -89,6 +89,43 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
+def load_tensor_peak():
+    """Dense BF16 TFLOP/s for a kernel timed on its own (burst figure)."""
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["bf16_tflops"]), "measured"
+    return 1590.0, "fallback"
+
+
+def net_roofline(net, bd, fd, dims, h, reps=5):
+    """The learned stage's network forward on this pressure system, timed
+    alone with CUDA events, as tensor-core throughput (the FLOPs of its nine
+    3x3x3 convolutions per voxel, pyro_b200.learned.flops_per_voxel) against
+    the measured dense BF16 peak."""
+    import torch
+    from pyro_b200.learned import flops_per_voxel
+    phi = torch.empty_like(bd)
+    s = torch.cuda.current_stream().cuda_stream
+    for _ in range(2):
+        net.forward(bd.data_ptr(), fd.data_ptr(), dims, 1, h, phi.data_ptr(), stream=s)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        net.forward(bd.data_ptr(), fd.data_ptr(), dims, 1, h, phi.data_ptr(), stream=s)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    vox = dims[0] * dims[1] * dims[2]
+    tf = flops_per_voxel() * vox / (ms * 1e-3) / 1e12
+    peak, kind = load_tensor_peak()
+    return {"bound": "tensor", "forward_ms": round(ms, 3), "achieved": tf, "peak": peak,
+            "peak_kind": kind, "unit": "TFLOP/s", "frac": tf / peak,
+            "flops_per_voxel": flops_per_voxel(), "voxels": vox}
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed
     region."""
@@ -305,6 +342,8 @@ def sim_solver_bench(sim):
     v, l = res.get("vcycle_fp32_to_1e-3"), res.get("mgpcg_bf16_learned_to_1e-4")
     out = {"config": f"the bench's last substep, {sim.dims[0]}x{sim.dims[1]}x{sim.dims[2]}, "
                      "phi0 = 0", "runs": res}
+    if net is not None:
+        out["net_roofline"] = net_roofline(net, bd, fd, tuple(sim.dims), sim.dx)
     if v and l:
         out["speedup_learned_1e-4_vs_vcycle_1e-3"] = v["ms"] / l["ms"]
     b16 = res.get("mgpcg_bf16_to_1e-4")
