@@ -252,6 +252,8 @@ int pyro_k_solid(const PyroParams* params_dev, uint32_t nx, uint32_t ny,
 int pyro_k_curl(const PyroParams* params_dev, uint32_t nx, uint32_t ny,
                 uint32_t nz, const float* u, const float* v, const float* w,
                 float* curl, float* stats, void* stream);
+/* adv_vel1 then adv_vel2; allocates a temporary device buffer for the
+ * predictor's limiter bounds and returns after the stream has finished. */
 int pyro_k_adv_vel(const PyroParams* params_dev, uint32_t nx, uint32_t ny,
                    uint32_t nz, const float* u, const float* v, const float* w,
                    float* hu, float* hv, float* hw, float* ou, float* ov,

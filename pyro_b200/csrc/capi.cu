@@ -72,9 +72,15 @@ int pyro_k_adv_vel(const PyroParams* params_dev, uint32_t nx, uint32_t ny, uint3
   KDIMS(pyro_k_adv_vel)
   PYRO_REQUIRE(u && v && w && hu && hv && hw && ou && ov && ow && flags,
                "pyro_k_adv_vel: null buffer");
-  cudaError_t e = launch_adv_vel1(params_dev, d, u, v, w, hu, hv, hw, S(stream));
+  // the predictor's min / max at the backtrace, handed to the corrector
+  DevBuf lohi;
+  int rc = lohi.alloc((size_t)(nx + 1) * (ny + 1) * (nz + 1) * 6 * 4);
+  if (rc != PYRO_OK) return rc;
+  cudaError_t e = launch_adv_vel1(params_dev, d, u, v, w, hu, hv, hw, lohi.as<float>(), S(stream));
   if (e == cudaSuccess)
-    e = launch_adv_vel2(params_dev, d, u, v, w, hu, hv, hw, ou, ov, ow, flags, S(stream));
+    e = launch_adv_vel2(params_dev, d, u, v, w, hu, hv, hw, lohi.as<float>(), ou, ov, ow, flags,
+                        S(stream));
+  if (e == cudaSuccess) e = cudaStreamSynchronize(S(stream));  // before lohi is freed
   return ret(e, "pyro_k_adv_vel");
 }
 

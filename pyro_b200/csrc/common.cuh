@@ -184,6 +184,30 @@ __device__ __forceinline__ void mmC(const float* __restrict__ X, const Grid& gr,
   lo = fminf(fminf(fminf(fminf(fminf(fminf(fminf(1e30f, v0), v1), v2), v3), v4), v5), fminf(v6, v7));
   hv = fmaxf(fmaxf(fmaxf(fmaxf(fmaxf(fmaxf(fmaxf(-1e30f, v0), v1), v2), v3), v4), v5), fmaxf(v6, v7));
 }
+// triC and mmC at the same point from one set of 8 corner loads: the
+// trilinear value, and the corners' min / max with mmC's expression order.
+__device__ __forceinline__ float triC_mm(const float* __restrict__ X, const Grid& gr, F3 g0,
+                                        I3 hi, float& lo, float& hv) {
+  float gx = wclamp(g0.x, 0.0f, (float)hi.x);
+  float gy = wclamp(g0.y, 0.0f, (float)hi.y);
+  float gz = wclamp(g0.z, 0.0f, (float)hi.z);
+  int bx = min((int)floorf(gx), hi.x - 1);
+  int by = min((int)floorf(gy), hi.y - 1);
+  int bz = min((int)floorf(gz), hi.z - 1);
+  float fx = gx - (float)bx, fy = gy - (float)by, fz = gz - (float)bz;
+  const int sy = gr.nx + 1, sz = (gr.nx + 1) * (gr.ny + 1);
+  int i = bx + sy * by + sz * bz;
+  float v0 = __ldg(X + i), v1 = __ldg(X + i + 1), v2 = __ldg(X + i + sy),
+        v3 = __ldg(X + i + sy + 1), v4 = __ldg(X + i + sz), v5 = __ldg(X + i + sz + 1),
+        v6 = __ldg(X + i + sy + sz), v7 = __ldg(X + i + sy + sz + 1);
+  lo = fminf(fminf(fminf(fminf(fminf(fminf(fminf(1e30f, v0), v1), v2), v3), v4), v5), fminf(v6, v7));
+  hv = fmaxf(fmaxf(fmaxf(fmaxf(fmaxf(fmaxf(fmaxf(-1e30f, v0), v1), v2), v3), v4), v5), fmaxf(v6, v7));
+  float c00 = wmix(v0, v1, fx);
+  float c10 = wmix(v2, v3, fx);
+  float c01 = wmix(v4, v5, fx);
+  float c11 = wmix(v6, v7, fx);
+  return wmix(wmix(c00, c10, fy), wmix(c01, c11, fy), fz);
+}
 // Cell-centred vec4 trilinear sample (tmpl_scalar.wgsl:2-15).
 __device__ __forceinline__ float4 triS(const float4* __restrict__ X, const Grid& gr, F3 gc0) {
   float gx = wclamp(gc0.x, 0.0f, (float)(gr.nx - 1));
@@ -309,6 +333,12 @@ struct Vel {
     F3 u1 = first(g, k, c);
     F3 u2 = at(g, x - (0.5f * kk) * u1);
     return x - kk * u2;
+  }
+  __device__ __forceinline__ F3 fwd_at(const Grid& g, float kk, int k, I3 c, F3 x) const {
+    F3 u1 = first(g, k, c);
+    F3 h = (0.5f * kk) * u1;
+    F3 uf = at(g, x + h);
+    return x + kk * uf;
   }
   __device__ __forceinline__ void both_at(const Grid& g, float kk, int k, I3 c, F3 x, F3& b,
                                           F3& f) const {

@@ -240,28 +240,41 @@ __device__ __forceinline__ const float* pick3(int k, const float* a, const float
   return k == 0 ? a : (k == 1 ? b : c);
 }
 
+// Predictor: h = v(backtrace(x)) per valid face component.  It also keeps
+// the min / max of v over the 8 corners of that trilinear sample (the
+// corrector's limiter, advect.wgsl:55-68, samples the same point), in
+// lohi[0..2] / lohi[3..5] per component, so the corrector does not trace
+// back again.
 __global__ void __launch_bounds__(256) k_adv_vel1(const PyroParams* __restrict__ Pp, Grid g,
                                                   const float* __restrict__ u,
                                                   const float* __restrict__ v,
                                                   const float* __restrict__ w,
                                                   float* __restrict__ hu,
                                                   float* __restrict__ hv,
-                                                  float* __restrict__ hw) {
+                                                  float* __restrict__ hw,
+                                                  float* __restrict__ lohi) {
   I3 c = thread_cell();
   if (c.x > g.nx || c.y > g.ny || c.z > g.nz) return;
   const float kk = Pp->dt / Pp->dx;
+  const size_t nv = (size_t)(g.nx + 1) * (g.ny + 1) * (g.nz + 1);
   Vel V{u, v, w};
   int i = g.vidx(c);
 #pragma unroll
   for (int k = 0; k < 3; k++) {
     if (!g.compValid(k, c)) continue;
     F3 off = compOff(k);
-    float r = triC(pick3(k, u, v, w), g, V.back_at(g, kk, k, c, tof3(c) + off) - off,
-                   g.compHi(k));
+    float lo, hi;
+    float r = triC_mm(pick3(k, u, v, w), g, V.back_at(g, kk, k, c, tof3(c) + off) - off,
+                      g.compHi(k), lo, hi);
     if (k == 0) hu[i] = r; else if (k == 1) hv[i] = r; else hw[i] = r;
+    lohi[k * nv + i] = lo;
+    lohi[(3 + k) * nv + i] = hi;
   }
 }
 
+// Corrector: clamp(h + (v - h(fwdtrace(x))) / 2, min, max of v at the
+// backtrace) (advect.wgsl:22-70); blocked faces 0.  The backtrace's
+// min / max come from the predictor.
 __global__ void __launch_bounds__(256) k_adv_vel2(const PyroParams* __restrict__ Pp, Grid g,
                                                   const float* __restrict__ u,
                                                   const float* __restrict__ v,
@@ -269,6 +282,7 @@ __global__ void __launch_bounds__(256) k_adv_vel2(const PyroParams* __restrict__
                                                   const float* __restrict__ hu,
                                                   const float* __restrict__ hv,
                                                   const float* __restrict__ hw,
+                                                  const float* __restrict__ lohi,
                                                   float* __restrict__ ou,
                                                   float* __restrict__ ov,
                                                   float* __restrict__ ow,
@@ -276,6 +290,7 @@ __global__ void __launch_bounds__(256) k_adv_vel2(const PyroParams* __restrict__
   I3 c = thread_cell();
   if (c.x > g.nx || c.y > g.ny || c.z > g.nz) return;
   const float kk = Pp->dt / Pp->dx;
+  const size_t nv = (size_t)(g.nx + 1) * (g.ny + 1) * (g.nz + 1);
   Vel V{u, v, w};
   int i = g.vidx(c);
   bool sc = g.inb(c) && __ldg(flags + g.sidx(c)) == 1u;
@@ -291,14 +306,10 @@ __global__ void __launch_bounds__(256) k_adv_vel2(const PyroParams* __restrict__
       F3 off = compOff(k);
       I3 hi = g.compHi(k);
       F3 x = tof3(c) + off;
-      F3 b, f;
-      V.both_at(g, kk, k, c, x, b, f);
-      b = b - off;
-      f = f - off;
+      F3 f = V.fwd_at(g, kk, k, c, x) - off;
       const float* vk = pick3(k, u, v, w);
       const float* hk = pick3(k, hu, hv, hw);
-      float lo, hv2;
-      mmC(vk, g, b, hi, lo, hv2);
+      const float lo = __ldg(lohi + k * nv + i), hv2 = __ldg(lohi + (3 + k) * nv + i);
       r = wclamp(__ldg(hk + i) + 0.5f * (__ldg(vk + i) - triC(hk, g, f, hi)), lo, hv2);
     }
     if (k == 0) ou[i] = r; else if (k == 1) ov[i] = r; else ow[i] = r;
@@ -674,19 +685,20 @@ cudaError_t launch_curl(const PyroParams* P, Dims3 d, const float* u, const floa
   return cudaGetLastError();
 }
 cudaError_t launch_adv_vel1(const PyroParams* P, Dims3 d, const float* u, const float* v,
-                            const float* w, float* hu, float* hv, float* hw, cudaStream_t st) {
+                            const float* w, float* hu, float* hv, float* hw, float* lohi,
+                            cudaStream_t st) {
   Grid g{d.nx, d.ny, d.nz};
   k_adv_vel1<<<grid_for(d.nx + 1, d.ny + 1, d.nz + 1), PYRO_BLOCK, 0, st>>>(P, g, u, v, w, hu, hv,
-                                                                           hw);
+                                                                           hw, lohi);
   return cudaGetLastError();
 }
 cudaError_t launch_adv_vel2(const PyroParams* P, Dims3 d, const float* u, const float* v,
                             const float* w, const float* hu, const float* hv, const float* hw,
-                            float* ou, float* ov, float* ow, const uint32_t* flags,
-                            cudaStream_t st) {
+                            const float* lohi, float* ou, float* ov, float* ow,
+                            const uint32_t* flags, cudaStream_t st) {
   Grid g{d.nx, d.ny, d.nz};
   k_adv_vel2<<<grid_for(d.nx + 1, d.ny + 1, d.nz + 1), PYRO_BLOCK, 0, st>>>(
-      P, g, u, v, w, hu, hv, hw, ou, ov, ow, flags);
+      P, g, u, v, w, hu, hv, hw, lohi, ou, ov, ow, flags);
   return cudaGetLastError();
 }
 cudaError_t launch_adv_s1(const PyroParams* P, Dims3 d, const float* u, const float* v,

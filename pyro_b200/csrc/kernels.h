@@ -23,12 +23,16 @@ cudaError_t launch_solid(const PyroParams* P, Dims3 d, const float4* solIn, floa
                          cudaStream_t st);
 cudaError_t launch_curl(const PyroParams* P, Dims3 d, const float* u, const float* v,
                         const float* w, float4* curl, float* stats, cudaStream_t st);
+// lohi: 6 face arrays of (nx+1)(ny+1)(nz+1) floats, the predictor's
+// per-component min (0..2) and max (3..5) of v at the backtrace, written by
+// adv_vel1 and read by adv_vel2.
 cudaError_t launch_adv_vel1(const PyroParams* P, Dims3 d, const float* u, const float* v,
-                            const float* w, float* hu, float* hv, float* hw, cudaStream_t st);
+                            const float* w, float* hu, float* hv, float* hw, float* lohi,
+                            cudaStream_t st);
 cudaError_t launch_adv_vel2(const PyroParams* P, Dims3 d, const float* u, const float* v,
                             const float* w, const float* hu, const float* hv, const float* hw,
-                            float* ou, float* ov, float* ow, const uint32_t* flags,
-                            cudaStream_t st);
+                            const float* lohi, float* ou, float* ov, float* ow,
+                            const uint32_t* flags, cudaStream_t st);
 cudaError_t launch_adv_s1(const PyroParams* P, Dims3 d, const float* u, const float* v,
                           const float* w, const float4* s0, const float4* s1, float4* h0,
                           float4* h1, cudaStream_t st);

@@ -40,7 +40,7 @@ struct PyroSim {
   int cur = 0;  // velocity and solid ping-pong index (equal in the reference)
   cudaStream_t stream = nullptr;
 
-  DevBuf vel[2][3], hat[3];
+  DevBuf vel[2][3], hat[3], lohi;
   DevBuf s0, s1, s0b, s1b, h0, h1, sol[2], pyr, curl, flags, phi0, b0;
   DevBuf stats, params;
   Multigrid mg;
@@ -86,10 +86,11 @@ struct PyroSim {
       return e;
     if ((e = launch_curl(P, d, ua, va, wa, curl.as<float4>(), S, st)) != cudaSuccess) return e;
     if ((e = launch_adv_vel1(P, d, ua, va, wa, hat[0].as<float>(), hat[1].as<float>(),
-                             hat[2].as<float>(), st)) != cudaSuccess)
+                             hat[2].as<float>(), lohi.as<float>(), st)) != cudaSuccess)
       return e;
     if ((e = launch_adv_vel2(P, d, ua, va, wa, hat[0].as<float>(), hat[1].as<float>(),
-                             hat[2].as<float>(), ub, vb, wb, flags.as<uint32_t>(), st)) !=
+                             hat[2].as<float>(), lohi.as<float>(), ub, vb, wb,
+                             flags.as<uint32_t>(), st)) !=
         cudaSuccess)
       return e;
     if ((e = launch_adv_s1(P, d, ua, va, wa, s0.as<float4>(), s1.as<float4>(), h0.as<float4>(),
@@ -180,6 +181,7 @@ struct PyroSim {
     for (auto& a : vel)
       for (auto& b : a) s += b.bytes;
     for (auto& b : hat) s += b.bytes;
+    s += lohi.bytes;
     const DevBuf* list[] = {&s0, &s1, &s0b, &s1b, &h0, &h1, &sol[0], &sol[1], &pyr,
                             &curl, &flags, &phi0, &b0, &stats, &params};
     for (auto* b : list) s += b->bytes;
@@ -224,6 +226,7 @@ int pyro_sim_create(const PyroParams* params, const float* sol_init, uint32_t pr
       if ((rc = S->vel[a][k].alloc(nv * 4)) != PYRO_OK) return fail(rc);
   for (int k = 0; k < 3; k++)
     if ((rc = S->hat[k].alloc(nv * 4)) != PYRO_OK) return fail(rc);
+  if ((rc = S->lohi.alloc(nv * 6 * 4)) != PYRO_OK) return fail(rc);
   DevBuf* f4s[] = {&S->s0, &S->s1, &S->s0b, &S->s1b, &S->h0, &S->h1,
                    &S->sol[0], &S->sol[1], &S->pyr, &S->curl};
   for (auto* b : f4s)
@@ -346,11 +349,12 @@ int pyro_sim_profile_step(PyroSim* S, float dt, float time, float ign_on, int wa
   mark();
   if (e == cudaSuccess)
     e = launch_adv_vel1(P, S->d, ua, va, wa, S->hat[0].as<float>(), S->hat[1].as<float>(),
-                        S->hat[2].as<float>(), st);
+                        S->hat[2].as<float>(), S->lohi.as<float>(), st);
   mark();
   if (e == cudaSuccess)
     e = launch_adv_vel2(P, S->d, ua, va, wa, S->hat[0].as<float>(), S->hat[1].as<float>(),
-                        S->hat[2].as<float>(), ub, vb, wb, S->flags.as<uint32_t>(), st);
+                        S->hat[2].as<float>(), S->lohi.as<float>(), ub, vb, wb,
+                        S->flags.as<uint32_t>(), st);
   mark();
   if (e == cudaSuccess)
     e = launch_adv_s1(P, S->d, ua, va, wa, S->s0.as<float4>(), S->s1.as<float4>(),
