@@ -72,6 +72,34 @@ __device__ __forceinline__ I3 dir6(int k) {
             k == 4 ? 1 : (k == 5 ? -1 : 0)};
 }
 
+// ------------------------------------------------ programmatic dependent launch
+// A kernel launched with launch_pdl may be scheduled while the kernel before
+// it in the stream is still finishing.  It calls pdl_trigger() first (so
+// that the next one may be scheduled once all of its own blocks are
+// running) and pdl_wait() before its first global memory access (which
+// returns once the previous kernel has completed and its writes are
+// visible).  Without the launch attribute both are no-ops.
+__device__ __forceinline__ void pdl_trigger() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                              cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 // --------------------------------------------------------- integer division
 // Division of unsigned 32-bit values by a divisor fixed at launch, by a
 // multiply-high and shifts (Granlund and Montgomery, "Division by invariant

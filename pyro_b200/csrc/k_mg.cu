@@ -222,6 +222,8 @@ __global__ void __launch_bounds__(COARSE_THREADS, 1)
                         const uint32_t* __restrict__ f, TS* __restrict__ p, int iters,
                         float omega, int bc_mode, int symmetric) {
   namespace cg = cooperative_groups;
+  pdl_trigger();
+  pdl_wait();
   cg::cluster_group cl = cg::this_cluster();
   extern __shared__ float sp[];
   const int C = (int)cl.num_blocks();
@@ -391,13 +393,15 @@ cudaError_t mg_coarse_t(Dims3 d, float h, const TS* b, const uint32_t* f, TS* p,
   cfg.blockDim = dim3(COARSE_THREADS, 1, 1);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
-  cudaLaunchAttribute at[1];
+  cudaLaunchAttribute at[2];
   at[0].id = cudaLaunchAttributeClusterDimension;
   at[0].val.clusterDim.x = (unsigned)C;
   at[0].val.clusterDim.y = 1;
   at[0].val.clusterDim.z = 1;
+  at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;  // see launch_pdl
+  at[1].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
-  cfg.numAttrs = 1;
+  cfg.numAttrs = 2;
   return cudaLaunchKernelEx(&cfg, k_mg_coarse_cluster<TS>, Lvl{d.nx, d.ny, d.nz}, h * h, b, f, p,
                             iters, omega, bc_mode, symmetric);
 }

@@ -53,6 +53,8 @@ __device__ __forceinline__ int dirichlet_faces(const L& d, int x, int y, int z, 
 
 __global__ void __launch_bounds__(256) k_mg_meta(L d, const uint32_t* __restrict__ f,
                                                  uint8_t* __restrict__ meta) {
+  pdl_trigger();
+  pdl_wait();
   int x = blockIdx.x * 32 + threadIdx.x;
   int y = blockIdx.y * 4 + threadIdx.y;
   int z = blockIdx.z * 2 + threadIdx.z;
@@ -69,6 +71,8 @@ __global__ void __launch_bounds__(256) k_mg_meta(L d, const uint32_t* __restrict
 // Coarse solid flag = every in-domain child solid (mg.wgsl:73-82, fc).
 __global__ void __launch_bounds__(256) k_mg_flags_down(L df, const uint32_t* __restrict__ ff,
                                                        L dc, uint32_t* __restrict__ fc) {
+  pdl_trigger();
+  pdl_wait();
   int x = blockIdx.x * 32 + threadIdx.x;
   int y = blockIdx.y * 4 + threadIdx.y;
   int z = blockIdx.z * 2 + threadIdx.z;
@@ -303,6 +307,8 @@ __global__ void __launch_bounds__(256) k_mg_prolong_m(L df, const TS* __restrict
                                                       const uint8_t* __restrict__ mf,
                                                       TS* __restrict__ pf, L dc,
                                                       const uint8_t* __restrict__ mc) {
+  pdl_trigger();
+  pdl_wait();
   const int X = blockIdx.x * 32 + threadIdx.x;
   const int Y = blockIdx.y * 4 + threadIdx.y;
   const int Z = blockIdx.z * 2 + threadIdx.z;
@@ -369,6 +375,8 @@ __global__ void __launch_bounds__(256) k_mg_pass(L d, float h2, const TS* __rest
                                                  const uint8_t* __restrict__ meta,
                                                  TS* __restrict__ p, int color, float omega,
                                                  int bc_mode) {
+  pdl_trigger();
+  pdl_wait();
   int y = blockIdx.y * 4 + threadIdx.y;
   int z = blockIdx.z * 2 + threadIdx.z;
   int x = (int)(blockIdx.x * 32 + threadIdx.x) * 2 + ((y + z + color) & 1);
@@ -417,6 +425,8 @@ __global__ void __launch_bounds__(256) k_mg_pass4(L d, float h2, const TS* __res
                                                   const uint8_t* __restrict__ meta,
                                                   TS* __restrict__ p, int color, float omega,
                                                   int bc_mode, FastDiv by_cpr, FastDiv by_ny) {
+  pdl_trigger();
+  pdl_wait();
   // chunk c of 4 cells, x fastest; rows of nx / 4 chunks (divisions by the
   // row length and ny by multiply-high)
   const int cpr = d.nx >> 2;
@@ -502,6 +512,8 @@ __global__ void __launch_bounds__(256) k_mg_restrict_m(L df, float h2, const TS*
                                                        const uint8_t* __restrict__ mf, L dc,
                                                        TS* __restrict__ bc, TS* __restrict__ pc,
                                                        int bc_mode) {
+  pdl_trigger();
+  pdl_wait();
   const int X = blockIdx.x * 32 + threadIdx.x;
   const int Y = blockIdx.y * 4 + threadIdx.y;
   const int Z = blockIdx.z * 2 + threadIdx.z;
@@ -588,6 +600,8 @@ __global__ void __launch_bounds__(256) k_mg_resid_w(L d, float h2, const TS* __r
                                                     const uint8_t* __restrict__ m0, L dc,
                                                     const uint8_t* __restrict__ mc,
                                                     int bc_mode, TS* __restrict__ rt) {
+  pdl_trigger();
+  pdl_wait();
   int x = blockIdx.x * 32 + threadIdx.x;
   int y = blockIdx.y * 4 + threadIdx.y;
   int z = blockIdx.z * 2 + threadIdx.z;
@@ -630,6 +644,8 @@ __global__ void __launch_bounds__(256) k_mg_restrict_t(L df, const TS* __restric
                                                        const uint8_t* __restrict__ mf, L dc,
                                                        const uint8_t* __restrict__ mc,
                                                        TS* __restrict__ bc, TS* __restrict__ pc) {
+  pdl_trigger();
+  pdl_wait();
   int X = blockIdx.x * 32 + threadIdx.x;
   int Y = blockIdx.y * 4 + threadIdx.y;
   int Z = blockIdx.z * 2 + threadIdx.z;
@@ -692,26 +708,20 @@ cudaError_t pass_t(Dims3 d, float h, const TS* b, const uint8_t* meta, TS* p, in
                    float omega, int bc_mode, cudaStream_t st) {
   if (d.nx % 4 == 0) {
     const long chunks = (long)(d.nx / 4) * d.ny * d.nz;
-    k_mg_pass4<TS><<<(unsigned)((chunks + 255) / 256), 256, 0, st>>>(
-        L{d.nx, d.ny, d.nz}, h * h, b, meta, p, color, omega, bc_mode,
-        FastDiv((uint32_t)(d.nx / 4)), FastDiv((uint32_t)d.ny));
-    return cudaGetLastError();
+    return launch_pdl(k_mg_pass4<TS>, dim3((unsigned)((chunks + 255) / 256)), dim3(256), 0, st,
+                      L{d.nx, d.ny, d.nz}, h * h, b, meta, p, color, omega, bc_mode,
+                      FastDiv((uint32_t)(d.nx / 4)), FastDiv((uint32_t)d.ny));
   }
   dim3 grid(((d.nx + 1) / 2 + 31) / 32, (d.ny + 3) / 4, (d.nz + 1) / 2);
-  k_mg_pass<TS><<<grid, dim3(32, 4, 2), 0, st>>>(L{d.nx, d.ny, d.nz}, h * h, b, meta, p, color,
-                                                omega, bc_mode);
-  return cudaGetLastError();
+  return launch_pdl(k_mg_pass<TS>, grid, dim3(32, 4, 2), 0, st, L{d.nx, d.ny, d.nz}, h * h, b,
+                    meta, p, color, omega, bc_mode);
 }
 template <typename TS>
 cudaError_t restrict_t(Dims3 df, float h, const TS* pf, const TS* bf, const uint8_t* mf,
                        Dims3 dc, TS* bc, TS* pc, int bc_mode, cudaStream_t st) {
-  if (df.nx % 2 == 0)
-    k_mg_restrict_m<TS, true><<<g3(dc), dim3(32, 4, 2), 0, st>>>(
-        L{df.nx, df.ny, df.nz}, h * h, pf, bf, mf, L{dc.nx, dc.ny, dc.nz}, bc, pc, bc_mode);
-  else
-    k_mg_restrict_m<TS, false><<<g3(dc), dim3(32, 4, 2), 0, st>>>(
-        L{df.nx, df.ny, df.nz}, h * h, pf, bf, mf, L{dc.nx, dc.ny, dc.nz}, bc, pc, bc_mode);
-  return cudaGetLastError();
+  auto kern = df.nx % 2 == 0 ? k_mg_restrict_m<TS, true> : k_mg_restrict_m<TS, false>;
+  return launch_pdl(kern, g3(dc), dim3(32, 4, 2), 0, st, L{df.nx, df.ny, df.nz}, h * h, pf, bf,
+                    mf, L{dc.nx, dc.ny, dc.nz}, bc, pc, bc_mode);
 }
 
 cudaError_t launch_mg_pass(Dims3 d, float h, const float* b, const uint8_t* meta, float* p,
@@ -739,13 +749,12 @@ template <typename TS>
 cudaError_t restrict_sym_t(Dims3 df, float h, const TS* pf, const TS* bf, const uint8_t* mf,
                            TS* rt, Dims3 dc, const uint8_t* mc, TS* bc, TS* pc, int bc_mode,
                            cudaStream_t st) {
-  k_mg_resid_w<TS><<<g3(df), dim3(32, 4, 2), 0, st>>>(L{df.nx, df.ny, df.nz}, h * h, pf, bf, mf,
-                                                      L{dc.nx, dc.ny, dc.nz}, mc, bc_mode, rt);
-  cudaError_t e = cudaGetLastError();
+  cudaError_t e = launch_pdl(k_mg_resid_w<TS>, g3(df), dim3(32, 4, 2), 0, st,
+                             L{df.nx, df.ny, df.nz}, h * h, pf, bf, mf, L{dc.nx, dc.ny, dc.nz},
+                             mc, bc_mode, rt);
   if (e != cudaSuccess) return e;
-  k_mg_restrict_t<TS><<<g3(dc), dim3(32, 4, 2), 0, st>>>(L{df.nx, df.ny, df.nz}, rt, mf,
-                                                         L{dc.nx, dc.ny, dc.nz}, mc, bc, pc);
-  return cudaGetLastError();
+  return launch_pdl(k_mg_restrict_t<TS>, g3(dc), dim3(32, 4, 2), 0, st, L{df.nx, df.ny, df.nz},
+                    (const TS*)rt, mf, L{dc.nx, dc.ny, dc.nz}, mc, bc, pc);
 }
 
 cudaError_t launch_mg_restrict_sym(Dims3 df, float h, const float* pf, const float* bf,
@@ -763,15 +772,13 @@ cudaError_t launch_mg_restrict_sym_bf16(Dims3 df, float h, const void* pf, const
 }
 
 cudaError_t launch_mg_meta(Dims3 d, const uint32_t* f, uint8_t* meta, cudaStream_t st) {
-  k_mg_meta<<<g3(d), dim3(32, 4, 2), 0, st>>>(L{d.nx, d.ny, d.nz}, f, meta);
-  return cudaGetLastError();
+  return launch_pdl(k_mg_meta, g3(d), dim3(32, 4, 2), 0, st, L{d.nx, d.ny, d.nz}, f, meta);
 }
 
 cudaError_t launch_mg_flags_down(Dims3 df, const uint32_t* ff, Dims3 dc, uint32_t* fc,
                                  cudaStream_t st) {
-  k_mg_flags_down<<<g3(dc), dim3(32, 4, 2), 0, st>>>(L{df.nx, df.ny, df.nz}, ff,
-                                                    L{dc.nx, dc.ny, dc.nz}, fc);
-  return cudaGetLastError();
+  return launch_pdl(k_mg_flags_down, g3(dc), dim3(32, 4, 2), 0, st, L{df.nx, df.ny, df.nz}, ff,
+                    L{dc.nx, dc.ny, dc.nz}, fc);
 }
 
 cudaError_t launch_mg_rb(Dims3 d, float h, const float* b, const uint8_t* meta, const float* pin,
@@ -789,13 +796,9 @@ cudaError_t launch_mg_rb_restrict(Dims3 d, float h, const float* b, const uint8_
 template <typename TS>
 cudaError_t prolong_t(Dims3 df, const TS* pc, const uint8_t* mf, TS* pf, Dims3 dc,
                       const uint8_t* mc, cudaStream_t st) {
-  if (df.nx % 2 == 0)
-    k_mg_prolong_m<TS, true><<<g3(dc), dim3(32, 4, 2), 0, st>>>(L{df.nx, df.ny, df.nz}, pc, mf,
-                                                                pf, L{dc.nx, dc.ny, dc.nz}, mc);
-  else
-    k_mg_prolong_m<TS, false><<<g3(dc), dim3(32, 4, 2), 0, st>>>(L{df.nx, df.ny, df.nz}, pc, mf,
-                                                                 pf, L{dc.nx, dc.ny, dc.nz}, mc);
-  return cudaGetLastError();
+  auto kern = df.nx % 2 == 0 ? k_mg_prolong_m<TS, true> : k_mg_prolong_m<TS, false>;
+  return launch_pdl(kern, g3(dc), dim3(32, 4, 2), 0, st, L{df.nx, df.ny, df.nz}, pc, mf, pf,
+                    L{dc.nx, dc.ny, dc.nz}, mc);
 }
 
 cudaError_t launch_mg_prolong_m(Dims3 df, const float* pc, const uint8_t* mf, float* pf,
