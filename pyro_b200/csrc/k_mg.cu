@@ -306,11 +306,15 @@ __global__ void __launch_bounds__(COARSE_THREADS, 1)
 
 __global__ void k_f32_to_bf16(const float* __restrict__ a, __nv_bfloat16* __restrict__ b,
                               size_t n) {
+  pdl_trigger();
+  pdl_wait();
   size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (i < n) b[i] = __float2bfloat16_rn(a[i]);
 }
 __global__ void k_bf16_to_f32(const __nv_bfloat16* __restrict__ a, float* __restrict__ b,
                               size_t n) {
+  pdl_trigger();
+  pdl_wait();
   size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (i < n) b[i] = __bfloat162float(a[i]);
 }
@@ -440,12 +444,12 @@ cudaError_t launch_mg_coarse(Dims3 d, float h, const float* b, const uint32_t* f
 
 // ---- BF16-storage hierarchy (MGPCG preconditioner) -----------------------
 cudaError_t launch_f32_to_bf16(const float* a, void* b, size_t n, cudaStream_t st) {
-  k_f32_to_bf16<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a, (__nv_bfloat16*)b, n);
-  return cudaGetLastError();
+  return launch_pdl(k_f32_to_bf16, dim3((unsigned)((n + 255) / 256)), dim3(256), 0, st, a,
+                    (__nv_bfloat16*)b, n);
 }
 cudaError_t launch_bf16_to_f32(const void* a, float* b, size_t n, cudaStream_t st) {
-  k_bf16_to_f32<<<(unsigned)((n + 255) / 256), 256, 0, st>>>((const __nv_bfloat16*)a, b, n);
-  return cudaGetLastError();
+  return launch_pdl(k_bf16_to_f32, dim3((unsigned)((n + 255) / 256)), dim3(256), 0, st,
+                    (const __nv_bfloat16*)a, b, n);
 }
 cudaError_t launch_mg_smooth_bf16(Dims3 d, float h, const void* b, const uint32_t* f, void* p,
                                   int color, float omega, int bc_mode, cudaStream_t st) {

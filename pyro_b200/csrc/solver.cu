@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstring>
 
+#include "common.cuh"
 #include "net.h"
 #include "solver.h"
 
@@ -88,6 +89,8 @@ __global__ void __launch_bounds__(256) k_resid(L3 d, double ih2, const float* __
                                                const float* __restrict__ b,
                                                const uint32_t* __restrict__ f, int bc_mode,
                                                float* __restrict__ r, double* __restrict__ sc) {
+  pdl_trigger();
+  pdl_wait();
   __shared__ double sh[32];
   CELL_PROLOGUE
   double r2 = 0.0, b2 = 0.0;
@@ -110,6 +113,8 @@ __global__ void __launch_bounds__(256) k_apply_dot(L3 d, double ih2, const float
                                                    const uint32_t* __restrict__ f, int bc_mode,
                                                    float* __restrict__ q,
                                                    double* __restrict__ sc) {
+  pdl_trigger();
+  pdl_wait();
   __shared__ double sh[32];
   CELL_PROLOGUE
   double pq = 0.0;
@@ -133,6 +138,8 @@ __global__ void __launch_bounds__(256) k_update_xr(L3 d, const uint32_t* __restr
                                                    const float* __restrict__ p,
                                                    const float* __restrict__ q,
                                                    double* __restrict__ sc) {
+  pdl_trigger();
+  pdl_wait();
   __shared__ double sh[32];
   CELL_PROLOGUE
   double rr = 0.0;
@@ -152,6 +159,8 @@ __global__ void __launch_bounds__(256) k_dots(L3 d, const uint32_t* __restrict__
                                               const float* __restrict__ r,
                                               const float* __restrict__ q,
                                               double* __restrict__ sc) {
+  pdl_trigger();
+  pdl_wait();
   __shared__ double sh[32];
   CELL_PROLOGUE
   double zr = 0.0, zq = 0.0;
@@ -169,6 +178,8 @@ __global__ void __launch_bounds__(256) k_update_p(L3 d, const uint32_t* __restri
                                                   float* __restrict__ p,
                                                   const float* __restrict__ zv,
                                                   const double* __restrict__ sc, int first) {
+  pdl_trigger();
+  pdl_wait();
   CELL_PROLOGUE
   if (!in) return;
   if (!fluid) { p[i] = 0.0f; return; }
@@ -177,6 +188,8 @@ __global__ void __launch_bounds__(256) k_update_p(L3 d, const uint32_t* __restri
 }
 
 __global__ void k_roll(double* sc) {
+  pdl_trigger();
+  pdl_wait();
   // rz <- rz_new, clear the accumulators of the next iteration
   sc[SC_RZ] = sc[SC_RZN];
   sc[SC_RZN] = 0.0;
@@ -353,7 +366,7 @@ int Solver::true_resid(cudaStream_t st, const float* phi, const float* b, double
                        double* bn) {
   L3 l{d.nx, d.ny, d.nz};
   PYRO_CU(cudaMemsetAsync(sc.p, 0, SC_N * 8, st));
-  k_resid<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, 1.0 / ((double)mg->h[0] * mg->h[0]), phi, b,
+  launch_pdl(k_resid, grid_for(d), dim3(BX, BY, BZ), 0, st, l, 1.0 / ((double)mg->h[0] * mg->h[0]), phi, b,
                                                    mg->f[0], mg->bc_mode, nullptr,
                                                    sc.as<double>());
   PYRO_CU(cudaGetLastError());
@@ -391,9 +404,9 @@ int Solver::learned_stage(cudaStream_t st, float* phi, double* rr, PyroSolveInfo
       (rc = net->output(f0, mg->h[0], z.as<float>(), v, st)) || (rc = net->check_err(st)))
     return rc;
   PYRO_CU(cudaMemsetAsync(sc.p, 0, SC_N * 8, st));
-  k_apply_dot<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, ih2, z.as<float>(), f0, mg->bc_mode,
+  launch_pdl(k_apply_dot, grid_for(d), dim3(BX, BY, BZ), 0, st, l, ih2, z.as<float>(), f0, mg->bc_mode,
                                                        q.as<float>(), S);
-  k_dots<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, f0, z.as<float>(), r.as<float>(), nullptr,
+  launch_pdl(k_dots, grid_for(d), dim3(BX, BY, BZ), 0, st, l, f0, z.as<float>(), r.as<float>(), nullptr,
                                                   S);
   PYRO_CU(cudaGetLastError());
   PYRO_CU(cudaMemcpyAsync(host_sc, sc.p, SC_N * 8, cudaMemcpyDeviceToHost, st));
@@ -401,7 +414,7 @@ int Solver::learned_stage(cudaStream_t st, float* phi, double* rr, PyroSolveInfo
   const double re = host_sc[SC_RZN], eae = host_sc[SC_PQ];
   // <Ae, r>, <Ae, Ae>
   PYRO_CU(cudaMemsetAsync(sc.p, 0, SC_N * 8, st));
-  k_dots<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, f0, q.as<float>(), r.as<float>(),
+  launch_pdl(k_dots, grid_for(d), dim3(BX, BY, BZ), 0, st, l, f0, q.as<float>(), r.as<float>(),
                                                   q.as<float>(), S);
   PYRO_CU(cudaGetLastError());
   PYRO_CU(cudaMemcpyAsync(host_sc, sc.p, SC_N * 8, cudaMemcpyDeviceToHost, st));
@@ -415,7 +428,7 @@ int Solver::learned_stage(cudaStream_t st, float* phi, double* rr, PyroSolveInfo
     host_sc[SC_RZ] = re;
     host_sc[SC_PQ] = eae;
     PYRO_CU(cudaMemcpyAsync(sc.p, host_sc, SC_N * 8, cudaMemcpyHostToDevice, st));
-    k_update_xr<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, f0, phi, r.as<float>(),
+    launch_pdl(k_update_xr, grid_for(d), dim3(BX, BY, BZ), 0, st, l, f0, phi, r.as<float>(),
                                                          z.as<float>(), q.as<float>(), S);
     PYRO_CU(cudaGetLastError());
     PYRO_CU(cudaMemcpyAsync(host_sc, sc.p, SC_N * 8, cudaMemcpyDeviceToHost, st));
@@ -488,7 +501,7 @@ int Solver::solve(cudaStream_t st, float* phi, const float* b, int mode, float t
     } rebind{mg, save_phi, save_b, save_f0};
     // r = b - A phi, |r|, |b|
     PYRO_CU(cudaMemsetAsync(sc.p, 0, SC_N * 8, st));
-    k_resid<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, ih2, phi, b, f0, mg->bc_mode,
+    launch_pdl(k_resid, grid_for(d), dim3(BX, BY, BZ), 0, st, l, ih2, phi, b, f0, mg->bc_mode,
                                                      r.as<float>(), S);
     PYRO_CU(cudaGetLastError());
     PYRO_CU(cudaMemcpyAsync(host_sc, sc.p, SC_N * 8, cudaMemcpyDeviceToHost, st));
@@ -510,18 +523,18 @@ int Solver::solve(cudaStream_t st, float* phi, const float* b, int mode, float t
     int restarts = 0;
     while (rel > tol && iters < max_iters && restarts < 8) {
       PYRO_CU(precond(st, bf16));
-      k_dots<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, f0, z.as<float>(), r.as<float>(),
+      launch_pdl(k_dots, grid_for(d), dim3(BX, BY, BZ), 0, st, l, f0, z.as<float>(), r.as<float>(),
                                                       nullptr, S);
       PYRO_CU(cudaGetLastError());
-      k_roll<<<1, 1, 0, st>>>(S);
-      k_update_p<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, f0, p.as<float>(), z.as<float>(),
+      launch_pdl(k_roll, dim3(1), dim3(1), 0, st, S);
+      launch_pdl(k_update_p, grid_for(d), dim3(BX, BY, BZ), 0, st, l, f0, p.as<float>(), z.as<float>(),
                                                           S, 1);
       PYRO_CU(cudaGetLastError());
       bool stalled = false;
       while (iters < max_iters) {
-        k_apply_dot<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, ih2, p.as<float>(), f0,
+        launch_pdl(k_apply_dot, grid_for(d), dim3(BX, BY, BZ), 0, st, l, ih2, p.as<float>(), f0,
                                                              mg->bc_mode, q.as<float>(), S);
-        k_update_xr<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, f0, phi, r.as<float>(),
+        launch_pdl(k_update_xr, grid_for(d), dim3(BX, BY, BZ), 0, st, l, f0, phi, r.as<float>(),
                                                              p.as<float>(), q.as<float>(), S);
         PYRO_CU(cudaGetLastError());
         PYRO_CU(cudaMemcpyAsync(host_sc, sc.p, SC_N * 8, cudaMemcpyDeviceToHost, st));
@@ -534,16 +547,16 @@ int Solver::solve(cudaStream_t st, float* phi, const float* b, int mode, float t
         }
         if (bb2 > 0 && std::sqrt(rr / bb2) <= tol) break;
         PYRO_CU(precond(st, bf16));
-        k_dots<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, f0, z.as<float>(), r.as<float>(),
+        launch_pdl(k_dots, grid_for(d), dim3(BX, BY, BZ), 0, st, l, f0, z.as<float>(), r.as<float>(),
                                                         q.as<float>(), S);
-        k_update_p<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, f0, p.as<float>(),
+        launch_pdl(k_update_p, grid_for(d), dim3(BX, BY, BZ), 0, st, l, f0, p.as<float>(),
                                                             z.as<float>(), S, 0);
-        k_roll<<<1, 1, 0, st>>>(S);
+        launch_pdl(k_roll, dim3(1), dim3(1), 0, st, S);
         PYRO_CU(cudaGetLastError());
       }
       // true residual into r (and |r|, |b|)
       PYRO_CU(cudaMemsetAsync(sc.p, 0, SC_N * 8, st));
-      k_resid<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, ih2, phi, b, f0, mg->bc_mode,
+      launch_pdl(k_resid, grid_for(d), dim3(BX, BY, BZ), 0, st, l, ih2, phi, b, f0, mg->bc_mode,
                                                        r.as<float>(), S);
       PYRO_CU(cudaGetLastError());
       PYRO_CU(cudaMemcpyAsync(host_sc, sc.p, SC_N * 8, cudaMemcpyDeviceToHost, st));
