@@ -648,13 +648,17 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
 // --------------------------------------------------------- direct (CUDA cores)
 // Layers too narrow for the tensor cores to pay: 2 -> 16 channels (the
 // network's input layer, K = 54) and 16 -> 1 (its output layer, N = 1).
-// A thread computes DV consecutive voxels of an x-row, so every weight read
-// from shared memory (FP32, [tap][ci][co]) feeds DV fused multiply-adds.
-// FP32 accumulation over the taps in order (dz, dy, dx); a tap outside the
-// volume reads zero (zero padding).
-// voxels per thread: 4 for 2 -> 16 (weight reuse), 1 for 16 -> 1
+// A thread computes DV consecutive voxels of an x-row.  For every (dz, dy)
+// input row it loads the DV + 2 voxels x0-1 .. x0+DV once (zero outside
+// the volume), in chunks of CC input channels, and the three dx taps of
+// all DV outputs read them from registers; every weight read from shared
+// memory (FP32, [tap][ci][co]) feeds DV fused multiply-adds.  FP32
+// accumulation.
 template <int CIN, int COUT>
-constexpr int direct_dv() { return CIN == 2 ? 4 : 1; }
+struct DirectShape {
+  static constexpr int DV = 4;                  // voxels per thread
+  static constexpr int CC = CIN == 2 ? 2 : 8;   // input channels per chunk
+};
 
 template <int CIN, int COUT>
 __global__ void __launch_bounds__(256) k_conv_direct(const bf16* __restrict__ x, Vol g,
@@ -663,7 +667,7 @@ __global__ void __launch_bounds__(256) k_conv_direct(const bf16* __restrict__ x,
                                                      bf16* __restrict__ y_bf16,
                                                      float* __restrict__ y_f32) {
   static_assert(CIN == 2 || CIN % 8 == 0, "input rows are loaded as 4- or 16-byte chunks");
-  constexpr int DV = direct_dv<CIN, COUT>();
+  constexpr int DV = DirectShape<CIN, COUT>::DV, CC = DirectShape<CIN, COUT>::CC;
   __shared__ __align__(16) float ws[27 * CIN * COUT];
   for (int i = threadIdx.x; i < 27 * CIN * COUT; i += blockDim.x) {
     const int co = i / (27 * CIN), t = (i / CIN) % 27, ci = i % CIN;  // w[co][t][ci]
@@ -692,44 +696,45 @@ __global__ void __launch_bounds__(256) k_conv_direct(const bf16* __restrict__ x,
 #pragma unroll 1
     for (int dy = -1; dy <= 1; dy++) {
       if ((unsigned)(yy + dy) >= (unsigned)g.ny) continue;
+      const long vr = v0 + sy * dy + sz * dz;  // voxel x0 of the input row
 #pragma unroll
-      for (int dx = -1; dx <= 1; dx++) {
-        const int t = (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
-        float xin[DV][CIN];
+      for (int c0 = 0; c0 < CIN; c0 += CC) {
+        float xin[DV + 2][CC];
 #pragma unroll
-        for (int i = 0; i < DV; i++) {
-          const int xs = x0 + i + dx;
+        for (int i = 0; i < DV + 2; i++) {
+          const int xs = x0 - 1 + i;
           const bool in = (unsigned)xs < (unsigned)g.nx;
-          const long vs = v0 + i + dx + sy * dy + sz * dz;
+          const long vs = vr - 1 + i;
           if constexpr (CIN == 2) {
             float2 f = make_float2(0.0f, 0.0f);
             if (in) f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(x + vs * 2));
             xin[i][0] = f.x;
             xin[i][1] = f.y;
           } else {
+            uint4 u = make_uint4(0, 0, 0, 0);
+            if (in) u = __ldg(reinterpret_cast<const uint4*>(x + act_off(vs, c0, CIN, V)));
+            const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
 #pragma unroll
-            for (int c8 = 0; c8 < CIN; c8 += 8) {
-              uint4 u = make_uint4(0, 0, 0, 0);
-              if (in) u = __ldg(reinterpret_cast<const uint4*>(x + act_off(vs, c8, CIN, V)));
-              const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
-#pragma unroll
-              for (int j = 0; j < 4; j++) {
-                const float2 f = __bfloat1622float2(h[j]);
-                xin[i][c8 + 2 * j] = f.x;
-                xin[i][c8 + 2 * j + 1] = f.y;
-              }
+            for (int j = 0; j < 4; j++) {
+              const float2 f = __bfloat1622float2(h[j]);
+              xin[i][2 * j] = f.x;
+              xin[i][2 * j + 1] = f.y;
             }
           }
         }
-        const float* wt = ws + t * CIN * COUT;
 #pragma unroll
-        for (int ci = 0; ci < CIN; ci++)
+        for (int dx = 0; dx < 3; dx++) {
+          const float* wt = ws + ((dx + 3 * (dy + 1) + 9 * (dz + 1)) * CIN + c0) * COUT;
 #pragma unroll
-          for (int co = 0; co < COUT; co++) {
-            const float wv = wt[ci * COUT + co];
+          for (int ci = 0; ci < CC; ci++)
 #pragma unroll
-            for (int i = 0; i < DV; i++) acc[i][co] = __fmaf_rn(xin[i][ci], wv, acc[i][co]);
-          }
+            for (int co = 0; co < COUT; co++) {
+              const float wv = wt[ci * COUT + co];
+#pragma unroll
+              for (int i = 0; i < DV; i++)
+                acc[i][co] = __fmaf_rn(xin[i + dx][ci], wv, acc[i][co]);
+            }
+        }
       }
     }
   }
@@ -897,11 +902,11 @@ cudaError_t conv3_direct(const bf16* x, int C, int nx, int ny, int nz, int nb, c
     return (unsigned)(((long)((nx + dv - 1) / dv) * ny * nz * nb + 255) / 256);
   };
   if (C == 2 && Cout == 16)
-    k_conv_direct<2, 16><<<blocks(direct_dv<2, 16>()), 256, 0, st>>>(x, g, w, bias, relu, y_bf16,
-                                                                     y_f32);
+    k_conv_direct<2, 16><<<blocks(DirectShape<2, 16>::DV), 256, 0, st>>>(x, g, w, bias, relu,
+                                                                         y_bf16, y_f32);
   else if (C == 16 && Cout == 1)
-    k_conv_direct<16, 1><<<blocks(direct_dv<16, 1>()), 256, 0, st>>>(x, g, w, bias, relu, y_bf16,
-                                                                     y_f32);
+    k_conv_direct<16, 1><<<blocks(DirectShape<16, 1>::DV), 256, 0, st>>>(x, g, w, bias, relu,
+                                                                         y_bf16, y_f32);
   else
     return cudaErrorInvalidValue;
   return cudaGetLastError();

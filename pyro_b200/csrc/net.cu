@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(NT) k_upcat(const bf16* __restrict__ a, int Ca
                                               const bf16* __restrict__ skip, int Cb, Dv fd,
                                               bf16* __restrict__ out) {
   Dv cd{(fd.nx + 1) / 2, (fd.ny + 1) / 2, (fd.nz + 1) / 2, fd.nb};
-  const int Ct = Ca + Cb, ch = Ct / 8;
+  const int Ct = Ca + Cb, ch = (skip ? Ct : Ca) / 8;  // skip null: already in place
   GRID_LOOP(i, fd.voxels() * ch) {
     const size_t fv = i % fd.voxels();
     const int c = (int)(i / fd.voxels()) * 8;
@@ -464,8 +464,8 @@ int PyroNet::ensure(NetVol v, bool bwd) {
     DevBuf* b;
     size_t n;
   };
-  std::vector<A> fw = {{&in0, V0 * 2},  {&e0a, V0 * 16}, {&e0, V0 * 16}, {&p1, V1 * 16},
-                       {&e1a, V1 * 32}, {&e1, V1 * 32},  {&p2, V2 * 32}, {&e2a, V2 * 64},
+  std::vector<A> fw = {{&in0, V0 * 2},  {&e0a, V0 * 16}, {&p1, V1 * 16},
+                       {&e1a, V1 * 32}, {&p2, V2 * 32}, {&e2a, V2 * 64},
                        {&e2, V2 * 64},  {&c1, V1 * 96},  {&d1, V1 * 32}, {&c0, V0 * 48},
                        {&d0, V0 * 16}};
   std::vector<A> bw = {{&g9, V0 * 1},   {&g8, V0 * 16}, {&gc0, V0 * 48}, {&g7, V1 * 32},
@@ -511,32 +511,33 @@ int PyroNet::forward(const float* b, const uint32_t* flags, NetVol v, cudaStream
   k_input<<<blocks_for(cells * v.nb), NT, 0, st>>>(b, flags, cells, v.nb, S,
                                                    in0.as<__nv_bfloat162>());
   NET_CU(cudaGetLastError());
-  auto conv = [&](const DevBuf& x, int l, NetVol g, DevBuf* y, float* yf) -> cudaError_t {
+  auto conv = [&](const bf16* x, int l, NetVol g, bf16* y, float* yf) -> cudaError_t {
     const NetLayer& L = NET_SPEC[l];
     if (conv3_direct_fits(L.cin, L.cout))
-      return conv3_direct(x.as<bf16>(), L.cin, g.nx, g.ny, g.nz, g.nb, w(l), L.cout, bias(l),
-                          L.relu, y ? y->as<bf16>() : nullptr, yf, st);
+      return conv3_direct(x, L.cin, g.nx, g.ny, g.nz, g.nb, w(l), L.cout, bias(l), L.relu, y, yf,
+                          st);
     if (L.cin % 16 == 0)
-      return conv3_tma(x.as<bf16>(), L.cin, g.nx, g.ny, g.nz, g.nb, wf(l), L.cout, bias(l),
-                       L.relu, nullptr, y ? y->as<bf16>() : nullptr, yf, E, st);
-    return conv3_forward(x.as<bf16>(), L.cin, g.nx, g.ny, g.nz, g.nb, w(l), L.cout, bias(l),
-                         L.relu, y ? y->as<bf16>() : nullptr, yf, E, st);
+      return conv3_tma(x, L.cin, g.nx, g.ny, g.nz, g.nb, wf(l), L.cout, bias(l), L.relu, nullptr,
+                       y, yf, E, st);
+    return conv3_forward(x, L.cin, g.nx, g.ny, g.nz, g.nb, w(l), L.cout, bias(l), L.relu, y, yf,
+                         E, st);
   };
-  NET_CU(conv(in0, 0, v, &e0a, nullptr));
-  NET_CU(conv(e0a, 1, v, &e0, nullptr));
-  k_pool<<<blocks_for(v1.voxels() * 2), NT, 0, st>>>(e0.as<bf16>(), 16, dv(v), p1.as<bf16>());
-  NET_CU(conv(p1, 2, v1, &e1a, nullptr));
-  NET_CU(conv(e1a, 3, v1, &e1, nullptr));
-  k_pool<<<blocks_for(v2.voxels() * 4), NT, 0, st>>>(e1.as<bf16>(), 32, dv(v1), p2.as<bf16>());
-  NET_CU(conv(p2, 4, v2, &e2a, nullptr));
-  NET_CU(conv(e2a, 5, v2, &e2, nullptr));
-  k_upcat<<<blocks_for(v1.voxels() * 12), NT, 0, st>>>(e2.as<bf16>(), 64, e1.as<bf16>(), 32,
-                                                       dv(v1), c1.as<bf16>());
-  NET_CU(conv(c1, 6, v1, &d1, nullptr));
-  k_upcat<<<blocks_for(v.voxels() * 6), NT, 0, st>>>(d1.as<bf16>(), 32, e0.as<bf16>(), 16, dv(v),
-                                                     c0.as<bf16>());
-  NET_CU(conv(c0, 7, v, &d0, nullptr));
-  NET_CU(conv(d0, 8, v, nullptr, out.as<float>()));
+  auto B = [](const DevBuf& d) { return d.as<bf16>(); };
+  // the skip connections e0, e1 are written straight into their planes of
+  // the concatenations c0, c1
+  NET_CU(conv(B(in0), 0, v, B(e0a), nullptr));
+  NET_CU(conv(B(e0a), 1, v, skip0(), nullptr));
+  k_pool<<<blocks_for(v1.voxels() * 2), NT, 0, st>>>(skip0(), 16, dv(v), B(p1));
+  NET_CU(conv(B(p1), 2, v1, B(e1a), nullptr));
+  NET_CU(conv(B(e1a), 3, v1, skip1(), nullptr));
+  k_pool<<<blocks_for(v2.voxels() * 4), NT, 0, st>>>(skip1(), 32, dv(v1), B(p2));
+  NET_CU(conv(B(p2), 4, v2, B(e2a), nullptr));
+  NET_CU(conv(B(e2a), 5, v2, B(e2), nullptr));
+  k_upcat<<<blocks_for(v1.voxels() * 8), NT, 0, st>>>(B(e2), 64, nullptr, 32, dv(v1), B(c1));
+  NET_CU(conv(B(c1), 6, v1, B(d1), nullptr));
+  k_upcat<<<blocks_for(v.voxels() * 4), NT, 0, st>>>(B(d1), 32, nullptr, 16, dv(v), B(c0));
+  NET_CU(conv(B(c0), 7, v, B(d0), nullptr));
+  NET_CU(conv(B(d0), 8, v, nullptr, out.as<float>()));
   return PYRO_OK;
 }
 
@@ -598,14 +599,14 @@ int PyroNet::loss_backward(const float* b, const uint32_t* flags, const float* p
   NET_CU(wg(p2, g5, 4, v2));
   NET_CU(bd(g5, 4, v2, nullptr, gp2));
   k_poolback<<<blocks_for(v1.voxels() * 4), NT, 0, st>>>(gp2.as<bf16>(), 32, gc1.as<bf16>(), 96,
-                                                         64, e1.as<bf16>(), dv(v1),
+                                                         64, skip1(), dv(v1),
                                                          g4.as<bf16>());
   NET_CU(wg(e1a, g4, 3, v1));
   NET_CU(bd(g4, 3, v1, &e1a, g3));
   NET_CU(wg(p1, g3, 2, v1));
   NET_CU(bd(g3, 2, v1, nullptr, gp1));
   k_poolback<<<blocks_for(v.voxels() * 2), NT, 0, st>>>(gp1.as<bf16>(), 16, gc0.as<bf16>(), 48,
-                                                        32, e0.as<bf16>(), dv(v), g2.as<bf16>());
+                                                        32, skip0(), dv(v), g2.as<bf16>());
   NET_CU(wg(e0a, g2, 1, v));
   NET_CU(bd(g2, 1, v, &e0a, g1));
   NET_CU(wg(in0, g1, 0, v));

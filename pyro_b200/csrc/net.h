@@ -90,7 +90,13 @@ struct PyroNet {
   // activation buffers for the current volume shape
   pyro::NetVol vol{0, 0, 0, 0};
   bool has_bwd = false;
-  pyro::DevBuf in0, e0a, e0, p1, e1a, e1, p2, e2a, e2, c1, d1, c0, d0, out, res;
+  pyro::DevBuf in0, e0a, p1, e1a, p2, e2a, e2, c1, d1, c0, d0, out, res;
+  // skip activations e0 (16 channels, level 0) and e1 (32, level 1): the
+  // last 2 / 4 planes of the concatenations c0 / c1
+  __nv_bfloat16* skip0() const { return c0.as<__nv_bfloat16>() + (size_t)4 * vol.voxels() * 8; }
+  __nv_bfloat16* skip1() const {
+    return c1.as<__nv_bfloat16>() + (size_t)8 * vol.half().voxels() * 8;
+  }
   pyro::DevBuf g9, g8, gc0, g7, gc1, g6, g5, gp2, g4, g3, gp1, g2, g1;
   cudaStream_t stream = nullptr;
 
