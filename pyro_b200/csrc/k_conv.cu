@@ -661,7 +661,7 @@ struct DirectShape {
 };
 
 template <int CIN, int COUT>
-__global__ void __launch_bounds__(256) k_conv_direct(const bf16* __restrict__ x, Vol g,
+__global__ void __launch_bounds__(256, 2) k_conv_direct(const bf16* __restrict__ x, Vol g,
                                                      const bf16* __restrict__ w,
                                                      const float* __restrict__ bias, int relu,
                                                      bf16* __restrict__ y_bf16,

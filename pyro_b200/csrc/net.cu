@@ -54,13 +54,14 @@ __device__ __forceinline__ double vol_rms(const double* sc, int vol) {
 
 struct Dv {  // volume dims on the device
   int nx, ny, nz, nb;
+  // 32-bit arithmetic: a volume set holds fewer than 2^31 voxels (ensure())
   __device__ __forceinline__ void coords(size_t v, int& x, int& y, int& z, int& b) const {
-    x = (int)(v % nx);
-    size_t r = v / nx;
-    y = (int)(r % ny);
-    r /= ny;
-    z = (int)(r % nz);
-    b = (int)(r / nz);
+    const uint32_t u = (uint32_t)v, r1 = u / (uint32_t)nx, r2 = r1 / (uint32_t)ny,
+                   r3 = r2 / (uint32_t)nz;
+    x = (int)(u - r1 * (uint32_t)nx);
+    y = (int)(r1 - r2 * (uint32_t)ny);
+    z = (int)(r2 - r3 * (uint32_t)nz);
+    b = (int)r3;
   }
   __device__ __forceinline__ size_t idx(int x, int y, int z, int b) const {
     return (((size_t)b * nz + z) * ny + y) * nx + x;
@@ -68,6 +69,19 @@ struct Dv {  // volume dims on the device
   __device__ __forceinline__ size_t voxels() const { return (size_t)nx * ny * nz * nb; }
 };
 inline Dv dv(NetVol v) { return Dv{v.nx, v.ny, v.nz, v.nb}; }
+
+// Flat index i over (plane p, voxel v) of V voxels per plane, with 32-bit
+// division when i fits.
+__device__ __forceinline__ void plane_split(size_t i, size_t V, size_t& v, int& p) {
+  if (i <= 0xFFFFFFFFull) {
+    const uint32_t q = (uint32_t)i / (uint32_t)V;
+    p = (int)q;
+    v = (uint32_t)i - q * (uint32_t)V;
+  } else {
+    p = (int)(i / V);
+    v = i - (size_t)p * V;
+  }
+}
 
 // Activation layout: a tensor of C channels over V voxels with C a multiple
 // of 8 is stored as C / 8 planes of [V][8 channels] (a plane is one 16-byte
@@ -141,8 +155,9 @@ __global__ void __launch_bounds__(NT) k_pool(const bf16* __restrict__ in, int C,
   Dv cd{(fd.nx + 1) / 2, (fd.ny + 1) / 2, (fd.nz + 1) / 2, fd.nb};
   const int ch = C / 8;
   GRID_LOOP(i, cd.voxels() * ch) {
-    const size_t cv = i % cd.voxels();
-    const int c8 = (int)(i / cd.voxels());
+    size_t cv;
+    int c8;
+    plane_split(i, cd.voxels(), cv, c8);
     int x, y, z, b;
     cd.coords(cv, x, y, z, b);
     float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -174,8 +189,10 @@ __global__ void __launch_bounds__(NT) k_upcat(const bf16* __restrict__ a, int Ca
   Dv cd{(fd.nx + 1) / 2, (fd.ny + 1) / 2, (fd.nz + 1) / 2, fd.nb};
   const int Ct = Ca + Cb, ch = (skip ? Ct : Ca) / 8;  // skip null: already in place
   GRID_LOOP(i, fd.voxels() * ch) {
-    const size_t fv = i % fd.voxels();
-    const int c = (int)(i / fd.voxels()) * 8;
+    size_t fv;
+    int c;
+    plane_split(i, fd.voxels(), fv, c);
+    c *= 8;
     uint4 u;
     if (c < Ca) {
       int x, y, z, b;
@@ -195,8 +212,10 @@ __global__ void __launch_bounds__(NT) k_upback(const bf16* __restrict__ dc, int 
   Dv cd{(fd.nx + 1) / 2, (fd.ny + 1) / 2, (fd.nz + 1) / 2, fd.nb};
   const int ch = Ca / 8;
   GRID_LOOP(i, cd.voxels() * ch) {
-    const size_t cv = i % cd.voxels();
-    const int c = (int)(i / cd.voxels()) * 8;
+    size_t cv;
+    int c;
+    plane_split(i, cd.voxels(), cv, c);
+    c *= 8;
     int x, y, z, b;
     cd.coords(cv, x, y, z, b);
     float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -226,8 +245,10 @@ __global__ void __launch_bounds__(NT) k_poolback(const bf16* __restrict__ dp, in
   Dv cd{(fd.nx + 1) / 2, (fd.ny + 1) / 2, (fd.nz + 1) / 2, fd.nb};
   const int ch = C / 8;
   GRID_LOOP(i, fd.voxels() * ch) {
-    const size_t fv = i % fd.voxels();
-    const int c = (int)(i / fd.voxels()) * 8;
+    size_t fv;
+    int c;
+    plane_split(i, fd.voxels(), fv, c);
+    c *= 8;
     int x, y, z, b;
     fd.coords(fv, x, y, z, b);
     int px = x >> 1, py = y >> 1, pz = z >> 1;

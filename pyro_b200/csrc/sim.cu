@@ -48,6 +48,9 @@ struct PyroSim {
 
   PyroParams* ring = nullptr;  // pinned
   cudaEvent_t ring_ev[PARAM_RING] = {};
+  // auxiliary streams and events of the substep's independent branches
+  cudaStream_t aux[3] = {};
+  cudaEvent_t fork_ev = nullptr, join_ev[3] = {};
   int ring_pos = 0;
   float* staging = nullptr;  // pinned stats copy
 
@@ -64,6 +67,11 @@ struct PyroSim {
         if (g) cudaGraphExecDestroy(g);
     for (auto& e : ring_ev)
       if (e) cudaEventDestroy(e);
+    for (auto& e : join_ev)
+      if (e) cudaEventDestroy(e);
+    if (fork_ev) cudaEventDestroy(fork_ev);
+    for (auto& a : aux)
+      if (a) cudaStreamDestroy(a);
     if (ring) cudaFreeHost(ring);
     if (staging) cudaFreeHost(staging);
     if (stream) cudaStreamDestroy(stream);
@@ -81,25 +89,37 @@ struct PyroSim {
     float4* sb = sol[1 - c].as<float4>();
     const float *ua = vp(c, 0), *va = vp(c, 1), *wa = vp(c, 2);
     float *ub = vp(1 - c, 0), *vb = vp(1 - c, 1), *wb = vp(1 - c, 2);
+    // Three independent branches run on auxiliary streams (parallel
+    // branches of the captured graph): curl; adv_vel1; adv_s1 -> adv_s2.
+    // solid stays on st.  adv_vel2 needs solid's flags and adv_vel1's
+    // predictor, react needs curl and adv_s2.  None of them writes what
+    // another branch reads (sol[c], s0, s1 and vel[c] are only read).
+    if ((e = cudaEventRecord(fork_ev, st)) != cudaSuccess) return e;
+    for (auto& a : aux)
+      if ((e = cudaStreamWaitEvent(a, fork_ev, 0)) != cudaSuccess) return e;
+    if ((e = launch_curl(P, d, ua, va, wa, curl.as<float4>(), S, aux[0])) != cudaSuccess) return e;
+    if ((e = launch_adv_vel1(P, d, ua, va, wa, hat[0].as<float>(), hat[1].as<float>(),
+                             hat[2].as<float>(), lohi.as<float>(), aux[1])) != cudaSuccess)
+      return e;
+    if ((e = launch_adv_s1(P, d, ua, va, wa, s0.as<float4>(), s1.as<float4>(), h0.as<float4>(),
+                           h1.as<float4>(), aux[2])) != cudaSuccess)
+      return e;
+    if ((e = launch_adv_s2(P, d, ua, va, wa, s0.as<float4>(), s1.as<float4>(), h0.as<float4>(),
+                           h1.as<float4>(), s0b.as<float4>(), s1b.as<float4>(), aux[2])) !=
+        cudaSuccess)
+      return e;
+    for (int k = 0; k < 3; k++)
+      if ((e = cudaEventRecord(join_ev[k], aux[k])) != cudaSuccess) return e;
     if ((e = launch_solid(P, d, sa, sb, pyr.as<float4>(), flags.as<uint32_t>(), s0.as<float4>(),
                           S, st)) != cudaSuccess)
       return e;
-    if ((e = launch_curl(P, d, ua, va, wa, curl.as<float4>(), S, st)) != cudaSuccess) return e;
-    if ((e = launch_adv_vel1(P, d, ua, va, wa, hat[0].as<float>(), hat[1].as<float>(),
-                             hat[2].as<float>(), lohi.as<float>(), st)) != cudaSuccess)
-      return e;
+    if ((e = cudaStreamWaitEvent(st, join_ev[1], 0)) != cudaSuccess) return e;
     if ((e = launch_adv_vel2(P, d, ua, va, wa, hat[0].as<float>(), hat[1].as<float>(),
                              hat[2].as<float>(), lohi.as<float>(), ub, vb, wb,
-                             flags.as<uint32_t>(), st)) !=
-        cudaSuccess)
+                             flags.as<uint32_t>(), st)) != cudaSuccess)
       return e;
-    if ((e = launch_adv_s1(P, d, ua, va, wa, s0.as<float4>(), s1.as<float4>(), h0.as<float4>(),
-                           h1.as<float4>(), st)) != cudaSuccess)
-      return e;
-    if ((e = launch_adv_s2(P, d, ua, va, wa, s0.as<float4>(), s1.as<float4>(), h0.as<float4>(),
-                           h1.as<float4>(), s0b.as<float4>(), s1b.as<float4>(), st)) !=
-        cudaSuccess)
-      return e;
+    if ((e = cudaStreamWaitEvent(st, join_ev[0], 0)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(st, join_ev[2], 0)) != cudaSuccess) return e;
     if ((e = launch_react(P, d, s0b.as<float4>(), s1b.as<float4>(), s0.as<float4>(),
                           s1.as<float4>(), flags.as<uint32_t>(), sb, pyr.as<float4>(),
                           curl.as<float4>(), S, st)) != cudaSuccess)
@@ -246,6 +266,20 @@ int pyro_sim_create(const PyroParams* params, const float* sol_init, uint32_t pr
   }
   std::memset(S->staging, 0, PYRO_STATS_N * 4);
   for (auto& e : S->ring_ev)
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+      set_error("pyro_sim_create: cudaEventCreate failed");
+      return fail(PYRO_E_CUDA);
+    }
+  for (auto& a : S->aux)
+    if (cudaStreamCreateWithFlags(&a, cudaStreamNonBlocking) != cudaSuccess) {
+      set_error("pyro_sim_create: cudaStreamCreate failed");
+      return fail(PYRO_E_CUDA);
+    }
+  if (cudaEventCreateWithFlags(&S->fork_ev, cudaEventDisableTiming) != cudaSuccess) {
+    set_error("pyro_sim_create: cudaEventCreate failed");
+    return fail(PYRO_E_CUDA);
+  }
+  for (auto& e : S->join_ev)
     if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
       set_error("pyro_sim_create: cudaEventCreate failed");
       return fail(PYRO_E_CUDA);
