@@ -28,6 +28,18 @@ inline dim3 grid_for(Dims3 d) {
 
 enum { SC_RZ = 0, SC_PQ, SC_RR, SC_BB, SC_ZQ, SC_RZN, SC_N = 8 };
 
+unsigned vec_blocks(size_t n) {
+  static int nsm = 0;
+  if (nsm <= 0) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        nsm <= 0)
+      nsm = 148;
+  }
+  return (unsigned)std::min<size_t>((n + 255) / 256, (size_t)nsm * 8);
+}
+
 __device__ __forceinline__ double warp_sum_d(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -85,23 +97,47 @@ __device__ __forceinline__ double apply_A(const L3& d, double ih2, const float* 
   int i = in ? d.idx(x, y, z) : 0;             \
   bool fluid = in && __ldg(f + i) != 1u;
 
-__global__ void __launch_bounds__(256) k_resid(L3 d, double ih2, const float* __restrict__ phi,
-                                               const float* __restrict__ b,
-                                               const uint32_t* __restrict__ f, int bc_mode,
-                                               float* __restrict__ r, double* __restrict__ sc) {
+// The CG vector kernels run on a 1-D grid capped at 8 blocks per SM; each
+// thread strides over the cells, so a kernel's block sums meet in ~1,200
+// FP64 atomics instead of one per 256 cells (32,000 at 8.2 M cells, which
+// serialised on one address).
+constexpr int VT = 256;
+struct Cells {
+  L3 d;
+  FastDiv by_nx, by_plane;
+  int n;
+  __device__ __forceinline__ void coords(int i, int& x, int& y, int& z) const {
+    z = (int)by_plane.div((uint32_t)i);
+    const int r = i - z * d.nx * d.ny;
+    y = (int)by_nx.div((uint32_t)r);
+    x = r - y * d.nx;
+  }
+};
+inline Cells cells_of(Dims3 d) {
+  return Cells{L3{d.nx, d.ny, d.nz}, FastDiv((uint32_t)d.nx), FastDiv((uint32_t)(d.nx * d.ny)),
+               (int)d.cells()};
+}
+#define CELL_LOOP(i) \
+  for (int i = blockIdx.x * VT + threadIdx.x; i < c.n; i += gridDim.x * VT)
+
+__global__ void __launch_bounds__(VT) k_resid(Cells c, double ih2, const float* __restrict__ phi,
+                                              const float* __restrict__ b,
+                                              const uint32_t* __restrict__ f, int bc_mode,
+                                              float* __restrict__ r, double* __restrict__ sc) {
   pdl_trigger();
   pdl_wait();
   __shared__ double sh[32];
-  CELL_PROLOGUE
   double r2 = 0.0, b2 = 0.0;
-  if (in) {
+  CELL_LOOP(i) {
     float ri = 0.0f;
-    if (fluid) {
+    if (__ldg(f + i) != 1u) {
+      int x, y, z;
+      c.coords(i, x, y, z);
       float bi = __ldg(b + i);
-      double rd = (double)bi - apply_A(d, ih2, phi, f, x, y, z, bc_mode, __ldg(phi + i));
+      double rd = (double)bi - apply_A(c.d, ih2, phi, f, x, y, z, bc_mode, __ldg(phi + i));
       ri = (float)rd;
-      r2 = rd * rd;
-      b2 = (double)bi * (double)bi;
+      r2 += rd * rd;
+      b2 += (double)bi * (double)bi;
     }
     if (r) r[i] = ri;
   }
@@ -109,22 +145,23 @@ __global__ void __launch_bounds__(256) k_resid(L3 d, double ih2, const float* __
   block_add_d(sh, b2, sc + SC_BB);
 }
 
-__global__ void __launch_bounds__(256) k_apply_dot(L3 d, double ih2, const float* __restrict__ p,
-                                                   const uint32_t* __restrict__ f, int bc_mode,
-                                                   float* __restrict__ q,
-                                                   double* __restrict__ sc) {
+__global__ void __launch_bounds__(VT) k_apply_dot(Cells c, double ih2, const float* __restrict__ p,
+                                                  const uint32_t* __restrict__ f, int bc_mode,
+                                                  float* __restrict__ q,
+                                                  double* __restrict__ sc) {
   pdl_trigger();
   pdl_wait();
   __shared__ double sh[32];
-  CELL_PROLOGUE
   double pq = 0.0;
-  if (in) {
+  CELL_LOOP(i) {
     float qi = 0.0f;
-    if (fluid) {
+    if (__ldg(f + i) != 1u) {
+      int x, y, z;
+      c.coords(i, x, y, z);
       float pi = __ldg(p + i);
-      double qd = apply_A(d, ih2, p, f, x, y, z, bc_mode, pi);
+      double qd = apply_A(c.d, ih2, p, f, x, y, z, bc_mode, pi);
       qi = (float)qd;
-      pq = (double)pi * qd;
+      pq += (double)pi * qd;
     }
     q[i] = qi;
   }
@@ -132,59 +169,68 @@ __global__ void __launch_bounds__(256) k_apply_dot(L3 d, double ih2, const float
 }
 
 // phi += alpha p; r -= alpha q; accumulate |r|^2
-__global__ void __launch_bounds__(256) k_update_xr(L3 d, const uint32_t* __restrict__ f,
-                                                   float* __restrict__ phi,
-                                                   float* __restrict__ r,
-                                                   const float* __restrict__ p,
-                                                   const float* __restrict__ q,
-                                                   double* __restrict__ sc) {
+__global__ void __launch_bounds__(VT) k_update_xr(Cells c, const uint32_t* __restrict__ f,
+                                                  float* __restrict__ phi,
+                                                  float* __restrict__ r,
+                                                  const float* __restrict__ p,
+                                                  const float* __restrict__ q,
+                                                  double* __restrict__ sc) {
   pdl_trigger();
   pdl_wait();
   __shared__ double sh[32];
-  CELL_PROLOGUE
+  __shared__ float s_alpha;
+  if (threadIdx.x == 0) s_alpha = (float)(sc[SC_RZ] / sc[SC_PQ]);
+  __syncthreads();
+  const float alpha = s_alpha;
   double rr = 0.0;
-  if (fluid) {
-    float alpha = (float)(sc[SC_RZ] / sc[SC_PQ]);
+  CELL_LOOP(i) {
+    if (__ldg(f + i) == 1u) continue;
     phi[i] += alpha * p[i];
     float ri = r[i] - alpha * q[i];
     r[i] = ri;
-    rr = (double)ri * (double)ri;
+    rr += (double)ri * (double)ri;
   }
   block_add_d(sh, rr, sc + SC_RR);
 }
 
 // <z,r> -> SC_RZN and, when q is given, <z,q> -> SC_ZQ
-__global__ void __launch_bounds__(256) k_dots(L3 d, const uint32_t* __restrict__ f,
-                                              const float* __restrict__ zv,
-                                              const float* __restrict__ r,
-                                              const float* __restrict__ q,
-                                              double* __restrict__ sc) {
+__global__ void __launch_bounds__(VT) k_dots(Cells c, const uint32_t* __restrict__ f,
+                                             const float* __restrict__ zv,
+                                             const float* __restrict__ r,
+                                             const float* __restrict__ q,
+                                             double* __restrict__ sc) {
   pdl_trigger();
   pdl_wait();
   __shared__ double sh[32];
-  CELL_PROLOGUE
   double zr = 0.0, zq = 0.0;
-  if (fluid) {
+  CELL_LOOP(i) {
+    if (__ldg(f + i) == 1u) continue;
     float zi = zv[i];
-    zr = (double)zi * (double)r[i];
-    if (q) zq = (double)zi * (double)q[i];
+    zr += (double)zi * (double)r[i];
+    if (q) zq += (double)zi * (double)q[i];
   }
   block_add_d(sh, zr, sc + SC_RZN);
   if (q) block_add_d(sh, zq, sc + SC_ZQ);
 }
 
 // p = z + beta p with beta = -<z,q>/<p,q> (first iteration: p = z)
-__global__ void __launch_bounds__(256) k_update_p(L3 d, const uint32_t* __restrict__ f,
-                                                  float* __restrict__ p,
-                                                  const float* __restrict__ zv,
-                                                  const double* __restrict__ sc, int first) {
+__global__ void __launch_bounds__(VT) k_update_p(Cells c, const uint32_t* __restrict__ f,
+                                                 float* __restrict__ p,
+                                                 const float* __restrict__ zv,
+                                                 const double* __restrict__ sc, int first) {
   pdl_trigger();
   pdl_wait();
-  CELL_PROLOGUE
-  if (!in) return;
-  if (!fluid) { p[i] = 0.0f; return; }
-  float beta = first ? 0.0f : (float)(-sc[SC_ZQ] / sc[SC_PQ]);
-  p[i] = first ? zv[i] : zv[i] + beta * p[i];
+  __shared__ float s_beta;
+  if (threadIdx.x == 0) s_beta = first ? 0.0f : (float)(-sc[SC_ZQ] / sc[SC_PQ]);
+  __syncthreads();
+  const float beta = s_beta;
+  CELL_LOOP(i) {
+    if (__ldg(f + i) == 1u) {
+      p[i] = 0.0f;
+      continue;
+    }
+    p[i] = first ? zv[i] : zv[i] + beta * p[i];
+  }
 }
 
 __global__ void k_roll(double* sc) {
@@ -366,7 +412,7 @@ int Solver::true_resid(cudaStream_t st, const float* phi, const float* b, double
                        double* bn) {
   L3 l{d.nx, d.ny, d.nz};
   PYRO_CU(cudaMemsetAsync(sc.p, 0, SC_N * 8, st));
-  launch_pdl(k_resid, grid_for(d), dim3(BX, BY, BZ), 0, st, l, 1.0 / ((double)mg->h[0] * mg->h[0]), phi, b,
+  launch_pdl(k_resid, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), 1.0 / ((double)mg->h[0] * mg->h[0]), phi, b,
                                                    mg->f[0], mg->bc_mode, nullptr,
                                                    sc.as<double>());
   PYRO_CU(cudaGetLastError());
@@ -404,9 +450,9 @@ int Solver::learned_stage(cudaStream_t st, float* phi, double* rr, PyroSolveInfo
       (rc = net->output(f0, mg->h[0], z.as<float>(), v, st)) || (rc = net->check_err(st)))
     return rc;
   PYRO_CU(cudaMemsetAsync(sc.p, 0, SC_N * 8, st));
-  launch_pdl(k_apply_dot, grid_for(d), dim3(BX, BY, BZ), 0, st, l, ih2, z.as<float>(), f0, mg->bc_mode,
+  launch_pdl(k_apply_dot, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), ih2, z.as<float>(), f0, mg->bc_mode,
                                                        q.as<float>(), S);
-  launch_pdl(k_dots, grid_for(d), dim3(BX, BY, BZ), 0, st, l, f0, z.as<float>(), r.as<float>(), nullptr,
+  launch_pdl(k_dots, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), f0, z.as<float>(), r.as<float>(), nullptr,
                                                   S);
   PYRO_CU(cudaGetLastError());
   PYRO_CU(cudaMemcpyAsync(host_sc, sc.p, SC_N * 8, cudaMemcpyDeviceToHost, st));
@@ -414,7 +460,7 @@ int Solver::learned_stage(cudaStream_t st, float* phi, double* rr, PyroSolveInfo
   const double re = host_sc[SC_RZN], eae = host_sc[SC_PQ];
   // <Ae, r>, <Ae, Ae>
   PYRO_CU(cudaMemsetAsync(sc.p, 0, SC_N * 8, st));
-  launch_pdl(k_dots, grid_for(d), dim3(BX, BY, BZ), 0, st, l, f0, q.as<float>(), r.as<float>(),
+  launch_pdl(k_dots, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), f0, q.as<float>(), r.as<float>(),
                                                   q.as<float>(), S);
   PYRO_CU(cudaGetLastError());
   PYRO_CU(cudaMemcpyAsync(host_sc, sc.p, SC_N * 8, cudaMemcpyDeviceToHost, st));
@@ -428,7 +474,7 @@ int Solver::learned_stage(cudaStream_t st, float* phi, double* rr, PyroSolveInfo
     host_sc[SC_RZ] = re;
     host_sc[SC_PQ] = eae;
     PYRO_CU(cudaMemcpyAsync(sc.p, host_sc, SC_N * 8, cudaMemcpyHostToDevice, st));
-    launch_pdl(k_update_xr, grid_for(d), dim3(BX, BY, BZ), 0, st, l, f0, phi, r.as<float>(),
+    launch_pdl(k_update_xr, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), f0, phi, r.as<float>(),
                                                          z.as<float>(), q.as<float>(), S);
     PYRO_CU(cudaGetLastError());
     PYRO_CU(cudaMemcpyAsync(host_sc, sc.p, SC_N * 8, cudaMemcpyDeviceToHost, st));
@@ -501,7 +547,7 @@ int Solver::solve(cudaStream_t st, float* phi, const float* b, int mode, float t
     } rebind{mg, save_phi, save_b, save_f0};
     // r = b - A phi, |r|, |b|
     PYRO_CU(cudaMemsetAsync(sc.p, 0, SC_N * 8, st));
-    launch_pdl(k_resid, grid_for(d), dim3(BX, BY, BZ), 0, st, l, ih2, phi, b, f0, mg->bc_mode,
+    launch_pdl(k_resid, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), ih2, phi, b, f0, mg->bc_mode,
                                                      r.as<float>(), S);
     PYRO_CU(cudaGetLastError());
     PYRO_CU(cudaMemcpyAsync(host_sc, sc.p, SC_N * 8, cudaMemcpyDeviceToHost, st));
@@ -523,18 +569,18 @@ int Solver::solve(cudaStream_t st, float* phi, const float* b, int mode, float t
     int restarts = 0;
     while (rel > tol && iters < max_iters && restarts < 8) {
       PYRO_CU(precond(st, bf16));
-      launch_pdl(k_dots, grid_for(d), dim3(BX, BY, BZ), 0, st, l, f0, z.as<float>(), r.as<float>(),
+      launch_pdl(k_dots, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), f0, z.as<float>(), r.as<float>(),
                                                       nullptr, S);
       PYRO_CU(cudaGetLastError());
       launch_pdl(k_roll, dim3(1), dim3(1), 0, st, S);
-      launch_pdl(k_update_p, grid_for(d), dim3(BX, BY, BZ), 0, st, l, f0, p.as<float>(), z.as<float>(),
+      launch_pdl(k_update_p, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), f0, p.as<float>(), z.as<float>(),
                                                           S, 1);
       PYRO_CU(cudaGetLastError());
       bool stalled = false;
       while (iters < max_iters) {
-        launch_pdl(k_apply_dot, grid_for(d), dim3(BX, BY, BZ), 0, st, l, ih2, p.as<float>(), f0,
+        launch_pdl(k_apply_dot, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), ih2, p.as<float>(), f0,
                                                              mg->bc_mode, q.as<float>(), S);
-        launch_pdl(k_update_xr, grid_for(d), dim3(BX, BY, BZ), 0, st, l, f0, phi, r.as<float>(),
+        launch_pdl(k_update_xr, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), f0, phi, r.as<float>(),
                                                              p.as<float>(), q.as<float>(), S);
         PYRO_CU(cudaGetLastError());
         PYRO_CU(cudaMemcpyAsync(host_sc, sc.p, SC_N * 8, cudaMemcpyDeviceToHost, st));
@@ -547,16 +593,16 @@ int Solver::solve(cudaStream_t st, float* phi, const float* b, int mode, float t
         }
         if (bb2 > 0 && std::sqrt(rr / bb2) <= tol) break;
         PYRO_CU(precond(st, bf16));
-        launch_pdl(k_dots, grid_for(d), dim3(BX, BY, BZ), 0, st, l, f0, z.as<float>(), r.as<float>(),
+        launch_pdl(k_dots, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), f0, z.as<float>(), r.as<float>(),
                                                         q.as<float>(), S);
-        launch_pdl(k_update_p, grid_for(d), dim3(BX, BY, BZ), 0, st, l, f0, p.as<float>(),
+        launch_pdl(k_update_p, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), f0, p.as<float>(),
                                                             z.as<float>(), S, 0);
         launch_pdl(k_roll, dim3(1), dim3(1), 0, st, S);
         PYRO_CU(cudaGetLastError());
       }
       // true residual into r (and |r|, |b|)
       PYRO_CU(cudaMemsetAsync(sc.p, 0, SC_N * 8, st));
-      launch_pdl(k_resid, grid_for(d), dim3(BX, BY, BZ), 0, st, l, ih2, phi, b, f0, mg->bc_mode,
+      launch_pdl(k_resid, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), ih2, phi, b, f0, mg->bc_mode,
                                                        r.as<float>(), S);
       PYRO_CU(cudaGetLastError());
       PYRO_CU(cudaMemcpyAsync(host_sc, sc.p, SC_N * 8, cudaMemcpyDeviceToHost, st));
