@@ -218,7 +218,8 @@ cudaError_t Multigrid::vcycles_bf16(int cycles, cudaStream_t st, DevBuf* bphi, D
   return launch_bf16_to_f32(bphi[0].p, phi[0], n0, st);
 }
 
-cudaError_t Multigrid::vcycle_sym(cudaStream_t st, DevBuf* bphi, DevBuf* bphi2, DevBuf* bb) {
+cudaError_t Multigrid::vcycle_sym(cudaStream_t st, DevBuf* bphi, DevBuf* bphi2, DevBuf* bb,
+                                   bool prep) {
   int nl = (int)dims.size();
   const bool lo = bphi != nullptr;
   cudaError_t e;
@@ -232,16 +233,16 @@ cudaError_t Multigrid::vcycle_sym(cudaStream_t st, DevBuf* bphi, DevBuf* bphi2, 
       }
     }
   }
-  if ((e = prepare(st)) != cudaSuccess) return e;
+  if (prep && (e = prepare(st)) != cudaSuccess) return e;
   auto M = [&](int l) { return meta[l].as<uint8_t>(); };
   // storage of level l: phi, b, scratch
   auto P = [&](int l) -> void* { return lo ? bphi[l].p : (void*)phi[l]; };
   auto B = [&](int l) -> void* { return lo ? bb[l].p : (void*)b[l]; };
   auto T = [&](int l) -> void* { return lo ? bphi2[l].p : phi2[l].p; };
   size_t n0 = dims[0].cells();
-  if (lo) {
+  if (lo) {  // the initial guess is zero: level 0 of the BF16 copy starts cleared
     if ((e = launch_f32_to_bf16(b[0], bb[0].p, n0, st)) != cudaSuccess) return e;
-    if ((e = launch_f32_to_bf16(phi[0], bphi[0].p, n0, st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(bphi[0].p, 0, n0 * 2, st)) != cudaSuccess) return e;
   }
   auto pass = [&](int l, int c, float om) -> cudaError_t {
     return lo ? launch_mg_pass_bf16(dims[l], h[l], B(l), M(l), P(l), c, om, bc_mode, st)

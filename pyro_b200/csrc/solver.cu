@@ -424,15 +424,17 @@ int Solver::true_resid(cudaStream_t st, const float* phi, const float* b, double
   return PYRO_OK;
 }
 
-cudaError_t Solver::precond(cudaStream_t st, bool bf16) {
-  // z = V(r): one V-cycle from a zero initial guess.
-  cudaError_t e = cudaMemsetAsync(z.p, 0, d.cells() * 4, st);
-  if (e != cudaSuccess) return e;
+cudaError_t Solver::precond(cudaStream_t st, bool bf16, bool prep) {
+  // z = V(r): one V-cycle from a zero initial guess (the BF16 V-cycle
+  // writes every cell of z and does not read it).
+  cudaError_t e = cudaSuccess;
+  if (!bf16 && (e = cudaMemsetAsync(z.p, 0, d.cells() * 4, st)) != cudaSuccess) return e;
   float* save_phi = mg->phi[0];
   float* save_b = mg->b[0];
   const uint32_t* save_f = mg->f[0];
   mg->bind_level0(z.as<float>(), r.as<float>(), save_f);
-  e = bf16 ? mg->vcycle_sym(st, bphi, bphi2, bb) : mg->vcycle_sym(st, nullptr, nullptr, nullptr);
+  e = bf16 ? mg->vcycle_sym(st, bphi, bphi2, bb, prep)
+           : mg->vcycle_sym(st, nullptr, nullptr, nullptr, prep);
   mg->bind_level0(save_phi, save_b, save_f);
   return e;
 }
@@ -567,8 +569,10 @@ int Solver::solve(cudaStream_t st, float* phi, const float* b, int mode, float t
     // meets the tolerance the true residual is recomputed; if it does not
     // meet it, CG restarts from the true residual.
     int restarts = 0;
+    bool prepared = false;  // the level masks of the reachable-fluid flags
     while (rel > tol && iters < max_iters && restarts < 8) {
-      PYRO_CU(precond(st, bf16));
+      PYRO_CU(precond(st, bf16, !prepared));
+      prepared = true;
       launch_pdl(k_dots, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), f0, z.as<float>(), r.as<float>(),
                                                       nullptr, S);
       PYRO_CU(cudaGetLastError());
@@ -592,7 +596,7 @@ int Solver::solve(cudaStream_t st, float* phi, const float* b, int mode, float t
           break;
         }
         if (bb2 > 0 && std::sqrt(rr / bb2) <= tol) break;
-        PYRO_CU(precond(st, bf16));
+        PYRO_CU(precond(st, bf16, false));
         launch_pdl(k_dots, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), f0, z.as<float>(), r.as<float>(),
                                                         q.as<float>(), S);
         launch_pdl(k_update_p, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), f0, p.as<float>(),

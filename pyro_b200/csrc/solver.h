@@ -34,7 +34,7 @@ struct Solver {
             PyroSolveInfo* info);
 
  private:
-  cudaError_t precond(cudaStream_t st, bool bf16);
+  cudaError_t precond(cudaStream_t st, bool bf16, bool prep);
   int true_resid(cudaStream_t st, const float* phi, const float* b, double* rel, double* bn);
   // phi += alpha net(r) when that lowers |r| (r = b - A phi on entry, kept
   // consistent); *rr is |r|^2 in and out.
