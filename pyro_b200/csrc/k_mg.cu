@@ -451,29 +451,6 @@ cudaError_t launch_bf16_to_f32(const void* a, float* b, size_t n, cudaStream_t s
   return launch_pdl(k_bf16_to_f32, dim3((unsigned)((n + 255) / 256)), dim3(256), 0, st,
                     (const __nv_bfloat16*)a, b, n);
 }
-cudaError_t launch_mg_smooth_bf16(Dims3 d, float h, const void* b, const uint32_t* f, void* p,
-                                  int color, float omega, int bc_mode, cudaStream_t st) {
-  return mg_smooth_t<__nv_bfloat16>(d, h, (const __nv_bfloat16*)b, f, (__nv_bfloat16*)p, color,
-                                    omega, bc_mode, st);
-}
-cudaError_t launch_mg_restrict_bf16(Dims3 df, float hf, const void* pf, const void* bf,
-                                    const uint32_t* ff, Dims3 dc, void* bc, void* pc,
-                                    uint32_t* fc, int bc_mode, cudaStream_t st) {
-  return mg_restrict_t<__nv_bfloat16>(df, hf, (const __nv_bfloat16*)pf,
-                                      (const __nv_bfloat16*)bf, ff, dc, (__nv_bfloat16*)bc,
-                                      (__nv_bfloat16*)pc, fc, bc_mode, st);
-}
-cudaError_t launch_mg_prolong_bf16(Dims3 df, const void* pc, const uint32_t* ff, void* pf,
-                                   Dims3 dc, const uint32_t* fc, cudaStream_t st) {
-  return mg_prolong_t<__nv_bfloat16>(df, (const __nv_bfloat16*)pc, ff, (__nv_bfloat16*)pf, dc,
-                                     fc, st);
-}
-cudaError_t launch_mg_coarse_bf16(Dims3 d, float h, const void* b, const uint32_t* f, void* p,
-                                  int iters, float omega, int bc_mode, cudaStream_t st) {
-  return mg_coarse_t<__nv_bfloat16>(d, h, (const __nv_bfloat16*)b, f, (__nv_bfloat16*)p, iters,
-                                    omega, bc_mode, st);
-}
-
 cudaError_t launch_mg_coarse_sym(Dims3 d, float h, const float* b, const uint32_t* f, float* p,
                                  int iters, float omega, int bc_mode, cudaStream_t st) {
   return mg_coarse_t<float>(d, h, b, f, p, iters, omega, bc_mode, st, 1);

@@ -8,15 +8,9 @@
 //    (k = +x,-x,+y,-y,+z,-z) = neighbour k is inside the level and fluid,
 //    bit 6 = the cell is solid.  The smoother's neighbour count is the
 //    popcount plus the Dirichlet faces the cell touches.
-//  * k_mg_rb does one whole red-black iteration (red pass, then black pass)
-//    on a 32x8x8 tile staged in shared memory with a halo of H cells:
-//    red cells are updated over the tile plus H-1 halo layers, black cells
-//    over the tile plus H-2, so the tile's result equals two global passes.
-//    It reads phi from one buffer and writes the other (tiles of other CTAs
-//    read the old values meanwhile).
-//  * With RESTRICT (H = 3) it also forms the fine residual of the tile after
-//    the black pass and writes the fluid-averaged coarse right-hand side and
-//    a zero coarse guess for the tile's coarse cells (mg.wgsl:52-83).
+//  * k_mg_pass4 updates the cells of one colour four per thread (float4
+//    rows, lane shuffles for the x halo); k_mg_restrict_m / k_mg_prolong_m
+//    work one thread per coarse cell.
 //
 // Per-cell arithmetic is the reference's, in its order, so results equal the
 // per-pass kernels bit for bit.
@@ -84,185 +78,6 @@ __global__ void __launch_bounds__(256) k_mg_flags_down(L df, const uint32_t* __r
     if (df.inb(cx, cy, cz) && __ldg(ff + df.idx(cx, cy, cz)) != 1u) fluid = true;
   }
   fc[dc.idx(x, y, z)] = fluid ? 0u : 1u;
-}
-
-constexpr int TX = 32, TY = 8, TZ = 8;
-constexpr int RB_THREADS = 512;
-
-template <int H>
-struct RbShape {
-  static constexpr int PX = TX + 2 * H, PY = TY + 2 * H, PZ = TZ + 2 * H;  // phi
-  static constexpr int BX = TX + 2 * (H - 1), BY = TY + 2 * (H - 1), BZ = TZ + 2 * (H - 1);
-  static constexpr int PN = PX * PY * PZ, BN = BX * BY * BZ;
-  static constexpr size_t smem(bool restrict_) {
-    return (size_t)PN * 4 + (size_t)BN * 4 + (size_t)BN + (restrict_ ? TX * TY * TZ * 4 : 0);
-  }
-};
-
-// Update every cell of colour `col` inside the box [lo, hi) (tile-local
-// coordinates relative to the tile origin), reading and writing phi in
-// shared memory.
-template <int H>
-__device__ __forceinline__ void rb_pass(const L& d, int x0, int y0, int z0, int col, int lo_x,
-                                        int hi_x, int lo_y, int hi_y, int lo_z, int hi_z,
-                                        float* sp, const float* sb, const uint8_t* sm,
-                                        float omega, int bc_mode) {
-  using S = RbShape<H>;
-  const int ex = hi_x - lo_x, ey = hi_y - lo_y, ez = hi_z - lo_z;
-  // only cells of colour `col`: x parity is fixed per (y, z) row
-  const int hx = (ex + 1) / 2;
-  const int n = hx * ey * ez;
-  for (int t = threadIdx.x; t < n; t += RB_THREADS) {
-    int q = t / hx;
-    int ix = t - q * hx;
-    int iz = q / ey;
-    int iy = q - iz * ey;
-    int ly = lo_y + iy, lz = lo_z + iz;
-    int gy = y0 + ly, gz = z0 + lz;
-    // first x of this row with (gx + gy + gz) & 1 == col
-    int gx_lo = x0 + lo_x;
-    int gx = gx_lo + ((col - gx_lo - gy - gz) & 1) + 2 * ix;
-    int lx = gx - x0;
-    if (lx >= hi_x) continue;
-    if (!d.inb(gx, gy, gz)) continue;
-    int bi = (lx + (H - 1)) + S::BX * ((ly + (H - 1)) + S::BY * (lz + (H - 1)));
-    uint8_t m = sm[bi];
-    if (m & META_SOLID) continue;
-    int pi = (lx + H) + S::PX * ((ly + H) + S::PY * (lz + H));
-    float sum = 0.0f;
-    if (m & 1u) sum += sp[pi + 1];
-    if (m & 2u) sum += sp[pi - 1];
-    if (m & 4u) sum += sp[pi + S::PX];
-    if (m & 8u) sum += sp[pi - S::PX];
-    if (m & 16u) sum += sp[pi + S::PX * S::PY];
-    if (m & 32u) sum += sp[pi - S::PX * S::PY];
-    float cnt = (float)(__popc(m & 63u) + dirichlet_faces(d, gx, gy, gz, bc_mode));
-    if (cnt < 0.5f) continue;
-    sp[pi] = wmix(sp[pi], (sum - sb[bi]) / cnt, omega);
-  }
-}
-
-template <typename TS, int H, bool RESTRICT>
-__global__ void __launch_bounds__(RB_THREADS) k_mg_rb(L d, float h2, const TS* __restrict__ b,
-                                                      const uint8_t* __restrict__ meta,
-                                                      const TS* __restrict__ pin,
-                                                      TS* __restrict__ pout, float omega,
-                                                      int bc_mode, L dc, TS* __restrict__ bc,
-                                                      TS* __restrict__ pc) {
-  using S = RbShape<H>;
-  extern __shared__ float smem[];
-  float* sp = smem;
-  float* sb = smem + S::PN;
-  uint8_t* sm = reinterpret_cast<uint8_t*>(sb + S::BN);
-  float* sr = reinterpret_cast<float*>(sm + ((S::BN + 15) & ~15));
-  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = blockIdx.z * TZ;
-  // stage phi (halo H) and h^2 b, meta (halo H-1); loads are batched so
-  // that each thread keeps several in flight
-  constexpr int BATCH = 8;
-  for (int t0 = threadIdx.x; t0 < S::PN; t0 += BATCH * RB_THREADS) {
-    float v[BATCH];
-#pragma unroll
-    for (int k = 0; k < BATCH; k++) {
-      int t = t0 + k * RB_THREADS;
-      int lz = t / (S::PX * S::PY), r = t - lz * (S::PX * S::PY);
-      int ly = r / S::PX, lx = r - ly * S::PX;
-      int gx = x0 + lx - H, gy = y0 + ly - H, gz = z0 + lz - H;
-      v[k] = (t < S::PN && d.inb(gx, gy, gz)) ? ldv(pin + d.idx(gx, gy, gz)) : 0.0f;
-    }
-#pragma unroll
-    for (int k = 0; k < BATCH; k++) {
-      int t = t0 + k * RB_THREADS;
-      if (t < S::PN) sp[t] = v[k];
-    }
-  }
-  for (int t0 = threadIdx.x; t0 < S::BN; t0 += BATCH * RB_THREADS) {
-    float v[BATCH];
-    uint8_t m[BATCH];
-#pragma unroll
-    for (int k = 0; k < BATCH; k++) {
-      int t = t0 + k * RB_THREADS;
-      int lz = t / (S::BX * S::BY), r = t - lz * (S::BX * S::BY);
-      int ly = r / S::BX, lx = r - ly * S::BX;
-      int gx = x0 + lx - (H - 1), gy = y0 + ly - (H - 1), gz = z0 + lz - (H - 1);
-      bool in = t < S::BN && d.inb(gx, gy, gz);
-      int gi = in ? d.idx(gx, gy, gz) : 0;
-      v[k] = in ? ldv(b + gi) : 0.0f;
-      m[k] = in ? __ldg(meta + gi) : META_SOLID;
-    }
-#pragma unroll
-    for (int k = 0; k < BATCH; k++) {
-      int t = t0 + k * RB_THREADS;
-      if (t < S::BN) {
-        sb[t] = h2 * v[k];
-        sm[t] = m[k];
-      }
-    }
-  }
-  __syncthreads();
-  // red over the tile + (H-1) halo, black over the tile + (H-2) halo
-  rb_pass<H>(d, x0, y0, z0, 0, -(H - 1), TX + H - 1, -(H - 1), TY + H - 1, -(H - 1),
-             TZ + H - 1, sp, sb, sm, omega, bc_mode);
-  __syncthreads();
-  rb_pass<H>(d, x0, y0, z0, 1, -(H - 2), TX + H - 2, -(H - 2), TY + H - 2, -(H - 2),
-             TZ + H - 2, sp, sb, sm, omega, bc_mode);
-  __syncthreads();
-  // write the tile
-  for (int t = threadIdx.x; t < TX * TY * TZ; t += RB_THREADS) {
-    int lz = t / (TX * TY), r = t - lz * (TX * TY);
-    int ly = r / TX, lx = r - ly * TX;
-    int gx = x0 + lx, gy = y0 + ly, gz = z0 + lz;
-    if (!d.inb(gx, gy, gz)) continue;
-    stv(pout + d.idx(gx, gy, gz), sp[(lx + H) + S::PX * ((ly + H) + S::PY * (lz + H))]);
-  }
-  if constexpr (RESTRICT) {
-    // fine residual r = b - (sum - cnt p) / h^2 of the tile (mg.wgsl:52-66)
-    for (int t = threadIdx.x; t < TX * TY * TZ; t += RB_THREADS) {
-      int lz = t / (TX * TY), r = t - lz * (TX * TY);
-      int ly = r / TX, lx = r - ly * TX;
-      int gx = x0 + lx, gy = y0 + ly, gz = z0 + lz;
-      float res = 0.0f;
-      if (d.inb(gx, gy, gz)) {
-        int bi = (lx + (H - 1)) + S::BX * ((ly + (H - 1)) + S::BY * (lz + (H - 1)));
-        uint8_t m = sm[bi];
-        if (!(m & META_SOLID)) {
-          int pi = (lx + H) + S::PX * ((ly + H) + S::PY * (lz + H));
-          float sum = 0.0f;
-          if (m & 1u) sum += sp[pi + 1];
-          if (m & 2u) sum += sp[pi - 1];
-          if (m & 4u) sum += sp[pi + S::PX];
-          if (m & 8u) sum += sp[pi - S::PX];
-          if (m & 16u) sum += sp[pi + S::PX * S::PY];
-          if (m & 32u) sum += sp[pi - S::PX * S::PY];
-          float cnt = (float)(__popc(m & 63u) + dirichlet_faces(d, gx, gy, gz, bc_mode));
-          res = ldv(b + d.idx(gx, gy, gz)) - (sum - cnt * sp[pi]) / h2;
-        }
-      }
-      sr[t] = res;
-    }
-    __syncthreads();
-    // fluid-averaged restriction to the tile's coarse cells (mg.wgsl:67-83)
-    constexpr int CX = TX / 2, CY = TY / 2, CZ = TZ / 2;
-    for (int t = threadIdx.x; t < CX * CY * CZ; t += RB_THREADS) {
-      int cz = t / (CX * CY), r = t - cz * (CX * CY);
-      int cy = r / CX, cx = r - cy * CX;
-      int gx = x0 / 2 + cx, gy = y0 / 2 + cy, gz = z0 / 2 + cz;
-      if (!dc.inb(gx, gy, gz)) continue;
-      float acc = 0.0f, nfl = 0.0f;
-#pragma unroll
-      for (int k = 0; k < 8; k++) {
-        int lx = 2 * cx + (k & 1), ly = 2 * cy + ((k >> 1) & 1), lz = 2 * cz + ((k >> 2) & 1);
-        if (!d.inb(x0 + lx, y0 + ly, z0 + lz)) continue;
-        int bi = (lx + (H - 1)) + S::BX * ((ly + (H - 1)) + S::BY * (lz + (H - 1)));
-        if (!(sm[bi] & META_SOLID)) {
-          nfl += 1.0f;
-          acc += sr[lx + TX * (ly + TY * lz)];
-        }
-      }
-      int ci = dc.idx(gx, gy, gz);
-      stv(bc + ci, (nfl > 0.0f) ? acc / fmaxf(nfl, 1.0f) : 0.0f);
-      stv(pc + ci, 0.0f);
-    }
-  }
 }
 
 // Two cells x0, x0 + 1 of a row (x0 even).  V2: the row length is even, so
@@ -683,24 +498,6 @@ __global__ void __launch_bounds__(256) k_mg_restrict_t(L df, const TS* __restric
 
 inline dim3 g3(Dims3 d) { return dim3((d.nx + 31) / 32, (d.ny + 3) / 4, (d.nz + 1) / 2); }
 
-template <typename TS, int H, bool R>
-cudaError_t rb_launch(Dims3 d, float h, const TS* b, const uint8_t* meta, const TS* pin, TS* pout,
-                      float omega, int bc_mode, Dims3 dc, TS* bc, TS* pc, cudaStream_t st) {
-  static bool attr = false;
-  size_t smem = RbShape<H>::smem(R) + 16;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(k_mg_rb<TS, H, R>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
-  dim3 grid((d.nx + TX - 1) / TX, (d.ny + TY - 1) / TY, (d.nz + TZ - 1) / TZ);
-  k_mg_rb<TS, H, R><<<grid, RB_THREADS, smem, st>>>(
-      L{d.nx, d.ny, d.nz}, h * h, b, meta, pin, pout, omega, bc_mode, L{dc.nx, dc.ny, dc.nz}, bc,
-      pc);
-  return cudaGetLastError();
-}
-
 }  // namespace
 
 template <typename TS>
@@ -738,13 +535,6 @@ cudaError_t launch_mg_restrict_m(Dims3 df, float h, const float* pf, const float
                                  cudaStream_t st) {
   return restrict_t<float>(df, h, pf, bf, mf, dc, bc, pc, bc_mode, st);
 }
-cudaError_t launch_mg_restrict_m_bf16(Dims3 df, float h, const void* pf, const void* bf,
-                                      const uint8_t* mf, Dims3 dc, void* bc, void* pc,
-                                      int bc_mode, cudaStream_t st) {
-  using T = __nv_bfloat16;
-  return restrict_t<T>(df, h, (const T*)pf, (const T*)bf, mf, dc, (T*)bc, (T*)pc, bc_mode, st);
-}
-
 template <typename TS>
 cudaError_t restrict_sym_t(Dims3 df, float h, const TS* pf, const TS* bf, const uint8_t* mf,
                            TS* rt, Dims3 dc, const uint8_t* mc, TS* bc, TS* pc, int bc_mode,
@@ -781,18 +571,6 @@ cudaError_t launch_mg_flags_down(Dims3 df, const uint32_t* ff, Dims3 dc, uint32_
                     L{dc.nx, dc.ny, dc.nz}, fc);
 }
 
-cudaError_t launch_mg_rb(Dims3 d, float h, const float* b, const uint8_t* meta, const float* pin,
-                         float* pout, float omega, int bc_mode, cudaStream_t st) {
-  return rb_launch<float, 2, false>(d, h, b, meta, pin, pout, omega, bc_mode, d, nullptr, nullptr,
-                                    st);
-}
-
-cudaError_t launch_mg_rb_restrict(Dims3 d, float h, const float* b, const uint8_t* meta,
-                                  const float* pin, float* pout, float omega, int bc_mode,
-                                  Dims3 dc, float* bc, float* pc, cudaStream_t st) {
-  return rb_launch<float, 3, true>(d, h, b, meta, pin, pout, omega, bc_mode, dc, bc, pc, st);
-}
-
 template <typename TS>
 cudaError_t prolong_t(Dims3 df, const TS* pc, const uint8_t* mf, TS* pf, Dims3 dc,
                       const uint8_t* mc, cudaStream_t st) {
@@ -804,22 +582,6 @@ cudaError_t prolong_t(Dims3 df, const TS* pc, const uint8_t* mf, TS* pf, Dims3 d
 cudaError_t launch_mg_prolong_m(Dims3 df, const float* pc, const uint8_t* mf, float* pf,
                                 Dims3 dc, const uint8_t* mc, cudaStream_t st) {
   return prolong_t<float>(df, pc, mf, pf, dc, mc, st);
-}
-
-cudaError_t launch_mg_rb_bf16(Dims3 d, float h, const void* b, const uint8_t* meta,
-                              const void* pin, void* pout, float omega, int bc_mode,
-                              cudaStream_t st) {
-  using T = __nv_bfloat16;
-  return rb_launch<T, 2, false>(d, h, (const T*)b, meta, (const T*)pin, (T*)pout, omega, bc_mode,
-                                d, nullptr, nullptr, st);
-}
-
-cudaError_t launch_mg_rb_restrict_bf16(Dims3 d, float h, const void* b, const uint8_t* meta,
-                                       const void* pin, void* pout, float omega, int bc_mode,
-                                       Dims3 dc, void* bc, void* pc, cudaStream_t st) {
-  using T = __nv_bfloat16;
-  return rb_launch<T, 3, true>(d, h, (const T*)b, meta, (const T*)pin, (T*)pout, omega, bc_mode,
-                               dc, (T*)bc, (T*)pc, st);
 }
 
 cudaError_t launch_mg_prolong_m_bf16(Dims3 df, const void* pc, const uint8_t* mf, void* pf,

@@ -74,35 +74,14 @@ cudaError_t launch_mg_coarse(Dims3 d, float h, const float* b, const uint32_t* f
 // the low-precision MGPCG preconditioner; pointers are bf16 arrays.
 cudaError_t launch_f32_to_bf16(const float* a, void* b, size_t n, cudaStream_t st);
 cudaError_t launch_bf16_to_f32(const void* a, float* b, size_t n, cudaStream_t st);
-cudaError_t launch_mg_smooth_bf16(Dims3 d, float h, const void* b, const uint32_t* f, void* p,
-                                  int color, float omega, int bc_mode, cudaStream_t st);
-cudaError_t launch_mg_restrict_bf16(Dims3 df, float hf, const void* pf, const void* bf,
-                                    const uint32_t* ff, Dims3 dc, void* bc, void* pc,
-                                    uint32_t* fc, int bc_mode, cudaStream_t st);
-cudaError_t launch_mg_prolong_bf16(Dims3 df, const void* pc, const uint32_t* ff, void* pf,
-                                   Dims3 dc, const uint32_t* fc, cudaStream_t st);
-cudaError_t launch_mg_coarse_bf16(Dims3 d, float h, const void* b, const uint32_t* f, void* p,
-                                  int iters, float omega, int bc_mode, cudaStream_t st);
 
-// Fused multigrid (k_mgf.cu): per-level neighbour masks, one red-black
-// iteration per launch on shared-memory tiles (phi ping-pong pin -> pout),
-// optionally with the restriction to the next level fused in.
+// Multigrid on neighbour masks (k_mgf.cu): per-level masks, coarse solid
+// flags and the prolongation.
 cudaError_t launch_mg_meta(Dims3 d, const uint32_t* f, uint8_t* meta, cudaStream_t st);
 cudaError_t launch_mg_flags_down(Dims3 df, const uint32_t* ff, Dims3 dc, uint32_t* fc,
                                  cudaStream_t st);
-cudaError_t launch_mg_rb(Dims3 d, float h, const float* b, const uint8_t* meta, const float* pin,
-                         float* pout, float omega, int bc_mode, cudaStream_t st);
-cudaError_t launch_mg_rb_restrict(Dims3 d, float h, const float* b, const uint8_t* meta,
-                                  const float* pin, float* pout, float omega, int bc_mode,
-                                  Dims3 dc, float* bc, float* pc, cudaStream_t st);
 cudaError_t launch_mg_prolong_m(Dims3 df, const float* pc, const uint8_t* mf, float* pf,
                                 Dims3 dc, const uint8_t* mc, cudaStream_t st);
-cudaError_t launch_mg_rb_bf16(Dims3 d, float h, const void* b, const uint8_t* meta,
-                              const void* pin, void* pout, float omega, int bc_mode,
-                              cudaStream_t st);
-cudaError_t launch_mg_rb_restrict_bf16(Dims3 d, float h, const void* b, const uint8_t* meta,
-                                       const void* pin, void* pout, float omega, int bc_mode,
-                                       Dims3 dc, void* bc, void* pc, cudaStream_t st);
 cudaError_t launch_mg_prolong_m_bf16(Dims3 df, const void* pc, const uint8_t* mf, void* pf,
                                      Dims3 dc, const uint8_t* mc, cudaStream_t st);
 
@@ -114,9 +93,6 @@ cudaError_t launch_mg_pass_bf16(Dims3 d, float h, const void* b, const uint8_t* 
 cudaError_t launch_mg_restrict_m(Dims3 df, float h, const float* pf, const float* bf,
                                  const uint8_t* mf, Dims3 dc, float* bc, float* pc, int bc_mode,
                                  cudaStream_t st);
-cudaError_t launch_mg_restrict_m_bf16(Dims3 df, float h, const void* pf, const void* bf,
-                                      const uint8_t* mf, Dims3 dc, void* bc, void* pc,
-                                      int bc_mode, cudaStream_t st);
 
 // Symmetric V-cycle pieces for the MGPCG preconditioner: residual divided
 // by the fluid prolongation weight into `rt`, then the transpose (P^T / 8)

@@ -99,26 +99,6 @@ cudaError_t Multigrid::smooth(int l, int iters, bool coarse, cudaStream_t st) {
   return cudaSuccess;
 }
 
-cudaError_t Multigrid::vcycles_passes(int cycles, cudaStream_t st) {
-  int nl = (int)dims.size();
-  cudaError_t e;
-  for (int cy = 0; cy < cycles; cy++) {
-    for (int l = 0; l < nl - 1; l++) {
-      if ((e = smooth(l, 2, false, st)) != cudaSuccess) return e;
-      e = launch_mg_restrict(dims[l], h[l], phi[l], b[l], f[l], dims[l + 1], b[l + 1],
-                             phi[l + 1], const_cast<uint32_t*>(f[l + 1]), bc_mode, st);
-      if (e != cudaSuccess) return e;
-    }
-    if ((e = smooth(nl - 1, 80, true, st)) != cudaSuccess) return e;
-    for (int l = nl - 2; l >= 0; l--) {
-      e = launch_mg_prolong(dims[l], phi[l + 1], f[l], phi[l], dims[l + 1], f[l + 1], st);
-      if (e != cudaSuccess) return e;
-      if ((e = smooth(l, 2, false, st)) != cudaSuccess) return e;
-    }
-  }
-  return cudaSuccess;
-}
-
 cudaError_t Multigrid::prepare(cudaStream_t st) {
   int nl = (int)dims.size();
   cudaError_t e;
@@ -160,62 +140,6 @@ cudaError_t Multigrid::vcycles(int cycles, cudaStream_t st) {
     }
   }
   return cudaSuccess;
-}
-
-cudaError_t Multigrid::vcycles_bf16(int cycles, cudaStream_t st, DevBuf* bphi, DevBuf* bphi2,
-                                     DevBuf* bb) {
-  int nl = (int)dims.size();
-  for (int l = 0; l < nl; l++) {
-    size_t need = dims[l].cells() * 2;
-    if (bphi[l].bytes != need) {
-      if (bphi[l].alloc(need) != PYRO_OK || bphi2[l].alloc(need) != PYRO_OK ||
-          bb[l].alloc(need) != PYRO_OK)
-        return cudaErrorMemoryAllocation;
-    }
-  }
-  size_t n0 = dims[0].cells();
-  cudaError_t e;
-  if ((e = prepare(st)) != cudaSuccess) return e;
-  auto M = [&](int l) { return meta[l].as<uint8_t>(); };
-  // level 0: b <- r (BF16), phi <- current guess (BF16)
-  if ((e = launch_f32_to_bf16(b[0], bb[0].p, n0, st)) != cudaSuccess) return e;
-  if ((e = launch_f32_to_bf16(phi[0], bphi[0].p, n0, st)) != cudaSuccess) return e;
-  auto sm16 = [&](int l) -> cudaError_t {
-    for (int it = 0; it < 2; it++)
-      for (int c = 0; c < 2; c++) {
-        cudaError_t e2 =
-            launch_mg_pass_bf16(dims[l], h[l], bb[l].p, M(l), bphi[l].p, c, 1.0f, bc_mode, st);
-        if (e2 != cudaSuccess) return e2;
-      }
-    return cudaSuccess;
-  };
-  for (int cy = 0; cy < cycles; cy++) {
-    for (int l = 0; l < nl - 1; l++) {
-      if ((e = sm16(l)) != cudaSuccess) return e;
-      if ((e = launch_mg_restrict_m_bf16(dims[l], h[l], bphi[l].p, bb[l].p, M(l), dims[l + 1],
-                                         bb[l + 1].p, bphi[l + 1].p, bc_mode, st)) !=
-          cudaSuccess)
-        return e;
-    }
-    int lc = nl - 1;
-    if (coarse_one_cta) {
-      e = launch_mg_coarse_bf16(dims[lc], h[lc], bb[lc].p, f[lc], bphi[lc].p, 80, 1.6f, bc_mode,
-                                st);
-    } else {
-      for (int it = 0; it < 80 && e == cudaSuccess; it++)
-        for (int c = 0; c < 2 && e == cudaSuccess; c++)
-          e = launch_mg_smooth_bf16(dims[lc], h[lc], bb[lc].p, f[lc], bphi[lc].p, c, 1.6f,
-                                    bc_mode, st);
-    }
-    if (e != cudaSuccess) return e;
-    for (int l = nl - 2; l >= 0; l--) {
-      if ((e = launch_mg_prolong_m_bf16(dims[l], bphi[l + 1].p, M(l), bphi[l].p, dims[l + 1],
-                                        M(l + 1), st)) != cudaSuccess)
-        return e;
-      if ((e = sm16(l)) != cudaSuccess) return e;
-    }
-  }
-  return launch_bf16_to_f32(bphi[0].p, phi[0], n0, st);
 }
 
 cudaError_t Multigrid::vcycle_sym(cudaStream_t st, DevBuf* bphi, DevBuf* bphi2, DevBuf* bb,

@@ -76,12 +76,6 @@ struct Multigrid {
   // `cycles` V-cycles (src/sim.rs:451-491) on the bound level-0 arrays with
   // the fused kernels (k_mgf.cu); calls prepare() first.
   cudaError_t vcycles(int cycles, cudaStream_t st);
-  // The same schedule with one launch per colour pass (mg.wgsl as written).
-  cudaError_t vcycles_passes(int cycles, cudaStream_t st);
-  // One BF16-storage V-cycle as a preconditioner: z = V(r) from a zero
-  // guess, with bphi/bb the BF16 level arrays (allocated on first use).
-  cudaError_t vcycles_bf16(int cycles, cudaStream_t st, DevBuf* bphi, DevBuf* bphi2,
-                           DevBuf* bb);
   // Symmetric V-cycle for the CG preconditioner: pre-smoothing red-black,
   // post-smoothing black-red, restriction P^T/8 of the fluid-normalised
   // trilinear prolongation, coarsest level by alternating SOR sweeps.  With
