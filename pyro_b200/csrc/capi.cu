@@ -91,11 +91,17 @@ int pyro_k_adv_scalars(const PyroParams* params_dev, uint32_t nx, uint32_t ny, u
   KDIMS(pyro_k_adv_scalars)
   PYRO_REQUIRE(u && v && w && s0 && s1 && h0 && h1 && o0 && o1,
                "pyro_k_adv_scalars: null buffer");
+  // the predictor's backtrace, handed to the corrector
+  DevBuf bt;
+  int rc = bt.alloc((size_t)nx * ny * nz * 3 * 4);
+  if (rc != PYRO_OK) return rc;
   cudaError_t e = launch_adv_s1(params_dev, d, u, v, w, (const float4*)s0, (const float4*)s1,
-                                (float4*)h0, (float4*)h1, S(stream));
+                                (float4*)h0, (float4*)h1, bt.as<float>(), S(stream));
   if (e == cudaSuccess)
     e = launch_adv_s2(params_dev, d, u, v, w, (const float4*)s0, (const float4*)s1,
-                      (const float4*)h0, (const float4*)h1, (float4*)o0, (float4*)o1, S(stream));
+                      (const float4*)h0, (const float4*)h1, bt.as<float>(), (float4*)o0,
+                      (float4*)o1, S(stream));
+  if (e == cudaSuccess) e = cudaStreamSynchronize(S(stream));  // before bt is freed
   return ret(e, "pyro_k_adv_scalars");
 }
 

@@ -343,7 +343,8 @@ __global__ void __launch_bounds__(256) k_adv_s1(const PyroParams* __restrict__ P
                                                 const float4* __restrict__ s0,
                                                 const float4* __restrict__ s1,
                                                 float4* __restrict__ h0,
-                                                float4* __restrict__ h1) {
+                                                float4* __restrict__ h1,
+                                                float* __restrict__ bt) {
   I3 c = thread_cell();
   if (!g.inb(c)) return;
   const PyroParams& P = *Pp;
@@ -353,6 +354,11 @@ __global__ void __launch_bounds__(256) k_adv_s1(const PyroParams* __restrict__ P
   F3 b = V.back_at(g, kk, 3, c, tof3(c) + half) - half;
   float t = wclamp(g.outside(b), 0.0f, 1.0f);
   int i = g.sidx(c);
+  // the backtrace, for the corrector's limiter (adv_s2)
+  const size_t n = (size_t)g.nx * g.ny * g.nz;
+  bt[i] = b.x;
+  bt[n + i] = b.y;
+  bt[2 * n + i] = b.z;
   h0[i] = wmix4(triS(s0, g, b), make_float4(P.t0, 0.0f, P.yo2, 0.0f), t);
   h1[i] = wmix4(triS(s1, g, b), make_float4(0.0f, 0.0f, 0.0f, 0.0f), t);
 }
@@ -365,6 +371,7 @@ __global__ void __launch_bounds__(256, 4) k_adv_s2(const PyroParams* __restrict_
                                                 const float4* __restrict__ s1,
                                                 const float4* __restrict__ h0,
                                                 const float4* __restrict__ h1,
+                                                const float* __restrict__ bt,
                                                 float4* __restrict__ o0,
                                                 float4* __restrict__ o1) {
   I3 c = thread_cell();
@@ -373,11 +380,11 @@ __global__ void __launch_bounds__(256, 4) k_adv_s2(const PyroParams* __restrict_
   Vel V{u, v, w};
   const F3 half{0.5f, 0.5f, 0.5f};
   F3 x = tof3(c) + half;
-  F3 b, f;
-  V.both_at(g, kk, 3, c, x, b, f);
-  b = b - half;
-  f = f - half;
   int i = g.sidx(c);
+  // the backtrace from the predictor (the same expressions as both_at's)
+  const size_t n = (size_t)g.nx * g.ny * g.nz;
+  const F3 b{__ldg(bt + i), __ldg(bt + n + i), __ldg(bt + 2 * n + i)};
+  const F3 f = V.fwd_at(g, kk, 3, c, x) - half;
   float4 r0 = __ldg(h0 + i), r1 = __ldg(h1 + i);
   if (g.outside(b) <= 0.0f && g.outside(f) <= 0.0f) {
     float4 l0, u0, l1, u1;
@@ -415,6 +422,13 @@ __global__ void __launch_bounds__(256) k_react(const PyroParams* __restrict__ Pp
     } else {
       float4 a = __ldg(s0in + i);
       float4 b = __ldg(s1in + i);
+      // in-domain solid neighbours, bit k for direction k (+x -x +y -y +z -z)
+      uint32_t smask = 0;
+#pragma unroll
+      for (int k = 0; k < 6; k++) {
+        I3 n = c + dir6(k);
+        if (g.inb(n) && __ldg(flags + g.sidx(n)) == 1u) smask |= 1u << k;
+      }
       float nut = (P.cs * P.dx) * (P.cs * P.dx) * __ldg(curl + i).w;
       if (P.cs > 0.0f) {
         float kd = fminf(nut / 0.5f * P.dt / (P.dx * P.dx), 0.15f);
@@ -426,7 +440,7 @@ __global__ void __launch_bounds__(256) k_react(const PyroParams* __restrict__ Pp
           I3 n = c + dir6(k);
           if (g.inb(n)) {
             int j = g.sidx(n);
-            if (__ldg(flags + j) != 1u) {
+            if (!((smask >> k) & 1u)) {
               lapA = lapA + (__ldg(s0in + j) - a);
               lapB += __ldg(s1in + j).x - b.x;
             }
@@ -444,12 +458,12 @@ __global__ void __launch_bounds__(256) k_react(const PyroParams* __restrict__ Pp
       float ys = fmaxf(a.w, 0.0f);
       float ym = fmaxf(b.x, 0.0f);
       float S = 0.0f;
+      // solid neighbours in direction order (combust.wgsl:188-208)
 #pragma unroll 1
-      for (int k = 0; k < 6; k++) {
+      for (uint32_t sm = smask; sm; sm &= sm - 1u) {
+        const int k = __ffs(sm) - 1;
         I3 n = c + dir6(k);
-        if (!g.inb(n)) continue;
         int j = g.sidx(n);
-        if (__ldg(flags + j) != 1u) continue;
         float4 pr = __ldg(pyr + j);
         float Ts = __ldg(sol + j).w;
         float rho = rhoOf(P, T);
@@ -723,17 +737,18 @@ cudaError_t launch_adv_vel2(const PyroParams* P, Dims3 d, const float* u, const 
 }
 cudaError_t launch_adv_s1(const PyroParams* P, Dims3 d, const float* u, const float* v,
                           const float* w, const float4* s0, const float4* s1, float4* h0,
-                          float4* h1, cudaStream_t st) {
+                          float4* h1, float* bt, cudaStream_t st) {
   Grid g{d.nx, d.ny, d.nz};
-  k_adv_s1<<<grid_for(d.nx, d.ny, d.nz), PYRO_BLOCK, 0, st>>>(P, g, u, v, w, s0, s1, h0, h1);
+  k_adv_s1<<<grid_for(d.nx, d.ny, d.nz), PYRO_BLOCK, 0, st>>>(P, g, u, v, w, s0, s1, h0, h1, bt);
   return cudaGetLastError();
 }
 cudaError_t launch_adv_s2(const PyroParams* P, Dims3 d, const float* u, const float* v,
                           const float* w, const float4* s0, const float4* s1, const float4* h0,
-                          const float4* h1, float4* o0, float4* o1, cudaStream_t st) {
+                          const float4* h1, const float* bt, float4* o0, float4* o1,
+                          cudaStream_t st) {
   Grid g{d.nx, d.ny, d.nz};
-  k_adv_s2<<<grid_for(d.nx, d.ny, d.nz), PYRO_BLOCK, 0, st>>>(P, g, u, v, w, s0, s1, h0, h1, o0,
-                                                            o1);
+  k_adv_s2<<<grid_for(d.nx, d.ny, d.nz), PYRO_BLOCK, 0, st>>>(P, g, u, v, w, s0, s1, h0, h1, bt,
+                                                            o0, o1);
   return cudaGetLastError();
 }
 cudaError_t launch_react(const PyroParams* P, Dims3 d, const float4* s0in, const float4* s1in,

@@ -33,12 +33,15 @@ cudaError_t launch_adv_vel2(const PyroParams* P, Dims3 d, const float* u, const 
                             const float* w, const float* hu, const float* hv, const float* hw,
                             const float* lohi, float* ou, float* ov, float* ow,
                             const uint32_t* flags, cudaStream_t st);
+// bt: 3 cell arrays (x, y, z) of the cell-centred backtrace, written by
+// adv_s1 and read by adv_s2.
 cudaError_t launch_adv_s1(const PyroParams* P, Dims3 d, const float* u, const float* v,
                           const float* w, const float4* s0, const float4* s1, float4* h0,
-                          float4* h1, cudaStream_t st);
+                          float4* h1, float* bt, cudaStream_t st);
 cudaError_t launch_adv_s2(const PyroParams* P, Dims3 d, const float* u, const float* v,
                           const float* w, const float4* s0, const float4* s1, const float4* h0,
-                          const float4* h1, float4* o0, float4* o1, cudaStream_t st);
+                          const float4* h1, const float* bt, float4* o0, float4* o1,
+                          cudaStream_t st);
 cudaError_t launch_react(const PyroParams* P, Dims3 d, const float4* s0in, const float4* s1in,
                          float4* s0out, float4* s1out, const uint32_t* flags, const float4* sol,
                          const float4* pyr, const float4* curl, float* stats, cudaStream_t st);

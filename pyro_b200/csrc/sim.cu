@@ -40,7 +40,7 @@ struct PyroSim {
   int cur = 0;  // velocity and solid ping-pong index (equal in the reference)
   cudaStream_t stream = nullptr;
 
-  DevBuf vel[2][3], hat[3], lohi;
+  DevBuf vel[2][3], hat[3], lohi, btrace;
   DevBuf s0, s1, s0b, s1b, h0, h1, sol[2], pyr, curl, flags, phi0, b0;
   DevBuf stats, params;
   Multigrid mg;
@@ -102,11 +102,11 @@ struct PyroSim {
                              hat[2].as<float>(), lohi.as<float>(), aux[1])) != cudaSuccess)
       return e;
     if ((e = launch_adv_s1(P, d, ua, va, wa, s0.as<float4>(), s1.as<float4>(), h0.as<float4>(),
-                           h1.as<float4>(), aux[2])) != cudaSuccess)
+                           h1.as<float4>(), btrace.as<float>(), aux[2])) != cudaSuccess)
       return e;
     if ((e = launch_adv_s2(P, d, ua, va, wa, s0.as<float4>(), s1.as<float4>(), h0.as<float4>(),
-                           h1.as<float4>(), s0b.as<float4>(), s1b.as<float4>(), aux[2])) !=
-        cudaSuccess)
+                           h1.as<float4>(), btrace.as<float>(), s0b.as<float4>(),
+                           s1b.as<float4>(), aux[2])) != cudaSuccess)
       return e;
     for (int k = 0; k < 3; k++)
       if ((e = cudaEventRecord(join_ev[k], aux[k])) != cudaSuccess) return e;
@@ -201,7 +201,7 @@ struct PyroSim {
     for (auto& a : vel)
       for (auto& b : a) s += b.bytes;
     for (auto& b : hat) s += b.bytes;
-    s += lohi.bytes;
+    s += lohi.bytes + btrace.bytes;
     const DevBuf* list[] = {&s0, &s1, &s0b, &s1b, &h0, &h1, &sol[0], &sol[1], &pyr,
                             &curl, &flags, &phi0, &b0, &stats, &params};
     for (auto* b : list) s += b->bytes;
@@ -247,6 +247,7 @@ int pyro_sim_create(const PyroParams* params, const float* sol_init, uint32_t pr
   for (int k = 0; k < 3; k++)
     if ((rc = S->hat[k].alloc(nv * 4)) != PYRO_OK) return fail(rc);
   if ((rc = S->lohi.alloc(nv * 6 * 4)) != PYRO_OK) return fail(rc);
+  if ((rc = S->btrace.alloc(n * 3 * 4)) != PYRO_OK) return fail(rc);
   DevBuf* f4s[] = {&S->s0, &S->s1, &S->s0b, &S->s1b, &S->h0, &S->h1,
                    &S->sol[0], &S->sol[1], &S->pyr, &S->curl};
   for (auto* b : f4s)
@@ -392,12 +393,12 @@ int pyro_sim_profile_step(PyroSim* S, float dt, float time, float ign_on, int wa
   mark();
   if (e == cudaSuccess)
     e = launch_adv_s1(P, S->d, ua, va, wa, S->s0.as<float4>(), S->s1.as<float4>(),
-                      S->h0.as<float4>(), S->h1.as<float4>(), st);
+                      S->h0.as<float4>(), S->h1.as<float4>(), S->btrace.as<float>(), st);
   mark();
   if (e == cudaSuccess)
     e = launch_adv_s2(P, S->d, ua, va, wa, S->s0.as<float4>(), S->s1.as<float4>(),
-                      S->h0.as<float4>(), S->h1.as<float4>(), S->s0b.as<float4>(),
-                      S->s1b.as<float4>(), st);
+                      S->h0.as<float4>(), S->h1.as<float4>(), S->btrace.as<float>(),
+                      S->s0b.as<float4>(), S->s1b.as<float4>(), st);
   mark();
   if (e == cudaSuccess)
     e = launch_react(P, S->d, S->s0b.as<float4>(), S->s1b.as<float4>(), S->s0.as<float4>(),
