@@ -66,6 +66,11 @@ WORKLOADS = {
 # written once at the reference's width; read-modify-write twice).
 ALG_BYTES = {"solid": 68, "curl": 28, "adv_vel1": 24, "adv_vel2": 40, "adv_s1": 76,
              "adv_s2": 108, "react": 116, "forces": 76, "divergence": 36, "project": 32}
+# the renderer's input pack per cell: s0, s1, sol (16 each), flags (4) and the
+# cell's three faces (4 each) in, three binary16 volumes (8 each) out; the
+# bricks read two of those volumes once
+RENDER_PACK_BYTES = 16 * 3 + 4 + 12 + 24
+RENDER_BRICKS_BYTES = 16
 MG_LEVEL_BYTES = 122.5   # 4 sweeps (96) + restrict (13.5) + prolong (13) per level cell
 COARSE_SWEEP_BYTES = 24.0
 
@@ -476,6 +481,32 @@ def run_ours(args):
     achieved = dom_bytes / (kern[dom] * 1e-3) / 1e9
     traffic = load_traffic().get(dom, {}).get("dram_bytes_per_launch")
 
+    # ---- the renderer's per-frame input pack (render.wgsl:3-61): the pack
+    # alone, then pack + bricks; inputs (0.5 GB) exceed L2 between launches
+    sim.render_pack(True)  # first call allocates the volumes
+    sim.sync()
+    reps = 20
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    ev[0].record(stream)
+    for _ in range(reps):
+        _abi.check("pyro_sim_render_pack", lib.pyro_sim_render_pack(sim._h, 0))
+    ev[1].record(stream)
+    for _ in range(reps):
+        _abi.check("pyro_sim_render_pack", lib.pyro_sim_render_pack(sim._h, 1))
+    ev[2].record(stream)
+    ev[2].synchronize()
+    pack_ms = ev[0].elapsed_time(ev[1]) / reps
+    bricks_ms = max(ev[1].elapsed_time(ev[2]) / reps - pack_ms, 1e-6)
+    frame_pack = {
+        "pack_ms": pack_ms, "bricks_ms": bricks_ms,
+        "alg_bytes_per_cell": {"pack": RENDER_PACK_BYTES, "bricks": RENDER_BRICKS_BYTES},
+        "pack_gbs": RENDER_PACK_BYTES * cells / (pack_ms * 1e-3) / 1e9,
+        "bricks_gbs": RENDER_BRICKS_BYTES * cells / (bricks_ms * 1e-3) / 1e9,
+    }
+    frame_pack["pack_frac"] = frame_pack["pack_gbs"] / load_peaks()[0]
+    log(f"render pack {pack_ms:.3f} ms ({frame_pack['pack_gbs']:.0f} GB/s), "
+        f"bricks {bricks_ms:.3f} ms")
+
     # gather max over ranks
     vals = torch.tensor([ms, ms_e2e], dtype=torch.float64, device="cuda")
     if world > 1:
@@ -524,6 +555,7 @@ def run_ours(args):
         "step_roofline": {"alg_bytes": step_bytes, "achieved_gbs": step_bytes / (ms * 1e-3) / 1e9,
                           "frac": step_bytes / (ms * 1e-3) / 1e9 / peak},
         "kernels_ms": kern,
+        "frame_pack": frame_pack,
         "throughput": {"value": world * cells / (ms * 1e-3), "unit": "cells*substeps/s"},
         "cpu_baseline": cpu,
         "solver": solver,

@@ -81,7 +81,15 @@ enum PyroField {
   PYRO_F_V = 7,     /* float * Nv                                         */
   PYRO_F_W = 8,     /* float * Nv                                         */
   PYRO_F_PHI = 9,   /* float * N, level-0 pressure (warm start)           */
-  PYRO_F_B = 10     /* float * N, level-0 right-hand side                 */
+  PYRO_F_B = 10,    /* float * N, level-0 right-hand side                 */
+  /* the renderer input pack of the last pyro_sim_render_pack (none before
+   * the first call): 4 IEEE binary16 values per cell                     */
+  PYRO_F_RVOL = 11,   /* half4 * N: soot ppm, T K, smoke g/m^3, HRR kW/m^3 */
+  PYRO_F_RSOL = 12,   /* half4 * N: occupancy, then Ts, char fraction and
+                         material slot premultiplied by the occupancy     */
+  PYRO_F_RVEL = 13,   /* half4 * N: cell-centred velocity m/s, 0          */
+  PYRO_F_BRICKS = 14  /* float * ceil(nx/8)*ceil(ny/8)*ceil(nz/8): the
+                         visibility maximum of each 8^3 brick             */
 };
 
 /* Pressure solver modes for pyro_sim_set_solver / pyro_poisson_solve. */
@@ -184,6 +192,16 @@ int pyro_sim_last_solve(PyroSim* sim, PyroSolveInfo* info);
 /* Network used by PYRO_SOLVER_MGPCG_LEARNED (NULL detaches; the caller
  * keeps ownership and keeps it alive while attached). */
 int pyro_sim_set_net(PyroSim* sim, PyroNet* net);
+/* The renderer's per-frame input pack (src/shaders/render.wgsl:3-61, the
+ * pack and bricks dispatches of src/render.rs:270-292) from the current
+ * fields, into volumes the simulation holds (PYRO_F_RVOL, PYRO_F_RSOL,
+ * PYRO_F_RVEL; PYRO_F_BRICKS when with_bricks != 0), read with
+ * pyro_sim_read_field or borrowed with pyro_sim_device_ptr.  The
+ * reference's rgba16float textures become linear buffers of 4 binary16
+ * values per cell (cell index order, round to nearest even).  Asynchronous
+ * on the simulation's stream; the first call allocates the volumes
+ * (24 bytes per cell) and so must not run inside a stream capture. */
+int pyro_sim_render_pack(PyroSim* sim, int with_bricks);
 int pyro_sim_destroy(PyroSim* sim);
 
 /* ---- scene voxelizer (Scene::voxelize, src/scene.rs:621-667) ---------- */
@@ -312,6 +330,19 @@ int pyro_k_mg_prolong(uint32_t fnx, uint32_t fny, uint32_t fnz,
 int pyro_k_mg_resid(uint32_t nx, uint32_t ny, uint32_t nz, float h,
                     const float* phi, const float* b, const uint32_t* flags,
                     float* stats, void* stream);
+/* Renderer input pack on explicit buffers (render.wgsl:3-36): s0, s1, sol
+ * float4 * N, flags u32 * N, u, v, w face arrays; vol, sol_out, vel receive
+ * 4 binary16 values per cell (8 * N bytes each). */
+int pyro_k_render_pack(const PyroParams* params_dev, uint32_t nx, uint32_t ny,
+                       uint32_t nz, const float* s0, const float* s1,
+                       const float* sol, const uint32_t* flags, const float* u,
+                       const float* v, const float* w, void* vol, void* sol_out,
+                       void* vel, void* stream);
+/* Brick maxima (render.wgsl:38-61) from packed vol and sol volumes into
+ * bricks, float * ceil(nx/8)*ceil(ny/8)*ceil(nz/8), x fastest. */
+int pyro_k_render_bricks(uint32_t nx, uint32_t ny, uint32_t nz,
+                         const void* vol, const void* sol_packed, float* bricks,
+                         void* stream);
 /* Coarsest-level solve: `iters` red-black SOR sweeps (omega) in one
  * launch (src/sim.rs:473 runs 80 sweeps at omega 1.6 as 160 dispatches). */
 int pyro_k_mg_coarse(uint32_t nx, uint32_t ny, uint32_t nz, float h,

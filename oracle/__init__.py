@@ -40,6 +40,10 @@ _SIGS = {
     "or_forces": (None, [_P] * 8),
     "or_divergence": (None, [_P] * 7),
     "or_project": (None, [_P] * 6),
+    "or_render_pack": (None, [_P] * 11),
+    "or_render_bricks": (None, [_I, _I, _I, _P, _P, _P]),
+    "or_f32_to_f16": (None, [_P, _P, ctypes.c_size_t]),
+    "or_f16_to_f32": (None, [_P, _P, ctypes.c_size_t]),
     "or_mg_smooth": (None, [_I, _I, _I, _F, _P, _P, _P, _I, _F, _I]),
     "or_mg_restrict": (None, [_I, _I, _I, _F, _P, _P, _P, _I, _I, _I, _P, _P, _P, _I]),
     "or_mg_prolong": (None, [_I, _I, _I, _P, _P, _P, _I, _I, _I, _P]),
@@ -163,6 +167,38 @@ def project(P, u, v, w, phi, flags):
     u, v, w = u.copy(), v.copy(), w.copy()
     lib().or_project(ptr(P), ptr(u), ptr(v), ptr(w), ptr(phi), ptr(flags))
     return u, v, w
+
+
+def render_pack(P, s0, s1, sol, flags, u, v, w):
+    """render.wgsl:17-35: (vol, sol, vel), float16 (nz, ny, nx, 4) each."""
+    nx, ny, nz = dims_of(P)
+    vol, solt, vel = (np.zeros((nz, ny, nx, 4), np.float16) for _ in range(3))
+    lib().or_render_pack(ptr(P), ptr(s0), ptr(s1), ptr(sol), ptr(flags), ptr(u), ptr(v), ptr(w),
+                         ptr(vol), ptr(solt), ptr(vel))
+    return vol, solt, vel
+
+
+def render_bricks(dims, vol, solt):
+    """render.wgsl:38-61: float32 (ceil(nz/8), ceil(ny/8), ceil(nx/8))."""
+    nx, ny, nz = dims
+    out = np.zeros(((nz + 7) // 8, (ny + 7) // 8, (nx + 7) // 8), np.float32)
+    lib().or_render_bricks(nx, ny, nz, ptr(vol), ptr(solt), ptr(out))
+    return out
+
+
+def f32_to_f16(x):
+    """The oracle's binary32 -> binary16 conversion (round to nearest even)."""
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    h = np.zeros(x.shape, np.uint16)
+    lib().or_f32_to_f16(ptr(x), ptr(h), ctypes.c_size_t(x.size))
+    return h
+
+
+def f16_to_f32(h):
+    h = np.ascontiguousarray(h, dtype=np.uint16)
+    x = np.zeros(h.shape, np.float32)
+    lib().or_f16_to_f32(ptr(h), ptr(x), ctypes.c_size_t(h.size))
+    return x
 
 
 def mg_smooth(dims, h, b, f, p, color, omega, bc_mode=0):

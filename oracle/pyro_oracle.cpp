@@ -989,6 +989,101 @@ void vcycles(Hier& H, float* phi0, const float* b0, const uint32_t* f0, int cycl
 
 // ===========================================================================
 // C API of the oracle (ctypes from the tests and bench.py's CPU legs).
+// ---------------------------------------------------------------------------
+// Renderer input pack: src/shaders/render.wgsl:3-61 (dispatched by
+// src/render.rs:263-292).  The reference stores into rgba16float textures;
+// the texel conversion is IEEE 754 binary32 -> binary16 with round to
+// nearest even (pinned against numpy's float16 conversion in the tests).
+
+// binary32 -> binary16, round to nearest, ties to even; finite values that
+// round past 65504 give infinity; NaN stays a (quiet) NaN.
+static uint16_t f32_to_f16(float f) {
+  uint32_t x;
+  std::memcpy(&x, &f, 4);
+  const uint16_t sign = (uint16_t)((x >> 16) & 0x8000u);
+  const uint32_t ax = x & 0x7fffffffu;
+  if (ax > 0x7f800000u) return sign | 0x7e00u;   // NaN
+  if (ax >= 0x477ff000u) return sign | 0x7c00u;  // >= 65520 (or inf): infinity
+  const int e = (int)(ax >> 23) - 127;           // unbiased exponent
+  const uint32_t mant = ax & 0x7fffffu;
+  if (e >= -14) {  // normal binary16: keep 10 of the 23 fraction bits
+    uint32_t h = ((uint32_t)(e + 15) << 10) | (mant >> 13);
+    const uint32_t r = mant & 0x1fffu;
+    if (r > 0x1000u || (r == 0x1000u && (h & 1u))) h++;  // a carry moves into the exponent
+    return sign | (uint16_t)h;
+  }
+  // subnormal binary16 (units of 2^-24): significand 1.mant shifted right
+  const int shift = -(e + 1);  // >= 14
+  if (shift > 24) return sign;  // below 2^-25: rounds to zero
+  const uint32_t m = 0x800000u | mant;
+  uint32_t h = m >> shift;
+  const uint32_t r = m & ((1u << shift) - 1u), half = 1u << (shift - 1);
+  if (r > half || (r == half && (h & 1u))) h++;
+  return sign | (uint16_t)h;
+}
+static float f16_to_f32(uint16_t h) {
+  const int e = (h >> 10) & 0x1f;
+  const uint32_t m = h & 0x3ffu;
+  float v;
+  if (e == 0) v = std::ldexp((float)m, -24);
+  else if (e == 31) v = m ? NAN : INFINITY;
+  else v = std::ldexp((float)(m | 0x400u), e - 25);
+  return (h & 0x8000u) ? -v : v;
+}
+static void store_h4(uint16_t* t, size_t i, float a, float b, float c, float d) {
+  t[4 * i] = f32_to_f16(a);
+  t[4 * i + 1] = f32_to_f16(b);
+  t[4 * i + 2] = f32_to_f16(c);
+  t[4 * i + 3] = f32_to_f16(d);
+}
+
+// render.wgsl:17-35, one cell
+static void render_pack(const Ctx& C, const F4* s0, const F4* s1, const F4* sol,
+                        const uint32_t* flags, const float* vu, const float* vv, const float* vw,
+                        uint16_t* volT, uint16_t* solT, uint16_t* velT) {
+  for (int z = 0; z < C.nz; z++)
+    for (int y = 0; y < C.ny; y++)
+      for (int x = 0; x < C.nx; x++) {
+        const I3 c{x, y, z};
+        const size_t i = C.sidx(c);
+        const F4 a = s0[i], b = s1[i];
+        const float rho = C.rhoOf(a.x);
+        const bool solid = flags[i] == 1u;
+        if (solid) store_h4(volT, i, 0.0f, a.x, 0.0f, 0.0f);
+        else store_h4(volT, i, rho * a.w / RHO_SOOT * 1e6f, a.x, rho * b.x * 1e3f, b.y * 1e-3f);
+        const F4 so = sol[i];
+        const float tot = so.y + so.z;
+        const float oc = solid ? 1.0f : 0.0f;
+        store_h4(solT, i, oc, so.w * oc, so.z / wmax(tot, 1e-6f) * oc, so.x * oc);
+        const size_t f = C.vidx(c);
+        const size_t sy = (size_t)C.nx + 1, sz = sy * ((size_t)C.ny + 1);
+        store_h4(velT, i, 0.5f * (vu[f] + vu[f + 1]), 0.5f * (vv[f] + vv[f + sy]),
+                 0.5f * (vw[f] + vw[f + sz]), 0.0f);
+      }
+}
+
+// render.wgsl:38-61: per 8^3 brick, max over the brick and a one-cell shell
+static void render_bricks(int nx, int ny, int nz, const uint16_t* volT, const uint16_t* solT,
+                          float* bricks) {
+  const int bx = (nx + 7) / 8, by = (ny + 7) / 8, bz = (nz + 7) / 8;
+  for (int k = 0; k < bz; k++)
+    for (int j = 0; j < by; j++)
+      for (int i = 0; i < bx; i++) {
+        float m = 0.0f;
+        for (int z = -1; z < 9; z++)
+          for (int y = -1; y < 9; y++)
+            for (int x = -1; x < 9; x++) {
+              const int cx = i * 8 + x, cy = j * 8 + y, cz = k * 8 + z;
+              if (cx < 0 || cy < 0 || cz < 0 || cx >= nx || cy >= ny || cz >= nz) continue;
+              const size_t c = (size_t)cx + (size_t)nx * ((size_t)cy + (size_t)ny * cz);
+              const float vx = f16_to_f32(volT[4 * c]), vz = f16_to_f32(volT[4 * c + 2]);
+              const float vw = f16_to_f32(volT[4 * c + 3]), sx = f16_to_f32(solT[4 * c]);
+              m = wmax(m, wmax(wmax(vx * 10.0f, vz * 2.0f), wmax(vw * 0.1f, sx * 10.0f)));
+            }
+        bricks[i + bx * (j + by * k)] = m;
+      }
+}
+
 extern "C" {
 
 void or_set_threads(int n) {
@@ -1080,6 +1175,22 @@ void or_project(const PyroParams* P, float* u, float* v, float* w, const float* 
                 const uint32_t* flags) {
   Ctx C(P);
   k_project(C, u, v, w, phi, flags);
+}
+void or_render_pack(const PyroParams* P, const float* s0, const float* s1, const float* sol,
+                    const uint32_t* flags, const float* u, const float* v, const float* w,
+                    uint16_t* vol, uint16_t* solt, uint16_t* vel) {
+  Ctx C(P);
+  render_pack(C, (const F4*)s0, (const F4*)s1, (const F4*)sol, flags, u, v, w, vol, solt, vel);
+}
+void or_render_bricks(int nx, int ny, int nz, const uint16_t* vol, const uint16_t* solt,
+                      float* bricks) {
+  render_bricks(nx, ny, nz, vol, solt, bricks);
+}
+void or_f32_to_f16(const float* x, uint16_t* h, size_t n) {
+  for (size_t i = 0; i < n; i++) h[i] = f32_to_f16(x[i]);
+}
+void or_f16_to_f32(const uint16_t* h, float* x, size_t n) {
+  for (size_t i = 0; i < n; i++) x[i] = f16_to_f32(h[i]);
 }
 void or_mg_smooth(int nx, int ny, int nz, float h, const float* b, const uint32_t* f, float* p,
                   int color, float omega, int bc_mode) {

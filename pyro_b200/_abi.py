@@ -24,6 +24,7 @@ MAX_LAYERS = 1024
 ABI_VERSION = 2
 
 F_S0, F_S1, F_SOL, F_PYR, F_FLAGS, F_CURL, F_U, F_V, F_W, F_PHI, F_B = range(11)
+F_RVOL, F_RSOL, F_RVEL, F_BRICKS = range(11, 15)  # renderer input pack
 
 PROFILE_PHASES = ["solid", "curl", "adv_vel1", "adv_vel2", "adv_s1", "adv_s2", "react",
                   "forces", "divergence", "pressure", "project", "total"]
@@ -133,6 +134,7 @@ SIGNATURES = {
     "pyro_sim_set_solver": [_P, _I, _F, _I],
     "pyro_sim_last_solve": [_P, ctypes.POINTER(PyroSolveInfo)],
     "pyro_sim_destroy": [_P],
+    "pyro_sim_render_pack": [_P, _I],
     "pyro_voxelize": [ctypes.POINTER(PyroShape), _U32, _U32, _U32, _U32, _F, _F, _U32,
                       _P, _P, _P, _P],
     "pyro_poisson_create": [_U32, _U32, _U32, _F, _I, ctypes.POINTER(_P)],
@@ -155,6 +157,8 @@ SIGNATURES = {
     "pyro_k_mg_resid": [_U32, _U32, _U32, _F, _P, _P, _P, _P, _P],
     "pyro_k_mg_coarse": [_U32, _U32, _U32, _F, _P, _P, _P, _I, _F, _P],
     "pyro_k_mg_coarse_sym": [_U32, _U32, _U32, _F, _P, _P, _P, _I, _F, _I, _P],
+    "pyro_k_render_pack": [_P, _U32, _U32, _U32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
+    "pyro_k_render_bricks": [_U32, _U32, _U32, _P, _P, _P, _P],
     "pyro_conv3_forward": [_P, _I, _I, _I, _I, _I, _P, _I, _P, _I, _P, _I, _P],
     "pyro_conv3_backward_data": [_P, _I, _I, _I, _I, _I, _P, _I, _P, _P, _I, _P],
     "pyro_conv3_backward_weight": [_P, _I, _P, _I, _I, _I, _I, _I, _P, _P],

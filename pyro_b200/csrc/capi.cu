@@ -230,6 +230,28 @@ int pyro_k_mg_coarse_sym(uint32_t nx, uint32_t ny, uint32_t nz, float h, const f
              "pyro_k_mg_coarse_sym");
 }
 
+int pyro_k_render_pack(const PyroParams* params_dev, uint32_t nx, uint32_t ny, uint32_t nz,
+                       const float* s0, const float* s1, const float* sol,
+                       const uint32_t* flags, const float* u, const float* v, const float* w,
+                       void* vol, void* sol_out, void* vel, void* stream) {
+  KDIMS(pyro_k_render_pack)
+  PYRO_REQUIRE(params_dev && s0 && s1 && sol && flags && u && v && w && vol && sol_out && vel,
+               "pyro_k_render_pack: null buffer");
+  return ret(launch_render_pack(params_dev, d, (const float4*)s0, (const float4*)s1,
+                                (const float4*)sol, flags, u, v, w, vol, sol_out, vel,
+                                S(stream)),
+             "pyro_k_render_pack");
+}
+
+int pyro_k_render_bricks(uint32_t nx, uint32_t ny, uint32_t nz, const void* vol,
+                         const void* sol_packed, float* bricks, void* stream) {
+  clear_error();
+  PYRO_REQUIRE(dims_ok(nx, ny, nz), "pyro_k_render_bricks: invalid grid dimensions");
+  PYRO_REQUIRE(vol && sol_packed && bricks, "pyro_k_render_bricks: null buffer");
+  Dims3 d{(int)nx, (int)ny, (int)nz};
+  return ret(launch_render_bricks(d, vol, sol_packed, bricks, S(stream)), "pyro_k_render_bricks");
+}
+
 int pyro_voxelize(const PyroShape* shapes, uint32_t n_shapes, uint32_t nx, uint32_t ny,
                   uint32_t nz, float dx, float t0, uint32_t seed, const float* slot_density,
                   const uint32_t* slot_kind, float* sol_out, void* stream) {

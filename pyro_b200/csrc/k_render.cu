@@ -1,0 +1,130 @@
+// k_render.cu — the renderer's per-frame input pack (src/shaders/render.wgsl:3-61,
+// dispatched by src/render.rs:270-292).
+//
+// The reference packs the step's fields into three rgba16float 3D textures
+// that the volume path tracer samples with hardware trilinear filtering,
+// then marks the 8^3 bricks that hold anything visible.  Here the volumes
+// are linear device buffers of 4 IEEE binary16 values per cell (x fastest,
+// the cell index of the simulation grid), converted with round to nearest
+// even; a CUDA consumer can sample them directly or copy them into a
+// cudaArray for filtering.
+//
+//  * k_render_pack: one thread per cell, float4 loads of s0, s1 and sol,
+//    the flag, the six faces of the cell, three 8-byte stores.  It is a
+//    stream: 64 bytes in and 24 out per cell, bound by HBM.
+//  * k_render_bricks: one CTA per brick, the maximum over the brick and a
+//    one-cell shell (the reach of trilinear filtering) read back from the
+//    half volumes, as the reference reads its textures.
+//
+// Per-cell arithmetic is the reference's in its order (--fmad=false keeps
+// each product rounded), so the half values equal the oracle's bit for bit.
+#include <cuda_fp16.h>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace pyro {
+
+namespace {
+
+constexpr int RP_BX = 32, RP_BY = 8;
+
+__device__ __forceinline__ uint2 half4(float a, float b, float c, float d) {
+  const __half2 lo = __floats2half2_rn(a, b), hi = __floats2half2_rn(c, d);
+  return make_uint2(*reinterpret_cast<const uint32_t*>(&lo),
+                    *reinterpret_cast<const uint32_t*>(&hi));
+}
+
+// vol = (soot volume fraction ppm, T K, smoke g/m^3, heat release kW/m^3),
+// sol = (occupancy, Ts, char fraction, material slot) premultiplied by the
+// occupancy, vel = (cell-centred velocity m/s, 0)  (render.wgsl:17-35).
+__global__ void __launch_bounds__(RP_BX * RP_BY) k_render_pack(
+    const PyroParams* __restrict__ Pp, Grid g, const float4* __restrict__ s0,
+    const float4* __restrict__ s1, const float4* __restrict__ sol,
+    const uint32_t* __restrict__ flags, const float* __restrict__ u,
+    const float* __restrict__ v, const float* __restrict__ w, uint2* __restrict__ vol,
+    uint2* __restrict__ solp, uint2* __restrict__ velp) {
+  const int x = blockIdx.x * RP_BX + threadIdx.x, y = blockIdx.y * RP_BY + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny) return;
+  const I3 c{x, y, z};
+  const int i = g.sidx(c), f = g.vidx(c);
+  const float4 a = __ldg(s0 + i), b = __ldg(s1 + i), so = __ldg(sol + i);
+  const bool solid = __ldg(flags + i) == 1u;
+  const float rho = rhoOf(*Pp, a.x);
+  vol[i] = solid ? half4(0.0f, a.x, 0.0f, 0.0f)
+                 : half4(rho * a.w / RHO_SOOT * 1e6f, a.x, rho * b.x * 1e3f, b.y * 1e-3f);
+  const float tot = so.y + so.z;
+  const float oc = solid ? 1.0f : 0.0f;
+  solp[i] = half4(oc, so.w * oc, so.z / fmaxf(tot, 1e-6f) * oc, so.x * oc);
+  const int sy = g.nx + 1, sz = (g.nx + 1) * (g.ny + 1);
+  velp[i] = half4(0.5f * (__ldg(u + f) + __ldg(u + f + 1)), 0.5f * (__ldg(v + f) + __ldg(v + f + sy)),
+                  0.5f * (__ldg(w + f) + __ldg(w + f + sz)), 0.0f);
+}
+
+constexpr int RB_THREADS = 256;
+
+__device__ __forceinline__ float4 unhalf4(uint2 q) {
+  const float2 lo = __half22float2(*reinterpret_cast<const __half2*>(&q.x));
+  const float2 hi = __half22float2(*reinterpret_cast<const __half2*>(&q.y));
+  return make_float4(lo.x, lo.y, hi.x, hi.y);
+}
+
+// Brick b (x fastest over ceil(n / 8) bricks per axis): the maximum of
+// max(max(vol.x * 10, vol.z * 2), max(vol.w * 0.1, sol.x * 10)) over the
+// cells of [8 b - 1, 8 b + 9) inside the grid, at least 0
+// (render.wgsl:38-61).
+__global__ void __launch_bounds__(RB_THREADS) k_render_bricks(Grid g, int bnx, int bny,
+                                                              const uint2* __restrict__ vol,
+                                                              const uint2* __restrict__ solp,
+                                                              float* __restrict__ bricks) {
+  __shared__ float red[RB_THREADS / 32];
+  const int b = blockIdx.x;
+  const int bx = b % bnx, by = (b / bnx) % bny, bz = b / (bnx * bny);
+  const int x0 = max(8 * bx - 1, 0), x1 = min(8 * bx + 9, g.nx);
+  const int y0 = max(8 * by - 1, 0), y1 = min(8 * by + 9, g.ny);
+  const int z0 = max(8 * bz - 1, 0), z1 = min(8 * bz + 9, g.nz);
+  const int ex = x1 - x0, ey = y1 - y0, n = ex * ey * (z1 - z0);
+  float m = 0.0f;
+  for (int t = threadIdx.x; t < n; t += RB_THREADS) {
+    const int r = t / ex, lx = t - r * ex;
+    const int lz = r / ey, ly = r - lz * ey;
+    const int i = g.sidx(I3{x0 + lx, y0 + ly, z0 + lz});
+    const float4 vv = unhalf4(__ldg(vol + i)), ss = unhalf4(__ldg(solp + i));
+    m = fmaxf(m, fmaxf(fmaxf(vv.x * 10.0f, vv.z * 2.0f), fmaxf(vv.w * 0.1f, ss.x * 10.0f)));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float r = red[0];
+#pragma unroll
+    for (int k = 1; k < RB_THREADS / 32; k++) r = fmaxf(r, red[k]);
+    bricks[b] = r;
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_render_pack(const PyroParams* P, Dims3 d, const float4* s0, const float4* s1,
+                               const float4* sol, const uint32_t* flags, const float* u,
+                               const float* v, const float* w, void* vol, void* solp, void* vel,
+                               cudaStream_t st) {
+  dim3 grid((d.nx + RP_BX - 1) / RP_BX, (d.ny + RP_BY - 1) / RP_BY, d.nz);
+  k_render_pack<<<grid, dim3(RP_BX, RP_BY), 0, st>>>(P, Grid{d.nx, d.ny, d.nz}, s0, s1, sol,
+                                                      flags, u, v, w, (uint2*)vol, (uint2*)solp,
+                                                      (uint2*)vel);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_render_bricks(Dims3 d, const void* vol, const void* solp, float* bricks,
+                                 cudaStream_t st) {
+  const int bnx = (d.nx + 7) / 8, bny = (d.ny + 7) / 8, bnz = (d.nz + 7) / 8;
+  k_render_bricks<<<bnx * bny * bnz, RB_THREADS, 0, st>>>(Grid{d.nx, d.ny, d.nz}, bnx, bny,
+                                                          (const uint2*)vol, (const uint2*)solp,
+                                                          bricks);
+  return cudaGetLastError();
+}
+
+}  // namespace pyro

@@ -53,6 +53,14 @@ cudaError_t launch_forces(const PyroParams* P, Dims3 d, float* u, float* v, floa
 cudaError_t launch_divergence(const PyroParams* P, Dims3 d, const float* u, const float* v,
                               const float* w, const float4* s1, const uint32_t* flags, float* b,
                               cudaStream_t st);
+// Renderer input pack (k_render.cu): three volumes of 4 binary16 values per
+// cell, and the 8^3 brick maxima read back from two of them.
+cudaError_t launch_render_pack(const PyroParams* P, Dims3 d, const float4* s0, const float4* s1,
+                               const float4* sol, const uint32_t* flags, const float* u,
+                               const float* v, const float* w, void* vol, void* solp, void* vel,
+                               cudaStream_t st);
+cudaError_t launch_render_bricks(Dims3 d, const void* vol, const void* solp, float* bricks,
+                                 cudaStream_t st);
 cudaError_t launch_project(const PyroParams* P, Dims3 d, float* u, float* v, float* w,
                            const float* phi, const uint32_t* flags, cudaStream_t st);
 

@@ -43,6 +43,7 @@ struct PyroSim {
   DevBuf vel[2][3], hat[3], lohi, btrace;
   DevBuf s0, s1, s0b, s1b, h0, h1, sol[2], pyr, curl, flags, phi0, b0;
   DevBuf stats, params;
+  DevBuf rvol, rsol, rvel, bricks;  // renderer input pack, allocated by its first call
   Multigrid mg;
   Solver solver;
 
@@ -192,6 +193,10 @@ struct PyroSim {
       case PYRO_F_W: *bytes = nv * 4; return vel[cur][2].p;
       case PYRO_F_PHI: *bytes = n * 4; return phi0.p;
       case PYRO_F_B: *bytes = n * 4; return b0.p;
+      case PYRO_F_RVOL: *bytes = rvol.bytes; return rvol.p;
+      case PYRO_F_RSOL: *bytes = rsol.bytes; return rsol.p;
+      case PYRO_F_RVEL: *bytes = rvel.bytes; return rvel.p;
+      case PYRO_F_BRICKS: *bytes = bricks.bytes; return bricks.p;
       default: *bytes = 0; return nullptr;
     }
   }
@@ -203,7 +208,8 @@ struct PyroSim {
     for (auto& b : hat) s += b.bytes;
     s += lohi.bytes + btrace.bytes;
     const DevBuf* list[] = {&s0, &s1, &s0b, &s1b, &h0, &h1, &sol[0], &sol[1], &pyr,
-                            &curl, &flags, &phi0, &b0, &stats, &params};
+                            &curl, &flags, &phi0, &b0, &stats, &params, &rvol, &rsol, &rvel,
+                            &bricks};
     for (auto* b : list) s += b->bytes;
     return s + mg.device_bytes() + solver.device_bytes();
   }
@@ -459,7 +465,7 @@ int pyro_sim_read_field(PyroSim* S, int which, void* host, size_t bytes) {
   PYRO_REQUIRE(S && host, "pyro_sim_read_field: null argument");
   size_t nb = 0;
   void* p = S->field(which, &nb);
-  PYRO_REQUIRE(p, "pyro_sim_read_field: unknown field");
+  PYRO_REQUIRE(p, "pyro_sim_read_field: unknown field (render volumes exist after pyro_sim_render_pack)");
   PYRO_REQUIRE(nb == bytes, "pyro_sim_read_field: size mismatch");
   PYRO_CU(cudaMemcpyAsync(host, p, nb, cudaMemcpyDeviceToHost, S->stream));
   PYRO_CU(cudaStreamSynchronize(S->stream));
@@ -482,7 +488,7 @@ int pyro_sim_device_ptr(PyroSim* S, int which, void** dptr, size_t* bytes) {
   clear_error();
   PYRO_REQUIRE(S && dptr && bytes, "pyro_sim_device_ptr: null argument");
   *dptr = S->field(which, bytes);
-  PYRO_REQUIRE(*dptr, "pyro_sim_device_ptr: unknown field");
+  PYRO_REQUIRE(*dptr, "pyro_sim_device_ptr: unknown field (render volumes exist after pyro_sim_render_pack)");
   return PYRO_OK;
 }
 
@@ -547,6 +553,28 @@ int pyro_sim_last_solve(PyroSim* S, PyroSolveInfo* info) {
   clear_error();
   PYRO_REQUIRE(S && info, "pyro_sim_last_solve: null argument");
   *info = S->last;
+  return PYRO_OK;
+}
+
+int pyro_sim_render_pack(PyroSim* S, int with_bricks) {
+  clear_error();
+  PYRO_REQUIRE(S, "pyro_sim_render_pack: null simulation");
+  const size_t n = S->d.cells();
+  const size_t nb = (size_t)((S->d.nx + 7) / 8) * ((S->d.ny + 7) / 8) * ((S->d.nz + 7) / 8);
+  int rc;
+  if (!S->rvol.p) {  // first call: the three volumes and the brick maxima
+    if ((rc = S->rvol.alloc(n * 8)) != PYRO_OK || (rc = S->rsol.alloc(n * 8)) != PYRO_OK ||
+        (rc = S->rvel.alloc(n * 8)) != PYRO_OK || (rc = S->bricks.alloc(nb * 4)) != PYRO_OK)
+      return rc;
+  }
+  const int c = S->cur;
+  PYRO_CU(launch_render_pack(S->params.as<PyroParams>(), S->d, S->s0.as<float4>(),
+                             S->s1.as<float4>(), S->sol[c].as<float4>(),
+                             S->flags.as<uint32_t>(), S->vel[c][0].as<float>(),
+                             S->vel[c][1].as<float>(), S->vel[c][2].as<float>(), S->rvol.p,
+                             S->rsol.p, S->rvel.p, S->stream));
+  if (with_bricks)
+    PYRO_CU(launch_render_bricks(S->d, S->rvol.p, S->rsol.p, S->bricks.as<float>(), S->stream));
   return PYRO_OK;
 }
 

@@ -147,7 +147,11 @@ class Sim:
 
     def read_field(self, which: int) -> np.ndarray:
         nx, ny, nz = self.dims
-        if which in (_abi.F_U, _abi.F_V, _abi.F_W):
+        if which in (_abi.F_RVOL, _abi.F_RSOL, _abi.F_RVEL):
+            out = np.empty((nz, ny, nx, 4), dtype=np.float16)
+        elif which == _abi.F_BRICKS:
+            out = np.empty(((nz + 7) // 8, (ny + 7) // 8, (nx + 7) // 8), dtype=np.float32)
+        elif which in (_abi.F_U, _abi.F_V, _abi.F_W):
             out = np.empty((nz + 1, ny + 1, nx + 1), dtype=np.float32)
         elif which == _abi.F_FLAGS:
             out = np.empty((nz, ny, nx), dtype=np.uint32)
@@ -167,6 +171,20 @@ class Sim:
     def read_scalars(self) -> Tuple[np.ndarray, np.ndarray]:
         """(s0, s1) copies, each (nz, ny, nx, 4) (src/sim.rs:494-508)."""
         return self.read_field(_abi.F_S0), self.read_field(_abi.F_S1)
+
+    def render_pack(self, bricks: bool = True) -> None:
+        """The renderer's per-frame input pack (render.wgsl:3-61) into the
+        simulation's volumes; read them with read_field(F_RVOL / F_RSOL /
+        F_RVEL / F_BRICKS) or borrow them with device_ptr."""
+        _abi.check("pyro_sim_render_pack",
+                   self._lib.pyro_sim_render_pack(self._h, 1 if bricks else 0))
+
+    def read_render_volumes(self, bricks: bool = True):
+        """(vol, sol, vel) float16 (nz, ny, nx, 4) and the brick maxima
+        (float32, one per 8^3 brick, or None) of a fresh pack."""
+        self.render_pack(bricks)
+        return (self.read_field(_abi.F_RVOL), self.read_field(_abi.F_RSOL),
+                self.read_field(_abi.F_RVEL), self.read_field(_abi.F_BRICKS) if bricks else None)
 
     def set_solver(self, mode: int, tol: float = 1e-3, max_iters: int = 50) -> None:
         _abi.check("pyro_sim_set_solver",

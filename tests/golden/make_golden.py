@@ -2,7 +2,8 @@
 
     python tests/golden/make_golden.py [--ref /root/reference] [--only name,...]
 
-For each simulation kernel the script assembles the shader source exactly as
+For each simulation kernel (and the renderer's input pack, render.wgsl) the
+script assembles the shader source exactly as
 the reference's host does (src/gpu.rs:190-237: common.wgsl first unless the
 kernel is a multigrid one, then the template / velocity / statistics blocks
 its //@ directives name, then the kernel body), interprets it with
@@ -63,6 +64,9 @@ class Ref:
         self.kernels = {}
         for f in ("advect.wgsl", "fluid.wgsl", "combust.wgsl", "mg.wgsl"):
             self.kernels.update(split_kernels(rd(f)))
+        # the renderer's input pack (src/render.rs:135,229-230: with common.wgsl)
+        rk = split_kernels(rd("render.wgsl"))
+        self.kernels["pack"], self.kernels["bricks"] = rk["pack"], rk["bricks"]
 
     def assemble(self, name):
         """src/gpu.rs:212-237."""
@@ -228,6 +232,37 @@ def gen_sim(ref, only):
     return out
 
 
+def gen_render(ref, only):
+    """The pack and bricks dispatches of src/render.rs:263-292 on the step's
+    fields: three rgba16float textures (binary16 arrays here) and the 8^3
+    brick maxima read back from two of them."""
+    if only is not None and "render" not in only:
+        return {}
+    out = {}
+    for case, (dims, seed) in enumerate([(GOLDEN_DIMS, 21), ((17, 9, 11), 22)]):
+        nx, ny, nz = dims
+        n = (nz, ny, nx)
+        P = params_for(nx, ny, nz, dx=0.05, dt=0.02, ign_on=1.0, wind=0.0, sponge=2.0)
+        S = random_state(P, seed=seed)
+        pb = np.frombuffer(P.to_bytes(), np.uint8).copy()
+        vol = np.zeros(n + (4,), np.float16)
+        solt = np.zeros(n + (4,), np.float16)
+        vel = np.zeros(n + (4,), np.float16)
+        t1 = run_kernel(ref, "pack", P, {1: flat(S["s0"]), 2: flat(S["s1"]), 3: flat(S["sol"]),
+                                         4: flat(S["flags"]), 5: flat(S["u"]), 6: flat(S["v"]),
+                                         7: flat(S["w"]), 8: vol, 9: solt, 10: vel},
+                        groups3(dims))
+        nb = tuple((v + 7) // 8 for v in dims)
+        bricks = np.zeros(nb[0] * nb[1] * nb[2], np.float32)
+        t2 = run_kernel(ref, "bricks", P, {1: vol, 2: solt, 3: bricks}, groups3(nb))
+        out[f"render_c{case}"] = dict(params=pb, s0=S["s0"], s1=S["s1"], sol=S["sol"],
+                                      flags=S["flags"], u=S["u"], v=S["v"], w=S["w"], vol=vol,
+                                      solt=solt, vel=vel,
+                                      bricks=bricks.reshape(nb[2], nb[1], nb[0]))
+        print(f"render c{case} {t1:.1f}+{t2:.1f}s", flush=True)
+    return out
+
+
 def lv(d, h):
     return {"nx": np.uint32(d[0]), "ny": np.uint32(d[1]), "nz": np.uint32(d[2]), "h": np.float32(h)}
 
@@ -311,6 +346,7 @@ def main():
     out = {}
     out.update(gen_sim(ref, only))
     out.update(gen_mg(ref, only))
+    out.update(gen_render(ref, only))
     for k, d in out.items():
         np.savez_compressed(os.path.join(HERE, k + ".npz"), **d)
     print(f"wrote {len(out)} fixtures to {HERE}")

@@ -521,7 +521,23 @@ def _atomic_max(r, v):
     return cur
 
 
+def _texture_store(tex, c, v):
+    """textureStore on a 3D storage texture bound as an (nz, ny, nx, 4)
+    array: the texel keeps the texture's precision (an rgba16float array
+    holds binary16, converted with round to nearest even); stores outside
+    the texture are discarded."""
+    x, y, z = int(c[0]), int(c[1]), int(c[2])
+    if 0 <= z < tex.shape[0] and 0 <= y < tex.shape[1] and 0 <= x < tex.shape[2]:
+        tex[z, y, x] = np.asarray(v, dtype=F32).astype(tex.dtype)
+
+
+def _texture_load(tex, c, level):
+    """textureLoad of one texel of a 3D texture, as vec4<f32>."""
+    return tex[int(c[2]), int(c[1]), int(c[0])].astype(F32)
+
+
 BUILTINS: Dict[str, Callable] = {
+    "textureStore": _texture_store, "textureLoad": _texture_load,
     "clamp": _clamp, "min": _minmax(np.minimum), "max": _minmax(np.maximum), "mix": _mix,
     "smoothstep": _smoothstep, "select": _select, "exp": np.exp, "sqrt": np.sqrt,
     "length": _length, "cross": _cross, "floor": np.floor, "abs": np.abs,
@@ -946,6 +962,9 @@ def _shr(a, b):
 def _div(a, b):
     if type(a) is int and type(b) is int:
         return int(a / b)
+    rt = np.result_type(a, b)
+    if np.issubdtype(rt, np.integer):  # WGSL integer division truncates toward zero
+        return np.trunc(np.true_divide(a, b)).astype(rt)
     return a / b
 
 

@@ -169,3 +169,20 @@ def test_fixture_set_is_complete():
     want |= {"mg_smooth_c0_w10", "mg_smooth_c1_w10", "mg_smooth_c0_w16", "mg_smooth_c1_w16",
              "mg_restrict", "mg_prolong", "mg_resid"}
     assert want <= names, want - names
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_render_pack_and_bricks(case):
+    """The renderer's input pack (render.wgsl:3-61): the oracle's three
+    binary16 volumes and the brick maxima equal the interpreted WGSL's bit
+    for bit (the texture store rounds to nearest even in both)."""
+    d = _load(f"render_{case}")
+    P = _params(d)
+    vol, solt, vel = oracle.render_pack(P, d["s0"], d["s1"], d["sol"], d["flags"], d["u"],
+                                        d["v"], d["w"])
+    assert np.array_equal(vol.view(np.uint16), d["vol"].view(np.uint16))
+    assert np.array_equal(solt.view(np.uint16), d["solt"].view(np.uint16))
+    assert np.array_equal(vel.view(np.uint16), d["vel"].view(np.uint16))
+    b = oracle.render_bricks((P.nx, P.ny, P.nz), d["vol"], d["solt"])
+    assert np.array_equal(b, d["bricks"])
+    assert (d["flags"] == 1).any() and (d["flags"] != 1).any()

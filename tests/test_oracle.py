@@ -106,3 +106,25 @@ def test_quiescent_scene_stays_quiescent_without_ignition():
     s0 = sim.read_field(oracle.F_S0)
     assert np.allclose(s0[..., 0], P.t0)
     assert np.abs(sim.read_field(oracle.F_V)).max() < 1e-6
+
+
+def test_f16_conversion_matches_ieee_round_to_nearest_even():
+    """The oracle's binary32 -> binary16 conversion (the renderer's texture
+    stores) against numpy's, which rounds to nearest even: normal,
+    subnormal and overflowing values, the ties at both ends of the range."""
+    rng = np.random.default_rng(3)
+    x = np.concatenate([
+        rng.normal(0, 1, 100000), rng.normal(0, 1e4, 100000), rng.normal(0, 1e-5, 100000),
+        np.array([65504, 65519.99, 65520, 65535, 1e6, -1e6, 5.96e-8, 2.98e-8, 2.9802322e-08,
+                  2.9802326e-08, 1e-9, 0.0, -0.0, 6.1035156e-05, 6.1e-05, np.inf, -np.inf]),
+    ]).astype(np.float32)
+    with np.errstate(over="ignore"):
+        ref = x.astype(np.float16).view(np.uint16)
+    assert np.array_equal(oracle.f32_to_f16(x), ref)
+    # ties: halfway between two binary16 values rounds to the even one
+    lo = np.arange(0x3c00, 0x3c40, dtype=np.uint16).view(np.float16).astype(np.float64)
+    mid = ((lo[:-1] + lo[1:]) / 2).astype(np.float32)
+    assert np.array_equal(oracle.f32_to_f16(mid), mid.astype(np.float16).view(np.uint16))
+    bits = np.arange(65536, dtype=np.uint16)
+    fin = np.isfinite(bits.view(np.float16))
+    assert np.array_equal(oracle.f16_to_f32(bits)[fin], bits.view(np.float16).astype(np.float32)[fin])
