@@ -504,6 +504,26 @@ def run_ours(args):
         "bricks_gbs": RENDER_BRICKS_BYTES * cells / (bricks_ms * 1e-3) / 1e9,
     }
     frame_pack["pack_frac"] = frame_pack["pack_gbs"] / load_peaks()[0]
+    # the fire-light sampling tables: ecells and the FP64 CDF scan
+    from pyro_b200 import color
+    lut_dev = torch.from_numpy(color.build_lut()).cuda()
+    chemi = color.chemi_block()
+    chp = chemi.ctypes.data_as(__import__("ctypes").c_void_p)
+    _abi.check("pyro_sim_render_emission",
+               lib.pyro_sim_render_emission(sim._h, __import__("ctypes").c_void_p(
+                   lut_dev.data_ptr()), chp))  # first call allocates
+    sim.sync()
+    ev[0].record(stream)
+    for _ in range(reps):
+        _abi.check("pyro_sim_render_emission", lib.pyro_sim_render_emission(
+            sim._h, __import__("ctypes").c_void_p(lut_dev.data_ptr()), chp))
+    ev[1].record(stream)
+    ev[1].synchronize()
+    frame_pack["emission_ms"] = ev[0].elapsed_time(ev[1]) / reps
+    ecell = sim.read_field(_abi.F_ECELL)
+    frame_pack["emitting_cells"] = int((ecell > 0).sum())
+    log(f"render emission (ecells + CDF) {frame_pack['emission_ms']:.3f} ms, "
+        f"{frame_pack['emitting_cells']} emitting cells")
     log(f"render pack {pack_ms:.3f} ms ({frame_pack['pack_gbs']:.0f} GB/s), "
         f"bricks {bricks_ms:.3f} ms")
 
@@ -527,6 +547,13 @@ def run_ours(args):
                 log(f"field {f}: {bad} non-finite values")
         cms, cores = cpu_baseline_run(sc, sim.p, fields[A.F_SOL], fields, args.cpu_steps, dt,
                                       float(sim.time))
+        # the reference forms the emission CDF on the CPU from a read-back
+        # buffer (src/render.rs:316-333): its loop, timed here on the same
+        # emission values (the copies to and from the device not included)
+        import oracle
+        t0_ = time.perf_counter()
+        oracle.render_cdf(ecell)
+        frame_pack["cdf_cpu_ms_reference_loop"] = (time.perf_counter() - t0_) * 1e3
         cpu = {"value": cms, "unit": UNIT, "cores": cores, "kind": "port",
                "sample": f"{args.cpu_steps} full substeps of the same developed state "
                          "(C++ oracle restating the reference's WGSL kernels, OpenMP)"}

@@ -88,8 +88,13 @@ enum PyroField {
   PYRO_F_RSOL = 12,   /* half4 * N: occupancy, then Ts, char fraction and
                          material slot premultiplied by the occupancy     */
   PYRO_F_RVEL = 13,   /* half4 * N: cell-centred velocity m/s, 0          */
-  PYRO_F_BRICKS = 14  /* float * ceil(nx/8)*ceil(ny/8)*ceil(nz/8): the
+  PYRO_F_BRICKS = 14, /* float * ceil(nx/8)*ceil(ny/8)*ceil(nz/8): the
                          visibility maximum of each 8^3 brick             */
+  /* the renderer's fire-light sampling tables of the last
+   * pyro_sim_render_emission (none before the first call)                */
+  PYRO_F_ECELL = 15,  /* float * N: emission power per cell               */
+  PYRO_F_ECDF = 16    /* float * (N + 1): its cumulative distribution,
+                         then the total                                   */
 };
 
 /* Pressure solver modes for pyro_sim_set_solver / pyro_poisson_solve. */
@@ -202,6 +207,19 @@ int pyro_sim_set_net(PyroSim* sim, PyroNet* net);
  * on the simulation's stream; the first call allocates the volumes
  * (24 bytes per cell) and so must not run inside a stream capture. */
 int pyro_sim_render_pack(PyroSim* sim, int with_bricks);
+/* The renderer's fire-light sampling tables (src/render.rs:304-333): the
+ * ecells kernel (render.wgsl:63-98) on the packed volume, then the emission
+ * CDF.  The reference reads the emission back and forms the CDF on the CPU
+ * (FP64 running sum, then c / total as f32, and the total last); here it
+ * is an FP64 scan on the GPU.  lut_dev: the first 1024 float4 rows of the
+ * renderer's colour table (soot emission, src/color.rs:46-70), on the
+ * device; chemi: 4 host floats (chemiluminescence strength, soot
+ * extinction per ppm at 550 nm, smoke extinction per g/m^3, 0;
+ * src/render.rs:169-174).  Needs a pyro_sim_render_pack first.
+ * Asynchronous on the simulation's stream; the first call allocates
+ * 8 bytes per cell and so must not run inside a stream capture. */
+int pyro_sim_render_emission(PyroSim* sim, const float* lut_dev,
+                             const float* chemi);
 int pyro_sim_destroy(PyroSim* sim);
 
 /* ---- scene voxelizer (Scene::voxelize, src/scene.rs:621-667) ---------- */
@@ -338,6 +356,15 @@ int pyro_k_render_pack(const PyroParams* params_dev, uint32_t nx, uint32_t ny,
                        const float* sol, const uint32_t* flags, const float* u,
                        const float* v, const float* w, void* vol, void* sol_out,
                        void* vel, void* stream);
+/* Emission power per cell (render.wgsl:63-98) from a packed vol volume;
+ * lut (device) and chemi (host) as pyro_sim_render_emission. */
+int pyro_k_render_ecells(const PyroParams* params_dev, uint32_t nx,
+                         uint32_t ny, uint32_t nz, const void* vol,
+                         const float* lut, const float* chemi, float* ecell,
+                         void* stream);
+/* The emission CDF of n values into cdf (n + 1 floats; src/render.rs:316-333).
+ * Allocates its scratch and blocks until done. */
+int pyro_k_render_cdf(uint64_t n, const float* ecell, float* cdf, void* stream);
 /* Brick maxima (render.wgsl:38-61) from packed vol and sol volumes into
  * bricks, float * ceil(nx/8)*ceil(ny/8)*ceil(nz/8), x fastest. */
 int pyro_k_render_bricks(uint32_t nx, uint32_t ny, uint32_t nz,

@@ -42,6 +42,8 @@ _SIGS = {
     "or_project": (None, [_P] * 6),
     "or_render_pack": (None, [_P] * 11),
     "or_render_bricks": (None, [_I, _I, _I, _P, _P, _P]),
+    "or_render_ecells": (None, [_P] * 5),
+    "or_render_cdf": (None, [ctypes.c_size_t, _P, _P]),
     "or_f32_to_f16": (None, [_P, _P, ctypes.c_size_t]),
     "or_f16_to_f32": (None, [_P, _P, ctypes.c_size_t]),
     "or_mg_smooth": (None, [_I, _I, _I, _F, _P, _P, _P, _I, _F, _I]),
@@ -184,6 +186,24 @@ def render_bricks(dims, vol, solt):
     out = np.zeros(((nz + 7) // 8, (ny + 7) // 8, (nx + 7) // 8), np.float32)
     lib().or_render_bricks(nx, ny, nz, ptr(vol), ptr(solt), ptr(out))
     return out
+
+
+def render_ecells(P, vol, lut, chemi):
+    """render.wgsl:63-98: float32 (nz, ny, nx) emission power per cell."""
+    nx, ny, nz = dims_of(P)
+    e = np.zeros((nz, ny, nx), np.float32)
+    lib().or_render_ecells(ptr(P), ptr(np.ascontiguousarray(vol)),
+                           ptr(np.ascontiguousarray(lut, np.float32)),
+                           ptr(np.ascontiguousarray(chemi, np.float32)), ptr(e))
+    return e
+
+
+def render_cdf(e):
+    """src/render.rs:316-333: float32 (n + 1,)."""
+    e = np.ascontiguousarray(e, np.float32).reshape(-1)
+    cdf = np.zeros(e.size + 1, np.float32)
+    lib().or_render_cdf(ctypes.c_size_t(e.size), ptr(e), ptr(cdf))
+    return cdf
 
 
 def f32_to_f16(x):

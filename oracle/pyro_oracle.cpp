@@ -1084,6 +1084,61 @@ static void render_bricks(int nx, int ny, int nz, const uint16_t* volT, const ui
       }
 }
 
+// render.wgsl:63-98: emission power per cell with the six-axis escape
+static void render_ecells(const Ctx& C, const uint16_t* volT, const F4* lut, const float* chemi,
+                          float* ecell) {
+  const float dx = C.P->dx;
+  for (int z = 0; z < C.nz; z++)
+    for (int y = 0; y < C.ny; y++)
+      for (int x = 0; x < C.nx; x++) {
+        const I3 c{x, y, z};
+        const size_t i = C.sidx(c);
+        const float vx = f16_to_f32(volT[4 * i]), vy = f16_to_f32(volT[4 * i + 1]);
+        const float vw = f16_to_f32(volT[4 * i + 3]);
+        // lutAt (render.wgsl:68-72)
+        const float xt = clampf((vy - 300.0f) / 3000.0f, 0.0f, 1.0f) * 1023.0f;
+        const uint32_t li = (uint32_t)std::floor(xt);
+        const F4 l0 = lut[li], l1 = lut[std::min(li + 1u, 1023u)];
+        const float fr = xt - (float)li;
+        const float sx = wmax(vx, 0.0f);
+        const float a = chemi[0] * wmax(vw, 0.0f) * std::exp(-20.0f * sx);
+        const float er = mixf(l0.x, l1.x, fr) * sx * 1e-6f + a * 0.12f;
+        const float eg = mixf(l0.y, l1.y, fr) * sx * 1e-6f + a * 0.28f;
+        const float eb = mixf(l0.z, l1.z, fr) * sx * 1e-6f + a * 1.0f;
+        float e = (er * 0.2126f + eg * 0.7152f + eb * 0.0722f) * dx * dx * dx;
+        if (e > 0.0f) {
+          float esc = 0.0f;
+          for (int k = 0; k < 6; k++) {
+            float od = 0.0f;
+            I3 p = c;
+            for (int s = 0; s < 48; s++) {
+              p = I3{p.x + DIRS[k].x, p.y + DIRS[k].y, p.z + DIRS[k].z};
+              if (!C.inb(p) || od > 7.0f) break;
+              const size_t q = C.sidx(p);
+              const float wx = f16_to_f32(volT[4 * q]), wz = f16_to_f32(volT[4 * q + 2]);
+              od += (chemi[1] * wmax(wx, 0.0f) + chemi[2] * wmax(wz, 0.0f)) * dx;
+            }
+            esc += std::exp(-od);
+          }
+          e *= wmax(esc / 6.0f, 0.02f);
+        }
+        ecell[i] = e;
+      }
+}
+
+// src/render.rs:316-333: FP64 running sum, c / total as f32, the total last
+static void render_cdf(size_t n, const float* e, float* cdf) {
+  std::vector<double> out(n);
+  double acc = 0.0;
+  for (size_t i = 0; i < n; i++) {
+    acc += (double)wmax(e[i], 0.0f);
+    out[i] = acc;
+  }
+  const double total = acc;
+  for (size_t i = 0; i < n; i++) cdf[i] = total > 0.0 ? (float)(out[i] / total) : 0.0f;
+  cdf[n] = (float)total;
+}
+
 extern "C" {
 
 void or_set_threads(int n) {
@@ -1186,6 +1241,12 @@ void or_render_bricks(int nx, int ny, int nz, const uint16_t* vol, const uint16_
                       float* bricks) {
   render_bricks(nx, ny, nz, vol, solt, bricks);
 }
+void or_render_ecells(const PyroParams* P, const uint16_t* vol, const float* lut,
+                      const float* chemi, float* ecell) {
+  Ctx C(P);
+  render_ecells(C, vol, (const F4*)lut, chemi, ecell);
+}
+void or_render_cdf(size_t n, const float* ecell, float* cdf) { render_cdf(n, ecell, cdf); }
 void or_f32_to_f16(const float* x, uint16_t* h, size_t n) {
   for (size_t i = 0; i < n; i++) h[i] = f32_to_f16(x[i]);
 }

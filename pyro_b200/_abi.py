@@ -25,6 +25,7 @@ ABI_VERSION = 2
 
 F_S0, F_S1, F_SOL, F_PYR, F_FLAGS, F_CURL, F_U, F_V, F_W, F_PHI, F_B = range(11)
 F_RVOL, F_RSOL, F_RVEL, F_BRICKS = range(11, 15)  # renderer input pack
+F_ECELL, F_ECDF = 15, 16  # renderer fire-light sampling tables
 
 PROFILE_PHASES = ["solid", "curl", "adv_vel1", "adv_vel2", "adv_s1", "adv_s2", "react",
                   "forces", "divergence", "pressure", "project", "total"]
@@ -135,6 +136,7 @@ SIGNATURES = {
     "pyro_sim_last_solve": [_P, ctypes.POINTER(PyroSolveInfo)],
     "pyro_sim_destroy": [_P],
     "pyro_sim_render_pack": [_P, _I],
+    "pyro_sim_render_emission": [_P, _P, _P],
     "pyro_voxelize": [ctypes.POINTER(PyroShape), _U32, _U32, _U32, _U32, _F, _F, _U32,
                       _P, _P, _P, _P],
     "pyro_poisson_create": [_U32, _U32, _U32, _F, _I, ctypes.POINTER(_P)],
@@ -159,6 +161,8 @@ SIGNATURES = {
     "pyro_k_mg_coarse_sym": [_U32, _U32, _U32, _F, _P, _P, _P, _I, _F, _I, _P],
     "pyro_k_render_pack": [_P, _U32, _U32, _U32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
     "pyro_k_render_bricks": [_U32, _U32, _U32, _P, _P, _P, _P],
+    "pyro_k_render_ecells": [_P, _U32, _U32, _U32, _P, _P, _P, _P, _P],
+    "pyro_k_render_cdf": [ctypes.c_uint64, _P, _P, _P],
     "pyro_conv3_forward": [_P, _I, _I, _I, _I, _I, _P, _I, _P, _I, _P, _I, _P],
     "pyro_conv3_backward_data": [_P, _I, _I, _I, _I, _I, _P, _I, _P, _P, _I, _P],
     "pyro_conv3_backward_weight": [_P, _I, _P, _I, _I, _I, _I, _I, _P, _P],

@@ -252,6 +252,27 @@ int pyro_k_render_bricks(uint32_t nx, uint32_t ny, uint32_t nz, const void* vol,
   return ret(launch_render_bricks(d, vol, sol_packed, bricks, S(stream)), "pyro_k_render_bricks");
 }
 
+int pyro_k_render_ecells(const PyroParams* params_dev, uint32_t nx, uint32_t ny, uint32_t nz,
+                         const void* vol, const float* lut, const float* chemi, float* ecell,
+                         void* stream) {
+  KDIMS(pyro_k_render_ecells)
+  PYRO_REQUIRE(vol && lut && chemi && ecell, "pyro_k_render_ecells: null buffer");
+  return ret(launch_render_ecells(params_dev, d, vol, lut, chemi, ecell, S(stream)),
+             "pyro_k_render_ecells");
+}
+
+int pyro_k_render_cdf(uint64_t n, const float* ecell, float* cdf, void* stream) {
+  clear_error();
+  PYRO_REQUIRE(n >= 1 && n <= (uint64_t)1 << 34, "pyro_k_render_cdf: invalid length");
+  PYRO_REQUIRE(ecell && cdf, "pyro_k_render_cdf: null buffer");
+  DevBuf scratch;  // the scan's block sums
+  int rc = scratch.alloc(render_cdf_scratch_bytes((long)n));
+  if (rc != PYRO_OK) return rc;
+  cudaError_t e = launch_render_cdf((long)n, ecell, cdf, scratch.p, S(stream));
+  if (e == cudaSuccess) e = cudaStreamSynchronize(S(stream));  // before scratch is freed
+  return ret(e, "pyro_k_render_cdf");
+}
+
 int pyro_voxelize(const PyroShape* shapes, uint32_t n_shapes, uint32_t nx, uint32_t ny,
                   uint32_t nz, float dx, float t0, uint32_t seed, const float* slot_density,
                   const uint32_t* slot_kind, float* sol_out, void* stream) {

@@ -105,7 +105,177 @@ __global__ void __launch_bounds__(RB_THREADS) k_render_bricks(Grid g, int bnx, i
   }
 }
 
+// Emission power of each cell for the renderer's fire-light sampling
+// (render.wgsl:63-98): soot emission from the first 1024 rows of the colour
+// table at the cell's temperature plus chemiluminescence, luminance times
+// the cell volume, weighted by the mean escape transmittance along the six
+// axes (rays of up to 48 cells that stop once the optical depth passes 7).
+// The ray samples are loaded eight at a time before the sequential sum,
+// which keeps the reference's stopping rule and summation order.
+__device__ __forceinline__ float ray_depth(const Grid& g, const uint2* __restrict__ vol, I3 c,
+                                           I3 d, float ks, float km, float dx) {
+  float od = 0.0f;
+  for (int s0 = 1; s0 <= 48; s0 += 8) {
+    float w[8];
+    bool in[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      const int s = s0 + j;
+      const I3 p{c.x + s * d.x, c.y + s * d.y, c.z + s * d.z};
+      in[j] = s <= 48 && g.inb(p);
+      w[j] = 0.0f;
+      if (in[j]) {
+        const float4 v = unhalf4(__ldg(vol + g.sidx(p)));
+        w[j] = ks * fmaxf(v.x, 0.0f) + km * fmaxf(v.z, 0.0f);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      if (!in[j] || od > 7.0f) return od;
+      od += w[j] * dx;
+    }
+  }
+  return od;
+}
+
+__global__ void __launch_bounds__(RP_BX * RP_BY) k_render_ecells(
+    const PyroParams* __restrict__ Pp, Grid g, const uint2* __restrict__ vol,
+    const float4* __restrict__ lut, float4 chemi, float* __restrict__ ecell) {
+  const int x = blockIdx.x * RP_BX + threadIdx.x, y = blockIdx.y * RP_BY + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny) return;
+  const I3 c{x, y, z};
+  const int i = g.sidx(c);
+  const float dx = Pp->dx;
+  const float4 v = unhalf4(__ldg(vol + i));
+  // lutAt(T): linear in the table's 1024 temperature rows
+  const float xt = wclamp((v.y - 300.0f) / 3000.0f, 0.0f, 1.0f) * 1023.0f;
+  const uint32_t li = (uint32_t)floorf(xt);
+  const float4 l0 = __ldg(lut + li), l1 = __ldg(lut + min(li + 1u, 1023u));
+  const float fr = xt - (float)li;
+  const float sx = fmaxf(v.x, 0.0f);
+  const float a = chemi.x * fmaxf(v.w, 0.0f) * expf(-20.0f * sx);
+  const float er = wmix(l0.x, l1.x, fr) * sx * 1e-6f + a * 0.12f;
+  const float eg = wmix(l0.y, l1.y, fr) * sx * 1e-6f + a * 0.28f;
+  const float eb = wmix(l0.z, l1.z, fr) * sx * 1e-6f + a * 1.0f;
+  float e = (er * 0.2126f + eg * 0.7152f + eb * 0.0722f) * dx * dx * dx;
+  if (e > 0.0f) {
+    float esc = 0.0f;
+#pragma unroll 1
+    for (int k = 0; k < 6; k++) esc += expf(-ray_depth(g, vol, c, dir6(k), chemi.y, chemi.z, dx));
+    e *= fmaxf(esc / 6.0f, 0.02f);
+  }
+  ecell[i] = e;
+}
+
+// The emission CDF (src/render.rs:316-333, a CPU loop over a read-back
+// buffer in the reference): cdf[i] = (sum_{j<=i} max(e_j, 0)) / total as
+// float, cdf[n] = total, all sums in FP64.  Three deterministic passes:
+// per-block sums, one block scanning those, per-block scan plus offset.
+constexpr int CDF_T = 512, CDF_PER = 16, CDF_SPAN = CDF_T * CDF_PER;
+
+// exclusive scan of one double per thread across the block (fixed order)
+__device__ __forceinline__ double block_exscan(double v, double* sh, double* total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  double inc = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const double t = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += t;
+  }
+  if (lane == 31) sh[wid] = inc;
+  __syncthreads();
+  if (wid == 0) {
+    double w = lane < CDF_T / 32 ? sh[lane] : 0.0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const double t = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += t;
+    }
+    if (lane < CDF_T / 32) sh[lane] = w;  // inclusive warp prefixes
+  }
+  __syncthreads();
+  const double off = wid > 0 ? sh[wid - 1] : 0.0;
+  *total = sh[CDF_T / 32 - 1];
+  return off + inc - v;
+}
+
+__global__ void __launch_bounds__(CDF_T) k_cdf_sums(const float* __restrict__ e, long n,
+                                                    double* __restrict__ bsum) {
+  __shared__ double sh[CDF_T / 32];
+  const long base = (long)blockIdx.x * CDF_SPAN + (long)threadIdx.x * CDF_PER;
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < CDF_PER; k++)
+    if (base + k < n) s += (double)fmaxf(__ldg(e + base + k), 0.0f);
+  double tot;
+  block_exscan(s, sh, &tot);
+  if (threadIdx.x == 0) bsum[blockIdx.x] = tot;
+}
+
+// bsum[0..nb) -> exclusive prefixes in place, bsum[nb] = the total
+__global__ void __launch_bounds__(CDF_T) k_cdf_blocks(double* __restrict__ bsum, int nb) {
+  __shared__ double sh[CDF_T / 32];
+  double carry = 0.0;
+  for (int b0 = 0; b0 < nb; b0 += CDF_T) {
+    const int b = b0 + threadIdx.x;
+    const double v = b < nb ? bsum[b] : 0.0;
+    double tot;
+    const double ex = block_exscan(v, sh, &tot);
+    __syncthreads();  // every thread has read sh before the next chunk writes it
+    if (b < nb) bsum[b] = carry + ex;
+    carry += tot;
+  }
+  if (threadIdx.x == 0) bsum[nb] = carry;
+}
+
+__global__ void __launch_bounds__(CDF_T) k_cdf_final(const float* __restrict__ e, long n,
+                                                     const double* __restrict__ bsum, int nb,
+                                                     float* __restrict__ cdf) {
+  __shared__ double sh[CDF_T / 32];
+  const long base = (long)blockIdx.x * CDF_SPAN + (long)threadIdx.x * CDF_PER;
+  float v[CDF_PER];
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < CDF_PER; k++) {
+    v[k] = base + k < n ? fmaxf(__ldg(e + base + k), 0.0f) : 0.0f;
+    s += (double)v[k];
+  }
+  double tot;
+  double acc = bsum[blockIdx.x] + block_exscan(s, sh, &tot);
+  const double total = bsum[nb];
+#pragma unroll
+  for (int k = 0; k < CDF_PER; k++) {
+    acc += (double)v[k];
+    if (base + k < n) cdf[base + k] = total > 0.0 ? (float)(acc / total) : 0.0f;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) cdf[n] = (float)total;
+}
+
 }  // namespace
+
+size_t render_cdf_scratch_bytes(long n) {
+  return (size_t)((n + CDF_SPAN - 1) / CDF_SPAN + 1) * sizeof(double);
+}
+
+cudaError_t launch_render_ecells(const PyroParams* P, Dims3 d, const void* vol, const float* lut,
+                                 const float* chemi, float* ecell, cudaStream_t st) {
+  dim3 grid((d.nx + RP_BX - 1) / RP_BX, (d.ny + RP_BY - 1) / RP_BY, d.nz);
+  k_render_ecells<<<grid, dim3(RP_BX, RP_BY), 0, st>>>(
+      P, Grid{d.nx, d.ny, d.nz}, (const uint2*)vol, (const float4*)lut,
+      make_float4(chemi[0], chemi[1], chemi[2], chemi[3]), ecell);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_render_cdf(long n, const float* ecell, float* cdf, void* scratch,
+                              cudaStream_t st) {
+  const int nb = (int)((n + CDF_SPAN - 1) / CDF_SPAN);
+  double* bsum = (double*)scratch;
+  k_cdf_sums<<<nb, CDF_T, 0, st>>>(ecell, n, bsum);
+  k_cdf_blocks<<<1, CDF_T, 0, st>>>(bsum, nb);
+  k_cdf_final<<<nb, CDF_T, 0, st>>>(ecell, n, bsum, nb, cdf);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_render_pack(const PyroParams* P, Dims3 d, const float4* s0, const float4* s1,
                                const float4* sol, const uint32_t* flags, const float* u,

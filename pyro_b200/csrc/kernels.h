@@ -61,6 +61,14 @@ cudaError_t launch_render_pack(const PyroParams* P, Dims3 d, const float4* s0, c
                                cudaStream_t st);
 cudaError_t launch_render_bricks(Dims3 d, const void* vol, const void* solp, float* bricks,
                                  cudaStream_t st);
+// Emission power per cell from the packed vol and the soot colour table
+// (1024 float4), chemi = 4 host floats; and its FP64 cumulative
+// distribution (n + 1 floats) with render_cdf_scratch_bytes(n) of scratch.
+cudaError_t launch_render_ecells(const PyroParams* P, Dims3 d, const void* vol, const float* lut,
+                                 const float* chemi, float* ecell, cudaStream_t st);
+size_t render_cdf_scratch_bytes(long n);
+cudaError_t launch_render_cdf(long n, const float* ecell, float* cdf, void* scratch,
+                              cudaStream_t st);
 cudaError_t launch_project(const PyroParams* P, Dims3 d, float* u, float* v, float* w,
                            const float* phi, const uint32_t* flags, cudaStream_t st);
 

@@ -44,6 +44,7 @@ struct PyroSim {
   DevBuf s0, s1, s0b, s1b, h0, h1, sol[2], pyr, curl, flags, phi0, b0;
   DevBuf stats, params;
   DevBuf rvol, rsol, rvel, bricks;  // renderer input pack, allocated by its first call
+  DevBuf ecell, ecdf, cdf_scratch;  // renderer emission power and its CDF (first call)
   Multigrid mg;
   Solver solver;
 
@@ -197,6 +198,8 @@ struct PyroSim {
       case PYRO_F_RSOL: *bytes = rsol.bytes; return rsol.p;
       case PYRO_F_RVEL: *bytes = rvel.bytes; return rvel.p;
       case PYRO_F_BRICKS: *bytes = bricks.bytes; return bricks.p;
+      case PYRO_F_ECELL: *bytes = ecell.bytes; return ecell.p;
+      case PYRO_F_ECDF: *bytes = ecdf.bytes; return ecdf.p;
       default: *bytes = 0; return nullptr;
     }
   }
@@ -209,7 +212,7 @@ struct PyroSim {
     s += lohi.bytes + btrace.bytes;
     const DevBuf* list[] = {&s0, &s1, &s0b, &s1b, &h0, &h1, &sol[0], &sol[1], &pyr,
                             &curl, &flags, &phi0, &b0, &stats, &params, &rvol, &rsol, &rvel,
-                            &bricks};
+                            &bricks, &ecell, &ecdf, &cdf_scratch};
     for (auto* b : list) s += b->bytes;
     return s + mg.device_bytes() + solver.device_bytes();
   }
@@ -575,6 +578,24 @@ int pyro_sim_render_pack(PyroSim* S, int with_bricks) {
                              S->rsol.p, S->rvel.p, S->stream));
   if (with_bricks)
     PYRO_CU(launch_render_bricks(S->d, S->rvol.p, S->rsol.p, S->bricks.as<float>(), S->stream));
+  return PYRO_OK;
+}
+
+int pyro_sim_render_emission(PyroSim* S, const float* lut_dev, const float* chemi) {
+  clear_error();
+  PYRO_REQUIRE(S && lut_dev && chemi, "pyro_sim_render_emission: null argument");
+  PYRO_REQUIRE(S->rvol.p, "pyro_sim_render_emission: call pyro_sim_render_pack first");
+  const size_t n = S->d.cells();
+  int rc;
+  if (!S->ecell.p) {  // first call: emission, CDF and the scan's block sums
+    if ((rc = S->ecell.alloc(n * 4)) != PYRO_OK || (rc = S->ecdf.alloc((n + 1) * 4)) != PYRO_OK ||
+        (rc = S->cdf_scratch.alloc(render_cdf_scratch_bytes((long)n))) != PYRO_OK)
+      return rc;
+  }
+  PYRO_CU(launch_render_ecells(S->params.as<PyroParams>(), S->d, S->rvol.p, lut_dev, chemi,
+                               S->ecell.as<float>(), S->stream));
+  PYRO_CU(launch_render_cdf((long)n, S->ecell.as<float>(), S->ecdf.as<float>(), S->cdf_scratch.p,
+                            S->stream));
   return PYRO_OK;
 }
 

@@ -149,6 +149,10 @@ class Sim:
         nx, ny, nz = self.dims
         if which in (_abi.F_RVOL, _abi.F_RSOL, _abi.F_RVEL):
             out = np.empty((nz, ny, nx, 4), dtype=np.float16)
+        elif which == _abi.F_ECELL:
+            out = np.empty((nz, ny, nx), dtype=np.float32)
+        elif which == _abi.F_ECDF:
+            out = np.empty(nx * ny * nz + 1, dtype=np.float32)
         elif which == _abi.F_BRICKS:
             out = np.empty(((nz + 7) // 8, (ny + 7) // 8, (nx + 7) // 8), dtype=np.float32)
         elif which in (_abi.F_U, _abi.F_V, _abi.F_W):
@@ -185,6 +189,23 @@ class Sim:
         self.render_pack(bricks)
         return (self.read_field(_abi.F_RVOL), self.read_field(_abi.F_RSOL),
                 self.read_field(_abi.F_RVEL), self.read_field(_abi.F_BRICKS) if bricks else None)
+
+    def render_emission(self, chemi: Optional[np.ndarray] = None, lut=None) -> None:
+        """The renderer's fire-light sampling tables (render.rs:304-333) from
+        the last render_pack: emission power per cell and its CDF (read with
+        read_field(F_ECELL / F_ECDF)).  `lut`: a CUDA tensor of the colour
+        table (color.build_lut(), its first 1024 rows are used); by default
+        the table is built once and kept on the device.  `chemi`: the four
+        floats of color.chemi_block()."""
+        from . import color
+        if lut is None:
+            if getattr(self, "_lut_dev", None) is None:
+                import torch  # device memory for the table only
+                self._lut_dev = torch.from_numpy(color.build_lut()).cuda()
+            lut = self._lut_dev
+        ch = np.ascontiguousarray(color.chemi_block() if chemi is None else chemi, np.float32)
+        _abi.check("pyro_sim_render_emission", self._lib.pyro_sim_render_emission(
+            self._h, ctypes.c_void_p(lut.data_ptr()), ch.ctypes.data_as(ctypes.c_void_p)))
 
     def set_solver(self, mode: int, tol: float = 1e-3, max_iters: int = 50) -> None:
         _abi.check("pyro_sim_set_solver",

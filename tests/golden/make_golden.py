@@ -66,7 +66,8 @@ class Ref:
             self.kernels.update(split_kernels(rd(f)))
         # the renderer's input pack (src/render.rs:135,229-230: with common.wgsl)
         rk = split_kernels(rd("render.wgsl"))
-        self.kernels["pack"], self.kernels["bricks"] = rk["pack"], rk["bricks"]
+        for k in ("pack", "bricks", "ecells"):
+            self.kernels[k] = rk[k]
 
     def assemble(self, name):
         """src/gpu.rs:212-237."""
@@ -255,11 +256,20 @@ def gen_render(ref, only):
         nb = tuple((v + 7) // 8 for v in dims)
         bricks = np.zeros(nb[0] * nb[1] * nb[2], np.float32)
         t2 = run_kernel(ref, "bricks", P, {1: vol, 2: solt, 3: bricks}, groups3(nb))
+        # the fire-light emission per cell (render.wgsl:63-98) on the packed
+        # volume, with the colour table and uniform of src/render.rs:128-174
+        from pyro_b200 import color
+        lut = color.build_lut()
+        chemi = color.chemi_block()
+        ecell = np.zeros(nx * ny * nz, np.float32)
+        t3 = run_kernel(ref, "ecells", P, {1: vol, 2: lut.copy(), 3: ecell, 4: chemi.copy()},
+                        groups3(dims))
         out[f"render_c{case}"] = dict(params=pb, s0=S["s0"], s1=S["s1"], sol=S["sol"],
                                       flags=S["flags"], u=S["u"], v=S["v"], w=S["w"], vol=vol,
                                       solt=solt, vel=vel,
-                                      bricks=bricks.reshape(nb[2], nb[1], nb[0]))
-        print(f"render c{case} {t1:.1f}+{t2:.1f}s", flush=True)
+                                      bricks=bricks.reshape(nb[2], nb[1], nb[0]), lut=lut,
+                                      chemi=chemi, ecell=ecell.reshape(n))
+        print(f"render c{case} {t1:.1f}+{t2:.1f}+{t3:.1f}s", flush=True)
     return out
 
 

@@ -531,13 +531,24 @@ def _texture_store(tex, c, v):
         tex[z, y, x] = np.asarray(v, dtype=F32).astype(tex.dtype)
 
 
+def _dot(a, b):
+    """Sum of the products in component order, each step rounded to f32
+    (no fused multiply-add)."""
+    a = np.asarray(a, dtype=F32)
+    b = np.asarray(b, dtype=F32)
+    r = F32(a[0] * b[0])
+    for k in range(1, len(a)):
+        r = F32(r + F32(a[k] * b[k]))
+    return r
+
+
 def _texture_load(tex, c, level):
     """textureLoad of one texel of a 3D texture, as vec4<f32>."""
     return tex[int(c[2]), int(c[1]), int(c[0])].astype(F32)
 
 
 BUILTINS: Dict[str, Callable] = {
-    "textureStore": _texture_store, "textureLoad": _texture_load,
+    "textureStore": _texture_store, "textureLoad": _texture_load, "dot": _dot,
     "clamp": _clamp, "min": _minmax(np.minimum), "max": _minmax(np.maximum), "mix": _mix,
     "smoothstep": _smoothstep, "select": _select, "exp": np.exp, "sqrt": np.sqrt,
     "length": _length, "cross": _cross, "floor": np.floor, "abs": np.abs,

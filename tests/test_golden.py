@@ -186,3 +186,19 @@ def test_render_pack_and_bricks(case):
     b = oracle.render_bricks((P.nx, P.ny, P.nz), d["vol"], d["solt"])
     assert np.array_equal(b, d["bricks"])
     assert (d["flags"] == 1).any() and (d["flags"] != 1).any()
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_render_emission(case):
+    """The fire-light emission per cell (render.wgsl:63-98; it calls exp(),
+    so 1e-5 relative) and the CDF the reference forms on the CPU
+    (src/render.rs:316-333)."""
+    d = _load(f"render_{case}")
+    P = _params(d)
+    e = oracle.render_ecells(P, d["vol"], d["lut"], d["chemi"])
+    close(e, d["ecell"], name="ecell")
+    assert (d["ecell"] > 0).sum() > d["ecell"].size // 2
+    cdf = oracle.render_cdf(d["ecell"])
+    assert cdf.shape == (d["ecell"].size + 1,)
+    assert np.all(np.diff(cdf[:-1]) >= 0) and cdf[-2] == 1.0
+    assert abs(cdf[-1] - np.maximum(d["ecell"], 0).astype(np.float64).sum()) <= 1e-6 * cdf[-1]
