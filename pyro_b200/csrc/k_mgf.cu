@@ -161,6 +161,22 @@ __global__ void __launch_bounds__(256) k_mg_prolong_m(L df, const TS* __restrict
 #pragma unroll
       for (int sx = 0; sx < 2; sx++) {
         if ((sx ? m1 : m0) & META_SOLID) continue;
+        if (solid == 0u) {
+          // no solid coarse neighbour: the eight weights are multiples of
+          // 1/64 that sum to exactly 1, so acc / ws is acc itself
+          float acc = 0.0f;
+#pragma unroll
+          for (int k = 0; k < 8; k++) {
+            const int ox = k & 1, oy = (k >> 1) & 1, oz = (k >> 2) & 1;
+            const int q = (sx + ox) + 3 * (sy + oy) + 9 * (sz + oz);
+            const float w = (sx != ox ? 0.75f : 0.25f) * (sy != oy ? 0.75f : 0.25f) *
+                            (sz != oz ? 0.75f : 0.25f);
+            acc += w * cv[q];
+          }
+          if (sx) P.y = P.y + acc;
+          else P.x = P.x + acc;
+          continue;
+        }
         float acc = 0.0f, ws = 0.0f;
 #pragma unroll
         for (int k = 0; k < 8; k++) {
@@ -385,7 +401,8 @@ __global__ void __launch_bounds__(256) k_mg_restrict_m(L df, float h2, const TS*
     }
   }
   const int ci = dc.idx(X, Y, Z);
-  stv(bc + ci, (nfl > 0.0f) ? r / fmaxf(nfl, 1.0f) : 0.0f);
+  // eight fluid children: dividing by 8 is the exact product with 1/8
+  stv(bc + ci, nfl == 8.0f ? r * 0.125f : (nfl > 0.0f) ? r / fmaxf(nfl, 1.0f) : 0.0f);
   stv(pc + ci, 0.0f);
 }
 
