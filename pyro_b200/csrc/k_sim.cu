@@ -492,26 +492,37 @@ __global__ void __launch_bounds__(256) k_react(const PyroParams* __restrict__ Pp
           yf += P.ign_fuel * wgt * P.dt;
         }
       }
-      float rho = rhoOf(P, T);
-      float tauU = 0.049f * P.dx * P.dx / (nut + 1e-6f);
-      float tauG = sqrtf(2.0f * P.dx / P.g);
-      float tau = fmaxf(fminf(tauU, tauG), P.tau_min);
-      float gate = smoothstep(P.t_ign - 100.0f, P.t_ign + 100.0f, T);
-      float lim = fminf(yf, yo / P.s_o2);
-      float dY = lim * (1.0f - expf(-gate * P.dt / tau));
-      yf -= dY;
-      yo = fmaxf(yo - P.s_o2 * dY, 0.0f);
-      T += dY * P.dhc / cpOf(T + 0.5f * dY * P.dhc / cpOf(T));
-      float q = rho * dY * P.dhc / P.dt;
-      float rich = smoothstep(0.0f, 0.03f, yf);
-      ys += P.soot_form * dY * (0.25f + 0.75f * rich);
-      float oxg = smoothstep(P.soot_ox_t, P.soot_ox_t + 300.0f, T) * (yo / P.yo2);
-      ys *= expf(-P.soot_ox * oxg * P.dt);
+      // Exact shortcuts for cold cells and the interior, where a factor is
+      // exactly 0: with gate = 0, 1 - exp(-0) = 0 makes dY = +0 (lim >= 0), and
+      // every update below by dY, q and the soot formation adds or subtracts
+      // a zero (yf, yo, ys >= 0 here), leaving its value unchanged bit for bit.
+      float q = 0.0f;
+      const float gate = smoothstep(P.t_ign - 100.0f, P.t_ign + 100.0f, T);
+      if (gate != 0.0f) {
+        float rho = rhoOf(P, T);
+        float tauU = 0.049f * P.dx * P.dx / (nut + 1e-6f);
+        float tauG = sqrtf(2.0f * P.dx / P.g);
+        float tau = fmaxf(fminf(tauU, tauG), P.tau_min);
+        float lim = fminf(yf, yo / P.s_o2);
+        float dY = lim * (1.0f - expf(-gate * P.dt / tau));
+        yf -= dY;
+        yo = fmaxf(yo - P.s_o2 * dY, 0.0f);
+        T += dY * P.dhc / cpOf(T + 0.5f * dY * P.dhc / cpOf(T));
+        q = rho * dY * P.dhc / P.dt;
+        float rich = smoothstep(0.0f, 0.03f, yf);
+        ys += P.soot_form * dY * (0.25f + 0.75f * rich);
+      }
+      // below the oxidation onset the factor is exp(-0) = 1
+      const float oxs = smoothstep(P.soot_ox_t, P.soot_ox_t + 300.0f, T);
+      if (oxs != 0.0f) {
+        float oxg = oxs * (yo / P.yo2);
+        ys *= expf(-P.soot_ox * oxg * P.dt);
+      }
       float cold = 1.0f - smoothstep(450.0f, 650.0f, T);
       float cv = yf * fminf(P.smoke_conv * cold * P.dt, 1.0f);
       yf -= cv;
       ym += cv;
-      rho = rhoOf(P, T);
+      float rho = rhoOf(P, T);
       float kap = kapP(P, T, yo, ys);
       float tl = kap * P.rad_len;
       float esc = (tl > 1e-3f) ? (1.0f - expf(-tl)) / tl : 1.0f;
@@ -521,12 +532,14 @@ __global__ void __launch_bounds__(256) k_react(const PyroParams* __restrict__ Pp
       float prl = dTr * rho * cpOf(T) / P.dt;
       S += (q - prl) / (rho * cpOf(T) * T);
       float sp = fmaxf(spongeSide(P, g, c), spongeTop(P, g, c));
-      float dec = 1.0f - expf(-P.dt * 4.0f * sp);
-      T = wmix(T, P.t0, dec);
-      yf *= 1.0f - dec;
-      yo = wmix(yo, P.yo2, dec);
-      ys *= 1.0f - dec;
-      ym *= 1.0f - dec;
+      if (sp != 0.0f) {  // outside the sponge layers dec = 1 - exp(-0) = 0: no change
+        float dec = 1.0f - expf(-P.dt * 4.0f * sp);
+        T = wmix(T, P.t0, dec);
+        yf *= 1.0f - dec;
+        yo = wmix(yo, P.yo2, dec);
+        ys *= 1.0f - dec;
+        ym *= 1.0f - dec;
+      }
       T = wclamp(T, 250.0f, 2600.0f);
       s0out[i] = make_float4(T, yf, yo, ys);
       s1out[i] = make_float4(ym, q, S, 0.0f);
