@@ -492,13 +492,21 @@ __global__ void __launch_bounds__(256) k_react(const PyroParams* __restrict__ Pp
           yf += P.ign_fuel * wgt * P.dt;
         }
       }
-      // Exact shortcuts for cold cells and the interior, where a factor is
-      // exactly 0: with gate = 0, 1 - exp(-0) = 0 makes dY = +0 (lim >= 0), and
-      // every update below by dY, q and the soot formation adds or subtracts
-      // a zero (yf, yo, ys >= 0 here), leaving its value unchanged bit for bit.
-      float q = 0.0f;
+      // Exact shortcuts where a factor is exactly zero.  With gate = 0 the
+      // factor 1 - exp(-0) is +0, so dY = lim * 0 (a signed zero); T then
+      // changes by a zero (T > 0 stays), q = rho dY dhc / dt and the soot
+      // term soot_form dY (...) are zeros of dY's sign (every other factor
+      // is positive), so yf, yo, ys take exactly the values the full
+      // expressions give, signs of zero included.
+      float q;
       const float gate = smoothstep(P.t_ign - 100.0f, P.t_ign + 100.0f, T);
-      if (gate != 0.0f) {
+      if (gate == 0.0f) {
+        const float dY = fminf(yf, yo / P.s_o2) * 0.0f;
+        yf -= dY;
+        yo = fmaxf(yo - P.s_o2 * dY, 0.0f);
+        q = dY;
+        ys += dY;
+      } else {
         float rho = rhoOf(P, T);
         float tauU = 0.049f * P.dx * P.dx / (nut + 1e-6f);
         float tauG = sqrtf(2.0f * P.dx / P.g);
@@ -532,13 +540,17 @@ __global__ void __launch_bounds__(256) k_react(const PyroParams* __restrict__ Pp
       float prl = dTr * rho * cpOf(T) / P.dt;
       S += (q - prl) / (rho * cpOf(T) * T);
       float sp = fmaxf(spongeSide(P, g, c), spongeTop(P, g, c));
-      if (sp != 0.0f) {  // outside the sponge layers dec = 1 - exp(-0) = 0: no change
+      if (sp != 0.0f) {
         float dec = 1.0f - expf(-P.dt * 4.0f * sp);
         T = wmix(T, P.t0, dec);
         yf *= 1.0f - dec;
         yo = wmix(yo, P.yo2, dec);
         ys *= 1.0f - dec;
         ym *= 1.0f - dec;
+      } else {
+        // outside the sponge layers dec = 1 - exp(-0) = +0: T (> 0), yf, ys
+        // and ym keep their values; yo gains yo2 * 0 as the mix does
+        yo = wmix(yo, P.yo2, 0.0f);
       }
       T = wclamp(T, 250.0f, 2600.0f);
       s0out[i] = make_float4(T, yf, yo, ys);
@@ -644,15 +656,21 @@ __global__ void __launch_bounds__(256) k_forces(const PyroParams* __restrict__ P
     float fc = 0.0f, n = 0.0f;
     if (ia) { fc = fc + comp4(__ldg(conf + iaa), k); n += 1.0f; }
     if (ib) { fc = fc + comp4(cc, k); n += 1.0f; }
-    if (n > 0.0f) f += fc / n;
+    // n is 1 or 2: the quotient equals the product with 1 or 1/2 exactly
+    if (n > 0.0f) f += fc * (n == 2.0f ? 0.5f : 1.0f);
     float* vk = k == 0 ? u : (k == 1 ? v : w);
     float uu = vk[i];
     uu += f * P.dt;
     if (k != 1) {
-      float hot = smoothstep(350.0f, 900.0f, Tc);
-      float kr = P.wind_relax * (1.0f - 0.85f * hot) + 8.0f * ss;
+      // without wind the relaxation rate is 8 ss; where that is 0 too, the
+      // mix weight 1 - exp(-0) is +0 and the mix is uu * 1 + wv * 0
+      float kr = 8.0f * ss;
+      if (P.wind_relax != 0.0f) {
+        float hot = smoothstep(350.0f, 900.0f, Tc);
+        kr = P.wind_relax * (1.0f - 0.85f * hot) + 8.0f * ss;
+      }
       float wv = k == 0 ? P.wind_x : P.wind_z;
-      uu = wmix(uu, wv, 1.0f - expf(-kr * P.dt));
+      uu = kr != 0.0f ? wmix(uu, wv, 1.0f - expf(-kr * P.dt)) : uu + wv * 0.0f;
     } else {
       float st = spongeTop(P, g, cl);
       if (st > 0.0f) uu = wmix(uu, fmaxf(uu, 0.0f), 1.0f - expf(-8.0f * st * P.dt));
