@@ -200,14 +200,31 @@ __device__ __forceinline__ double block_exscan(double v, double* sh, double* tot
   return off + inc - v;
 }
 
+// A block's 8192 values staged in shared memory: global loads and stores
+// coalesced (element j of the block at k * CDF_T + t for thread t), each
+// thread then works on its own CDF_PER contiguous values.  One padding word
+// per 32 keeps both access patterns free of bank conflicts.
+__device__ __forceinline__ int cdf_pad(int j) { return j + (j >> 5); }
+constexpr int CDF_SMEM = CDF_SPAN + CDF_SPAN / 32;
+
+__device__ __forceinline__ void cdf_stage(const float* __restrict__ e, long n, float* se) {
+  const long base = (long)blockIdx.x * CDF_SPAN;
+#pragma unroll
+  for (int k = 0; k < CDF_PER; k++) {
+    const int j = k * CDF_T + threadIdx.x;
+    se[cdf_pad(j)] = base + j < n ? fmaxf(__ldg(e + base + j), 0.0f) : 0.0f;
+  }
+  __syncthreads();
+}
+
 __global__ void __launch_bounds__(CDF_T) k_cdf_sums(const float* __restrict__ e, long n,
                                                     double* __restrict__ bsum) {
   __shared__ double sh[CDF_T / 32];
-  const long base = (long)blockIdx.x * CDF_SPAN + (long)threadIdx.x * CDF_PER;
+  __shared__ float se[CDF_SMEM];
+  cdf_stage(e, n, se);
   double s = 0.0;
 #pragma unroll
-  for (int k = 0; k < CDF_PER; k++)
-    if (base + k < n) s += (double)fmaxf(__ldg(e + base + k), 0.0f);
+  for (int k = 0; k < CDF_PER; k++) s += (double)se[cdf_pad(threadIdx.x * CDF_PER + k)];
   double tot;
   block_exscan(s, sh, &tot);
   if (threadIdx.x == 0) bsum[blockIdx.x] = tot;
@@ -233,21 +250,30 @@ __global__ void __launch_bounds__(CDF_T) k_cdf_final(const float* __restrict__ e
                                                      const double* __restrict__ bsum, int nb,
                                                      float* __restrict__ cdf) {
   __shared__ double sh[CDF_T / 32];
-  const long base = (long)blockIdx.x * CDF_SPAN + (long)threadIdx.x * CDF_PER;
+  __shared__ float se[CDF_SMEM];
+  cdf_stage(e, n, se);
+  const int t0 = threadIdx.x * CDF_PER;
   float v[CDF_PER];
   double s = 0.0;
 #pragma unroll
   for (int k = 0; k < CDF_PER; k++) {
-    v[k] = base + k < n ? fmaxf(__ldg(e + base + k), 0.0f) : 0.0f;
+    v[k] = se[cdf_pad(t0 + k)];
     s += (double)v[k];
   }
   double tot;
   double acc = bsum[blockIdx.x] + block_exscan(s, sh, &tot);
   const double total = bsum[nb];
 #pragma unroll
-  for (int k = 0; k < CDF_PER; k++) {
+  for (int k = 0; k < CDF_PER; k++) {  // each thread rewrites only its own values
     acc += (double)v[k];
-    if (base + k < n) cdf[base + k] = total > 0.0 ? (float)(acc / total) : 0.0f;
+    se[cdf_pad(t0 + k)] = total > 0.0 ? (float)(acc / total) : 0.0f;
+  }
+  __syncthreads();
+  const long base = (long)blockIdx.x * CDF_SPAN;
+#pragma unroll
+  for (int k = 0; k < CDF_PER; k++) {
+    const int j = k * CDF_T + threadIdx.x;
+    if (base + j < n) cdf[base + j] = se[cdf_pad(j)];
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) cdf[n] = (float)total;
 }
