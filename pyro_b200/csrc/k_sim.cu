@@ -710,21 +710,36 @@ __global__ void __launch_bounds__(256) k_project(const PyroParams* __restrict__ 
   if (c.x > g.nx || c.y > g.ny || c.z > g.nz) return;
   const float dx = Pp->dx;
   int i = g.vidx(c);
+  // every load first: the cell's and its three lower neighbours' flag and
+  // phi, and the three faces
   bool ib = g.inb(c);
-  bool sc = ib && __ldg(flags + g.sidx(c)) == 1u;
-  float pc = ib ? __ldg(phi + g.sidx(c)) : 0.0f;
+  const int ic = ib ? g.sidx(c) : 0;
+  const uint32_t fc = ib ? __ldg(flags + ic) : 0u;
+  const float pc = ib ? __ldg(phi + ic) : 0.0f;
+  bool ia[3], valid[3];
+  uint32_t fa[3];
+  float pa[3], vv[3];
 #pragma unroll
   for (int k = 0; k < 3; k++) {
-    if (!g.compValid(k, c)) continue;
-    I3 a = c - unitI(k);
-    bool ia = g.inb(a);
-    bool sa = ia && __ldg(flags + g.sidx(a)) == 1u;
+    const I3 a = c - unitI(k);
+    ia[k] = g.inb(a);
+    const int ja = ia[k] ? g.sidx(a) : 0;
+    fa[k] = ia[k] ? __ldg(flags + ja) : 0u;
+    pa[k] = ia[k] ? __ldg(phi + ja) : 0.0f;
+    valid[k] = g.compValid(k, c);
+    const float* vk = k == 0 ? u : (k == 1 ? v : w);
+    vv[k] = valid[k] ? vk[i] : 0.0f;
+  }
+  const bool sc = ib && fc == 1u;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    if (!valid[k]) continue;
+    const bool sa = ia[k] && fa[k] == 1u;
     float* vk = k == 0 ? u : (k == 1 ? v : w);
     float uu = 0.0f;
     if (!((k == 1 && c.y == 0) || sc || sa)) {
-      float pa = ia ? __ldg(phi + g.sidx(a)) : 0.0f;
-      uu = vk[i];
-      uu -= (pc - pa) / dx;
+      uu = vv[k];
+      uu -= (pc - pa[k]) / dx;
     }
     vk[i] = uu;
   }
