@@ -140,9 +140,10 @@ __global__ void __launch_bounds__(256) k_mg_prolong_m(L df, const TS* __restrict
 #pragma unroll
   for (int q = 0; q < 27; q++) {
     const int j = cx[q % 3] + cy[(q / 3) % 3] + cz[q / 9];
+    const float raw = ldv(pc + j);  // loaded regardless, so it need not wait for the mask
     const bool s = (__ldg(mc + j) & META_SOLID) != 0;
     solid |= (uint32_t)s << q;
-    cv[q] = s ? 0.0f : ldv(pc + j);
+    cv[q] = s ? 0.0f : raw;
   }
   const int fx = 2 * X;
   const bool two = fx + 1 < df.nx;
@@ -363,20 +364,23 @@ __global__ void __launch_bounds__(256) k_mg_restrict_m(L df, float h2, const TS*
       const int fy = 2 * Y + s_y;
       if (fy >= df.ny) break;
       const int i = df.idx(fx, fy, fz);
-      const uint32_t m0 = __ldg(mf + i), m1 = two ? __ldg(mf + i + 1) : META_SOLID;
-      if (m0 & m1 & META_SOLID) continue;
+      // the row's loads are issued together, none waiting for the masks
       const float2 zero = make_float2(0.0f, 0.0f);
       const float2 P = ldp<V2>(pf + i, two), B = ldp<V2>(bf + i, two);
       const float2 Yp = fy + 1 < df.ny ? ldp<V2>(pf + i + sy, two) : zero;
       const float2 Ym = fy > 0 ? ldp<V2>(pf + i - sy, two) : zero;
       const float2 Zp = fz + 1 < df.nz ? ldp<V2>(pf + i + sz, two) : zero;
       const float2 Zm = fz > 0 ? ldp<V2>(pf + i - sz, two) : zero;
+      const float pl = fx > 0 ? ldv(pf + i - 1) : 0.0f;
+      const float pr = fx + 2 < df.nx ? ldv(pf + i + 2) : 0.0f;
+      const uint32_t m0 = __ldg(mf + i), m1 = two ? __ldg(mf + i + 1) : META_SOLID;
+      if (m0 & m1 & META_SOLID) continue;
       const int dyz = (fy == df.ny - 1) + (open ? (fz == 0) + (fz == df.nz - 1) : 0);
       if (!(m0 & META_SOLID)) {
         nfl += 1.0f;
         float sum = 0.0f;
         if (m0 & 1u) sum += P.y;
-        if (m0 & 2u) sum += ldv(pf + i - 1);
+        if (m0 & 2u) sum += pl;
         if (m0 & 4u) sum += Yp.x;
         if (m0 & 8u) sum += Ym.x;
         if (m0 & 16u) sum += Zp.x;
@@ -388,7 +392,7 @@ __global__ void __launch_bounds__(256) k_mg_restrict_m(L df, float h2, const TS*
       if (!(m1 & META_SOLID)) {
         nfl += 1.0f;
         float sum = 0.0f;
-        if (m1 & 1u) sum += ldv(pf + i + 2);
+        if (m1 & 1u) sum += pr;
         if (m1 & 2u) sum += P.x;
         if (m1 & 4u) sum += Yp.y;
         if (m1 & 8u) sum += Ym.y;
