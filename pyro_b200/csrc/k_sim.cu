@@ -691,13 +691,14 @@ __global__ void __launch_bounds__(256) k_divergence(const PyroParams* __restrict
   I3 c = thread_cell();
   if (!g.inb(c)) return;
   int i = g.sidx(c);
-  if (__ldg(flags + i) == 1u) { b[i] = 0.0f; return; }
   int j = g.vidx(c);
   const int sy = g.nx + 1, sz = (g.nx + 1) * (g.ny + 1);
-  float d = (__ldg(u + j + 1) - __ldg(u + j) + __ldg(v + j + sy) - __ldg(v + j) +
-             __ldg(w + j + sz) - __ldg(w + j)) /
-            Pp->dx;
-  b[i] = d - __ldg(s1 + i).z;
+  // every load first, then the flag decides
+  const float u0 = __ldg(u + j), u1 = __ldg(u + j + 1), v0 = __ldg(v + j), v1 = __ldg(v + j + sy);
+  const float w0 = __ldg(w + j), w1 = __ldg(w + j + sz), src = __ldg(s1 + i).z;
+  if (__ldg(flags + i) == 1u) { b[i] = 0.0f; return; }
+  float d = (u1 - u0 + v1 - v0 + w1 - w0) / Pp->dx;
+  b[i] = d - src;
 }
 
 // ----------------------------------------------------------------- project
