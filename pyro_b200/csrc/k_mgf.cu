@@ -253,7 +253,7 @@ __device__ __forceinline__ void st4(__nv_bfloat16* p, float4 v) {
 }
 
 template <typename TS>
-__global__ void __launch_bounds__(256) k_mg_pass4(L d, float h2, const TS* __restrict__ b,
+__global__ void __launch_bounds__(256, 6) k_mg_pass4(L d, float h2, const TS* __restrict__ b,
                                                   const uint8_t* __restrict__ meta,
                                                   TS* __restrict__ p, int color, float omega,
                                                   int bc_mode, FastDiv by_cpr, FastDiv by_ny) {
@@ -339,7 +339,7 @@ __global__ void __launch_bounds__(256) k_mg_pass4(L d, float h2, const TS* __res
 // +-z neighbour values are loaded as pairs and whose outer x neighbours as
 // scalars.
 template <typename TS, bool V2>
-__global__ void __launch_bounds__(256) k_mg_restrict_m(L df, float h2, const TS* __restrict__ pf,
+__global__ void __launch_bounds__(256, 6) k_mg_restrict_m(L df, float h2, const TS* __restrict__ pf,
                                                        const TS* __restrict__ bf,
                                                        const uint8_t* __restrict__ mf, L dc,
                                                        TS* __restrict__ bc, TS* __restrict__ pc,

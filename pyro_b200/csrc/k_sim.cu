@@ -336,7 +336,7 @@ __global__ void __launch_bounds__(256) k_adv_vel2(const PyroParams* __restrict__
   }
 }
 
-__global__ void __launch_bounds__(256) k_adv_s1(const PyroParams* __restrict__ Pp, Grid g,
+__global__ void __launch_bounds__(256, 6) k_adv_s1(const PyroParams* __restrict__ Pp, Grid g,
                                                 const float* __restrict__ u,
                                                 const float* __restrict__ v,
                                                 const float* __restrict__ w,
@@ -398,7 +398,7 @@ __global__ void __launch_bounds__(256, 4) k_adv_s2(const PyroParams* __restrict_
 }
 
 // ------------------------------------------------------------------- react
-__global__ void __launch_bounds__(256) k_react(const PyroParams* __restrict__ Pp, Grid g,
+__global__ void __launch_bounds__(256, 8) k_react(const PyroParams* __restrict__ Pp, Grid g,
                                                const float4* __restrict__ s0in,
                                                const float4* __restrict__ s1in,
                                                float4* __restrict__ s0out,
