@@ -447,6 +447,38 @@ __device__ __forceinline__ void block_add(float* sh, float v, float* dst) {
     if (t == 0 && s != 0.0f) atomicAdd(dst, s);
   }
 }
+// N statistics of one block in one pass: each value is reduced over the
+// warp (a sum, or for bit k of max_mask the maximum of non-negative values),
+// the warps' results meet in shared memory (sh: N * 32 floats, not otherwise
+// in use) behind a single barrier, and warp 0 reduces them and adds (or
+// atomicMax-es) them into stats[slot[k]].  Per value the order of the sums
+// is block_add's.  Every thread of the block must call it.
+template <int N>
+__device__ __forceinline__ void block_stats(float* sh, float (&v)[N], float* stats,
+                                            const int (&slot)[N], uint32_t max_mask) {
+  const int t = lin_tid();
+  const int nw = (blockDim.x * blockDim.y * blockDim.z) >> 5;
+#pragma unroll
+  for (int k = 0; k < N; k++)
+    v[k] = ((max_mask >> k) & 1u) ? warp_max(fmaxf(v[k], 0.0f)) : warp_sum(v[k]);
+  if ((t & 31) == 0) {
+#pragma unroll
+    for (int k = 0; k < N; k++) sh[k * 32 + (t >> 5)] = v[k];
+  }
+  __syncthreads();
+  if (t < 32) {
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+      const bool mx = ((max_mask >> k) & 1u) != 0;
+      float s = t < nw ? sh[k * 32 + t] : 0.0f;
+      s = mx ? warp_max(s) : warp_sum(s);
+      if (t == 0) {
+        if (mx) atomicMax(reinterpret_cast<unsigned int*>(stats + slot[k]), __float_as_uint(s));
+        else if (s != 0.0f) atomicAdd(stats + slot[k], s);
+      }
+    }
+  }
+}
 // max of non-negative values via integer atomicMax on the bits (stats.wgsl:14)
 __device__ __forceinline__ void block_max(float* sh, float v, float* dst) {
   int t = lin_tid();

@@ -175,22 +175,21 @@ __global__ void __launch_bounds__(256) k_mg_resid(Lvl d, float h2, const float* 
                                                   const float* __restrict__ b,
                                                   const uint32_t* __restrict__ f, int bc_mode,
                                                   float* __restrict__ stats) {
-  __shared__ float sh[32];
+  __shared__ float sh[2 * 32];
   int x = blockIdx.x * BX + threadIdx.x;
   int y = blockIdx.y * BY + threadIdx.y;
   int z = blockIdx.z * BZ + threadIdx.z;
-  float r2 = 0.0f, b2 = 0.0f;
+  float vals[2] = {0.0f, 0.0f};  // r^2, b^2
   if (d.inb(x, y, z)) {
     int i = d.idx(x, y, z);
     if (__ldg(f + i) != 1u) {
       float r = resid_cell(d, h2, p, b, f, x, y, z, bc_mode);
       float bi = __ldg(b + i);
-      r2 = r * r;
-      b2 = bi * bi;
+      vals[0] = r * r;
+      vals[1] = bi * bi;
     }
   }
-  block_add(sh, r2, stats + 10);
-  block_add(sh, b2, stats + 11);
+  block_stats<2>(sh, vals, stats, {10, 11}, 0u);
 }
 
 // ------------------------------------------------------------ coarse solve

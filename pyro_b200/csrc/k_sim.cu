@@ -124,7 +124,7 @@ __global__ void __launch_bounds__(256) k_solid(const PyroParams* __restrict__ Pp
                                                uint32_t* __restrict__ flags,
                                                const float4* __restrict__ s0,
                                                float* __restrict__ stats) {
-  __shared__ float sh[32];
+  __shared__ float sh[3 * 32];
   const PyroParams& P = *Pp;
   SolidCtx C{P, g, solIn, s0};
   I3 c = thread_cell();
@@ -214,9 +214,8 @@ __global__ void __launch_bounds__(256) k_solid(const PyroParams* __restrict__ Pp
     flags[i] = fl;
   }
   if (stats) {
-    block_add(sh, stPyro, stats + 2);
-    block_add(sh, stMass, stats + 7);
-    block_add(sh, stArea, stats + 9);
+    float vals[3] = {stPyro, stMass, stArea};
+    block_stats<3>(sh, vals, stats, {2, 7, 9}, 0u);
   }
 }
 
@@ -408,7 +407,7 @@ __global__ void __launch_bounds__(256, 8) k_react(const PyroParams* __restrict__
                                                const float4* __restrict__ pyr,
                                                const float4* __restrict__ curl,
                                                float* __restrict__ stats) {
-  __shared__ float sh[32];
+  __shared__ float sh[6 * 32];
   const PyroParams& P = *Pp;
   I3 c = thread_cell();
   float stH = 0, stR = 0, stS = 0, stF = 0, stM = 0, stT = 0;
@@ -572,12 +571,8 @@ __global__ void __launch_bounds__(256, 8) k_react(const PyroParams* __restrict__
     float lay = (active && stH > 1.0f) ? stH : 0.0f;
     lay = warp_sum(lay);
     if (threadIdx.x == 0 && lay != 0.0f && c.y < PYRO_MAX_LAYERS) atomicAdd(stats + 16 + c.y, lay);
-    block_add(sh, stH, stats + 0);
-    block_add(sh, stR, stats + 1);
-    block_add(sh, stS, stats + 3);
-    block_add(sh, stF, stats + 6);
-    block_add(sh, stM, stats + 8);
-    block_max(sh, stT, stats + 4);
+    float vals[6] = {stH, stR, stS, stF, stM, stT};
+    block_stats<6>(sh, vals, stats, {0, 1, 3, 6, 8, 4}, 1u << 5);
   }
 }
 
