@@ -46,6 +46,18 @@ __device__ __forceinline__ float wmix(float a, float b, float t) { return a * (1
 __device__ __forceinline__ float4 wmix4(float4 a, float4 b, float t) {
   return make_float4(wmix(a.x, b.x, t), wmix(a.y, b.y, t), wmix(a.z, b.z, t), wmix(a.w, b.w, t));
 }
+// Two mixes a*(1-t) + b*t at once (omt = 1 - t): the four products as two
+// paired FP32 multiplies of sm_100 (FMUL2), the two sums as scalar adds.
+// Each lane rounds as the scalar multiply does, so the pair equals two
+// wmix calls bit for bit.  The sums stay scalar on purpose: a paired
+// multiply feeding a paired add is contracted into a paired fused
+// multiply-add even under --fmad=false (measured on B200), which would
+// change the rounding.
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 mix2(float2 a, float2 b, float2 omt, float2 t) {
+  const float2 p = __fmul2_rn(a, omt), q = __fmul2_rn(b, t);
+  return f2(p.x + q.x, p.y + q.y);
+}
 __device__ __forceinline__ float4 min4(float4 a, float4 b) {
   return make_float4(fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z), fminf(a.w, b.w));
 }
@@ -236,6 +248,29 @@ __device__ __forceinline__ float triC_mm(const float* __restrict__ X, const Grid
   float c11 = wmix(v6, v7, fx);
   return wmix(wmix(c00, c10, fy), wmix(c01, c11, fy), fz);
 }
+// triC_mm with the x and y stages as paired multiplies (same values).
+__device__ __forceinline__ float triC_mm_p(const float* __restrict__ X, const Grid& gr, F3 g0,
+                                          I3 hi, float& lo, float& hv) {
+  float gx = wclamp(g0.x, 0.0f, (float)hi.x);
+  float gy = wclamp(g0.y, 0.0f, (float)hi.y);
+  float gz = wclamp(g0.z, 0.0f, (float)hi.z);
+  int bx = min((int)floorf(gx), hi.x - 1);
+  int by = min((int)floorf(gy), hi.y - 1);
+  int bz = min((int)floorf(gz), hi.z - 1);
+  float fx = gx - (float)bx, fy = gy - (float)by, fz = gz - (float)bz;
+  const int sy = gr.nx + 1, sz = (gr.nx + 1) * (gr.ny + 1);
+  int i = bx + sy * by + sz * bz;
+  float v0 = __ldg(X + i), v1 = __ldg(X + i + 1), v2 = __ldg(X + i + sy),
+        v3 = __ldg(X + i + sy + 1), v4 = __ldg(X + i + sz), v5 = __ldg(X + i + sz + 1),
+        v6 = __ldg(X + i + sy + sz), v7 = __ldg(X + i + sy + sz + 1);
+  lo = fminf(fminf(fminf(fminf(fminf(fminf(fminf(1e30f, v0), v1), v2), v3), v4), v5), fminf(v6, v7));
+  hv = fmaxf(fmaxf(fmaxf(fmaxf(fmaxf(fmaxf(fmaxf(-1e30f, v0), v1), v2), v3), v4), v5), fmaxf(v6, v7));
+  const float ox = 1.0f - fx, oy = 1.0f - fy;
+  const float2 c0010 = mix2(f2(v0, v2), f2(v1, v3), f2(ox, ox), f2(fx, fx));
+  const float2 c0111 = mix2(f2(v4, v6), f2(v5, v7), f2(ox, ox), f2(fx, fx));
+  const float2 c01 = mix2(f2(c0010.x, c0111.x), f2(c0010.y, c0111.y), f2(oy, oy), f2(fy, fy));
+  return wmix(c01.x, c01.y, fz);
+}
 // Cell-centred vec4 trilinear sample (tmpl_scalar.wgsl:2-15).
 __device__ __forceinline__ float4 triS(const float4* __restrict__ X, const Grid& gr, F3 gc0) {
   float gx = wclamp(gc0.x, 0.0f, (float)(gr.nx - 1));
@@ -301,6 +336,43 @@ __device__ __forceinline__ float tri_axes(const float* __restrict__ X, const Gri
   return c0 * az.omf + c1 * az.f;
 }
 
+// tri_axes with the x and y stages as paired multiplies (same value bit for bit).
+__device__ __forceinline__ float tri_axes_p(const float* __restrict__ X, const Grid& gr, Axis ax,
+                                            Axis ay, Axis az) {
+  const int sy = gr.nx + 1, sz = (gr.nx + 1) * (gr.ny + 1);
+  int i = ax.b + sy * ay.b + sz * az.b;
+  const float2 OX = f2(ax.omf, ax.omf), FX = f2(ax.f, ax.f);
+  const float2 c0010 = mix2(f2(__ldg(X + i), __ldg(X + i + sy)),
+                            f2(__ldg(X + i + 1), __ldg(X + i + sy + 1)), OX, FX);
+  const float2 c0111 = mix2(f2(__ldg(X + i + sz), __ldg(X + i + sy + sz)),
+                            f2(__ldg(X + i + sz + 1), __ldg(X + i + sy + sz + 1)), OX, FX);
+  const float2 c01 = mix2(f2(c0010.x, c0111.x), f2(c0010.y, c0111.y), f2(ay.omf, ay.omf),
+                          f2(ay.f, ay.f));
+  return c01.x * az.omf + c01.y * az.f;
+}
+// Two tri_axes samples (components X and Y, each with its own axes), every
+// stage paired across the two.
+__device__ __forceinline__ float2 tri_axes_p2(const float* __restrict__ X,
+                                              const float* __restrict__ Y, const Grid& gr,
+                                              Axis axX, Axis ayX, Axis azX, Axis axY, Axis ayY,
+                                              Axis azY) {
+  const int sy = gr.nx + 1, sz = (gr.nx + 1) * (gr.ny + 1);
+  const int i = axX.b + sy * ayX.b + sz * azX.b, j = axY.b + sy * ayY.b + sz * azY.b;
+  const float2 OX = f2(axX.omf, axY.omf), FX = f2(axX.f, axY.f);
+  const float2 c00 = mix2(f2(__ldg(X + i), __ldg(Y + j)), f2(__ldg(X + i + 1), __ldg(Y + j + 1)),
+                          OX, FX);
+  const float2 c10 = mix2(f2(__ldg(X + i + sy), __ldg(Y + j + sy)),
+                          f2(__ldg(X + i + sy + 1), __ldg(Y + j + sy + 1)), OX, FX);
+  const float2 c01 = mix2(f2(__ldg(X + i + sz), __ldg(Y + j + sz)),
+                          f2(__ldg(X + i + sz + 1), __ldg(Y + j + sz + 1)), OX, FX);
+  const float2 c11 = mix2(f2(__ldg(X + i + sy + sz), __ldg(Y + j + sy + sz)),
+                          f2(__ldg(X + i + sy + sz + 1), __ldg(Y + j + sy + sz + 1)), OX, FX);
+  const float2 OY = f2(ayX.omf, ayY.omf), FY = f2(ayX.f, ayY.f);
+  const float2 c0 = mix2(c00, c10, OY, FY);
+  const float2 c1 = mix2(c01, c11, OY, FY);
+  return mix2(c0, c1, f2(azX.omf, azY.omf), f2(azX.f, azY.f));
+}
+
 // Staggered velocity and RK2 traces in grid units (vel.wgsl:2-19).
 struct Vel {
   const float* __restrict__ u;
@@ -310,10 +382,17 @@ struct Vel {
   // p - (.5,0,.5) to (nx-1, ny, nz-1), w at p - (.5,.5,0) to
   // (nx-1, ny-1, nz).  Per axis only two offset/bound pairs occur, so six
   // axis set-ups serve the three samples.
+  // PAIRED: the same values with paired FP32 multiplies (mix2); it pays only
+  // where the FP32 pipe is the limit (the velocity predictor).
+  template <bool PAIRED = false>
   __device__ __forceinline__ F3 at(const Grid& g, F3 p) const {
     Axis xu = axis(p.x - 0.0f, g.nx), xvw = axis(p.x - 0.5f, g.nx - 1);
     Axis yv = axis(p.y - 0.0f, g.ny), yuw = axis(p.y - 0.5f, g.ny - 1);
     Axis zw = axis(p.z - 0.0f, g.nz), zuv = axis(p.z - 0.5f, g.nz - 1);
+    if constexpr (PAIRED) {
+      const float2 uv = tri_axes_p2(u, v, g, xu, yuw, zuv, xvw, yv, zuv);
+      return F3{uv.x, uv.y, tri_axes_p(w, g, xvw, yuw, zw)};
+    }
     return F3{tri_axes(u, g, xu, yuw, zuv), tri_axes(v, g, xvw, yv, zuv),
               tri_axes(w, g, xvw, yuw, zw)};
   }
@@ -357,9 +436,10 @@ struct Vel {
   __device__ __forceinline__ F3 first(const Grid& g, int k, I3 c) const {
     return k == 3 ? at_center(g, c) : at_face(g, k, c);
   }
+  template <bool PAIRED = false>
   __device__ __forceinline__ F3 back_at(const Grid& g, float kk, int k, I3 c, F3 x) const {
     F3 u1 = first(g, k, c);
-    F3 u2 = at(g, x - (0.5f * kk) * u1);
+    F3 u2 = at<PAIRED>(g, x - (0.5f * kk) * u1);
     return x - kk * u2;
   }
   __device__ __forceinline__ F3 fwd_at(const Grid& g, float kk, int k, I3 c, F3 x) const {

@@ -283,7 +283,7 @@ __global__ void __launch_bounds__(256) k_adv_vel1(const PyroParams* __restrict__
     if (!g.compValid(k, c)) continue;
     F3 off = compOff(k);
     float lo, hi;
-    float r = triC_mm(pick3(k, u, v, w), g, V.back_at(g, kk, k, c, tof3(c) + off) - off,
+    float r = triC_mm_p(pick3(k, u, v, w), g, V.back_at<true>(g, kk, k, c, tof3(c) + off) - off,
                       g.compHi(k), lo, hi);
     if (k == 0) hu[i] = r; else if (k == 1) hv[i] = r; else hw[i] = r;
     lohi[k * nv + i] = lo;
