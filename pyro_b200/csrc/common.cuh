@@ -224,6 +224,26 @@ __device__ __forceinline__ void mmC(const float* __restrict__ X, const Grid& gr,
   lo = fminf(fminf(fminf(fminf(fminf(fminf(fminf(1e30f, v0), v1), v2), v3), v4), v5), fminf(v6, v7));
   hv = fmaxf(fmaxf(fmaxf(fmaxf(fmaxf(fmaxf(fmaxf(-1e30f, v0), v1), v2), v3), v4), v5), fmaxf(v6, v7));
 }
+// triC with the x and y stages as paired multiplies (same value).
+__device__ __forceinline__ float triC_p(const float* __restrict__ X, const Grid& gr, F3 g0, I3 hi) {
+  float gx = wclamp(g0.x, 0.0f, (float)hi.x);
+  float gy = wclamp(g0.y, 0.0f, (float)hi.y);
+  float gz = wclamp(g0.z, 0.0f, (float)hi.z);
+  int bx = min((int)floorf(gx), hi.x - 1);
+  int by = min((int)floorf(gy), hi.y - 1);
+  int bz = min((int)floorf(gz), hi.z - 1);
+  float fx = gx - (float)bx, fy = gy - (float)by, fz = gz - (float)bz;
+  const int sy = gr.nx + 1, sz = (gr.nx + 1) * (gr.ny + 1);
+  int i = bx + sy * by + sz * bz;
+  const float ox = 1.0f - fx, oy = 1.0f - fy;
+  const float2 c0010 = mix2(f2(__ldg(X + i), __ldg(X + i + sy)),
+                            f2(__ldg(X + i + 1), __ldg(X + i + sy + 1)), f2(ox, ox), f2(fx, fx));
+  const float2 c0111 = mix2(f2(__ldg(X + i + sz), __ldg(X + i + sy + sz)),
+                            f2(__ldg(X + i + sz + 1), __ldg(X + i + sy + sz + 1)), f2(ox, ox),
+                            f2(fx, fx));
+  const float2 c01 = mix2(f2(c0010.x, c0111.x), f2(c0010.y, c0111.y), f2(oy, oy), f2(fy, fy));
+  return wmix(c01.x, c01.y, fz);
+}
 // triC and mmC at the same point from one set of 8 corner loads: the
 // trilinear value, and the corners' min / max with mmC's expression order.
 __device__ __forceinline__ float triC_mm(const float* __restrict__ X, const Grid& gr, F3 g0,
@@ -382,8 +402,9 @@ struct Vel {
   // p - (.5,0,.5) to (nx-1, ny, nz-1), w at p - (.5,.5,0) to
   // (nx-1, ny-1, nz).  Per axis only two offset/bound pairs occur, so six
   // axis set-ups serve the three samples.
-  // PAIRED: the same values with paired FP32 multiplies (mix2); it pays only
-  // where the FP32 pipe is the limit (the velocity predictor).
+  // PAIRED: the same values with paired FP32 multiplies (mix2), u paired
+  // with v; it pays only where the FP32 pipe is the limit (the velocity
+  // predictor; measured slower in the other advection kernels).
   template <bool PAIRED = false>
   __device__ __forceinline__ F3 at(const Grid& g, F3 p) const {
     Axis xu = axis(p.x - 0.0f, g.nx), xvw = axis(p.x - 0.5f, g.nx - 1);

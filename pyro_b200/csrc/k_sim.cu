@@ -329,7 +329,7 @@ __global__ void __launch_bounds__(256) k_adv_vel2(const PyroParams* __restrict__
       const float* vk = pick3(k, u, v, w);
       const float* hk = pick3(k, hu, hv, hw);
       const float lo = __ldg(lohi + k * nv + i), hv2 = __ldg(lohi + (3 + k) * nv + i);
-      r = wclamp(__ldg(hk + i) + 0.5f * (__ldg(vk + i) - triC(hk, g, f, hi)), lo, hv2);
+      r = wclamp(__ldg(hk + i) + 0.5f * (__ldg(vk + i) - triC_p(hk, g, f, hi)), lo, hv2);
     }
     if (k == 0) ou[i] = r; else if (k == 1) ov[i] = r; else ow[i] = r;
   }
