@@ -1,5 +1,7 @@
-// k_render.cu — the renderer's per-frame input pack (src/shaders/render.wgsl:3-61,
-// dispatched by src/render.rs:270-292).
+// k_render.cu — the renderer's per-frame prologue: its input pack
+// (src/shaders/render.wgsl:3-61) and its fire-light sampling tables
+// (render.wgsl:63-98 and the CDF of src/render.rs:316-333), dispatched by
+// src/render.rs:263-333.
 //
 // The reference packs the step's fields into three rgba16float 3D textures
 // that the volume path tracer samples with hardware trilinear filtering,
@@ -15,6 +17,11 @@
 //  * k_render_bricks: one CTA per brick, the maximum over the brick and a
 //    one-cell shell (the reach of trilinear filtering) read back from the
 //    half volumes, as the reference reads its textures.
+//  * k_render_ecells: one thread per cell, the emission power with the
+//    six-axis escape weighting, rays loaded eight samples ahead.
+//  * k_cdf_sums / k_cdf_blocks / k_cdf_final: the emission CDF as a
+//    deterministic FP64 scan on the device, where the reference reads the
+//    emission back and sums it on the CPU.
 //
 // Per-cell arithmetic is the reference's in its order (--fmad=false keeps
 // each product rounded), so the half values equal the oracle's bit for bit.
