@@ -36,6 +36,8 @@ cells*substeps/s over ranks.
 from __future__ import annotations
 
 import argparse
+import ctypes
+import datetime
 import faulthandler
 import json
 import math
@@ -394,7 +396,7 @@ def run_ours(args):
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     else:
         torch.cuda.set_device(0)
     dev = torch.cuda.current_device()
@@ -462,7 +464,7 @@ def run_ours(args):
     buf = (np.zeros(12, np.float32))
     for k in range(nprof):
         rc = lib.pyro_sim_profile_step(sim._h, float(dt), float(sim.time), 0.0, 1 if k == 0 else 0,
-                                       buf.ctypes.data_as(__import__("ctypes").c_void_p), 12)
+                                       buf.ctypes.data_as(ctypes.c_void_p), 12)
         _abi.check("pyro_sim_profile_step", rc)
         sim.time = np.float32(sim.time + dt)
         phases += buf
@@ -508,15 +510,14 @@ def run_ours(args):
     from pyro_b200 import color
     lut_dev = torch.from_numpy(color.build_lut()).cuda()
     chemi = color.chemi_block()
-    chp = chemi.ctypes.data_as(__import__("ctypes").c_void_p)
+    chp = chemi.ctypes.data_as(ctypes.c_void_p)
     _abi.check("pyro_sim_render_emission",
-               lib.pyro_sim_render_emission(sim._h, __import__("ctypes").c_void_p(
-                   lut_dev.data_ptr()), chp))  # first call allocates
+               lib.pyro_sim_render_emission(sim._h, ctypes.c_void_p(lut_dev.data_ptr()), chp))  # first call allocates
     sim.sync()
     ev[0].record(stream)
     for _ in range(reps):
         _abi.check("pyro_sim_render_emission", lib.pyro_sim_render_emission(
-            sim._h, __import__("ctypes").c_void_p(lut_dev.data_ptr()), chp))
+            sim._h, ctypes.c_void_p(lut_dev.data_ptr()), chp))
     ev[1].record(stream)
     ev[1].synchronize()
     frame_pack["emission_ms"] = ev[0].elapsed_time(ev[1]) / reps
