@@ -563,7 +563,14 @@ def run_ours(args):
     if rank == 0 and not args.no_solver:
         log("solver bench")
         solver = {"sim_pressure": sim_solver_bench(sim), "poisson_256": solver_bench()}
-    launches_per_step = 10 + sc.sim.pressure_cycles * (10 * (info.levels - 1) + 1)
+    # kernels per substep: 11 step kernels (solid, curl, adv_vel1/2, adv_s1/2,
+    # react, confine, forces, divergence, project), the level preparation
+    # (flags_down per coarse level, a mask per level) and per V-cycle 4 + 1 + 5
+    # per non-coarsest level plus the coarsest solve; mg_resid on the
+    # statistics substeps (checked against the ncu launch list)
+    L = info.levels
+    launches_per_step = 11 + (L - 1) + L + sc.sim.pressure_cycles * (10 * (L - 1) + 1)
+    stats_steps = sum(1 for k in range(args.steps) if (k % n) == n - 1)
     line = {
         "metric": METRIC, "value": ms, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
@@ -587,7 +594,7 @@ def run_ours(args):
         "throughput": {"value": world * cells / (ms * 1e-3), "unit": "cells*substeps/s"},
         "cpu_baseline": cpu,
         "solver": solver,
-        "gpu_launches": launches_per_step * args.steps,
+        "gpu_launches": launches_per_step * args.steps + stats_steps,
         "clocks": clocks.summary(),
     }
     if rank == 0:
