@@ -190,41 +190,10 @@ __device__ __forceinline__ float spongeTop(const PyroParams& P, const Grid& g, I
 }
 
 // --------------------------------------------------------------- samplers
-// Trilinear sample of staggered component X at grid point g0 (tmpl_comp.wgsl:2-15).
-__device__ __forceinline__ float triC(const float* __restrict__ X, const Grid& gr, F3 g0, I3 hi) {
-  float gx = wclamp(g0.x, 0.0f, (float)hi.x);
-  float gy = wclamp(g0.y, 0.0f, (float)hi.y);
-  float gz = wclamp(g0.z, 0.0f, (float)hi.z);
-  int bx = min((int)floorf(gx), hi.x - 1);
-  int by = min((int)floorf(gy), hi.y - 1);
-  int bz = min((int)floorf(gz), hi.z - 1);
-  float fx = gx - (float)bx, fy = gy - (float)by, fz = gz - (float)bz;
-  const int sy = gr.nx + 1, sz = (gr.nx + 1) * (gr.ny + 1);
-  int i = bx + sy * by + sz * bz;
-  float c00 = wmix(__ldg(X + i), __ldg(X + i + 1), fx);
-  float c10 = wmix(__ldg(X + i + sy), __ldg(X + i + sy + 1), fx);
-  float c01 = wmix(__ldg(X + i + sz), __ldg(X + i + sz + 1), fx);
-  float c11 = wmix(__ldg(X + i + sy + sz), __ldg(X + i + sy + sz + 1), fx);
-  return wmix(wmix(c00, c10, fy), wmix(c01, c11, fy), fz);
-}
-// 8-corner min/max (tmpl_comp.wgsl:16-25).
-__device__ __forceinline__ void mmC(const float* __restrict__ X, const Grid& gr, F3 g0, I3 hi,
-                                    float& lo, float& hv) {
-  float gx = wclamp(g0.x, 0.0f, (float)hi.x);
-  float gy = wclamp(g0.y, 0.0f, (float)hi.y);
-  float gz = wclamp(g0.z, 0.0f, (float)hi.z);
-  int bx = min((int)floorf(gx), hi.x - 1);
-  int by = min((int)floorf(gy), hi.y - 1);
-  int bz = min((int)floorf(gz), hi.z - 1);
-  const int sy = gr.nx + 1, sz = (gr.nx + 1) * (gr.ny + 1);
-  int i = bx + sy * by + sz * bz;
-  float v0 = __ldg(X + i), v1 = __ldg(X + i + 1), v2 = __ldg(X + i + sy),
-        v3 = __ldg(X + i + sy + 1), v4 = __ldg(X + i + sz), v5 = __ldg(X + i + sz + 1),
-        v6 = __ldg(X + i + sy + sz), v7 = __ldg(X + i + sy + sz + 1);
-  lo = fminf(fminf(fminf(fminf(fminf(fminf(fminf(1e30f, v0), v1), v2), v3), v4), v5), fminf(v6, v7));
-  hv = fmaxf(fmaxf(fmaxf(fmaxf(fmaxf(fmaxf(fmaxf(-1e30f, v0), v1), v2), v3), v4), v5), fmaxf(v6, v7));
-}
-// triC with the x and y stages as paired multiplies (same value).
+// Trilinear sample of staggered component X at grid point g0
+// (tmpl_comp.wgsl:2-15): clamp to [0, hi], base cell min(floor, hi - 1),
+// mix along x, then y, then z, with the x and y stages as paired multiplies
+// (mix2: the same value as the scalar mixes bit for bit).
 __device__ __forceinline__ float triC_p(const float* __restrict__ X, const Grid& gr, F3 g0, I3 hi) {
   float gx = wclamp(g0.x, 0.0f, (float)hi.x);
   float gy = wclamp(g0.y, 0.0f, (float)hi.y);
@@ -244,31 +213,8 @@ __device__ __forceinline__ float triC_p(const float* __restrict__ X, const Grid&
   const float2 c01 = mix2(f2(c0010.x, c0111.x), f2(c0010.y, c0111.y), f2(oy, oy), f2(fy, fy));
   return wmix(c01.x, c01.y, fz);
 }
-// triC and mmC at the same point from one set of 8 corner loads: the
-// trilinear value, and the corners' min / max with mmC's expression order.
-__device__ __forceinline__ float triC_mm(const float* __restrict__ X, const Grid& gr, F3 g0,
-                                        I3 hi, float& lo, float& hv) {
-  float gx = wclamp(g0.x, 0.0f, (float)hi.x);
-  float gy = wclamp(g0.y, 0.0f, (float)hi.y);
-  float gz = wclamp(g0.z, 0.0f, (float)hi.z);
-  int bx = min((int)floorf(gx), hi.x - 1);
-  int by = min((int)floorf(gy), hi.y - 1);
-  int bz = min((int)floorf(gz), hi.z - 1);
-  float fx = gx - (float)bx, fy = gy - (float)by, fz = gz - (float)bz;
-  const int sy = gr.nx + 1, sz = (gr.nx + 1) * (gr.ny + 1);
-  int i = bx + sy * by + sz * bz;
-  float v0 = __ldg(X + i), v1 = __ldg(X + i + 1), v2 = __ldg(X + i + sy),
-        v3 = __ldg(X + i + sy + 1), v4 = __ldg(X + i + sz), v5 = __ldg(X + i + sz + 1),
-        v6 = __ldg(X + i + sy + sz), v7 = __ldg(X + i + sy + sz + 1);
-  lo = fminf(fminf(fminf(fminf(fminf(fminf(fminf(1e30f, v0), v1), v2), v3), v4), v5), fminf(v6, v7));
-  hv = fmaxf(fmaxf(fmaxf(fmaxf(fmaxf(fmaxf(fmaxf(-1e30f, v0), v1), v2), v3), v4), v5), fmaxf(v6, v7));
-  float c00 = wmix(v0, v1, fx);
-  float c10 = wmix(v2, v3, fx);
-  float c01 = wmix(v4, v5, fx);
-  float c11 = wmix(v6, v7, fx);
-  return wmix(wmix(c00, c10, fy), wmix(c01, c11, fy), fz);
-}
-// triC_mm with the x and y stages as paired multiplies (same values).
+// triC_p at g0 and the 8 corners' min / max (tmpl_comp.wgsl:16-25, in its
+// expression order) from one set of corner loads.
 __device__ __forceinline__ float triC_mm_p(const float* __restrict__ X, const Grid& gr, F3 g0,
                                           I3 hi, float& lo, float& hv) {
   float gx = wclamp(g0.x, 0.0f, (float)hi.x);
@@ -519,9 +465,10 @@ struct Vel {
 };
 
 // -------------------------------------------------------------- statistics
-// Block-wide sum / max then one global atomic per block (replaces the
-// 64-lane tree + CAS add of stats.wgsl:1-36).  Every thread of the block must
-// call it.  `sh` needs 32 floats of shared memory.
+// Block-wide reductions then one global atomic per value and block (they
+// replace the 64-lane tree + CAS add of stats.wgsl:1-36): block_max for one
+// maximum (`sh`: 32 floats), block_stats for several sums and maxima at
+// once.  Every thread of the block must call them.
 __device__ __forceinline__ float warp_sum(float v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -535,25 +482,13 @@ __device__ __forceinline__ float warp_max(float v) {
 __device__ __forceinline__ int lin_tid() {
   return threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
 }
-__device__ __forceinline__ void block_add(float* sh, float v, float* dst) {
-  int t = lin_tid();
-  int nthreads = blockDim.x * blockDim.y * blockDim.z;
-  v = warp_sum(v);
-  __syncthreads();
-  if ((t & 31) == 0) sh[t >> 5] = v;
-  __syncthreads();
-  if (t < 32) {
-    float s = t < (nthreads >> 5) ? sh[t] : 0.0f;
-    s = warp_sum(s);
-    if (t == 0 && s != 0.0f) atomicAdd(dst, s);
-  }
-}
 // N statistics of one block in one pass: each value is reduced over the
 // warp (a sum, or for bit k of max_mask the maximum of non-negative values),
 // the warps' results meet in shared memory (sh: N * 32 floats, not otherwise
 // in use) behind a single barrier, and warp 0 reduces them and adds (or
-// atomicMax-es) them into stats[slot[k]].  Per value the order of the sums
-// is block_add's.  Every thread of the block must call it.
+// atomicMax-es) them into stats[slot[k]] (the reference's float atomics,
+// stats.wgsl:1-36, as one atomic per block).  Every thread of the block must
+// call it.
 template <int N>
 __device__ __forceinline__ void block_stats(float* sh, float (&v)[N], float* stats,
                                             const int (&slot)[N], uint32_t max_mask) {
