@@ -44,6 +44,10 @@ _SIGS = {
     "or_render_bricks": (None, [_I, _I, _I, _P, _P, _P]),
     "or_render_ecells": (None, [_P] * 5),
     "or_render_cdf": (None, [ctypes.c_size_t, _P, _P]),
+    "or_render_lightvol": (None, [_P] * 7 + [_I, _I, _I, _I, _P, _P]),
+    "or_render_lightground": (None, [_P] * 7 + [_I, _I, _P]),
+    "or_render_blur": (None, [_P, _P, _I, _I, _I, _I, _I]),
+    "or_render_trace": (None, [_P] * 7 + [_P, _P, _I, _I, _I, _P, _I, _P]),
     "or_f32_to_f16": (None, [_P, _P, ctypes.c_size_t]),
     "or_f16_to_f32": (None, [_P, _P, ctypes.c_size_t]),
     "or_mg_smooth": (None, [_I, _I, _I, _F, _P, _P, _P, _I, _F, _I]),
@@ -204,6 +208,59 @@ def render_cdf(e):
     cdf = np.zeros(e.size + 1, np.float32)
     lib().or_render_cdf(ctypes.c_size_t(e.size), ptr(e), ptr(cdf))
     return cdf
+
+
+def _h(a):
+    return np.ascontiguousarray(a, np.float16)
+
+
+def render_lightvol(rp, vol, solt, vel, bricks, lut, ecdf, lv_dims, lv_n=96):
+    """render.wgsl:217-251: (lvA, lvB) float16 (lz, ly, lx, 4)."""
+    lx, ly, lz = lv_dims
+    a = np.zeros((lz, ly, lx, 4), np.float16)
+    b = np.zeros_like(a)
+    lib().or_render_lightvol(ptr(np.ascontiguousarray(rp, np.float64)), ptr(_h(vol)), ptr(_h(solt)),
+                             ptr(_h(vel)), ptr(np.ascontiguousarray(bricks, np.float32)),
+                             ptr(np.ascontiguousarray(lut, np.float32)),
+                             ptr(np.ascontiguousarray(ecdf, np.float32)), lx, ly, lz, lv_n,
+                             ptr(a), ptr(b))
+    return a, b
+
+
+def render_lightground(rp, vol, solt, vel, bricks, lut, ecdf, gres, gr_n=128):
+    """render.wgsl:253-269: gE float16 (1, gres, gres, 4)."""
+    g = np.zeros((1, gres, gres, 4), np.float16)
+    lib().or_render_lightground(ptr(np.ascontiguousarray(rp, np.float64)), ptr(_h(vol)),
+                                ptr(_h(solt)), ptr(_h(vel)),
+                                ptr(np.ascontiguousarray(bricks, np.float32)),
+                                ptr(np.ascontiguousarray(lut, np.float32)),
+                                ptr(np.ascontiguousarray(ecdf, np.float32)), gres, gr_n, ptr(g))
+    return g
+
+
+def render_blur(src, axis, r):
+    """render.wgsl:271-304: one axis of the separable Gaussian."""
+    src = _h(src)
+    dst = np.zeros_like(src)
+    nz, ny, nx = src.shape[:3]
+    lib().or_render_blur(ptr(src), ptr(dst), nx, ny, nz, axis, r)
+    return dst
+
+
+def render_trace(rp, vol, solt, vel, bricks, lut, ecdf, lvA, lvB, gE, accum=None):
+    """render.wgsl:132-215: accum (res.y * res.x, 4) float32 += the samples."""
+    rp = np.ascontiguousarray(rp, np.float64)
+    w, h = int(rp[0, 0]), int(rp[0, 1])
+    acc = np.zeros((w * h, 4), np.float32) if accum is None else np.ascontiguousarray(
+        accum, np.float32).copy()
+    lvA, lvB, gE = _h(lvA), _h(lvB), _h(gE)
+    lz, ly, lx = lvA.shape[:3]
+    lib().or_render_trace(ptr(rp), ptr(_h(vol)), ptr(_h(solt)), ptr(_h(vel)),
+                          ptr(np.ascontiguousarray(bricks, np.float32)),
+                          ptr(np.ascontiguousarray(lut, np.float32)),
+                          ptr(np.ascontiguousarray(ecdf, np.float32)), ptr(lvA), ptr(lvB), lx,
+                          ly, lz, ptr(gE), gE.shape[1], ptr(acc))
+    return acc
 
 
 def f32_to_f16(x):

@@ -66,13 +66,16 @@ class Ref:
             self.kernels.update(split_kernels(rd(f)))
         # the renderer's input pack (src/render.rs:135,229-230: with common.wgsl)
         rk = split_kernels(rd("render.wgsl"))
-        for k in ("pack", "bricks", "ecells"):
+        for k in ("pack", "bricks", "ecells", "trace", "lightvol", "lightground", "blur"):
             self.kernels[k] = rk[k]
+        self.trace_lib = rd("trace_lib.wgsl")
 
     def assemble(self, name):
-        """src/gpu.rs:212-237."""
+        """src/gpu.rs:212-237 (the renderer's trace kernels and blur are
+        assembled without common.wgsl, src/render.rs:229-236)."""
         body = self.kernels[name]
-        s = self.common if not name.startswith("mg_") else ""
+        no_common = name.startswith("mg_") or name in ("trace", "lightvol", "lightground", "blur")
+        s = "" if no_common else self.common
         for line in body.splitlines():
             t = line.strip()
             if t.startswith("//@COMP "):
@@ -85,6 +88,8 @@ class Ref:
                 s += self.vel
             elif t.startswith("//@STATS "):
                 s += self.stats.replace("STATSB", t[len("//@STATS "):].strip())
+            elif t == "//@TRACE":
+                s += self.trace_lib
         return s + body
 
 
@@ -273,6 +278,142 @@ def gen_render(ref, only):
     return out
 
 
+def render_rp(P, w, h, spp, frame, cache, bounces):
+    """The trace kernels' uniform block (trace_lib.wgsl:1-14) for a camera
+    outside the domain looking at its centre, built as src/render.rs:142-210
+    does (fov 45 degrees, shutter 180 degrees at 30 fps, ground on, sky
+    0.003, soot albedo 0.25)."""
+    from pyro_b200 import color
+    dx = float(np.float32(P.dx))
+    ext = np.array([P.nx * dx, P.ny * dx, P.nz * dx])
+    target = 0.5 * ext
+    pos = target + np.array([0.13, 0.07, -1.1])
+    fwd = (target - pos) / np.linalg.norm(target - pos)
+    right = np.cross(fwd, [0.0, 1.0, 0.0])
+    right = right / np.linalg.norm(right)
+    up = np.cross(right, fwd)
+    focus = float(np.linalg.norm(target - pos))
+    se = color.soot_extinction(0.25)
+    side = 3.0 * max(ext[0], ext[2])
+    f = np.float32
+    return {
+        "res": np.array([w, h, 0, spp], np.uint32),
+        "dims": np.array([P.nx, P.ny, P.nz, frame], np.uint32),
+        "camPos": np.array([*pos, np.tan(np.radians(45.0) * 0.5)], f),
+        "camFwd": np.array([*fwd, w / h], f),
+        "camRight": np.array([*right, 0.0], f),
+        "camUp": np.array([*up, focus], f),
+        "a": np.array([dx, 0.6, 180.0 / 360.0 / 30.0, 0.003], f),
+        "b": np.array([1.0, 0.12, bounces, 0.05], f),
+        "soot": np.array([se[0], se[1], se[2], 0.25], f),
+        "c": np.array([5.0, 0.92, 0.55, P.t0], f),
+        "alb": [np.array([0.32, 0.05, 0.05, 0.05], f), np.array([0.05, 0.05, 0.05, 0.05], f)],
+        "gc": np.array([0.5 * ext[0] - 0.5 * side, 0.5 * ext[2] - 0.5 * side, side,
+                        1.0 if cache else 0.0], f),
+    }
+
+
+RP_FIELDS = ("res", "dims", "camPos", "camFwd", "camRight", "camUp", "a", "b", "soot", "c",
+             "alb0", "alb1", "gc")
+
+
+def rp_array(rp):
+    """The uniform block as 13 rows of 4 (u32 rows stored as their values)."""
+    rows = []
+    for k in RP_FIELDS:
+        v = rp["alb"][int(k[-1])] if k.startswith("alb") else rp[k]
+        rows.append(np.asarray(v, np.float64))
+    return np.stack(rows)
+
+
+def gen_trace(ref, only):
+    """The renderer's light caches and camera rays (render.wgsl:100-304,
+    trace_lib.wgsl) on the render golden's packed volumes, in the order of
+    src/render.rs:351-418: lightvol, lightground, the blur chain, then
+    trace.  Sizes are cut for the interpreter: an 8x8 ground cache (256^2 in
+    the reference) and 8 shadow rays per cache cell (LV_N = 96, GR_N = 128)."""
+    if only is not None and "trace" not in only:
+        return {}
+    from pyro_b200 import color
+    d = np.load(os.path.join(HERE, "render_c0.npz"))
+    P = params_from(d["params"])
+    nx, ny, nz = int(P.nx), int(P.ny), int(P.nz)
+    # a glowing-smoke volume: the random golden state's soot, heat release
+    # and temperature clamped to 2 ppm, 500 kW/m^3 and 1000 K
+    v32 = d["vol"].astype(np.float32)
+    v32[..., 0] = np.clip(v32[..., 0], 0.0, 2.0)
+    v32[..., 3] = np.clip(v32[..., 3], 0.0, 500.0)
+    v32[..., 1] = np.minimum(v32[..., 1], 1000.0)  # cached flux stays within binary16
+    vol, solt, vel = v32.astype(np.float16), d["solt"], d["vel"]
+    bricks = d["bricks"].reshape(-1).astype(np.float32)
+    lut = color.build_lut()
+    # the emission CDF as the reference forms it: its ecells kernel on this
+    # volume, then the FP64 running sum of src/render.rs:316-333
+    e32 = np.zeros(nx * ny * nz, np.float32)
+    run_kernel(ref, "ecells", P, {1: vol, 2: lut.copy(), 3: e32, 4: color.chemi_block()},
+               groups3((nx, ny, nz)))
+    e = np.maximum(e32, 0).astype(np.float64)
+    acc = np.cumsum(e)
+    tot = acc[-1]
+    ecdf = np.append((acc / tot).astype(np.float32), np.float32(tot))
+    lvd = ((nx + 1) // 2, (ny + 1) // 2, (nz + 1) // 2)
+    gres = 8
+    over = {"LV_N": np.uint32(8), "GR_N": np.uint32(8)}
+    out = {}
+    for mode, (w, h, spp, bounces) in (("cache", (6, 4, 2, 2.0)), ("path", (4, 3, 2, 2.0))):
+        cache = mode == "cache"
+        rp = render_rp(P, w, h, spp, 3, cache, bounces)
+        lvA = np.zeros((lvd[2], lvd[1], lvd[0], 4), np.float16)
+        lvB = np.zeros_like(lvA)
+        gE = np.zeros((1, gres, gres, 4), np.float16)
+        base = {0: rp, 1: vol, 2: solt, 3: vel, 4: None, 5: bricks, 6: lut, 8: ecdf}
+        t0 = time.time()
+        if cache:
+            m = wgsl.Module(ref.assemble("lightvol"), overrides=over)
+            for b_, v_ in {**base, 12: lvA, 13: lvB}.items():
+                m.bind(b_, v_)
+            m.dispatch(groups3(lvd))
+            m = wgsl.Module(ref.assemble("lightground"), overrides=over)
+            for b_, v_ in {**base, 14: gE}.items():
+                m.bind(b_, v_)
+            m.dispatch(((gres + 7) // 8, (gres + 7) // 8, 1), wg=(8, 8, 1))
+            raw = dict(lvA=lvA.copy(), lvB=lvB.copy(), gE=gE.copy())
+            t1 = np.zeros_like(lvA)
+            t2 = np.zeros_like(lvA)
+            gt = np.zeros_like(gE)
+            chain = [((0, 2), lvA, t1), ((1, 2), t1, t2), ((2, 2), t2, lvA),
+                     ((0, 2), lvB, t1), ((1, 2), t1, t2), ((2, 2), t2, lvB),
+                     ((0, 3), gE, gt), ((1, 3), gt, gE)]
+            for (axis, rad), src, dst in chain:
+                m = wgsl.Module(ref.assemble("blur"))
+                m.bind(0, {"axis": np.array([axis, rad, 0, 0], np.uint32)})
+                m.bind(1, src)
+                m.bind(2, dst)
+                dd = (src.shape[2], src.shape[1], src.shape[0])
+                m.dispatch(groups3(dd))
+        accum = np.zeros((w * h, 4), np.float32)
+        m = wgsl.Module(ref.assemble("trace"), overrides=over)
+        for b_, v_ in {**base, 7: accum, 9: lvA, 10: lvB, 11: gE}.items():
+            m.bind(b_, v_)
+        m.dispatch(((w + 7) // 8, (h + 7) // 8, 1), wg=(8, 8, 1))
+        rec = dict(params=d["params"], vol=vol, solt=solt, vel=vel, bricks=bricks, lut=lut,
+                   ecdf=ecdf, rp=rp_array(rp), lvA=lvA, lvB=lvB, gE=gE, accum=accum)
+        if cache:
+            rec.update({k + "_raw": v for k, v in raw.items()})
+        out[f"trace_{mode}"] = rec
+        print(f"trace {mode} {time.time() - t0:.1f}s", flush=True)
+    return out
+
+
+def params_from(pb):
+    from pyro_b200 import _abi
+    import ctypes
+    P = _abi.PyroParams()
+    b = bytes(pb)
+    ctypes.memmove(ctypes.byref(P), b, len(b))
+    return P
+
+
 def lv(d, h):
     return {"nx": np.uint32(d[0]), "ny": np.uint32(d[1]), "nz": np.uint32(d[2]), "h": np.float32(h)}
 
@@ -357,6 +498,7 @@ def main():
     out.update(gen_sim(ref, only))
     out.update(gen_mg(ref, only))
     out.update(gen_render(ref, only))
+    out.update(gen_trace(ref, only))
     for k, d in out.items():
         np.savez_compressed(os.path.join(HERE, k + ".npz"), **d)
     print(f"wrote {len(out)} fixtures to {HERE}")

@@ -542,6 +542,66 @@ def _dot(a, b):
     return r
 
 
+def _f32_unary(fn, x):
+    """An f32 builtin on a scalar (kept a scalar) or a vector."""
+    if isinstance(x, np.ndarray):
+        return fn(x.astype(F32))
+    return F32(fn(F32(x)))
+
+
+class Mat3:
+    """mat3x3<f32> as its three column vectors.  matrix * vector is
+    c0 * v.x + c1 * v.y + c2 * v.z, summed in that order in f32."""
+
+    def __init__(self, cols):
+        self.c = [np.asarray(c, dtype=F32) for c in cols]
+
+    def __mul__(self, v):
+        v = np.asarray(v, dtype=F32)
+        return (self.c[0] * v[0] + self.c[1] * v[1]) + self.c[2] * v[2]
+
+
+def _normalize(v):
+    v = np.asarray(v, dtype=F32)
+    return v / _length(v)
+
+
+def _texture_dimensions(tex, *level):
+    """A 3D texture bound as an (nz, ny, nx, 4) array: vec3u(nx, ny, nz)."""
+    return np.array([tex.shape[2], tex.shape[1], tex.shape[0]], dtype=U32)
+
+
+def _texture_sample_level(tex, samp, uv, level):
+    """textureSampleLevel with the renderer's sampler (linear filtering,
+    clamp-to-edge addressing; src/render.rs:121-125), modelled exactly in
+    f32: per axis p = u * n - 0.5, texels floor(p) and floor(p) + 1 clamped
+    to the texture, weight p - floor(p); mixes along x, then y, then z."""
+    uv = np.asarray(uv, dtype=F32)
+
+    def ax(u, n):
+        p = F32(F32(u) * F32(n)) - F32(0.5)
+        f0 = np.floor(p)
+        w = F32(p - f0)
+        i0 = int(f0)
+        return min(max(i0, 0), n - 1), min(max(i0 + 1, 0), n - 1), w
+
+    nz, ny, nx = tex.shape[0], tex.shape[1], tex.shape[2]
+    x0, x1, fx = ax(uv[0], nx)
+    y0, y1, fy = ax(uv[1], ny)
+    z0, z1, fz = ax(uv[2], nz)
+
+    def t(z, y, x):
+        return tex[z, y, x].astype(F32)
+
+    def mix(a, b, w):
+        return a * (F32(1.0) - w) + b * w
+    c00 = mix(t(z0, y0, x0), t(z0, y0, x1), fx)
+    c10 = mix(t(z0, y1, x0), t(z0, y1, x1), fx)
+    c01 = mix(t(z1, y0, x0), t(z1, y0, x1), fx)
+    c11 = mix(t(z1, y1, x0), t(z1, y1, x1), fx)
+    return mix(mix(c00, c10, fy), mix(c01, c11, fy), fz)
+
+
 def _texture_load(tex, c, level):
     """textureLoad of one texel of a 3D texture, as vec4<f32>."""
     return tex[int(c[2]), int(c[1]), int(c[0])].astype(F32)
@@ -549,6 +609,9 @@ def _texture_load(tex, c, level):
 
 BUILTINS: Dict[str, Callable] = {
     "textureStore": _texture_store, "textureLoad": _texture_load, "dot": _dot,
+    "textureDimensions": _texture_dimensions, "textureSampleLevel": _texture_sample_level,
+    "normalize": _normalize, "cos": lambda x: _f32_unary(np.cos, x),
+    "sin": lambda x: _f32_unary(np.sin, x), "round": lambda x: _f32_unary(np.round, x),
     "clamp": _clamp, "min": _minmax(np.minimum), "max": _minmax(np.maximum), "mix": _mix,
     "smoothstep": _smoothstep, "select": _select, "exp": np.exp, "sqrt": np.sqrt,
     "length": _length, "cross": _cross, "floor": np.floor, "abs": np.abs,
@@ -909,6 +972,8 @@ class Module:
                 d = dt or (F32 if any(isinstance(x, np.floating) for x in flat) else I32)
                 return np.array([_convert(x, d) for x in flat], dtype=d)
             return ctor
+        if name in ("mat3x3f", "mat3x3"):
+            return lambda fr: Mat3([f(fr) for f in fs])
         if name in ("f32", "i32", "u32", "bool"):
             dt = _scalar_kind(name)
             return lambda fr: _convert(fs[0](fr), dt)

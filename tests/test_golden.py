@@ -202,3 +202,45 @@ def test_render_emission(case):
     assert cdf.shape == (d["ecell"].size + 1,)
     assert np.all(np.diff(cdf[:-1]) >= 0) and cdf[-2] == 1.0
     assert abs(cdf[-1] - np.maximum(d["ecell"], 0).astype(np.float64).sum()) <= 1e-6 * cdf[-1]
+
+
+def test_render_light_caches_and_blur():
+    """The path tracer's light caches (render.wgsl:217-269) and their blur
+    chain (render.wgsl:271-304, src/render.rs:362-396): the oracle's binary16
+    caches equal the interpreted WGSL's bit for bit (8 shadow rays per cell
+    instead of 96 / 128, an 8x8 ground cache instead of 256^2)."""
+    d = _load("trace_cache")
+    lvd = (d["lvA"].shape[2], d["lvA"].shape[1], d["lvA"].shape[0])
+    a, b = oracle.render_lightvol(d["rp"], d["vol"], d["solt"], d["vel"], d["bricks"], d["lut"],
+                                  d["ecdf"], lvd, lv_n=8)
+    assert np.array_equal(a.view(np.uint16), d["lvA_raw"].view(np.uint16))
+    assert np.array_equal(b.view(np.uint16), d["lvB_raw"].view(np.uint16))
+    g = oracle.render_lightground(d["rp"], d["vol"], d["solt"], d["vel"], d["bricks"], d["lut"],
+                                  d["ecdf"], d["gE_raw"].shape[1], gr_n=8)
+    assert np.array_equal(g.view(np.uint16), d["gE_raw"].view(np.uint16))
+    A, B, G = d["lvA_raw"], d["lvB_raw"], d["gE_raw"]
+    for ax in (0, 1, 2):
+        A = oracle.render_blur(A, ax, 2)
+        B = oracle.render_blur(B, ax, 2)
+    for ax in (0, 1):
+        G = oracle.render_blur(G, ax, 3)
+    for got, want in ((A, d["lvA"]), (B, d["lvB"]), (G, d["gE"])):
+        assert np.array_equal(got.view(np.uint16), want.view(np.uint16))
+    assert np.isfinite(d["lvA"].astype(np.float32)).all() and d["lvA"].astype(np.float32).max() > 0
+
+
+@pytest.mark.parametrize("mode", ["cache", "path"])
+def test_render_trace(mode):
+    """Camera rays (render.wgsl:132-215 with trace_lib.wgsl): light-cache mode
+    and pure path tracing (2 bounces, next-event estimation with MIS,
+    Russian roulette), motion blur on.  The random numbers are the
+    reference's PCG hash, so the oracle follows the interpreted WGSL's paths;
+    pixels agree to the rounding of exp / sin / cos / sqrt (1e-5 relative of
+    the image's largest value)."""
+    d = _load(f"trace_{mode}")
+    acc = oracle.render_trace(d["rp"], d["vol"], d["solt"], d["vel"], d["bricks"], d["lut"],
+                              d["ecdf"], d["lvA"], d["lvB"], d["gE"])
+    want = d["accum"]
+    assert np.all(acc[:, 3] == want[:, 3])
+    assert np.max(np.abs(acc[:, :3] - want[:, :3])) <= 1e-5 * np.abs(want[:, :3]).max()
+    assert np.count_nonzero(want[:, :3]) > want[:, :3].size // 2
