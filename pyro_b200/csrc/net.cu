@@ -5,7 +5,7 @@
 //
 // The network has no counterpart in the reference: it is the learned warm
 // start that stands beside the multigrid pressure solve of
-// src/sim.rs:451-491, which remains the fallback and the judge of its error.
+// src/sim.rs:451-491, which remains the fallback and the measure of its error.
 #include <cuda_bf16.h>
 
 #include <cmath>
