@@ -631,6 +631,8 @@ void or_render_lightvol(const double* rp, const uint16_t* vol, const uint16_t* s
   C.lut = lut;
   C.ecdf = ecdf;
   const int bd[3] = {(nx + 7) / 8, (ny + 7) / 8, (nz + 7) / 8};
+  // cells are independent (each seeds its own random numbers)
+#pragma omp parallel for collapse(2) firstprivate(C) schedule(dynamic)
   for (int z = 0; z < lz; z++)
     for (int y = 0; y < ly; y++)
       for (int x = 0; x < lx; x++) {
@@ -683,6 +685,7 @@ void or_render_lightground(const double* rp, const uint16_t* vol, const uint16_t
   C.bricks = bricks;
   C.lut = lut;
   C.ecdf = ecdf;
+#pragma omp parallel for firstprivate(C) schedule(dynamic)
   for (int y = 0; y < gres; y++)
     for (int x = 0; x < gres; x++) {
       C.rs = Ctx::pcg((uint32_t)(x + gres * y) * 7919u + C.R.dims[3] * 104729u + 5u);
@@ -704,6 +707,7 @@ void or_render_blur(const uint16_t* src, uint16_t* dst, int nx, int ny, int nz, 
                     int r) {
   const Tex s = tex_of(src, nx, ny, nz);
   const float s2 = 0.5f * (float)(r * r) + 0.5f;
+#pragma omp parallel for
   for (int z = 0; z < nz; z++)
     for (int y = 0; y < ny; y++)
       for (int x = 0; x < nx; x++) {
@@ -743,6 +747,8 @@ void or_render_trace(const double* rp, const uint16_t* vol, const uint16_t* sol,
   C.lut = lut;
   C.ecdf = ecdf;
   C.cache_inscatter = true;
+  // pixels are independent (each seeds its own random numbers)
+#pragma omp parallel for firstprivate(C) schedule(dynamic)
   for (uint32_t y = 0; y < C.R.res[1]; y++)
     for (uint32_t x = 0; x < C.R.res[0]; x++) {
       const F4 v = C.tracePixel(x, y);
