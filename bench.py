@@ -226,6 +226,18 @@ def cpu_baseline_run(sc, P, sol, fields, n_steps, dt, t0, threads=None):
     return 1e3 * float(np.mean(times)), cores
 
 
+def max_over_ranks(values, device):
+    """The slowest rank's figures: an all-reduce MAX of `values` over the
+    process group when one is running with more than one rank (the timing
+    rule for N replicas), else the values themselves."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
 def run_reference(args):
     """CPU restatement of the reference step on all host cores."""
     rank = int(os.environ.get("RANK", "0"))
@@ -529,10 +541,7 @@ def run_ours(args):
         f"bricks {bricks_ms:.3f} ms")
 
     # gather max over ranks
-    vals = torch.tensor([ms, ms_e2e], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(vals, op=dist.ReduceOp.MAX)
-    ms, ms_e2e = float(vals[0]), float(vals[1])
+    ms, ms_e2e = max_over_ranks([ms, ms_e2e], "cuda")
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
