@@ -370,6 +370,70 @@ int pyro_k_render_cdf(uint64_t n, const float* ecell, float* cdf, void* stream);
 int pyro_k_render_bricks(uint32_t nx, uint32_t ny, uint32_t nz,
                          const void* vol, const void* sol_packed, float* bricks,
                          void* stream);
+
+/* The volume path tracer's uniform block (struct RP of
+ * src/shaders/trace_lib.wgsl:1-14, filled by src/render.rs:180-210 and per
+ * frame / dispatch at src/render.rs:335-337, 410-412): 13 rows of 16 bytes,
+ * the same layout. */
+typedef struct PyroRenderParams {
+  uint32_t res[4];   /* width, height, first sample index, samples now     */
+  uint32_t dims[4];  /* nx, ny, nz, frame number                           */
+  float cam_pos[4];  /* camera position, tan(half field of view)           */
+  float cam_fwd[4];  /* forward unit vector, aspect (width / height)       */
+  float cam_right[4];/* right unit vector, aperture radius (m)             */
+  float cam_up[4];   /* up unit vector, focus distance (m)                 */
+  float a[4];        /* dx (m), march step (cells), shutter (s), sky       */
+  float b[4];        /* ground on, ground albedo, bounces, chemi strength  */
+  float soot[4];     /* soot extinction per ppm (rgb, 1/m), soot albedo    */
+  float c[4];        /* smoke extinction (m^2/g), smoke albedo, HG g, T0   */
+  float alb[8];      /* surface albedo per material slot                   */
+  float gc[4];       /* ground cache x0, z0, side (m); mode: 1 light cache,
+                        0 pure path tracing                                */
+} PyroRenderParams;
+
+/* The path tracer's kernels on explicit device buffers.  `rp` is a HOST
+ * pointer (copied into the launch).  vol, sol, vel: the packed volumes of
+ * pyro_k_render_pack (rp->dims cells, 4 binary16 each); bricks as
+ * pyro_k_render_bricks; lut: the colour table, 2048 float4 rows (soot
+ * emission, then surface emission; src/color.rs:46-75); ecdf: the emission
+ * CDF of pyro_k_render_cdf (cells + 1 floats).  Light-cache volumes are
+ * (lz, ly, lx) cells of 4 binary16 values, x fastest; the reference sizes
+ * them ceil(n / 2) per axis (src/render.rs:104); the ground cache is
+ * gres x gres (256 in the reference, src/render.rs:12). */
+
+/* lightvol (render.wgsl:217-251): per cache cell, `rays` next-event shadow
+ * rays (96 in the reference) toward the fire; lvA = mean flux (rgb, 0),
+ * lvB = luminance-weighted mean direction (xyz, 0). */
+int pyro_k_render_lightvol(const PyroRenderParams* rp, const void* vol,
+                           const void* sol, const void* vel,
+                           const float* bricks, const float* lut,
+                           const float* ecdf, uint32_t lx, uint32_t ly,
+                           uint32_t lz, uint32_t rays, void* lvA, void* lvB,
+                           void* stream);
+/* lightground (render.wgsl:253-269): ground irradiance per texel of the
+ * gres x gres cache over the square rp->gc, `rays` shadow rays (128). */
+int pyro_k_render_lightground(const PyroRenderParams* rp, const void* vol,
+                              const void* sol, const void* vel,
+                              const float* bricks, const float* lut,
+                              const float* ecdf, uint32_t gres, uint32_t rays,
+                              void* gE, void* stream);
+/* blur (render.wgsl:271-304): Gaussian of radius `radius` (1..16) along
+ * `axis` (0 = x, 1 = y, 2 = z), clamp-to-edge, src -> dst (distinct
+ * buffers of nx*ny*nz cells of 4 binary16 values). */
+int pyro_k_render_blur(const void* src, void* dst, uint32_t nx, uint32_t ny,
+                       uint32_t nz, uint32_t axis, uint32_t radius,
+                       void* stream);
+/* trace (render.wgsl:132-215): for each pixel of rp->res.xy, adds the sum
+ * of samples rp->res.z .. rp->res.z + rp->res.w - 1 to accum (float4 per
+ * pixel: rgb, sample count).  Light-cache mode (rp->gc[3] > 0.5) reads the
+ * blurred caches lvA, lvB (lx, ly, lz) and gE (gres); pure path tracing
+ * (rp->b[2] bounces) ignores them (they may be NULL). */
+int pyro_k_render_trace(const PyroRenderParams* rp, const void* vol,
+                        const void* sol, const void* vel, const float* bricks,
+                        const float* lut, const float* ecdf, const void* lvA,
+                        const void* lvB, uint32_t lx, uint32_t ly, uint32_t lz,
+                        const void* gE, uint32_t gres, float* accum,
+                        void* stream);
 /* Coarsest-level solve: `iters` red-black SOR sweeps (omega) in one
  * launch (src/sim.rs:473 runs 80 sweeps at omega 1.6 as 160 dispatches). */
 int pyro_k_mg_coarse(uint32_t nx, uint32_t ny, uint32_t nz, float h,

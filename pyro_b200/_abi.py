@@ -66,6 +66,46 @@ PARAM_SCALARS = [
 ]
 
 
+class PyroRenderParams(ctypes.Structure):
+    """The path tracer's uniform block (struct RP, trace_lib.wgsl:1-14)."""
+    _fields_ = [("res", ctypes.c_uint32 * 4), ("dims", ctypes.c_uint32 * 4),
+                ("cam_pos", ctypes.c_float * 4), ("cam_fwd", ctypes.c_float * 4),
+                ("cam_right", ctypes.c_float * 4), ("cam_up", ctypes.c_float * 4),
+                ("a", ctypes.c_float * 4), ("b", ctypes.c_float * 4),
+                ("soot", ctypes.c_float * 4), ("c", ctypes.c_float * 4),
+                ("alb", ctypes.c_float * 8), ("gc", ctypes.c_float * 4)]
+    ROWS = ("res", "dims", "cam_pos", "cam_fwd", "cam_right", "cam_up", "a", "b", "soot", "c",
+            "alb", "alb", "gc")
+
+    @classmethod
+    def from_rows(cls, rows) -> "PyroRenderParams":
+        """From 13 rows of 4 numbers in the block's order (u32 rows as their
+        values; rows 10 and 11 the eight albedos)."""
+        rows = [list(map(float, r)) for r in rows]
+        if len(rows) != 13 or any(len(r) != 4 for r in rows):
+            raise ValueError("render parameters: expected 13 rows of 4")
+        p = cls()
+        for k, name in enumerate(cls.ROWS):
+            if name == "alb":
+                continue
+            dst = getattr(p, name)
+            for j in range(4):
+                dst[j] = int(rows[k][j]) if name in ("res", "dims") else rows[k][j]
+        for j in range(8):
+            p.alb[j] = rows[10 + j // 4][j % 4]
+        return p
+
+    def rows(self):
+        """The 13 x 4 rows (inverse of from_rows)."""
+        out = []
+        for k, name in enumerate(self.ROWS):
+            if name == "alb":
+                out.append([float(self.alb[4 * (k - 10) + j]) for j in range(4)])
+            else:
+                out.append([float(v) for v in getattr(self, name)])
+        return out
+
+
 class PyroParams(ctypes.Structure):
     _fields_ = PARAM_SCALARS + [("mats", (ctypes.c_float * 12) * 8)]
 
@@ -79,6 +119,7 @@ class PyroParams(ctypes.Structure):
 
 
 assert ctypes.sizeof(PyroParams) == 576
+assert ctypes.sizeof(PyroRenderParams) == 208
 
 
 class PyroShape(ctypes.Structure):
@@ -163,6 +204,11 @@ SIGNATURES = {
     "pyro_k_render_bricks": [_U32, _U32, _U32, _P, _P, _P, _P],
     "pyro_k_render_ecells": [_P, _U32, _U32, _U32, _P, _P, _P, _P, _P],
     "pyro_k_render_cdf": [ctypes.c_uint64, _P, _P, _P],
+    "pyro_k_render_lightvol": [_P, _P, _P, _P, _P, _P, _P, _U32, _U32, _U32, _U32, _P, _P, _P],
+    "pyro_k_render_lightground": [_P, _P, _P, _P, _P, _P, _P, _U32, _U32, _P, _P],
+    "pyro_k_render_blur": [_P, _P, _U32, _U32, _U32, _U32, _U32, _P],
+    "pyro_k_render_trace": [_P, _P, _P, _P, _P, _P, _P, _P, _P, _U32, _U32, _U32, _P, _U32, _P,
+                            _P],
     "pyro_conv3_forward": [_P, _I, _I, _I, _I, _I, _P, _I, _P, _I, _P, _I, _P],
     "pyro_conv3_backward_data": [_P, _I, _I, _I, _I, _I, _P, _I, _P, _P, _I, _P],
     "pyro_conv3_backward_weight": [_P, _I, _P, _I, _I, _I, _I, _I, _P, _P],

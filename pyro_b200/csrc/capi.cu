@@ -27,6 +27,11 @@ bool dims_ok(uint32_t nx, uint32_t ny, uint32_t nz) {
          (uint64_t)(nx + 1) * (ny + 1) * (nz + 1) < (1ull << 31);
 }
 
+// light caches, ground cache and images: at least one texel, < 2^31 texels
+bool cache_dims_ok(uint32_t lx, uint32_t ly, uint32_t lz) {
+  return lx >= 1 && ly >= 1 && lz >= 1 && (uint64_t)lx * ly * lz < (1ull << 31);
+}
+
 }  // namespace
 
 namespace pyro {
@@ -271,6 +276,79 @@ int pyro_k_render_cdf(uint64_t n, const float* ecell, float* cdf, void* stream) 
   cudaError_t e = launch_render_cdf((long)n, ecell, cdf, scratch.p, S(stream));
   if (e == cudaSuccess) e = cudaStreamSynchronize(S(stream));  // before scratch is freed
   return ret(e, "pyro_k_render_cdf");
+}
+
+// The tracer's uniform block and the bindings every tracer kernel reads:
+// the grid (as pyro_k_render_pack), dx, and the volumes and tables.
+#define TRACE_COMMON(name)                                                                  \
+  clear_error();                                                                            \
+  PYRO_REQUIRE(rp, #name ": null render parameters");                                       \
+  PYRO_REQUIRE(dims_ok(rp->dims[0], rp->dims[1], rp->dims[2]),                              \
+               #name ": invalid grid dimensions");                                          \
+  PYRO_REQUIRE(rp->a[0] > 0.0f, #name ": dx (a[0]) must be positive");                      \
+  PYRO_REQUIRE(vol && sol && vel && bricks && lut && ecdf, #name ": null buffer");
+
+int pyro_k_render_lightvol(const PyroRenderParams* rp, const void* vol, const void* sol,
+                           const void* vel, const float* bricks, const float* lut,
+                           const float* ecdf, uint32_t lx, uint32_t ly, uint32_t lz,
+                           uint32_t rays, void* lvA, void* lvB, void* stream) {
+  TRACE_COMMON(pyro_k_render_lightvol)
+  PYRO_REQUIRE(cache_dims_ok(lx, ly, lz), "pyro_k_render_lightvol: invalid cache dimensions");
+  PYRO_REQUIRE(rays >= 1 && rays <= 65536, "pyro_k_render_lightvol: rays must be 1 .. 65536");
+  PYRO_REQUIRE(lvA && lvB && lvA != lvB, "pyro_k_render_lightvol: lvA, lvB must be distinct");
+  return ret(launch_render_lightvol(*rp, vol, sol, vel, bricks, lut, ecdf, (int)lx, (int)ly,
+                                    (int)lz, (int)rays, lvA, lvB, S(stream)),
+             "pyro_k_render_lightvol");
+}
+
+int pyro_k_render_lightground(const PyroRenderParams* rp, const void* vol, const void* sol,
+                              const void* vel, const float* bricks, const float* lut,
+                              const float* ecdf, uint32_t gres, uint32_t rays, void* gE,
+                              void* stream) {
+  TRACE_COMMON(pyro_k_render_lightground)
+  PYRO_REQUIRE(cache_dims_ok(gres, gres, 1), "pyro_k_render_lightground: invalid gres");
+  PYRO_REQUIRE(rays >= 1 && rays <= 65536, "pyro_k_render_lightground: rays must be 1 .. 65536");
+  PYRO_REQUIRE(rp->gc[2] > 0.0f, "pyro_k_render_lightground: ground side (gc[2]) must be positive");
+  PYRO_REQUIRE(gE, "pyro_k_render_lightground: null gE");
+  return ret(launch_render_lightground(*rp, vol, sol, vel, bricks, lut, ecdf, (int)gres,
+                                       (int)rays, gE, S(stream)),
+             "pyro_k_render_lightground");
+}
+
+int pyro_k_render_blur(const void* src, void* dst, uint32_t nx, uint32_t ny, uint32_t nz,
+                       uint32_t axis, uint32_t radius, void* stream) {
+  clear_error();
+  PYRO_REQUIRE(cache_dims_ok(nx, ny, nz), "pyro_k_render_blur: invalid dimensions");
+  PYRO_REQUIRE(axis <= 2, "pyro_k_render_blur: axis must be 0, 1 or 2");
+  PYRO_REQUIRE(radius >= 1 && (int)radius <= render_blur_max_radius(),
+               "pyro_k_render_blur: radius must be 1 .. 16");
+  PYRO_REQUIRE(src && dst && src != dst, "pyro_k_render_blur: src, dst must be distinct buffers");
+  return ret(launch_render_blur(src, dst, Dims3{(int)nx, (int)ny, (int)nz}, (int)axis,
+                                (int)radius, S(stream)),
+             "pyro_k_render_blur");
+}
+
+int pyro_k_render_trace(const PyroRenderParams* rp, const void* vol, const void* sol,
+                        const void* vel, const float* bricks, const float* lut,
+                        const float* ecdf, const void* lvA, const void* lvB, uint32_t lx,
+                        uint32_t ly, uint32_t lz, const void* gE, uint32_t gres, float* accum,
+                        void* stream) {
+  TRACE_COMMON(pyro_k_render_trace)
+  PYRO_REQUIRE(accum, "pyro_k_render_trace: null accum");
+  PYRO_REQUIRE(cache_dims_ok(rp->res[0], rp->res[1], 1),
+               "pyro_k_render_trace: invalid image size (res[0], res[1])");
+  PYRO_REQUIRE(rp->res[3] <= 1024, "pyro_k_render_trace: at most 1024 samples per dispatch");
+  PYRO_REQUIRE(rp->b[2] >= 0.0f && rp->b[2] <= 64.0f,
+               "pyro_k_render_trace: bounces (b[2]) must be 0 .. 64");
+  if (rp->gc[3] > 0.5f) {
+    PYRO_REQUIRE(lvA && lvB && gE, "pyro_k_render_trace: light-cache mode needs lvA, lvB, gE");
+    PYRO_REQUIRE(cache_dims_ok(lx, ly, lz) && cache_dims_ok(gres, gres, 1),
+                 "pyro_k_render_trace: invalid cache dimensions");
+    PYRO_REQUIRE(rp->gc[2] > 0.0f, "pyro_k_render_trace: ground side (gc[2]) must be positive");
+  }
+  return ret(launch_render_trace(*rp, vol, sol, vel, bricks, lut, ecdf, lvA, lvB, (int)lx,
+                                 (int)ly, (int)lz, gE, (int)gres, accum, S(stream)),
+             "pyro_k_render_trace");
 }
 
 int pyro_voxelize(const PyroShape* shapes, uint32_t n_shapes, uint32_t nx, uint32_t ny,

@@ -69,6 +69,25 @@ cudaError_t launch_render_ecells(const PyroParams* P, Dims3 d, const void* vol, 
 size_t render_cdf_scratch_bytes(long n);
 cudaError_t launch_render_cdf(long n, const float* ecell, float* cdf, void* scratch,
                               cudaStream_t st);
+// The volume path tracer (k_trace.cu) on the packed volumes: camera rays
+// into accum, the two light caches, and the caches' separable blur (radius
+// 1 .. render_blur_max_radius()).
+cudaError_t launch_render_trace(const PyroRenderParams& R, const void* vol, const void* sol,
+                                const void* vel, const float* bricks, const float* lut,
+                                const float* ecdf, const void* lvA, const void* lvB, int lx,
+                                int ly, int lz, const void* gE, int gres, float* accum,
+                                cudaStream_t st);
+cudaError_t launch_render_lightvol(const PyroRenderParams& R, const void* vol, const void* sol,
+                                   const void* vel, const float* bricks, const float* lut,
+                                   const float* ecdf, int lx, int ly, int lz, int rays,
+                                   void* lvA, void* lvB, cudaStream_t st);
+cudaError_t launch_render_lightground(const PyroRenderParams& R, const void* vol,
+                                      const void* sol, const void* vel, const float* bricks,
+                                      const float* lut, const float* ecdf, int gres, int rays,
+                                      void* gE, cudaStream_t st);
+int render_blur_max_radius();
+cudaError_t launch_render_blur(const void* src, void* dst, Dims3 d, int axis, int r,
+                               cudaStream_t st);
 cudaError_t launch_project(const PyroParams* P, Dims3 d, float* u, float* v, float* w,
                            const float* phi, const uint32_t* flags, cudaStream_t st);
 

@@ -146,6 +146,30 @@ class Object:
 
 
 @dataclass
+class RenderCfg:
+    """The [render] table (src/scene.rs:141-190), with its defaults."""
+    width: int = 1280
+    height: int = 720
+    spp: int = 64
+    camera: List[float] = field(default_factory=lambda: [0.0, 1.5, -6.0])
+    target: List[float] = field(default_factory=lambda: [0.0, 2.0, 0.0])
+    fov: float = 45.0
+    exposure: float = 0.0
+    auto_exposure: bool = True
+    shutter: float = 180.0
+    ground: bool = True
+    ground_albedo: float = 0.12
+    sky: float = 0.003
+    bounces: int = 2
+    step: float = 0.6
+    glare: float = 0.04
+    aperture: float = 0.0
+    focus: float = 0.0
+    chemi: float = 0.05
+    mode: str = "cache"
+
+
+@dataclass
 class OutputCfg:
     dir: str = "out"
     preroll: float = 0.0
@@ -169,8 +193,7 @@ class Grid:
 
 @dataclass
 class Scene:
-    """A parsed scene (src/scene.rs:8-25).  The render table is accepted and
-    ignored: rendering is not part of the simulation step."""
+    """A parsed scene (src/scene.rs:8-25)."""
     domain: Domain
     sim: SimCfg = field(default_factory=SimCfg)
     wind: Wind = field(default_factory=Wind)
@@ -178,6 +201,7 @@ class Scene:
     fuel: FuelCfg = field(default_factory=FuelCfg)
     objects: List[Object] = field(default_factory=list)
     output: OutputCfg = field(default_factory=OutputCfg)
+    render: RenderCfg = field(default_factory=RenderCfg)
     # Exact grid dimensions for synthetic workloads of a named shape (the
     # reference always rounds to multiples of 16; None keeps that rule).
     dims_override: Optional[List[int]] = None
@@ -203,6 +227,8 @@ class Scene:
             sc.fuel = _fill(FuelCfg, d["fuel"], "fuel")
         if "output" in d:
             sc.output = _fill(OutputCfg, d["output"], "output")
+        if "render" in d:
+            sc.render = _fill(RenderCfg, d["render"], "render")
         for o in d.get("object", []):
             sc.objects.append(_fill(Object, o, "object"))
         return sc
