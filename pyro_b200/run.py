@@ -1,7 +1,8 @@
-"""The `--sim-only` frame loop of the reference (src/main.rs:121-279).
+"""The frame loop of the reference (src/main.rs:56-279).
 
-    python -m pyro_b200.run scene.toml [--duration S] [--cell M] [--preroll S]
-                                       [--out DIR] [--slice] [--quiet]
+    python -m pyro_b200.run scene.toml [--sim-only] [--duration S] [--cell M]
+                                       [--preroll S] [--out DIR] [--slice] [--quiet]
+                                       [--spp N] [--res WxH] [--ev EV] [--still T]
 
 Per output frame: CFL substep count n = ceil(frame_dt / (cfl*dx/max(u,1))),
 n substeps with statistics on the last, one statistics read (the frame's
@@ -10,8 +11,10 @@ only device synchronisation), time averages over t >= max(preroll,
 burning area and rate per area, 50/90/99 % cumulative heat-release heights
 and the Heskestad height for pools.  `--slice` writes the 5-panel mid-z
 image (T, Y_F, Y_O2, soot volume fraction, heat release) of src/main.rs:
-201-239 as a PNG.  Rendering flags of the reference CLI (--spp, --res, --ev,
---still, --open) drive the renderer, which is not part of this library.
+201-239 as a PNG.  Without --sim-only every frame from the end of the preroll
+on (or one still with --still T) is rendered by the GPU path tracer
+(pyro_b200.render), developed (pyro_b200.post) and written as a PNG, with
+--spp, --res WxH and --ev as in the reference CLI.
 
 `run_frames` works on any object with the Sim interface (step, read_stats,
 time, dx, dims), so the host logic is tested without a GPU.
@@ -73,16 +76,25 @@ def height_at(layers_avg: np.ndarray, frac: float, dx: float) -> float:
 
 
 def run_frames(scene, sim, duration: Optional[float] = None, preroll: Optional[float] = None,
-               on_frame: Optional[Callable] = None, quiet: bool = True) -> Summary:
-    """The frame loop (src/main.rs:121-157) on `sim`."""
+               on_frame: Optional[Callable] = None, quiet: bool = True,
+               still: Optional[float] = None,
+               on_render: Optional[Callable[[int], None]] = None) -> Summary:
+    """The frame loop (src/main.rs:121-197) on `sim`.  `on_render(f)` is
+    called for the frames the reference renders: every frame from the end
+    of the preroll on, or with `still` = t only the last frame of a run of
+    t + half a frame."""
     fps = scene.sim.fps
     frame_dt = F(1.0) / F(fps)
-    pre = scene.output.preroll if preroll is None else preroll
-    dur = scene.sim.duration if duration is None else duration
-    total = pre + dur
-    frames = int(round(total * fps))
+    # f32 as in src/main.rs:121-130; f32::round rounds halves away from zero
+    pre = F(scene.output.preroll if preroll is None else preroll)
+    dur = F(scene.sim.duration if duration is None else duration)
+    total = F(pre + dur)
+    if still is not None:
+        pre, total = F(still), F(F(still) + frame_dt * F(0.5))
+    frames = int(math.floor(float(F(total * F(fps))) + 0.5))
     max_u = 2.0
-    avg_from = max(pre, 0.4 * total)
+    avg_from = float(max(pre, F(F(0.4) * total)))
+    render_from = float(F(pre - F(1e-4)))
     n_avg = 0
     hrr = rad = pyro = area = 0.0
     ny = sim.dims[1]
@@ -106,6 +118,9 @@ def run_frames(scene, sim, duration: Optional[float] = None, preroll: Optional[f
             layers[:len(lay)] += lay
         if on_frame is not None:
             on_frame(f, n, st)
+        rendering = (f == frames - 1) if still is not None else float(sim.time) >= render_from
+        if on_render is not None and rendering:
+            on_render(f)
         if not quiet:
             print(f"t={float(sim.time):5.2f}s substeps {n:2d} HRR {st.hrr / 1e3:7.1f} kW "
                   f"rad {100.0 * st.rad / st.hrr if st.hrr > 0 else 0.0:4.0f}% "
@@ -184,13 +199,17 @@ def print_summary(scene, s: Summary) -> None:
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(prog="pyro_b200.run", description=__doc__.split("\n")[0])
     ap.add_argument("scene")
-    ap.add_argument("--sim-only", action="store_true", help="accepted; this tool only simulates")
+    ap.add_argument("--sim-only", action="store_true", help="simulate and print statistics only")
     ap.add_argument("--duration", type=float)
     ap.add_argument("--cell", type=float)
     ap.add_argument("--preroll", type=float)
     ap.add_argument("--out")
     ap.add_argument("--slice", action="store_true")
     ap.add_argument("--quiet", action="store_true")
+    ap.add_argument("--spp", type=int, help="samples per pixel")
+    ap.add_argument("--res", help="image size, e.g. 1920x1080")
+    ap.add_argument("--ev", type=float, help="exposure compensation (EV)")
+    ap.add_argument("--still", type=float, help="render one still at t seconds")
     a = ap.parse_args(argv)
     from .scene import Scene
     from .sim import Sim
@@ -201,12 +220,39 @@ def main(argv=None) -> int:
         sc.domain.cell = a.cell
     if a.preroll is not None:
         sc.output.preroll = a.preroll
+    if a.spp is not None:
+        sc.render.spp = a.spp
+    if a.res:
+        v = [int(x) for x in a.res.split("x") if x.isdigit()]
+        if len(v) == 2:
+            sc.render.width, sc.render.height = v
+    if a.ev is not None:
+        sc.render.exposure = a.ev
     g = sc.grid()
     print(f"grid {g.dims[0]}x{g.dims[1]}x{g.dims[2]} ({np.prod(g.dims) / 1e6:.1f} M cells, "
           f"{g.dx * 100:.1f} cm)")
     sim = Sim(sc)
-    s = run_frames(sc, sim, quiet=a.quiet)
     out_dir = a.out or os.path.join(os.path.dirname(os.path.abspath(a.scene)), sc.output.dir)
+    on_render = None
+    if not a.sim_only:  # src/main.rs:100-104, 113-119, 180-197
+        from .post import Camera
+        from .render import Renderer
+        os.makedirs(out_dir, exist_ok=True)
+        rend = Renderer(sc, sim)
+        cam = Camera(sc.render.auto_exposure, sc.render.exposure, sc.render.glare)
+        frame_dt = float(F(1.0) / F(sc.sim.fps))
+        idx = [0]
+
+        def on_render(f):
+            img = rend.render(sim, f, sc.render.spp)
+            name = (f"still_{float(sim.time):.1f}s.png" if a.still is not None
+                    else f"frame_{idx[0]:05d}.png")
+            path = os.path.join(out_dir, name)
+            write_png(path, cam.develop(img, frame_dt))
+            idx[0] += 1
+            if not a.quiet:
+                print(f"  rendered {path}")
+    s = run_frames(sc, sim, quiet=a.quiet, still=a.still, on_render=on_render)
     if a.slice:
         os.makedirs(out_dir, exist_ok=True)
         s0, s1 = sim.read_scalars()

@@ -99,3 +99,24 @@ def test_slice_image_and_png(tmp_path):
     idat = data[data.index(b"IDAT") + 4:data.index(b"IEND") - 8]
     raw = zlib.decompress(idat)
     assert len(raw) == ny * (1 + 3 * w)
+
+
+def test_rendered_frames_follow_the_reference_rule():
+    """src/main.rs:122-128, 158-161: every frame once the preroll has passed;
+    with a still at t, a run of t + half a frame and only its last frame."""
+    sc = Scene.from_toml_str(SCENE)
+    sim = FakeSim([16, 32, 16], 0.1, umax=7.0)
+    seen, times = [], []
+
+    def rec(f):
+        seen.append(f)
+        times.append(float(sim.time))
+
+    s = run_frames(sc, sim, on_render=rec)
+    assert seen == list(range(seen[0], s.frames)) and min(times) >= 0.5 - 1e-4
+    assert seen[0] == 4  # t = 0.5 s after the fifth frame (fps 10)
+    sim = FakeSim([16, 32, 16], 0.1, umax=7.0)
+    seen.clear()
+    s = run_frames(sc, sim, still=1.2, on_render=seen.append)
+    # f32: 1.2 + 0.05 = 1.25, x 10 = 12.5, rounded half away from zero
+    assert s.frames == 13 and seen == [s.frames - 1]
