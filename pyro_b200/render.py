@@ -197,8 +197,19 @@ class Renderer:
         st = sim.stream()
         sim.render_pack(True)
         sim.render_emission(chemi=self.chemi, lut=self.lut)
-        vol, sol, vel = (sim.device_ptr(f)[0] for f in (_abi.F_RVOL, _abi.F_RSOL, _abi.F_RVEL))
-        bricks, ecdf = sim.device_ptr(_abi.F_BRICKS)[0], sim.device_ptr(_abi.F_ECDF)[0]
+        cells = self.dims[0] * self.dims[1] * self.dims[2]
+        nb = ((self.dims[0] + 7) // 8) * ((self.dims[1] + 7) // 8) * ((self.dims[2] + 7) // 8)
+        want = {_abi.F_RVOL: 8 * cells, _abi.F_RSOL: 8 * cells, _abi.F_RVEL: 8 * cells,
+                _abi.F_BRICKS: 4 * nb, _abi.F_ECDF: 4 * (cells + 1)}
+        ptrs = {}
+        for f, nbytes in want.items():
+            p, size = sim.device_ptr(f)
+            if size < nbytes:
+                raise ValueError(f"render: field {f} holds {size} bytes, the grid "
+                                 f"{self.dims} needs {nbytes}")
+            ptrs[f] = p
+        vol, sol, vel = ptrs[_abi.F_RVOL], ptrs[_abi.F_RSOL], ptrs[_abi.F_RVEL]
+        bricks, ecdf = ptrs[_abi.F_BRICKS], ptrs[_abi.F_ECDF]
         rp = _rp_copy(self.base)
         rp.dims[3] = frame
         with torch.cuda.stream(torch.cuda.ExternalStream(st)):
