@@ -278,11 +278,12 @@ def gen_render(ref, only):
     return out
 
 
-def render_rp(P, w, h, spp, frame, cache, bounces):
+def render_rp(P, w, h, spp, frame, cache, bounces, aperture=0.0, first=0):
     """The trace kernels' uniform block (trace_lib.wgsl:1-14) for a camera
     outside the domain looking at its centre, built as src/render.rs:142-210
     does (fov 45 degrees, shutter 180 degrees at 30 fps, ground on, sky
-    0.003, soot albedo 0.25)."""
+    0.003, soot albedo 0.25); `aperture` > 0 is a thin lens focused on the
+    centre, `first` the dispatch's first sample index."""
     from pyro_b200 import color
     dx = float(np.float32(P.dx))
     ext = np.array([P.nx * dx, P.ny * dx, P.nz * dx])
@@ -297,11 +298,11 @@ def render_rp(P, w, h, spp, frame, cache, bounces):
     side = 3.0 * max(ext[0], ext[2])
     f = np.float32
     return {
-        "res": np.array([w, h, 0, spp], np.uint32),
+        "res": np.array([w, h, first, spp], np.uint32),
         "dims": np.array([P.nx, P.ny, P.nz, frame], np.uint32),
         "camPos": np.array([*pos, np.tan(np.radians(45.0) * 0.5)], f),
         "camFwd": np.array([*fwd, w / h], f),
-        "camRight": np.array([*right, 0.0], f),
+        "camRight": np.array([*right, aperture], f),
         "camUp": np.array([*up, focus], f),
         "a": np.array([dx, 0.6, 180.0 / 360.0 / 30.0, 0.003], f),
         "b": np.array([1.0, 0.12, bounces, 0.05], f),
@@ -332,7 +333,12 @@ def gen_trace(ref, only):
     src/render.rs:351-418: lightvol, lightground, the blur chain, then
     trace.  Sizes are cut for the interpreter: an 8x8 ground cache (256^2 in
     the reference) and 8 shadow rays per cache cell (LV_N = 96, GR_N = 128)."""
+    cases = {"cache": (6, 4, 2, 2.0, 0.0, 0, 3), "path": (4, 3, 2, 2.0, 0.0, 0, 3),
+             # a thin lens, another frame and a later first sample
+             "lens": (4, 3, 2, 2.0, 0.03, 5, 9)}
     if only is not None and "trace" not in only:
+        cases = {k: v for k, v in cases.items() if f"trace_{k}" in only}
+    if not cases:
         return {}
     from pyro_b200 import color
     d = np.load(os.path.join(HERE, "render_c0.npz"))
@@ -360,9 +366,9 @@ def gen_trace(ref, only):
     gres = 8
     over = {"LV_N": np.uint32(8), "GR_N": np.uint32(8)}
     out = {}
-    for mode, (w, h, spp, bounces) in (("cache", (6, 4, 2, 2.0)), ("path", (4, 3, 2, 2.0))):
-        cache = mode == "cache"
-        rp = render_rp(P, w, h, spp, 3, cache, bounces)
+    for mode, (w, h, spp, bounces, aperture, first, frame) in cases.items():
+        cache = mode != "path"
+        rp = render_rp(P, w, h, spp, frame, cache, bounces, aperture, first)
         lvA = np.zeros((lvd[2], lvd[1], lvd[0], 4), np.float16)
         lvB = np.zeros_like(lvA)
         gE = np.zeros((1, gres, gres, 4), np.float16)

@@ -229,11 +229,12 @@ def test_render_light_caches_and_blur():
     assert np.isfinite(d["lvA"].astype(np.float32)).all() and d["lvA"].astype(np.float32).max() > 0
 
 
-@pytest.mark.parametrize("mode", ["cache", "path"])
+@pytest.mark.parametrize("mode", ["cache", "path", "lens"])
 def test_render_trace(mode):
     """Camera rays (render.wgsl:132-215 with trace_lib.wgsl): light-cache mode
     and pure path tracing (2 bounces, next-event estimation with MIS,
-    Russian roulette), motion blur on.  The random numbers are the
+    Russian roulette), motion blur on; "lens" is light-cache mode through a
+    thin lens (render.wgsl:148-154) at another frame and first sample.  The random numbers are the
     reference's PCG hash, so the oracle follows the interpreted WGSL's paths;
     pixels agree to the rounding of exp / sin / cos / sqrt (1e-5 relative of
     the image's largest value)."""
