@@ -87,6 +87,27 @@ def mg_cycle_bytes(dims_list):
     return b, n0
 
 
+def mg_class_bytes(dims_list, cycles):
+    """Algorithmic bytes of each V-cycle launch class over one pressure
+    solve of `cycles` V-cycles (the classes of pyro_sim_profile_pressure):
+    12 B per level cell per colour pass, 13.5 per restriction and 13 per
+    prolongation (per fine cell), 80 sweeps of 24 B on the coarsest level;
+    the preparation reads each level's u32 flags and writes its mask byte,
+    and per coarse level reads the fine flags and writes the coarse ones."""
+    n = [d[0] * d[1] * d[2] for d in dims_list]
+    L = len(n)
+    out = {"mg_prepare": sum(5.0 * m for m in n) + sum(4.0 * n[l - 1] + 4.0 * n[l]
+                                                     for l in range(1, L)),
+           "mg_pass_l0": cycles * 8 * 12.0 * n[0],
+           "mg_restrict_l0": cycles * 13.5 * n[0] if L > 1 else 0.0,
+           "mg_prolong_l0": cycles * 13.0 * n[0] if L > 1 else 0.0,
+           "mg_pass_mid": cycles * sum(8 * 12.0 * n[l] for l in range(1, L - 1)),
+           "mg_restrict_mid": cycles * sum(13.5 * n[l] for l in range(1, L - 1)),
+           "mg_prolong_mid": cycles * sum(13.0 * n[l] for l in range(1, L - 1)),
+           "mg_coarse": cycles * 80 * COARSE_SWEEP_BYTES * n[-1]}
+    return out
+
+
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -484,15 +505,40 @@ def run_ours(args):
     log("profiled " + " ".join(f"{v:.3f}" for v in phases))
     names = _abi.PROFILE_PHASES
     kern = {names[i]: float(phases[i]) for i in range(12)}
-    single = {k: v for k, v in kern.items() if k in ALG_BYTES}
-    dom = max(single, key=single.get)
     peak, peak_kind = load_peaks()
     info = sim.info()
     lvl = [tuple(info.level_dims[l]) for l in range(info.levels)]
     cyc_bytes, _ = mg_cycle_bytes(lvl)
     step_bytes = sum(ALG_BYTES.values()) * cells + sc.sim.pressure_cycles * cyc_bytes
-    dom_bytes = ALG_BYTES[dom] * cells
-    achieved = dom_bytes / (kern[dom] * 1e-3) / 1e9
+    # the pressure solve per launch class, an event after every launch
+    mg_ms = np.zeros(len(_abi.MG_CLASSES))
+    mg_n = np.zeros(len(_abi.MG_CLASSES), np.int32)
+    ms_buf = np.zeros(len(_abi.MG_CLASSES), np.float32)
+    for k in range(nprof):
+        _abi.check("pyro_sim_profile_pressure", lib.pyro_sim_profile_pressure(
+            sim._h, ms_buf.ctypes.data_as(ctypes.c_void_p), mg_n.ctypes.data_as(ctypes.c_void_p),
+            len(_abi.MG_CLASSES)))
+        mg_ms += ms_buf
+    mg_ms /= nprof
+    mg_bytes = mg_class_bytes(lvl, sc.sim.pressure_cycles)
+    # every launch class of the substep: launches, device ms per substep and
+    # per launch, algorithmic bytes per launch and the HBM fraction
+    classes = {}
+    for k in ALG_BYTES:
+        classes[k] = {"launches": 1, "ms": kern[k], "alg_bytes": ALG_BYTES[k] * cells}
+    for i, k in enumerate(_abi.MG_CLASSES):
+        if mg_n[i] > 0:
+            classes[k] = {"launches": int(mg_n[i]), "ms": float(mg_ms[i]),
+                          "alg_bytes": mg_bytes[k] / int(mg_n[i])}
+    for k, c in classes.items():
+        c["ms_per_launch"] = c["ms"] / c["launches"]
+        c["gbs"] = c["alg_bytes"] / (c["ms_per_launch"] * 1e-3) / 1e9
+        c["frac"] = c["gbs"] / peak
+    log("pressure classes " + " ".join(f"{k}={c['ms']:.3f}" for k, c in classes.items()
+                                       if k.startswith("mg_")))
+    dom = max(classes, key=lambda k: classes[k]["ms"])
+    dom_bytes = classes[dom]["alg_bytes"]
+    achieved = classes[dom]["gbs"]
     traffic = load_traffic().get(dom, {}).get("dram_bytes_per_launch")
 
     # ---- the renderer's per-frame input pack (render.wgsl:3-61): the pack
@@ -595,10 +641,12 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "alg_bytes_per_launch": dom_bytes,
-                     "launch_ms": kern[dom]},
+                     "launch_ms": classes[dom]["ms_per_launch"],
+                     "launches_per_substep": classes[dom]["launches"]},
         "step_roofline": {"alg_bytes": step_bytes, "achieved_gbs": step_bytes / (ms * 1e-3) / 1e9,
                           "frac": step_bytes / (ms * 1e-3) / 1e9 / peak},
         "kernels_ms": kern,
+        "kernel_classes": classes,
         "frame_pack": frame_pack,
         "throughput": {"value": world * cells / (ms * 1e-3), "unit": "cells*substeps/s"},
         "cpu_baseline": cpu,

@@ -184,6 +184,18 @@ int pyro_sim_stream(PyroSim* sim, void** stream);
 #define PYRO_PROFILE_PHASES 12
 int pyro_sim_profile_step(PyroSim* sim, float dt, float time, float ign_on,
                           int want_stats, float* ms_out, int n);
+/* The fixed V-cycle pressure solve of a substep (src/sim.rs:451-491) on the
+ * simulation's current right-hand side, launched with a CUDA event after
+ * every launch; blocks, leaves every field as it was (the warm start is
+ * restored), and writes per launch class the summed device time in ms and
+ * the launch count to ms_out / launches_out[0..min(n, 8)):
+ * 0 level masks and coarse flags, 1 level-0 colour pass, 2 level-0
+ * restriction, 3 prolongation onto level 0, 4 colour pass on a middle
+ * level, 5 restriction from a middle level, 6 prolongation onto a middle
+ * level, 7 the coarsest-level solve.  No counterpart in the reference. */
+#define PYRO_PROFILE_MG_CLASSES 8
+int pyro_sim_profile_pressure(PyroSim* sim, float* ms_out, int* launches_out,
+                              int n);
 /* Wait for all enqueued work. */
 int pyro_sim_sync(PyroSim* sim);
 int pyro_sim_info(PyroSim* sim, PyroSimInfo* info);
@@ -319,7 +331,13 @@ int pyro_k_forces(const PyroParams* params_dev, uint32_t nx, uint32_t ny,
  * that device current, looks up the array's device address; make that first
  * call before any stream capture.  All calls share the one array: calls that
  * overlap on the GPU (different streams, other threads) race on it and must
- * be serialised by the caller.  Results equal pyro_k_forces. */
+ * be serialised by the caller.  Results equal pyro_k_forces.  The call is
+ * stream-ordered: it queues the kernels on `stream` and returns without
+ * waiting (pyro_k_forces waits, to free its scratch), so an error raised by
+ * a running kernel shows up at the caller's next synchronisation of that
+ * stream.  The array's device address is looked up once per device and kept
+ * for the process: a cudaDeviceReset after the first call on a device is not
+ * supported. */
 #define PYRO_NOALLOC_MAX_CELLS (1u << 19)
 int pyro_k_forces_noalloc(const PyroParams* params_dev, uint32_t nx,
                           uint32_t ny, uint32_t nz, float* u, float* v,
@@ -333,7 +351,12 @@ int pyro_k_divergence(const PyroParams* params_dev, uint32_t nx, uint32_t ny,
 int pyro_k_project(const PyroParams* params_dev, uint32_t nx, uint32_t ny,
                    uint32_t nz, float* u, float* v, float* w, const float* phi,
                    const uint32_t* flags, void* stream);
-/* Multigrid kernels on one level (dims, spacing h). */
+/* Multigrid kernels on one level (dims, spacing h), with the reference's
+ * per-cell solid flags: mg_smooth (mg.wgsl:5-36), mg_restrict
+ * (mg.wgsl:38-83, also writes the coarse flags) and mg_prolong
+ * (mg.wgsl:85-120).  They run the kernels the V-cycle launches: the level's
+ * neighbour masks are built into a temporary buffer first, and each call
+ * waits for its stream before returning. */
 int pyro_k_mg_smooth(uint32_t nx, uint32_t ny, uint32_t nz, float h,
                      const float* b, const uint32_t* flags, float* phi,
                      int color, float omega, void* stream);
@@ -345,6 +368,31 @@ int pyro_k_mg_prolong(uint32_t fnx, uint32_t fny, uint32_t fnz,
                       const float* pc, const uint32_t* ff, float* pf,
                       uint32_t cnx, uint32_t cny, uint32_t cnz,
                       const uint32_t* fc, void* stream);
+/* The same kernels on caller-owned neighbour masks, as the V-cycle runs
+ * them, with the storage of phi and b selectable (FP32, or BF16 with FP32
+ * arithmetic: the MGPCG preconditioner) and bc_mode as
+ * pyro_poisson_create.  The mask byte of a cell (pyro_k_mg_meta): bit k =
+ * neighbour k (+x, -x, +y, -y, +z, -z) is inside the level and fluid, bit 6
+ * = the cell is solid.  pyro_k_mg_flags_down gives the coarse solid flags
+ * (every in-domain child solid, mg.wgsl:73-82).  Asynchronous on `stream`. */
+#define PYRO_MG_F32 0
+#define PYRO_MG_BF16 1
+int pyro_k_mg_meta(uint32_t nx, uint32_t ny, uint32_t nz,
+                   const uint32_t* flags, uint8_t* meta, void* stream);
+int pyro_k_mg_flags_down(uint32_t fnx, uint32_t fny, uint32_t fnz,
+                         const uint32_t* ff, uint32_t cnx, uint32_t cny,
+                         uint32_t cnz, uint32_t* fc, void* stream);
+int pyro_k_mg_pass(uint32_t nx, uint32_t ny, uint32_t nz, float h,
+                   const void* b, const uint8_t* meta, void* phi, int color,
+                   float omega, int bc_mode, int storage, void* stream);
+int pyro_k_mg_restrict_m(uint32_t fnx, uint32_t fny, uint32_t fnz, float fh,
+                         const void* pf, const void* bf, const uint8_t* mf,
+                         uint32_t cnx, uint32_t cny, uint32_t cnz, void* bc,
+                         void* pc, int bc_mode, int storage, void* stream);
+int pyro_k_mg_prolong_m(uint32_t fnx, uint32_t fny, uint32_t fnz,
+                        const void* pc, const uint8_t* mf, void* pf,
+                        uint32_t cnx, uint32_t cny, uint32_t cnz,
+                        const uint8_t* mc, int storage, void* stream);
 int pyro_k_mg_resid(uint32_t nx, uint32_t ny, uint32_t nz, float h,
                     const float* phi, const float* b, const uint32_t* flags,
                     float* stats, void* stream);

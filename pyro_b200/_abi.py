@@ -30,6 +30,11 @@ F_ECELL, F_ECDF = 15, 16  # renderer fire-light sampling tables
 PROFILE_PHASES = ["solid", "curl", "adv_vel1", "adv_vel2", "adv_s1", "adv_s2", "react",
                   "forces", "divergence", "pressure", "project", "total"]
 
+MG_F32, MG_BF16 = 0, 1  # storage of phi and b in the pyro_k_mg_* mask entries
+# launch classes of pyro_sim_profile_pressure
+MG_CLASSES = ["mg_prepare", "mg_pass_l0", "mg_restrict_l0", "mg_prolong_l0", "mg_pass_mid",
+              "mg_restrict_mid", "mg_prolong_mid", "mg_coarse"]
+
 SOLVER_VCYCLE = 0
 SOLVER_VCYCLE_TOL = 1
 SOLVER_MGPCG = 2
@@ -172,6 +177,7 @@ SIGNATURES = {
     "pyro_sim_stream": [_P, ctypes.POINTER(_P)],
     "pyro_sim_sync": [_P],
     "pyro_sim_profile_step": [_P, _F, _F, _F, _I, _P, _I],
+    "pyro_sim_profile_pressure": [_P, _P, _P, _I],
     "pyro_sim_info": [_P, ctypes.POINTER(PyroSimInfo)],
     "pyro_sim_set_solver": [_P, _I, _F, _I],
     "pyro_sim_last_solve": [_P, ctypes.POINTER(PyroSolveInfo)],
@@ -197,6 +203,12 @@ SIGNATURES = {
     "pyro_k_mg_smooth": [_U32, _U32, _U32, _F, _P, _P, _P, _I, _F, _P],
     "pyro_k_mg_restrict": [_U32, _U32, _U32, _F, _P, _P, _P, _U32, _U32, _U32, _P, _P, _P, _P],
     "pyro_k_mg_prolong": [_U32, _U32, _U32, _P, _P, _P, _U32, _U32, _U32, _P, _P],
+    "pyro_k_mg_meta": [_U32, _U32, _U32, _P, _P, _P],
+    "pyro_k_mg_flags_down": [_U32, _U32, _U32, _P, _U32, _U32, _U32, _P, _P],
+    "pyro_k_mg_pass": [_U32, _U32, _U32, _F, _P, _P, _P, _I, _F, _I, _I, _P],
+    "pyro_k_mg_restrict_m": [_U32, _U32, _U32, _F, _P, _P, _P, _U32, _U32, _U32, _P, _P, _I,
+                             _I, _P],
+    "pyro_k_mg_prolong_m": [_U32, _U32, _U32, _P, _P, _P, _U32, _U32, _U32, _P, _I, _P],
     "pyro_k_mg_resid": [_U32, _U32, _U32, _F, _P, _P, _P, _P, _P],
     "pyro_k_mg_coarse": [_U32, _U32, _U32, _F, _P, _P, _P, _I, _F, _P],
     "pyro_k_mg_coarse_sym": [_U32, _U32, _U32, _F, _P, _P, _P, _I, _F, _I, _P],

@@ -155,15 +155,26 @@ int pyro_k_project(const PyroParams* params_dev, uint32_t nx, uint32_t ny, uint3
   return ret(launch_project(params_dev, d, u, v, w, phi, flags, S(stream)), "pyro_k_project");
 }
 
+// The reference's per-flag multigrid dispatches (mg.wgsl) run here on the
+// kernels the V-cycle itself launches: the level's neighbour masks are built
+// into a temporary buffer (k_mg_meta), then the mask-driven pass,
+// restriction or prolongation runs.  Each call waits for its stream before
+// the temporaries are freed.
 int pyro_k_mg_smooth(uint32_t nx, uint32_t ny, uint32_t nz, float h, const float* b,
                      const uint32_t* flags, float* phi, int color, float omega, void* stream) {
   clear_error();
   PYRO_REQUIRE(dims_ok(nx, ny, nz), "pyro_k_mg_smooth: invalid grid dimensions");
   PYRO_REQUIRE(b && flags && phi, "pyro_k_mg_smooth: null buffer");
   PYRO_REQUIRE(color == 0 || color == 1, "pyro_k_mg_smooth: color must be 0 or 1");
-  return ret(launch_mg_smooth(Dims3{(int)nx, (int)ny, (int)nz}, h, b, flags, phi, color, omega, 0,
-                              S(stream)),
-             "pyro_k_mg_smooth");
+  Dims3 d{(int)nx, (int)ny, (int)nz};
+  DevBuf meta;
+  int rc = meta.alloc(d.cells());
+  if (rc != PYRO_OK) return rc;
+  cudaError_t e = launch_mg_meta(d, flags, meta.as<uint8_t>(), S(stream));
+  if (e == cudaSuccess)
+    e = launch_mg_pass(d, h, b, meta.as<uint8_t>(), phi, color, omega, 0, S(stream));
+  if (e == cudaSuccess) e = cudaStreamSynchronize(S(stream));
+  return ret(e, "pyro_k_mg_smooth");
 }
 
 int pyro_k_mg_restrict(uint32_t fnx, uint32_t fny, uint32_t fnz, float fh, const float* pf,
@@ -175,9 +186,16 @@ int pyro_k_mg_restrict(uint32_t fnx, uint32_t fny, uint32_t fnz, float fh, const
   PYRO_REQUIRE(cnx == (fnx + 1) / 2 && cny == (fny + 1) / 2 && cnz == (fnz + 1) / 2,
                "pyro_k_mg_restrict: coarse dims must be ceil(fine / 2)");
   PYRO_REQUIRE(pf && bf && ff && bc && pc && fc, "pyro_k_mg_restrict: null buffer");
-  return ret(launch_mg_restrict(Dims3{(int)fnx, (int)fny, (int)fnz}, fh, pf, bf, ff,
-                                Dims3{(int)cnx, (int)cny, (int)cnz}, bc, pc, fc, 0, S(stream)),
-             "pyro_k_mg_restrict");
+  Dims3 df{(int)fnx, (int)fny, (int)fnz}, dc{(int)cnx, (int)cny, (int)cnz};
+  DevBuf meta;
+  int rc = meta.alloc(df.cells());
+  if (rc != PYRO_OK) return rc;
+  cudaError_t e = launch_mg_meta(df, ff, meta.as<uint8_t>(), S(stream));
+  if (e == cudaSuccess) e = launch_mg_flags_down(df, ff, dc, fc, S(stream));
+  if (e == cudaSuccess)
+    e = launch_mg_restrict_m(df, fh, pf, bf, meta.as<uint8_t>(), dc, bc, pc, 0, S(stream));
+  if (e == cudaSuccess) e = cudaStreamSynchronize(S(stream));
+  return ret(e, "pyro_k_mg_restrict");
 }
 
 int pyro_k_mg_prolong(uint32_t fnx, uint32_t fny, uint32_t fnz, const float* pc,
@@ -188,9 +206,93 @@ int pyro_k_mg_prolong(uint32_t fnx, uint32_t fny, uint32_t fnz, const float* pc,
   PYRO_REQUIRE(cnx == (fnx + 1) / 2 && cny == (fny + 1) / 2 && cnz == (fnz + 1) / 2,
                "pyro_k_mg_prolong: coarse dims must be ceil(fine / 2)");
   PYRO_REQUIRE(pc && ff && pf && fc, "pyro_k_mg_prolong: null buffer");
-  return ret(launch_mg_prolong(Dims3{(int)fnx, (int)fny, (int)fnz}, pc, ff, pf,
-                               Dims3{(int)cnx, (int)cny, (int)cnz}, fc, S(stream)),
-             "pyro_k_mg_prolong");
+  Dims3 df{(int)fnx, (int)fny, (int)fnz}, dc{(int)cnx, (int)cny, (int)cnz};
+  DevBuf mf, mc;
+  int rc = mf.alloc(df.cells());
+  if (rc == PYRO_OK) rc = mc.alloc(dc.cells());
+  if (rc != PYRO_OK) return rc;
+  cudaError_t e = launch_mg_meta(df, ff, mf.as<uint8_t>(), S(stream));
+  if (e == cudaSuccess) e = launch_mg_meta(dc, fc, mc.as<uint8_t>(), S(stream));
+  if (e == cudaSuccess)
+    e = launch_mg_prolong_m(df, pc, mf.as<uint8_t>(), pf, dc, mc.as<uint8_t>(), S(stream));
+  if (e == cudaSuccess) e = cudaStreamSynchronize(S(stream));
+  return ret(e, "pyro_k_mg_prolong");
+}
+
+int pyro_k_mg_meta(uint32_t nx, uint32_t ny, uint32_t nz, const uint32_t* flags, uint8_t* meta,
+                   void* stream) {
+  clear_error();
+  PYRO_REQUIRE(dims_ok(nx, ny, nz), "pyro_k_mg_meta: invalid grid dimensions");
+  PYRO_REQUIRE(flags && meta, "pyro_k_mg_meta: null buffer");
+  return ret(launch_mg_meta(Dims3{(int)nx, (int)ny, (int)nz}, flags, meta, S(stream)),
+             "pyro_k_mg_meta");
+}
+
+int pyro_k_mg_flags_down(uint32_t fnx, uint32_t fny, uint32_t fnz, const uint32_t* ff,
+                         uint32_t cnx, uint32_t cny, uint32_t cnz, uint32_t* fc, void* stream) {
+  clear_error();
+  PYRO_REQUIRE(dims_ok(fnx, fny, fnz), "pyro_k_mg_flags_down: invalid grid dimensions");
+  PYRO_REQUIRE(cnx == (fnx + 1) / 2 && cny == (fny + 1) / 2 && cnz == (fnz + 1) / 2,
+               "pyro_k_mg_flags_down: coarse dims must be ceil(fine / 2)");
+  PYRO_REQUIRE(ff && fc, "pyro_k_mg_flags_down: null buffer");
+  return ret(launch_mg_flags_down(Dims3{(int)fnx, (int)fny, (int)fnz}, ff,
+                                  Dims3{(int)cnx, (int)cny, (int)cnz}, fc, S(stream)),
+             "pyro_k_mg_flags_down");
+}
+
+int pyro_k_mg_pass(uint32_t nx, uint32_t ny, uint32_t nz, float h, const void* b,
+                   const uint8_t* meta, void* phi, int color, float omega, int bc_mode,
+                   int storage, void* stream) {
+  clear_error();
+  PYRO_REQUIRE(dims_ok(nx, ny, nz), "pyro_k_mg_pass: invalid grid dimensions");
+  PYRO_REQUIRE(b && meta && phi, "pyro_k_mg_pass: null buffer");
+  PYRO_REQUIRE(color == 0 || color == 1, "pyro_k_mg_pass: color must be 0 or 1");
+  PYRO_REQUIRE(bc_mode == 0 || bc_mode == 1, "pyro_k_mg_pass: bc_mode must be 0 or 1");
+  PYRO_REQUIRE(storage == PYRO_MG_F32 || storage == PYRO_MG_BF16,
+               "pyro_k_mg_pass: storage must be PYRO_MG_F32 or PYRO_MG_BF16");
+  Dims3 d{(int)nx, (int)ny, (int)nz};
+  return ret(storage == PYRO_MG_BF16
+                 ? launch_mg_pass_bf16(d, h, b, meta, phi, color, omega, bc_mode, S(stream))
+                 : launch_mg_pass(d, h, (const float*)b, meta, (float*)phi, color, omega,
+                                  bc_mode, S(stream)),
+             "pyro_k_mg_pass");
+}
+
+int pyro_k_mg_restrict_m(uint32_t fnx, uint32_t fny, uint32_t fnz, float fh, const void* pf,
+                         const void* bf, const uint8_t* mf, uint32_t cnx, uint32_t cny,
+                         uint32_t cnz, void* bc, void* pc, int bc_mode, int storage,
+                         void* stream) {
+  clear_error();
+  PYRO_REQUIRE(dims_ok(fnx, fny, fnz), "pyro_k_mg_restrict_m: invalid grid dimensions");
+  PYRO_REQUIRE(cnx == (fnx + 1) / 2 && cny == (fny + 1) / 2 && cnz == (fnz + 1) / 2,
+               "pyro_k_mg_restrict_m: coarse dims must be ceil(fine / 2)");
+  PYRO_REQUIRE(pf && bf && mf && bc && pc, "pyro_k_mg_restrict_m: null buffer");
+  PYRO_REQUIRE(bc_mode == 0 || bc_mode == 1, "pyro_k_mg_restrict_m: bc_mode must be 0 or 1");
+  PYRO_REQUIRE(storage == PYRO_MG_F32 || storage == PYRO_MG_BF16,
+               "pyro_k_mg_restrict_m: storage must be PYRO_MG_F32 or PYRO_MG_BF16");
+  Dims3 df{(int)fnx, (int)fny, (int)fnz}, dc{(int)cnx, (int)cny, (int)cnz};
+  return ret(storage == PYRO_MG_BF16
+                 ? launch_mg_restrict_m_bf16(df, fh, pf, bf, mf, dc, bc, pc, bc_mode, S(stream))
+                 : launch_mg_restrict_m(df, fh, (const float*)pf, (const float*)bf, mf, dc,
+                                        (float*)bc, (float*)pc, bc_mode, S(stream)),
+             "pyro_k_mg_restrict_m");
+}
+
+int pyro_k_mg_prolong_m(uint32_t fnx, uint32_t fny, uint32_t fnz, const void* pc,
+                        const uint8_t* mf, void* pf, uint32_t cnx, uint32_t cny, uint32_t cnz,
+                        const uint8_t* mc, int storage, void* stream) {
+  clear_error();
+  PYRO_REQUIRE(dims_ok(fnx, fny, fnz), "pyro_k_mg_prolong_m: invalid grid dimensions");
+  PYRO_REQUIRE(cnx == (fnx + 1) / 2 && cny == (fny + 1) / 2 && cnz == (fnz + 1) / 2,
+               "pyro_k_mg_prolong_m: coarse dims must be ceil(fine / 2)");
+  PYRO_REQUIRE(pc && mf && pf && mc, "pyro_k_mg_prolong_m: null buffer");
+  PYRO_REQUIRE(storage == PYRO_MG_F32 || storage == PYRO_MG_BF16,
+               "pyro_k_mg_prolong_m: storage must be PYRO_MG_F32 or PYRO_MG_BF16");
+  Dims3 df{(int)fnx, (int)fny, (int)fnz}, dc{(int)cnx, (int)cny, (int)cnz};
+  return ret(storage == PYRO_MG_BF16
+                 ? launch_mg_prolong_m_bf16(df, pc, mf, pf, dc, mc, S(stream))
+                 : launch_mg_prolong_m(df, (const float*)pc, mf, (float*)pf, dc, mc, S(stream)),
+             "pyro_k_mg_prolong_m");
 }
 
 int pyro_k_mg_resid(uint32_t nx, uint32_t ny, uint32_t nz, float h, const float* phi,
@@ -213,10 +315,15 @@ int pyro_k_mg_coarse(uint32_t nx, uint32_t ny, uint32_t nz, float h, const float
   cudaError_t e = cudaSuccess;
   if (mg_coarse_fits(d)) {
     e = launch_mg_coarse(d, h, b, flags, phi, iters, omega, 0, S(stream));
-  } else {
+  } else {  // the V-cycle's own fallback: one mask-driven launch per colour
+    DevBuf meta;
+    int rc = meta.alloc(d.cells());
+    if (rc != PYRO_OK) return rc;
+    e = launch_mg_meta(d, flags, meta.as<uint8_t>(), S(stream));
     for (int it = 0; it < iters && e == cudaSuccess; it++)
       for (int c = 0; c < 2 && e == cudaSuccess; c++)
-        e = launch_mg_smooth(d, h, b, flags, phi, c, omega, 0, S(stream));
+        e = launch_mg_pass(d, h, b, meta.as<uint8_t>(), phi, c, omega, 0, S(stream));
+    if (e == cudaSuccess) e = cudaStreamSynchronize(S(stream));
   }
   return ret(e, "pyro_k_mg_coarse");
 }

@@ -8,13 +8,12 @@
 // top face Dirichlet.  Neighbours are visited in the reference's order
 // (+x, -x, +y, -y, +z, -z) so sums round identically.
 //
-//   mg_smooth    mg.wgsl:5-36   red-black Gauss-Seidel / SOR, one colour
-//   mg_restrict  mg.wgsl:38-83  fine residual -> fluid-averaged coarse rhs
-//   mg_prolong   mg.wgsl:85-120 fluid-weighted trilinear correction
 //   mg_resid     mg.wgsl:122-158 sums of r^2 and b^2
 //   mg_coarse    the whole coarsest-level solve (src/sim.rs:473: 80 SOR
 //                sweeps at omega 1.6) in one thread-block cluster with the
 //                level in distributed shared memory, replacing 160 dispatches.
+// The per-colour smoother, the restriction and the prolongation of every
+// other level run on per-cell neighbour masks (k_mgf.cu).
 #include <cooperative_groups.h>
 #include <cstdlib>
 #include <cuda_bf16.h>
@@ -73,25 +72,6 @@ __device__ __forceinline__ void neigh_sum(const Lvl& d, int x, int y, int z, int
 }
 
 template <typename TS>
-__global__ void __launch_bounds__(256) k_mg_smooth(Lvl d, float h2, const TS* __restrict__ b,
-                                                   const uint32_t* __restrict__ f,
-                                                   TS* __restrict__ p, int color,
-                                                   float omega, int bc_mode) {
-  int y = blockIdx.y * BY + threadIdx.y;
-  int z = blockIdx.z * BZ + threadIdx.z;
-  int x = (int)(blockIdx.x * BX + threadIdx.x) * 2 + ((y + z + color) & 1);
-  if (!d.inb(x, y, z)) return;
-  int i = d.idx(x, y, z);
-  if (__ldg(f + i) == 1u) return;
-  float sum, cnt;
-  neigh_sum(
-      d, x, y, z, bc_mode, [&](int j) { return ldv(p + j); },
-      [&](int j) { return __ldg(f + j) == 1u; }, sum, cnt);
-  if (cnt < 0.5f) return;
-  stv(p + i, wmix(ldv(p + i), (sum - h2 * ldv(b + i)) / cnt, omega));
-}
-
-template <typename TS>
 __device__ __forceinline__ float resid_cell(const Lvl& d, float h2, const TS* __restrict__ p,
                                             const TS* __restrict__ b,
                                             const uint32_t* __restrict__ f, int x, int y, int z,
@@ -104,71 +84,6 @@ __device__ __forceinline__ float resid_cell(const Lvl& d, float h2, const TS* __
       d, x, y, z, bc_mode, [&](int j) { return ldv(p + j); },
       [&](int j) { return __ldg(f + j) == 1u; }, sum, cnt);
   return ldv(b + i) - (sum - cnt * pcen) / h2;
-}
-
-template <typename TS>
-__global__ void __launch_bounds__(256) k_mg_restrict(Lvl df, float h2f,
-                                                     const TS* __restrict__ pf,
-                                                     const TS* __restrict__ bf,
-                                                     const uint32_t* __restrict__ ff, Lvl dc,
-                                                     TS* __restrict__ bc,
-                                                     TS* __restrict__ pc,
-                                                     uint32_t* __restrict__ fc, int bc_mode) {
-  int x = blockIdx.x * BX + threadIdx.x;
-  int y = blockIdx.y * BY + threadIdx.y;
-  int z = blockIdx.z * BZ + threadIdx.z;
-  if (!dc.inb(x, y, z)) return;
-  float r = 0.0f, nfl = 0.0f;
-#pragma unroll
-  for (int k = 0; k < 8; k++) {
-    int cx = 2 * x + (k & 1), cy = 2 * y + ((k >> 1) & 1), cz = 2 * z + ((k >> 2) & 1);
-    if (!df.inb(cx, cy, cz)) continue;
-    if (__ldg(ff + df.idx(cx, cy, cz)) != 1u) {
-      nfl += 1.0f;
-      r += resid_cell(df, h2f, pf, bf, ff, cx, cy, cz, bc_mode);
-    }
-  }
-  int i = dc.idx(x, y, z);
-  stv(bc + i, (nfl > 0.0f) ? r / fmaxf(nfl, 1.0f) : 0.0f);
-  stv(pc + i, 0.0f);
-  fc[i] = (nfl > 0.0f) ? 0u : 1u;
-}
-
-template <typename TS>
-__global__ void __launch_bounds__(256) k_mg_prolong(Lvl df, const TS* __restrict__ pc,
-                                                    const uint32_t* __restrict__ ff,
-                                                    TS* __restrict__ pf, Lvl dc,
-                                                    const uint32_t* __restrict__ fc) {
-  int x = blockIdx.x * BX + threadIdx.x;
-  int y = blockIdx.y * BY + threadIdx.y;
-  int z = blockIdx.z * BZ + threadIdx.z;
-  if (!df.inb(x, y, z)) return;
-  int i = df.idx(x, y, z);
-  if (__ldg(ff + i) == 1u) return;
-  // x = (c + 0.5) * 0.5 - 0.5: even c -> i0 = c/2 - 1, frac 0.75;
-  // odd c -> i0 = (c-1)/2, frac 0.25 (exact in FP32).
-  float gx = ((float)x + 0.5f) * 0.5f - 0.5f;
-  float gy = ((float)y + 0.5f) * 0.5f - 0.5f;
-  float gz = ((float)z + 0.5f) * 0.5f - 0.5f;
-  int i0x = (int)floorf(gx), i0y = (int)floorf(gy), i0z = (int)floorf(gz);
-  float frx = gx - (float)i0x, fry = gy - (float)i0y, frz = gz - (float)i0z;
-  float acc = 0.0f, ws = 0.0f;
-#pragma unroll
-  for (int k = 0; k < 8; k++) {
-    int ox = k & 1, oy = (k >> 1) & 1, oz = (k >> 2) & 1;
-    int cx = min(max(i0x + ox, 0), dc.nx - 1);
-    int cy = min(max(i0y + oy, 0), dc.ny - 1);
-    int cz = min(max(i0z + oz, 0), dc.nz - 1);
-    int j = dc.idx(cx, cy, cz);
-    if (__ldg(fc + j) == 1u) continue;
-    float wx = ox ? frx : 1.0f - frx;
-    float wy = oy ? fry : 1.0f - fry;
-    float wz = oz ? frz : 1.0f - frz;
-    float w = wx * wy * wz;
-    acc += w * ldv(pc + j);
-    ws += w;
-  }
-  if (ws > 1e-4f) stv(pf + i, ldv(pf + i) + acc / ws);
 }
 
 __global__ void __launch_bounds__(256) k_mg_resid(Lvl d, float h2, const float* __restrict__ p,
@@ -318,32 +233,6 @@ __global__ void k_bf16_to_f32(const __nv_bfloat16* __restrict__ a, float* __rest
   if (i < n) b[i] = __bfloat162float(a[i]);
 }
 
-template <typename TS>
-cudaError_t mg_smooth_t(Dims3 d, float h, const TS* b, const uint32_t* f, TS* p, int color,
-                        float omega, int bc_mode, cudaStream_t st) {
-  Lvl l{d.nx, d.ny, d.nz};
-  k_mg_smooth<TS><<<grid_for((d.nx + 1) / 2, d.ny, d.nz), dim3(BX, BY, BZ), 0, st>>>(
-      l, h * h, b, f, p, color, omega, bc_mode);
-  return cudaGetLastError();
-}
-
-template <typename TS>
-cudaError_t mg_restrict_t(Dims3 df, float hf, const TS* pf, const TS* bf, const uint32_t* ff,
-                          Dims3 dc, TS* bc, TS* pc, uint32_t* fc, int bc_mode, cudaStream_t st) {
-  k_mg_restrict<TS><<<grid_for(dc.nx, dc.ny, dc.nz), dim3(BX, BY, BZ), 0, st>>>(
-      Lvl{df.nx, df.ny, df.nz}, hf * hf, pf, bf, ff, Lvl{dc.nx, dc.ny, dc.nz}, bc, pc, fc,
-      bc_mode);
-  return cudaGetLastError();
-}
-
-template <typename TS>
-cudaError_t mg_prolong_t(Dims3 df, const TS* pc, const uint32_t* ff, TS* pf, Dims3 dc,
-                         const uint32_t* fc, cudaStream_t st) {
-  k_mg_prolong<TS><<<grid_for(df.nx, df.ny, df.nz), dim3(BX, BY, BZ), 0, st>>>(
-      Lvl{df.nx, df.ny, df.nz}, pc, ff, pf, Lvl{dc.nx, dc.ny, dc.nz}, fc);
-  return cudaGetLastError();
-}
-
 // Cluster size for a level: the largest of 16 / 8 whose slabs keep every
 // CTA within COARSE_K cells per thread and the level fits the cluster.
 int coarse_cluster_size(Dims3 d) {
@@ -412,22 +301,6 @@ cudaError_t mg_coarse_t(Dims3 d, float h, const TS* b, const uint32_t* f, TS* p,
 }  // namespace
 
 bool mg_coarse_fits(Dims3 d) { return coarse_cluster_size(d) != 0; }
-
-cudaError_t launch_mg_smooth(Dims3 d, float h, const float* b, const uint32_t* f, float* p,
-                             int color, float omega, int bc_mode, cudaStream_t st) {
-  return mg_smooth_t<float>(d, h, b, f, p, color, omega, bc_mode, st);
-}
-
-cudaError_t launch_mg_restrict(Dims3 df, float hf, const float* pf, const float* bf,
-                               const uint32_t* ff, Dims3 dc, float* bc, float* pc, uint32_t* fc,
-                               int bc_mode, cudaStream_t st) {
-  return mg_restrict_t<float>(df, hf, pf, bf, ff, dc, bc, pc, fc, bc_mode, st);
-}
-
-cudaError_t launch_mg_prolong(Dims3 df, const float* pc, const uint32_t* ff, float* pf, Dims3 dc,
-                              const uint32_t* fc, cudaStream_t st) {
-  return mg_prolong_t<float>(df, pc, ff, pf, dc, fc, st);
-}
 
 cudaError_t launch_mg_resid(Dims3 d, float h, const float* p, const float* b, const uint32_t* f,
                             int bc_mode, float* stats, cudaStream_t st) {

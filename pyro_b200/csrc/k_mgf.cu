@@ -556,6 +556,12 @@ cudaError_t launch_mg_restrict_m(Dims3 df, float h, const float* pf, const float
                                  cudaStream_t st) {
   return restrict_t<float>(df, h, pf, bf, mf, dc, bc, pc, bc_mode, st);
 }
+cudaError_t launch_mg_restrict_m_bf16(Dims3 df, float h, const void* pf, const void* bf,
+                                      const uint8_t* mf, Dims3 dc, void* bc, void* pc,
+                                      int bc_mode, cudaStream_t st) {
+  using T = __nv_bfloat16;
+  return restrict_t<T>(df, h, (const T*)pf, (const T*)bf, mf, dc, (T*)bc, (T*)pc, bc_mode, st);
+}
 template <typename TS>
 cudaError_t restrict_sym_t(Dims3 df, float h, const TS* pf, const TS* bf, const uint8_t* mf,
                            TS* rt, Dims3 dc, const uint8_t* mc, TS* bc, TS* pc, int bc_mode,

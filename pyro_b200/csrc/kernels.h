@@ -93,13 +93,6 @@ cudaError_t launch_project(const PyroParams* P, Dims3 d, float* u, float* v, flo
 
 // Multigrid level kernels (src/shaders/mg.wgsl).  bc_mode 0 = reference
 // boundaries, 1 = Dirichlet on the top face only.
-cudaError_t launch_mg_smooth(Dims3 d, float h, const float* b, const uint32_t* f, float* p,
-                             int color, float omega, int bc_mode, cudaStream_t st);
-cudaError_t launch_mg_restrict(Dims3 df, float hf, const float* pf, const float* bf,
-                               const uint32_t* ff, Dims3 dc, float* bc, float* pc, uint32_t* fc,
-                               int bc_mode, cudaStream_t st);
-cudaError_t launch_mg_prolong(Dims3 df, const float* pc, const uint32_t* ff, float* pf, Dims3 dc,
-                              const uint32_t* fc, cudaStream_t st);
 cudaError_t launch_mg_resid(Dims3 d, float h, const float* p, const float* b, const uint32_t* f,
                             int bc_mode, float* stats, cudaStream_t st);
 // Whole coarsest-level solve in one CTA (shared memory); returns
@@ -131,6 +124,9 @@ cudaError_t launch_mg_pass_bf16(Dims3 d, float h, const void* b, const uint8_t* 
 cudaError_t launch_mg_restrict_m(Dims3 df, float h, const float* pf, const float* bf,
                                  const uint8_t* mf, Dims3 dc, float* bc, float* pc, int bc_mode,
                                  cudaStream_t st);
+cudaError_t launch_mg_restrict_m_bf16(Dims3 df, float h, const void* pf, const void* bf,
+                                      const uint8_t* mf, Dims3 dc, void* bc, void* pc,
+                                      int bc_mode, cudaStream_t st);
 
 // Symmetric V-cycle pieces for the MGPCG preconditioner: residual divided
 // by the fluid prolongation weight into `rt`, then the transpose (P^T / 8)

@@ -37,6 +37,43 @@ void DevBuf::release() {
   bytes = 0;
 }
 
+MgTimer::~MgTimer() {
+  for (auto e : ev) cudaEventDestroy(e);
+}
+
+cudaError_t MgTimer::start(cudaStream_t st) {
+  for (auto e : ev) cudaEventDestroy(e);
+  ev.clear();
+  cls.clear();
+  return mark(-1, st);
+}
+
+cudaError_t MgTimer::mark(int c, cudaStream_t st) {
+  cudaEvent_t e;
+  cudaError_t r = cudaEventCreate(&e);
+  if (r != cudaSuccess) return r;
+  ev.push_back(e);
+  cls.push_back(c);
+  return cudaEventRecord(e, st);
+}
+
+cudaError_t MgTimer::read(float* ms, int* launches) const {
+  for (int c = 0; c < MG_CLASSES; c++) {
+    ms[c] = 0.0f;
+    launches[c] = 0;
+  }
+  for (size_t i = 1; i < ev.size(); i++) {
+    float t = 0.0f;
+    cudaError_t r = cudaEventElapsedTime(&t, ev[i - 1], ev[i]);
+    if (r != cudaSuccess) return r;
+    if (cls[i] >= 0 && cls[i] < MG_CLASSES) {
+      ms[cls[i]] += t;
+      launches[cls[i]] += 1;
+    }
+  }
+  return cudaSuccess;
+}
+
 std::vector<Dims3> mg_level_dims(Dims3 d, int max_levels) {
   std::vector<Dims3> v;
   for (int l = 0; l < max_levels; l++) {
@@ -47,9 +84,18 @@ std::vector<Dims3> mg_level_dims(Dims3 d, int max_levels) {
   return v;
 }
 
-int Multigrid::init(Dims3 d0, float h0, int bc) {
+std::vector<Dims3> mg_level_dims_deep(Dims3 d, size_t direct_max) {
+  std::vector<Dims3> v{d};
+  while (d.cells() > direct_max && std::min(std::min(d.nx, d.ny), d.nz) >= 4) {
+    d = Dims3{(d.nx + 1) / 2, (d.ny + 1) / 2, (d.nz + 1) / 2};
+    v.push_back(d);
+  }
+  return v;
+}
+
+int Multigrid::init(Dims3 d0, float h0, int bc, size_t direct_max) {
   bc_mode = bc;
-  dims = mg_level_dims(d0, 4);
+  dims = direct_max ? mg_level_dims_deep(d0, direct_max) : mg_level_dims(d0, 4);
   size_t L = dims.size();
   h.resize(L);
   phi.assign(L, nullptr);
@@ -93,7 +139,8 @@ cudaError_t Multigrid::smooth(int l, int iters, bool coarse, cudaStream_t st) {
     return launch_mg_coarse(dims[l], h[l], b[l], f[l], phi[l], iters, om, bc_mode, st);
   for (int it = 0; it < iters; it++)
     for (int c = 0; c < 2; c++) {
-      cudaError_t e = launch_mg_smooth(dims[l], h[l], b[l], f[l], phi[l], c, om, bc_mode, st);
+      cudaError_t e = launch_mg_pass(dims[l], h[l], b[l], meta[l].as<uint8_t>(), phi[l], c, om,
+                                     bc_mode, st);
       if (e != cudaSuccess) return e;
     }
   return cudaSuccess;
@@ -114,12 +161,17 @@ cudaError_t Multigrid::prepare(cudaStream_t st) {
 cudaError_t Multigrid::vcycles(int cycles, cudaStream_t st) {
   int nl = (int)dims.size();
   cudaError_t e;
+  // with a timer, an event after every launch credits it to its class
+  auto tick = [&](int cls) -> cudaError_t { return timer ? timer->mark(cls, st) : cudaSuccess; };
+  if (timer && (e = timer->start(st)) != cudaSuccess) return e;
   if ((e = prepare(st)) != cudaSuccess) return e;
+  if ((e = tick(MG_PREPARE)) != cudaSuccess) return e;
   auto M = [&](int l) { return meta[l].as<uint8_t>(); };
   auto sm = [&](int l) -> cudaError_t {  // two red-black iterations, omega 1
     for (int it = 0; it < 2; it++)
       for (int c = 0; c < 2; c++) {
         cudaError_t e2 = launch_mg_pass(dims[l], h[l], b[l], M(l), phi[l], c, 1.0f, bc_mode, st);
+        if (e2 == cudaSuccess) e2 = tick(l == 0 ? MG_PASS_L0 : MG_PASS_MID);
         if (e2 != cudaSuccess) return e2;
       }
     return cudaSuccess;
@@ -130,12 +182,15 @@ cudaError_t Multigrid::vcycles(int cycles, cudaStream_t st) {
       if ((e = launch_mg_restrict_m(dims[l], h[l], phi[l], b[l], M(l), dims[l + 1], b[l + 1],
                                     phi[l + 1], bc_mode, st)) != cudaSuccess)
         return e;
+      if ((e = tick(l == 0 ? MG_RESTRICT_L0 : MG_RESTRICT_MID)) != cudaSuccess) return e;
     }
     if ((e = smooth(nl - 1, 80, true, st)) != cudaSuccess) return e;
+    if ((e = tick(MG_COARSE)) != cudaSuccess) return e;
     for (int l = nl - 2; l >= 0; l--) {
       if ((e = launch_mg_prolong_m(dims[l], phi[l + 1], M(l), phi[l], dims[l + 1], M(l + 1), st)) !=
           cudaSuccess)
         return e;
+      if ((e = tick(l == 0 ? MG_PROLONG_L0 : MG_PROLONG_MID)) != cudaSuccess) return e;
       if ((e = sm(l)) != cudaSuccess) return e;
     }
   }
@@ -185,7 +240,9 @@ cudaError_t Multigrid::vcycle_sym(cudaStream_t st, DevBuf* bphi, DevBuf* bphi2, 
     if (e != cudaSuccess) return e;
   }
   int lc = nl - 1;
-  if (coarse_one_cta) {
+  if (direct) {
+    if ((e = direct->apply(st, B(lc), P(lc), lo)) != cudaSuccess) return e;
+  } else if (coarse_one_cta) {
     e = lo ? launch_mg_coarse_sym_bf16(dims[lc], h[lc], B(lc), f[lc], P(lc), 80, 1.6f, bc_mode, st)
            : launch_mg_coarse_sym(dims[lc], h[lc], (const float*)B(lc), f[lc], (float*)P(lc), 80,
                                   1.6f, bc_mode, st);

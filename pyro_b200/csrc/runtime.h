@@ -47,9 +47,50 @@ struct DevBuf {
 };
 
 // Multigrid hierarchy (src/sim.rs:142-168): <= 4 levels, stop after the
-// first level whose smallest dimension is < 16, halve with ceil, h doubles.
-// Level 0 arrays are bound from outside; the coarse levels are owned.
+// Launch classes of the V-cycle, for per-launch timing
+// (pyro_sim_profile_pressure).
+enum MgClass {
+  MG_PREPARE = 0,  // coarse flags and neighbour masks of every level
+  MG_PASS_L0,      // one colour pass of the smoother on level 0
+  MG_RESTRICT_L0,  // restriction from level 0
+  MG_PROLONG_L0,   // prolongation onto level 0
+  MG_PASS_MID,     // a colour pass on a level between 0 and the coarsest
+  MG_RESTRICT_MID,
+  MG_PROLONG_MID,
+  MG_COARSE,       // the coarsest-level solve
+  MG_CLASSES
+};
+
+// Per-launch timer of the V-cycle: start() records an event, then mark()
+// after each launch records the next one and credits the interval to its
+// class.  Read after the stream has finished.
+struct MgTimer {
+  std::vector<cudaEvent_t> ev;
+  std::vector<int> cls;
+  ~MgTimer();
+  cudaError_t start(cudaStream_t st);
+  cudaError_t mark(int c, cudaStream_t st);
+  // per-class totals (ms) and launch counts
+  cudaError_t read(float* ms, int* launches) const;
+};
+
+// The direct solve of the coarsest level of the CG preconditioner
+// (solver.cu): phi = A^-1 b with b and phi in the level's storage (FP32 or
+// BF16).
+struct CoarseDirect {
+  virtual ~CoarseDirect() = default;
+  virtual cudaError_t apply(cudaStream_t st, const void* b, void* phi, bool bf16) = 0;
+};
+
+// Multigrid hierarchy.  Reference rule (src/sim.rs:142-168): <= 4 levels,
+// stop after the first level whose smallest dimension is < 16, halve with
+// ceil, h doubles.  Deep rule (the CG preconditioner): halve until the
+// coarsest level has at most `direct_max` cells, which are then solved
+// directly.  Level 0 arrays are bound from outside; the coarse levels are
+// owned.
 struct Multigrid {
+  MgTimer* timer = nullptr;  // set only while pyro_sim_profile_pressure runs
+  CoarseDirect* direct = nullptr;  // coarsest solve of vcycle_sym, when set
   int bc_mode = 0;
   std::vector<Dims3> dims;
   std::vector<float> h;
@@ -61,7 +102,8 @@ struct Multigrid {
   bool coarse_one_cta = false;
   float* stats = nullptr;  // device, for mg_resid
 
-  int init(Dims3 d0, float h0, int bc);
+  // direct_max == 0: the reference rule; else the deep rule.
+  int init(Dims3 d0, float h0, int bc, size_t direct_max = 0);
   void bind_level0(float* phi0, const float* b0, const uint32_t* f0) {
     phi[0] = phi0;
     b[0] = const_cast<float*>(b0);
@@ -91,5 +133,8 @@ struct Multigrid {
 
 // Level dims of the reference rule (shared with the C ABI).
 std::vector<Dims3> mg_level_dims(Dims3 d0, int max_levels);
+// Level dims of the deep rule: halve (ceil) until the level has at most
+// direct_max cells or a dimension would drop below 2.
+std::vector<Dims3> mg_level_dims_deep(Dims3 d0, size_t direct_max);
 
 }  // namespace pyro

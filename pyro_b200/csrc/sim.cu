@@ -454,6 +454,38 @@ int pyro_sim_profile_step(PyroSim* S, float dt, float time, float ign_on, int wa
   return PYRO_OK;
 }
 
+int pyro_sim_profile_pressure(PyroSim* S, float* ms_out, int* launches_out, int n) {
+  clear_error();
+  PYRO_REQUIRE(S && ms_out && launches_out && n >= 0,
+               "pyro_sim_profile_pressure: null argument");
+  // the solve runs on a copy of the warm start, which is put back after
+  const size_t bytes = S->d.cells() * 4;
+  DevBuf keep;
+  int rc = keep.alloc(bytes);
+  if (rc != PYRO_OK) return rc;
+  cudaStream_t st = S->stream;
+  PYRO_CU(cudaMemcpyAsync(keep.p, S->phi0.p, bytes, cudaMemcpyDeviceToDevice, st));
+  MgTimer timer;
+  S->mg.timer = &timer;
+  cudaError_t e = S->mg.vcycles((int)S->cycles, st);
+  S->mg.timer = nullptr;
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(S->phi0.p, keep.p, bytes, cudaMemcpyDeviceToDevice, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  float ms[MG_CLASSES];
+  int cnt[MG_CLASSES];
+  if (e == cudaSuccess) e = timer.read(ms, cnt);
+  if (e != cudaSuccess) {
+    set_error(std::string("pyro_sim_profile_pressure: ") + cudaGetErrorString(e));
+    return PYRO_E_CUDA;
+  }
+  for (int i = 0; i < n && i < MG_CLASSES; i++) {
+    ms_out[i] = ms[i];
+    launches_out[i] = cnt[i];
+  }
+  return PYRO_OK;
+}
+
 int pyro_sim_read_stats(PyroSim* S, float* out, size_t n) {
   clear_error();
   PYRO_REQUIRE(S && out, "pyro_sim_read_stats: null argument");

@@ -8,9 +8,12 @@
 //   beta  = <z_new, r_new - r_old> / <z_old, r_old> = -<z_new, q> / <p,q>
 // (Polak-Ribiere form, valid for the non-symmetric V-cycle), p = z + beta p.
 // Vectors are FP32; every dot product and norm is accumulated in FP64.
+#include <cuda_bf16.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <new>
 
 #include "common.cuh"
 #include "net.h"
@@ -19,6 +22,13 @@
 namespace pyro {
 
 namespace {
+
+__device__ __forceinline__ float cvt_load(const float* p) { return *p; }
+__device__ __forceinline__ float cvt_load(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+__device__ __forceinline__ void cvt_store(float* p, float v) { *p = v; }
+__device__ __forceinline__ void cvt_store(__nv_bfloat16* p, float v) {
+  *p = __float2bfloat16_rn(v);
+}
 
 constexpr int BX = 32, BY = 4, BZ = 2;
 inline dim3 grid_for(Dims3 d) {
@@ -328,6 +338,162 @@ __global__ void __launch_bounds__(256) k_reach_final(L3 d, uint32_t* __restrict_
 
 }  // namespace
 
+// ---- coarsest level of the preconditioner: FP64 direct solve --------------
+// The preconditioner's hierarchy halves the grid until its coarsest level
+// has at most DIRECT_MAX cells (Multigrid deep rule).  That level is solved
+// exactly: M = -A (symmetric positive definite on the fluid cells, the
+// identity on solid ones) is assembled densely in FP64 and inverted in
+// place by Gauss-Jordan elimination without pivoting (stable for SPD
+// matrices), one pivot per step: with p = m_kk,
+//   m_kk <- 1/p,  m_kj <- m_kj/p,  m_ik <- -m_ik/p,  m_ij <- m_ij - m_ik m_kj/p.
+// The inverse is kept until the level's flags change; each application is
+// one FP64 matrix-vector product, phi = -M^-1 b.  A pivot that is not
+// positive (a fluid region with no Dirichlet face, which the CG modes'
+// reachability flags exclude) is replaced by the cell's h^-2, as if the cell
+// touched a Dirichlet face, and counted.
+namespace {
+
+__global__ void __launch_bounds__(256) k_dc_assemble(L3 d, double ih2,
+                                                     const uint32_t* __restrict__ f, int bc_mode,
+                                                     double* __restrict__ M) {
+  const int n = d.nx * d.ny * d.nz;
+  const int i = blockIdx.x * 256 + threadIdx.x;
+  if (i >= n) return;
+  const int x = i % d.nx, y = (i / d.nx) % d.ny, z = i / (d.nx * d.ny);
+  double* row = M + (size_t)i * n;
+  if (f[i] == 1u) {
+    row[i] = 1.0;
+    return;
+  }
+  double cnt = 0.0;
+#pragma unroll
+  for (int k = 0; k < 6; k++) {
+    int a = x + (k == 0) - (k == 1), b = y + (k == 2) - (k == 3), c = z + (k == 4) - (k == 5);
+    if (b < 0) continue;
+    if (!d.inb(a, b, c)) {
+      if (bc_mode == 0 || b >= d.ny) cnt += 1.0;
+      continue;
+    }
+    const int j = d.idx(a, b, c);
+    if (f[j] == 1u) continue;
+    row[j] = -ih2;
+    cnt += 1.0;
+  }
+  row[i] = cnt * ih2;
+}
+
+// The pivot row and column of step k (the matrix as the previous step left
+// it), with the pivot itself checked.
+__global__ void k_dc_pivot(double* __restrict__ M, int n, int k, double ih2,
+                           double* __restrict__ col, double* __restrict__ row,
+                           int* __restrict__ bad) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    col[t] = M[(size_t)t * n + k];
+    double r = M[(size_t)k * n + t];
+    if (t == k && !(r > 1e-9 * ih2)) {
+      r = ih2;
+      atomicAdd(bad, 1);
+    }
+    row[t] = r;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_dc_eliminate(double* __restrict__ M, int n, int k,
+                                                      const double* __restrict__ col,
+                                                      const double* __restrict__ row) {
+  const int j = blockIdx.x * 32 + threadIdx.x;
+  const int i = blockIdx.y * 8 + threadIdx.y;
+  if (i >= n || j >= n) return;
+  const double ip = 1.0 / row[k];
+  double* m = M + (size_t)i * n + j;
+  if (i == k) *m = (j == k) ? ip : row[j] * ip;
+  else if (j == k) *m = -col[i] * ip;
+  else *m = *m - col[i] * row[j] * ip;
+}
+
+// phi_i = -(M^-1 b)_i on fluid cells, 0 on solid ones: one warp per row,
+// b staged in shared memory as FP64 (solid entries 0).
+template <typename TS>
+__global__ void __launch_bounds__(256) k_dc_apply(const double* __restrict__ Minv, int n,
+                                                  const TS* __restrict__ b,
+                                                  const uint32_t* __restrict__ f,
+                                                  TS* __restrict__ phi) {
+  extern __shared__ double sb[];
+  pdl_trigger();
+  pdl_wait();
+  for (int t = threadIdx.x; t < n; t += blockDim.x)
+    sb[t] = f[t] == 1u ? 0.0 : (double)cvt_load(b + t);
+  __syncthreads();
+  const int i = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (i >= n) return;
+  const double* r = Minv + (size_t)i * n;
+  double acc = 0.0;
+  for (int j = lane; j < n; j += 32) acc += r[j] * sb[j];
+  acc = warp_sum_d(acc);
+  if (lane == 0) cvt_store(phi + i, f[i] == 1u ? 0.0f : (float)(-acc));
+}
+
+}  // namespace
+
+struct DirectSolve : CoarseDirect {
+  Dims3 dc{};
+  float h = 1.0f;
+  int bc_mode = 0;
+  const uint32_t* f = nullptr;  // the level's flags (device, owned by the hierarchy)
+  DevBuf minv, piv, bad;
+  std::vector<uint32_t> flags_host, flags_now;
+  bool valid = false;
+  int singular = 0;  // pivots replaced at the last factorisation
+
+  size_t n() const { return dc.cells(); }
+  // Factor when the level's flags differ from those of the last
+  // factorisation (they are compared on the host after a copy).
+  int refresh(cudaStream_t st) {
+    const size_t nn = n();
+    if (!minv.p) {
+      int rc;
+      if ((rc = minv.alloc(nn * nn * 8)) != PYRO_OK || (rc = piv.alloc(nn * 16)) != PYRO_OK ||
+          (rc = bad.alloc(16)) != PYRO_OK)
+        return rc;
+    }
+    flags_now.resize(nn);
+    PYRO_CU(cudaMemcpyAsync(flags_now.data(), f, nn * 4, cudaMemcpyDeviceToHost, st));
+    PYRO_CU(cudaStreamSynchronize(st));
+    if (valid && flags_now == flags_host) return PYRO_OK;
+    const double ih2 = 1.0 / ((double)h * h);
+    L3 l{dc.nx, dc.ny, dc.nz};
+    PYRO_CU(cudaMemsetAsync(minv.p, 0, nn * nn * 8, st));
+    PYRO_CU(cudaMemsetAsync(bad.p, 0, 4, st));
+    k_dc_assemble<<<(unsigned)((nn + 255) / 256), 256, 0, st>>>(l, ih2, f, bc_mode,
+                                                                minv.as<double>());
+    PYRO_CU(cudaGetLastError());
+    double* col = piv.as<double>();
+    double* row = col + nn;
+    dim3 eg((unsigned)((nn + 31) / 32), (unsigned)((nn + 7) / 8));
+    for (size_t k = 0; k < nn; k++) {
+      k_dc_pivot<<<(unsigned)((nn + 255) / 256), 256, 0, st>>>(minv.as<double>(), (int)nn, (int)k,
+                                                                ih2, col, row, bad.as<int>());
+      k_dc_eliminate<<<eg, dim3(32, 8), 0, st>>>(minv.as<double>(), (int)nn, (int)k, col, row);
+    }
+    PYRO_CU(cudaGetLastError());
+    PYRO_CU(cudaMemcpyAsync(&singular, bad.p, 4, cudaMemcpyDeviceToHost, st));
+    PYRO_CU(cudaStreamSynchronize(st));
+    flags_host = flags_now;
+    valid = true;
+    return PYRO_OK;
+  }
+  cudaError_t apply(cudaStream_t st, const void* b, void* phi, bool bf16) override {
+    const size_t nn = n();
+    const unsigned blocks = (unsigned)((nn + 7) / 8);
+    if (bf16)
+      return launch_pdl(k_dc_apply<__nv_bfloat16>, dim3(blocks), dim3(256), nn * 8, st,
+                        (const double*)minv.as<double>(), (int)nn, (const __nv_bfloat16*)b, f,
+                        (__nv_bfloat16*)phi);
+    return launch_pdl(k_dc_apply<float>, dim3(blocks), dim3(256), nn * 8, st,
+                      (const double*)minv.as<double>(), (int)nn, (const float*)b, f, (float*)phi);
+  }
+};
+
 int Solver::update_reach(cudaStream_t st) {
   const uint32_t* f0 = mg->f[0];
   L3 l{d.nx, d.ny, d.nz};
@@ -391,10 +557,30 @@ int Solver::init(Multigrid* m) {
     set_error("solver: cudaEventCreate failed");
     return PYRO_E_CUDA;
   }
+  // the preconditioner's hierarchy: down to <= DIRECT_MAX cells, solved
+  // directly when the coarsest level got there
+  if ((rc = pc.init(d, m->h[0], m->bc_mode, DIRECT_MAX)) != PYRO_OK) return rc;
+  const size_t L = pc.levels();
+  bphi.resize(L);
+  bphi2.resize(L);
+  bb.resize(L);
+  if (pc.dims.back().cells() <= DIRECT_MAX) {
+    direct = new (std::nothrow) DirectSolve();
+    if (!direct) {
+      set_error("solver: host allocation failed");
+      return PYRO_E_NOMEM;
+    }
+    direct->dc = pc.dims.back();
+    direct->h = pc.h.back();
+    direct->bc_mode = pc.bc_mode;
+    direct->f = pc.f.back();
+    pc.direct = direct;
+  }
   return PYRO_OK;
 }
 
 Solver::~Solver() {
+  delete direct;
   if (host_sc) cudaFreeHost(host_sc);
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
@@ -404,7 +590,9 @@ Solver::~Solver() {
 
 size_t Solver::device_bytes() const {
   size_t s = r.bytes + z.bytes + p.bytes + q.bytes + sc.bytes + fa.bytes + reach_dev.bytes;
-  for (int l = 0; l < 4; l++) s += bphi[l].bytes + bphi2[l].bytes + bb[l].bytes;
+  for (size_t l = 0; l < bphi.size(); l++) s += bphi[l].bytes + bphi2[l].bytes + bb[l].bytes;
+  s += pc.device_bytes();
+  if (direct) s += direct->minv.bytes + direct->piv.bytes + direct->bad.bytes;
   return s;
 }
 
@@ -429,14 +617,9 @@ cudaError_t Solver::precond(cudaStream_t st, bool bf16, bool prep) {
   // writes every cell of z and does not read it).
   cudaError_t e = cudaSuccess;
   if (!bf16 && (e = cudaMemsetAsync(z.p, 0, d.cells() * 4, st)) != cudaSuccess) return e;
-  float* save_phi = mg->phi[0];
-  float* save_b = mg->b[0];
-  const uint32_t* save_f = mg->f[0];
-  mg->bind_level0(z.as<float>(), r.as<float>(), save_f);
-  e = bf16 ? mg->vcycle_sym(st, bphi, bphi2, bb, prep)
-           : mg->vcycle_sym(st, nullptr, nullptr, nullptr, prep);
-  mg->bind_level0(save_phi, save_b, save_f);
-  return e;
+  pc.bind_level0(z.as<float>(), r.as<float>(), fa.as<uint32_t>());
+  return bf16 ? pc.vcycle_sym(st, bphi.data(), bphi2.data(), bb.data(), prep)
+              : pc.vcycle_sym(st, nullptr, nullptr, nullptr, prep);
 }
 
 int Solver::learned_stage(cudaStream_t st, float* phi, double* rr, PyroSolveInfo* info) {
@@ -568,11 +751,17 @@ int Solver::solve(cudaStream_t st, float* phi, const float* b, int mode, float t
     // CG with residual replacement: when the recursively updated residual
     // meets the tolerance the true residual is recomputed; if it does not
     // meet it, CG restarts from the true residual.
+    // the preconditioner's level flags and masks from the reachable-fluid
+    // flags, and its coarsest-level inverse when that level's flags changed
+    pc.bind_level0(z.as<float>(), r.as<float>(), fa.as<uint32_t>());
+    PYRO_CU(pc.prepare(st));
+    if (direct) {
+      direct->f = pc.f.back();  // level 0's flags when the grid is the coarsest level
+      if ((rc = direct->refresh(st)) != PYRO_OK) return rc;
+    }
     int restarts = 0;
-    bool prepared = false;  // the level masks of the reachable-fluid flags
     while (rel > tol && iters < max_iters && restarts < 8) {
-      PYRO_CU(precond(st, bf16, !prepared));
-      prepared = true;
+      PYRO_CU(precond(st, bf16, false));
       launch_pdl(k_dots, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), f0, z.as<float>(), r.as<float>(),
                                                       nullptr, S);
       PYRO_CU(cudaGetLastError());

@@ -8,14 +8,22 @@
 
 namespace pyro {
 
+struct DirectSolve;
+
+// Cells of the preconditioner's coarsest level, which is solved directly in
+// FP64 (a dense inverse of DIRECT_MAX^2 doubles at most: 75 MB).
+constexpr size_t DIRECT_MAX = 3072;
+
 struct Solver {
-  Multigrid* mg = nullptr;
+  Multigrid* mg = nullptr;  // the reference hierarchy (fixed V-cycle modes)
+  Multigrid pc;             // the preconditioner's deep hierarchy (CG modes)
+  DirectSolve* direct = nullptr;  // its coarsest-level solve (owned)
   Dims3 d{};
   DevBuf r, z, p, q;        // level-0 work vectors (FP32)
   DevBuf sc;                // FP64 device scalars
   double* host_sc = nullptr;  // pinned mirror
   // BF16 hierarchy for the low-precision preconditioner
-  DevBuf bphi[4], bphi2[4], bb[4];
+  std::vector<DevBuf> bphi, bphi2, bb;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evl0 = nullptr, evl1 = nullptr;
   PyroNet* net = nullptr;   // learned stage of PYRO_SOLVER_MGPCG_LEARNED (not owned)
   // flags of the CG modes: fluid cells without a fluid path to a Dirichlet

@@ -1,6 +1,8 @@
 """Generate golden vectors by executing the reference's own WGSL kernels.
 
-    python tests/golden/make_golden.py [--ref /root/reference] [--only name,...]
+    python tests/golden/make_golden.py --ref <reference checkout> [--only name,...]
+
+(or set PYRO_REFERENCE to the checkout instead of passing --ref)
 
 For each simulation kernel (and the renderer's input pack, render.wgsl) the
 script assembles the shader source exactly as
@@ -495,9 +497,12 @@ def gen_mg(ref, only):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("PYRO_REFERENCE"),
+                    help="the reference checkout (default: $PYRO_REFERENCE)")
     ap.add_argument("--only", default=None)
     a = ap.parse_args()
+    if not a.ref:
+        ap.error("give the reference checkout with --ref or PYRO_REFERENCE")
     only = set(a.only.split(",")) if a.only else None
     ref = Ref(a.ref)
     out = {}

@@ -65,6 +65,13 @@ def test_invalid_arguments_fail_before_the_device(lib):
         _abi.PYRO_E_INVALID
     assert lib.pyro_k_mg_restrict(16, 16, 16, 0.1, buf, buf, buf, 9, 8, 8, buf, buf, buf,
                                   None) == _abi.PYRO_E_INVALID
+    assert lib.pyro_k_mg_pass(16, 16, 16, 0.1, buf, buf, buf, 0, 1.0, 0, 2, None) == \
+        _abi.PYRO_E_INVALID
+    assert b"storage" in lib.pyro_last_error()
+    assert lib.pyro_k_mg_pass(16, 16, 16, 0.1, buf, buf, buf, 0, 1.0, 3, 0, None) == \
+        _abi.PYRO_E_INVALID
+    assert lib.pyro_k_mg_prolong_m(16, 16, 16, buf, buf, buf, 8, 9, 8, buf, 0, None) == \
+        _abi.PYRO_E_INVALID
     assert lib.pyro_poisson_create(4, 4, 4, 0.1, 7, ctypes.byref(h)) == _abi.PYRO_E_INVALID
     assert lib.pyro_sim_destroy(None) == _abi.PYRO_OK
 

@@ -15,6 +15,7 @@ import pytest
 import oracle
 from fields import close, face_valid_mask, params_for, random_state
 from gpu_util import dev, host, params_dev, ptr, require_cuda, stats_dev
+from pyro_b200 import _abi
 
 pytestmark = pytest.mark.gpu
 
@@ -200,6 +201,72 @@ def test_mg_kernels(lib, nx, ny, nz, seed, h):
     assert lib.pyro_k_mg_resid(nx, ny, nz, h, ptr(pd), ptr(bd), ptr(fd), ptr(sd), None) == 0
     g = host(sd)
     assert abs(g[10] - r2) <= 1e-4 * r2 and abs(g[11] - b2) <= 1e-4 * b2
+
+
+def _bf16_bits(x):
+    """float32 -> BF16 bit patterns, round to nearest even (as
+    __float2bfloat16_rn for finite values)."""
+    u = np.ascontiguousarray(x, np.float32).view(np.uint32).astype(np.uint64)
+    r = (u + 0x7FFF + ((u >> 16) & 1)) >> 16
+    return r.astype(np.uint16)
+
+
+def _bf16_val(bits):
+    return (bits.astype(np.uint32) << 16).view(np.float32)
+
+
+# the shapes the V-cycle meets: rows of a multiple of 4 cells (the
+# four-cells-per-thread pass, even row pairs in the transfers) and odd rows
+MASK_CASES = MG_CASES + [(64, 40, 24, 3, 0.04), (20, 40, 20, 4, 0.16), (10, 20, 10, 5, 0.32)]
+
+
+@pytest.mark.parametrize("nx,ny,nz,seed,h", MASK_CASES)
+@pytest.mark.parametrize("bc_mode", [0, 1])
+@pytest.mark.parametrize("storage", [_abi.MG_F32, _abi.MG_BF16])
+def test_mg_mask_kernels_as_the_vcycle_runs_them(lib, nx, ny, nz, seed, h, bc_mode, storage):
+    """The smoother pass, restriction and prolongation on the level's
+    neighbour masks, both boundary modes, FP32 or BF16 storage of phi and b,
+    against the oracle's per-flag kernels (mg.wgsl).  BF16: the inputs are
+    BF16 values, the arithmetic is FP32 on both sides and the oracle's
+    result is rounded to BF16, so the bits must agree exactly."""
+    rng = np.random.default_rng(100 + seed)
+    f = (rng.random((nz, ny, nx)) < 0.2).astype(np.uint32)
+    b = rng.normal(0, 1, (nz, ny, nx)).astype(np.float32)
+    p = rng.normal(0, 1, (nz, ny, nx)).astype(np.float32)
+    lo = storage == _abi.MG_BF16
+    if lo:
+        b, p = _bf16_val(_bf16_bits(b)), _bf16_val(_bf16_bits(p))
+    enc = (lambda a: _bf16_bits(a)) if lo else (lambda a: np.ascontiguousarray(a, np.float32))
+    fd = dev(f)
+    meta = dev(np.zeros((nz, ny, nx), np.uint8))
+    assert lib.pyro_k_mg_meta(nx, ny, nz, ptr(fd), ptr(meta), None) == 0
+    bd = dev(enc(b))
+    for color, om in [(0, 1.0), (1, 1.0), (0, 1.6), (1, 1.6)]:
+        e = oracle.mg_smooth((nx, ny, nz), h, b, f, p, color, om, bc_mode=bc_mode)
+        pd = dev(enc(p))
+        assert lib.pyro_k_mg_pass(nx, ny, nz, h, ptr(bd), ptr(meta), ptr(pd), color, om, bc_mode,
+                                  storage, None) == 0, lib.pyro_last_error()
+        assert np.array_equal(host(pd), enc(e)), (color, om)
+    cx, cy, cz = (nx + 1) // 2, (ny + 1) // 2, (nz + 1) // 2
+    bc_o, pc_o, fc_o = oracle.mg_restrict((nx, ny, nz), h, p, b, f, bc_mode=bc_mode)
+    fc = dev(np.ones_like(fc_o))
+    assert lib.pyro_k_mg_flags_down(nx, ny, nz, ptr(fd), cx, cy, cz, ptr(fc), None) == 0
+    assert np.array_equal(host(fc), fc_o)
+    bc, pc = dev(enc(np.ones_like(bc_o))), dev(enc(np.ones_like(pc_o)))
+    assert lib.pyro_k_mg_restrict_m(nx, ny, nz, h, ptr(dev(enc(p))), ptr(bd), ptr(meta), cx, cy,
+                                    cz, ptr(bc), ptr(pc), bc_mode, storage, None) == 0
+    assert np.array_equal(host(bc), enc(bc_o))
+    assert np.array_equal(host(pc), enc(pc_o))
+    mc = dev(np.zeros((cz, cy, cx), np.uint8))
+    assert lib.pyro_k_mg_meta(cx, cy, cz, ptr(fc), ptr(mc), None) == 0
+    pcv = rng.normal(0, 1, bc_o.shape).astype(np.float32)
+    if lo:
+        pcv = _bf16_val(_bf16_bits(pcv))
+    pf_o = oracle.mg_prolong((nx, ny, nz), pcv, f, p, fc_o)
+    pd = dev(enc(p))
+    assert lib.pyro_k_mg_prolong_m(nx, ny, nz, ptr(dev(enc(pcv))), ptr(meta), ptr(pd), cx, cy,
+                                   cz, ptr(mc), storage, None) == 0
+    assert np.array_equal(host(pd), enc(pf_o))
 
 
 COARSE_CASES = MG_CASES + [(8, 20, 8, 3, 0.32), (32, 32, 22, 4, 0.2), (20, 40, 20, 5, 0.16),

@@ -108,6 +108,71 @@ def test_tolerance_solvers_vs_fp64(lib, mode, tol, bc_mode):
     lib.pyro_poisson_destroy(ps)
 
 
+@pytest.mark.parametrize("bc_mode", [0, 1])
+def test_coarsest_direct_solve_is_exact(lib, bc_mode):
+    """A grid of at most 3072 cells is the preconditioner's coarsest level
+    itself, solved by the FP64 inverse: FP32 MGPCG then converges in one or
+    two iterations to the limit of FP32 vectors, and the preconditioner
+    alone (first iterate) is within FP32 rounding of the FP64 oracle."""
+    dims = (12, 16, 12)
+    assert dims[0] * dims[1] * dims[2] <= 3072
+    f, b = _case(*dims, 5, solid=0.0)
+    f[3:6, 0:5, 4:9] = 1  # one solid block on the floor
+    b[f == 1] = 0.0
+    h = 0.1
+    x64, it, rel64 = oracle.poisson_f64(dims, h, b, f, tol=1e-13, bc_mode=bc_mode)
+    ps = _solver(lib, dims, h, f, bc_mode)
+    bd, pd = dev(b), dev(np.zeros_like(b))
+    info = _abi.PyroSolveInfo()
+    rc = lib.pyro_poisson_solve(ps, ptr(bd), ptr(pd), _abi.SOLVER_MGPCG, 1e-6, 20,
+                                ctypes.byref(info))
+    assert rc == 0, lib.pyro_last_error()
+    assert info.iterations <= 2, info.iterations
+    phi = host(pd)
+    fl = f == 0
+    err = np.abs(phi[fl] - x64[fl]).max() / np.abs(x64[fl]).max()
+    assert err <= 1e-5, err
+    lib.pyro_poisson_destroy(ps)
+
+
+@pytest.mark.parametrize("dims", [(160, 320, 160), (150, 365, 150)])
+@pytest.mark.parametrize("mode", [_abi.SOLVER_MGPCG, _abi.SOLVER_MGPCG_BF16])
+def test_mgpcg_at_the_2cm_pool_shapes(lib, dims, mode):
+    """The preconditioner's deep hierarchy with its FP64 coarsest solve at
+    the 2 cm pool's reference rounding and at the exact shape 150x365x150
+    (whose levels do not halve evenly; the reference V-cycle needs the
+    rounding), to 1e-4 against the float64 residual of the oracle."""
+    f, b = _case(*dims, 7)
+    h = 0.02
+    ps = _solver(lib, dims, h, f, 0)
+    bd, pd = dev(b), dev(np.zeros_like(b))
+    info = _abi.PyroSolveInfo()
+    rc = lib.pyro_poisson_solve(ps, ptr(bd), ptr(pd), mode, 1e-4, 100, ctypes.byref(info))
+    assert rc == 0, lib.pyro_last_error()
+    # the residual over the fluid connected to a Dirichlet face (sealed
+    # pockets, if the boxes make any, are not solved)
+    reach = _reachable(f, 0)
+    flags_r = np.where(reach, 0, 1).astype(np.uint32)
+    b_r = np.where(reach, b, 0.0).astype(np.float32)
+    rel = oracle.poisson_relres(dims, h, host(pd), b_r, flags_r, 0)
+    assert info.converged == 1 and rel <= 1.05e-4, (info.iterations, rel)
+    assert abs(rel - info.rel_resid) <= 1e-3 * rel
+    lib.pyro_poisson_destroy(ps)
+
+
+def _reachable(f, bc_mode):
+    """Fluid cells with a 6-connected fluid path to a Dirichlet face (the
+    top, and with bc_mode 0 the four sides)."""
+    from scipy import ndimage
+    lab, n = ndimage.label(f == 0)
+    faces = [lab[:, -1, :]]
+    if bc_mode == 0:
+        faces += [lab[0], lab[-1], lab[:, :, 0], lab[:, :, -1]]
+    keep = np.unique(np.concatenate([a.ravel() for a in faces]))
+    keep = keep[keep > 0]
+    return np.isin(lab, keep)
+
+
 @pytest.mark.parametrize("mode", [_abi.SOLVER_MGPCG, _abi.SOLVER_MGPCG_BF16])
 def test_mgpcg_sealed_pockets(lib, mode):
     """Fluid sealed by solids (no path to a Dirichlet face) makes the system

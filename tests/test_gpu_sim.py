@@ -100,6 +100,33 @@ def test_one_substep_matches_oracle(lib):
     sim.close()
 
 
+def test_one_substep_matches_oracle_at_the_2cm_pool(lib):
+    """The metric's workload: the 2 cm pool at the reference's rounding,
+    160 x 320 x 160 = 8.19 M cells, 4 multigrid levels.  Developed on the GPU
+    for 0.5 s of simulated time at the frame loop's CFL substep, then one
+    substep (graph replay, statistics on) against the oracle from the same
+    state."""
+    sc = _scene("pool_2cm")
+    sim = Sim(sc)
+    assert tuple(sim.dims) == (160, 320, 160)
+    dt = np.float32(1.0 / 180.0)
+    for k in range(90):
+        sim.step(dt, False)
+    sim.sync()
+    assert float(np.abs(sim.read_field(_abi.F_V)).max()) > 0.1  # the plume is moving
+    o = _copy_to_oracle(sim)
+    t = np.float32(sim.time)
+    sim.step(dt, True)
+    o.step(dt, t, 1.0, True)
+    _compare(sim, o, sim.p, 1e-5, 1e-5, "2 cm step")
+    g = sim.read_stats().raw
+    e = o.read_stats()
+    for i in (0, 1, 2, 3, 6, 7, 8, 9, 10, 11):
+        assert abs(g[i] - e[i]) <= 2e-4 * abs(e[i]) + 1e-12, (i, g[i], e[i])
+    o.close()
+    sim.close()
+
+
 def test_several_substeps_stay_within_drift_budget(lib):
     sc, sim = _developed(steps=40)
     o = _copy_to_oracle(sim)
