@@ -1,7 +1,9 @@
 """Benchmark of the fire-simulation step (one substep = Sim::step).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload pool_2cm|pool_small_8cm|pallets_5cm|bonfire_10cm]
+                    [--workload pool_2cm|pool_small_8cm|pallets_5cm|bonfire_10cm|
+                                pool_2cm_exact]
+                    [--solver vcycle|mgpcg|mgpcg_bf16] [--tol T]
 
 Workload (default): the 1 m n-heptane pool fire on a 2 cm grid,
 160 x 320 x 160 = 8.19 M cells (x, y up, z; scene file
@@ -63,7 +65,12 @@ WORKLOADS = {
     "pool_small_8cm": "pool_small_8cm.toml",  # 32 x 80 x 32
     "pallets_5cm": "pallets_5cm.toml",        # 128 x 240 x 128
     "bonfire_10cm": "bonfire_10cm.toml",      # 160 x 240 x 160
+    # the 2 cm pool at the exact 3.0 x 7.3 x 3.0 m shape, 150 x 365 x 150 =
+    # 8.21 M cells (no rounding): CG pressure solves only
+    "pool_2cm_exact": "pool_2cm_exact.toml",
 }
+EXACT_DIMS = {"pool_2cm_exact": [150, 365, 150]}
+SOLVERS = {"vcycle": 0, "mgpcg": 2, "mgpcg_bf16": 3}
 # Algorithmic bytes per cell per launch (each distinct array element read or
 # written once at the reference's width; read-modify-write twice).
 ALG_BYTES = {"solid": 68, "curl": 28, "adv_vel1": 24, "adv_vel2": 40, "adv_s1": 76,
@@ -216,7 +223,18 @@ class ClockSampler:
 
 def build_workload(name):
     from pyro_b200.scene import Scene
-    return Scene.load(os.path.join(ROOT, "pyro_b200", "scenes", WORKLOADS[name]))
+    sc = Scene.load(os.path.join(ROOT, "pyro_b200", "scenes", WORKLOADS[name]))
+    if name in EXACT_DIMS:
+        sc.dims_override = list(EXACT_DIMS[name])
+    return sc
+
+
+def solver_for(args):
+    """The pressure solver of the run: --solver, else the reference's fixed
+    V-cycles, except on shapes whose levels do not halve evenly (CG)."""
+    if args.solver:
+        return args.solver
+    return "mgpcg_bf16" if args.workload in EXACT_DIMS else "vcycle"
 
 
 def cfl_substeps(sc, max_u):
@@ -259,6 +277,29 @@ def max_over_ranks(values, device):
     return [float(v) for v in t.tolist()]
 
 
+TIMED_SUBSTEPS_PER_FRAME = 6
+
+
+def timed_substeps(sc):
+    """Substeps per 1/fps frame and their dt in the timed region of both
+    arms: 6, the frame loop's CFL count for the developed 2 cm pool
+    (src/main.rs:140-142 at max |u| ~ 6 m/s), so the two arms time the same
+    substep."""
+    n = TIMED_SUBSTEPS_PER_FRAME
+    return n, np.float32(np.float32(1.0) / np.float32(sc.sim.fps) / np.float32(n))
+
+
+def bench_config(args, dims, cycles, levels, solver, n, dt):
+    """The `config` object of both arms' lines."""
+    return {"workload": f"{args.workload} {dims[0]}x{dims[1]}x{dims[2]} (x,y-up,z)",
+            "cells": int(dims[0] * dims[1] * dims[2]), "substeps_per_frame": n,
+            "dt": float(dt),
+            "pressure": (f"{cycles} V-cycles, {levels} levels" if solver == "vcycle" else
+                         f"{solver} to {args.tol:g}"),
+            "l2": "working set 1.9 GB > L2, no flush",
+            "parallelism": f"replicas x{args.gpus}"}
+
+
 def run_reference(args):
     """CPU restatement of the reference step on all host cores."""
     rank = int(os.environ.get("RANK", "0"))
@@ -273,7 +314,7 @@ def run_reference(args):
     dens, kind = sc.slot_tables()
     sol = oracle.voxelize(shapes_array(sh), len(sh), g.dims[0], g.dims[1], g.dims[2], g.dx,
                           float(np.float32(sc.sim.ambient_temp)), sc.sim.seed, dens, kind)
-    n, dt = cfl_substeps(sc, 2.0)
+    n, dt = timed_substeps(sc)
     cores = oracle.max_threads()
     o = oracle.OracleSim(P, sol, sc.sim.pressure_cycles)
     t = np.float32(0.0)
@@ -292,9 +333,10 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": ms, "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic", "config": {"workload": f"{args.workload} {g.dims[0]}x{g.dims[1]}x"
-                                        f"{g.dims[2]} (x,y-up,z)", "cells": cells,
-                                        "substeps_per_frame": n, "dt": float(dt)},
+        "data": "synthetic",
+        "config": bench_config(args, g.dims, sc.sim.pressure_cycles,
+                               len(oracle.mg_levels(*g.dims)), "vcycle", n, dt),
+        "state": "from ignition (the oracle's cost per substep hardly depends on the state)",
         "cpu_baseline": {"value": ms, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": f"{args.steps} full substeps of the workload from ignition "
                                    "(C++ oracle restating the reference's WGSL kernels, OpenMP)"},
@@ -359,6 +401,40 @@ def metric_runs():
             ("mgpcg_fp32_to_1e-4", _abi.SOLVER_MGPCG, 1e-4, 200),
             ("mgpcg_bf16_to_1e-4", _abi.SOLVER_MGPCG_BF16, 1e-4, 200),
             ("mgpcg_bf16_learned_to_1e-4", _abi.SOLVER_MGPCG_LEARNED, 1e-4, 200)]
+
+
+def render_frames(sc, sim, stream, spp=64, reps=2):
+    """The path tracer's frame (pyro_b200.render.Renderer.render: input
+    pack, emission tables, light caches and blur in light-cache mode, then
+    the camera rays) on the developed state at the scene's render settings
+    (1280 x 720, `spp` samples), in light-cache and pure path-tracing mode.
+    Device time from CUDA events on the simulation's stream around each
+    frame, after one untimed frame per mode; the image read-back at the end
+    of a frame is included."""
+    import torch
+    from pyro_b200.render import Renderer
+    out = {"width": int(sc.render.width), "height": int(sc.render.height), "spp": spp}
+    for mode in ("cache", "path"):
+        cfg = type(sc.render)(**{**sc.render.__dict__, "mode": mode})
+        r = Renderer(sc, sim, cfg)
+        r.render(sim, frame=0, spp=spp)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        times = []
+        for k in range(reps):
+            e0.record(stream)
+            t0 = time.perf_counter()
+            img = r.render(sim, frame=k + 1, spp=spp)
+            wall = time.perf_counter() - t0
+            e1.record(stream)
+            e1.synchronize()
+            times.append((e0.elapsed_time(e1), wall * 1e3))
+        ms = min(t[0] for t in times)
+        out[mode] = {"frame_ms": ms, "frame_wall_ms": min(t[1] for t in times),
+                     "mean_radiance": float(np.mean(img)),
+                     "pixel_samples_per_s": out["width"] * out["height"] * spp / (ms * 1e-3)}
+        log(f"render {mode}: {ms:.1f} ms per {out['width']}x{out['height']} frame at {spp} spp")
+        del r
+    return out
 
 
 def sim_solver_bench(sim):
@@ -438,7 +514,10 @@ def run_ours(args):
     log(f"creating {args.workload} {sc.grid().dims}")
     sim = Sim(sc)
     cells = sim.cells()
-    log("created")
+    solver = solver_for(args)
+    if solver != "vcycle":
+        sim.set_solver(SOLVERS[solver], args.tol, 200)
+    log(f"created; pressure solver {solver}")
     lib = _abi.load()
     stream = torch.cuda.ExternalStream(sim.stream())
 
@@ -452,8 +531,9 @@ def run_ours(args):
         st = sim.read_stats()
         max_u = max(st.max_u, 1.0)
         t_pre += float(n * dt)
-    log(f"preroll done t={t_pre:.3f}s max_u={max_u:.2f}")
-    n, dt = cfl_substeps(sc, max_u)
+    log(f"preroll done t={t_pre:.3f}s max_u={max_u:.2f} (CFL substeps per frame "
+        f"{cfl_substeps(sc, max_u)[0]})")
+    n, dt = timed_substeps(sc)
     for k in range(args.warmup):
         sim.step(dt, (k % n) == n - 1)
     sim.sync()
@@ -509,12 +589,20 @@ def run_ours(args):
     info = sim.info()
     lvl = [tuple(info.level_dims[l]) for l in range(info.levels)]
     cyc_bytes, _ = mg_cycle_bytes(lvl)
-    step_bytes = sum(ALG_BYTES.values()) * cells + sc.sim.pressure_cycles * cyc_bytes
-    # the pressure solve per launch class, an event after every launch
+    if solver == "vcycle":
+        step_bytes = sum(ALG_BYTES.values()) * cells + sc.sim.pressure_cycles * cyc_bytes
+    else:
+        # per CG iteration one V-cycle of the preconditioner's hierarchy
+        # (counted at FP32 width, the reference rule's levels) plus the
+        # matrix-vector product and vector updates (about 48 B per cell)
+        cg_it = max(sim.last_solve().iterations, 1)
+        step_bytes = sum(ALG_BYTES.values()) * cells + cg_it * (cyc_bytes + 48.0 * cells)
+    # the pressure solve per launch class, an event after every launch (the
+    # fixed V-cycle schedule; the CG solver is timed as one phase)
     mg_ms = np.zeros(len(_abi.MG_CLASSES))
     mg_n = np.zeros(len(_abi.MG_CLASSES), np.int32)
     ms_buf = np.zeros(len(_abi.MG_CLASSES), np.float32)
-    for k in range(nprof):
+    for k in range(nprof if solver == "vcycle" else 0):
         _abi.check("pyro_sim_profile_pressure", lib.pyro_sim_profile_pressure(
             sim._h, ms_buf.ctypes.data_as(ctypes.c_void_p), mg_n.ctypes.data_as(ctypes.c_void_p),
             len(_abi.MG_CLASSES)))
@@ -526,6 +614,9 @@ def run_ours(args):
     classes = {}
     for k in ALG_BYTES:
         classes[k] = {"launches": 1, "ms": kern[k], "alg_bytes": ALG_BYTES[k] * cells}
+    if solver != "vcycle":
+        classes["pressure_cg"] = {"launches": 1, "ms": kern["pressure"],
+                                  "alg_bytes": step_bytes - sum(ALG_BYTES.values()) * cells}
     for i, k in enumerate(_abi.MG_CLASSES):
         if mg_n[i] > 0:
             classes[k] = {"launches": int(mg_n[i]), "ms": float(mg_ms[i]),
@@ -585,6 +676,9 @@ def run_ours(args):
         f"{frame_pack['emitting_cells']} emitting cells")
     log(f"render pack {pack_ms:.3f} ms ({frame_pack['pack_gbs']:.0f} GB/s), "
         f"bricks {bricks_ms:.3f} ms")
+    frame_render = None
+    if not args.no_render:
+        frame_render = render_frames(sc, sim, stream)
 
     # gather max over ranks
     ms, ms_e2e = max_over_ranks([ms, ms_e2e], "cuda")
@@ -630,12 +724,12 @@ def run_ours(args):
         "metric": METRIC, "value": ms, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"{args.workload} {sim.dims[0]}x{sim.dims[1]}x{sim.dims[2]} "
-                               "(x,y-up,z), developed flame", "cells": cells,
-                   "preroll_s": args.preroll_s, "substeps_per_frame": n, "dt": float(dt),
-                   "ms_per_frame": ms * n, "pressure": f"{sc.sim.pressure_cycles} V-cycles, "
-                   f"{info.levels} levels", "l2": "working set 1.9 GB > L2, no flush",
-                   "parallelism": f"replicas x{world}"},
+        "config": bench_config(args, sim.dims, sc.sim.pressure_cycles, info.levels, solver, n,
+                               dt),
+        "state": f"developed flame after a {args.preroll_s:g} s preroll of the frame loop",
+        "ms_per_frame": ms * n,
+        "cg_iterations_last_solve": (sim.last_solve().iterations if solver != "vcycle"
+                                     else None),
         "e2e": {"value": ms_e2e, "unit": UNIT, "h2d_bytes_per_step": 576,
                 "d2h_bytes_per_step": 4 * _abi.STATS_N},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
@@ -648,6 +742,7 @@ def run_ours(args):
         "kernels_ms": kern,
         "kernel_classes": classes,
         "frame_pack": frame_pack,
+        "frame_render": frame_render,
         "throughput": {"value": world * cells / (ms * 1e-3), "unit": "cells*substeps/s"},
         "cpu_baseline": cpu,
         "solver": solver,
@@ -674,6 +769,11 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-solver", action="store_true")
+    ap.add_argument("--no-render", action="store_true")
+    ap.add_argument("--solver", choices=sorted(SOLVERS), default=None,
+                    help="pressure solver of the timed substeps (default: the reference's "
+                         "fixed V-cycles; CG on shapes that do not halve evenly)")
+    ap.add_argument("--tol", type=float, default=1e-4, help="CG relative residual")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -8,9 +8,10 @@
 //    (k = +x,-x,+y,-y,+z,-z) = neighbour k is inside the level and fluid,
 //    bit 6 = the cell is solid.  The smoother's neighbour count is the
 //    popcount plus the Dirichlet faces the cell touches.
-//  * k_mg_pass4 updates the cells of one colour four per thread (float4
-//    rows, lane shuffles for the x halo); k_mg_restrict_m / k_mg_prolong_m
-//    work one thread per coarse cell.
+//  * k_mg_pass4z updates the cells of one colour in 4-cell row chunks,
+//    two planes per thread, with the colour parity the same across each
+//    warp (no per-lane selects); k_mg_restrict_m / k_mg_prolong_m work one
+//    thread per coarse cell.
 //
 // Per-cell arithmetic is the reference's, in its order, so results equal the
 // per-pass kernels bit for bit.
@@ -229,12 +230,7 @@ __global__ void __launch_bounds__(256) k_mg_pass(L d, float h2, const TS* __rest
   stv(p + i, wmix(ldv(p + i), (sum - h2 * ldv(b + i)) / cnt, omega));
 }
 
-// The same pass four cells at a time, for rows of a multiple of 4 cells:
-// thread (tx, y, z) loads cells x0..x0+3 (x0 = 4 tx) of phi, b, the masks
-// and the four neighbour rows as vectors, takes phi at x0 - 1 and x0 + 4
-// from the neighbouring lanes, updates the two cells of the pass's colour
-// with the per-cell arithmetic above and stores the four values back (the
-// other colour's two unchanged; nothing else writes them in this pass).
+// Four cells of a row as one vector access (FP32 or BF16 storage).
 __device__ __forceinline__ float4 ld4(const float* p) {
   return *reinterpret_cast<const float4*>(p);
 }
@@ -252,84 +248,158 @@ __device__ __forceinline__ void st4(__nv_bfloat16* p, float4 v) {
   *reinterpret_cast<uint2*>(p) = u;
 }
 
-template <typename TS>
-__global__ void __launch_bounds__(256, 6) k_mg_pass4(L d, float h2, const TS* __restrict__ b,
-                                                  const uint8_t* __restrict__ meta,
-                                                  TS* __restrict__ p, int color, float omega,
-                                                  int bc_mode, FastDiv by_cpr, FastDiv by_ny) {
-  pdl_trigger();
-  pdl_wait();
-  // chunk c of 4 cells, x fastest; rows of nx / 4 chunks (divisions by the
-  // row length and ny by multiply-high)
-  const int cpr = d.nx >> 2;
-  const int nchunks = cpr * d.ny * d.nz;
-  const int c = blockIdx.x * 256 + threadIdx.x;
-  const int lane = threadIdx.x & 31;
-  const bool act = c < nchunks;
-  const int cc = act ? c : 0;
-  const int row = (int)by_cpr.div((uint32_t)cc);
-  const int x0 = (cc - row * cpr) * 4;
-  const int z = (int)by_ny.div((uint32_t)row), y = row - z * d.ny;
-  const int sy = d.nx, sz = d.nx * d.ny;
-  const int i0 = row * d.nx + x0;
-  // every load first
-  const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
-  const float4 P0 = act ? ld4(p + i0) : zero;
-  const uint32_t m4 = act ? *reinterpret_cast<const uint32_t*>(meta + i0) : 0x40404040u;
-  const float4 B = act ? ld4(b + i0) : zero;
-  const float4 Yp = (act && y + 1 < d.ny) ? ld4(p + i0 + sy) : zero;
-  const float4 Ym = (act && y > 0) ? ld4(p + i0 - sy) : zero;
-  const float4 Zp = (act && z + 1 < d.nz) ? ld4(p + i0 + sz) : zero;
-  const float4 Zm = (act && z > 0) ? ld4(p + i0 - sz) : zero;
-  // phi at x0 - 1 and x0 + 4: the neighbouring lanes' chunks when they are
-  // in the same row, else a load
-  float left = __shfl_up_sync(0xffffffffu, P0.w, 1);
-  float right = __shfl_down_sync(0xffffffffu, P0.x, 1);
-  if (!act) return;
-  if (x0 > 0 && lane == 0) left = ldv(p + i0 - 1);
-  if (x0 + 4 < d.nx && lane == 31) right = ldv(p + i0 + 4);
-  // the two cells of the pass's colour: x0 + par (a) and x0 + par + 2 (b)
-  const bool odd = ((y + z + color) & 1) != 0;
-  const uint32_t ma = (m4 >> (odd ? 8 : 0)) & 0xFFu, mb = (m4 >> (odd ? 24 : 16)) & 0xFFu;
-  if ((ma & META_SOLID) && (mb & META_SOLID)) return;
-  // Dirichlet faces: y and z terms shared, x terms only at the row ends
-  const int dyz = (y == d.ny - 1) + (bc_mode == 0 ? (z == 0) + (z == d.nz - 1) : 0);
-  const int da = dyz + (bc_mode == 0 && !odd && x0 == 0);
-  const int db = dyz + (bc_mode == 0 && odd && x0 + 4 == d.nx);
-  const float own_a = odd ? P0.y : P0.x, own_b = odd ? P0.w : P0.z;
-  float4 P = P0;
+// The two cells of the pass's colour in one 4-cell chunk x0..x0+3 of a row
+// whose colour parity ODD = (y + z + colour) & 1 is known at compile time:
+// cell a = x0 + ODD and cell b = x0 + ODD + 2, each with the reference's
+// per-cell arithmetic (mg.wgsl:17-36) and neighbour order (+x, -x, +y, -y,
+// +z, -z).  P0 is the chunk, left / right phi at x0 - 1 and x0 + 4, Yp ... Zm
+// the neighbour rows' chunks, m4 the four mask bytes, da / db the Dirichlet
+// faces of cells a and b.
+template <bool ODD>
+__device__ __forceinline__ bool chunk_colour(float4& P, const float4 P0, float left, float right,
+                                             const float4 Yp, const float4 Ym, const float4 Zp,
+                                             const float4 Zm, const float4 B, uint32_t m4, int da,
+                                             int db, float h2, float omega) {
+  const uint32_t ma = ODD ? (m4 >> 8) & 0xFFu : m4 & 0xFFu;
+  const uint32_t mb = ODD ? (m4 >> 24) : (m4 >> 16) & 0xFFu;
   bool any = false;
   if (!(ma & META_SOLID)) {
     float sum = 0.0f;
-    if (ma & 1u) sum += odd ? P0.z : P0.y;
-    if (ma & 2u) sum += odd ? P0.x : left;
-    if (ma & 4u) sum += odd ? Yp.y : Yp.x;
-    if (ma & 8u) sum += odd ? Ym.y : Ym.x;
-    if (ma & 16u) sum += odd ? Zp.y : Zp.x;
-    if (ma & 32u) sum += odd ? Zm.y : Zm.x;
+    if (ma & 1u) sum += ODD ? P0.z : P0.y;
+    if (ma & 2u) sum += ODD ? P0.x : left;
+    if (ma & 4u) sum += ODD ? Yp.y : Yp.x;
+    if (ma & 8u) sum += ODD ? Ym.y : Ym.x;
+    if (ma & 16u) sum += ODD ? Zp.y : Zp.x;
+    if (ma & 32u) sum += ODD ? Zm.y : Zm.x;
     const float cnt = (float)(__popc(ma & 63u) + da);
     if (cnt >= 0.5f) {
-      const float v = wmix(own_a, (sum - h2 * (odd ? B.y : B.x)) / cnt, omega);
-      if (odd) P.y = v; else P.x = v;
+      const float v = wmix(ODD ? P0.y : P0.x, (sum - h2 * (ODD ? B.y : B.x)) / cnt, omega);
+      if (ODD) P.y = v; else P.x = v;
       any = true;
     }
   }
   if (!(mb & META_SOLID)) {
     float sum = 0.0f;
-    if (mb & 1u) sum += odd ? right : P0.w;
-    if (mb & 2u) sum += odd ? P0.z : P0.y;
-    if (mb & 4u) sum += odd ? Yp.w : Yp.z;
-    if (mb & 8u) sum += odd ? Ym.w : Ym.z;
-    if (mb & 16u) sum += odd ? Zp.w : Zp.z;
-    if (mb & 32u) sum += odd ? Zm.w : Zm.z;
+    if (mb & 1u) sum += ODD ? right : P0.w;
+    if (mb & 2u) sum += ODD ? P0.z : P0.y;
+    if (mb & 4u) sum += ODD ? Yp.w : Yp.z;
+    if (mb & 8u) sum += ODD ? Ym.w : Ym.z;
+    if (mb & 16u) sum += ODD ? Zp.w : Zp.z;
+    if (mb & 32u) sum += ODD ? Zm.w : Zm.z;
     const float cnt = (float)(__popc(mb & 63u) + db);
     if (cnt >= 0.5f) {
-      const float v = wmix(own_b, (sum - h2 * (odd ? B.w : B.z)) / cnt, omega);
-      if (odd) P.w = v; else P.z = v;
+      const float v = wmix(ODD ? P0.w : P0.z, (sum - h2 * (ODD ? B.w : B.z)) / cnt, omega);
+      if (ODD) P.w = v; else P.z = v;
       any = true;
     }
   }
-  if (any) st4(p + i0, P);
+  return any;
+}
+
+// One colour pass over rows of a multiple of 4 cells with warp-uniform
+// colour parity.  Block (8, 16): thread (tx, ty) takes the 4-cell chunk
+// 8 blockIdx.x + tx of row y = 16 blockIdx.y + ry and ZT consecutive planes
+// from z = ZT blockIdx.z, where warp w = ty / 4 holds rows
+// ry = 8 (w / 2) + 2 (ty % 4) + w % 2: the four rows of a warp have one
+// parity, so (y + z + colour) & 1 is the same in every lane and the update
+// is compiled once per parity with its cells at fixed positions in the
+// chunk (chunk_colour).  Per plane a thread loads b, the masks and the
+// +-y rows; the -z row, the chunk and the +z row carry over from the
+// previous plane (their cells of the other colour are not written in this
+// pass), and phi at x0 - 1 and x0 + 4 comes from the neighbouring lanes of
+// the same row.  Results equal the reference's pass bit for bit.
+//
+// Two more forms serve the first and the last pass on level 0 of the CG
+// preconditioner's V-cycle:
+//  * PASS_FIRST: phi is zero everywhere (the V-cycle's initial guess), so
+//    no phi is read; the right-hand side comes in FP32 (b32) and, with BF16
+//    storage, is written rounded to BF16 into b (the copy later passes
+//    read) and used rounded; every cell of the chunk is written (the
+//    colour's cells updated, the others 0).  This replaces clearing phi,
+//    converting b and the pass itself.
+//  * PASS_LAST_F32: the pass on BF16 storage whose chunk, every cell, is
+//    written widened to FP32 into out (the V-cycle's result) instead of
+//    back into p; the updated cells are rounded to BF16 first, as a store
+//    to p and a conversion would do.
+enum { PASS = 0, PASS_FIRST = 1, PASS_LAST_F32 = 2 };
+
+template <typename TS>
+__device__ __forceinline__ float4 round_to(float4 v) {
+  if constexpr (sizeof(TS) == 2) {
+    const float2 a = __bfloat1622float2(__floats2bfloat162_rn(v.x, v.y));
+    const float2 c = __bfloat1622float2(__floats2bfloat162_rn(v.z, v.w));
+    return make_float4(a.x, a.y, c.x, c.y);
+  }
+  return v;
+}
+
+template <typename TS, int ZT, int MODE>
+__global__ void __launch_bounds__(128) k_mg_pass4z(L d, float h2, TS* __restrict__ b,
+                                                   const uint8_t* __restrict__ meta,
+                                                   TS* __restrict__ p, int color, float omega,
+                                                   int bc_mode, const float* __restrict__ b32,
+                                                   float* __restrict__ out) {
+  pdl_trigger();
+  pdl_wait();
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int w = ty >> 2;
+  const int y = blockIdx.y * 16 + (w >> 1) * 8 + 2 * (ty & 3) + (w & 1);
+  const int x0 = (blockIdx.x * 8 + tx) * 4;
+  const bool act = x0 < d.nx && y < d.ny;
+  const bool rd = act && MODE != PASS_FIRST;  // phi is read (not the zero guess)
+  const int sy = d.nx, sz = d.nx * d.ny;
+  const int zb = blockIdx.z * ZT;
+  const bool open = bc_mode == 0;
+  const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+  // row start of plane zb; the window -z / chunk / +z
+  int i0 = (zb * d.ny + y) * d.nx + x0;
+  float4 Zm = (rd && zb > 0) ? ld4(p + i0 - sz) : zero;
+  float4 P0 = rd ? ld4(p + i0) : zero;
+  float4 Zp = (rd && zb + 1 < d.nz) ? ld4(p + i0 + sz) : zero;
+  const int dy = (y == d.ny - 1);
+  const int dxa = (open && x0 == 0), dxb = (open && x0 + 4 == d.nx);
+#pragma unroll
+  for (int k = 0; k < ZT; k++) {
+    const int z = zb + k;
+    if (z >= d.nz) break;  // the same in every thread of the block
+    float4 B = zero;
+    if (MODE == PASS_FIRST) {
+      if (act) {
+        B = round_to<TS>(ld4(b32 + i0));
+        if constexpr (sizeof(TS) == 2) st4(b + i0, B);
+      }
+    } else {
+      B = act ? ld4(b + i0) : zero;
+    }
+    const uint32_t m4 = act ? *reinterpret_cast<const uint32_t*>(meta + i0) : 0x40404040u;
+    const float4 Yp = (rd && y + 1 < d.ny) ? ld4(p + i0 + sy) : zero;
+    const float4 Ym = (rd && y > 0) ? ld4(p + i0 - sy) : zero;
+    // the next plane's +z row, loaded ahead
+    const float4 Zn = (rd && k + 1 < ZT && z + 2 < d.nz) ? ld4(p + i0 + 2 * sz) : zero;
+    float left = __shfl_up_sync(0xffffffffu, P0.w, 1);
+    float right = __shfl_down_sync(0xffffffffu, P0.x, 1);
+    if (rd && tx == 0 && x0 > 0) left = ldv(p + i0 - 1);
+    if (rd && tx == 7 && x0 + 4 < d.nx) right = ldv(p + i0 + 4);
+    const int dyz = dy + (open ? (z == 0) + (z == d.nz - 1) : 0);
+    float4 P = P0;
+    const bool odd = ((y + z + color) & 1) != 0;  // the same in every lane of the warp
+    bool any;
+    if (odd)
+      any = chunk_colour<true>(P, P0, left, right, Yp, Ym, Zp, Zm, B, m4, dyz, dyz + dxb, h2,
+                               omega);
+    else
+      any = chunk_colour<false>(P, P0, left, right, Yp, Ym, Zp, Zm, B, m4, dyz + dxa, dyz, h2,
+                                omega);
+    if (MODE == PASS_LAST_F32) {
+      if (act) *reinterpret_cast<float4*>(out + i0) = round_to<TS>(P);
+    } else if (act && (any || MODE == PASS_FIRST)) {
+      st4(p + i0, P);
+    }
+    Zm = P0;
+    P0 = Zp;
+    Zp = Zn;
+    i0 += sz;
+  }
 }
 
 // Restriction with the neighbour mask (mg.wgsl:38-83): coarse rhs = mean of
@@ -521,18 +591,50 @@ inline dim3 g3(Dims3 d) { return dim3((d.nx + 31) / 32, (d.ny + 3) / 4, (d.nz + 
 
 }  // namespace
 
+constexpr int PASS_ZT = 2;  // planes per thread of k_mg_pass4z
+
+inline dim3 pass4z_grid(Dims3 d) {
+  return dim3((unsigned)((d.nx / 4 + 7) / 8), (unsigned)((d.ny + 15) / 16),
+              (unsigned)((d.nz + PASS_ZT - 1) / PASS_ZT));
+}
+
 template <typename TS>
 cudaError_t pass_t(Dims3 d, float h, const TS* b, const uint8_t* meta, TS* p, int color,
                    float omega, int bc_mode, cudaStream_t st) {
-  if (d.nx % 4 == 0) {
-    const long chunks = (long)(d.nx / 4) * d.ny * d.nz;
-    return launch_pdl(k_mg_pass4<TS>, dim3((unsigned)((chunks + 255) / 256)), dim3(256), 0, st,
-                      L{d.nx, d.ny, d.nz}, h * h, b, meta, p, color, omega, bc_mode,
-                      FastDiv((uint32_t)(d.nx / 4)), FastDiv((uint32_t)d.ny));
-  }
+  if (d.nx % 4 == 0)
+    return launch_pdl(k_mg_pass4z<TS, PASS_ZT, PASS>, pass4z_grid(d), dim3(8, 16), 0, st,
+                      L{d.nx, d.ny, d.nz}, h * h, const_cast<TS*>(b), meta, p, color, omega,
+                      bc_mode, (const float*)nullptr, (float*)nullptr);
   dim3 grid(((d.nx + 1) / 2 + 31) / 32, (d.ny + 3) / 4, (d.nz + 1) / 2);
   return launch_pdl(k_mg_pass<TS>, grid, dim3(32, 4, 2), 0, st, L{d.nx, d.ny, d.nz}, h * h, b,
                     meta, p, color, omega, bc_mode);
+}
+
+bool mg_pass_fused_ok(Dims3 d) { return d.nx % 4 == 0; }
+
+cudaError_t launch_mg_pass_first(Dims3 d, float h, const float* r, void* bq,
+                                 const uint8_t* meta, void* p, int color, float omega,
+                                 int bc_mode, bool bf16, cudaStream_t st) {
+  if (!mg_pass_fused_ok(d)) return cudaErrorNotSupported;
+  if (bf16) {
+    using T = __nv_bfloat16;
+    return launch_pdl(k_mg_pass4z<T, PASS_ZT, PASS_FIRST>, pass4z_grid(d), dim3(8, 16), 0, st,
+                      L{d.nx, d.ny, d.nz}, h * h, (T*)bq, meta, (T*)p, color, omega, bc_mode, r,
+                      (float*)nullptr);
+  }
+  return launch_pdl(k_mg_pass4z<float, PASS_ZT, PASS_FIRST>, pass4z_grid(d), dim3(8, 16), 0, st,
+                    L{d.nx, d.ny, d.nz}, h * h, const_cast<float*>(r), meta, (float*)p, color,
+                    omega, bc_mode, r, (float*)nullptr);
+}
+
+cudaError_t launch_mg_pass_last_f32(Dims3 d, float h, const void* b, const uint8_t* meta,
+                                    void* p, float* out, int color, float omega, int bc_mode,
+                                    cudaStream_t st) {
+  if (!mg_pass_fused_ok(d)) return cudaErrorNotSupported;
+  using T = __nv_bfloat16;
+  return launch_pdl(k_mg_pass4z<T, PASS_ZT, PASS_LAST_F32>, pass4z_grid(d), dim3(8, 16), 0, st,
+                    L{d.nx, d.ny, d.nz}, h * h, (T*)const_cast<void*>(b), meta, (T*)p, color,
+                    omega, bc_mode, (const float*)nullptr, out);
 }
 template <typename TS>
 cudaError_t restrict_t(Dims3 df, float h, const TS* pf, const TS* bf, const uint8_t* mf,

@@ -219,9 +219,18 @@ cudaError_t Multigrid::vcycle_sym(cudaStream_t st, DevBuf* bphi, DevBuf* bphi2, 
   auto B = [&](int l) -> void* { return lo ? bb[l].p : (void*)b[l]; };
   auto T = [&](int l) -> void* { return lo ? bphi2[l].p : phi2[l].p; };
   size_t n0 = dims[0].cells();
-  if (lo) {  // the initial guess is zero: level 0 of the BF16 copy starts cleared
-    if ((e = launch_f32_to_bf16(b[0], bb[0].p, n0, st)) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(bphi[0].p, 0, n0 * 2, st)) != cudaSuccess) return e;
+  // The first and last level-0 passes take the zero guess, the FP32
+  // right-hand side and (BF16) the FP32 result directly when the row length
+  // allows (mg_pass_fused_ok); otherwise level 0 is cleared and converted
+  // here and converted back at the end.
+  const bool fuse = nl > 1 && mg_pass_fused_ok(dims[0]);
+  if (!fuse) {
+    if (lo) {
+      if ((e = launch_f32_to_bf16(b[0], bb[0].p, n0, st)) != cudaSuccess) return e;
+      if ((e = cudaMemsetAsync(bphi[0].p, 0, n0 * 2, st)) != cudaSuccess) return e;
+    } else if ((e = cudaMemsetAsync(phi[0], 0, n0 * 4, st)) != cudaSuccess) {
+      return e;
+    }
   }
   auto pass = [&](int l, int c, float om) -> cudaError_t {
     return lo ? launch_mg_pass_bf16(dims[l], h[l], B(l), M(l), P(l), c, om, bc_mode, st)
@@ -230,8 +239,13 @@ cudaError_t Multigrid::vcycle_sym(cudaStream_t st, DevBuf* bphi, DevBuf* bphi2, 
   };
   for (int l = 0; l < nl - 1; l++) {
     for (int it = 0; it < 2; it++)
-      for (int c = 0; c < 2; c++)
-        if ((e = pass(l, c, 1.0f)) != cudaSuccess) return e;
+      for (int c = 0; c < 2; c++) {
+        e = (fuse && l == 0 && it == 0 && c == 0)
+                ? launch_mg_pass_first(dims[0], h[0], b[0], lo ? bb[0].p : nullptr, M(0), P(0), 0,
+                                       1.0f, bc_mode, lo, st)
+                : pass(l, c, 1.0f);
+        if (e != cudaSuccess) return e;
+      }
     e = lo ? launch_mg_restrict_sym_bf16(dims[l], h[l], P(l), B(l), M(l), T(l), dims[l + 1],
                                          M(l + 1), B(l + 1), P(l + 1), bc_mode, st)
            : launch_mg_restrict_sym(dims[l], h[l], (const float*)P(l), (const float*)B(l), M(l),
@@ -258,10 +272,15 @@ cudaError_t Multigrid::vcycle_sym(cudaStream_t st, DevBuf* bphi, DevBuf* bphi2, 
                                  dims[l + 1], M(l + 1), st);
     if (e != cudaSuccess) return e;
     for (int it = 0; it < 2; it++)
-      for (int c = 1; c >= 0; c--)
-        if ((e = pass(l, c, 1.0f)) != cudaSuccess) return e;
+      for (int c = 1; c >= 0; c--) {
+        e = (fuse && lo && l == 0 && it == 1 && c == 0)
+                ? launch_mg_pass_last_f32(dims[0], h[0], B(0), M(0), P(0), phi[0], 0, 1.0f,
+                                          bc_mode, st)
+                : pass(l, c, 1.0f);
+        if (e != cudaSuccess) return e;
+      }
   }
-  if (lo) return launch_bf16_to_f32(bphi[0].p, phi[0], n0, st);
+  if (lo && !fuse) return launch_bf16_to_f32(bphi[0].p, phi[0], n0, st);
   return cudaSuccess;
 }
 

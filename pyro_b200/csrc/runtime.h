@@ -120,10 +120,11 @@ struct Multigrid {
   cudaError_t vcycles(int cycles, cudaStream_t st);
   // Symmetric V-cycle for the CG preconditioner: pre-smoothing red-black,
   // post-smoothing black-red, restriction P^T/8 of the fluid-normalised
-  // trilinear prolongation, coarsest level by alternating SOR sweeps.  With
-  // bphi != nullptr phi and b are stored in BF16 (FP32 arithmetic).  The
-  // initial guess is zero: level 0's phi must hold zeros in FP32 storage
-  // and is not read in BF16 storage (the result overwrites all of it).
+  // trilinear prolongation, coarsest level by the direct solve when set,
+  // else alternating SOR sweeps.  With bphi != nullptr phi and b are stored
+  // in BF16 (FP32 arithmetic).  The initial guess is zero: level 0's phi is
+  // not read, the result overwrites all of it (FP32), and level 0's b is the
+  // FP32 right-hand side in both storages.
   // prep = false skips the per-level masks (valid while the level flags
   // are unchanged since the last prepare()).
   cudaError_t vcycle_sym(cudaStream_t st, DevBuf* bphi, DevBuf* bphi2, DevBuf* bb,

@@ -613,10 +613,8 @@ int Solver::true_resid(cudaStream_t st, const float* phi, const float* b, double
 }
 
 cudaError_t Solver::precond(cudaStream_t st, bool bf16, bool prep) {
-  // z = V(r): one V-cycle from a zero initial guess (the BF16 V-cycle
-  // writes every cell of z and does not read it).
-  cudaError_t e = cudaSuccess;
-  if (!bf16 && (e = cudaMemsetAsync(z.p, 0, d.cells() * 4, st)) != cudaSuccess) return e;
+  // z = V(r): one V-cycle from a zero initial guess (it writes every cell
+  // of z and does not read it).
   pc.bind_level0(z.as<float>(), r.as<float>(), fa.as<uint32_t>());
   return bf16 ? pc.vcycle_sym(st, bphi.data(), bphi2.data(), bb.data(), prep)
               : pc.vcycle_sym(st, nullptr, nullptr, nullptr, prep);

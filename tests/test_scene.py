@@ -109,8 +109,11 @@ def test_params_block_layout_and_constants():
 def test_scene_files_parse():
     files = sorted(glob.glob(os.path.join(SCENES, "*.toml")))
     assert len(files) >= 4
+    # pool_2cm_exact: the loader's rounding of 3.0 x 7.3 x 3.0 m; the bench
+    # sets the exact 150 x 365 x 150 with dims_override
     expect = {"pool_small_8cm": [32, 80, 32], "pool_2cm": [160, 320, 160],
-              "pallets_5cm": [128, 240, 128], "bonfire_10cm": [160, 240, 160]}
+              "pallets_5cm": [128, 240, 128], "bonfire_10cm": [160, 240, 160],
+              "pool_2cm_exact": [144, 368, 144]}
     for f in files:
         sc = Scene.load(f)
         name = os.path.basename(f)[:-5]
