@@ -482,6 +482,30 @@ int pyro_k_render_trace(const PyroRenderParams* rp, const void* vol,
                         const void* lvB, uint32_t lx, uint32_t ly, uint32_t lz,
                         const void* gE, uint32_t gres, float* accum,
                         void* stream);
+
+/* ---- frame development (src/post.rs:25-160, CPU code in the reference) --- */
+/* The tracer's accumulation image `accum` (w*h float4: radiance sums and
+ * sample count) to its mean radiance `img` (w*h*3 floats, sums divided by
+ * max(count, 1)), and the k-th smallest pixel luminance
+ * 0.2126 r + 0.7152 g + 0.0722 b (k counted from 0; the auto exposure uses
+ * k = min(floor(0.995 w h), w h - 1), post.rs:31-35) into *kth (host),
+ * exactly.  keys: w*h uint32 scratch, sel: PYRO_POST_SEL_WORDS uint32
+ * scratch (device).  Blocks until *kth is available. */
+#define PYRO_POST_SEL_WORDS 260
+int pyro_post_select(const float* accum, uint32_t w, uint32_t h, uint32_t k,
+                     float* img, uint32_t* keys, uint32_t* sel, float* kth,
+                     void* stream);
+/* img * gain, then with glare > 0 the three box-blurred glare scales mixed
+ * in (post.rs:90-160, the box filters' running sums in the reference's
+ * order), the ACES curve, sRGB, the per-pixel dither and 8-bit
+ * quantisation into out (w*h*3 bytes, device).  scratch: 12*w*h floats;
+ * lin_out (optional, w*h*3 floats) receives the linear image after the
+ * glare mix.  Asynchronous on `stream`.  The gain 2^exposure comes from the
+ * host's exposure state (pyro_b200.post.Camera). */
+int pyro_post_develop(const float* img, uint32_t w, uint32_t h, float gain,
+                      float glare, float* scratch, uint8_t* out,
+                      float* lin_out, void* stream);
+
 /* Coarsest-level solve: `iters` red-black SOR sweeps (omega) in one
  * launch (src/sim.rs:473 runs 80 sweeps at omega 1.6 as 160 dispatches). */
 int pyro_k_mg_coarse(uint32_t nx, uint32_t ny, uint32_t nz, float h,

@@ -20,6 +20,7 @@ PYRO_E_TIMEOUT = -6
 
 STATS_N = 1040
 NOALLOC_MAX_CELLS = 1 << 19
+POST_SEL_WORDS = 260  # radix-select scratch of pyro_post_select
 MAX_LAYERS = 1024
 ABI_VERSION = 2
 
@@ -178,6 +179,8 @@ SIGNATURES = {
     "pyro_sim_sync": [_P],
     "pyro_sim_profile_step": [_P, _F, _F, _F, _I, _P, _I],
     "pyro_sim_profile_pressure": [_P, _P, _P, _I],
+    "pyro_post_select": [_P, _U32, _U32, _U32, _P, _P, _P, ctypes.POINTER(_F), _P],
+    "pyro_post_develop": [_P, _U32, _U32, _F, _F, _P, _P, _P, _P],
     "pyro_sim_info": [_P, ctypes.POINTER(PyroSimInfo)],
     "pyro_sim_set_solver": [_P, _I, _F, _I],
     "pyro_sim_last_solve": [_P, ctypes.POINTER(PyroSolveInfo)],

@@ -458,6 +458,34 @@ int pyro_k_render_trace(const PyroRenderParams* rp, const void* vol, const void*
              "pyro_k_render_trace");
 }
 
+int pyro_post_select(const float* accum, uint32_t w, uint32_t h, uint32_t k, float* img,
+                     uint32_t* keys, uint32_t* sel, float* kth, void* stream) {
+  clear_error();
+  PYRO_REQUIRE(accum && img && keys && sel && kth, "pyro_post_select: null argument");
+  PYRO_REQUIRE(w >= 1 && h >= 1 && (uint64_t)w * h * 3 < (1ull << 31),
+               "pyro_post_select: invalid image size");
+  PYRO_REQUIRE((uint64_t)k < (uint64_t)w * h, "pyro_post_select: rank k must be < w * h");
+  cudaStream_t st = S(stream);
+  PYRO_CU(launch_post_select(accum, (int)(w * h), (int)k, img, keys, sel, st));
+  uint32_t key = 0;
+  PYRO_CU(cudaMemcpyAsync(&key, sel + 3, 4, cudaMemcpyDeviceToHost, st));
+  PYRO_CU(cudaStreamSynchronize(st));
+  *kth = post_key_value(key);
+  return PYRO_OK;
+}
+
+int pyro_post_develop(const float* img, uint32_t w, uint32_t h, float gain, float glare,
+                      float* scratch, uint8_t* out, float* lin_out, void* stream) {
+  clear_error();
+  PYRO_REQUIRE(img && scratch && out, "pyro_post_develop: null argument");
+  PYRO_REQUIRE(w >= 1 && h >= 1 && (uint64_t)w * h * 12 < (1ull << 31),
+               "pyro_post_develop: invalid image size");
+  PYRO_REQUIRE(glare >= 0.0f && glare <= 1.0f, "pyro_post_develop: glare must be in [0, 1]");
+  return ret(launch_post_develop(img, (int)w, (int)h, gain, glare, scratch, out, lin_out,
+                                 S(stream)),
+             "pyro_post_develop");
+}
+
 int pyro_voxelize(const PyroShape* shapes, uint32_t n_shapes, uint32_t nx, uint32_t ny,
                   uint32_t nz, float dx, float t0, uint32_t seed, const float* slot_density,
                   const uint32_t* slot_kind, float* sol_out, void* stream) {

@@ -91,6 +91,18 @@ cudaError_t launch_render_blur(const void* src, void* dst, Dims3 d, int axis, in
 cudaError_t launch_project(const PyroParams* P, Dims3 d, float* u, float* v, float* w,
                            const float* phi, const uint32_t* flags, cudaStream_t st);
 
+// Frame development (k_post.cu): the mean radiance of n = w*h pixels from
+// the tracer's accumulation image, each pixel's luminance key, and the
+// radix select of the k-th smallest luminance (its key ends in sel[3]; sel
+// holds POST_SEL_WORDS words); then the exposure, glare, tone curve and
+// 8-bit image.  scratch: 4 * 3n floats.
+constexpr int POST_SEL_WORDS = 260;
+cudaError_t launch_post_select(const float* accum, int n, int k, float* img, uint32_t* keys,
+                               uint32_t* sel, cudaStream_t st);
+float post_key_value(uint32_t key);
+cudaError_t launch_post_develop(const float* img, int w, int h, float gain, float glare,
+                                float* scratch, uint8_t* out, float* lin_out, cudaStream_t st);
+
 // Multigrid level kernels (src/shaders/mg.wgsl).  bc_mode 0 = reference
 // boundaries, 1 = Dirichlet on the top face only.
 cudaError_t launch_mg_resid(Dims3 d, float h, const float* p, const float* b, const uint32_t* f,

@@ -75,6 +75,12 @@ def box_v(b: np.ndarray, r: int) -> np.ndarray:
     return out
 
 
+def percentile_rank(n: int) -> int:
+    """Rank (from 0) of the auto exposure's 99.5th luminance percentile
+    among n pixels (post.rs:31-35)."""
+    return min(int(F32(n) * F32(0.995)), n - 1)
+
+
 def glare(img: np.ndarray) -> np.ndarray:
     """Lens glare: three scales of three box passes per axis, weighted
     (post.rs:90-107)."""
@@ -106,8 +112,15 @@ class Camera:
             return self.ev_offset
         p = img.reshape(-1, 3)
         l = F32(0.2126) * p[:, 0] + F32(0.7152) * p[:, 1] + F32(0.0722) * p[:, 2]
-        k = min(int(F32(l.size) * F32(0.995)), l.size - 1)
-        v = np.partition(l, k)[k]
+        k = percentile_rank(l.size)
+        return self.exposure_from(np.partition(l, k)[k], frame_dt)
+
+    def exposure_from(self, v, frame_dt: float) -> np.float32:
+        """The exposure state's update from the frame's 99.5th luminance
+        percentile v (the GPU development selects v on the device)."""
+        if not self.auto:
+            return self.ev_offset
+        v = F32(v)
         target = np.log2(F32(4.0) / max(v, F32(1e-3)))
         if self.ev is None:
             ev = F32(target)

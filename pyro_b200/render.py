@@ -193,6 +193,14 @@ class Renderer:
 
     def render(self, sim, frame: int, spp: int) -> np.ndarray:
         """One frame: the mean radiance per pixel, (h, w, 3) float32."""
+        self.render_device(sim, frame, spp)
+        acc = self.accum.cpu().numpy()
+        n = np.maximum(acc[:, 3:4], 1.0)
+        return (acc[:, :3] / n).reshape(self.h, self.w, 3)
+
+    def render_device(self, sim, frame: int, spp: int) -> None:
+        """One frame into self.accum (h*w float4 radiance sums and sample
+        counts, on the device), for pyro_b200.develop.Developer."""
         import torch
         st = sim.stream()
         sim.render_pack(True)
@@ -231,6 +239,3 @@ class Renderer:
                 trace(rp, vol, sol, vel, bricks, self.lut, ecdf, self.lvA, self.lvB,
                       self.lv_dims, self.gE, self.gres, self.accum, stream=st)
         torch.cuda.ExternalStream(st).synchronize()
-        acc = self.accum.cpu().numpy()
-        n = np.maximum(acc[:, 3:4], 1.0)
-        return (acc[:, :3] / n).reshape(self.h, self.w, 3)

@@ -235,20 +235,24 @@ def main(argv=None) -> int:
     out_dir = a.out or os.path.join(os.path.dirname(os.path.abspath(a.scene)), sc.output.dir)
     on_render = None
     if not a.sim_only:  # src/main.rs:100-104, 113-119, 180-197
+        from .develop import Developer
         from .post import Camera
         from .render import Renderer
         os.makedirs(out_dir, exist_ok=True)
         rend = Renderer(sc, sim)
+        dev = Developer(rend.w, rend.h)
         cam = Camera(sc.render.auto_exposure, sc.render.exposure, sc.render.glare)
         frame_dt = float(F(1.0) / F(sc.sim.fps))
         idx = [0]
 
         def on_render(f):
-            img = rend.render(sim, f, sc.render.spp)
+            # trace and develop on the GPU; one 8-bit image comes back
+            rend.render_device(sim, f, sc.render.spp)
+            rgb8 = dev.develop(cam, rend.accum.data_ptr(), frame_dt, sim.stream())
             name = (f"still_{float(sim.time):.1f}s.png" if a.still is not None
                     else f"frame_{idx[0]:05d}.png")
             path = os.path.join(out_dir, name)
-            write_png(path, cam.develop(img, frame_dt))
+            write_png(path, rgb8)
             idx[0] += 1
             if not a.quiet:
                 print(f"  rendered {path}")
