@@ -708,10 +708,10 @@ def run_ours(args):
                "sample": f"{args.cpu_steps} full substeps of the same developed state "
                          "(C++ oracle restating the reference's WGSL kernels, OpenMP)"}
 
-    solver = None
+    solver_runs = None
     if rank == 0 and not args.no_solver:
         log("solver bench")
-        solver = {"sim_pressure": sim_solver_bench(sim), "poisson_256": solver_bench()}
+        solver_runs = {"sim_pressure": sim_solver_bench(sim), "poisson_256": solver_bench()}
     # kernels per substep: 11 step kernels (solid, curl, adv_vel1/2, adv_s1/2,
     # react, confine, forces, divergence, project), the level preparation
     # (flags_down per coarse level, a mask per level) and per V-cycle 4 + 1 + 5
@@ -745,7 +745,7 @@ def run_ours(args):
         "frame_render": frame_render,
         "throughput": {"value": world * cells / (ms * 1e-3), "unit": "cells*substeps/s"},
         "cpu_baseline": cpu,
-        "solver": solver,
+        "solver": solver_runs,
         "gpu_launches": launches_per_step * args.steps + stats_steps,
         "clocks": clocks.summary(),
     }

@@ -599,11 +599,16 @@ void rp_from_rows(const double* rows, RP& R) {
   }
 }
 
+// rgba16float cache store.  WGSL leaves the conversion of values beyond the
+// largest finite binary16 to the implementation; they are stored as 65504
+// (saturated), the choice the CUDA tracer makes too.  Below that range the
+// store is round to nearest even.
+float sat16(float v) { return std::fmin(std::fmax(v, -65504.0f), 65504.0f); }
 void store_h4(uint16_t* t, size_t i, float a, float b, float c, float d) {
-  t[4 * i] = f32_to_f16(a);
-  t[4 * i + 1] = f32_to_f16(b);
-  t[4 * i + 2] = f32_to_f16(c);
-  t[4 * i + 3] = f32_to_f16(d);
+  t[4 * i] = f32_to_f16(sat16(a));
+  t[4 * i + 1] = f32_to_f16(sat16(b));
+  t[4 * i + 2] = f32_to_f16(sat16(c));
+  t[4 * i + 3] = f32_to_f16(sat16(d));
 }
 
 }  // namespace

@@ -111,30 +111,33 @@ __global__ void __launch_bounds__(256) k_mg_resid(Lvl d, float h2, const float* 
 // The coarsest level is swept 80 times per V-cycle (src/sim.rs:473), 160
 // dependent red-black passes over ~10-30 k cells.  One thread-block cluster
 // of up to 16 CTAs runs them all in a single launch: CTA r owns z-planes
-// [r*nz/C, (r+1)*nz/C) of phi in its shared memory, a thread owns up to
-// COARSE_K cells with their neighbour mask, count and h^2 b precomputed in
-// registers, neighbours across a slab boundary are read from the owning
-// CTA's shared memory (distributed shared memory), and the hardware cluster
-// barrier separates the colour passes.  The arithmetic per cell is the
-// reference's, in the same order, so the result equals 160 separate passes.
-constexpr int COARSE_THREADS = 1024;
-constexpr int COARSE_K = 2;
+// [r*nz/C, (r+1)*nz/C) of phi in its shared memory, neighbours across a
+// slab boundary are read from the owning CTA's shared memory (distributed
+// shared memory), and the hardware cluster barrier separates the colour
+// passes.  Threads are sorted by colour: thread t holds, per colour c, the
+// cells q = t + T k (k < K) of the slab in the reference smoother's own
+// numbering (x = 2 hx + ((y + z + c) & 1), mg.wgsl:17-19), with the
+// neighbour mask, count and h^2 b in registers, so every lane of a warp
+// updates a cell of the pass's colour and a barrier waits on few warps.  A
+// thread loads all neighbours of its cells of the pass before it computes
+// any of them.  The arithmetic per cell is the reference's, in the same
+// order, so the result equals 160 separate passes bit for bit.
 constexpr int COARSE_MAX_CLUSTER = 16;
+constexpr int COARSE_SMEM = 200 * 1024;
 
 struct CoarseCell {
-  int j;             // index in the own slab (-1: none)
-  uint32_t meta;     // bits 0-5: fluid in-domain neighbour, bit 6: colour, bit 7: skip
+  int j;             // index in the own slab (0 for an empty slot)
+  uint32_t meta;     // bits 0-5: fluid in-domain neighbour, bit 7: skip
   float cnt;
   float hb;
-  const float* zp;   // +z neighbour (local or remote), null when absent
+  const float* zp;   // +z neighbour (local or remote); the cell itself when absent
   const float* zm;   // -z neighbour
 };
 
-template <typename TS>
-__global__ void __launch_bounds__(COARSE_THREADS, 1)
-    k_mg_coarse_cluster(Lvl d, float h2, const TS* __restrict__ b,
-                        const uint32_t* __restrict__ f, TS* __restrict__ p, int iters,
-                        float omega, int bc_mode, int symmetric) {
+template <typename TS, int T, int K>
+__global__ void __launch_bounds__(T, 1)
+    k_mg_coarse_rb(Lvl d, float h2, const TS* __restrict__ b, const uint32_t* __restrict__ f,
+                   TS* __restrict__ p, int iters, float omega, int bc_mode, int symmetric) {
   namespace cg = cooperative_groups;
   pdl_trigger();
   pdl_wait();
@@ -145,51 +148,61 @@ __global__ void __launch_bounds__(COARSE_THREADS, 1)
   const int plane = d.nx * d.ny;
   const int z0 = rank * d.nz / C, z1 = (rank + 1) * d.nz / C;
   const int own = (z1 - z0) * plane;
-  for (int j = threadIdx.x; j < own; j += COARSE_THREADS) sp[j] = ldv(p + z0 * plane + j);
+  for (int j = threadIdx.x; j < own; j += T) sp[j] = ldv(p + z0 * plane + j);
   cl.sync();  // every slab is loaded before any remote read
-  CoarseCell cell[COARSE_K];
+  const int hxn = (d.nx + 1) / 2;
+  const int vpc = hxn * d.ny * (z1 - z0);  // virtual cells per colour
+  CoarseCell cell[2][K];
 #pragma unroll
-  for (int r = 0; r < COARSE_K; r++) {
-    int j = threadIdx.x + r * COARSE_THREADS;
-    cell[r].j = -1;
-    cell[r].meta = 0x80u;
-    cell[r].cnt = 1.0f;
-    cell[r].hb = 0.0f;
-    cell[r].zp = nullptr;
-    cell[r].zm = nullptr;
-    if (j >= own) continue;
-    int zl = j / plane, rem = j - zl * plane;
-    int y = rem / d.nx, x = rem - y * d.nx, z = z0 + zl;
-    int gi = d.idx(x, y, z);
-    cell[r].j = j;
-    uint32_t meta = (uint32_t)((x + y + z) & 1) << 6;
-    float cnt = 0.0f;
+  for (int c = 0; c < 2; c++)
 #pragma unroll
-    for (int k = 0; k < 6; k++) {
-      int ax = x + (k == 0) - (k == 1), ay = y + (k == 2) - (k == 3), az = z + (k == 4) - (k == 5);
-      if (ay < 0) continue;
-      if (!d.inb(ax, ay, az)) {
-        if (bc_mode == 0 || ay >= d.ny) cnt += 1.0f;
-        continue;
+    for (int k = 0; k < K; k++) {
+      CoarseCell& q = cell[c][k];
+      q.j = 0;
+      q.meta = 0x80u;
+      q.cnt = 1.0f;
+      q.hb = 0.0f;
+      q.zp = sp;
+      q.zm = sp;
+      const int v = threadIdx.x + T * k;
+      if (v >= vpc) continue;
+      const int hx = v % hxn, r = v / hxn;
+      const int y = r % d.ny, zl = r / d.ny, z = z0 + zl;
+      const int x = 2 * hx + ((y + z + c) & 1);
+      if (x >= d.nx) continue;
+      const int rem = y * d.nx + x, j = zl * plane + rem;
+      const int gi = d.idx(x, y, z);
+      q.j = j;
+      q.zp = sp + j;
+      q.zm = sp + j;
+      uint32_t meta = 0u;
+      float cnt = 0.0f;
+#pragma unroll
+      for (int nb = 0; nb < 6; nb++) {
+        int ax = x + (nb == 0) - (nb == 1), ay = y + (nb == 2) - (nb == 3),
+            az = z + (nb == 4) - (nb == 5);
+        if (ay < 0) continue;
+        if (!d.inb(ax, ay, az)) {
+          if (bc_mode == 0 || ay >= d.ny) cnt += 1.0f;
+          continue;
+        }
+        if (f[d.idx(ax, ay, az)] == 1u) continue;
+        meta |= 1u << nb;
+        cnt += 1.0f;
+        if (nb >= 4) {
+          // owner of plane az and its slab-local index
+          int o = 0;
+          while (o + 1 < C && (o + 1) * d.nz / C <= az) o++;
+          const float* base = (az >= z0 && az < z1) ? sp : cl.map_shared_rank(sp, o);
+          const float* a = base + (az - o * d.nz / C) * plane + rem;
+          if (nb == 4) q.zp = a; else q.zm = a;
+        }
       }
-      if (f[d.idx(ax, ay, az)] == 1u) continue;
-      meta |= 1u << k;
-      cnt += 1.0f;
-      if (k >= 4) {
-        // owner of plane az and its slab-local index
-        int o = 0;
-        while (o + 1 < C && (o + 1) * d.nz / C <= az) o++;
-        const float* base = (az >= z0 && az < z1) ? sp : cl.map_shared_rank(sp, o);
-        int oz0 = o * d.nz / C;
-        const float* q = base + (az - oz0) * plane + rem;
-        if (k == 4) cell[r].zp = q; else cell[r].zm = q;
-      }
+      if (f[gi] == 1u || cnt < 0.5f) meta |= 0x80u;
+      q.meta = meta;
+      q.cnt = cnt;
+      q.hb = h2 * ldv(b + gi);
     }
-    if (f[gi] == 1u || cnt < 0.5f) meta |= 0x80u;
-    cell[r].meta = meta;
-    cell[r].cnt = cnt;
-    cell[r].hb = h2 * ldv(b + gi);
-  }
   const int nx = d.nx;
 #pragma unroll 1
   for (int it = 0; it < iters; it++) {
@@ -198,24 +211,40 @@ __global__ void __launch_bounds__(COARSE_THREADS, 1)
 #pragma unroll
     for (int cc = 0; cc < 2; cc++) {
       const int c = cc ^ first;
+      float nbv[K][6], ownv[K];
+      // every load of the pass first: absent neighbours read the cell itself
+      // (a valid address) and are not added
 #pragma unroll
-      for (int r = 0; r < COARSE_K; r++) {
-        uint32_t m = cell[r].meta;
-        if ((m & 0x80u) || ((m >> 6) & 1u) != (uint32_t)c) continue;
-        int j = cell[r].j;
+      for (int k = 0; k < K; k++) {
+        const CoarseCell& q = c ? cell[1][k] : cell[0][k];
+        const int j = q.j;
+        const uint32_t m = q.meta;
+        nbv[k][0] = sp[(m & 1u) ? j + 1 : j];
+        nbv[k][1] = sp[(m & 2u) ? j - 1 : j];
+        nbv[k][2] = sp[(m & 4u) ? j + nx : j];
+        nbv[k][3] = sp[(m & 8u) ? j - nx : j];
+        nbv[k][4] = *q.zp;
+        nbv[k][5] = *q.zm;
+        ownv[k] = sp[j];
+      }
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        const CoarseCell& q = c ? cell[1][k] : cell[0][k];
+        const uint32_t m = q.meta;
+        if (m & 0x80u) continue;
         float sum = 0.0f;
-        if (m & 1u) sum += sp[j + 1];
-        if (m & 2u) sum += sp[j - 1];
-        if (m & 4u) sum += sp[j + nx];
-        if (m & 8u) sum += sp[j - nx];
-        if (m & 16u) sum += *cell[r].zp;
-        if (m & 32u) sum += *cell[r].zm;
-        sp[j] = wmix(sp[j], (sum - cell[r].hb) / cell[r].cnt, omega);
+        if (m & 1u) sum += nbv[k][0];
+        if (m & 2u) sum += nbv[k][1];
+        if (m & 4u) sum += nbv[k][2];
+        if (m & 8u) sum += nbv[k][3];
+        if (m & 16u) sum += nbv[k][4];
+        if (m & 32u) sum += nbv[k][5];
+        sp[q.j] = wmix(ownv[k], (sum - q.hb) / q.cnt, omega);
       }
       cl.sync();
     }
   }
-  for (int j = threadIdx.x; j < own; j += COARSE_THREADS) stv(p + z0 * plane + j, sp[j]);
+  for (int j = threadIdx.x; j < own; j += T) stv(p + z0 * plane + j, sp[j]);
 }
 
 __global__ void k_f32_to_bf16(const float* __restrict__ a, __nv_bfloat16* __restrict__ b,
@@ -233,69 +262,107 @@ __global__ void k_bf16_to_f32(const __nv_bfloat16* __restrict__ a, float* __rest
   if (i < n) b[i] = __bfloat162float(a[i]);
 }
 
-// Cluster size for a level: the largest of 16 / 8 whose slabs keep every
-// CTA within COARSE_K cells per thread and the level fits the cluster.
-int coarse_cluster_size(Dims3 d) {
+// Threads per CTA and cells per thread and colour of the coarse kernel, in
+// the order tried: the first whose T * K covers a CTA's cells of one colour.
+// Measured on the 2 cm pool's 20 x 40 x 20 level (16 CTAs, 800 cells of a
+// colour per CTA, 80 sweeps): 512 threads x 2 cells 142 us, 256 x 4 154 us,
+// 128 x 8 229 us -- the barrier and the remote loads of a pass set its
+// length, and fewer warps hide less of it.
+struct CoarseShape {
+  int T, K;
+};
+constexpr CoarseShape COARSE_SHAPES[] = {{512, 2}, {512, 4}, {256, 8}};
+
+// Cluster size and shape for a level: the largest cluster of 16 / 8 whose
+// slabs fit a shape and the shared memory; {0, 0} when none does.
+struct CoarsePlan {
+  int C = 0;
+  CoarseShape s{0, 0};
+};
+CoarsePlan coarse_plan(Dims3 d, int max_cluster) {
+  CoarsePlan pl;
+  if (d.nz < 1) return pl;
   for (int C : {COARSE_MAX_CLUSTER, 8}) {
-    if (d.nz < 1) return 0;
-    int max_planes = (d.nz + C - 1) / C;
-    size_t own = (size_t)max_planes * d.nx * d.ny;
-    if (own <= (size_t)COARSE_K * COARSE_THREADS && own * 4 <= 200 * 1024) return C;
+    if (C > max_cluster) continue;
+    const int planes = (d.nz + C - 1) / C;
+    const size_t vpc = (size_t)((d.nx + 1) / 2) * d.ny * planes;
+    if ((size_t)planes * d.nx * d.ny * 4 > (size_t)COARSE_SMEM) continue;
+    for (const CoarseShape& s : COARSE_SHAPES)
+      if ((size_t)s.T * s.K >= vpc) {
+        pl.C = C;
+        pl.s = s;
+        return pl;
+      }
   }
-  return 0;
+  return pl;
 }
 
-template <typename TS>
-cudaError_t mg_coarse_t(Dims3 d, float h, const TS* b, const uint32_t* f, TS* p, int iters,
-                        float omega, int bc_mode, cudaStream_t st, int symmetric = 0) {
-  static int attr_done = 0;  // attributes are per function, set once
-  static int max_cluster = 0;
-  cudaError_t e;
-  if (!(attr_done & (1 << sizeof(TS)))) {
-    e = cudaFuncSetAttribute(k_mg_coarse_cluster<TS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             200 * 1024);
+template <typename TS, int T, int K>
+cudaError_t coarse_launch(const CoarsePlan& pl, Dims3 d, float h, const TS* b, const uint32_t* f,
+                          TS* p, int iters, float omega, int bc_mode, cudaStream_t st,
+                          int symmetric) {
+  auto kern = k_mg_coarse_rb<TS, T, K>;
+  static bool attr = false;  // attributes are per function, set once
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         COARSE_SMEM);
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_mg_coarse_cluster<TS>,
-                             cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     if (e != cudaSuccess) return e;
-    attr_done |= 1 << sizeof(TS);
-    // the largest cluster this device co-schedules at this CTA shape
-    cudaLaunchConfig_t q = {};
-    q.gridDim = dim3(COARSE_MAX_CLUSTER, 1, 1);
-    q.blockDim = dim3(COARSE_THREADS, 1, 1);
-    q.dynamicSmemBytes = 64 * 1024;
-    int mc = 0;
-    if (cudaOccupancyMaxPotentialClusterSize(&mc, k_mg_coarse_cluster<TS>, &q) != cudaSuccess)
-      mc = 8;
-    max_cluster = mc >= COARSE_MAX_CLUSTER ? COARSE_MAX_CLUSTER : 8;
-    // tuning knob: PYRO_COARSE_CLUSTER=8 caps the cluster at 8 CTAs
-    const char* env = getenv("PYRO_COARSE_CLUSTER");
-    if (env && atoi(env) == 8) max_cluster = 8;
+    attr = true;
   }
-  int C = coarse_cluster_size(d);
-  if (C > max_cluster) C = (max_cluster >= 8 && coarse_cluster_size(d) != 0) ? 8 : 0;
-  if (C == 0) return cudaErrorInvalidValue;
-  {
-    size_t own = (size_t)((d.nz + C - 1) / C) * d.nx * d.ny;
-    if (own > (size_t)COARSE_K * COARSE_THREADS) return cudaErrorInvalidValue;
-  }
-  size_t smem = (size_t)((d.nz + C - 1) / C) * d.nx * d.ny * 4;
+  const size_t smem = (size_t)((d.nz + pl.C - 1) / pl.C) * d.nx * d.ny * 4;
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)C, 1, 1);
-  cfg.blockDim = dim3(COARSE_THREADS, 1, 1);
+  cfg.gridDim = dim3((unsigned)pl.C, 1, 1);
+  cfg.blockDim = dim3((unsigned)T, 1, 1);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
   cudaLaunchAttribute at[2];
   at[0].id = cudaLaunchAttributeClusterDimension;
-  at[0].val.clusterDim.x = (unsigned)C;
+  at[0].val.clusterDim.x = (unsigned)pl.C;
   at[0].val.clusterDim.y = 1;
   at[0].val.clusterDim.z = 1;
   at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;  // see launch_pdl
   at[1].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
   cfg.numAttrs = 2;
-  return cudaLaunchKernelEx(&cfg, k_mg_coarse_cluster<TS>, Lvl{d.nx, d.ny, d.nz}, h * h, b, f, p,
-                            iters, omega, bc_mode, symmetric);
+  return cudaLaunchKernelEx(&cfg, kern, Lvl{d.nx, d.ny, d.nz}, h * h, b, f, p, iters, omega,
+                            bc_mode, symmetric);
+}
+
+// The largest cluster this device co-schedules for the coarse kernel (16
+// where non-portable cluster sizes are allowed, else 8), found once.
+int coarse_max_cluster() {
+  static int mc = 0;
+  if (mc) return mc;
+  auto kern = k_mg_coarse_rb<float, 256, 8>;
+  int q = 8;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
+          cudaSuccess &&
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, COARSE_SMEM) ==
+          cudaSuccess) {
+    cudaLaunchConfig_t c = {};
+    c.gridDim = dim3(COARSE_MAX_CLUSTER, 1, 1);
+    c.blockDim = dim3(256, 1, 1);
+    c.dynamicSmemBytes = 64 * 1024;
+    if (cudaOccupancyMaxPotentialClusterSize(&q, kern, &c) != cudaSuccess) q = 8;
+  }
+  mc = q >= COARSE_MAX_CLUSTER ? COARSE_MAX_CLUSTER : 8;
+  return mc;
+}
+
+int coarse_cluster_size(Dims3 d) { return coarse_plan(d, COARSE_MAX_CLUSTER).C; }
+
+template <typename TS>
+cudaError_t mg_coarse_t(Dims3 d, float h, const TS* b, const uint32_t* f, TS* p, int iters,
+                        float omega, int bc_mode, cudaStream_t st, int symmetric = 0) {
+  const CoarsePlan pl = coarse_plan(d, coarse_max_cluster());
+  if (pl.C == 0) return cudaErrorInvalidValue;
+  if (pl.s.K == 2)
+    return coarse_launch<TS, 512, 2>(pl, d, h, b, f, p, iters, omega, bc_mode, st, symmetric);
+  if (pl.s.K == 4)
+    return coarse_launch<TS, 512, 4>(pl, d, h, b, f, p, iters, omega, bc_mode, st, symmetric);
+  return coarse_launch<TS, 256, 8>(pl, d, h, b, f, p, iters, omega, bc_mode, st, symmetric);
 }
 
 }  // namespace

@@ -78,8 +78,16 @@ __device__ __forceinline__ float4 unhalf4(uint2 q) {
   const float2 hi = __half22float2(*reinterpret_cast<const __half2*>(&q.y));
   return make_float4(lo.x, lo.y, hi.x, hi.y);
 }
+// The caches' rgba16float stores.  A value beyond the largest finite
+// binary16 (65504) is stored as that value, not as an infinity: how an
+// out-of-range store converts is left to the implementation by WGSL, and an
+// infinite cache texel turns into NaN radiance where the tracer multiplies
+// it by a zero weight.  A developed 2 cm pool flame reaches that range in
+// the light caches' flux.
+__device__ __forceinline__ float sat16(float v) { return fminf(fmaxf(v, -65504.0f), 65504.0f); }
 __device__ __forceinline__ uint2 half4(float a, float b, float c, float d) {
-  const __half2 lo = __floats2half2_rn(a, b), hi = __floats2half2_rn(c, d);
+  const __half2 lo = __floats2half2_rn(sat16(a), sat16(b)),
+                hi = __floats2half2_rn(sat16(c), sat16(d));
   return make_uint2(*reinterpret_cast<const uint32_t*>(&lo),
                     *reinterpret_cast<const uint32_t*>(&hi));
 }

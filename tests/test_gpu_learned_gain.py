@@ -1,9 +1,15 @@
-"""What the trained learned stage (pyro_b200/weights/warmstart.pnet) gains
-on a pressure system it was not trained on: the 2 cm pool fire at t = 1 s
-(the training pairs come from t >= 5 s of the same scene and from the
-pallet and bonfire scenes).  The same system is solved to a relative
-residual of 1e-4 from a zero guess by BF16 MGPCG with and without the
-learned warm start."""
+"""What the trained learned stage (pyro_b200/weights/warmstart.pnet) does on
+a pressure system it was not trained on: the 2 cm pool fire at t = 1 s (the
+training pairs come from t >= 5 s of the same scene and from the pallet and
+bonfire scenes).  The same system is solved to a relative residual of 1e-4
+from a zero guess by BF16 MGPCG with and without the learned warm start.
+
+The stage removes most of the initial residual (it is kept, and the
+residual after it is below 0.35 of the start), but the CG iterations from
+there are not fewer than from zero: the V-cycle preconditioner removes the
+same high-frequency error in its first application.  So the learned mode
+costs the network's forward pass and saves nothing; the solver keeps it
+off by default, and this test pins the measured behaviour, not a gain."""
 import json
 import os
 
@@ -22,7 +28,7 @@ ROOT = os.path.dirname(HERE)
 WEIGHTS = os.path.join(ROOT, "pyro_b200", "weights", "warmstart.pnet")
 
 
-def test_learned_warm_start_gain():
+def test_learned_stage_cuts_the_initial_residual_but_not_the_iterations():
     require_cuda()
     from pyro_b200.pairs import collect
     pair = next(collect(os.path.join(ROOT, "pyro_b200", "scenes", "pool_2cm.toml"), 1, every=1,
@@ -51,7 +57,7 @@ def test_learned_warm_start_gain():
     # the stage is kept and removes most of the initial residual
     assert w["learned"] == 1
     assert w["resid_after_learned"] <= 0.35, w
-    # CG from there needs no more iterations than from zero (plus one)
-    assert w["iterations"] <= wo["iterations"] + 1
+    # CG from there needs about as many iterations as from zero
+    assert abs(w["iterations"] - wo["iterations"]) <= 1, (w, wo)
     ps.set_net(None)
     ps.close()
