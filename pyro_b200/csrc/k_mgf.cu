@@ -587,194 +587,29 @@ __global__ void __launch_bounds__(256) k_mg_restrict_t(L df, const TS* __restric
   stv(pc + J, 0.0f);
 }
 
-// The transfers two coarse cells at a time, for fine rows of a multiple of 4
-// cells (so the coarse rows have an even length): thread (tx, Y, Z) takes
-// the coarse pair X0 = 2 tx, X0 + 1 and the four fine cells 4 tx .. 4 tx + 3
-// of each of its fine rows, as one vector access per row.  Per fine cell and
-// per coarse cell the arithmetic and its order are those of the one-cell
-// kernels above (and of the reference), so the results are the same bit for
-// bit; the neighbouring cells' values are loaded once for the pair.
-
-// Prolongation: the coarse columns X0 - 1 .. X0 + 2 (clamped) of the 3 x 3
-// coarse rows around (Y, Z); fine cell 4 tx + sx (a child of coarse cell
-// X0 + sx / 2 on side s = sx % 2) takes the window's columns
-// sx / 2 + s + o, o = 0, 1, with the weights of k_mg_prolong_m.
-template <typename TS>
-__global__ void __launch_bounds__(256) k_mg_prolong_x2(L df, const TS* __restrict__ pc,
-                                                       const uint8_t* __restrict__ mf,
-                                                       TS* __restrict__ pf, L dc,
-                                                       const uint8_t* __restrict__ mc) {
-  pdl_trigger();
-  pdl_wait();
-  const int tx = blockIdx.x * 32 + threadIdx.x;
-  const int Y = blockIdx.y * 4 + threadIdx.y;
-  const int Z = blockIdx.z * 2 + threadIdx.z;
-  const int X0 = 2 * tx;
-  if (X0 >= dc.nx || Y >= dc.ny || Z >= dc.nz) return;
-  int cx[4], cy[3], cz[3];
-#pragma unroll
-  for (int q = 0; q < 4; q++) cx[q] = min(max(X0 - 1 + q, 0), dc.nx - 1);
-#pragma unroll
-  for (int q = 0; q < 3; q++) {
-    cy[q] = min(max(Y - 1 + q, 0), dc.ny - 1) * dc.nx;
-    cz[q] = min(max(Z - 1 + q, 0), dc.nz - 1) * (dc.nx * dc.ny);
-  }
-  float cv[36];  // [z][y][x], x fastest (4 columns)
-  uint64_t solid = 0;
-#pragma unroll
-  for (int q = 0; q < 36; q++) {
-    const int j = cx[q & 3] + cy[(q >> 2) % 3] + cz[q / 12];
-    const float raw = ldv(pc + j);
-    const bool s = (__ldg(mc + j) & META_SOLID) != 0;
-    solid |= (uint64_t)s << q;
-    cv[q] = s ? 0.0f : raw;
-  }
-  const int fx = 4 * tx;
-#pragma unroll
-  for (int sz = 0; sz < 2; sz++) {
-    const int fz = 2 * Z + sz;
-    if (fz >= df.nz) break;
-#pragma unroll
-    for (int sy = 0; sy < 2; sy++) {
-      const int fy = 2 * Y + sy;
-      if (fy >= df.ny) break;
-      const int i = df.idx(fx, fy, fz);
-      const uint32_t m4 = *reinterpret_cast<const uint32_t*>(mf + i);
-      if ((m4 & 0x40404040u) == 0x40404040u) continue;
-      float4 P = ld4(pf + i);
-      float pv[4] = {P.x, P.y, P.z, P.w};
-#pragma unroll
-      for (int sx = 0; sx < 4; sx++) {
-        if ((m4 >> (8 * sx)) & META_SOLID) continue;
-        const int s = sx & 1, base = (sx >> 1) + s;
-        float acc = 0.0f, ws = 0.0f;
-        bool any_solid = false;
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-          const int ox = k & 1, oy = (k >> 1) & 1, oz = (k >> 2) & 1;
-          const int q = (base + ox) + 4 * (sy + oy) + 12 * (sz + oz);
-          any_solid |= ((solid >> q) & 1u) != 0;
-        }
-        if (!any_solid) {
-          // no solid coarse neighbour: the eight weights are multiples of
-          // 1/64 that sum to exactly 1, so acc / ws is acc itself
-#pragma unroll
-          for (int k = 0; k < 8; k++) {
-            const int ox = k & 1, oy = (k >> 1) & 1, oz = (k >> 2) & 1;
-            const int q = (base + ox) + 4 * (sy + oy) + 12 * (sz + oz);
-            const float w = (s != ox ? 0.75f : 0.25f) * (sy != oy ? 0.75f : 0.25f) *
-                            (sz != oz ? 0.75f : 0.25f);
-            acc += w * cv[q];
-          }
-          pv[sx] = pv[sx] + acc;
-          continue;
-        }
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-          const int ox = k & 1, oy = (k >> 1) & 1, oz = (k >> 2) & 1;
-          const int q = (base + ox) + 4 * (sy + oy) + 12 * (sz + oz);
-          if ((solid >> q) & 1u) continue;
-          const float w = (s != ox ? 0.75f : 0.25f) * (sy != oy ? 0.75f : 0.25f) *
-                          (sz != oz ? 0.75f : 0.25f);
-          acc += w * cv[q];
-          ws += w;
-        }
-        if (ws > 1e-4f) pv[sx] = pv[sx] + acc / ws;
-      }
-      st4(pf + i, make_float4(pv[0], pv[1], pv[2], pv[3]));
-    }
-  }
-}
-
-// Restriction: the residual of each of the four fine cells of a row with
-// the neighbour order and Dirichlet faces of k_mg_restrict_m, summed into
-// coarse cell X0 (fine cells 0, 1) and X0 + 1 (fine cells 2, 3) in the
-// reference's child order.
-template <typename TS>
-__global__ void __launch_bounds__(256) k_mg_restrict_x2(L df, float h2, const TS* __restrict__ pf,
-                                                        const TS* __restrict__ bf,
-                                                        const uint8_t* __restrict__ mf, L dc,
-                                                        TS* __restrict__ bc, TS* __restrict__ pc,
-                                                        int bc_mode) {
-  pdl_trigger();
-  pdl_wait();
-  const int tx = blockIdx.x * 32 + threadIdx.x;
-  const int Y = blockIdx.y * 4 + threadIdx.y;
-  const int Z = blockIdx.z * 2 + threadIdx.z;
-  const int X0 = 2 * tx;
-  if (X0 >= dc.nx || Y >= dc.ny || Z >= dc.nz) return;
-  const int sy = df.nx, sz = df.nx * df.ny;
-  const int fx = 4 * tx;
-  const bool open = bc_mode == 0;
-  float r[2] = {0.0f, 0.0f}, nfl[2] = {0.0f, 0.0f};
-  const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-  for (int s_z = 0; s_z < 2; s_z++) {
-    const int fz = 2 * Z + s_z;
-    if (fz >= df.nz) break;
-#pragma unroll
-    for (int s_y = 0; s_y < 2; s_y++) {
-      const int fy = 2 * Y + s_y;
-      if (fy >= df.ny) break;
-      const int i = df.idx(fx, fy, fz);
-      // the row's loads are issued together, none waiting for the masks
-      const float4 P = ld4(pf + i), B = ld4(bf + i);
-      const float4 Yp = fy + 1 < df.ny ? ld4(pf + i + sy) : zero;
-      const float4 Ym = fy > 0 ? ld4(pf + i - sy) : zero;
-      const float4 Zp = fz + 1 < df.nz ? ld4(pf + i + sz) : zero;
-      const float4 Zm = fz > 0 ? ld4(pf + i - sz) : zero;
-      const float pl = fx > 0 ? ldv(pf + i - 1) : 0.0f;
-      const float pr = fx + 4 < df.nx ? ldv(pf + i + 4) : 0.0f;
-      const uint32_t m4 = *reinterpret_cast<const uint32_t*>(mf + i);
-      if ((m4 & 0x40404040u) == 0x40404040u) continue;
-      const int dyz = (fy == df.ny - 1) + (open ? (fz == 0) + (fz == df.nz - 1) : 0);
-      const float pv[6] = {pl, P.x, P.y, P.z, P.w, pr};
-      const float bv[4] = {B.x, B.y, B.z, B.w};
-      const float yp[4] = {Yp.x, Yp.y, Yp.z, Yp.w}, ym[4] = {Ym.x, Ym.y, Ym.z, Ym.w};
-      const float zp[4] = {Zp.x, Zp.y, Zp.z, Zp.w}, zm[4] = {Zm.x, Zm.y, Zm.z, Zm.w};
-#pragma unroll
-      for (int k = 0; k < 4; k++) {
-        const uint32_t m = (m4 >> (8 * k)) & 0xFFu;
-        if (m & META_SOLID) continue;
-        nfl[k >> 1] += 1.0f;
-        float sum = 0.0f;
-        if (m & 1u) sum += pv[k + 2];
-        if (m & 2u) sum += pv[k];
-        if (m & 4u) sum += yp[k];
-        if (m & 8u) sum += ym[k];
-        if (m & 16u) sum += zp[k];
-        if (m & 32u) sum += zm[k];
-        const int dx = open ? (fx + k == 0) + (fx + k == df.nx - 1) : 0;
-        const float cnt = (float)(__popc(m & 63u) + dyz + dx);
-        r[k >> 1] += bv[k] - (sum - cnt * pv[k + 1]) / h2;
-      }
-    }
-  }
-  const int ci = dc.idx(X0, Y, Z);
-  // eight fluid children: dividing by 8 is the exact product with 1/8
-  float2 out;
-  out.x = nfl[0] == 8.0f ? r[0] * 0.125f : (nfl[0] > 0.0f) ? r[0] / fmaxf(nfl[0], 1.0f) : 0.0f;
-  out.y = nfl[1] == 8.0f ? r[1] * 0.125f : (nfl[1] > 0.0f) ? r[1] / fmaxf(nfl[1], 1.0f) : 0.0f;
-  st2(bc + ci, out);
-  st2(pc + ci, make_float2(0.0f, 0.0f));
-}
-
 inline dim3 g3(Dims3 d) { return dim3((d.nx + 31) / 32, (d.ny + 3) / 4, (d.nz + 1) / 2); }
-// one thread per coarse pair in x
-inline dim3 g3x2(Dims3 d) { return dim3((d.nx / 2 + 31) / 32, (d.ny + 3) / 4, (d.nz + 1) / 2); }
 
 }  // namespace
 
-constexpr int PASS_ZT = 2;  // planes per thread of k_mg_pass4z
+// Planes per thread of k_mg_pass4z: 2, and 4 on levels of at least
+// PASS_ZT4_CELLS cells (measured on the 2 cm pool: level-0 passes 0.677 ms
+// per substep with 2 planes, 0.662 with 4; the 1 M and 128 k cell levels
+// lose with 4, their grids get too small).
+constexpr int PASS_ZT = 2;
+constexpr size_t PASS_ZT4_CELLS = 4u << 20;
 
-inline dim3 pass4z_grid(Dims3 d) {
+inline dim3 pass4z_grid(Dims3 d, int zt = PASS_ZT) {
   return dim3((unsigned)((d.nx / 4 + 7) / 8), (unsigned)((d.ny + 15) / 16),
-              (unsigned)((d.nz + PASS_ZT - 1) / PASS_ZT));
+              (unsigned)((d.nz + zt - 1) / zt));
 }
 
 template <typename TS>
 cudaError_t pass_t(Dims3 d, float h, const TS* b, const uint8_t* meta, TS* p, int color,
                    float omega, int bc_mode, cudaStream_t st) {
+  if (d.nx % 4 == 0 && d.cells() >= PASS_ZT4_CELLS)
+    return launch_pdl(k_mg_pass4z<TS, 4, PASS>, pass4z_grid(d, 4), dim3(8, 16), 0, st,
+                      L{d.nx, d.ny, d.nz}, h * h, const_cast<TS*>(b), meta, p, color, omega,
+                      bc_mode, (const float*)nullptr, (float*)nullptr);
   if (d.nx % 4 == 0)
     return launch_pdl(k_mg_pass4z<TS, PASS_ZT, PASS>, pass4z_grid(d), dim3(8, 16), 0, st,
                       L{d.nx, d.ny, d.nz}, h * h, const_cast<TS*>(b), meta, p, color, omega,
@@ -813,10 +648,6 @@ cudaError_t launch_mg_pass_last_f32(Dims3 d, float h, const void* b, const uint8
 template <typename TS>
 cudaError_t restrict_t(Dims3 df, float h, const TS* pf, const TS* bf, const uint8_t* mf,
                        Dims3 dc, TS* bc, TS* pc, int bc_mode, cudaStream_t st) {
-  if (df.nx % 4 == 0)
-    return launch_pdl(k_mg_restrict_x2<TS>, g3x2(dc), dim3(32, 4, 2), 0, st,
-                      L{df.nx, df.ny, df.nz}, h * h, pf, bf, mf, L{dc.nx, dc.ny, dc.nz}, bc, pc,
-                      bc_mode);
   auto kern = df.nx % 2 == 0 ? k_mg_restrict_m<TS, true> : k_mg_restrict_m<TS, false>;
   return launch_pdl(kern, g3(dc), dim3(32, 4, 2), 0, st, L{df.nx, df.ny, df.nz}, h * h, pf, bf,
                     mf, L{dc.nx, dc.ny, dc.nz}, bc, pc, bc_mode);
@@ -881,9 +712,6 @@ cudaError_t launch_mg_flags_down(Dims3 df, const uint32_t* ff, Dims3 dc, uint32_
 template <typename TS>
 cudaError_t prolong_t(Dims3 df, const TS* pc, const uint8_t* mf, TS* pf, Dims3 dc,
                       const uint8_t* mc, cudaStream_t st) {
-  if (df.nx % 4 == 0)
-    return launch_pdl(k_mg_prolong_x2<TS>, g3x2(dc), dim3(32, 4, 2), 0, st,
-                      L{df.nx, df.ny, df.nz}, pc, mf, pf, L{dc.nx, dc.ny, dc.nz}, mc);
   auto kern = df.nx % 2 == 0 ? k_mg_prolong_m<TS, true> : k_mg_prolong_m<TS, false>;
   return launch_pdl(kern, g3(dc), dim3(32, 4, 2), 0, st, L{df.nx, df.ny, df.nz}, pc, mf, pf,
                     L{dc.nx, dc.ny, dc.nz}, mc);

@@ -86,3 +86,44 @@ class PoissonSolver:
             self.close()
         except Exception:
             pass
+
+
+MODES = {"vcycle": _abi.SOLVER_VCYCLE, "vcycle_tol": _abi.SOLVER_VCYCLE_TOL,
+         "mgpcg": _abi.SOLVER_MGPCG, "mgpcg_bf16": _abi.SOLVER_MGPCG_BF16}
+
+
+def main(argv=None) -> None:
+    """Solve the seeded n^3 case on cuda:0 and print one JSON line: the
+    iterations, relative residual and device time of the last of `reps`
+    solves from a zero guess (a small, fixed case for profilers)."""
+    import argparse
+    import json
+
+    import torch
+    ap = argparse.ArgumentParser(prog="pyro_b200.poisson",
+                                 description="Solve the seeded n^3 Poisson case on cuda:0.")
+    ap.add_argument("--n", type=int, default=128, help="cells per edge")
+    ap.add_argument("--h", type=float, default=0.02)
+    ap.add_argument("--mode", choices=sorted(MODES), default="vcycle")
+    ap.add_argument("--tol", type=float, default=1e-4)
+    ap.add_argument("--iters", type=int, default=1, help="V-cycles, or CG iterations at most")
+    ap.add_argument("--reps", type=int, default=2)
+    a = ap.parse_args(argv)
+    f, b = poisson_case(a.n, a.n, a.n, seed=1)
+    fd, bd = torch.from_numpy(f).cuda(), torch.from_numpy(b).cuda()
+    ps = PoissonSolver((a.n, a.n, a.n), a.h, 0)
+    ps.set_flags(fd.data_ptr())
+    phi = torch.zeros_like(bd)
+    for _ in range(a.reps):
+        phi.zero_()
+        torch.cuda.synchronize()
+        info = ps.solve(bd.data_ptr(), phi.data_ptr(), MODES[a.mode], a.tol, a.iters,
+                        allow_cap=True)
+    torch.cuda.synchronize()
+    print(json.dumps({"n": a.n, "mode": a.mode, "iterations": info.iterations,
+                      "rel_resid": info.rel_resid, "ms": info.ms}))
+    ps.close()
+
+
+if __name__ == "__main__":
+    main()

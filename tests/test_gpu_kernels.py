@@ -217,7 +217,8 @@ def _bf16_val(bits):
 
 # the shapes the V-cycle meets: rows of a multiple of 4 cells (the
 # four-cells-per-thread pass, even row pairs in the transfers) and odd rows
-MASK_CASES = MG_CASES + [(64, 40, 24, 3, 0.04), (20, 40, 20, 4, 0.16), (10, 20, 10, 5, 0.32)]
+MASK_CASES = MG_CASES + [(64, 40, 24, 3, 0.04), (20, 40, 20, 4, 0.16), (10, 20, 10, 5, 0.32),
+                         (256, 128, 128, 6, 0.02)]  # >= 4 Mi cells: four planes per thread
 
 
 @pytest.mark.parametrize("nx,ny,nz,seed,h", MASK_CASES)
@@ -269,8 +270,9 @@ def test_mg_mask_kernels_as_the_vcycle_runs_them(lib, nx, ny, nz, seed, h, bc_mo
     assert np.array_equal(host(pd), enc(pf_o))
 
 
+# slabs of one to three planes per CTA of the cluster (nz = 3: three CTAs)
 COARSE_CASES = MG_CASES + [(8, 20, 8, 3, 0.32), (32, 32, 22, 4, 0.2), (20, 40, 20, 5, 0.16),
-                           (16, 30, 16, 6, 0.16), (20, 40, 17, 7, 0.16)]
+                           (16, 30, 16, 6, 0.16), (20, 40, 17, 7, 0.16), (12, 20, 3, 11, 0.3)]
 
 
 @pytest.mark.parametrize("nx,ny,nz,seed,h", COARSE_CASES)
