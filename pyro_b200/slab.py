@@ -342,3 +342,76 @@ class SlabPoisson:
             phi_own.copy_(self._phi[0][s0.z0:s0.z1])
         else:
             phi_own.copy_(self._phi[0][s0.lo:s0.lo + n0])
+
+
+def main(argv=None) -> None:
+    """Under torchrun, one rank per GPU: the seeded Poisson case
+    (pyro_b200.poisson.poisson_case) split into z-slabs, `--cycles`
+    V-cycles timed with CUDA events (max over ranks), and on rank 0 the
+    gathered result compared with the single-GPU V-cycles of the same
+    system.  Prints one JSON line on rank 0."""
+    import argparse
+    import datetime
+    import json
+    import os
+
+    import numpy as np
+
+    from .poisson import PoissonSolver, poisson_case
+    ap = argparse.ArgumentParser(prog="pyro_b200.slab",
+                                 description="z-slab V-cycles across the ranks of torchrun")
+    ap.add_argument("--dims", default="160,320,160")
+    ap.add_argument("--h", type=float, default=0.02)
+    ap.add_argument("--cycles", type=int, default=4)
+    ap.add_argument("--reps", type=int, default=5)
+    a = ap.parse_args(argv)
+    dims = tuple(int(v) for v in a.dims.split(","))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1:
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    rank = dist.get_rank() if dist.is_initialized() else 0
+    f, b, _ = poisson_case(*dims, seed=1)
+    n = dims[2] // world
+    own = slice(rank * n, (rank + 1) * n)
+    sp = SlabPoisson(dims, a.h)
+    sp.set_flags(torch.from_numpy(f[own].view(np.int32).copy()).cuda())
+    bo = torch.from_numpy(b[own].copy()).cuda()
+    phi = torch.zeros_like(bo)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    times = []
+    for _ in range(a.reps):
+        phi.zero_()
+        if dist.is_initialized():
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0.record()
+        sp.vcycles(phi, bo, a.cycles)
+        e1.record()
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    ms = torch.tensor([min(times)], device="cuda")
+    full = sp._gather_own(phi)
+    if dist.is_initialized():
+        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    if rank == 0:
+        ps = PoissonSolver(dims, a.h, 0)
+        fd = torch.from_numpy(f.view(np.int32)).cuda()
+        ps.set_flags(fd.data_ptr())
+        bd = torch.from_numpy(b).cuda()
+        ref = torch.zeros_like(bd)
+        ps.solve(bd.data_ptr(), ref.data_ptr(), _abi.SOLVER_VCYCLE, 0.0, a.cycles,
+                 allow_cap=True)
+        torch.cuda.synchronize()
+        ps.close()
+        print(json.dumps({"dims": dims, "ranks": world, "distributed_levels": sp.lg,
+                          "cycles": a.cycles, "ms": float(ms.item()),
+                          "equal_to_single_gpu": bool(torch.equal(full, ref))}))
+    if dist.is_initialized():
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()
