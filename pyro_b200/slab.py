@@ -372,7 +372,7 @@ def main(argv=None) -> None:
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     rank = dist.get_rank() if dist.is_initialized() else 0
-    f, b, _ = poisson_case(*dims, seed=1)
+    f, b = poisson_case(*dims, seed=1)
     n = dims[2] // world
     own = slice(rank * n, (rank + 1) * n)
     sp = SlabPoisson(dims, a.h)
