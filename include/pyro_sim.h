@@ -506,6 +506,14 @@ int pyro_post_develop(const float* img, uint32_t w, uint32_t h, float gain,
                       float glare, float* scratch, uint8_t* out,
                       float* lin_out, void* stream);
 
+/* q = A p, the pressure operator of the multigrid levels (mg.wgsl:25-35:
+ * (sum of fluid neighbours - count * p) / h^2, Dirichlet faces counted as
+ * bc_mode says), evaluated in FP64 and rounded; 0 in solid cells.  The
+ * operator of CG solvers built on the level kernels.  Asynchronous on
+ * `stream`. */
+int pyro_k_mg_apply(uint32_t nx, uint32_t ny, uint32_t nz, float h,
+                    const uint32_t* flags, const float* p, float* q,
+                    int bc_mode, void* stream);
 /* Coarsest-level solve: `iters` red-black SOR sweeps (omega) in one
  * launch (src/sim.rs:473 runs 80 sweeps at omega 1.6 as 160 dispatches). */
 int pyro_k_mg_coarse(uint32_t nx, uint32_t ny, uint32_t nz, float h,

@@ -214,6 +214,7 @@ SIGNATURES = {
     "pyro_k_mg_prolong_m": [_U32, _U32, _U32, _P, _P, _P, _U32, _U32, _U32, _P, _I, _P],
     "pyro_k_mg_resid": [_U32, _U32, _U32, _F, _P, _P, _P, _P, _P],
     "pyro_k_mg_coarse": [_U32, _U32, _U32, _F, _P, _P, _P, _I, _F, _P],
+    "pyro_k_mg_apply": [_U32, _U32, _U32, _F, _P, _P, _P, _I, _P],
     "pyro_k_mg_coarse_sym": [_U32, _U32, _U32, _F, _P, _P, _P, _I, _F, _I, _P],
     "pyro_k_render_pack": [_P, _U32, _U32, _U32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
     "pyro_k_render_bricks": [_U32, _U32, _U32, _P, _P, _P, _P],

@@ -178,6 +178,23 @@ __global__ void __launch_bounds__(VT) k_apply_dot(Cells c, double ih2, const flo
   block_add_d(sh, pq, sc + SC_PQ);
 }
 
+// q = A p (FP64 evaluation, rounded), 0 in solids.
+__global__ void __launch_bounds__(VT) k_apply(Cells c, double ih2, const float* __restrict__ p,
+                                              const uint32_t* __restrict__ f, int bc_mode,
+                                              float* __restrict__ q) {
+  pdl_trigger();
+  pdl_wait();
+  CELL_LOOP(i) {
+    float qi = 0.0f;
+    if (__ldg(f + i) != 1u) {
+      int x, y, z;
+      c.coords(i, x, y, z);
+      qi = (float)apply_A(c.d, ih2, p, f, x, y, z, bc_mode, __ldg(p + i));
+    }
+    q[i] = qi;
+  }
+}
+
 // phi += alpha p; r -= alpha q; accumulate |r|^2
 __global__ void __launch_bounds__(VT) k_update_xr(Cells c, const uint32_t* __restrict__ f,
                                                   float* __restrict__ phi,
@@ -822,6 +839,12 @@ int Solver::solve(cudaStream_t st, float* phi, const float* b, int mode, float t
   return PYRO_OK;
 }
 
+cudaError_t launch_mg_apply(Dims3 d, float h, const uint32_t* f, const float* p, float* q,
+                            int bc_mode, cudaStream_t st) {
+  return launch_pdl(k_apply, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d),
+                    1.0 / ((double)h * h), p, f, bc_mode, q);
+}
+
 }  // namespace pyro
 
 // ------------------------------------------------------ stand-alone solver
@@ -842,6 +865,18 @@ struct PyroPoisson {
 };
 
 extern "C" {
+
+int pyro_k_mg_apply(uint32_t nx, uint32_t ny, uint32_t nz, float h, const uint32_t* flags,
+                    const float* p, float* q, int bc_mode, void* stream) {
+  clear_error();
+  PYRO_REQUIRE(nx && ny && nz && (size_t)nx * ny * nz < ((size_t)1 << 31),
+               "pyro_k_mg_apply: invalid grid dimensions");
+  PYRO_REQUIRE(flags && p && q && p != q, "pyro_k_mg_apply: null or aliased buffer");
+  PYRO_REQUIRE(bc_mode == 0 || bc_mode == 1, "pyro_k_mg_apply: bc_mode must be 0 or 1");
+  PYRO_CU(launch_mg_apply(Dims3{(int)nx, (int)ny, (int)nz}, h, flags, p, q, bc_mode,
+                          static_cast<cudaStream_t>(stream)));
+  return PYRO_OK;
+}
 
 int pyro_poisson_create(uint32_t nx, uint32_t ny, uint32_t nz, float h, int bc_mode,
                         PyroPoisson** out) {

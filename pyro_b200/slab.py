@@ -163,6 +163,11 @@ class LevelOps:
             *fd, self._p(pc), self._p(mf), self._p(pf), *cd, self._p(mc), _abi.MG_F32,
             self._st()))
 
+    def apply(self, d: Dims, h: float, flags, p, q):
+        """q = A p (pyro_k_mg_apply)."""
+        self._ok("pyro_k_mg_apply", self.lib.pyro_k_mg_apply(
+            *d, h, self._p(flags), self._p(p), self._p(q), self.bc_mode, self._st()))
+
     def coarse(self, d: Dims, h: float, b, flags, meta, phi):
         if self.bc_mode == 0:
             self._ok("pyro_k_mg_coarse", self.lib.pyro_k_mg_coarse(
@@ -300,6 +305,84 @@ class SlabPoisson:
             ops.prolong(self.dims[l], self._phi[l + 1], self._meta[l], self._phi[l],
                         self.dims[l + 1], self._meta[l + 1])
             self._smooth(l, False)
+
+    def _dot(self, a: torch.Tensor, b: torch.Tensor) -> float:
+        """Sum over this rank's fluid cells, all-reduced, in FP64."""
+        v = torch.sum(a.double() * b.double() * self._fluid).reshape(1)
+        if self.world > 1:
+            src = v.cpu() if self._via_host else v
+            dist.all_reduce(src, group=self.group)
+            v = src
+        return float(v.item())
+
+    def mgpcg(self, phi_own: torch.Tensor, b_own: torch.Tensor, tol: float,
+              max_iters: int) -> Tuple[int, float]:
+        """Flexible preconditioned CG (Polak-Ribiere beta) on the slabs:
+        phi_own (the initial guess) is updated in place until
+        |b - A phi| <= tol |b| over the fluid cells or after max_iters
+        iterations.  The operator reads the neighbours' boundary plane of
+        the search direction (one exchange per iteration); the
+        preconditioner is one slab V-cycle from zero; every dot product is
+        this rank's FP64 sum all-reduced across the group.  The fluid cells
+        must reach a Dirichlet face (otherwise the system is singular).
+        Returns (iterations, relative residual)."""
+        if not self._phi:
+            raise RuntimeError("SlabPoisson.mgpcg: set_flags first")
+        ops, s0 = self.ops, self.slabs[0]
+        n0, lo = s0.z1 - s0.z0, s0.lo
+        d0 = s0.local_dims if self.lg else self.dims[0]
+        f0 = self._flags[0]
+        # local extended arrays for the vectors the operator reads
+        if self.lg:
+            own = slice(lo, lo + n0)
+            fl_own = f0[own]
+        else:
+            own = slice(s0.z0, s0.z1)
+            fl_own = f0[own]
+        self._fluid = (fl_own != 1).double()
+        ext = ops.empty(d0, torch.float32)
+        q = ops.empty(d0, torch.float32)
+
+        def apply_own(x_own):
+            """A x on the own planes (x_own: own planes)."""
+            if self.lg:
+                ext[own].copy_(x_own)
+                self._swap(ext, s0, 1)
+            else:
+                ext.copy_(self._gather_own(x_own))
+            ops.apply(d0, self.h[0], f0, ext, q)
+            return q[own].clone()
+
+        r = b_own - apply_own(phi_own)
+        bn = self._dot(b_own, b_own) ** 0.5
+        if bn == 0.0:
+            phi_own.zero_()
+            return 0, 0.0
+        rn = self._dot(r, r) ** 0.5
+        if rn <= tol * bn:
+            return 0, rn / bn
+        z = torch.zeros_like(r)
+        self.vcycles(z, r, 1)
+        p = z.clone()
+        rz = self._dot(r, z)
+        it = 0
+        while it < max_iters:
+            it += 1
+            ap = apply_own(p)
+            alpha = rz / self._dot(p, ap)
+            phi_own.add_(p, alpha=alpha)
+            r_old = r.clone()
+            r.sub_(ap, alpha=alpha)
+            rn = self._dot(r, r) ** 0.5
+            if rn <= tol * bn:
+                break
+            z.zero_()
+            self.vcycles(z, r, 1)
+            rz_new = self._dot(r, z)
+            beta = (rz_new - self._dot(r_old, z)) / rz
+            rz = rz_new
+            p.mul_(beta).add_(z)
+        return it, rn / bn
 
     def vcycles(self, phi_own: torch.Tensor, b_own: torch.Tensor, cycles: int) -> None:
         if not self._phi:

@@ -51,3 +51,28 @@ class OracleOps:
         for _ in range(80):
             for c in (0, 1):
                 self.smooth_pass(d, h, b, meta, phi, c, 1.6)
+
+    def apply(self, d, h, flags, p, q):
+        """q = A p: (sum of fluid neighbours - count p) / h^2 in FP64, the
+        Dirichlet faces counted as mg.wgsl:25-35 does (bc_mode 0: every face
+        but the floor; 1: the top), 0 in solids."""
+        f = _u32(flags).reshape(d[2], d[1], d[0])
+        v = _f32(p).astype(np.float64).reshape(f.shape)
+        fluid = f != 1
+        s = np.zeros_like(v)
+        cnt = np.zeros_like(v)
+        for axis, side in ((2, 1), (2, -1), (1, 1), (1, -1), (0, 1), (0, -1)):
+            nb = np.roll(v, -side, axis=axis)
+            nf = np.roll(fluid, -side, axis=axis)
+            edge = np.zeros(f.shape, bool)
+            idx = [slice(None)] * 3
+            idx[axis] = -1 if side == 1 else 0
+            edge[tuple(idx)] = True
+            floor = axis == 1 and side == -1
+            top = axis == 1 and side == 1
+            dirichlet = edge & (not floor) & (self.bc_mode == 0 or top)
+            inside = ~edge & nf
+            s += np.where(inside, nb, 0.0)
+            cnt += inside + dirichlet
+        out = np.where(fluid, (s - cnt * v) / (float(np.float32(h)) ** 2), 0.0)
+        q.copy_(torch.from_numpy(out.astype(np.float32)))
