@@ -25,3 +25,18 @@ def test_bf16_mgpcg_step_keeps_flame_statistics_within_5_percent():
     assert ref["frames_averaged"] == mix["frames_averaged"] > 0
     for k in ("hrr_w", "burning_rate_kg_m2s", "h50_m"):
         assert ref[k] > 0 and abs(res["drift"][k]) <= 0.05, (k, ref[k], mix[k])
+
+
+def test_learned_warm_start_step_keeps_flame_statistics_within_5_percent():
+    """The same with each CG solve started from the committed network's
+    warm start (BASELINE's large-scene form: BF16 MGPCG + learned stage)."""
+    require_cuda()
+    from pyro_b200.learned import Net
+    weights = os.path.join(os.path.dirname(SCENE), os.pardir, "weights", "warmstart.pnet")
+    sc = Scene.load(SCENE)
+    res = compare(sc, preroll=0.0, duration=6.0, tol=1e-4, net=Net.load(weights))
+    assert res["learned"]
+    ref, mix = res["fp32_vcycle"], res["bf16_mgpcg"]
+    assert ref["frames_averaged"] == mix["frames_averaged"] > 0
+    for k in ("hrr_w", "burning_rate_kg_m2s", "h50_m"):
+        assert ref[k] > 0 and abs(res["drift"][k]) <= 0.05, (k, ref[k], mix[k])
