@@ -47,7 +47,6 @@ def run_mode(scene, mode, tol, preroll, duration, sol=None, max_iters=100, net=N
         sim.set_solver(mode, tol, max_iters)
     t0 = time.time()
     s = run_frames(scene, sim, duration=duration, preroll=preroll)
-    sim.set_net(None)
     sim.close()
     out = {k: float(getattr(s, k)) for k in KEYS}
     out.update(frames=s.frames, frames_averaged=s.frames_averaged, substeps=s.substeps,
