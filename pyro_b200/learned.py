@@ -17,6 +17,7 @@ weights [Cout][27][Cin], then every layer's biases).
 from __future__ import annotations
 
 import ctypes
+import os
 import struct
 from typing import Optional, Tuple
 
@@ -158,10 +159,65 @@ def flops_per_voxel() -> float:
     return f
 
 
+def evaluate(scene_path: str, net: "Net", n_systems: int, every: int, after: float,
+             tol: float = 1e-4) -> dict:
+    """The learned stage on pressure systems of a scene it was not trained
+    on: `n_systems` systems, one every `every` substeps once the time
+    passes the scene's preroll + `after` seconds (later than the training
+    pairs), each solved from zero to `tol` by BF16 MGPCG without and with
+    the stage (warm timing: the second of two solves).  Returns per system
+    the iterations, device ms, the residual after the stage and whether
+    the stage was kept, and the fallback rate (systems where it was
+    discarded)."""
+    import torch
+
+    from . import _abi
+    from .pairs import collect
+    from .poisson import PoissonSolver
+    from .scene import Scene
+    sc = Scene.load(scene_path)
+    rows = []
+    ps = None
+    for pair in collect(scene_path, n_systems, every=every, preroll=sc.output.preroll + after,
+                        refine_iters=1):
+        nz, ny, nx = pair["b"].shape
+        if ps is None:
+            ps = PoissonSolver((nx, ny, nz), pair["h"], bc_mode=0)
+            ps.set_net(net)
+        b = torch.from_numpy(pair["b"]).cuda()
+        ps.set_flags(torch.from_numpy(pair["flags"].astype(np.int32)).cuda().data_ptr())
+        phi = torch.zeros_like(b)
+        row = {"time_s": pair["time"]}
+        for mode, tag in ((_abi.SOLVER_MGPCG_BF16, "without"), (_abi.SOLVER_MGPCG_LEARNED, "with")):
+            for _ in range(2):
+                phi.zero_()
+                torch.cuda.synchronize()
+                info = ps.solve(b.data_ptr(), phi.data_ptr(), mode, tol, 100, allow_cap=True)
+            row[tag] = {"iterations": info.iterations, "ms": round(info.ms, 3),
+                        "rel_resid": info.rel_resid}
+            if tag == "with":
+                row[tag].update(kept=int(info.learned), learned_ms=round(info.learned_ms, 3),
+                                resid_after_stage=info.rel_resid_learned)
+        rows.append(row)
+    if ps is not None:
+        ps.set_net(None)
+        ps.close()
+    kept = [r["with"]["kept"] for r in rows]
+    return {"scene": os.path.basename(scene_path), "systems": rows,
+            "fallback_rate": 1.0 - sum(kept) / max(len(kept), 1),
+            "mean_iterations": {t: sum(r[t]["iterations"] for r in rows) / max(len(rows), 1)
+                                for t in ("without", "with")},
+            "mean_ms": {t: sum(r[t]["ms"] for r in rows) / max(len(rows), 1)
+                        for t in ("without", "with")}}
+
+
 def main(argv=None) -> int:
     """python -m pyro_b200.learned bench [--dims NX,NY,NZ] [--reps N]
     [--weights FILE]: device time of the network's forward pass on a seeded
-    Poisson right-hand side."""
+    Poisson right-hand side.
+    python -m pyro_b200.learned eval SCENE.toml ... [--systems N] [--every K]
+    [--after S] [--weights FILE]: the learned stage on held-out pressure
+    systems of each scene (evaluate)."""
     import argparse
     import json
 
@@ -169,11 +225,22 @@ def main(argv=None) -> int:
 
     from .poisson import poisson_case
     ap = argparse.ArgumentParser(prog="pyro_b200.learned")
-    ap.add_argument("cmd", choices=["bench"])
+    ap.add_argument("cmd", choices=["bench", "eval"])
+    ap.add_argument("scenes", nargs="*")
     ap.add_argument("--dims", default="160,320,160")
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--weights")
+    ap.add_argument("--systems", type=int, default=4)
+    ap.add_argument("--every", type=int, default=12)
+    ap.add_argument("--after", type=float, default=3.0)
     a = ap.parse_args(argv)
+    if a.cmd == "eval":
+        if not a.weights:
+            ap.error("eval needs --weights")
+        net = Net.load(a.weights)
+        out = [evaluate(sp, net, a.systems, a.every, a.after) for sp in a.scenes]
+        print(json.dumps(out, indent=1))
+        return 0
     nx, ny, nz = (int(v) for v in a.dims.split(","))
     f, b = poisson_case(nx, ny, nz, seed=1)
     net = Net.load(a.weights) if a.weights else Net(seed=0)
