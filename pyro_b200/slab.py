@@ -45,7 +45,7 @@ from __future__ import annotations
 
 import ctypes
 from dataclasses import dataclass
-from typing import List, Optional, Sequence, Tuple
+from typing import List, Optional, Tuple
 
 import torch
 import torch.distributed as dist
@@ -202,6 +202,7 @@ class SlabPoisson:
         self._meta: List[torch.Tensor] = []
         self._phi: List[torch.Tensor] = []
         self._b: List[torch.Tensor] = []
+        self._fluid: Optional[torch.Tensor] = None  # own fluid cells, for the CG dots
         # host staging for groups whose backend cannot move device tensors
         self._via_host = (dist.is_initialized() and dist.get_backend(group) == "gloo")
 
@@ -266,15 +267,13 @@ class SlabPoisson:
             flags.append(ops.flags_down(self.slabs[l - 1].local_dims, flags[-1],
                                         self.slabs[l].local_dims))
         # the gathered levels: level Lg whole, then halved on whole arrays
-        if self.lg < len(self.dims):
-            whole = [self._gather(flags[self.lg], self.slabs[self.lg])]
-            for l in range(self.lg + 1, len(self.dims)):
-                whole.append(ops.flags_down(self.dims[l - 1], whole[-1], self.dims[l]))
+        whole = [self._gather(flags[self.lg], self.slabs[self.lg])]
+        for l in range(self.lg + 1, len(self.dims)):
+            whole.append(ops.flags_down(self.dims[l - 1], whole[-1], self.dims[l]))
         self._flags = flags[:self.lg] + whole
         ld = [s.local_dims for s in self.slabs[:self.lg]] + self.dims[self.lg:]
         self._ld = ld
         self._meta = [ops.meta(d, f) for d, f in zip(ld, self._flags)]
-        self._lgflags_local = flags[self.lg]
         self._lgmeta_local = ops.meta(self.slabs[self.lg].local_dims, flags[self.lg])
         self._phi = [ops.empty(d, torch.float32) for d in ld]
         self._b = [ops.empty(d, torch.float32) for d in ld]
