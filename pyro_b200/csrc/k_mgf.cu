@@ -591,12 +591,15 @@ inline dim3 g3(Dims3 d) { return dim3((d.nx + 31) / 32, (d.ny + 3) / 4, (d.nz + 
 
 }  // namespace
 
-// Planes per thread of k_mg_pass4z: 2, and 4 on levels of at least
-// PASS_ZT4_CELLS cells (measured on the 2 cm pool: level-0 passes 0.677 ms
-// per substep with 2 planes, 0.662 with 4; the 1 M and 128 k cell levels
-// lose with 4, their grids get too small).
+// Planes per thread of k_mg_pass4z: 2; 4 on levels of at least
+// PASS_ZT4_CELLS cells and 1 on levels below PASS_ZT1_CELLS (measured on
+// the 2 cm pool: level-0 passes 0.677 ms per substep with 2 planes, 0.662
+// with 4; the middle levels 0.516 ms with 2 planes, 0.495 with one plane
+// on the 128 k-cell level 2 and 0.497 with one plane on level 1 as well,
+// where the whole substep got slower).
 constexpr int PASS_ZT = 2;
 constexpr size_t PASS_ZT4_CELLS = 4u << 20;
+constexpr size_t PASS_ZT1_CELLS = (size_t)1 << 18;
 
 inline dim3 pass4z_grid(Dims3 d, int zt = PASS_ZT) {
   return dim3((unsigned)((d.nx / 4 + 7) / 8), (unsigned)((d.ny + 15) / 16),
@@ -608,6 +611,10 @@ cudaError_t pass_t(Dims3 d, float h, const TS* b, const uint8_t* meta, TS* p, in
                    float omega, int bc_mode, cudaStream_t st) {
   if (d.nx % 4 == 0 && d.cells() >= PASS_ZT4_CELLS)
     return launch_pdl(k_mg_pass4z<TS, 4, PASS>, pass4z_grid(d, 4), dim3(8, 16), 0, st,
+                      L{d.nx, d.ny, d.nz}, h * h, const_cast<TS*>(b), meta, p, color, omega,
+                      bc_mode, (const float*)nullptr, (float*)nullptr);
+  if (d.nx % 4 == 0 && d.cells() < PASS_ZT1_CELLS)
+    return launch_pdl(k_mg_pass4z<TS, 1, PASS>, pass4z_grid(d, 1), dim3(8, 16), 0, st,
                       L{d.nx, d.ny, d.nz}, h * h, const_cast<TS*>(b), meta, p, color, omega,
                       bc_mode, (const float*)nullptr, (float*)nullptr);
   if (d.nx % 4 == 0)

@@ -216,9 +216,11 @@ def _bf16_val(bits):
 
 
 # the shapes the V-cycle meets: rows of a multiple of 4 cells (the
-# four-cells-per-thread pass, even row pairs in the transfers) and odd rows
+# four-cells-per-thread pass, even row pairs in the transfers) and odd rows;
+# the pass takes one plane per thread below 256 k cells, two up to 4 Mi,
+# four from there
 MASK_CASES = MG_CASES + [(64, 40, 24, 3, 0.04), (20, 40, 20, 4, 0.16), (10, 20, 10, 5, 0.32),
-                         (256, 128, 128, 6, 0.02)]  # >= 4 Mi cells: four planes per thread
+                         (80, 64, 64, 7, 0.04), (256, 128, 128, 6, 0.02)]
 
 
 @pytest.mark.parametrize("nx,ny,nz,seed,h", MASK_CASES)
