@@ -127,6 +127,34 @@ def test_one_substep_matches_oracle_at_the_2cm_pool(lib):
     sim.close()
 
 
+@pytest.mark.parametrize("name,dims,dt", [("pallets_5cm", (128, 240, 128), 1.0 / 90.0),
+                                          ("bonfire_10cm", (160, 240, 160), 1.0 / 60.0)])
+def test_one_substep_matches_oracle_at_the_named_shapes(lib, name, dims, dt):
+    """The other named workloads at full size: the 12-pallet stack at 5 cm
+    (3.9 M cells, wood with char) and the log bonfire at 10 cm (6.1 M cells,
+    wind), each developed on the GPU for 0.5 s and then stepped once on the
+    GPU and in the oracle from the same state."""
+    sc = _scene(name)
+    sim = Sim(sc)
+    assert tuple(sim.dims) == dims
+    dt = np.float32(dt)
+    for k in range(int(round(0.5 / float(dt)))):
+        sim.step(dt, False)
+    sim.sync()
+    assert float(np.abs(sim.read_field(_abi.F_V)).max()) > 0.05
+    o = _copy_to_oracle(sim)
+    t = np.float32(sim.time)
+    sim.step(dt, True)
+    o.step(dt, t, 1.0, True)
+    _compare(sim, o, sim.p, 1e-5, 1e-5, f"{name} step")
+    g = sim.read_stats().raw
+    e = o.read_stats()
+    for i in (0, 1, 2, 3, 6, 7, 8, 9, 10, 11):
+        assert abs(g[i] - e[i]) <= 2e-4 * abs(e[i]) + 1e-12, (i, g[i], e[i])
+    o.close()
+    sim.close()
+
+
 def test_several_substeps_stay_within_drift_budget(lib):
     sc, sim = _developed(steps=40)
     o = _copy_to_oracle(sim)
