@@ -18,9 +18,10 @@ no flush is needed between steps.
 
 One JSON line on stdout (rank 0).  `value` is device time per substep (ms,
 lower is better) from CUDA events on the simulation's stream, max over
-ranks.  `e2e` is the same metric through the public Python API (Sim.step +
-Sim.read_stats every substep: the 576-byte parameter block goes host ->
-device and the 4160-byte statistics block device -> host each substep).
+ranks.  `e2e` is the same metric through the public Python API (Sim.step
+every substep, each substep's statistics read on the host while the next
+one runs with Sim.read_stats_prev: the 576-byte parameter block goes host
+-> device and the 4160-byte statistics block device -> host each substep).
 `roofline` is the dominant single kernel's algorithmic bytes per launch over
 its CUDA-event duration, against the measured HBM copy bandwidth.
 `cpu_baseline` is the CPU oracle (a C++ restatement of the reference's
@@ -557,14 +558,19 @@ def run_ours(args):
     ms = e0.elapsed_time(e1) / args.steps
     log(f"timed {ms:.3f} ms/step")
 
-    # ---- e2e through the public API with a host read every substep
+    # ---- e2e through the public API: every substep uploads its parameters
+    # and brings its statistics back to the host; the host reads substep
+    # k - 1's statistics while substep k runs (Sim.read_stats_prev) and the
+    # last substep's after the loop
     e2 = torch.cuda.Event(enable_timing=True)
     e3 = torch.cuda.Event(enable_timing=True)
     barrier()
     e2.record(stream)
     for k in range(args.steps):
         sim.step(dt, True)
-        st = sim.read_stats()
+        if k:
+            st = sim.read_stats_prev()
+    st = sim.read_stats()
     e3.record(stream)
     e3.synchronize()
     barrier()

@@ -163,6 +163,12 @@ int pyro_sim_step(PyroSim* sim, float dt, float time, float ign_on,
 /* Sim::read_stats raw block (src/sim.rs:510-530): waits for the last
  * stats substep and copies min(n, PYRO_STATS_N) floats. */
 int pyro_sim_read_stats(PyroSim* sim, float* out, size_t n);
+/* The statistics block of the stats substep before the last one: waits
+ * only for that substep's copy, so a host loop can enqueue substep k and
+ * then read the statistics of substep k - 1 while k runs.  Valid until the
+ * next stats substep is enqueued (two copies are kept, used in turn);
+ * PYRO_E_INVALID before the second stats substep. */
+int pyro_sim_read_stats_prev(PyroSim* sim, float* out, size_t n);
 
 /* Sim::read_scalars generalised (src/sim.rs:494-508): blocking copy of one
  * field in the reference layout; `bytes` must equal the field's size. */

@@ -172,6 +172,7 @@ SIGNATURES = {
     "pyro_sim_create": [ctypes.POINTER(PyroParams), _P, _U32, ctypes.POINTER(_P)],
     "pyro_sim_step": [_P, _F, _F, _F, _I],
     "pyro_sim_read_stats": [_P, _P, ctypes.c_size_t],
+    "pyro_sim_read_stats_prev": [_P, _P, ctypes.c_size_t],
     "pyro_sim_read_field": [_P, _I, _P, ctypes.c_size_t],
     "pyro_sim_write_field": [_P, _I, _P, ctypes.c_size_t],
     "pyro_sim_device_ptr": [_P, _I, ctypes.POINTER(_P), ctypes.POINTER(ctypes.c_size_t)],

@@ -589,7 +589,73 @@ __global__ void __launch_bounds__(256) k_mg_restrict_t(L df, const TS* __restric
 
 inline dim3 g3(Dims3 d) { return dim3((d.nx + 31) / 32, (d.ny + 3) / 4, (d.nz + 1) / 2); }
 
+// Residual statistics of level 0 (mg.wgsl:122-158: the sums of r^2 and b^2
+// over the fluid cells, stats slots 10 and 11) from the neighbour masks,
+// for rows of a multiple of 4 cells.  Thread (tx, ty) of block (8, 16)
+// takes the 4-cell chunk 8 blockIdx.x + tx of row 16 blockIdx.y + ty in
+// plane blockIdx.z; phi at x0 - 1 and x0 + 4 comes from the neighbouring
+// lanes of the row.  Per cell r = b - (sum of fluid neighbours - count phi)
+// / h^2 with the neighbours in the reference's order, the same value as
+// k_mg_resid; the thread's four cells and then the block are summed before
+// one atomic per block and slot.
+__global__ void __launch_bounds__(128) k_mg_resid_m(L d, float h2, const float* __restrict__ p,
+                                                    const float* __restrict__ b,
+                                                    const uint8_t* __restrict__ meta,
+                                                    int bc_mode, float* __restrict__ stats) {
+  __shared__ float sh[2 * 32];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int x0 = (blockIdx.x * 8 + tx) * 4, y = blockIdx.y * 16 + ty, z = blockIdx.z;
+  const bool act = x0 < d.nx && y < d.ny;
+  const int sy = d.nx, sz = d.nx * d.ny;
+  const int i0 = act ? (z * d.ny + y) * d.nx + x0 : 0;
+  const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+  const float4 P0 = act ? ld4(p + i0) : zero;
+  float left = __shfl_up_sync(0xffffffffu, P0.w, 1);
+  float right = __shfl_down_sync(0xffffffffu, P0.x, 1);
+  float vals[2] = {0.0f, 0.0f};  // r^2, b^2
+  if (act) {
+    if (tx == 0 && x0 > 0) left = __ldg(p + i0 - 1);
+    if (tx == 7 && x0 + 4 < d.nx) right = __ldg(p + i0 + 4);
+    const float4 B = ld4(b + i0);
+    const uint32_t m4 = *reinterpret_cast<const uint32_t*>(meta + i0);
+    const float4 Yp = y + 1 < d.ny ? ld4(p + i0 + sy) : zero;
+    const float4 Ym = y > 0 ? ld4(p + i0 - sy) : zero;
+    const float4 Zp = z + 1 < d.nz ? ld4(p + i0 + sz) : zero;
+    const float4 Zm = z > 0 ? ld4(p + i0 - sz) : zero;
+    const float pc[6] = {left, P0.x, P0.y, P0.z, P0.w, right};
+    const float yp[4] = {Yp.x, Yp.y, Yp.z, Yp.w}, ym[4] = {Ym.x, Ym.y, Ym.z, Ym.w};
+    const float zp[4] = {Zp.x, Zp.y, Zp.z, Zp.w}, zm[4] = {Zm.x, Zm.y, Zm.z, Zm.w};
+    const float bb[4] = {B.x, B.y, B.z, B.w};
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const uint32_t m = (m4 >> (8 * j)) & 0xFFu;
+      if (m & META_SOLID) continue;
+      float sum = 0.0f;
+      if (m & 1u) sum += pc[j + 2];
+      if (m & 2u) sum += pc[j];
+      if (m & 4u) sum += yp[j];
+      if (m & 8u) sum += ym[j];
+      if (m & 16u) sum += zp[j];
+      if (m & 32u) sum += zm[j];
+      const float cnt = (float)(__popc(m & 63u) + dirichlet_faces(d, x0 + j, y, z, bc_mode));
+      const float r = bb[j] - (sum - cnt * pc[j + 1]) / h2;
+      vals[0] += r * r;
+      vals[1] += bb[j] * bb[j];
+    }
+  }
+  block_stats<2>(sh, vals, stats, {10, 11}, 0u);
+}
+
 }  // namespace
+
+cudaError_t launch_mg_resid_m(Dims3 d, float h, const float* p, const float* b,
+                              const uint8_t* meta, int bc_mode, float* stats, cudaStream_t st) {
+  if (d.nx % 4 != 0) return cudaErrorNotSupported;
+  k_mg_resid_m<<<dim3((unsigned)((d.nx / 4 + 7) / 8), (unsigned)((d.ny + 15) / 16),
+                      (unsigned)d.nz),
+                 dim3(8, 16), 0, st>>>(L{d.nx, d.ny, d.nz}, h * h, p, b, meta, bc_mode, stats);
+  return cudaGetLastError();
+}
 
 // Planes per thread of k_mg_pass4z: 2; 4 on levels of at least
 // PASS_ZT4_CELLS cells and 1 on levels below PASS_ZT1_CELLS (measured on

@@ -105,6 +105,11 @@ cudaError_t launch_post_develop(const float* img, int w, int h, float gain, floa
 
 // Multigrid level kernels (src/shaders/mg.wgsl).  bc_mode 0 = reference
 // boundaries, 1 = Dirichlet on the top face only.
+// The same statistics from the level's neighbour masks, four cells per
+// thread (k_mgf.cu); rows of a multiple of 4 cells, else
+// cudaErrorNotSupported.
+cudaError_t launch_mg_resid_m(Dims3 d, float h, const float* p, const float* b,
+                              const uint8_t* meta, int bc_mode, float* stats, cudaStream_t st);
 cudaError_t launch_mg_resid(Dims3 d, float h, const float* p, const float* b, const uint32_t* f,
                             int bc_mode, float* stats, cudaStream_t st);
 // Whole coarsest-level solve in one CTA (shared memory); returns

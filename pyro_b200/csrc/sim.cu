@@ -54,7 +54,11 @@ struct PyroSim {
   cudaStream_t aux[3] = {};
   cudaEvent_t fork_ev = nullptr, join_ev[3] = {};
   int ring_pos = 0;
-  float* staging = nullptr;  // pinned stats copy
+  // pinned copies of the statistics, two slots used in turn by the steps
+  // that produce statistics, each with the event of its copy
+  float* staging = nullptr;
+  cudaEvent_t staged_ev[2] = {};
+  int stage_next = 0, stage_last = -1, stage_prev = -1;
 
   cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
   int mode = PYRO_SOLVER_VCYCLE;
@@ -75,6 +79,8 @@ struct PyroSim {
     for (auto& a : aux)
       if (a) cudaStreamDestroy(a);
     if (ring) cudaFreeHost(ring);
+    for (auto& e : staged_ev)
+      if (e) cudaEventDestroy(e);
     if (staging) cudaFreeHost(staging);
     if (stream) cudaStreamDestroy(stream);
   }
@@ -138,15 +144,29 @@ struct PyroSim {
     const PyroParams* P = params.as<PyroParams>();
     cudaError_t e;
     if (want_stats) {
-      e = launch_mg_resid(d, p.dx, phi0.as<float>(), b0.as<float>(), flags.as<uint32_t>(), 0,
-                          stats.as<float>(), st);
+      // after the V-cycles the level-0 masks are current (Multigrid::prepare)
+      e = (mode == PYRO_SOLVER_VCYCLE && d.nx % 4 == 0)
+              ? launch_mg_resid_m(d, p.dx, phi0.as<float>(), b0.as<float>(),
+                                  mg.meta[0].as<uint8_t>(), 0, stats.as<float>(), st)
+              : launch_mg_resid(d, p.dx, phi0.as<float>(), b0.as<float>(),
+                                flags.as<uint32_t>(), 0, stats.as<float>(), st);
       if (e != cudaSuccess) return e;
     }
-    e = launch_project(P, d, vp(1 - c, 0), vp(1 - c, 1), vp(1 - c, 2), phi0.as<float>(),
-                       flags.as<uint32_t>(), st);
+    return launch_project(P, d, vp(1 - c, 0), vp(1 - c, 1), vp(1 - c, 2), phi0.as<float>(),
+                          flags.as<uint32_t>(), st);
+  }
+
+  // Copy the substep's statistics into the next staging slot (after the
+  // substep in stream order) and record its event.
+  cudaError_t stage_stats(cudaStream_t st) {
+    const int s = stage_next;
+    cudaError_t e = cudaMemcpyAsync(staging + (size_t)s * PYRO_STATS_N, stats.p,
+                                    PYRO_STATS_N * 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaEventRecord(staged_ev[s], st);
     if (e != cudaSuccess) return e;
-    if (want_stats)
-      return cudaMemcpyAsync(staging, stats.p, PYRO_STATS_N * 4, cudaMemcpyDeviceToHost, st);
+    stage_prev = stage_last;
+    stage_last = s;
+    stage_next = 1 - s;
     return cudaSuccess;
   }
 
@@ -270,11 +290,16 @@ int pyro_sim_create(const PyroParams* params, const float* sol_init, uint32_t pr
   S->mg.bind_level0(S->phi0.as<float>(), S->b0.as<float>(), S->flags.as<uint32_t>());
   if ((rc = S->solver.init(&S->mg)) != PYRO_OK) return fail(rc);
   if (cudaMallocHost(&S->ring, sizeof(PyroParams) * PARAM_RING) != cudaSuccess ||
-      cudaMallocHost(&S->staging, PYRO_STATS_N * 4) != cudaSuccess) {
+      cudaMallocHost(&S->staging, 2 * PYRO_STATS_N * 4) != cudaSuccess) {
     set_error("pyro_sim_create: pinned allocation failed");
     return fail(PYRO_E_NOMEM);
   }
-  std::memset(S->staging, 0, PYRO_STATS_N * 4);
+  std::memset(S->staging, 0, 2 * PYRO_STATS_N * 4);
+  for (auto& e : S->staged_ev)
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+      set_error("pyro_sim_create: cudaEventCreate failed");
+      return fail(PYRO_E_CUDA);
+    }
   for (auto& e : S->ring_ev)
     if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
       set_error("pyro_sim_create: cudaEventCreate failed");
@@ -341,6 +366,7 @@ int pyro_sim_step(PyroSim* S, float dt, float time, float ign_on, int want_stats
     if (rc != PYRO_OK && rc != PYRO_E_NOCONV) return rc;
     PYRO_CU(S->enqueue_post(c, ws, S->stream));
   }
+  if (ws) PYRO_CU(S->stage_stats(S->stream));
   S->cur = 1 - S->cur;
   S->p.frame += 1;
   return PYRO_OK;
@@ -438,6 +464,7 @@ int pyro_sim_profile_step(PyroSim* S, float dt, float time, float ign_on, int wa
   mark();
   if (e == cudaSuccess) e = S->enqueue_post(c, ws, st);
   mark();
+  if (e == cudaSuccess && ws) e = S->stage_stats(st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
     cleanup();
@@ -491,7 +518,19 @@ int pyro_sim_read_stats(PyroSim* S, float* out, size_t n) {
   PYRO_REQUIRE(S && out, "pyro_sim_read_stats: null argument");
   PYRO_CU(cudaStreamSynchronize(S->stream));
   size_t m = n < (size_t)PYRO_STATS_N ? n : (size_t)PYRO_STATS_N;
-  std::memcpy(out, S->staging, m * 4);
+  const int s = S->stage_last < 0 ? 0 : S->stage_last;
+  std::memcpy(out, S->staging + (size_t)s * PYRO_STATS_N, m * 4);
+  return PYRO_OK;
+}
+
+int pyro_sim_read_stats_prev(PyroSim* S, float* out, size_t n) {
+  clear_error();
+  PYRO_REQUIRE(S && out, "pyro_sim_read_stats_prev: null argument");
+  PYRO_REQUIRE(S->stage_prev >= 0,
+               "pyro_sim_read_stats_prev: fewer than two steps with statistics so far");
+  PYRO_CU(cudaEventSynchronize(S->staged_ev[S->stage_prev]));
+  size_t m = n < (size_t)PYRO_STATS_N ? n : (size_t)PYRO_STATS_N;
+  std::memcpy(out, S->staging + (size_t)S->stage_prev * PYRO_STATS_N, m * 4);
   return PYRO_OK;
 }
 

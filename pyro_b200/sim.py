@@ -145,6 +145,14 @@ class Sim:
             self._h, self._stats.ctypes.data_as(ctypes.c_void_p), STATS_N))
         return Stats.decode(self._stats.copy(), self.dims[1])
 
+    def read_stats_prev(self) -> Stats:
+        """Statistics of the stats substep before the last one, waiting only
+        for that substep: enqueue substep k, then read substep k - 1's while
+        k runs (valid until the next stats substep is enqueued)."""
+        _abi.check("pyro_sim_read_stats_prev", self._lib.pyro_sim_read_stats_prev(
+            self._h, self._stats.ctypes.data_as(ctypes.c_void_p), STATS_N))
+        return Stats.decode(self._stats.copy(), self.dims[1])
+
     def read_field(self, which: int) -> np.ndarray:
         nx, ny, nz = self.dims
         if which in (_abi.F_RVOL, _abi.F_RSOL, _abi.F_RVEL):

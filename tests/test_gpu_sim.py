@@ -155,6 +155,26 @@ def test_one_substep_matches_oracle_at_the_named_shapes(lib, name, dims, dt):
     sim.close()
 
 
+def test_statistics_of_the_previous_substep(lib):
+    """Sim.read_stats_prev returns the statistics block of the stats substep
+    before the last one, the same block read_stats gave right after it."""
+    sc, sim = _developed(steps=20)
+    dt = np.float32(0.008)
+    with pytest.raises(Exception):
+        sim.read_stats_prev()  # fewer than two stats substeps
+    sim.step(dt, True)
+    a = sim.read_stats().raw.copy()
+    sim.step(dt, False)
+    sim.step(dt, True)
+    p = sim.read_stats_prev().raw.copy()
+    b = sim.read_stats().raw.copy()
+    assert np.array_equal(p, a)
+    assert not np.array_equal(b, a)
+    sim.step(dt, True)
+    assert np.array_equal(sim.read_stats_prev().raw, b)
+    sim.close()
+
+
 def test_several_substeps_stay_within_drift_budget(lib):
     sc, sim = _developed(steps=40)
     o = _copy_to_oracle(sim)
