@@ -399,6 +399,22 @@ int pyro_k_mg_prolong_m(uint32_t fnx, uint32_t fny, uint32_t fnz,
                         const void* pc, const uint8_t* mf, void* pf,
                         uint32_t cnx, uint32_t cny, uint32_t cnz,
                         const uint8_t* mc, int storage, void* stream);
+/* The fused first and last level-0 passes of the MGPCG preconditioner's
+ * V-cycle (rows of even length; PYRO_E_INVALID otherwise).  pass_first:
+ * the pass of `color` from phi = 0 with the FP32 right-hand side r, every
+ * cell of phi written (cells not updated get 0); with BF16 storage r is
+ * also written rounded to BF16 into bq and used rounded.  pass_last: the
+ * pass of `color` on BF16 phi and b, its result (every cell) written
+ * widened to FP32 into out, phi left as it was.  Each equals the plain
+ * pyro_k_mg_pass on the cleared / converted buffers bit for bit. */
+int pyro_k_mg_pass_first(uint32_t nx, uint32_t ny, uint32_t nz, float h,
+                         const float* r, void* bq, const uint8_t* meta,
+                         void* phi, int color, float omega, int bc_mode,
+                         int storage, void* stream);
+int pyro_k_mg_pass_last(uint32_t nx, uint32_t ny, uint32_t nz, float h,
+                        const void* b, const uint8_t* meta, void* phi,
+                        float* out, int color, float omega, int bc_mode,
+                        void* stream);
 int pyro_k_mg_resid(uint32_t nx, uint32_t ny, uint32_t nz, float h,
                     const float* phi, const float* b, const uint32_t* flags,
                     float* stats, void* stream);

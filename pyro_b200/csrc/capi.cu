@@ -258,6 +258,38 @@ int pyro_k_mg_pass(uint32_t nx, uint32_t ny, uint32_t nz, float h, const void* b
              "pyro_k_mg_pass");
 }
 
+int pyro_k_mg_pass_first(uint32_t nx, uint32_t ny, uint32_t nz, float h, const float* r,
+                         void* bq, const uint8_t* meta, void* phi, int color, float omega,
+                         int bc_mode, int storage, void* stream) {
+  clear_error();
+  PYRO_REQUIRE(dims_ok(nx, ny, nz), "pyro_k_mg_pass_first: invalid grid dimensions");
+  Dims3 d{(int)nx, (int)ny, (int)nz};
+  PYRO_REQUIRE(mg_pass_fused_ok(d), "pyro_k_mg_pass_first: rows of even length only");
+  PYRO_REQUIRE(r && meta && phi && (storage != PYRO_MG_BF16 || bq),
+               "pyro_k_mg_pass_first: null buffer");
+  PYRO_REQUIRE(color == 0 || color == 1, "pyro_k_mg_pass_first: color must be 0 or 1");
+  PYRO_REQUIRE(bc_mode == 0 || bc_mode == 1, "pyro_k_mg_pass_first: bc_mode must be 0 or 1");
+  PYRO_REQUIRE(storage == PYRO_MG_F32 || storage == PYRO_MG_BF16,
+               "pyro_k_mg_pass_first: storage must be PYRO_MG_F32 or PYRO_MG_BF16");
+  return ret(launch_mg_pass_first(d, h, r, bq, meta, phi, color, omega, bc_mode,
+                                  storage == PYRO_MG_BF16, S(stream)),
+             "pyro_k_mg_pass_first");
+}
+
+int pyro_k_mg_pass_last(uint32_t nx, uint32_t ny, uint32_t nz, float h, const void* b,
+                        const uint8_t* meta, void* phi, float* out, int color, float omega,
+                        int bc_mode, void* stream) {
+  clear_error();
+  PYRO_REQUIRE(dims_ok(nx, ny, nz), "pyro_k_mg_pass_last: invalid grid dimensions");
+  Dims3 d{(int)nx, (int)ny, (int)nz};
+  PYRO_REQUIRE(mg_pass_fused_ok(d), "pyro_k_mg_pass_last: rows of even length only");
+  PYRO_REQUIRE(b && meta && phi && out, "pyro_k_mg_pass_last: null buffer");
+  PYRO_REQUIRE(color == 0 || color == 1, "pyro_k_mg_pass_last: color must be 0 or 1");
+  PYRO_REQUIRE(bc_mode == 0 || bc_mode == 1, "pyro_k_mg_pass_last: bc_mode must be 0 or 1");
+  return ret(launch_mg_pass_last_f32(d, h, b, meta, phi, out, color, omega, bc_mode, S(stream)),
+             "pyro_k_mg_pass_last");
+}
+
 int pyro_k_mg_restrict_m(uint32_t fnx, uint32_t fny, uint32_t fnz, float fh, const void* pf,
                          const void* bf, const uint8_t* mf, uint32_t cnx, uint32_t cny,
                          uint32_t cnz, void* bc, void* pc, int bc_mode, int storage,

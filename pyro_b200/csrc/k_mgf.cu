@@ -402,6 +402,108 @@ __global__ void __launch_bounds__(128) k_mg_pass4z(L d, float h2, TS* __restrict
   }
 }
 
+// The same pass for rows of an even length that is not a multiple of 4
+// (a float4 row access would be misaligned there): 2-cell chunks, one cell
+// of the pass's colour in each.  Block (16, 8): thread (tx, ty) takes the
+// chunk 16 blockIdx.x + tx of row y = 8 blockIdx.y + ry, where warp
+// w = ty / 2 holds rows ry = 4 (w / 2) + 2 (ty % 2) + w % 2, two rows of one
+// parity; the ZT-plane window, the modes and the arithmetic are those of
+// k_mg_pass4z.
+template <typename TS>
+__device__ __forceinline__ float2 round_to2(float2 v) {
+  if constexpr (sizeof(TS) == 2) return __bfloat1622float2(__floats2bfloat162_rn(v.x, v.y));
+  return v;
+}
+
+// The cell of a 2-cell chunk with the pass's colour: position 1 when ODD,
+// else 0 (left / right: phi at x0 - 1 and x0 + 2; dir: its Dirichlet
+// faces).
+template <bool ODD>
+__device__ __forceinline__ bool pair_colour(float2& P, const float2 P0, float left, float right,
+                                            const float2 Yp, const float2 Ym, const float2 Zp,
+                                            const float2 Zm, const float2 B, uint32_t m2, int dir,
+                                            float h2, float omega) {
+  const uint32_t m = ODD ? (m2 >> 8) : (m2 & 0xFFu);
+  if (m & META_SOLID) return false;
+  float sum = 0.0f;
+  if (m & 1u) sum += ODD ? right : P0.y;
+  if (m & 2u) sum += ODD ? P0.x : left;
+  if (m & 4u) sum += ODD ? Yp.y : Yp.x;
+  if (m & 8u) sum += ODD ? Ym.y : Ym.x;
+  if (m & 16u) sum += ODD ? Zp.y : Zp.x;
+  if (m & 32u) sum += ODD ? Zm.y : Zm.x;
+  const float cnt = (float)(__popc(m & 63u) + dir);
+  if (cnt < 0.5f) return false;
+  const float v = wmix(ODD ? P0.y : P0.x, (sum - h2 * (ODD ? B.y : B.x)) / cnt, omega);
+  if (ODD) P.y = v; else P.x = v;
+  return true;
+}
+
+template <typename TS, int ZT, int MODE>
+__global__ void __launch_bounds__(128) k_mg_pass2z(L d, float h2, TS* __restrict__ b,
+                                                   const uint8_t* __restrict__ meta,
+                                                   TS* __restrict__ p, int color, float omega,
+                                                   int bc_mode, const float* __restrict__ b32,
+                                                   float* __restrict__ out) {
+  pdl_trigger();
+  pdl_wait();
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int w = ty >> 1;
+  const int y = blockIdx.y * 8 + (w >> 1) * 4 + 2 * (ty & 1) + (w & 1);
+  const int x0 = (blockIdx.x * 16 + tx) * 2;
+  const bool act = x0 < d.nx && y < d.ny;
+  const bool rd = act && MODE != PASS_FIRST;  // phi is read (not the zero guess)
+  const int sy = d.nx, sz = d.nx * d.ny;
+  const int zb = blockIdx.z * ZT;
+  const bool open = bc_mode == 0;
+  const float2 zero = make_float2(0.f, 0.f);
+  int i0 = (zb * d.ny + y) * d.nx + x0;
+  float2 Zm = (rd && zb > 0) ? ld2(p + i0 - sz) : zero;
+  float2 P0 = rd ? ld2(p + i0) : zero;
+  float2 Zp = (rd && zb + 1 < d.nz) ? ld2(p + i0 + sz) : zero;
+  const int dy = (y == d.ny - 1);
+  const int dxa = (open && x0 == 0), dxb = (open && x0 + 2 == d.nx);
+#pragma unroll
+  for (int k = 0; k < ZT; k++) {
+    const int z = zb + k;
+    if (z >= d.nz) break;  // the same in every thread of the block
+    float2 B = zero;
+    if (MODE == PASS_FIRST) {
+      if (act) {
+        B = round_to2<TS>(ld2(b32 + i0));
+        if constexpr (sizeof(TS) == 2) st2(b + i0, B);
+      }
+    } else {
+      B = act ? ld2(b + i0) : zero;
+    }
+    const uint32_t m2 =
+        act ? (uint32_t)*reinterpret_cast<const uint16_t*>(meta + i0) : 0x4040u;
+    const float2 Yp = (rd && y + 1 < d.ny) ? ld2(p + i0 + sy) : zero;
+    const float2 Ym = (rd && y > 0) ? ld2(p + i0 - sy) : zero;
+    const float2 Zn = (rd && k + 1 < ZT && z + 2 < d.nz) ? ld2(p + i0 + 2 * sz) : zero;
+    float left = __shfl_up_sync(0xffffffffu, P0.y, 1);
+    float right = __shfl_down_sync(0xffffffffu, P0.x, 1);
+    if (rd && tx == 0 && x0 > 0) left = ldv(p + i0 - 1);
+    if (rd && tx == 15 && x0 + 2 < d.nx) right = ldv(p + i0 + 2);
+    const int dyz = dy + (open ? (z == 0) + (z == d.nz - 1) : 0);
+    float2 P = P0;
+    const bool odd = ((y + z + color) & 1) != 0;  // the same in every lane of the warp
+    const bool any = odd ? pair_colour<true>(P, P0, left, right, Yp, Ym, Zp, Zm, B, m2,
+                                             dyz + dxb, h2, omega)
+                         : pair_colour<false>(P, P0, left, right, Yp, Ym, Zp, Zm, B, m2,
+                                              dyz + dxa, h2, omega);
+    if (MODE == PASS_LAST_F32) {
+      if (act) *reinterpret_cast<float2*>(out + i0) = round_to2<TS>(P);
+    } else if (act && (any || MODE == PASS_FIRST)) {
+      st2(p + i0, P);
+    }
+    Zm = P0;
+    P0 = Zp;
+    Zp = Zn;
+    i0 += sz;
+  }
+}
+
 // Restriction with the neighbour mask (mg.wgsl:38-83): coarse rhs = mean of
 // the fine residuals of the fluid children, coarse guess 0.
 // One thread per coarse cell; the children are visited in the reference's
@@ -672,27 +774,52 @@ inline dim3 pass4z_grid(Dims3 d, int zt = PASS_ZT) {
               (unsigned)((d.nz + zt - 1) / zt));
 }
 
+// The chunked pass for a level: rows of a multiple of 4 cells take 4-cell
+// chunks (k_mg_pass4z), other even rows 2-cell chunks (k_mg_pass2z); zt
+// planes per thread (1, 2 or 4).
+template <typename TS, int MODE>
+cudaError_t pass_chunked(Dims3 d, float h, TS* b, const uint8_t* meta, TS* p, int color,
+                         float omega, int bc_mode, const float* b32, float* out, int zt,
+                         cudaStream_t st) {
+  const L l{d.nx, d.ny, d.nz};
+  if (d.nx % 4 == 0) {
+    const dim3 g = pass4z_grid(d, zt), blk(8, 16);
+    if (zt == 4)
+      return launch_pdl(k_mg_pass4z<TS, 4, MODE>, g, blk, 0, st, l, h * h, b, meta, p, color,
+                        omega, bc_mode, b32, out);
+    if (zt == 1)
+      return launch_pdl(k_mg_pass4z<TS, 1, MODE>, g, blk, 0, st, l, h * h, b, meta, p, color,
+                        omega, bc_mode, b32, out);
+    return launch_pdl(k_mg_pass4z<TS, 2, MODE>, g, blk, 0, st, l, h * h, b, meta, p, color,
+                      omega, bc_mode, b32, out);
+  }
+  const dim3 g((unsigned)((d.nx / 2 + 15) / 16), (unsigned)((d.ny + 7) / 8),
+               (unsigned)((d.nz + zt - 1) / zt)),
+      blk(16, 8);
+  if (zt == 4)
+    return launch_pdl(k_mg_pass2z<TS, 4, MODE>, g, blk, 0, st, l, h * h, b, meta, p, color,
+                      omega, bc_mode, b32, out);
+  if (zt == 1)
+    return launch_pdl(k_mg_pass2z<TS, 1, MODE>, g, blk, 0, st, l, h * h, b, meta, p, color,
+                      omega, bc_mode, b32, out);
+  return launch_pdl(k_mg_pass2z<TS, 2, MODE>, g, blk, 0, st, l, h * h, b, meta, p, color, omega,
+                    bc_mode, b32, out);
+}
+
 template <typename TS>
 cudaError_t pass_t(Dims3 d, float h, const TS* b, const uint8_t* meta, TS* p, int color,
                    float omega, int bc_mode, cudaStream_t st) {
-  if (d.nx % 4 == 0 && d.cells() >= PASS_ZT4_CELLS)
-    return launch_pdl(k_mg_pass4z<TS, 4, PASS>, pass4z_grid(d, 4), dim3(8, 16), 0, st,
-                      L{d.nx, d.ny, d.nz}, h * h, const_cast<TS*>(b), meta, p, color, omega,
-                      bc_mode, (const float*)nullptr, (float*)nullptr);
-  if (d.nx % 4 == 0 && d.cells() < PASS_ZT1_CELLS)
-    return launch_pdl(k_mg_pass4z<TS, 1, PASS>, pass4z_grid(d, 1), dim3(8, 16), 0, st,
-                      L{d.nx, d.ny, d.nz}, h * h, const_cast<TS*>(b), meta, p, color, omega,
-                      bc_mode, (const float*)nullptr, (float*)nullptr);
-  if (d.nx % 4 == 0)
-    return launch_pdl(k_mg_pass4z<TS, PASS_ZT, PASS>, pass4z_grid(d), dim3(8, 16), 0, st,
-                      L{d.nx, d.ny, d.nz}, h * h, const_cast<TS*>(b), meta, p, color, omega,
-                      bc_mode, (const float*)nullptr, (float*)nullptr);
+  if (d.nx % 2 == 0) {
+    const int zt = d.cells() >= PASS_ZT4_CELLS ? 4 : d.cells() < PASS_ZT1_CELLS ? 1 : PASS_ZT;
+    return pass_chunked<TS, PASS>(d, h, const_cast<TS*>(b), meta, p, color, omega, bc_mode,
+                                  nullptr, nullptr, zt, st);
+  }
   dim3 grid(((d.nx + 1) / 2 + 31) / 32, (d.ny + 3) / 4, (d.nz + 1) / 2);
   return launch_pdl(k_mg_pass<TS>, grid, dim3(32, 4, 2), 0, st, L{d.nx, d.ny, d.nz}, h * h, b,
                     meta, p, color, omega, bc_mode);
 }
 
-bool mg_pass_fused_ok(Dims3 d) { return d.nx % 4 == 0; }
+bool mg_pass_fused_ok(Dims3 d) { return d.nx % 2 == 0; }
 
 cudaError_t launch_mg_pass_first(Dims3 d, float h, const float* r, void* bq,
                                  const uint8_t* meta, void* p, int color, float omega,
@@ -700,13 +827,11 @@ cudaError_t launch_mg_pass_first(Dims3 d, float h, const float* r, void* bq,
   if (!mg_pass_fused_ok(d)) return cudaErrorNotSupported;
   if (bf16) {
     using T = __nv_bfloat16;
-    return launch_pdl(k_mg_pass4z<T, PASS_ZT, PASS_FIRST>, pass4z_grid(d), dim3(8, 16), 0, st,
-                      L{d.nx, d.ny, d.nz}, h * h, (T*)bq, meta, (T*)p, color, omega, bc_mode, r,
-                      (float*)nullptr);
+    return pass_chunked<T, PASS_FIRST>(d, h, (T*)bq, meta, (T*)p, color, omega, bc_mode, r,
+                                       nullptr, PASS_ZT, st);
   }
-  return launch_pdl(k_mg_pass4z<float, PASS_ZT, PASS_FIRST>, pass4z_grid(d), dim3(8, 16), 0, st,
-                    L{d.nx, d.ny, d.nz}, h * h, const_cast<float*>(r), meta, (float*)p, color,
-                    omega, bc_mode, r, (float*)nullptr);
+  return pass_chunked<float, PASS_FIRST>(d, h, const_cast<float*>(r), meta, (float*)p, color,
+                                         omega, bc_mode, r, nullptr, PASS_ZT, st);
 }
 
 cudaError_t launch_mg_pass_last_f32(Dims3 d, float h, const void* b, const uint8_t* meta,
@@ -714,9 +839,8 @@ cudaError_t launch_mg_pass_last_f32(Dims3 d, float h, const void* b, const uint8
                                     cudaStream_t st) {
   if (!mg_pass_fused_ok(d)) return cudaErrorNotSupported;
   using T = __nv_bfloat16;
-  return launch_pdl(k_mg_pass4z<T, PASS_ZT, PASS_LAST_F32>, pass4z_grid(d), dim3(8, 16), 0, st,
-                    L{d.nx, d.ny, d.nz}, h * h, (T*)const_cast<void*>(b), meta, (T*)p, color,
-                    omega, bc_mode, (const float*)nullptr, out);
+  return pass_chunked<T, PASS_LAST_F32>(d, h, (T*)const_cast<void*>(b), meta, (T*)p, color,
+                                        omega, bc_mode, nullptr, out, PASS_ZT, st);
 }
 template <typename TS>
 cudaError_t restrict_t(Dims3 df, float h, const TS* pf, const TS* bf, const uint8_t* mf,

@@ -139,7 +139,7 @@ cudaError_t launch_mg_pass(Dims3 d, float h, const float* b, const uint8_t* meta
 cudaError_t launch_mg_pass_bf16(Dims3 d, float h, const void* b, const uint8_t* meta, void* p,
                                 int color, float omega, int bc_mode, cudaStream_t st);
 // The first and last colour pass on level 0 of the CG preconditioner's
-// V-cycle (k_mg_pass4z, rows of a multiple of 4 cells, mg_pass_fused_ok):
+// V-cycle (k_mg_pass4z / k_mg_pass2z, rows of even length, mg_pass_fused_ok):
 // the first from the zero initial guess with the FP32 right-hand side r
 // (with BF16 storage also written rounded into bq), writing every cell of
 // p; the last on BF16 storage writing every cell widened to FP32 into out.

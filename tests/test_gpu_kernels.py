@@ -215,12 +215,15 @@ def _bf16_val(bits):
     return (bits.astype(np.uint32) << 16).view(np.float32)
 
 
-# the shapes the V-cycle meets: rows of a multiple of 4 cells (the
-# four-cells-per-thread pass, even row pairs in the transfers) and odd rows;
-# the pass takes one plane per thread below 256 k cells, two up to 4 Mi,
-# four from there
+# the shapes the V-cycle meets: rows of a multiple of 4 cells (4-cell
+# chunks in the pass, even row pairs in the transfers), of another even
+# length (2-cell chunks: 10, 38, 150, 130) and odd rows (one cell per
+# thread); the chunked passes take one plane per thread below 256 Ki cells,
+# two up to 4 Mi, four from there
 MASK_CASES = MG_CASES + [(64, 40, 24, 3, 0.04), (20, 40, 20, 4, 0.16), (10, 20, 10, 5, 0.32),
-                         (80, 64, 64, 7, 0.04), (256, 128, 128, 6, 0.02)]
+                         (80, 64, 64, 7, 0.04), (256, 128, 128, 6, 0.02),
+                         (38, 40, 20, 8, 0.16), (150, 96, 24, 9, 0.02),
+                         (130, 256, 128, 10, 0.02)]
 
 
 @pytest.mark.parametrize("nx,ny,nz,seed,h", MASK_CASES)
@@ -270,6 +273,58 @@ def test_mg_mask_kernels_as_the_vcycle_runs_them(lib, nx, ny, nz, seed, h, bc_mo
     assert lib.pyro_k_mg_prolong_m(nx, ny, nz, ptr(dev(enc(pcv))), ptr(meta), ptr(pd), cx, cy,
                                    cz, ptr(mc), storage, None) == 0
     assert np.array_equal(host(pd), enc(pf_o))
+
+
+@pytest.mark.parametrize("nx,ny,nz,seed,h", [(32, 48, 32, 0, 0.05), (38, 40, 20, 8, 0.16),
+                                             (150, 96, 24, 9, 0.02), (64, 40, 24, 3, 0.04)])
+@pytest.mark.parametrize("bc_mode", [0, 1])
+@pytest.mark.parametrize("storage", [_abi.MG_F32, _abi.MG_BF16])
+def test_mg_fused_first_and_last_passes_equal_the_plain_pass(lib, nx, ny, nz, seed, h, bc_mode,
+                                                             storage):
+    """The preconditioner's fused level-0 passes against the oracle's pass:
+    the first from phi = 0 on the FP32 right-hand side (BF16: rounded, and
+    the rounded copy written out), every cell of phi written; the last on
+    BF16 storage with its result widened into an FP32 array."""
+    rng = np.random.default_rng(200 + seed)
+    f = (rng.random((nz, ny, nx)) < 0.2).astype(np.uint32)
+    r = rng.normal(0, 1, (nz, ny, nx)).astype(np.float32)
+    lo = storage == _abi.MG_BF16
+    enc = (lambda a: _bf16_bits(a)) if lo else (lambda a: np.ascontiguousarray(a, np.float32))
+    meta = dev(np.zeros((nz, ny, nx), np.uint8))
+    assert lib.pyro_k_mg_meta(nx, ny, nz, ptr(dev(f)), ptr(meta), None) == 0
+    bq = _bf16_val(_bf16_bits(r)) if lo else r
+    for color, om in [(0, 1.0), (1, 1.6)]:
+        e = oracle.mg_smooth((nx, ny, nz), h, bq, f, np.zeros_like(r), color, om, bc_mode=bc_mode)
+        pd = dev(enc(np.full_like(r, 7.0)))  # every cell is overwritten
+        bqd = dev(np.zeros((nz, ny, nx), np.uint16)) if lo else None
+        assert lib.pyro_k_mg_pass_first(nx, ny, nz, h, ptr(dev(r)), ptr(bqd) if lo else None,
+                                        ptr(meta), ptr(pd), color, om, bc_mode, storage,
+                                        None) == 0, lib.pyro_last_error()
+        assert np.array_equal(host(pd), enc(e)), (color, om)
+        if lo:
+            assert np.array_equal(host(bqd), _bf16_bits(r))
+    if not lo:
+        return
+    b = _bf16_val(_bf16_bits(r))
+    p = _bf16_val(_bf16_bits(rng.normal(0, 1, (nz, ny, nx)).astype(np.float32)))
+    for color, om in [(0, 1.0), (1, 1.6)]:
+        e = oracle.mg_smooth((nx, ny, nz), h, b, f, p, color, om, bc_mode=bc_mode)
+        pd = dev(_bf16_bits(p))
+        out = dev(np.full_like(r, 7.0))
+        assert lib.pyro_k_mg_pass_last(nx, ny, nz, h, ptr(dev(_bf16_bits(b))), ptr(meta),
+                                       ptr(pd), ptr(out), color, om, bc_mode,
+                                       None) == 0, lib.pyro_last_error()
+        assert np.array_equal(host(out), _bf16_val(_bf16_bits(e))), (color, om)
+        assert np.array_equal(host(pd), _bf16_bits(p))
+
+
+def test_mg_fused_passes_refuse_odd_rows(lib):
+    z = dev(np.zeros(9 * 8 * 4, np.float32))
+    m = dev(np.zeros(9 * 8 * 4, np.uint8))
+    assert lib.pyro_k_mg_pass_first(9, 8, 4, 0.1, ptr(z), None, ptr(m), ptr(z), 0, 1.0, 0,
+                                    _abi.MG_F32, None) == _abi.PYRO_E_INVALID
+    assert lib.pyro_k_mg_pass_last(9, 8, 4, 0.1, ptr(z), ptr(m), ptr(z), ptr(z), 0, 1.0, 0,
+                                   None) == _abi.PYRO_E_INVALID
 
 
 # slabs of one to three planes per CTA of the cluster (nz = 3: three CTAs)
