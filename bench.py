@@ -373,17 +373,20 @@ def _learned_net():
 
 
 def solve_runs(ps, bd, runs, net=None):
-    """Each (name, mode, tol, cap) solved twice from phi = 0; the second
-    solve's device time (CUDA events inside the solver) is reported."""
+    """Each (name, mode, tol, cap) solved twice from phi = 0 into the same
+    array, as a simulation calls it; the second solve's device time (CUDA
+    events inside the solver) is reported.  The first allocates lazily and
+    captures the CG modes' iteration graph for that array."""
     import torch
     from pyro_b200 import _abi
     res = {}
+    phi = torch.zeros_like(bd)
     for name, mode, tol, cap in runs:
         if mode == _abi.SOLVER_MGPCG_LEARNED and net is None:
             continue
         best = None
-        for rep in range(2):          # first solve allocates lazily
-            phi = torch.zeros_like(bd)
+        for rep in range(2):
+            phi.zero_()
             torch.cuda.synchronize()
             best = ps.solve(bd.data_ptr(), phi.data_ptr(), mode, tol, cap, allow_cap=True)
         r = {"ms": round(best.ms, 3), "iterations": best.iterations,

@@ -195,13 +195,16 @@ __global__ void __launch_bounds__(VT) k_apply(Cells c, double ih2, const float* 
   }
 }
 
-// phi += alpha p; r -= alpha q; accumulate |r|^2
+// phi += alpha p; r -= alpha q; accumulate |r|^2.  phi is ctl->x when
+// the argument is null (the CG loop's graph, which serves any solution
+// array).
 __global__ void __launch_bounds__(VT) k_update_xr(Cells c, const uint32_t* __restrict__ f,
-                                                  float* __restrict__ phi,
+                                                  float* phi_arg,
                                                   float* __restrict__ r,
                                                   const float* __restrict__ p,
                                                   const float* __restrict__ q,
-                                                  double* __restrict__ sc) {
+                                                  double* __restrict__ sc,
+                                                  const CgCtl* __restrict__ ctl) {
   pdl_trigger();
   pdl_wait();
   __shared__ double sh[32];
@@ -209,6 +212,7 @@ __global__ void __launch_bounds__(VT) k_update_xr(Cells c, const uint32_t* __res
   if (threadIdx.x == 0) s_alpha = (float)(sc[SC_RZ] / sc[SC_PQ]);
   __syncthreads();
   const float alpha = s_alpha;
+  float* __restrict__ phi = phi_arg ? phi_arg : ctl->x;
   double rr = 0.0;
   CELL_LOOP(i) {
     if (__ldg(f + i) == 1u) continue;
@@ -240,17 +244,24 @@ __global__ void __launch_bounds__(VT) k_dots(Cells c, const uint32_t* __restrict
   if (q) block_add_d(sh, zq, sc + SC_ZQ);
 }
 
-// p = z + beta p with beta = -<z,q>/<p,q> (first iteration: p = z)
+// p = z + beta p with beta = -<z,q>/<p,q>; p = z when ctl->first is set
+// (the first iteration after a start or restart)
 __global__ void __launch_bounds__(VT) k_update_p(Cells c, const uint32_t* __restrict__ f,
                                                  float* __restrict__ p,
                                                  const float* __restrict__ zv,
-                                                 const double* __restrict__ sc, int first) {
+                                                 const double* __restrict__ sc,
+                                                 const CgCtl* __restrict__ ctl) {
   pdl_trigger();
   pdl_wait();
   __shared__ float s_beta;
-  if (threadIdx.x == 0) s_beta = first ? 0.0f : (float)(-sc[SC_ZQ] / sc[SC_PQ]);
+  __shared__ int s_first;
+  if (threadIdx.x == 0) {
+    s_first = ctl->first;
+    s_beta = s_first ? 0.0f : (float)(-sc[SC_ZQ] / sc[SC_PQ]);
+  }
   __syncthreads();
   const float beta = s_beta;
+  const bool first = s_first != 0;
   CELL_LOOP(i) {
     if (__ldg(f + i) == 1u) {
       p[i] = 0.0f;
@@ -258,6 +269,26 @@ __global__ void __launch_bounds__(VT) k_update_p(Cells c, const uint32_t* __rest
     }
     p[i] = first ? zv[i] : zv[i] + beta * p[i];
   }
+}
+
+// End of one CG iteration on the device: count it and let the loop's
+// conditional node run another unless |r| / |b| <= tol, the count reached
+// max_it, or the iteration stalled (|r|^2 not finite, <p, A p> = 0).  The
+// count rises by one per iteration and the cap is a host-checked int, so
+// the loop always ends.
+__global__ void k_cg_check(CgCtl* __restrict__ ctl, const double* __restrict__ sc,
+                           cudaGraphConditionalHandle h) {
+  pdl_trigger();
+  pdl_wait();
+  const double rr = sc[SC_RR], pq = sc[SC_PQ];
+  const int it = ctl->it + 1;
+  const bool stalled = !(rr >= 0.0) || !(pq < 0.0 || pq > 0.0);
+  const bool conv = ctl->bb2 > 0.0 && sqrt(rr / ctl->bb2) <= ctl->tol;
+  ctl->it = it;
+  ctl->rr = rr;
+  ctl->first = 0;
+  ctl->stalled = stalled ? 1 : 0;
+  cudaGraphSetConditional(h, (!stalled && !conv && it < ctl->max_it) ? 1u : 0u);
 }
 
 __global__ void k_roll(double* sc) {
@@ -511,23 +542,10 @@ struct DirectSolve : CoarseDirect {
   }
 };
 
-int Solver::update_reach(cudaStream_t st) {
+int Solver::update_reach(cudaStream_t st, unsigned long long h) {
   const uint32_t* f0 = mg->f[0];
   L3 l{d.nx, d.ny, d.nz};
-  if (!fa.p) {
-    int rc;
-    if ((rc = fa.alloc(d.cells() * 4)) != PYRO_OK || (rc = reach_dev.alloc(16)) != PYRO_OK)
-      return rc;
-  }
   unsigned long long* H = reach_dev.as<unsigned long long>();
-  PYRO_CU(cudaMemsetAsync(H, 0, 16, st));
-  k_flag_hash<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, f0, H);
-  PYRO_CU(cudaGetLastError());
-  PYRO_CU(cudaMemcpyAsync(host_sc, H, 8, cudaMemcpyDeviceToHost, st));
-  PYRO_CU(cudaStreamSynchronize(st));
-  unsigned long long h;
-  std::memcpy(&h, host_sc, 8);
-  if (reach_valid && h == reach_hash && reach_flags == f0) return PYRO_OK;
   k_reach_init<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, f0, mg->bc_mode, fa.as<uint32_t>());
   PYRO_CU(cudaGetLastError());
   dim3 tg((unsigned)((d.nx + RT - 1) / RT), (unsigned)((d.ny + RT - 1) / RT),
@@ -555,6 +573,129 @@ int Solver::update_reach(cudaStream_t st) {
   return PYRO_OK;
 }
 
+int Solver::begin_cg(cudaStream_t st, float* phi, const float* b) {
+  const uint32_t* f0 = mg->f[0];
+  L3 l{d.nx, d.ny, d.nz};
+  const double ih2 = 1.0 / ((double)mg->h[0] * mg->h[0]);
+  double* S = sc.as<double>();
+  int rc;
+  if (!fa.p) {
+    if ((rc = fa.alloc(d.cells() * 4)) != PYRO_OK || (rc = reach_dev.alloc(16)) != PYRO_OK)
+      return rc;
+  }
+  auto resid = [&]() -> cudaError_t {
+    cudaError_t e = cudaMemsetAsync(sc.p, 0, SC_N * 8, st);
+    if (e == cudaSuccess)
+      e = launch_pdl(k_resid, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), ih2,
+                     (const float*)phi, b, (const uint32_t*)fa.as<uint32_t>(), mg->bc_mode,
+                     r.as<float>(), S);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(host_sc, sc.p, SC_N * 8, cudaMemcpyDeviceToHost, st);
+    return e;
+  };
+  // The hash of the flag field and, when the last solve's reachable set
+  // and levels are still in place, the residual on them: one round trip.
+  unsigned long long* H = reach_dev.as<unsigned long long>();
+  PYRO_CU(cudaMemsetAsync(H, 0, 16, st));
+  k_flag_hash<<<grid_for(d), dim3(BX, BY, BZ), 0, st>>>(l, f0, H);
+  PYRO_CU(cudaGetLastError());
+  const bool spec = reach_valid && reach_flags == f0 && pc_ready;
+  if (spec) PYRO_CU(resid());
+  PYRO_CU(cudaMemcpyAsync(host_sc + SC_N, H, 8, cudaMemcpyDeviceToHost, st));
+  PYRO_CU(cudaStreamSynchronize(st));
+  unsigned long long h;
+  std::memcpy(&h, host_sc + SC_N, 8);
+  if (spec && h == reach_hash) return PYRO_OK;
+  // the flags changed (or first solve): reachable set, the
+  // preconditioner's level flags and masks, its coarsest-level inverse
+  pc_ready = false;
+  if ((rc = update_reach(st, h)) != PYRO_OK) return rc;
+  pc.bind_level0(z.as<float>(), r.as<float>(), fa.as<uint32_t>());
+  PYRO_CU(pc.prepare(st));
+  if (direct) {
+    direct->f = pc.f.back();  // level 0's flags when the grid is the coarsest level
+    if ((rc = direct->refresh(st)) != PYRO_OK) return rc;
+  }
+  pc_ready = true;
+  PYRO_CU(resid());
+  PYRO_CU(cudaStreamSynchronize(st));
+  return PYRO_OK;
+}
+
+int Solver::cg_loop(cudaStream_t st, float* phi, bool bf16, double bb2, float tol, int it0,
+                    int max_it) {
+  cudaGraphExec_t& exec = cg_exec[bf16 ? 1 : 0];
+  if (!exec) {
+    const uint32_t* f0 = fa.as<uint32_t>();
+    const double ih2 = 1.0 / ((double)mg->h[0] * mg->h[0]);
+    double* S = sc.as<double>();
+    CgCtl* C = ctl.as<CgCtl>();
+    // the BF16 levels exist before their addresses are captured
+    for (size_t l = 0; bf16 && l < bphi.size(); l++) {
+      const size_t need = pc.dims[l].cells() * 2;
+      int rc;
+      if (bphi[l].bytes != need &&
+          ((rc = bphi[l].alloc(need)) != PYRO_OK || (rc = bphi2[l].alloc(need)) != PYRO_OK ||
+           (rc = bb[l].alloc(need)) != PYRO_OK))
+        return rc;
+    }
+    cudaGraph_t g = nullptr;
+    PYRO_CU(cudaGraphCreate(&g, 0));
+    struct Own {
+      cudaGraph_t g;
+      ~Own() { cudaGraphDestroy(g); }
+    } own{g};
+    cudaGraphConditionalHandle hc;
+    PYRO_CU(cudaGraphConditionalHandleCreate(&hc, g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = hc;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    PYRO_CU(cudaGraphAddNode(&node, g, nullptr, 0, &np));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    // one iteration: z = V(r); <z,r>, <z,q>; p = z + beta p; roll the
+    // scalars; q = A p, <p,q>; phi += alpha p, r -= alpha q, |r|^2; check
+    PYRO_CU(cudaStreamBeginCaptureToGraph(cap_st, body, nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeRelaxed));
+    const dim3 vb(vec_blocks(d.cells())), vt(VT);
+    cudaError_t e = precond(cap_st, bf16, false);
+    if (e == cudaSuccess)
+      e = launch_pdl(k_dots, vb, vt, 0, cap_st, cells_of(d), f0, (const float*)z.as<float>(),
+                     (const float*)r.as<float>(), (const float*)q.as<float>(), S);
+    if (e == cudaSuccess)
+      e = launch_pdl(k_update_p, vb, vt, 0, cap_st, cells_of(d), f0, p.as<float>(),
+                     (const float*)z.as<float>(), (const double*)S, (const CgCtl*)C);
+    if (e == cudaSuccess) e = launch_pdl(k_roll, dim3(1), dim3(1), 0, cap_st, S);
+    if (e == cudaSuccess)
+      e = launch_pdl(k_apply_dot, vb, vt, 0, cap_st, cells_of(d), ih2,
+                     (const float*)p.as<float>(), f0, mg->bc_mode, q.as<float>(), S);
+    if (e == cudaSuccess)
+      e = launch_pdl(k_update_xr, vb, vt, 0, cap_st, cells_of(d), f0, (float*)nullptr,
+                     r.as<float>(), (const float*)p.as<float>(), (const float*)q.as<float>(), S,
+                     (const CgCtl*)C);
+    if (e == cudaSuccess)
+      e = launch_pdl(k_cg_check, dim3(1), dim3(1), 0, cap_st, C, (const double*)S, hc);
+    cudaGraph_t out = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(cap_st, &out);
+    PYRO_CU(e);
+    PYRO_CU(ec);
+    PYRO_CU(cudaGraphInstantiate(&exec, g, 0));
+  }
+  host_ctl->x = phi;
+  host_ctl->bb2 = bb2;
+  host_ctl->tol = (double)tol;
+  host_ctl->rr = 0.0;
+  host_ctl->it = it0;
+  host_ctl->max_it = max_it;
+  host_ctl->first = 1;
+  host_ctl->stalled = 0;
+  PYRO_CU(cudaMemcpyAsync(ctl.p, host_ctl, sizeof(CgCtl), cudaMemcpyHostToDevice, st));
+  PYRO_CU(cudaGraphLaunch(exec, st));
+  return PYRO_OK;
+}
+
 int Solver::init(Multigrid* m) {
   mg = m;
   d = m->dims[0];
@@ -565,10 +706,16 @@ int Solver::init(Multigrid* m) {
   if ((rc = p.alloc(n * 4)) != PYRO_OK) return rc;
   if ((rc = q.alloc(n * 4)) != PYRO_OK) return rc;
   if ((rc = sc.alloc(SC_N * 8)) != PYRO_OK) return rc;
-  if (cudaMallocHost(&host_sc, SC_N * 8) != cudaSuccess) {
+  if ((rc = ctl.alloc(sizeof(CgCtl))) != PYRO_OK) return rc;
+  // the scalars and one 8-byte word (the flag hash)
+  if (cudaMallocHost(&host_sc, (SC_N + 1) * 8) != cudaSuccess ||
+      cudaMallocHost(&host_ctl, sizeof(CgCtl)) != cudaSuccess) {
     set_error("solver: pinned allocation failed");
     return PYRO_E_NOMEM;
   }
+  // q is read (and its products discarded) by the first iteration's dots
+  PYRO_CU(cudaMemset(q.p, 0, n * 4));
+  PYRO_CU(cudaStreamCreateWithFlags(&cap_st, cudaStreamNonBlocking));
   if (cudaEventCreate(&ev0) != cudaSuccess || cudaEventCreate(&ev1) != cudaSuccess ||
       cudaEventCreate(&evl0) != cudaSuccess || cudaEventCreate(&evl1) != cudaSuccess) {
     set_error("solver: cudaEventCreate failed");
@@ -597,8 +744,12 @@ int Solver::init(Multigrid* m) {
 }
 
 Solver::~Solver() {
+  for (cudaGraphExec_t x : cg_exec)
+    if (x) cudaGraphExecDestroy(x);
+  if (cap_st) cudaStreamDestroy(cap_st);
   delete direct;
   if (host_sc) cudaFreeHost(host_sc);
+  if (host_ctl) cudaFreeHost(host_ctl);
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
   if (evl0) cudaEventDestroy(evl0);
@@ -606,7 +757,8 @@ Solver::~Solver() {
 }
 
 size_t Solver::device_bytes() const {
-  size_t s = r.bytes + z.bytes + p.bytes + q.bytes + sc.bytes + fa.bytes + reach_dev.bytes;
+  size_t s = r.bytes + z.bytes + p.bytes + q.bytes + sc.bytes + ctl.bytes + fa.bytes +
+             reach_dev.bytes;
   for (size_t l = 0; l < bphi.size(); l++) s += bphi[l].bytes + bphi2[l].bytes + bb[l].bytes;
   s += pc.device_bytes();
   if (direct) s += direct->minv.bytes + direct->piv.bytes + direct->bad.bytes;
@@ -615,7 +767,6 @@ size_t Solver::device_bytes() const {
 
 int Solver::true_resid(cudaStream_t st, const float* phi, const float* b, double* rel,
                        double* bn) {
-  L3 l{d.nx, d.ny, d.nz};
   PYRO_CU(cudaMemsetAsync(sc.p, 0, SC_N * 8, st));
   launch_pdl(k_resid, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), 1.0 / ((double)mg->h[0] * mg->h[0]), phi, b,
                                                    mg->f[0], mg->bc_mode, nullptr,
@@ -639,7 +790,6 @@ cudaError_t Solver::precond(cudaStream_t st, bool bf16, bool prep) {
 
 int Solver::learned_stage(cudaStream_t st, float* phi, double* rr, PyroSolveInfo* info) {
   const uint32_t* f0 = mg->f[0];
-  L3 l{d.nx, d.ny, d.nz};
   const double ih2 = 1.0 / ((double)mg->h[0] * mg->h[0]);
   double* S = sc.as<double>();
   PYRO_CU(cudaEventRecord(evl0, st));
@@ -675,7 +825,7 @@ int Solver::learned_stage(cudaStream_t st, float* phi, double* rr, PyroSolveInfo
     host_sc[SC_PQ] = eae;
     PYRO_CU(cudaMemcpyAsync(sc.p, host_sc, SC_N * 8, cudaMemcpyHostToDevice, st));
     launch_pdl(k_update_xr, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), f0, phi, r.as<float>(),
-                                                         z.as<float>(), q.as<float>(), S);
+                                                         z.as<float>(), q.as<float>(), S, (const CgCtl*)nullptr);
     PYRO_CU(cudaGetLastError());
     PYRO_CU(cudaMemcpyAsync(host_sc, sc.p, SC_N * 8, cudaMemcpyDeviceToHost, st));
   }
@@ -710,7 +860,6 @@ int Solver::solve(cudaStream_t st, float* phi, const float* b, int mode, float t
   int iters = 0;
   double rel = 0, bn = 0;
   int rc = PYRO_OK;
-  L3 l{d.nx, d.ny, d.nz};
   const double ih2 = 1.0 / ((double)mg->h[0] * mg->h[0]);
   if (mode == PYRO_SOLVER_VCYCLE || mode == PYRO_SOLVER_VCYCLE_TOL) {
     mg->bind_level0(phi, b, f0);
@@ -734,8 +883,8 @@ int Solver::solve(cudaStream_t st, float* phi, const float* b, int mode, float t
   } else {
     const bool bf16 = mode == PYRO_SOLVER_MGPCG_BF16 || mode == PYRO_SOLVER_MGPCG_LEARNED;
     double* S = sc.as<double>();
-    // CG and its V-cycle run on the reachable fluid cells only
-    if ((rc = update_reach(st)) != PYRO_OK) return rc;
+    // CG and its V-cycle run on the reachable fluid cells only; r = b - A phi
+    if ((rc = begin_cg(st, phi, b)) != PYRO_OK) return rc;
     f0 = fa.as<uint32_t>();
     mg->bind_level0(save_phi, save_b, f0);
     struct Rebind {
@@ -745,83 +894,40 @@ int Solver::solve(cudaStream_t st, float* phi, const float* b, int mode, float t
       const uint32_t* f;
       ~Rebind() { m->bind_level0(p, b, f); }
     } rebind{mg, save_phi, save_b, save_f0};
-    // r = b - A phi, |r|, |b|
-    PYRO_CU(cudaMemsetAsync(sc.p, 0, SC_N * 8, st));
-    launch_pdl(k_resid, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), ih2, phi, b, f0, mg->bc_mode,
-                                                     r.as<float>(), S);
-    PYRO_CU(cudaGetLastError());
-    PYRO_CU(cudaMemcpyAsync(host_sc, sc.p, SC_N * 8, cudaMemcpyDeviceToHost, st));
-    PYRO_CU(cudaStreamSynchronize(st));
     double bb2 = host_sc[SC_BB];
     bn = std::sqrt(bb2);
     rel = bb2 > 0 ? std::sqrt(host_sc[SC_RR] / bb2) : 0.0;
     info->rel_resid_start = rel;
     info->rel_resid_learned = rel;
+    bool rel_true = true;  // rel is of the true residual
     if (mode == PYRO_SOLVER_MGPCG_LEARNED && bb2 > 0 && rel > tol) {
       double rr = host_sc[SC_RR];
       if ((rc = learned_stage(st, phi, &rr, info)) != PYRO_OK) return rc;
       rel = std::sqrt(rr / bb2);
       info->rel_resid_learned = rel;
+      rel_true = false;
     }
-    // CG with residual replacement: when the recursively updated residual
-    // meets the tolerance the true residual is recomputed; if it does not
-    // meet it, CG restarts from the true residual.
-    // the preconditioner's level flags and masks from the reachable-fluid
-    // flags, and its coarsest-level inverse when that level's flags changed
-    pc.bind_level0(z.as<float>(), r.as<float>(), fa.as<uint32_t>());
-    PYRO_CU(pc.prepare(st));
-    if (direct) {
-      direct->f = pc.f.back();  // level 0's flags when the grid is the coarsest level
-      if ((rc = direct->refresh(st)) != PYRO_OK) return rc;
-    }
+    // CG with residual replacement: the iterations run on the device until
+    // the recursively updated residual meets the tolerance; then the true
+    // residual is recomputed and, if it does not meet it, CG restarts from it.
     int restarts = 0;
     while (rel > tol && iters < max_iters && restarts < 8) {
-      PYRO_CU(precond(st, bf16, false));
-      launch_pdl(k_dots, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), f0, z.as<float>(), r.as<float>(),
-                                                      nullptr, S);
-      PYRO_CU(cudaGetLastError());
-      launch_pdl(k_roll, dim3(1), dim3(1), 0, st, S);
-      launch_pdl(k_update_p, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), f0, p.as<float>(), z.as<float>(),
-                                                          S, 1);
-      PYRO_CU(cudaGetLastError());
-      bool stalled = false;
-      while (iters < max_iters) {
-        launch_pdl(k_apply_dot, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), ih2, p.as<float>(), f0,
-                                                             mg->bc_mode, q.as<float>(), S);
-        launch_pdl(k_update_xr, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), f0, phi, r.as<float>(),
-                                                             p.as<float>(), q.as<float>(), S);
-        PYRO_CU(cudaGetLastError());
-        PYRO_CU(cudaMemcpyAsync(host_sc, sc.p, SC_N * 8, cudaMemcpyDeviceToHost, st));
-        PYRO_CU(cudaStreamSynchronize(st));
-        iters++;
-        double rr = host_sc[SC_RR];
-        if (!(rr >= 0.0) || !(host_sc[SC_PQ] < 0.0 || host_sc[SC_PQ] > 0.0)) {
-          stalled = true;
-          break;
-        }
-        if (bb2 > 0 && std::sqrt(rr / bb2) <= tol) break;
-        PYRO_CU(precond(st, bf16, false));
-        launch_pdl(k_dots, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), f0, z.as<float>(), r.as<float>(),
-                                                        q.as<float>(), S);
-        launch_pdl(k_update_p, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), f0, p.as<float>(),
-                                                            z.as<float>(), S, 0);
-        launch_pdl(k_roll, dim3(1), dim3(1), 0, st, S);
-        PYRO_CU(cudaGetLastError());
-      }
+      if ((rc = cg_loop(st, phi, bf16, bb2, tol, iters, max_iters)) != PYRO_OK) return rc;
       // true residual into r (and |r|, |b|)
       PYRO_CU(cudaMemsetAsync(sc.p, 0, SC_N * 8, st));
-      launch_pdl(k_resid, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), ih2, phi, b, f0, mg->bc_mode,
-                                                       r.as<float>(), S);
+      launch_pdl(k_resid, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), ih2, phi, b,
+                 f0, mg->bc_mode, r.as<float>(), S);
       PYRO_CU(cudaGetLastError());
       PYRO_CU(cudaMemcpyAsync(host_sc, sc.p, SC_N * 8, cudaMemcpyDeviceToHost, st));
+      PYRO_CU(cudaMemcpyAsync(host_ctl, ctl.p, sizeof(CgCtl), cudaMemcpyDeviceToHost, st));
       PYRO_CU(cudaStreamSynchronize(st));
+      iters = host_ctl->it;
       rel = bb2 > 0 ? std::sqrt(host_sc[SC_RR] / bb2) : 0.0;
+      rel_true = true;
       restarts++;
-      if (stalled) break;
+      if (host_ctl->stalled) break;
     }
-    {
-      if ((rc = true_resid(st, phi, b, &rel, &bn)) != PYRO_OK) return rc;
-    }
+    if (!rel_true && (rc = true_resid(st, phi, b, &rel, &bn)) != PYRO_OK) return rc;
   }
   PYRO_CU(cudaEventRecord(ev1, st));
   PYRO_CU(cudaEventSynchronize(ev1));

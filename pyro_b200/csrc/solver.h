@@ -14,6 +14,19 @@ struct DirectSolve;
 // FP64 (a dense inverse of DIRECT_MAX^2 doubles at most: 75 MB).
 constexpr size_t DIRECT_MAX = 3072;
 
+// State of the device-driven CG loop: written by the host before the loop's
+// graph is launched, updated by its check kernel after every iteration.
+struct CgCtl {
+  float* x;     // the solution array
+  double bb2;   // |b|^2
+  double tol;   // relative residual target
+  double rr;    // |r|^2 after the last iteration
+  int it;       // iterations done (across restarts)
+  int max_it;   // iteration cap
+  int first;    // 1: the next search direction is p = z
+  int stalled;  // 1: |r|^2 not finite or <p, A p> = 0
+};
+
 struct Solver {
   Multigrid* mg = nullptr;  // the reference hierarchy (fixed V-cycle modes)
   Multigrid pc;             // the preconditioner's deep hierarchy (CG modes)
@@ -32,6 +45,16 @@ struct Solver {
   unsigned long long reach_hash = 0;
   const uint32_t* reach_flags = nullptr;
   bool reach_valid = false;
+  bool pc_ready = false;  // the hierarchy's flags and the coarsest inverse follow fa
+  // The CG iterations as one CUDA graph: a conditional while node whose body
+  // is one preconditioned iteration ending in k_cg_check, which decides on
+  // the device whether another iteration follows.  One per preconditioner
+  // storage (FP32, BF16), built on first use; the solution array is read
+  // from the control block.
+  cudaGraphExec_t cg_exec[2] = {nullptr, nullptr};
+  cudaStream_t cap_st = nullptr;  // the stream the loop body is captured on
+  DevBuf ctl;                     // CgCtl on the device
+  CgCtl* host_ctl = nullptr;      // pinned mirror
 
   int init(Multigrid* m);
   ~Solver();
@@ -47,7 +70,17 @@ struct Solver {
   // phi += alpha net(r) when that lowers |r| (r = b - A phi on entry, kept
   // consistent); *rr is |r|^2 in and out.
   int learned_stage(cudaStream_t st, float* phi, double* rr, PyroSolveInfo* info);
-  int update_reach(cudaStream_t st);
+  // The reachable-fluid flags fa, the preconditioner's levels and its
+  // coarsest inverse for the current flag field, and r = b - A phi with
+  // |r|^2, |b|^2 in host_sc (one host synchronisation when the flags did not
+  // change).
+  int begin_cg(cudaStream_t st, float* phi, const float* b);
+  // fa from the current flag field, whose hash is h
+  int update_reach(cudaStream_t st, unsigned long long h);
+  // Enqueue CG iterations from r (p = z first) until the recursive residual
+  // meets tol, the count reaches max_it or the iteration stalls.
+  int cg_loop(cudaStream_t st, float* phi, bool bf16, double bb2, float tol, int it0,
+              int max_it);
 };
 
 }  // namespace pyro
