@@ -77,28 +77,6 @@ struct L3 {
   __device__ __forceinline__ int idx(int x, int y, int z) const { return x + nx * (y + ny * z); }
 };
 
-// (A v)_i = (sum fluid nbrs v - cnt v_i) / h^2, 0 in solids; evaluated in
-// FP64 so residuals near 1e-6 of |b| are not lost to cancellation.
-__device__ __forceinline__ double apply_A(const L3& d, double ih2, const float* __restrict__ v,
-                                          const uint32_t* __restrict__ f, int x, int y, int z,
-                                          int bc_mode, float vi) {
-  double sum = 0.0, cnt = 0.0;
-#pragma unroll
-  for (int k = 0; k < 6; k++) {
-    int a = x + (k == 0) - (k == 1), b = y + (k == 2) - (k == 3), c = z + (k == 4) - (k == 5);
-    if (b < 0) continue;
-    if (!d.inb(a, b, c)) {
-      if (bc_mode == 0 || b >= d.ny) cnt += 1.0;
-      continue;
-    }
-    int j = d.idx(a, b, c);
-    if (__ldg(f + j) == 1u) continue;
-    sum += (double)__ldg(v + j);
-    cnt += 1.0;
-  }
-  return (sum - cnt * (double)vi) * ih2;
-}
-
 #define CELL_PROLOGUE                          \
   int x = blockIdx.x * BX + threadIdx.x;       \
   int y = blockIdx.y * BY + threadIdx.y;       \
@@ -130,9 +108,67 @@ inline Cells cells_of(Dims3 d) {
 #define CELL_LOOP(i) \
   for (int i = blockIdx.x * VT + threadIdx.x; i < c.n; i += gridDim.x * VT)
 
+// (A v)_i = (sum fluid nbrs v - cnt v_i) / h^2, 0 in solids; evaluated in
+// FP64 so residuals near 1e-6 of |b| are not lost to cancellation.  The
+// fluid neighbours are added in the order +x, -x, +y, -y, +z, -z and cnt
+// counts them and the Dirichlet faces (the top; with bc_mode 0 the sides).
+// Two sources of the cells' solidity give the same sums:
+//  * FlagMask: u32 solid flags (1 = solid), read at each neighbour (the
+//    fixed V-cycle modes and pyro_k_mg_apply, whose masks are not built
+//    yet when their residual is taken);
+//  * MetaMask: the CG modes' level-0 neighbour masks (bit k = neighbour k
+//    inside the grid and fluid, bit 6 = solid), one byte per cell.
+struct FlagMask {
+  const uint32_t* f;
+  __device__ __forceinline__ bool solid(int i) const { return __ldg(f + i) == 1u; }
+  __device__ __forceinline__ double apply(const Cells& c, double ih2, const float* __restrict__ v,
+                                         int i, int bc_mode, float vi) const {
+    int x, y, z;
+    c.coords(i, x, y, z);
+    const L3& d = c.d;
+    double sum = 0.0, cnt = 0.0;
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+      int a = x + (k == 0) - (k == 1), b = y + (k == 2) - (k == 3), cz = z + (k == 4) - (k == 5);
+      if (b < 0) continue;
+      if (!d.inb(a, b, cz)) {
+        if (bc_mode == 0 || b >= d.ny) cnt += 1.0;
+        continue;
+      }
+      int j = d.idx(a, b, cz);
+      if (__ldg(f + j) == 1u) continue;
+      sum += (double)__ldg(v + j);
+      cnt += 1.0;
+    }
+    return (sum - cnt * (double)vi) * ih2;
+  }
+};
+struct MetaMask {
+  const uint8_t* m;
+  __device__ __forceinline__ bool solid(int i) const { return (__ldg(m + i) & 0x40u) != 0; }
+  __device__ __forceinline__ double apply(const Cells& c, double ih2, const float* __restrict__ v,
+                                         int i, int bc_mode, float vi) const {
+    int x, y, z;
+    c.coords(i, x, y, z);
+    const uint32_t mi = __ldg(m + i);
+    const int sy = c.d.nx, sz = c.d.nx * c.d.ny;
+    double sum = 0.0;
+    if (mi & 1u) sum += (double)__ldg(v + i + 1);
+    if (mi & 2u) sum += (double)__ldg(v + i - 1);
+    if (mi & 4u) sum += (double)__ldg(v + i + sy);
+    if (mi & 8u) sum += (double)__ldg(v + i - sy);
+    if (mi & 16u) sum += (double)__ldg(v + i + sz);
+    if (mi & 32u) sum += (double)__ldg(v + i - sz);
+    int faces = (y == c.d.ny - 1);
+    if (bc_mode == 0) faces += (x == 0) + (x == c.d.nx - 1) + (z == 0) + (z == c.d.nz - 1);
+    const double cnt = (double)(__popc(mi & 63u) + faces);
+    return (sum - cnt * (double)vi) * ih2;
+  }
+};
+
+template <typename M>
 __global__ void __launch_bounds__(VT) k_resid(Cells c, double ih2, const float* __restrict__ phi,
-                                              const float* __restrict__ b,
-                                              const uint32_t* __restrict__ f, int bc_mode,
+                                              const float* __restrict__ b, M mk, int bc_mode,
                                               float* __restrict__ r, double* __restrict__ sc) {
   pdl_trigger();
   pdl_wait();
@@ -140,11 +176,9 @@ __global__ void __launch_bounds__(VT) k_resid(Cells c, double ih2, const float* 
   double r2 = 0.0, b2 = 0.0;
   CELL_LOOP(i) {
     float ri = 0.0f;
-    if (__ldg(f + i) != 1u) {
-      int x, y, z;
-      c.coords(i, x, y, z);
+    if (!mk.solid(i)) {
       float bi = __ldg(b + i);
-      double rd = (double)bi - apply_A(c.d, ih2, phi, f, x, y, z, bc_mode, __ldg(phi + i));
+      double rd = (double)bi - mk.apply(c, ih2, phi, i, bc_mode, __ldg(phi + i));
       ri = (float)rd;
       r2 += rd * rd;
       b2 += (double)bi * (double)bi;
@@ -155,9 +189,9 @@ __global__ void __launch_bounds__(VT) k_resid(Cells c, double ih2, const float* 
   block_add_d(sh, b2, sc + SC_BB);
 }
 
+template <typename M>
 __global__ void __launch_bounds__(VT) k_apply_dot(Cells c, double ih2, const float* __restrict__ p,
-                                                  const uint32_t* __restrict__ f, int bc_mode,
-                                                  float* __restrict__ q,
+                                                  M mk, int bc_mode, float* __restrict__ q,
                                                   double* __restrict__ sc) {
   pdl_trigger();
   pdl_wait();
@@ -165,11 +199,9 @@ __global__ void __launch_bounds__(VT) k_apply_dot(Cells c, double ih2, const flo
   double pq = 0.0;
   CELL_LOOP(i) {
     float qi = 0.0f;
-    if (__ldg(f + i) != 1u) {
-      int x, y, z;
-      c.coords(i, x, y, z);
+    if (!mk.solid(i)) {
       float pi = __ldg(p + i);
-      double qd = apply_A(c.d, ih2, p, f, x, y, z, bc_mode, pi);
+      double qd = mk.apply(c, ih2, p, i, bc_mode, pi);
       qi = (float)qd;
       pq += (double)pi * qd;
     }
@@ -180,17 +212,12 @@ __global__ void __launch_bounds__(VT) k_apply_dot(Cells c, double ih2, const flo
 
 // q = A p (FP64 evaluation, rounded), 0 in solids.
 __global__ void __launch_bounds__(VT) k_apply(Cells c, double ih2, const float* __restrict__ p,
-                                              const uint32_t* __restrict__ f, int bc_mode,
-                                              float* __restrict__ q) {
+                                              FlagMask mk, int bc_mode, float* __restrict__ q) {
   pdl_trigger();
   pdl_wait();
   CELL_LOOP(i) {
     float qi = 0.0f;
-    if (__ldg(f + i) != 1u) {
-      int x, y, z;
-      c.coords(i, x, y, z);
-      qi = (float)apply_A(c.d, ih2, p, f, x, y, z, bc_mode, __ldg(p + i));
-    }
+    if (!mk.solid(i)) qi = (float)mk.apply(c, ih2, p, i, bc_mode, __ldg(p + i));
     q[i] = qi;
   }
 }
@@ -198,8 +225,8 @@ __global__ void __launch_bounds__(VT) k_apply(Cells c, double ih2, const float* 
 // phi += alpha p; r -= alpha q; accumulate |r|^2.  phi is ctl->x when
 // the argument is null (the CG loop's graph, which serves any solution
 // array).
-__global__ void __launch_bounds__(VT) k_update_xr(Cells c, const uint32_t* __restrict__ f,
-                                                  float* phi_arg,
+template <typename M>
+__global__ void __launch_bounds__(VT) k_update_xr(Cells c, M mk, float* phi_arg,
                                                   float* __restrict__ r,
                                                   const float* __restrict__ p,
                                                   const float* __restrict__ q,
@@ -215,7 +242,7 @@ __global__ void __launch_bounds__(VT) k_update_xr(Cells c, const uint32_t* __res
   float* __restrict__ phi = phi_arg ? phi_arg : ctl->x;
   double rr = 0.0;
   CELL_LOOP(i) {
-    if (__ldg(f + i) == 1u) continue;
+    if (mk.solid(i)) continue;
     phi[i] += alpha * p[i];
     float ri = r[i] - alpha * q[i];
     r[i] = ri;
@@ -225,8 +252,8 @@ __global__ void __launch_bounds__(VT) k_update_xr(Cells c, const uint32_t* __res
 }
 
 // <z,r> -> SC_RZN and, when q is given, <z,q> -> SC_ZQ
-__global__ void __launch_bounds__(VT) k_dots(Cells c, const uint32_t* __restrict__ f,
-                                             const float* __restrict__ zv,
+template <typename M>
+__global__ void __launch_bounds__(VT) k_dots(Cells c, M mk, const float* __restrict__ zv,
                                              const float* __restrict__ r,
                                              const float* __restrict__ q,
                                              double* __restrict__ sc) {
@@ -235,7 +262,7 @@ __global__ void __launch_bounds__(VT) k_dots(Cells c, const uint32_t* __restrict
   __shared__ double sh[32];
   double zr = 0.0, zq = 0.0;
   CELL_LOOP(i) {
-    if (__ldg(f + i) == 1u) continue;
+    if (mk.solid(i)) continue;
     float zi = zv[i];
     zr += (double)zi * (double)r[i];
     if (q) zq += (double)zi * (double)q[i];
@@ -246,8 +273,8 @@ __global__ void __launch_bounds__(VT) k_dots(Cells c, const uint32_t* __restrict
 
 // p = z + beta p with beta = -<z,q>/<p,q>; p = z when ctl->first is set
 // (the first iteration after a start or restart)
-__global__ void __launch_bounds__(VT) k_update_p(Cells c, const uint32_t* __restrict__ f,
-                                                 float* __restrict__ p,
+template <typename M>
+__global__ void __launch_bounds__(VT) k_update_p(Cells c, M mk, float* __restrict__ p,
                                                  const float* __restrict__ zv,
                                                  const double* __restrict__ sc,
                                                  const CgCtl* __restrict__ ctl) {
@@ -263,7 +290,7 @@ __global__ void __launch_bounds__(VT) k_update_p(Cells c, const uint32_t* __rest
   const float beta = s_beta;
   const bool first = s_first != 0;
   CELL_LOOP(i) {
-    if (__ldg(f + i) == 1u) {
+    if (mk.solid(i)) {
       p[i] = 0.0f;
       continue;
     }
@@ -586,9 +613,9 @@ int Solver::begin_cg(cudaStream_t st, float* phi, const float* b) {
   auto resid = [&]() -> cudaError_t {
     cudaError_t e = cudaMemsetAsync(sc.p, 0, SC_N * 8, st);
     if (e == cudaSuccess)
-      e = launch_pdl(k_resid, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), ih2,
-                     (const float*)phi, b, (const uint32_t*)fa.as<uint32_t>(), mg->bc_mode,
-                     r.as<float>(), S);
+      e = launch_pdl(k_resid<MetaMask>, dim3(vec_blocks(d.cells())), dim3(VT), 0, st,
+                     cells_of(d), ih2, (const float*)phi, b, MetaMask{pc.meta[0].as<uint8_t>()},
+                     mg->bc_mode, r.as<float>(), S);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(host_sc, sc.p, SC_N * 8, cudaMemcpyDeviceToHost, st);
     return e;
@@ -626,7 +653,7 @@ int Solver::cg_loop(cudaStream_t st, float* phi, bool bf16, double bb2, float to
                     int max_it) {
   cudaGraphExec_t& exec = cg_exec[bf16 ? 1 : 0];
   if (!exec) {
-    const uint32_t* f0 = fa.as<uint32_t>();
+    const MetaMask mk{pc.meta[0].as<uint8_t>()};
     const double ih2 = 1.0 / ((double)mg->h[0] * mg->h[0]);
     double* S = sc.as<double>();
     CgCtl* C = ctl.as<CgCtl>();
@@ -662,17 +689,18 @@ int Solver::cg_loop(cudaStream_t st, float* phi, bool bf16, double bb2, float to
     const dim3 vb(vec_blocks(d.cells())), vt(VT);
     cudaError_t e = precond(cap_st, bf16, false);
     if (e == cudaSuccess)
-      e = launch_pdl(k_dots, vb, vt, 0, cap_st, cells_of(d), f0, (const float*)z.as<float>(),
-                     (const float*)r.as<float>(), (const float*)q.as<float>(), S);
+      e = launch_pdl(k_dots<MetaMask>, vb, vt, 0, cap_st, cells_of(d), mk,
+                     (const float*)z.as<float>(), (const float*)r.as<float>(),
+                     (const float*)q.as<float>(), S);
     if (e == cudaSuccess)
-      e = launch_pdl(k_update_p, vb, vt, 0, cap_st, cells_of(d), f0, p.as<float>(),
+      e = launch_pdl(k_update_p<MetaMask>, vb, vt, 0, cap_st, cells_of(d), mk, p.as<float>(),
                      (const float*)z.as<float>(), (const double*)S, (const CgCtl*)C);
     if (e == cudaSuccess) e = launch_pdl(k_roll, dim3(1), dim3(1), 0, cap_st, S);
     if (e == cudaSuccess)
-      e = launch_pdl(k_apply_dot, vb, vt, 0, cap_st, cells_of(d), ih2,
-                     (const float*)p.as<float>(), f0, mg->bc_mode, q.as<float>(), S);
+      e = launch_pdl(k_apply_dot<MetaMask>, vb, vt, 0, cap_st, cells_of(d), ih2,
+                     (const float*)p.as<float>(), mk, mg->bc_mode, q.as<float>(), S);
     if (e == cudaSuccess)
-      e = launch_pdl(k_update_xr, vb, vt, 0, cap_st, cells_of(d), f0, (float*)nullptr,
+      e = launch_pdl(k_update_xr<MetaMask>, vb, vt, 0, cap_st, cells_of(d), mk, (float*)nullptr,
                      r.as<float>(), (const float*)p.as<float>(), (const float*)q.as<float>(), S,
                      (const CgCtl*)C);
     if (e == cudaSuccess)
@@ -766,11 +794,17 @@ size_t Solver::device_bytes() const {
 }
 
 int Solver::true_resid(cudaStream_t st, const float* phi, const float* b, double* rel,
-                       double* bn) {
+                       double* bn, bool cg) {
   PYRO_CU(cudaMemsetAsync(sc.p, 0, SC_N * 8, st));
-  launch_pdl(k_resid, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), 1.0 / ((double)mg->h[0] * mg->h[0]), phi, b,
-                                                   mg->f[0], mg->bc_mode, nullptr,
-                                                   sc.as<double>());
+  const dim3 vb(vec_blocks(d.cells())), vt(VT);
+  const double ih2 = 1.0 / ((double)mg->h[0] * mg->h[0]);
+  float* none = nullptr;
+  if (cg)
+    launch_pdl(k_resid<MetaMask>, vb, vt, 0, st, cells_of(d), ih2, phi, b,
+               MetaMask{pc.meta[0].as<uint8_t>()}, mg->bc_mode, none, sc.as<double>());
+  else
+    launch_pdl(k_resid<FlagMask>, vb, vt, 0, st, cells_of(d), ih2, phi, b,
+               FlagMask{mg->f[0]}, mg->bc_mode, none, sc.as<double>());
   PYRO_CU(cudaGetLastError());
   PYRO_CU(cudaMemcpyAsync(host_sc, sc.p, SC_N * 8, cudaMemcpyDeviceToHost, st));
   PYRO_CU(cudaStreamSynchronize(st));
@@ -800,18 +834,20 @@ int Solver::learned_stage(cudaStream_t st, float* phi, double* rr, PyroSolveInfo
       (rc = net->output(f0, mg->h[0], z.as<float>(), v, st)) || (rc = net->check_err(st)))
     return rc;
   PYRO_CU(cudaMemsetAsync(sc.p, 0, SC_N * 8, st));
-  launch_pdl(k_apply_dot, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), ih2, z.as<float>(), f0, mg->bc_mode,
-                                                       q.as<float>(), S);
-  launch_pdl(k_dots, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), f0, z.as<float>(), r.as<float>(), nullptr,
-                                                  S);
+  const MetaMask mk{pc.meta[0].as<uint8_t>()};
+  const dim3 vb(vec_blocks(d.cells())), vt(VT);
+  launch_pdl(k_apply_dot<MetaMask>, vb, vt, 0, st, cells_of(d), ih2, (const float*)z.as<float>(),
+             mk, mg->bc_mode, q.as<float>(), S);
+  launch_pdl(k_dots<MetaMask>, vb, vt, 0, st, cells_of(d), mk, (const float*)z.as<float>(),
+             (const float*)r.as<float>(), (const float*)nullptr, S);
   PYRO_CU(cudaGetLastError());
   PYRO_CU(cudaMemcpyAsync(host_sc, sc.p, SC_N * 8, cudaMemcpyDeviceToHost, st));
   PYRO_CU(cudaStreamSynchronize(st));
   const double re = host_sc[SC_RZN], eae = host_sc[SC_PQ];
   // <Ae, r>, <Ae, Ae>
   PYRO_CU(cudaMemsetAsync(sc.p, 0, SC_N * 8, st));
-  launch_pdl(k_dots, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), f0, q.as<float>(), r.as<float>(),
-                                                  q.as<float>(), S);
+  launch_pdl(k_dots<MetaMask>, vb, vt, 0, st, cells_of(d), mk, (const float*)q.as<float>(),
+             (const float*)r.as<float>(), (const float*)q.as<float>(), S);
   PYRO_CU(cudaGetLastError());
   PYRO_CU(cudaMemcpyAsync(host_sc, sc.p, SC_N * 8, cudaMemcpyDeviceToHost, st));
   PYRO_CU(cudaStreamSynchronize(st));
@@ -824,8 +860,9 @@ int Solver::learned_stage(cudaStream_t st, float* phi, double* rr, PyroSolveInfo
     host_sc[SC_RZ] = re;
     host_sc[SC_PQ] = eae;
     PYRO_CU(cudaMemcpyAsync(sc.p, host_sc, SC_N * 8, cudaMemcpyHostToDevice, st));
-    launch_pdl(k_update_xr, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), f0, phi, r.as<float>(),
-                                                         z.as<float>(), q.as<float>(), S, (const CgCtl*)nullptr);
+    launch_pdl(k_update_xr<MetaMask>, vb, vt, 0, st, cells_of(d), mk, phi, r.as<float>(),
+               (const float*)z.as<float>(), (const float*)q.as<float>(), S,
+               (const CgCtl*)nullptr);
     PYRO_CU(cudaGetLastError());
     PYRO_CU(cudaMemcpyAsync(host_sc, sc.p, SC_N * 8, cudaMemcpyDeviceToHost, st));
   }
@@ -868,16 +905,16 @@ int Solver::solve(cudaStream_t st, float* phi, const float* b, int mode, float t
       mg->bind_level0(save_phi, save_b, f0);
       PYRO_CU(e);
       iters = max_iters;
-      if ((rc = true_resid(st, phi, b, &rel, &bn)) != PYRO_OK) return rc;
+      if ((rc = true_resid(st, phi, b, &rel, &bn, false)) != PYRO_OK) return rc;
     } else {
-      if ((rc = true_resid(st, phi, b, &rel, &bn)) != PYRO_OK) return rc;
+      if ((rc = true_resid(st, phi, b, &rel, &bn, false)) != PYRO_OK) return rc;
       while (rel > tol && iters < max_iters) {
         mg->bind_level0(phi, b, f0);
         cudaError_t e = mg->vcycles(1, st);
         mg->bind_level0(save_phi, save_b, f0);
         PYRO_CU(e);
         iters++;
-        if ((rc = true_resid(st, phi, b, &rel, &bn)) != PYRO_OK) return rc;
+        if ((rc = true_resid(st, phi, b, &rel, &bn, false)) != PYRO_OK) return rc;
       }
     }
   } else {
@@ -915,8 +952,9 @@ int Solver::solve(cudaStream_t st, float* phi, const float* b, int mode, float t
       if ((rc = cg_loop(st, phi, bf16, bb2, tol, iters, max_iters)) != PYRO_OK) return rc;
       // true residual into r (and |r|, |b|)
       PYRO_CU(cudaMemsetAsync(sc.p, 0, SC_N * 8, st));
-      launch_pdl(k_resid, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d), ih2, phi, b,
-                 f0, mg->bc_mode, r.as<float>(), S);
+      launch_pdl(k_resid<MetaMask>, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d),
+                 ih2, (const float*)phi, b, MetaMask{pc.meta[0].as<uint8_t>()}, mg->bc_mode,
+                 r.as<float>(), S);
       PYRO_CU(cudaGetLastError());
       PYRO_CU(cudaMemcpyAsync(host_sc, sc.p, SC_N * 8, cudaMemcpyDeviceToHost, st));
       PYRO_CU(cudaMemcpyAsync(host_ctl, ctl.p, sizeof(CgCtl), cudaMemcpyDeviceToHost, st));
@@ -927,7 +965,7 @@ int Solver::solve(cudaStream_t st, float* phi, const float* b, int mode, float t
       restarts++;
       if (host_ctl->stalled) break;
     }
-    if (!rel_true && (rc = true_resid(st, phi, b, &rel, &bn)) != PYRO_OK) return rc;
+    if (!rel_true && (rc = true_resid(st, phi, b, &rel, &bn, true)) != PYRO_OK) return rc;
   }
   PYRO_CU(cudaEventRecord(ev1, st));
   PYRO_CU(cudaEventSynchronize(ev1));
@@ -948,7 +986,7 @@ int Solver::solve(cudaStream_t st, float* phi, const float* b, int mode, float t
 cudaError_t launch_mg_apply(Dims3 d, float h, const uint32_t* f, const float* p, float* q,
                             int bc_mode, cudaStream_t st) {
   return launch_pdl(k_apply, dim3(vec_blocks(d.cells())), dim3(VT), 0, st, cells_of(d),
-                    1.0 / ((double)h * h), p, f, bc_mode, q);
+                    1.0 / ((double)h * h), p, FlagMask{f}, bc_mode, q);
 }
 
 }  // namespace pyro

@@ -66,7 +66,10 @@ struct Solver {
 
  private:
   cudaError_t precond(cudaStream_t st, bool bf16, bool prep);
-  int true_resid(cudaStream_t st, const float* phi, const float* b, double* rel, double* bn);
+  // |b - A phi| / |b| and |b|; cg: on the CG modes' reachable set (their
+  // level-0 masks), else on the solid flags of level 0
+  int true_resid(cudaStream_t st, const float* phi, const float* b, double* rel, double* bn,
+                 bool cg);
   // phi += alpha net(r) when that lowers |r| (r = b - A phi on entry, kept
   // consistent); *rr is |r|^2 in and out.
   int learned_stage(cudaStream_t st, float* phi, double* rr, PyroSolveInfo* info);
