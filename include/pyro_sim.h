@@ -399,6 +399,17 @@ int pyro_k_mg_prolong_m(uint32_t fnx, uint32_t fny, uint32_t fnz,
                         const void* pc, const uint8_t* mf, void* pf,
                         uint32_t cnx, uint32_t cny, uint32_t cnz,
                         const uint8_t* mc, int storage, void* stream);
+/* The MGPCG preconditioner's restriction R = P^T / 8, P the fluid-weighted
+ * trilinear prolongation of pyro_k_mg_prolong_m: the residual
+ * r = b - A phi of each fluid fine cell, divided by its prolongation row's
+ * fluid weight sum, gathered into each fluid coarse cell with P's weights
+ * and divided by 8 (bc); the coarse guess pc is set to 0.  Waits for the
+ * stream (it allocates its temporaries). */
+int pyro_k_mg_restrict_sym(uint32_t fnx, uint32_t fny, uint32_t fnz, float fh,
+                           const void* pf, const void* bf, const uint8_t* mf,
+                           uint32_t cnx, uint32_t cny, uint32_t cnz,
+                           const uint8_t* mc, void* bc, void* pc, int bc_mode,
+                           int storage, void* stream);
 /* The fused first and last level-0 passes of the MGPCG preconditioner's
  * V-cycle (rows of even length; PYRO_E_INVALID otherwise).  pass_first:
  * the pass of `color` from phi = 0 with the FP32 right-hand side r, every

@@ -210,6 +210,8 @@ SIGNATURES = {
     "pyro_k_mg_meta": [_U32, _U32, _U32, _P, _P, _P],
     "pyro_k_mg_flags_down": [_U32, _U32, _U32, _P, _U32, _U32, _U32, _P, _P],
     "pyro_k_mg_pass": [_U32, _U32, _U32, _F, _P, _P, _P, _I, _F, _I, _I, _P],
+    "pyro_k_mg_restrict_sym": [_U32, _U32, _U32, _F, _P, _P, _P, _U32, _U32, _U32, _P, _P, _P,
+                               _I, _I, _P],
     "pyro_k_mg_pass_first": [_U32, _U32, _U32, _F, _P, _P, _P, _P, _I, _F, _I, _I, _P],
     "pyro_k_mg_pass_last": [_U32, _U32, _U32, _F, _P, _P, _P, _P, _I, _F, _I, _P],
     "pyro_k_mg_restrict_m": [_U32, _U32, _U32, _F, _P, _P, _P, _U32, _U32, _U32, _P, _P, _I,

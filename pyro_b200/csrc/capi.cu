@@ -327,6 +327,36 @@ int pyro_k_mg_prolong_m(uint32_t fnx, uint32_t fny, uint32_t fnz, const void* pc
              "pyro_k_mg_prolong_m");
 }
 
+int pyro_k_mg_restrict_sym(uint32_t fnx, uint32_t fny, uint32_t fnz, float fh, const void* pf,
+                           const void* bf, const uint8_t* mf, uint32_t cnx, uint32_t cny,
+                           uint32_t cnz, const uint8_t* mc, void* bc, void* pc, int bc_mode,
+                           int storage, void* stream) {
+  clear_error();
+  PYRO_REQUIRE(dims_ok(fnx, fny, fnz), "pyro_k_mg_restrict_sym: invalid grid dimensions");
+  PYRO_REQUIRE(cnx == (fnx + 1) / 2 && cny == (fny + 1) / 2 && cnz == (fnz + 1) / 2,
+               "pyro_k_mg_restrict_sym: coarse dims must be ceil(fine / 2)");
+  PYRO_REQUIRE(pf && bf && mf && mc && bc && pc, "pyro_k_mg_restrict_sym: null buffer");
+  PYRO_REQUIRE(bc_mode == 0 || bc_mode == 1, "pyro_k_mg_restrict_sym: bc_mode must be 0 or 1");
+  PYRO_REQUIRE(storage == PYRO_MG_F32 || storage == PYRO_MG_BF16,
+               "pyro_k_mg_restrict_sym: storage must be PYRO_MG_F32 or PYRO_MG_BF16");
+  Dims3 df{(int)fnx, (int)fny, (int)fnz}, dc{(int)cnx, (int)cny, (int)cnz};
+  const bool lo = storage == PYRO_MG_BF16;
+  DevBuf wq, rt;
+  int rc = wq.alloc(df.cells());
+  if (rc == PYRO_OK) rc = rt.alloc(df.cells() * (lo ? 2 : 4));
+  if (rc != PYRO_OK) return rc;
+  cudaStream_t st = S(stream);
+  PYRO_CU(launch_mg_wsum(df, mf, dc, mc, wq.as<uint8_t>(), st));
+  PYRO_CU(lo ? launch_mg_restrict_sym_bf16(df, fh, pf, bf, mf, wq.as<uint8_t>(), rt.p, dc, mc, bc,
+                                           pc, bc_mode, st)
+             : launch_mg_restrict_sym(df, fh, (const float*)pf, (const float*)bf, mf,
+                                      wq.as<uint8_t>(), rt.as<float>(), dc, mc, (float*)bc,
+                                      (float*)pc, bc_mode, st));
+  // the temporaries are freed on return
+  PYRO_CU(cudaStreamSynchronize(st));
+  return PYRO_OK;
+}
+
 int pyro_k_mg_resid(uint32_t nx, uint32_t ny, uint32_t nz, float h, const float* phi,
                     const float* b, const uint32_t* flags, float* stats, void* stream) {
   clear_error();

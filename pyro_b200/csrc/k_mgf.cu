@@ -600,14 +600,46 @@ __device__ __forceinline__ float pw1(int c, int J, int nc) {
   return w;
 }
 
+// 64 W_c for each fluid fine cell c: W_c is the fluid weight sum of c's
+// prolongation row, a sum of products of the per-axis weights 1/4 and 3/4
+// (clamped taps counted per corner), so a multiple of 1/64 in [0, 1] and the
+// byte is exact; 0 for solid cells.  Built once per flag field.
+__global__ void __launch_bounds__(256) k_mg_wsum(L d, const uint8_t* __restrict__ m0, L dc,
+                                                 const uint8_t* __restrict__ mc,
+                                                 uint8_t* __restrict__ wq) {
+  pdl_trigger();
+  pdl_wait();
+  int x = blockIdx.x * 32 + threadIdx.x;
+  int y = blockIdx.y * 4 + threadIdx.y;
+  int z = blockIdx.z * 2 + threadIdx.z;
+  if (!d.inb(x, y, z)) return;
+  int i = d.idx(x, y, z);
+  float W = 0.0f;
+  if (!(__ldg(m0 + i) & META_SOLID)) {
+    float gx = ((float)x + 0.5f) * 0.5f - 0.5f, gy = ((float)y + 0.5f) * 0.5f - 0.5f,
+          gz = ((float)z + 0.5f) * 0.5f - 0.5f;
+    int ix = (int)floorf(gx), iy = (int)floorf(gy), iz = (int)floorf(gz);
+    float fx = gx - (float)ix, fy = gy - (float)iy, fz = gz - (float)iz;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      int ox = k & 1, oy = (k >> 1) & 1, oz = (k >> 2) & 1;
+      int cx = min(max(ix + ox, 0), dc.nx - 1), cy = min(max(iy + oy, 0), dc.ny - 1),
+          cz = min(max(iz + oz, 0), dc.nz - 1);
+      if (__ldg(mc + dc.idx(cx, cy, cz)) & META_SOLID) continue;
+      W += (ox ? fx : 1.0f - fx) * (oy ? fy : 1.0f - fy) * (oz ? fz : 1.0f - fz);
+    }
+  }
+  wq[i] = (uint8_t)(int)(W * 64.0f);
+}
+
 // r~ = (b - A p) / W_c for fluid fine cells whose prolongation row is not
-// empty, else 0.
+// empty (wq = 64 W_c from k_mg_wsum), else 0.
 template <typename TS>
 __global__ void __launch_bounds__(256) k_mg_resid_w(L d, float h2, const TS* __restrict__ p,
                                                     const TS* __restrict__ b,
-                                                    const uint8_t* __restrict__ m0, L dc,
-                                                    const uint8_t* __restrict__ mc,
-                                                    int bc_mode, TS* __restrict__ rt) {
+                                                    const uint8_t* __restrict__ m0,
+                                                    const uint8_t* __restrict__ wq, int bc_mode,
+                                                    TS* __restrict__ rt) {
   pdl_trigger();
   pdl_wait();
   int x = blockIdx.x * 32 + threadIdx.x;
@@ -616,8 +648,9 @@ __global__ void __launch_bounds__(256) k_mg_resid_w(L d, float h2, const TS* __r
   if (!d.inb(x, y, z)) return;
   int i = d.idx(x, y, z);
   uint32_t m = __ldg(m0 + i);
+  const uint32_t w = __ldg(wq + i);
   float out = 0.0f;
-  if (!(m & META_SOLID)) {
+  if (!(m & META_SOLID) && w != 0u) {
     const int sy = d.nx, sz = d.nx * d.ny;
     float sum = 0.0f;
     if (m & 1u) sum += ldv(p + i + 1);
@@ -628,25 +661,15 @@ __global__ void __launch_bounds__(256) k_mg_resid_w(L d, float h2, const TS* __r
     if (m & 32u) sum += ldv(p + i - sz);
     float cnt = (float)(__popc(m & 63u) + dirichlet_faces(d, x, y, z, bc_mode));
     float r = ldv(b + i) - (sum - cnt * ldv(p + i)) / h2;
-    float gx = ((float)x + 0.5f) * 0.5f - 0.5f, gy = ((float)y + 0.5f) * 0.5f - 0.5f,
-          gz = ((float)z + 0.5f) * 0.5f - 0.5f;
-    int ix = (int)floorf(gx), iy = (int)floorf(gy), iz = (int)floorf(gz);
-    float fx = gx - (float)ix, fy = gy - (float)iy, fz = gz - (float)iz;
-    float W = 0.0f;
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-      int ox = k & 1, oy = (k >> 1) & 1, oz = (k >> 2) & 1;
-      int cx = min(max(ix + ox, 0), dc.nx - 1), cy = min(max(iy + oy, 0), dc.ny - 1),
-          cz = min(max(iz + oz, 0), dc.nz - 1);
-      if (__ldg(mc + dc.idx(cx, cy, cz)) & META_SOLID) continue;
-      W += (ox ? fx : 1.0f - fx) * (oy ? fy : 1.0f - fy) * (oz ? fz : 1.0f - fz);
-    }
-    if (W > 1e-4f) out = r / W;
+    out = r / ((float)w * 0.015625f);
   }
   stv(rt + i, out);
 }
 
-// Coarse rhs = (1/8) sum_c P[c,J] r~[c]; coarse guess 0.
+// Coarse rhs = (1/8) sum_c P[c,J] r~[c]; coarse guess 0.  A coarse cell
+// with a neighbour on each side along every axis (1 <= X <= nc - 2) takes
+// the fine cells 2X - 1 .. 2X + 2 with weights 1/4, 3/4, 3/4, 1/4 per axis
+// and sums them axis by axis; the others evaluate the clamped weights.
 template <typename TS>
 __global__ void __launch_bounds__(256) k_mg_restrict_t(L df, const TS* __restrict__ rt,
                                                        const uint8_t* __restrict__ mf, L dc,
@@ -661,25 +684,44 @@ __global__ void __launch_bounds__(256) k_mg_restrict_t(L df, const TS* __restric
   int J = dc.idx(X, Y, Z);
   float acc = 0.0f;
   if (!(__ldg(mc + J) & META_SOLID)) {
-    float wx[4], wy[4], wz[4];
+    const bool inner = X >= 1 && X <= dc.nx - 2 && Y >= 1 && Y <= dc.ny - 2 && Z >= 1 &&
+                       Z <= dc.nz - 2;
+    if (inner) {
+      const TS* base = rt + df.idx(2 * X - 1, 2 * Y - 1, 2 * Z - 1);
+      const int sy = df.nx, sz = df.nx * df.ny;
+      float tz[4];
 #pragma unroll
-    for (int a = 0; a < 4; a++) {
-      int cx = 2 * X - 1 + a, cy = 2 * Y - 1 + a, cz = 2 * Z - 1 + a;
-      wx[a] = (cx >= 0 && cx < df.nx) ? pw1(cx, X, dc.nx) : 0.0f;
-      wy[a] = (cy >= 0 && cy < df.ny) ? pw1(cy, Y, dc.ny) : 0.0f;
-      wz[a] = (cz >= 0 && cz < df.nz) ? pw1(cz, Z, dc.nz) : 0.0f;
-    }
+      for (int c = 0; c < 4; c++) {
+        float ty[4];
 #pragma unroll
-    for (int c = 0; c < 4; c++) {
-      if (wz[c] == 0.0f) continue;
+        for (int bb = 0; bb < 4; bb++) {
+          const TS* row = base + c * sz + bb * sy;
+          ty[bb] = 0.25f * (ldv(row) + ldv(row + 3)) + 0.75f * (ldv(row + 1) + ldv(row + 2));
+        }
+        tz[c] = 0.25f * (ty[0] + ty[3]) + 0.75f * (ty[1] + ty[2]);
+      }
+      acc = 0.25f * (tz[0] + tz[3]) + 0.75f * (tz[1] + tz[2]);
+    } else {
+      float wx[4], wy[4], wz[4];
 #pragma unroll
-      for (int bb = 0; bb < 4; bb++) {
-        if (wy[bb] == 0.0f) continue;
+      for (int a = 0; a < 4; a++) {
+        int cx = 2 * X - 1 + a, cy = 2 * Y - 1 + a, cz = 2 * Z - 1 + a;
+        wx[a] = (cx >= 0 && cx < df.nx) ? pw1(cx, X, dc.nx) : 0.0f;
+        wy[a] = (cy >= 0 && cy < df.ny) ? pw1(cy, Y, dc.ny) : 0.0f;
+        wz[a] = (cz >= 0 && cz < df.nz) ? pw1(cz, Z, dc.nz) : 0.0f;
+      }
 #pragma unroll
-        for (int a = 0; a < 4; a++) {
-          if (wx[a] == 0.0f) continue;
-          int i = df.idx(2 * X - 1 + a, 2 * Y - 1 + bb, 2 * Z - 1 + c);
-          acc += wx[a] * wy[bb] * wz[c] * ldv(rt + i);
+      for (int c = 0; c < 4; c++) {
+        if (wz[c] == 0.0f) continue;
+#pragma unroll
+        for (int bb = 0; bb < 4; bb++) {
+          if (wy[bb] == 0.0f) continue;
+#pragma unroll
+          for (int a = 0; a < 4; a++) {
+            if (wx[a] == 0.0f) continue;
+            int i = df.idx(2 * X - 1 + a, 2 * Y - 1 + bb, 2 * Z - 1 + c);
+            acc += wx[a] * wy[bb] * wz[c] * ldv(rt + i);
+          }
         }
       }
     }
@@ -872,27 +914,32 @@ cudaError_t launch_mg_restrict_m_bf16(Dims3 df, float h, const void* pf, const v
 }
 template <typename TS>
 cudaError_t restrict_sym_t(Dims3 df, float h, const TS* pf, const TS* bf, const uint8_t* mf,
-                           TS* rt, Dims3 dc, const uint8_t* mc, TS* bc, TS* pc, int bc_mode,
-                           cudaStream_t st) {
+                           const uint8_t* wq, TS* rt, Dims3 dc, const uint8_t* mc, TS* bc,
+                           TS* pc, int bc_mode, cudaStream_t st) {
   cudaError_t e = launch_pdl(k_mg_resid_w<TS>, g3(df), dim3(32, 4, 2), 0, st,
-                             L{df.nx, df.ny, df.nz}, h * h, pf, bf, mf, L{dc.nx, dc.ny, dc.nz},
-                             mc, bc_mode, rt);
+                             L{df.nx, df.ny, df.nz}, h * h, pf, bf, mf, wq, bc_mode, rt);
   if (e != cudaSuccess) return e;
   return launch_pdl(k_mg_restrict_t<TS>, g3(dc), dim3(32, 4, 2), 0, st, L{df.nx, df.ny, df.nz},
                     (const TS*)rt, mf, L{dc.nx, dc.ny, dc.nz}, mc, bc, pc);
 }
 
+cudaError_t launch_mg_wsum(Dims3 df, const uint8_t* mf, Dims3 dc, const uint8_t* mc,
+                           uint8_t* wq, cudaStream_t st) {
+  return launch_pdl(k_mg_wsum, g3(df), dim3(32, 4, 2), 0, st, L{df.nx, df.ny, df.nz}, mf,
+                    L{dc.nx, dc.ny, dc.nz}, mc, wq);
+}
 cudaError_t launch_mg_restrict_sym(Dims3 df, float h, const float* pf, const float* bf,
-                                   const uint8_t* mf, float* rt, Dims3 dc, const uint8_t* mc,
-                                   float* bc, float* pc, int bc_mode, cudaStream_t st) {
-  return restrict_sym_t<float>(df, h, pf, bf, mf, rt, dc, mc, bc, pc, bc_mode, st);
+                                   const uint8_t* mf, const uint8_t* wq, float* rt, Dims3 dc,
+                                   const uint8_t* mc, float* bc, float* pc, int bc_mode,
+                                   cudaStream_t st) {
+  return restrict_sym_t<float>(df, h, pf, bf, mf, wq, rt, dc, mc, bc, pc, bc_mode, st);
 }
 cudaError_t launch_mg_restrict_sym_bf16(Dims3 df, float h, const void* pf, const void* bf,
-                                        const uint8_t* mf, void* rt, Dims3 dc,
-                                        const uint8_t* mc, void* bc, void* pc, int bc_mode,
-                                        cudaStream_t st) {
+                                        const uint8_t* mf, const uint8_t* wq, void* rt,
+                                        Dims3 dc, const uint8_t* mc, void* bc, void* pc,
+                                        int bc_mode, cudaStream_t st) {
   using T = __nv_bfloat16;
-  return restrict_sym_t<T>(df, h, (const T*)pf, (const T*)bf, mf, (T*)rt, dc, mc, (T*)bc,
+  return restrict_sym_t<T>(df, h, (const T*)pf, (const T*)bf, mf, wq, (T*)rt, dc, mc, (T*)bc,
                            (T*)pc, bc_mode, st);
 }
 

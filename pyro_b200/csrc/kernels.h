@@ -158,16 +158,21 @@ cudaError_t launch_mg_restrict_m_bf16(Dims3 df, float h, const void* pf, const v
                                       const uint8_t* mf, Dims3 dc, void* bc, void* pc,
                                       int bc_mode, cudaStream_t st);
 
-// Symmetric V-cycle pieces for the MGPCG preconditioner: residual divided
-// by the fluid prolongation weight into `rt`, then the transpose (P^T / 8)
-// restriction; the coarse solve alternating red-black / black-red.
+// Symmetric V-cycle pieces for the MGPCG preconditioner: wsum gives each
+// fine cell 64 x its fluid prolongation weight sum (a byte, exact; once per
+// flag field); the restriction divides the residual by that weight into
+// `rt`, then applies the transpose (P^T / 8); the coarse solve alternates
+// red-black / black-red.
+cudaError_t launch_mg_wsum(Dims3 df, const uint8_t* mf, Dims3 dc, const uint8_t* mc,
+                           uint8_t* wq, cudaStream_t st);
 cudaError_t launch_mg_restrict_sym(Dims3 df, float h, const float* pf, const float* bf,
-                                   const uint8_t* mf, float* rt, Dims3 dc, const uint8_t* mc,
-                                   float* bc, float* pc, int bc_mode, cudaStream_t st);
+                                   const uint8_t* mf, const uint8_t* wq, float* rt, Dims3 dc,
+                                   const uint8_t* mc, float* bc, float* pc, int bc_mode,
+                                   cudaStream_t st);
 cudaError_t launch_mg_restrict_sym_bf16(Dims3 df, float h, const void* pf, const void* bf,
-                                        const uint8_t* mf, void* rt, Dims3 dc,
-                                        const uint8_t* mc, void* bc, void* pc, int bc_mode,
-                                        cudaStream_t st);
+                                        const uint8_t* mf, const uint8_t* wq, void* rt,
+                                        Dims3 dc, const uint8_t* mc, void* bc, void* pc,
+                                        int bc_mode, cudaStream_t st);
 cudaError_t launch_mg_coarse_sym(Dims3 d, float h, const float* b, const uint32_t* f, float* p,
                                  int iters, float omega, int bc_mode, cudaStream_t st);
 cudaError_t launch_mg_coarse_sym_bf16(Dims3 d, float h, const void* b, const uint32_t* f,

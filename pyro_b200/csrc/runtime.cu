@@ -130,6 +130,7 @@ size_t Multigrid::device_bytes() const {
   size_t s = 0;
   for (size_t l = 1; l < dims.size(); l++) s += own_phi[l].bytes + own_b[l].bytes + own_f[l].bytes;
   for (size_t l = 0; l < dims.size(); l++) s += phi2[l].bytes + meta[l].bytes;
+  for (const DevBuf& w : wq) s += w.bytes;
   return s;
 }
 
@@ -156,6 +157,18 @@ cudaError_t Multigrid::prepare(cudaStream_t st) {
   for (int l = 0; l < nl; l++)
     if ((e = launch_mg_meta(dims[l], f[l], meta[l].as<uint8_t>(), st)) != cudaSuccess) return e;
   return cudaSuccess;
+}
+
+cudaError_t Multigrid::prepare_sym(cudaStream_t st) {
+  cudaError_t e = prepare(st);
+  const int nl = (int)dims.size();
+  if (wq.size() != dims.size()) wq.resize(dims.size());
+  for (int l = 0; e == cudaSuccess && l + 1 < nl; l++) {
+    if (!wq[l].p && wq[l].alloc(dims[l].cells()) != PYRO_OK) return cudaErrorMemoryAllocation;
+    e = launch_mg_wsum(dims[l], meta[l].as<uint8_t>(), dims[l + 1], meta[l + 1].as<uint8_t>(),
+                       wq[l].as<uint8_t>(), st);
+  }
+  return e;
 }
 
 cudaError_t Multigrid::vcycles(int cycles, cudaStream_t st) {
@@ -212,7 +225,7 @@ cudaError_t Multigrid::vcycle_sym(cudaStream_t st, DevBuf* bphi, DevBuf* bphi2, 
       }
     }
   }
-  if (prep && (e = prepare(st)) != cudaSuccess) return e;
+  if (prep && (e = prepare_sym(st)) != cudaSuccess) return e;
   auto M = [&](int l) { return meta[l].as<uint8_t>(); };
   // storage of level l: phi, b, scratch
   auto P = [&](int l) -> void* { return lo ? bphi[l].p : (void*)phi[l]; };
@@ -246,10 +259,11 @@ cudaError_t Multigrid::vcycle_sym(cudaStream_t st, DevBuf* bphi, DevBuf* bphi2, 
                 : pass(l, c, 1.0f);
         if (e != cudaSuccess) return e;
       }
-    e = lo ? launch_mg_restrict_sym_bf16(dims[l], h[l], P(l), B(l), M(l), T(l), dims[l + 1],
+    const uint8_t* W = wq[l].as<uint8_t>();
+    e = lo ? launch_mg_restrict_sym_bf16(dims[l], h[l], P(l), B(l), M(l), W, T(l), dims[l + 1],
                                          M(l + 1), B(l + 1), P(l + 1), bc_mode, st)
            : launch_mg_restrict_sym(dims[l], h[l], (const float*)P(l), (const float*)B(l), M(l),
-                                    (float*)T(l), dims[l + 1], M(l + 1), (float*)B(l + 1),
+                                    W, (float*)T(l), dims[l + 1], M(l + 1), (float*)B(l + 1),
                                     (float*)P(l + 1), bc_mode, st);
     if (e != cudaSuccess) return e;
   }

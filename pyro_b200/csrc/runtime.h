@@ -99,6 +99,7 @@ struct Multigrid {
   std::vector<DevBuf> own_phi, own_b, own_f;
   std::vector<DevBuf> phi2;   // ping-pong partner of phi on every level
   std::vector<DevBuf> meta;   // per-cell neighbour mask (k_mgf.cu)
+  std::vector<DevBuf> wq;     // 64 x prolongation weight sums (vcycle_sym, levels < last)
   bool coarse_one_cta = false;
   float* stats = nullptr;  // device, for mg_resid
 
@@ -115,6 +116,8 @@ struct Multigrid {
   // Coarse solid flags and neighbour masks of every level from the bound
   // level-0 flags; the V-cycles below need them (once per new flag field).
   cudaError_t prepare(cudaStream_t st);
+  // prepare() and the weight sums of the symmetric V-cycle's restriction.
+  cudaError_t prepare_sym(cudaStream_t st);
   // `cycles` V-cycles (src/sim.rs:451-491) on the bound level-0 arrays with
   // the fused kernels (k_mgf.cu); calls prepare() first.
   cudaError_t vcycles(int cycles, cudaStream_t st);
@@ -125,8 +128,8 @@ struct Multigrid {
   // in BF16 (FP32 arithmetic).  The initial guess is zero: level 0's phi is
   // not read, the result overwrites all of it (FP32), and level 0's b is the
   // FP32 right-hand side in both storages.
-  // prep = false skips the per-level masks (valid while the level flags
-  // are unchanged since the last prepare()).
+  // prep = false skips the per-level masks and weights (valid while the
+  // level flags are unchanged since the last prepare_sym()).
   cudaError_t vcycle_sym(cudaStream_t st, DevBuf* bphi, DevBuf* bphi2, DevBuf* bb,
                          bool prep = true);
   size_t device_bytes() const;

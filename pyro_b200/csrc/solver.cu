@@ -638,7 +638,7 @@ int Solver::begin_cg(cudaStream_t st, float* phi, const float* b) {
   pc_ready = false;
   if ((rc = update_reach(st, h)) != PYRO_OK) return rc;
   pc.bind_level0(z.as<float>(), r.as<float>(), fa.as<uint32_t>());
-  PYRO_CU(pc.prepare(st));
+  PYRO_CU(pc.prepare_sym(st));
   if (direct) {
     direct->f = pc.f.back();  // level 0's flags when the grid is the coarsest level
     if ((rc = direct->refresh(st)) != PYRO_OK) return rc;

@@ -318,6 +318,62 @@ def test_mg_fused_first_and_last_passes_equal_the_plain_pass(lib, nx, ny, nz, se
         assert np.array_equal(host(pd), _bf16_bits(p))
 
 
+@pytest.mark.parametrize("nx,ny,nz,seed,h", [(32, 48, 32, 0, 0.05), (19, 46, 19, 1, 0.16),
+                                             (38, 40, 20, 8, 0.16), (150, 96, 24, 9, 0.02)])
+@pytest.mark.parametrize("bc_mode", [0, 1])
+def test_mg_symmetric_restriction_is_the_adjoint_of_the_prolongation(lib, nx, ny, nz, seed, h,
+                                                                     bc_mode):
+    """The CG preconditioner's restriction R = P^T / 8 of the fluid-weighted
+    prolongation P (pyro_k_mg_prolong_m, pinned to mg.wgsl above): for random
+    fine r and coarse e, <R r, e> = <r, P e> / 8 (FP64 sums of the FP32
+    results), and with phi = 0 the coarse guess is cleared.  BF16 storage
+    gives the same restriction within its rounding."""
+    rng = np.random.default_rng(300 + seed)
+    f = (rng.random((nz, ny, nx)) < 0.25).astype(np.uint32)
+    cx, cy, cz = (nx + 1) // 2, (ny + 1) // 2, (nz + 1) // 2
+    fd = dev(f)
+    fc = dev(np.zeros((cz, cy, cx), np.uint32))
+    assert lib.pyro_k_mg_flags_down(nx, ny, nz, ptr(fd), cx, cy, cz, ptr(fc), None) == 0
+    mf = dev(np.zeros((nz, ny, nx), np.uint8))
+    mc = dev(np.zeros((cz, cy, cx), np.uint8))
+    assert lib.pyro_k_mg_meta(nx, ny, nz, ptr(fd), ptr(mf), None) == 0
+    assert lib.pyro_k_mg_meta(cx, cy, cz, ptr(fc), ptr(mc), None) == 0
+    zero_f = dev(np.zeros((nz, ny, nx), np.float32))
+    for k in range(3):
+        r = rng.normal(0, 1, (nz, ny, nx)).astype(np.float32)
+        e = rng.normal(0, 1, (cz, cy, cx)).astype(np.float32)
+        bc, pc = dev(np.ones((cz, cy, cx), np.float32)), dev(np.ones((cz, cy, cx), np.float32))
+        assert lib.pyro_k_mg_restrict_sym(nx, ny, nz, h, ptr(zero_f), ptr(dev(r)), ptr(mf), cx,
+                                          cy, cz, ptr(mc), ptr(bc), ptr(pc), bc_mode,
+                                          _abi.MG_F32, None) == 0, lib.pyro_last_error()
+        Rr = host(bc)
+        assert not host(pc).any()
+        pe = dev(np.zeros((nz, ny, nx), np.float32))
+        assert lib.pyro_k_mg_prolong_m(nx, ny, nz, ptr(dev(e)), ptr(mf), ptr(pe), cx, cy, cz,
+                                       ptr(mc), _abi.MG_F32, None) == 0
+        Pe = host(pe)
+        fl = f == 0
+        lhs = float(np.dot(Rr.ravel().astype(np.float64), e.ravel().astype(np.float64)))
+        rhs = float(np.dot(np.where(fl, r, 0).ravel().astype(np.float64),
+                           Pe.ravel().astype(np.float64))) / 8.0
+        scale = float(np.linalg.norm(Rr) * np.linalg.norm(e))
+        assert abs(lhs - rhs) <= 1e-5 * scale, (k, lhs, rhs, scale)
+        if k == 0:
+            rb = _bf16_bits(r)
+            bb, pb = dev(np.zeros((cz, cy, cx), np.uint16)), dev(np.ones((cz, cy, cx), np.uint16))
+            assert lib.pyro_k_mg_restrict_sym(nx, ny, nz, h, ptr(dev(np.zeros_like(rb))),
+                                              ptr(dev(rb)), ptr(mf), cx, cy, cz, ptr(mc),
+                                              ptr(bb), ptr(pb), bc_mode, _abi.MG_BF16,
+                                              None) == 0
+            assert not host(pb).any()
+            bf = dev(np.zeros((cz, cy, cx), np.float32))
+            assert lib.pyro_k_mg_restrict_sym(nx, ny, nz, h, ptr(zero_f), ptr(dev(_bf16_val(rb))),
+                                              ptr(mf), cx, cy, cz, ptr(mc), ptr(bf), ptr(pc),
+                                              bc_mode, _abi.MG_F32, None) == 0
+            lo, hi = _bf16_val(host(bb)), host(bf)
+            assert np.abs(lo - hi).max() <= 2e-2 * np.abs(hi).max()
+
+
 def test_mg_fused_passes_refuse_odd_rows(lib):
     z = dev(np.zeros(9 * 8 * 4, np.float32))
     m = dev(np.zeros(9 * 8 * 4, np.uint8))
