@@ -210,6 +210,14 @@ cudaError_t Multigrid::vcycles(int cycles, cudaStream_t st) {
   return cudaSuccess;
 }
 
+// Red-black sweeps before and after the coarse correction on level l of the
+// symmetric V-cycle: 2 on level 0, 4 on the coarser levels, whose passes
+// cost a fraction of level 0's.  Measured on the 2 cm pool's system and the
+// 256^3 case against 1..4 sweeps on level 0 and 1..8 below: fewer CG
+// iterations pay for the extra coarse passes (BF16 MGPCG to 1e-4 on the
+// pool: 8 iterations, 4.6 ms with 2 / 2; 6 iterations, 3.9 ms with 2 / 4).
+static int sym_sweeps(int l) { return l == 0 ? 2 : 4; }
+
 cudaError_t Multigrid::vcycle_sym(cudaStream_t st, DevBuf* bphi, DevBuf* bphi2, DevBuf* bb,
                                    bool prep) {
   int nl = (int)dims.size();
@@ -251,7 +259,7 @@ cudaError_t Multigrid::vcycle_sym(cudaStream_t st, DevBuf* bphi, DevBuf* bphi2, 
                                bc_mode, st);
   };
   for (int l = 0; l < nl - 1; l++) {
-    for (int it = 0; it < 2; it++)
+    for (int it = 0; it < sym_sweeps(l); it++)
       for (int c = 0; c < 2; c++) {
         e = (fuse && l == 0 && it == 0 && c == 0)
                 ? launch_mg_pass_first(dims[0], h[0], b[0], lo ? bb[0].p : nullptr, M(0), P(0), 0,
@@ -285,9 +293,9 @@ cudaError_t Multigrid::vcycle_sym(cudaStream_t st, DevBuf* bphi, DevBuf* bphi2, 
            : launch_mg_prolong_m(dims[l], (const float*)P(l + 1), M(l), (float*)P(l),
                                  dims[l + 1], M(l + 1), st);
     if (e != cudaSuccess) return e;
-    for (int it = 0; it < 2; it++)
+    for (int it = 0; it < sym_sweeps(l); it++)
       for (int c = 1; c >= 0; c--) {
-        e = (fuse && lo && l == 0 && it == 1 && c == 0)
+        e = (fuse && lo && l == 0 && it == sym_sweeps(0) - 1 && c == 0)
                 ? launch_mg_pass_last_f32(dims[0], h[0], B(0), M(0), P(0), phi[0], 0, 1.0f,
                                           bc_mode, st)
                 : pass(l, c, 1.0f);
