@@ -411,7 +411,7 @@ int pyro_k_mg_restrict_sym(uint32_t fnx, uint32_t fny, uint32_t fnz, float fh,
                            const uint8_t* mc, void* bc, void* pc, int bc_mode,
                            int storage, void* stream);
 /* The fused first and last level-0 passes of the MGPCG preconditioner's
- * V-cycle (rows of even length; PYRO_E_INVALID otherwise).  pass_first:
+ * V-cycle.  pass_first:
  * the pass of `color` from phi = 0 with the FP32 right-hand side r, every
  * cell of phi written (cells not updated get 0); with BF16 storage r is
  * also written rounded to BF16 into bq and used rounded.  pass_last: the

@@ -264,7 +264,6 @@ int pyro_k_mg_pass_first(uint32_t nx, uint32_t ny, uint32_t nz, float h, const f
   clear_error();
   PYRO_REQUIRE(dims_ok(nx, ny, nz), "pyro_k_mg_pass_first: invalid grid dimensions");
   Dims3 d{(int)nx, (int)ny, (int)nz};
-  PYRO_REQUIRE(mg_pass_fused_ok(d), "pyro_k_mg_pass_first: rows of even length only");
   PYRO_REQUIRE(r && meta && phi && (storage != PYRO_MG_BF16 || bq),
                "pyro_k_mg_pass_first: null buffer");
   PYRO_REQUIRE(color == 0 || color == 1, "pyro_k_mg_pass_first: color must be 0 or 1");
@@ -282,7 +281,6 @@ int pyro_k_mg_pass_last(uint32_t nx, uint32_t ny, uint32_t nz, float h, const vo
   clear_error();
   PYRO_REQUIRE(dims_ok(nx, ny, nz), "pyro_k_mg_pass_last: invalid grid dimensions");
   Dims3 d{(int)nx, (int)ny, (int)nz};
-  PYRO_REQUIRE(mg_pass_fused_ok(d), "pyro_k_mg_pass_last: rows of even length only");
   PYRO_REQUIRE(b && meta && phi && out, "pyro_k_mg_pass_last: null buffer");
   PYRO_REQUIRE(color == 0 || color == 1, "pyro_k_mg_pass_last: color must be 0 or 1");
   PYRO_REQUIRE(bc_mode == 0 || bc_mode == 1, "pyro_k_mg_pass_last: bc_mode must be 0 or 1");

@@ -8,10 +8,12 @@
 //    (k = +x,-x,+y,-y,+z,-z) = neighbour k is inside the level and fluid,
 //    bit 6 = the cell is solid.  The smoother's neighbour count is the
 //    popcount plus the Dirichlet faces the cell touches.
-//  * k_mg_pass4z updates the cells of one colour in 4-cell row chunks,
-//    two planes per thread, with the colour parity the same across each
-//    warp (no per-lane selects); k_mg_restrict_m / k_mg_prolong_m work one
-//    thread per coarse cell.
+//  * k_mg_pass4z / k_mg_pass2z update the cells of one colour in 4-cell
+//    (rows of a multiple of 4) or 2-cell (other even rows) chunks, one to
+//    four planes per thread, with the colour parity the same across each
+//    warp (no per-lane selects); odd rows take k_mg_pass, one colour cell
+//    per thread; k_mg_restrict_m / k_mg_prolong_m work one thread per
+//    coarse cell.
 //
 // Per-cell arithmetic is the reference's, in its order, so results equal the
 // per-pass kernels bit for bit.
@@ -200,36 +202,6 @@ __global__ void __launch_bounds__(256) k_mg_prolong_m(L df, const TS* __restrict
   }
 }
 
-// One colour pass with the neighbour mask: thread (hx, y, z) updates the
-// cell x = 2 hx + ((y + z + colour) & 1) (mg.wgsl:17-36) reading its own
-// mask and b and the neighbours the mask marks.
-template <typename TS>
-__global__ void __launch_bounds__(256) k_mg_pass(L d, float h2, const TS* __restrict__ b,
-                                                 const uint8_t* __restrict__ meta,
-                                                 TS* __restrict__ p, int color, float omega,
-                                                 int bc_mode) {
-  pdl_trigger();
-  pdl_wait();
-  int y = blockIdx.y * 4 + threadIdx.y;
-  int z = blockIdx.z * 2 + threadIdx.z;
-  int x = (int)(blockIdx.x * 32 + threadIdx.x) * 2 + ((y + z + color) & 1);
-  if (x >= d.nx || y >= d.ny || z >= d.nz) return;
-  int i = d.idx(x, y, z);
-  uint32_t m = __ldg(meta + i);
-  if (m & META_SOLID) return;
-  const int sy = d.nx, sz = d.nx * d.ny;
-  float sum = 0.0f;
-  if (m & 1u) sum += ldv(p + i + 1);
-  if (m & 2u) sum += ldv(p + i - 1);
-  if (m & 4u) sum += ldv(p + i + sy);
-  if (m & 8u) sum += ldv(p + i - sy);
-  if (m & 16u) sum += ldv(p + i + sz);
-  if (m & 32u) sum += ldv(p + i - sz);
-  float cnt = (float)(__popc(m & 63u) + dirichlet_faces(d, x, y, z, bc_mode));
-  if (cnt < 0.5f) return;
-  stv(p + i, wmix(ldv(p + i), (sum - h2 * ldv(b + i)) / cnt, omega));
-}
-
 // Four cells of a row as one vector access (FP32 or BF16 storage).
 __device__ __forceinline__ float4 ld4(const float* p) {
   return *reinterpret_cast<const float4*>(p);
@@ -295,6 +267,37 @@ __device__ __forceinline__ bool chunk_colour(float4& P, const float4 P0, float l
   }
   return any;
 }
+
+// One colour pass with the neighbour mask: thread (hx, y, z) updates the
+// cell x = 2 hx + ((y + z + colour) & 1) (mg.wgsl:17-36) reading its own
+// mask and b and the neighbours the mask marks.
+template <typename TS>
+__global__ void __launch_bounds__(256) k_mg_pass(L d, float h2, const TS* __restrict__ b,
+                                                 const uint8_t* __restrict__ meta,
+                                                 TS* __restrict__ p, int color, float omega,
+                                                 int bc_mode) {
+  pdl_trigger();
+  pdl_wait();
+  int y = blockIdx.y * 4 + threadIdx.y;
+  int z = blockIdx.z * 2 + threadIdx.z;
+  int x = (int)(blockIdx.x * 32 + threadIdx.x) * 2 + ((y + z + color) & 1);
+  if (x >= d.nx || y >= d.ny || z >= d.nz) return;
+  int i = d.idx(x, y, z);
+  uint32_t m = __ldg(meta + i);
+  if (m & META_SOLID) return;
+  const int sy = d.nx, sz = d.nx * d.ny;
+  float sum = 0.0f;
+  if (m & 1u) sum += ldv(p + i + 1);
+  if (m & 2u) sum += ldv(p + i - 1);
+  if (m & 4u) sum += ldv(p + i + sy);
+  if (m & 8u) sum += ldv(p + i - sy);
+  if (m & 16u) sum += ldv(p + i + sz);
+  if (m & 32u) sum += ldv(p + i - sz);
+  float cnt = (float)(__popc(m & 63u) + dirichlet_faces(d, x, y, z, bc_mode));
+  if (cnt < 0.5f) return;
+  stv(p + i, wmix(ldv(p + i), (sum - h2 * ldv(b + i)) / cnt, omega));
+}
+
 
 // One colour pass over rows of a multiple of 4 cells with warp-uniform
 // colour parity.  Block (8, 16): thread (tx, ty) takes the 4-cell chunk
@@ -402,13 +405,16 @@ __global__ void __launch_bounds__(128) k_mg_pass4z(L d, float h2, TS* __restrict
   }
 }
 
-// The same pass for rows of an even length that is not a multiple of 4
-// (a float4 row access would be misaligned there): 2-cell chunks, one cell
-// of the pass's colour in each.  Block (16, 8): thread (tx, ty) takes the
-// chunk 16 blockIdx.x + tx of row y = 8 blockIdx.y + ry, where warp
-// w = ty / 2 holds rows ry = 4 (w / 2) + 2 (ty % 2) + w % 2, two rows of one
-// parity; the ZT-plane window, the modes and the arithmetic are those of
-// k_mg_pass4z.
+// The same pass for rows whose length is not a multiple of 4 (a float4 row
+// access would be misaligned there): 2-cell chunks, one cell of the pass's
+// colour in each.  Block (16, 8): thread (tx, ty) takes the chunk
+// 16 blockIdx.x + tx of row y = 8 blockIdx.y + ry, where warp w = ty / 2
+// holds rows ry = 4 (w / 2) + 2 (ty % 2) + w % 2, two rows of one parity;
+// the ZT-plane window, the modes and the arithmetic are those of
+// k_mg_pass4z.  V2: the row length is even and a chunk is one aligned
+// vector access; odd rows take scalar accesses, and a row's last chunk
+// holds one cell (the second is treated as solid and never stored), which
+// touches the +x face.
 template <typename TS>
 __device__ __forceinline__ float2 round_to2(float2 v) {
   if constexpr (sizeof(TS) == 2) return __bfloat1622float2(__floats2bfloat162_rn(v.x, v.y));
@@ -439,7 +445,7 @@ __device__ __forceinline__ bool pair_colour(float2& P, const float2 P0, float le
   return true;
 }
 
-template <typename TS, int ZT, int MODE>
+template <typename TS, int ZT, int MODE, bool V2>
 __global__ void __launch_bounds__(128) k_mg_pass2z(L d, float h2, TS* __restrict__ b,
                                                    const uint8_t* __restrict__ meta,
                                                    TS* __restrict__ p, int color, float omega,
@@ -452,50 +458,75 @@ __global__ void __launch_bounds__(128) k_mg_pass2z(L d, float h2, TS* __restrict
   const int y = blockIdx.y * 8 + (w >> 1) * 4 + 2 * (ty & 1) + (w & 1);
   const int x0 = (blockIdx.x * 16 + tx) * 2;
   const bool act = x0 < d.nx && y < d.ny;
+  const bool two = V2 || x0 + 1 < d.nx;  // the chunk's second cell exists
   const bool rd = act && MODE != PASS_FIRST;  // phi is read (not the zero guess)
   const int sy = d.nx, sz = d.nx * d.ny;
   const int zb = blockIdx.z * ZT;
   const bool open = bc_mode == 0;
   const float2 zero = make_float2(0.f, 0.f);
   int i0 = (zb * d.ny + y) * d.nx + x0;
-  float2 Zm = (rd && zb > 0) ? ld2(p + i0 - sz) : zero;
-  float2 P0 = rd ? ld2(p + i0) : zero;
-  float2 Zp = (rd && zb + 1 < d.nz) ? ld2(p + i0 + sz) : zero;
+  float2 Zm = (rd && zb > 0) ? ldp<V2>(p + i0 - sz, two) : zero;
+  float2 P0 = rd ? ldp<V2>(p + i0, two) : zero;
+  float2 Zp = (rd && zb + 1 < d.nz) ? ldp<V2>(p + i0 + sz, two) : zero;
   const int dy = (y == d.ny - 1);
-  const int dxa = (open && x0 == 0), dxb = (open && x0 + 2 == d.nx);
+  // Dirichlet x faces of the chunk's cells (position 0 is a row's last cell
+  // only in odd rows)
+  const int dx0 = open ? (x0 == 0) + (x0 + 1 == d.nx) : 0, dx1 = (open && x0 + 2 == d.nx);
 #pragma unroll
   for (int k = 0; k < ZT; k++) {
     const int z = zb + k;
     if (z >= d.nz) break;  // the same in every thread of the block
-    float2 B = zero;
-    if (MODE == PASS_FIRST) {
-      if (act) {
-        B = round_to2<TS>(ld2(b32 + i0));
-        if constexpr (sizeof(TS) == 2) st2(b + i0, B);
+    const bool odd = ((y + z + color) & 1) != 0;  // the same in every lane of the warp
+    float2 B = zero, Yp = zero, Ym = zero;
+    uint32_t m2 = 0x4040u;
+    if constexpr (V2) {
+      if (MODE == PASS_FIRST) {
+        if (act) {
+          B = round_to2<TS>(ld2(b32 + i0));
+          if constexpr (sizeof(TS) == 2) st2(b + i0, B);
+        }
+      } else if (act) {
+        B = ld2(b + i0);
       }
+      if (act) m2 = *reinterpret_cast<const uint16_t*>(meta + i0);
+      if (rd && y + 1 < d.ny) Yp = ld2(p + i0 + sy);
+      if (rd && y > 0) Ym = ld2(p + i0 - sy);
     } else {
-      B = act ? ld2(b + i0) : zero;
+      // scalar accesses: of b, the mask and the +-y rows only the element
+      // of the pass's colour is used, so only it is loaded
+      const int c = odd ? 1 : 0;
+      const bool has = act && (c == 0 || two);  // the chunk holds that cell
+      auto put = [&](float v) { return odd ? make_float2(0.f, v) : make_float2(v, 0.f); };
+      if (MODE == PASS_FIRST) {
+        if (act) {
+          B = round_to2<TS>(ldp<false>(b32 + i0, two));
+          if constexpr (sizeof(TS) == 2) stp<false>(b + i0, B, two);
+        }
+      } else if (has) {
+        B = put(ldv(b + i0 + c));
+      }
+      if (has) {
+        const uint32_t mc = meta[i0 + c];
+        m2 = odd ? (mc << 8) | 0x40u : mc | 0x4000u;
+      }
+      if (rd && has && y + 1 < d.ny) Yp = put(ldv(p + i0 + c + sy));
+      if (rd && has && y > 0) Ym = put(ldv(p + i0 + c - sy));
     }
-    const uint32_t m2 =
-        act ? (uint32_t)*reinterpret_cast<const uint16_t*>(meta + i0) : 0x4040u;
-    const float2 Yp = (rd && y + 1 < d.ny) ? ld2(p + i0 + sy) : zero;
-    const float2 Ym = (rd && y > 0) ? ld2(p + i0 - sy) : zero;
-    const float2 Zn = (rd && k + 1 < ZT && z + 2 < d.nz) ? ld2(p + i0 + 2 * sz) : zero;
+    const float2 Zn = (rd && k + 1 < ZT && z + 2 < d.nz) ? ldp<V2>(p + i0 + 2 * sz, two) : zero;
     float left = __shfl_up_sync(0xffffffffu, P0.y, 1);
     float right = __shfl_down_sync(0xffffffffu, P0.x, 1);
     if (rd && tx == 0 && x0 > 0) left = ldv(p + i0 - 1);
     if (rd && tx == 15 && x0 + 2 < d.nx) right = ldv(p + i0 + 2);
     const int dyz = dy + (open ? (z == 0) + (z == d.nz - 1) : 0);
     float2 P = P0;
-    const bool odd = ((y + z + color) & 1) != 0;  // the same in every lane of the warp
     const bool any = odd ? pair_colour<true>(P, P0, left, right, Yp, Ym, Zp, Zm, B, m2,
-                                             dyz + dxb, h2, omega)
+                                             dyz + dx1, h2, omega)
                          : pair_colour<false>(P, P0, left, right, Yp, Ym, Zp, Zm, B, m2,
-                                              dyz + dxa, h2, omega);
+                                              dyz + dx0, h2, omega);
     if (MODE == PASS_LAST_F32) {
-      if (act) *reinterpret_cast<float2*>(out + i0) = round_to2<TS>(P);
+      if (act) stp<V2>(out + i0, round_to2<TS>(P), two);
     } else if (act && (any || MODE == PASS_FIRST)) {
-      st2(p + i0, P);
+      stp<V2>(p + i0, P, two);
     }
     Zm = P0;
     P0 = Zp;
@@ -817,8 +848,8 @@ inline dim3 pass4z_grid(Dims3 d, int zt = PASS_ZT) {
 }
 
 // The chunked pass for a level: rows of a multiple of 4 cells take 4-cell
-// chunks (k_mg_pass4z), other even rows 2-cell chunks (k_mg_pass2z); zt
-// planes per thread (1, 2 or 4).
+// chunks (k_mg_pass4z), other rows 2-cell chunks (k_mg_pass2z); zt planes
+// per thread (1, 2 or 4).
 template <typename TS, int MODE>
 cudaError_t pass_chunked(Dims3 d, float h, TS* b, const uint8_t* meta, TS* p, int color,
                          float omega, int bc_mode, const float* b32, float* out, int zt,
@@ -835,19 +866,33 @@ cudaError_t pass_chunked(Dims3 d, float h, TS* b, const uint8_t* meta, TS* p, in
     return launch_pdl(k_mg_pass4z<TS, 2, MODE>, g, blk, 0, st, l, h * h, b, meta, p, color,
                       omega, bc_mode, b32, out);
   }
-  const dim3 g((unsigned)((d.nx / 2 + 15) / 16), (unsigned)((d.ny + 7) / 8),
+  const dim3 g((unsigned)(((d.nx + 1) / 2 + 15) / 16), (unsigned)((d.ny + 7) / 8),
                (unsigned)((d.nz + zt - 1) / zt)),
       blk(16, 8);
+  if (d.nx % 2 == 0) {
+    if (zt == 4)
+      return launch_pdl(k_mg_pass2z<TS, 4, MODE, true>, g, blk, 0, st, l, h * h, b, meta, p,
+                        color, omega, bc_mode, b32, out);
+    if (zt == 1)
+      return launch_pdl(k_mg_pass2z<TS, 1, MODE, true>, g, blk, 0, st, l, h * h, b, meta, p,
+                        color, omega, bc_mode, b32, out);
+    return launch_pdl(k_mg_pass2z<TS, 2, MODE, true>, g, blk, 0, st, l, h * h, b, meta, p, color,
+                      omega, bc_mode, b32, out);
+  }
   if (zt == 4)
-    return launch_pdl(k_mg_pass2z<TS, 4, MODE>, g, blk, 0, st, l, h * h, b, meta, p, color,
-                      omega, bc_mode, b32, out);
+    return launch_pdl(k_mg_pass2z<TS, 4, MODE, false>, g, blk, 0, st, l, h * h, b, meta, p,
+                      color, omega, bc_mode, b32, out);
   if (zt == 1)
-    return launch_pdl(k_mg_pass2z<TS, 1, MODE>, g, blk, 0, st, l, h * h, b, meta, p, color,
-                      omega, bc_mode, b32, out);
-  return launch_pdl(k_mg_pass2z<TS, 2, MODE>, g, blk, 0, st, l, h * h, b, meta, p, color, omega,
-                    bc_mode, b32, out);
+    return launch_pdl(k_mg_pass2z<TS, 1, MODE, false>, g, blk, 0, st, l, h * h, b, meta, p,
+                      color, omega, bc_mode, b32, out);
+  return launch_pdl(k_mg_pass2z<TS, 2, MODE, false>, g, blk, 0, st, l, h * h, b, meta, p, color,
+                    omega, bc_mode, b32, out);
 }
 
+// Even rows take the chunked passes; odd rows one colour cell per thread
+// (k_mg_pass), which measured faster there than 2-cell chunks of scalar
+// accesses (150x365x150 with BF16 MGPCG, levels of 75 and 19 cells per
+// row: 5.82 against 6.19 ms per substep).
 template <typename TS>
 cudaError_t pass_t(Dims3 d, float h, const TS* b, const uint8_t* meta, TS* p, int color,
                    float omega, int bc_mode, cudaStream_t st) {
@@ -861,12 +906,9 @@ cudaError_t pass_t(Dims3 d, float h, const TS* b, const uint8_t* meta, TS* p, in
                     meta, p, color, omega, bc_mode);
 }
 
-bool mg_pass_fused_ok(Dims3 d) { return d.nx % 2 == 0; }
-
 cudaError_t launch_mg_pass_first(Dims3 d, float h, const float* r, void* bq,
                                  const uint8_t* meta, void* p, int color, float omega,
                                  int bc_mode, bool bf16, cudaStream_t st) {
-  if (!mg_pass_fused_ok(d)) return cudaErrorNotSupported;
   if (bf16) {
     using T = __nv_bfloat16;
     return pass_chunked<T, PASS_FIRST>(d, h, (T*)bq, meta, (T*)p, color, omega, bc_mode, r,
@@ -879,7 +921,6 @@ cudaError_t launch_mg_pass_first(Dims3 d, float h, const float* r, void* bq,
 cudaError_t launch_mg_pass_last_f32(Dims3 d, float h, const void* b, const uint8_t* meta,
                                     void* p, float* out, int color, float omega, int bc_mode,
                                     cudaStream_t st) {
-  if (!mg_pass_fused_ok(d)) return cudaErrorNotSupported;
   using T = __nv_bfloat16;
   return pass_chunked<T, PASS_LAST_F32>(d, h, (T*)const_cast<void*>(b), meta, (T*)p, color,
                                         omega, bc_mode, nullptr, out, PASS_ZT, st);

@@ -139,12 +139,10 @@ cudaError_t launch_mg_pass(Dims3 d, float h, const float* b, const uint8_t* meta
 cudaError_t launch_mg_pass_bf16(Dims3 d, float h, const void* b, const uint8_t* meta, void* p,
                                 int color, float omega, int bc_mode, cudaStream_t st);
 // The first and last colour pass on level 0 of the CG preconditioner's
-// V-cycle (k_mg_pass4z / k_mg_pass2z, rows of even length, mg_pass_fused_ok):
-// the first from the zero initial guess with the FP32 right-hand side r
-// (with BF16 storage also written rounded into bq), writing every cell of
-// p; the last on BF16 storage writing every cell widened to FP32 into out.
-// Both return cudaErrorNotSupported on other row lengths.
-bool mg_pass_fused_ok(Dims3 d);
+// V-cycle (k_mg_pass4z / k_mg_pass2z): the first from the zero initial
+// guess with the FP32 right-hand side r (with BF16 storage also written
+// rounded into bq), writing every cell of p; the last on BF16 storage
+// writing every cell widened to FP32 into out.
 cudaError_t launch_mg_pass_first(Dims3 d, float h, const float* r, void* bq,
                                  const uint8_t* meta, void* p, int color, float omega,
                                  int bc_mode, bool bf16, cudaStream_t st);

@@ -241,10 +241,10 @@ cudaError_t Multigrid::vcycle_sym(cudaStream_t st, DevBuf* bphi, DevBuf* bphi2, 
   auto T = [&](int l) -> void* { return lo ? bphi2[l].p : phi2[l].p; };
   size_t n0 = dims[0].cells();
   // The first and last level-0 passes take the zero guess, the FP32
-  // right-hand side and (BF16) the FP32 result directly when the row length
-  // allows (mg_pass_fused_ok); otherwise level 0 is cleared and converted
-  // here and converted back at the end.
-  const bool fuse = nl > 1 && mg_pass_fused_ok(dims[0]);
+  // right-hand side and (BF16) the FP32 result directly; a hierarchy of one
+  // level (solved directly) clears and converts level 0 here and converts
+  // back at the end.
+  const bool fuse = nl > 1;
   if (!fuse) {
     if (lo) {
       if ((e = launch_f32_to_bf16(b[0], bb[0].p, n0, st)) != cudaSuccess) return e;

@@ -37,6 +37,12 @@ inline dim3 grid_for(Dims3 d) {
 }
 
 enum { SC_RZ = 0, SC_PQ, SC_RR, SC_BB, SC_ZQ, SC_RZN, SC_N = 8 };
+constexpr int VT = 256;  // threads per block of the CG vector kernels
+
+// The FP64 scalars are followed in the same allocation by one row of block
+// partial sums per scalar and one arrival counter per scalar (block_add_d).
+constexpr int RED_MAXB = 4096;  // blocks of a reduction kernel at most
+constexpr size_t SC_BYTES = SC_N * 8 + (size_t)SC_N * RED_MAXB * 8 + SC_N * 4;
 
 unsigned vec_blocks(size_t n) {
   static int nsm = 0;
@@ -47,7 +53,8 @@ unsigned vec_blocks(size_t n) {
         nsm <= 0)
       nsm = 148;
   }
-  return (unsigned)std::min<size_t>((n + 255) / 256, (size_t)nsm * 8);
+  return (unsigned)std::min<size_t>(std::min<size_t>((n + 255) / 256, (size_t)nsm * 8),
+                                    (size_t)RED_MAXB);
 }
 
 __device__ __forceinline__ double warp_sum_d(double v) {
@@ -55,17 +62,43 @@ __device__ __forceinline__ double warp_sum_d(double v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
-// Block sum in FP64, one atomic per block.  Every thread must call.
-__device__ __forceinline__ void block_add_d(double* sh, double v, double* dst) {
-  int t = threadIdx.x + BX * (threadIdx.y + BY * threadIdx.z);
+// sc[slot] += the sum of v over every thread of the grid, in an order that
+// does not depend on scheduling: each block writes its sum (a fixed tree
+// over its threads) to the slot's row of partials; the block that arrives
+// last adds the row in index order and resets the counter.  So a solve
+// repeats bit for bit.  Every thread of every block must call; blocks of
+// VT threads.
+__device__ __forceinline__ void block_add_d(double* sh, double v, double* sc, int slot) {
+  __shared__ bool s_last;
+  const int t = threadIdx.x;
+  double* part = sc + SC_N + (size_t)slot * RED_MAXB;
+  unsigned* cnt = reinterpret_cast<unsigned*>(sc + SC_N + (size_t)SC_N * RED_MAXB) + slot;
   v = warp_sum_d(v);
   __syncthreads();
   if ((t & 31) == 0) sh[t >> 5] = v;
   __syncthreads();
   if (t < 32) {
-    double s = t < (BX * BY * BZ) / 32 ? sh[t] : 0.0;
+    double s = t < VT / 32 ? sh[t] : 0.0;
     s = warp_sum_d(s);
-    if (t == 0 && s != 0.0) atomicAdd(dst, s);
+    if (t == 0) {
+      part[blockIdx.x] = s;
+      __threadfence();
+      s_last = atomicAdd(cnt, 1u) == gridDim.x - 1;
+    }
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  double a = 0.0;
+  for (unsigned k = t; k < gridDim.x; k += VT) a += __ldcg(part + k);
+  a = warp_sum_d(a);
+  if ((t & 31) == 0) sh[t >> 5] = a;
+  __syncthreads();
+  if (t == 0) {
+    double s = 0.0;
+    for (int w = 0; w < VT / 32; w++) s += sh[w];
+    sc[slot] += s;
+    *cnt = 0u;
   }
 }
 
@@ -86,10 +119,8 @@ struct L3 {
   bool fluid = in && __ldg(f + i) != 1u;
 
 // The CG vector kernels run on a 1-D grid capped at 8 blocks per SM; each
-// thread strides over the cells, so a kernel's block sums meet in ~1,200
-// FP64 atomics instead of one per 256 cells (32,000 at 8.2 M cells, which
-// serialised on one address).
-constexpr int VT = 256;
+// thread strides over the cells, so a reduction adds ~1,200 block sums
+// (one per 256 cells would be 32,000 at 8.2 M cells).
 struct Cells {
   L3 d;
   FastDiv by_nx, by_plane;
@@ -185,8 +216,8 @@ __global__ void __launch_bounds__(VT) k_resid(Cells c, double ih2, const float* 
     }
     if (r) r[i] = ri;
   }
-  block_add_d(sh, r2, sc + SC_RR);
-  block_add_d(sh, b2, sc + SC_BB);
+  block_add_d(sh, r2, sc, SC_RR);
+  block_add_d(sh, b2, sc, SC_BB);
 }
 
 template <typename M>
@@ -207,7 +238,7 @@ __global__ void __launch_bounds__(VT) k_apply_dot(Cells c, double ih2, const flo
     }
     q[i] = qi;
   }
-  block_add_d(sh, pq, sc + SC_PQ);
+  block_add_d(sh, pq, sc, SC_PQ);
 }
 
 // q = A p (FP64 evaluation, rounded), 0 in solids.
@@ -248,7 +279,7 @@ __global__ void __launch_bounds__(VT) k_update_xr(Cells c, M mk, float* phi_arg,
     r[i] = ri;
     rr += (double)ri * (double)ri;
   }
-  block_add_d(sh, rr, sc + SC_RR);
+  block_add_d(sh, rr, sc, SC_RR);
 }
 
 // <z,r> -> SC_RZN and, when q is given, <z,q> -> SC_ZQ
@@ -267,8 +298,8 @@ __global__ void __launch_bounds__(VT) k_dots(Cells c, M mk, const float* __restr
     zr += (double)zi * (double)r[i];
     if (q) zq += (double)zi * (double)q[i];
   }
-  block_add_d(sh, zr, sc + SC_RZN);
-  if (q) block_add_d(sh, zq, sc + SC_ZQ);
+  block_add_d(sh, zr, sc, SC_RZN);
+  if (q) block_add_d(sh, zq, sc, SC_ZQ);
 }
 
 // p = z + beta p with beta = -<z,q>/<p,q>; p = z when ctl->first is set
@@ -733,7 +764,8 @@ int Solver::init(Multigrid* m) {
   if ((rc = z.alloc(n * 4)) != PYRO_OK) return rc;
   if ((rc = p.alloc(n * 4)) != PYRO_OK) return rc;
   if ((rc = q.alloc(n * 4)) != PYRO_OK) return rc;
-  if ((rc = sc.alloc(SC_N * 8)) != PYRO_OK) return rc;
+  if ((rc = sc.alloc(SC_BYTES)) != PYRO_OK) return rc;
+  PYRO_CU(cudaMemset(sc.p, 0, SC_BYTES));  // the reductions' counters start at 0
   if ((rc = ctl.alloc(sizeof(CgCtl))) != PYRO_OK) return rc;
   // the scalars and one 8-byte word (the flag hash)
   if (cudaMallocHost(&host_sc, (SC_N + 1) * 8) != cudaSuccess ||

@@ -217,13 +217,15 @@ def _bf16_val(bits):
 
 # the shapes the V-cycle meets: rows of a multiple of 4 cells (4-cell
 # chunks in the pass, even row pairs in the transfers), of another even
-# length (2-cell chunks: 10, 38, 150, 130) and odd rows (one cell per
-# thread); the chunked passes take one plane per thread below 256 Ki cells,
-# two up to 4 Mi, four from there
+# length (2-cell aligned chunks: 10, 38, 150, 130) and odd (2-cell scalar
+# chunks, the last of a row with one cell: 19, 17, 75, 33, 129); the
+# chunked passes take one plane per thread below 256 Ki cells, two up to
+# 4 Mi, four from there
 MASK_CASES = MG_CASES + [(64, 40, 24, 3, 0.04), (20, 40, 20, 4, 0.16), (10, 20, 10, 5, 0.32),
                          (80, 64, 64, 7, 0.04), (256, 128, 128, 6, 0.02),
                          (38, 40, 20, 8, 0.16), (150, 96, 24, 9, 0.02),
-                         (130, 256, 128, 10, 0.02)]
+                         (130, 256, 128, 10, 0.02), (75, 64, 64, 11, 0.04),
+                         (33, 8, 6, 12, 0.2), (129, 256, 128, 13, 0.02)]
 
 
 @pytest.mark.parametrize("nx,ny,nz,seed,h", MASK_CASES)
@@ -276,7 +278,8 @@ def test_mg_mask_kernels_as_the_vcycle_runs_them(lib, nx, ny, nz, seed, h, bc_mo
 
 
 @pytest.mark.parametrize("nx,ny,nz,seed,h", [(32, 48, 32, 0, 0.05), (38, 40, 20, 8, 0.16),
-                                             (150, 96, 24, 9, 0.02), (64, 40, 24, 3, 0.04)])
+                                             (150, 96, 24, 9, 0.02), (64, 40, 24, 3, 0.04),
+                                             (19, 46, 19, 1, 0.16), (75, 64, 40, 11, 0.04)])
 @pytest.mark.parametrize("bc_mode", [0, 1])
 @pytest.mark.parametrize("storage", [_abi.MG_F32, _abi.MG_BF16])
 def test_mg_fused_first_and_last_passes_equal_the_plain_pass(lib, nx, ny, nz, seed, h, bc_mode,
@@ -372,15 +375,6 @@ def test_mg_symmetric_restriction_is_the_adjoint_of_the_prolongation(lib, nx, ny
                                               bc_mode, _abi.MG_F32, None) == 0
             lo, hi = _bf16_val(host(bb)), host(bf)
             assert np.abs(lo - hi).max() <= 2e-2 * np.abs(hi).max()
-
-
-def test_mg_fused_passes_refuse_odd_rows(lib):
-    z = dev(np.zeros(9 * 8 * 4, np.float32))
-    m = dev(np.zeros(9 * 8 * 4, np.uint8))
-    assert lib.pyro_k_mg_pass_first(9, 8, 4, 0.1, ptr(z), None, ptr(m), ptr(z), 0, 1.0, 0,
-                                    _abi.MG_F32, None) == _abi.PYRO_E_INVALID
-    assert lib.pyro_k_mg_pass_last(9, 8, 4, 0.1, ptr(z), ptr(m), ptr(z), ptr(z), 0, 1.0, 0,
-                                   None) == _abi.PYRO_E_INVALID
 
 
 # slabs of one to three planes per CTA of the cluster (nz = 3: three CTAs)
