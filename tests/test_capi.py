@@ -72,6 +72,19 @@ def test_invalid_arguments_fail_before_the_device(lib):
         _abi.PYRO_E_INVALID
     assert lib.pyro_k_mg_prolong_m(16, 16, 16, buf, buf, buf, 8, 9, 8, buf, 0, None) == \
         _abi.PYRO_E_INVALID
+    # the CG preconditioner's pieces: coarse dims, null buffers, modes
+    assert lib.pyro_k_mg_restrict_sym(16, 16, 16, 0.1, buf, buf, buf, 8, 8, 9, buf, buf, buf, 0,
+                                      0, None) == _abi.PYRO_E_INVALID
+    assert b"ceil" in lib.pyro_last_error()
+    assert lib.pyro_k_mg_restrict_sym(16, 16, 16, 0.1, buf, buf, buf, 8, 8, 8, buf, buf, buf, 2,
+                                      0, None) == _abi.PYRO_E_INVALID
+    assert lib.pyro_k_mg_pass_first(16, 16, 16, 0.1, buf, None, buf, buf, 0, 1.0, 0,
+                                    _abi.MG_BF16, None) == _abi.PYRO_E_INVALID
+    assert b"null" in lib.pyro_last_error()
+    assert lib.pyro_k_mg_pass_first(16, 16, 16, 0.1, buf, None, buf, buf, 2, 1.0, 0,
+                                    _abi.MG_F32, None) == _abi.PYRO_E_INVALID
+    assert lib.pyro_k_mg_pass_last(16, 16, 1, 0.1, buf, buf, buf, buf, 0, 1.0, 0,
+                                   None) == _abi.PYRO_E_INVALID
     assert lib.pyro_poisson_create(4, 4, 4, 0.1, 7, ctypes.byref(h)) == _abi.PYRO_E_INVALID
     assert lib.pyro_sim_destroy(None) == _abi.PYRO_OK
 
