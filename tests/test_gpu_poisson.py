@@ -135,6 +135,36 @@ def test_coarsest_direct_solve_is_exact(lib, bc_mode):
     lib.pyro_poisson_destroy(ps)
 
 
+@pytest.mark.parametrize("bc_mode", [0, 1])
+def test_bf16_single_level_preconditioner_converges(lib, bc_mode):
+    """A grid that is its own coarsest level: the BF16 preconditioner is the
+    FP64 direct solve alone, with level 0 converted to BF16 on entry and
+    back on exit (no smoothing passes), so CG converges in a few
+    iterations to its tolerance, within 2e-3 of the FP64 solution."""
+    dims = (12, 16, 12)
+    f, b = _case(*dims, 6, solid=0.0)
+    f[2:5, 0:4, 3:7] = 1
+    b[f == 1] = 0.0
+    h = 0.1
+    x64, it, rel64 = oracle.poisson_f64(dims, h, b, f, tol=1e-13, bc_mode=bc_mode)
+    ps = _solver(lib, dims, h, f, bc_mode)
+    bd, pd = dev(b), dev(np.zeros_like(b))
+    info = _abi.PyroSolveInfo()
+    rc = lib.pyro_poisson_solve(ps, ptr(bd), ptr(pd), _abi.SOLVER_MGPCG_BF16, 1e-6, 30,
+                                ctypes.byref(info))
+    assert rc == 0, lib.pyro_last_error()
+    assert info.converged == 1 and info.iterations <= 10, (info.iterations, info.rel_resid)
+    phi = host(pd)
+    rel = oracle.poisson_relres(dims, h, phi, b, f, bc_mode)
+    # near 1e-7 the residual of an FP32 field is cancellation: the two FP64
+    # evaluations agree to a few per cent
+    assert rel <= 1.05e-6 and abs(rel - info.rel_resid) <= 0.05 * rel
+    fl = f == 0
+    err = np.abs(phi[fl] - x64[fl]).max() / np.abs(x64[fl]).max()
+    assert err <= 2e-3, err
+    lib.pyro_poisson_destroy(ps)
+
+
 @pytest.mark.parametrize("dims", [(160, 320, 160), (150, 365, 150)])
 @pytest.mark.parametrize("mode", [_abi.SOLVER_MGPCG, _abi.SOLVER_MGPCG_BF16])
 def test_mgpcg_at_the_2cm_pool_shapes(lib, dims, mode):
