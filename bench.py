@@ -457,11 +457,24 @@ def sim_solver_bench(sim):
     if net is not None:
         ps.set_net(net)
     res = solve_runs(ps, bd, metric_runs(), net)
+    # where a BF16 CG iteration's time goes: the same iterations one launch
+    # at a time, an event after each step (per iteration, event overhead
+    # included)
+    cg_classes = None
+    b16 = res.get("mgpcg_bf16_to_1e-4")
+    if b16:
+        phi = torch.zeros_like(bd)
+        k = max(int(b16["iterations"]), 1)
+        prof = ps.profile_cg(bd.data_ptr(), phi.data_ptr(), _abi.SOLVER_MGPCG_BF16, k)
+        cg_classes = {c: {"ms_per_iteration": round(v["ms"] / k, 4),
+                          "steps_per_iteration": v["steps"] / k} for c, v in prof.items()}
+        log("cg classes per iteration " + " ".join(
+            f"{c}={v['ms_per_iteration']:.3f}" for c, v in cg_classes.items()))
     ps.set_net(None)
     ps.close()
     v, l = res.get("vcycle_fp32_to_1e-3"), res.get("mgpcg_bf16_learned_to_1e-4")
     out = {"config": f"the bench's last substep, {sim.dims[0]}x{sim.dims[1]}x{sim.dims[2]}, "
-                     "phi0 = 0", "runs": res}
+                     "phi0 = 0", "runs": res, "cg_classes_bf16": cg_classes}
     if net is not None:
         out["net_roofline"] = net_roofline(net, bd, fd, tuple(sim.dims), sim.dx)
     if v and l:

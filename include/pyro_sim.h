@@ -283,6 +283,21 @@ int pyro_poisson_set_flags(PyroPoisson* ps, const uint32_t* flags);
 int pyro_poisson_solve(PyroPoisson* ps, const float* b, float* phi, int mode,
                        float tol, int max_iters, PyroSolveInfo* info);
 int pyro_poisson_stream(PyroPoisson* ps, void** stream);
+/* Where a CG iteration's time goes: `iters` iterations of mode
+ * PYRO_SOLVER_MGPCG or PYRO_SOLVER_MGPCG_BF16 from phi (updated in place as
+ * by a solve's iterations; no convergence test, no restart), one launch at
+ * a time with a CUDA event after each step instead of the solve's graph.
+ * Blocks.  Per class, ms_out / launches_out[0..min(n, 9)) get the summed
+ * device time and the number of steps: 0 level masks and weights (only
+ * when the flag field changed), 1 level-0 colour pass, 2 restriction from
+ * level 0 (residual and gather: two kernels per step), 3 prolongation onto
+ * level 0, 4 colour pass on a coarser level, 5 restriction from one, 6
+ * prolongation onto one, 7 the coarsest level's direct solve, 8 a CG
+ * vector kernel.  Each step carries its event's overhead (a few
+ * microseconds).  No counterpart in the reference. */
+#define PYRO_PROFILE_CG_CLASSES 9
+int pyro_poisson_profile_cg(PyroPoisson* ps, const float* b, float* phi, int mode,
+                            int iters, float* ms_out, int* launches_out, int n);
 /* Network used by PYRO_SOLVER_MGPCG_LEARNED (NULL detaches). */
 int pyro_poisson_set_net(PyroPoisson* ps, PyroNet* net);
 /* The learned stage's keep-or-discard rule, on host scalars: given

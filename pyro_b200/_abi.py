@@ -32,6 +32,10 @@ PROFILE_PHASES = ["solid", "curl", "adv_vel1", "adv_vel2", "adv_s1", "adv_s2", "
                   "forces", "divergence", "pressure", "project", "total"]
 
 MG_F32, MG_BF16 = 0, 1  # storage of phi and b in the pyro_k_mg_* mask entries
+# launch classes of pyro_poisson_profile_cg: those of
+# pyro_sim_profile_pressure, then the CG vector kernels
+CG_CLASSES = ["mg_prepare", "mg_pass_l0", "mg_restrict_l0", "mg_prolong_l0", "mg_pass_mid",
+              "mg_restrict_mid", "mg_prolong_mid", "mg_coarse", "cg_vector"]
 # launch classes of pyro_sim_profile_pressure
 MG_CLASSES = ["mg_prepare", "mg_pass_l0", "mg_restrict_l0", "mg_prolong_l0", "mg_pass_mid",
               "mg_restrict_mid", "mg_prolong_mid", "mg_coarse"]
@@ -180,6 +184,7 @@ SIGNATURES = {
     "pyro_sim_sync": [_P],
     "pyro_sim_profile_step": [_P, _F, _F, _F, _I, _P, _I],
     "pyro_sim_profile_pressure": [_P, _P, _P, _I],
+    "pyro_poisson_profile_cg": [_P, _P, _P, _I, _I, _P, _P, _I],
     "pyro_post_select": [_P, _U32, _U32, _U32, _P, _P, _P, ctypes.POINTER(_F), _P],
     "pyro_post_develop": [_P, _U32, _U32, _F, _F, _P, _P, _P, _P],
     "pyro_sim_info": [_P, ctypes.POINTER(PyroSimInfo)],

@@ -241,7 +241,10 @@ cudaError_t Multigrid::vcycle_sym(cudaStream_t st, DevBuf* bphi, DevBuf* bphi2, 
       }
     }
   }
+  // with a timer, an event after every step credits it to its class
+  auto tick = [&](int cls) -> cudaError_t { return timer ? timer->mark(cls, st) : cudaSuccess; };
   if (prep && (e = prepare_sym(st)) != cudaSuccess) return e;
+  if (prep && (e = tick(MG_PREPARE)) != cudaSuccess) return e;
   auto M = [&](int l) { return meta[l].as<uint8_t>(); };
   // storage of level l: phi, b, scratch
   auto P = [&](int l) -> void* { return lo ? bphi[l].p : (void*)phi[l]; };
@@ -273,6 +276,7 @@ cudaError_t Multigrid::vcycle_sym(cudaStream_t st, DevBuf* bphi, DevBuf* bphi2, 
                 ? launch_mg_pass_first(dims[0], h[0], b[0], lo ? bb[0].p : nullptr, M(0), P(0), 0,
                                        kSymOmega, bc_mode, lo, st)
                 : pass(l, c, kSymOmega);
+        if (e == cudaSuccess) e = tick(l == 0 ? MG_PASS_L0 : MG_PASS_MID);
         if (e != cudaSuccess) return e;
       }
     const uint8_t* W = wq[l].as<uint8_t>();
@@ -281,6 +285,7 @@ cudaError_t Multigrid::vcycle_sym(cudaStream_t st, DevBuf* bphi, DevBuf* bphi2, 
            : launch_mg_restrict_sym(dims[l], h[l], (const float*)P(l), (const float*)B(l), M(l),
                                     W, (float*)T(l), dims[l + 1], M(l + 1), (float*)B(l + 1),
                                     (float*)P(l + 1), bc_mode, st);
+    if (e == cudaSuccess) e = tick(l == 0 ? MG_RESTRICT_L0 : MG_RESTRICT_MID);
     if (e != cudaSuccess) return e;
   }
   int lc = nl - 1;
@@ -296,10 +301,12 @@ cudaError_t Multigrid::vcycle_sym(cudaStream_t st, DevBuf* bphi, DevBuf* bphi2, 
       for (int cc = 0; cc < 2; cc++)
         if ((e = pass(lc, cc ^ (it & 1), 1.6f)) != cudaSuccess) return e;
   }
+  if ((e = tick(MG_COARSE)) != cudaSuccess) return e;
   for (int l = nl - 2; l >= 0; l--) {
     e = lo ? launch_mg_prolong_m_bf16(dims[l], P(l + 1), M(l), P(l), dims[l + 1], M(l + 1), st)
            : launch_mg_prolong_m(dims[l], (const float*)P(l + 1), M(l), (float*)P(l),
                                  dims[l + 1], M(l + 1), st);
+    if (e == cudaSuccess) e = tick(l == 0 ? MG_PROLONG_L0 : MG_PROLONG_MID);
     if (e != cudaSuccess) return e;
     for (int it = 0; it < sym_sweeps(l); it++)
       for (int c = 1; c >= 0; c--) {
@@ -307,6 +314,7 @@ cudaError_t Multigrid::vcycle_sym(cudaStream_t st, DevBuf* bphi, DevBuf* bphi2, 
                 ? launch_mg_pass_last_f32(dims[0], h[0], B(0), M(0), P(0), phi[0], 0, kSymOmega,
                                           bc_mode, st)
                 : pass(l, c, kSymOmega);
+        if (e == cudaSuccess) e = tick(l == 0 ? MG_PASS_L0 : MG_PASS_MID);
         if (e != cudaSuccess) return e;
       }
   }

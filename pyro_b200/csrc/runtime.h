@@ -58,6 +58,7 @@ enum MgClass {
   MG_RESTRICT_MID,
   MG_PROLONG_MID,
   MG_COARSE,       // the coarsest-level solve
+  MG_CG_VECTOR,    // a CG vector kernel (dot products, updates, q = A p)
   MG_CLASSES
 };
 

@@ -151,9 +151,10 @@ inline Cells cells_of(Dims3 d) {
 //    inside the grid and fluid, bit 6 = solid), one byte per cell.
 struct FlagMask {
   const uint32_t* f;
-  __device__ __forceinline__ bool solid(int i) const { return __ldg(f + i) == 1u; }
+  __device__ __forceinline__ uint32_t load(int i) const { return __ldg(f + i); }
+  __device__ __forceinline__ bool solid(uint32_t raw) const { return raw == 1u; }
   __device__ __forceinline__ double apply(const Cells& c, double ih2, const float* __restrict__ v,
-                                         int i, int bc_mode, float vi) const {
+                                         int i, int bc_mode, float vi, uint32_t) const {
     int x, y, z;
     c.coords(i, x, y, z);
     const L3& d = c.d;
@@ -176,27 +177,35 @@ struct FlagMask {
 };
 struct MetaMask {
   const uint8_t* m;
-  __device__ __forceinline__ bool solid(int i) const { return (__ldg(m + i) & 0x40u) != 0; }
+  __device__ __forceinline__ uint32_t load(int i) const { return __ldg(m + i); }
+  __device__ __forceinline__ bool solid(uint32_t raw) const { return (raw & 0x40u) != 0; }
+  // The six neighbour values are loaded from the cell's coordinates (an
+  // in-grid index, the cell itself at the grid's edge) without waiting for
+  // the mask, which then selects the ones that are added.
   __device__ __forceinline__ double apply(const Cells& c, double ih2, const float* __restrict__ v,
-                                         int i, int bc_mode, float vi) const {
+                                         int i, int bc_mode, float vi, uint32_t mi) const {
     int x, y, z;
     c.coords(i, x, y, z);
-    const uint32_t mi = __ldg(m + i);
-    const int sy = c.d.nx, sz = c.d.nx * c.d.ny;
+    const int nx = c.d.nx, ny = c.d.ny, nz = c.d.nz, sy = nx, sz = nx * ny;
+    const float xp = __ldg(v + (x + 1 < nx ? i + 1 : i)), xm = __ldg(v + (x > 0 ? i - 1 : i));
+    const float yp = __ldg(v + (y + 1 < ny ? i + sy : i)), ym = __ldg(v + (y > 0 ? i - sy : i));
+    const float zp = __ldg(v + (z + 1 < nz ? i + sz : i)), zm = __ldg(v + (z > 0 ? i - sz : i));
     double sum = 0.0;
-    if (mi & 1u) sum += (double)__ldg(v + i + 1);
-    if (mi & 2u) sum += (double)__ldg(v + i - 1);
-    if (mi & 4u) sum += (double)__ldg(v + i + sy);
-    if (mi & 8u) sum += (double)__ldg(v + i - sy);
-    if (mi & 16u) sum += (double)__ldg(v + i + sz);
-    if (mi & 32u) sum += (double)__ldg(v + i - sz);
-    int faces = (y == c.d.ny - 1);
-    if (bc_mode == 0) faces += (x == 0) + (x == c.d.nx - 1) + (z == 0) + (z == c.d.nz - 1);
+    if (mi & 1u) sum += (double)xp;
+    if (mi & 2u) sum += (double)xm;
+    if (mi & 4u) sum += (double)yp;
+    if (mi & 8u) sum += (double)ym;
+    if (mi & 16u) sum += (double)zp;
+    if (mi & 32u) sum += (double)zm;
+    int faces = (y == ny - 1);
+    if (bc_mode == 0) faces += (x == 0) + (x == nx - 1) + (z == 0) + (z == nz - 1);
     const double cnt = (double)(__popc(mi & 63u) + faces);
     return (sum - cnt * (double)vi) * ih2;
   }
 };
 
+// In the kernels below every load of a cell is issued before its mask
+// decides what is used (one memory round trip per cell, not two).
 template <typename M>
 __global__ void __launch_bounds__(VT) k_resid(Cells c, double ih2, const float* __restrict__ phi,
                                               const float* __restrict__ b, M mk, int bc_mode,
@@ -206,10 +215,11 @@ __global__ void __launch_bounds__(VT) k_resid(Cells c, double ih2, const float* 
   __shared__ double sh[32];
   double r2 = 0.0, b2 = 0.0;
   CELL_LOOP(i) {
+    const uint32_t raw = mk.load(i);
+    const float bi = __ldg(b + i), pi = __ldg(phi + i);
     float ri = 0.0f;
-    if (!mk.solid(i)) {
-      float bi = __ldg(b + i);
-      double rd = (double)bi - mk.apply(c, ih2, phi, i, bc_mode, __ldg(phi + i));
+    if (!mk.solid(raw)) {
+      double rd = (double)bi - mk.apply(c, ih2, phi, i, bc_mode, pi, raw);
       ri = (float)rd;
       r2 += rd * rd;
       b2 += (double)bi * (double)bi;
@@ -229,10 +239,11 @@ __global__ void __launch_bounds__(VT) k_apply_dot(Cells c, double ih2, const flo
   __shared__ double sh[32];
   double pq = 0.0;
   CELL_LOOP(i) {
+    const uint32_t raw = mk.load(i);
+    const float pi = __ldg(p + i);
     float qi = 0.0f;
-    if (!mk.solid(i)) {
-      float pi = __ldg(p + i);
-      double qd = mk.apply(c, ih2, p, i, bc_mode, pi);
+    if (!mk.solid(raw)) {
+      double qd = mk.apply(c, ih2, p, i, bc_mode, pi, raw);
       qi = (float)qd;
       pq += (double)pi * qd;
     }
@@ -247,8 +258,10 @@ __global__ void __launch_bounds__(VT) k_apply(Cells c, double ih2, const float* 
   pdl_trigger();
   pdl_wait();
   CELL_LOOP(i) {
+    const uint32_t raw = mk.load(i);
+    const float pi = __ldg(p + i);
     float qi = 0.0f;
-    if (!mk.solid(i)) qi = (float)mk.apply(c, ih2, p, i, bc_mode, __ldg(p + i));
+    if (!mk.solid(raw)) qi = (float)mk.apply(c, ih2, p, i, bc_mode, pi, raw);
     q[i] = qi;
   }
 }
@@ -273,9 +286,11 @@ __global__ void __launch_bounds__(VT) k_update_xr(Cells c, M mk, float* phi_arg,
   float* __restrict__ phi = phi_arg ? phi_arg : ctl->x;
   double rr = 0.0;
   CELL_LOOP(i) {
-    if (mk.solid(i)) continue;
-    phi[i] += alpha * p[i];
-    float ri = r[i] - alpha * q[i];
+    const uint32_t raw = mk.load(i);
+    const float pi = p[i], qi = q[i], r0 = r[i], xi = phi[i];
+    if (mk.solid(raw)) continue;
+    phi[i] = xi + alpha * pi;
+    float ri = r0 - alpha * qi;
     r[i] = ri;
     rr += (double)ri * (double)ri;
   }
@@ -293,10 +308,11 @@ __global__ void __launch_bounds__(VT) k_dots(Cells c, M mk, const float* __restr
   __shared__ double sh[32];
   double zr = 0.0, zq = 0.0;
   CELL_LOOP(i) {
-    if (mk.solid(i)) continue;
-    float zi = zv[i];
-    zr += (double)zi * (double)r[i];
-    if (q) zq += (double)zi * (double)q[i];
+    const uint32_t raw = mk.load(i);
+    const float zi = zv[i], ri = r[i], qi = q ? q[i] : 0.0f;
+    if (mk.solid(raw)) continue;
+    zr += (double)zi * (double)ri;
+    if (q) zq += (double)zi * (double)qi;
   }
   block_add_d(sh, zr, sc, SC_RZN);
   if (q) block_add_d(sh, zq, sc, SC_ZQ);
@@ -321,11 +337,13 @@ __global__ void __launch_bounds__(VT) k_update_p(Cells c, M mk, float* __restric
   const float beta = s_beta;
   const bool first = s_first != 0;
   CELL_LOOP(i) {
-    if (mk.solid(i)) {
+    const uint32_t raw = mk.load(i);
+    const float zi = zv[i], pi = first ? 0.0f : p[i];
+    if (mk.solid(raw)) {
       p[i] = 0.0f;
       continue;
     }
-    p[i] = first ? zv[i] : zv[i] + beta * p[i];
+    p[i] = first ? zi : zi + beta * pi;
   }
 }
 
@@ -680,6 +698,18 @@ int Solver::begin_cg(cudaStream_t st, float* phi, const float* b) {
   return PYRO_OK;
 }
 
+int Solver::alloc_bf16_levels() {
+  for (size_t l = 0; l < bphi.size(); l++) {
+    const size_t need = pc.dims[l].cells() * 2;
+    int rc;
+    if (bphi[l].bytes != need &&
+        ((rc = bphi[l].alloc(need)) != PYRO_OK || (rc = bphi2[l].alloc(need)) != PYRO_OK ||
+         (rc = bb[l].alloc(need)) != PYRO_OK))
+      return rc;
+  }
+  return PYRO_OK;
+}
+
 int Solver::cg_loop(cudaStream_t st, float* phi, bool bf16, double bb2, float tol, int it0,
                     int max_it) {
   cudaGraphExec_t& exec = cg_exec[bf16 ? 1 : 0];
@@ -689,14 +719,8 @@ int Solver::cg_loop(cudaStream_t st, float* phi, bool bf16, double bb2, float to
     double* S = sc.as<double>();
     CgCtl* C = ctl.as<CgCtl>();
     // the BF16 levels exist before their addresses are captured
-    for (size_t l = 0; bf16 && l < bphi.size(); l++) {
-      const size_t need = pc.dims[l].cells() * 2;
-      int rc;
-      if (bphi[l].bytes != need &&
-          ((rc = bphi[l].alloc(need)) != PYRO_OK || (rc = bphi2[l].alloc(need)) != PYRO_OK ||
-           (rc = bb[l].alloc(need)) != PYRO_OK))
-        return rc;
-    }
+    int rc;
+    if (bf16 && (rc = alloc_bf16_levels()) != PYRO_OK) return rc;
     cudaGraph_t g = nullptr;
     PYRO_CU(cudaGraphCreate(&g, 0));
     struct Own {
@@ -911,6 +935,65 @@ int Solver::learned_stage(cudaStream_t st, float* phi, double* rr, PyroSolveInfo
   return PYRO_OK;
 }
 
+int Solver::profile_cg(cudaStream_t st, float* phi, const float* b, bool bf16, int iters,
+                       float* ms, int* launches) {
+  int rc;
+  if ((rc = begin_cg(st, phi, b)) != PYRO_OK) return rc;
+  float* save_phi = mg->phi[0];
+  float* save_b = mg->b[0];
+  const uint32_t* save_f0 = mg->f[0];
+  mg->bind_level0(save_phi, save_b, fa.as<uint32_t>());
+  struct Rebind {
+    Multigrid* m;
+    float* p;
+    float* b;
+    const uint32_t* f;
+    ~Rebind() { m->bind_level0(p, b, f); }
+  } rebind{mg, save_phi, save_b, save_f0};
+  // the BF16 levels exist before the first event
+  if (bf16 && (rc = alloc_bf16_levels()) != PYRO_OK) return rc;
+  const MetaMask mk{pc.meta[0].as<uint8_t>()};
+  const double ih2 = 1.0 / ((double)mg->h[0] * mg->h[0]);
+  double* S = sc.as<double>();
+  CgCtl* C = ctl.as<CgCtl>();
+  const dim3 vb(vec_blocks(d.cells())), vt(VT);
+  std::memset(host_ctl, 0, sizeof(CgCtl));
+  host_ctl->x = phi;
+  host_ctl->first = 1;
+  PYRO_CU(cudaMemcpyAsync(ctl.p, host_ctl, sizeof(CgCtl), cudaMemcpyHostToDevice, st));
+  MgTimer timer;
+  PYRO_CU(timer.start(st));
+  pc.timer = &timer;
+  struct Untime {
+    Multigrid* m;
+    ~Untime() { m->timer = nullptr; }
+  } untime{&pc};
+  auto tick = [&]() { return timer.mark(MG_CG_VECTOR, st); };
+  for (int it = 0; it < iters; it++) {
+    PYRO_CU(precond(st, bf16, false));
+    PYRO_CU(launch_pdl(k_dots<MetaMask>, vb, vt, 0, st, cells_of(d), mk,
+                       (const float*)z.as<float>(), (const float*)r.as<float>(),
+                       (const float*)q.as<float>(), S));
+    PYRO_CU(tick());
+    PYRO_CU(launch_pdl(k_update_p<MetaMask>, vb, vt, 0, st, cells_of(d), mk, p.as<float>(),
+                       (const float*)z.as<float>(), (const double*)S, (const CgCtl*)C));
+    if (it == 0) PYRO_CU(cudaMemsetAsync(&C->first, 0, sizeof(int), st));
+    PYRO_CU(tick());
+    PYRO_CU(launch_pdl(k_roll, dim3(1), dim3(1), 0, st, S));
+    PYRO_CU(tick());
+    PYRO_CU(launch_pdl(k_apply_dot<MetaMask>, vb, vt, 0, st, cells_of(d), ih2,
+                       (const float*)p.as<float>(), mk, mg->bc_mode, q.as<float>(), S));
+    PYRO_CU(tick());
+    PYRO_CU(launch_pdl(k_update_xr<MetaMask>, vb, vt, 0, st, cells_of(d), mk, (float*)nullptr,
+                       r.as<float>(), (const float*)p.as<float>(), (const float*)q.as<float>(),
+                       S, (const CgCtl*)C));
+    PYRO_CU(tick());
+  }
+  PYRO_CU(cudaStreamSynchronize(st));
+  PYRO_CU(timer.read(ms, launches));
+  return PYRO_OK;
+}
+
 int Solver::solve(cudaStream_t st, float* phi, const float* b, int mode, float tol,
                   int max_iters, PyroSolveInfo* info) {
   PYRO_REQUIRE(mode >= PYRO_SOLVER_VCYCLE && mode <= PYRO_SOLVER_MGPCG_LEARNED,
@@ -1099,6 +1182,26 @@ int pyro_poisson_solve(PyroPoisson* ps, const float* b, float* phi, int mode, fl
   clear_error();
   PYRO_REQUIRE(ps && b && phi && info, "pyro_poisson_solve: null argument");
   return ps->solver.solve(ps->stream, phi, b, mode, tol, max_iters, info);
+}
+
+int pyro_poisson_profile_cg(PyroPoisson* ps, const float* b, float* phi, int mode, int iters,
+                            float* ms_out, int* launches_out, int n) {
+  clear_error();
+  PYRO_REQUIRE(ps && b && phi && ms_out && launches_out && n >= 0,
+               "pyro_poisson_profile_cg: null argument");
+  PYRO_REQUIRE(mode == PYRO_SOLVER_MGPCG || mode == PYRO_SOLVER_MGPCG_BF16,
+               "pyro_poisson_profile_cg: mode must be PYRO_SOLVER_MGPCG or _BF16");
+  PYRO_REQUIRE(iters >= 1 && iters <= 1000, "pyro_poisson_profile_cg: iters must be 1..1000");
+  float ms[MG_CLASSES];
+  int cnt[MG_CLASSES];
+  int rc = ps->solver.profile_cg(ps->stream, phi, b, mode == PYRO_SOLVER_MGPCG_BF16, iters, ms,
+                                 cnt);
+  if (rc != PYRO_OK) return rc;
+  for (int i = 0; i < n && i < MG_CLASSES; i++) {
+    ms_out[i] = ms[i];
+    launches_out[i] = cnt[i];
+  }
+  return PYRO_OK;
 }
 
 int pyro_poisson_set_net(PyroPoisson* ps, PyroNet* net) {

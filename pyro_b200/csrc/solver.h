@@ -63,6 +63,12 @@ struct Solver {
   // PYRO_E_NOCONV (info filled either way) or an error.
   int solve(cudaStream_t st, float* phi, const float* b, int mode, float tol, int max_iters,
             PyroSolveInfo* info);
+  // `iters` CG iterations of mode PYRO_SOLVER_MGPCG or _BF16 from phi, one
+  // launch at a time with an event after each (no graph, no convergence
+  // test), credited to the launch classes of MgTimer; ms / launches per
+  // class out.  phi is updated like a solve's iterations update it.
+  int profile_cg(cudaStream_t st, float* phi, const float* b, bool bf16, int iters, float* ms,
+                 int* launches);
 
  private:
   cudaError_t precond(cudaStream_t st, bool bf16, bool prep);
@@ -80,6 +86,8 @@ struct Solver {
   int begin_cg(cudaStream_t st, float* phi, const float* b);
   // fa from the current flag field, whose hash is h
   int update_reach(cudaStream_t st, unsigned long long h);
+  // BF16 storage of every preconditioner level (allocated once)
+  int alloc_bf16_levels();
   // Enqueue CG iterations from r (p = z first) until the recursive residual
   // meets tol, the count reaches max_it or the iteration stalls.
   int cg_loop(cudaStream_t st, float* phi, bool bf16, double bb2, float tol, int it0,

@@ -64,6 +64,19 @@ class PoissonSolver:
             _abi.check("pyro_poisson_solve", rc)
         return info
 
+    def profile_cg(self, b_dev_ptr: int, phi_dev_ptr: int, mode: int, iters: int) -> dict:
+        """Device time and step count per launch class of `iters` CG
+        iterations run one launch at a time (pyro_poisson_profile_cg);
+        phi is updated in place."""
+        n = len(_abi.CG_CLASSES)
+        ms = (ctypes.c_float * n)()
+        cnt = (ctypes.c_int * n)()
+        _abi.check("pyro_poisson_profile_cg", self._lib.pyro_poisson_profile_cg(
+            self._h, ctypes.c_void_p(b_dev_ptr), ctypes.c_void_p(phi_dev_ptr), mode, iters, ms,
+            cnt, n))
+        return {k: {"ms": float(ms[i]), "steps": int(cnt[i])}
+                for i, k in enumerate(_abi.CG_CLASSES)}
+
     def set_net(self, net) -> None:
         """Network for mode SOLVER_MGPCG_LEARNED (None detaches); the
         caller keeps `net` alive while it is attached."""

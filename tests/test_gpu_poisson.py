@@ -165,6 +165,43 @@ def test_bf16_single_level_preconditioner_converges(lib, bc_mode):
     lib.pyro_poisson_destroy(ps)
 
 
+@pytest.mark.parametrize("mode", [_abi.SOLVER_MGPCG, _abi.SOLVER_MGPCG_BF16])
+def test_cg_profile_runs_the_solve_iterations(lib, mode):
+    """pyro_poisson_profile_cg runs the iterations of a solve one launch at
+    a time: k iterations from phi = 0 reach the residual the solve reports
+    after k iterations (the same kernels, only the scheduling differs; the
+    FP64 sums are in a fixed order), and the step counts per class follow
+    the hierarchy (64^3, 32^3, 16^3 smoothed, 8^3 solved directly: per
+    iteration 2 x 2 x 2 level-0 passes, 4 x 2 x 2 per coarser level, one
+    restriction and prolongation per smoothed level, one direct solve, 5 CG
+    vector kernels)."""
+    dims = (64, 64, 64)
+    f, b = _case(*dims, 3)
+    h = 0.02
+    ps = _solver(lib, dims, h, f)
+    bd = dev(b)
+    info = _abi.PyroSolveInfo()
+    pd = dev(np.zeros_like(b))
+    rc = lib.pyro_poisson_solve(ps, ptr(bd), ptr(pd), mode, 1e-12, 4, ctypes.byref(info))
+    assert rc == _abi.PYRO_E_NOCONV and info.iterations == 4
+    want = host(pd)
+    pp = dev(np.zeros_like(b))
+    n = len(_abi.CG_CLASSES)
+    ms, cnt = (ctypes.c_float * n)(), (ctypes.c_int * n)()
+    assert lib.pyro_poisson_profile_cg(ps, ptr(bd), ptr(pp), mode, 4, ms, cnt, n) == 0, \
+        lib.pyro_last_error()
+    assert np.array_equal(host(pp), want)
+    steps = dict(zip(_abi.CG_CLASSES, list(cnt)))
+    nmid = 2  # 32^3 and 16^3
+    assert steps["mg_pass_l0"] == 4 * 8
+    assert steps["mg_pass_mid"] == 4 * 16 * nmid
+    assert steps["mg_restrict_l0"] == 4 and steps["mg_prolong_l0"] == 4
+    assert steps["mg_restrict_mid"] == 4 * nmid and steps["mg_prolong_mid"] == 4 * nmid
+    assert steps["mg_coarse"] == 4 and steps["cg_vector"] == 4 * 5
+    assert all(ms[i] >= 0.0 for i in range(n)) and sum(ms) > 0.0
+    lib.pyro_poisson_destroy(ps)
+
+
 @pytest.mark.parametrize("dims", [(160, 320, 160), (150, 365, 150)])
 @pytest.mark.parametrize("mode", [_abi.SOLVER_MGPCG, _abi.SOLVER_MGPCG_BF16])
 def test_mgpcg_at_the_2cm_pool_shapes(lib, dims, mode):
