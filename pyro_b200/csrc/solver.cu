@@ -139,6 +139,28 @@ inline Cells cells_of(Dims3 d) {
 #define CELL_LOOP(i) \
   for (int i = blockIdx.x * VT + threadIdx.x; i < c.n; i += gridDim.x * VT)
 
+// The thread's cells of the grid-stride loop in order, CG_U at a time: the
+// loads of a group (ld(cell, slot)) are all issued before any is used
+// (use(cell, slot)), so a thread keeps CG_U cells' loads in flight instead
+// of one.  The order of the cells, and so of any per-thread sum, is the
+// plain loop's.
+constexpr int CG_U = 4;
+template <typename LD, typename USE>
+__device__ __forceinline__ void cells_grouped(const Cells& c, LD ld, USE use) {
+  const int s = gridDim.x * VT;
+  int i = blockIdx.x * VT + threadIdx.x;
+  for (; i + (CG_U - 1) * s < c.n; i += CG_U * s) {
+#pragma unroll
+    for (int u = 0; u < CG_U; u++) ld(i + u * s, u);
+#pragma unroll
+    for (int u = 0; u < CG_U; u++) use(i + u * s, u);
+  }
+  for (; i < c.n; i += s) {
+    ld(i, 0);
+    use(i, 0);
+  }
+}
+
 // (A v)_i = (sum fluid nbrs v - cnt v_i) / h^2, 0 in solids; evaluated in
 // FP64 so residuals near 1e-6 of |b| are not lost to cancellation.  The
 // fluid neighbours are added in the order +x, -x, +y, -y, +z, -z and cnt
@@ -297,15 +319,24 @@ __global__ void __launch_bounds__(VT) k_update_xr(Cells c, M mk, float* phi_arg,
   const float alpha = s_alpha;
   float* __restrict__ phi = phi_arg ? phi_arg : ctl->x;
   double rr = 0.0;
-  CELL_LOOP(i) {
-    const uint32_t raw = mk.load(i);
-    const float pi = p[i], qi = q[i], r0 = r[i], xi = phi[i];
-    if (mk.solid(raw)) continue;
-    phi[i] = xi + alpha * pi;
-    float ri = r0 - alpha * qi;
-    r[i] = ri;
-    rr += (double)ri * (double)ri;
-  }
+  uint32_t raw[CG_U];
+  float pv[CG_U], qv[CG_U], rv[CG_U], xv[CG_U];
+  cells_grouped(
+      c,
+      [&](int i, int u) {
+        raw[u] = mk.load(i);
+        pv[u] = p[i];
+        qv[u] = q[i];
+        rv[u] = r[i];
+        xv[u] = phi[i];
+      },
+      [&](int i, int u) {
+        if (mk.solid(raw[u])) return;
+        phi[i] = xv[u] + alpha * pv[u];
+        const float ri = rv[u] - alpha * qv[u];
+        r[i] = ri;
+        rr += (double)ri * (double)ri;
+      });
   block_add_d(sh, rr, sc, SC_RR);
 }
 
@@ -319,13 +350,21 @@ __global__ void __launch_bounds__(VT) k_dots(Cells c, M mk, const float* __restr
   pdl_wait();
   __shared__ double sh[32];
   double zr = 0.0, zq = 0.0;
-  CELL_LOOP(i) {
-    const uint32_t raw = mk.load(i);
-    const float zi = zv[i], ri = r[i], qi = q ? q[i] : 0.0f;
-    if (mk.solid(raw)) continue;
-    zr += (double)zi * (double)ri;
-    if (q) zq += (double)zi * (double)qi;
-  }
+  uint32_t raw[CG_U];
+  float zv_[CG_U], rv[CG_U], qv[CG_U];
+  cells_grouped(
+      c,
+      [&](int i, int u) {
+        raw[u] = mk.load(i);
+        zv_[u] = zv[i];
+        rv[u] = r[i];
+        qv[u] = q ? q[i] : 0.0f;
+      },
+      [&](int, int u) {
+        if (mk.solid(raw[u])) return;
+        zr += (double)zv_[u] * (double)rv[u];
+        if (q) zq += (double)zv_[u] * (double)qv[u];
+      });
   block_add_d(sh, zr, sc, SC_RZN);
   if (q) block_add_d(sh, zq, sc, SC_ZQ);
 }
@@ -348,15 +387,16 @@ __global__ void __launch_bounds__(VT) k_update_p(Cells c, M mk, float* __restric
   __syncthreads();
   const float beta = s_beta;
   const bool first = s_first != 0;
-  CELL_LOOP(i) {
-    const uint32_t raw = mk.load(i);
-    const float zi = zv[i], pi = first ? 0.0f : p[i];
-    if (mk.solid(raw)) {
-      p[i] = 0.0f;
-      continue;
-    }
-    p[i] = first ? zi : zi + beta * pi;
-  }
+  uint32_t raw[CG_U];
+  float zv_[CG_U], pv[CG_U];
+  cells_grouped(
+      c,
+      [&](int i, int u) {
+        raw[u] = mk.load(i);
+        zv_[u] = zv[i];
+        pv[u] = first ? 0.0f : p[i];
+      },
+      [&](int i, int u) { p[i] = mk.solid(raw[u]) ? 0.0f : (first ? zv_[u] : zv_[u] + beta * pv[u]); });
 }
 
 // End of one CG iteration on the device: count it and let the loop's

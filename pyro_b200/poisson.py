@@ -121,6 +121,9 @@ def main(argv=None) -> None:
     ap.add_argument("--tol", type=float, default=1e-4)
     ap.add_argument("--iters", type=int, default=1, help="V-cycles, or CG iterations at most")
     ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--profile", action="store_true",
+                    help="after the solves, run --iters CG iterations one launch at a time "
+                         "(pyro_poisson_profile_cg) and print device time per launch class")
     a = ap.parse_args(argv)
     f, b = poisson_case(a.n, a.n, a.n, seed=1)
     fd, bd = torch.from_numpy(f).cuda(), torch.from_numpy(b).cuda()
@@ -133,8 +136,14 @@ def main(argv=None) -> None:
         info = ps.solve(bd.data_ptr(), phi.data_ptr(), MODES[a.mode], a.tol, a.iters,
                         allow_cap=True)
     torch.cuda.synchronize()
-    print(json.dumps({"n": a.n, "mode": a.mode, "iterations": info.iterations,
-                      "rel_resid": info.rel_resid, "ms": info.ms}))
+    out = {"n": a.n, "mode": a.mode, "iterations": info.iterations,
+           "rel_resid": info.rel_resid, "ms": info.ms}
+    if a.profile:
+        if a.mode not in ("mgpcg", "mgpcg_bf16"):
+            raise SystemExit("--profile needs --mode mgpcg or mgpcg_bf16")
+        phi.zero_()
+        out["profile"] = ps.profile_cg(bd.data_ptr(), phi.data_ptr(), MODES[a.mode], a.iters)
+    print(json.dumps(out))
     ps.close()
 
 
