@@ -124,7 +124,7 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* mbar, uint32_t bytes) {
                : "memory");
 }
 
-// TMA tiled loads global -> shared (no multicast), completing on `mbar`.
+// TMA tiled loads global -> this CTA's shared memory, completing on `mbar`.
 // Coordinates are element indices, innermost first; out-of-range boxes are
 // zero-filled.  The innermost coordinate times the element size must be a
 // multiple of 16 bytes.
