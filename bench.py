@@ -464,6 +464,7 @@ def sim_solver_bench(sim):
     b16 = res.get("mgpcg_bf16_to_1e-4")
     if b16:
         phi = torch.zeros_like(bd)
+        torch.cuda.synchronize()  # the solver's stream does not wait for torch's
         k = max(int(b16["iterations"]), 1)
         prof = ps.profile_cg(bd.data_ptr(), phi.data_ptr(), _abi.SOLVER_MGPCG_BF16, k)
         cg_classes = {c: {"ms_per_iteration": round(v["ms"] / k, 4),

@@ -279,7 +279,9 @@ int pyro_poisson_create(uint32_t nx, uint32_t ny, uint32_t nz, float h,
  * flags. */
 int pyro_poisson_set_flags(PyroPoisson* ps, const uint32_t* flags);
 /* Solve in place: phi (device float * N) is the initial guess and the
- * result; b (device float * N) the right-hand side. */
+ * result; b (device float * N) the right-hand side.  The solve runs on the
+ * solver's own stream (pyro_poisson_stream), which does not wait for other
+ * streams: b, phi and the flags must be written before the call. */
 int pyro_poisson_solve(PyroPoisson* ps, const float* b, float* phi, int mode,
                        float tol, int max_iters, PyroSolveInfo* info);
 int pyro_poisson_stream(PyroPoisson* ps, void** stream);

@@ -714,7 +714,8 @@ int pyro_net_create(uint64_t seed, PyroNet** out) {
     std::normal_distribution<double> nd(0.0, sd);
     for (size_t i = n->w_off[l]; i < n->w_off[l + 1]; i++) p[i] = (float)nd(rng);
   }
-  if (cudaMemcpy(n->master.p, p.data(), n->n_params * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+  if (cudaMemcpyAsync(n->master.p, p.data(), n->n_params * 4, cudaMemcpyHostToDevice,
+                      n->stream) != cudaSuccess) {
     delete n;
     set_error("pyro_net_create: upload failed");
     return PYRO_E_CUDA;
@@ -762,9 +763,11 @@ int pyro_net_set_params(PyroNet* n, const float* host, uint64_t count, float out
   PYRO_REQUIRE(std::isfinite(out_scale) && out_scale > 0.0f,
                "pyro_net_set_params: out_scale must be positive");
   PYRO_CU(cudaStreamSynchronize(n->stream));
-  PYRO_CU(cudaMemcpy(n->master.p, host, count * 4, cudaMemcpyHostToDevice));
-  PYRO_CU(cudaMemset(n->adam_m.p, 0, n->adam_m.bytes));
-  PYRO_CU(cudaMemset(n->adam_v.p, 0, n->adam_v.bytes));
+  // on the network's stream, so the conversion below reads the new weights
+  // (a pageable cudaMemcpy may still be in flight when it returns)
+  PYRO_CU(cudaMemcpyAsync(n->master.p, host, count * 4, cudaMemcpyHostToDevice, n->stream));
+  PYRO_CU(cudaMemsetAsync(n->adam_m.p, 0, n->adam_m.bytes, n->stream));
+  PYRO_CU(cudaMemsetAsync(n->adam_v.p, 0, n->adam_v.bytes, n->stream));
   k_to_bf16<<<blocks_for(n->n_w), NT, 0, n->stream>>>(n->master.as<float>(), n->n_w,
                                                       n->wbf.as<bf16>());
   PYRO_CU(cudaGetLastError());

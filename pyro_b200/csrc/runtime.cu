@@ -23,7 +23,11 @@ int DevBuf::alloc(size_t n) {
     return e == cudaErrorMemoryAllocation ? PYRO_E_NOMEM : PYRO_E_CUDA;
   }
   bytes = n;
+  // The zero fill runs on the default stream, which the library's own
+  // (non-blocking) streams do not wait for: it must be finished before any
+  // of them touches the buffer.
   e = cudaMemset(p, 0, n);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(0);
   if (e != cudaSuccess) {
     set_error(std::string("cudaMemset: ") + cudaGetErrorString(e));
     return PYRO_E_CUDA;

@@ -142,6 +142,7 @@ def main(argv=None) -> None:
         if a.mode not in ("mgpcg", "mgpcg_bf16"):
             raise SystemExit("--profile needs --mode mgpcg or mgpcg_bf16")
         phi.zero_()
+        torch.cuda.synchronize()
         out["profile"] = ps.profile_cg(bd.data_ptr(), phi.data_ptr(), MODES[a.mode], a.iters)
     print(json.dumps(out))
     ps.close()
